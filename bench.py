@@ -1,0 +1,321 @@
+#!/usr/bin/env python3
+"""Benchmark of the MIMICA dynamical-core path on B200.
+
+Metric: Mcell-updates/s = interior cells x integrator steps / time / 1e6, one
+"step" = one full integrator step of the reference's scheme (two Heun stages,
+each: scalar advection of density + 5 density-weighted scalars, momentum
+advection/pgf/buoyancy, stage update, anelastic projection).
+
+Workload (default): the shallow-cumulus-like domain, 512 x 512 x 256 interior cells,
+dx = dy = 25 m, stretched dz (10 m -> 100 m), 3 momentum + density + 5 scalars
+(theta_l, qt, qr, nr, aerosol number), scalar scheme WENO (the reference's
+WENO3-switch), FD4 momentum, dt = 1 s, plain FP64 form.  Synthetic seeded inputs
+(no dataset exists for this benchmark); the working set (~16 GB) exceeds the
+126 MB L2, so no flush is needed between timed steps.
+
+`python bench.py --gpus N --steps K --warmup W` prints one JSON line.
+`--impl reference` times the reference's algorithm on the host cores instead
+(the CPU restatement, OpenMP over all cores, bounded sample).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    except Exception:
+        return PEAKS_FALLBACK, "fallback"
+
+
+# ---------------- algorithmic bytes (FP64 state), per interior cell ----------------
+def alg_bytes(nf_scalar: int, nsubp: int) -> dict:
+    """Minimal HBM traffic per interior cell of each kernel group (bytes).
+
+    K1 (all scalar fields incl. density), per launch averaged over the two stages:
+      stage 1: per field read psi_n, write psi*, T (24 B); momentum 24 B; two buoyancy
+               stage tendencies written (16 B)
+      stage 2: per field read psi*, psi_n, T, write psi_new (32 B); momentum 24 B; 16 B
+    K2 (momentum), per launch: stage 1: read m_n (24), p (8), dens/es/qt + their stage
+      tendencies (40), write m*, T (48); stage 2: read m*, m_n, T (72), p 8, 40, write m_new 24.
+    Projection pass (FP64 spectra, half spectrum ~8 B/cell per complex plane):
+      fft_x_fwd_div: read momentum 24, write spectrum 8; y/tridiag/y/x_inv: 4 x (8+8);
+      correction: read dp 8, m 24, p 8, write m 24, p 8.
+    """
+    f = nf_scalar
+    k1 = (f * 24 + 24 + 16 + f * 32 + 24 + 16) / 2.0
+    k2 = ((24 + 8 + 40 + 48) + (72 + 8 + 40 + 24)) / 2.0
+    proj = 32 + 64 + 72
+    step = 2 * (k1 + k2) + 2 * nsubp * proj
+    return {"k1_scalar_advection": k1, "k2_momentum": k2, "fft_x_fwd_div": 32.0,
+            "fft_y_tridiag_fft_y_fft_x_inv": 64.0, "correction_halo": 72.0, "step": step}
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def pinned_like(shape):
+    """numpy array in page-locked host memory (cudaMallocHost)."""
+    rt = C.CDLL("libcudart.so")
+    n = int(np.prod(shape)) * 8
+    p = C.c_void_p()
+    if rt.cudaMallocHost(C.byref(p), C.c_size_t(n)) != 0:
+        return np.zeros(shape)
+    buf = (C.c_double * int(np.prod(shape))).from_address(p.value)
+    return np.frombuffer(buf, dtype=np.float64).reshape(shape)
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def dist_max(x: float, ws: int) -> float:
+    if ws <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference(args, d_full, scheme, nsamp_steps=1, omp=True):
+    """The reference's algorithm timed on the host cores: the CPU restatement, bounded
+    sample = a horizontally reduced domain with the same dz profile, spacing and fields."""
+    from fdd3260_b200 import config
+    from oracle import oracle as O
+    mx = args.cpu_sample_xy
+    d = config.cumulus_domain(mx, mx, d_full.nz, scheme=scheme)
+    st = config.cumulus_state(d, seed=1000, n_extra=3)
+    orc = O.Oracle(d, omp=omp)
+    orc.stepping(st, nsteps=1, ntime0=1)   # warm-up (page faults, OpenMP pool)
+    t0 = time.perf_counter()
+    orc.stepping(st, nsteps=nsamp_steps, ntime0=1)
+    dt = time.perf_counter() - t0
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)) if omp else 1
+    val = d.cells * nsamp_steps / dt / 1e6
+    return val, cores, f"{mx}x{mx}x{d.nz} interior cells, {nsamp_steps} step(s), same dz/dt/fields as the workload"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mimica", choices=["mimica", "reference"])
+    ap.add_argument("--scheme", default="weno", choices=["weno", "ppm", "muscl"])
+    ap.add_argument("--maxx", type=int, default=512)
+    ap.add_argument("--nz", type=int, default=256)
+    ap.add_argument("--cpu-sample-xy", type=int, default=64)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    ws, rank, local = dist_init()
+    from fdd3260_b200 import Mimica, config
+    d = config.cumulus_domain(args.maxx, args.maxx, args.nz, scheme=args.scheme)
+    metric = "Mcell-updates/s per integrator step (2-stage Heun + projection)"
+    cfg = {"workload": f"shallow-cumulus domain {args.maxx}x{args.maxx}x{args.nz}, dx=dy=25 m, stretched dz 10->100 m, "
+                       f"3 momentum + density + 5 scalars, {args.scheme.upper()} (reference scheme), FD4 momentum, "
+                       f"dt=1 s, nsubp=1",
+           "form": "plain FP64", "scheme": args.scheme, "interior_cells": d.cells,
+           "l2": "inputs larger than L2 (~16 GB working set)", "parallelism": f"replicas x{ws}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        val, cores, sample = cpu_reference(args, d, args.scheme, nsamp_steps=1)
+        vals = [val]
+        for _ in range(max(0, min(args.steps, 2) - 1)):
+            vals.append(cpu_reference(args, d, args.scheme, nsamp_steps=1)[0])
+        v = statistics.median(vals)
+        line = {"impl": "reference", "metric": metric, "value": v, "unit": "Mcell-updates/s", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": d.cells / v / 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded)", "config": cfg,
+                "cpu_baseline": {"value": v, "unit": "Mcell-updates/s", "cores": cores, "kind": "port", "sample": sample},
+                "e2e": {"value": v, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    st = config.cumulus_state(d, seed=1000 + rank, n_extra=3)
+    m = Mimica(d, nscal=len(st.scal), iqt=st.iqt, device=local if ws > 1 else 0)
+    m.upload(st)
+    L = m._L
+    use_graph = not args.no_graph
+    # warm-up
+    m.stepping(args.warmup, ntime0=1, graph=use_graph)
+    m.synchronize()
+    # timed region (device time, CUDA events on the library stream), clocks sampled meanwhile
+    dist_barrier(ws)
+    ms = C.c_double(0.0)
+    with ClockSampler(local) as clk:
+        rc = L.mg_time_steps(m._h, args.steps, 1 + args.warmup, 1 if use_graph else 0, C.byref(ms))
+    if rc:
+        raise RuntimeError(f"mg_time_steps failed: {rc}")
+    t_ms = dist_max(ms.value, ws)
+    per_rank_rate = d.cells * args.steps / (t_ms / 1e3) / 1e6
+    value = per_rank_rate * ws
+    launches_per_step = m.launches_per_call
+
+    # per-kernel device times (separate eager pass, events around each launch group)
+    L.mg_profile_enable(m._h, 1)
+    nprof = 2
+    m.stepping(nprof, ntime0=1 + args.warmup + args.steps)
+    buf = C.create_string_buffer(8192)
+    L.mg_profile_report(m._h, buf, 8192)
+    L.mg_profile_enable(m._h, 0)
+    kern = {}
+    for ln in buf.value.decode().splitlines():
+        name, n, tot = ln.split()
+        kern[name] = {"launches": int(n), "total_ms": float(tot)}
+    ab = alg_bytes(1 + len(st.scal), d.nsubp)
+    pk, pk_src = peaks()
+    dom = max((k for k in kern if k in ab), key=lambda k: kern[k]["total_ms"])
+    avg_ms = kern[dom]["total_ms"] / kern[dom]["launches"]
+    alg = ab[dom] * d.cells
+    achieved = alg / (avg_ms / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_source": pk_src,
+            "algorithmic_bytes_per_cell": ab[dom], "avg_launch_ms": avg_ms,
+            "step_alg_bytes_per_cell": ab["step"],
+            "step_frac": ab["step"] * d.cells * args.steps / (t_ms / 1e3) / 1e9 / pk["hbm_gbs"]}
+    kshare = {k: round(v["total_ms"] / sum(x["total_ms"] for x in kern.values()), 4) for k, v in kern.items()}
+
+    # end-to-end through the public API with pinned host buffers: upload state, one step, download state
+    host = {n: pinned_like(d.shape) for n in ("u", "v", "w", "p", "dens")}
+    hscal = [pinned_like(d.shape) for _ in st.scal]
+    for n in ("u", "v", "w", "p", "dens"):
+        host[n][...] = getattr(st, n)
+    for a, b in zip(hscal, st.scal):
+        a[...] = b
+    hstate = config.State(host["u"], host["v"], host["w"], host["p"], host["dens"], hscal, st.iqt)
+    m.upload(hstate)
+    m.stepping(1, ntime0=1)
+    m.synchronize()
+    dist_barrier(ws)
+    t0 = time.perf_counter()
+    for s in range(args.e2e_steps):
+        m.upload(hstate)
+        m.stepping(1, ntime0=2 + s)
+        out = m.download()
+        hstate = out
+    m.synchronize()
+    e2e_s = dist_max(time.perf_counter() - t0, ws)
+    e2e_val = d.cells * args.e2e_steps * ws / e2e_s / 1e6
+    nbytes = (5 + len(st.scal)) * d.nx * d.ny * d.nz * 8
+
+    cpu = None
+    if rank == 0 and not args.skip_cpu:
+        try:
+            v, cores, sample = cpu_reference(args, d, args.scheme, nsamp_steps=1)
+            cpu = {"value": v, "unit": "Mcell-updates/s", "cores": cores, "kind": "port", "sample": sample}
+        except Exception as e:  # pragma: no cover
+            cpu = {"value": None, "unit": "Mcell-updates/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {"metric": metric, "value": value, "unit": "Mcell-updates/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)", "config": cfg,
+                "clocks": clk.summary(), "gpu_launches": launches_per_step * args.steps,
+                "e2e": {"value": e2e_val, "unit": "Mcell-updates/s", "h2d_bytes_per_step": nbytes,
+                        "d2h_bytes_per_step": nbytes, "timing": "host wall clock, synchronised, pinned buffers"},
+                "roofline": roof, "kernel_share": kshare, "cpu_baseline": cpu,
+                "graph": use_graph, "device_bytes": m.device_bytes}
+        print(json.dumps(line), flush=True)
+    m.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,112 @@
+"""ctypes binding of ``libmimica_gpu.so`` (the C ABI declared in include/mimica_gpu.h).
+
+The library is built in-tree by ``fdd3260_b200/build.py``; there is no CPU
+fallback: if the shared library is missing or fails to load, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmimica_gpu.so")
+
+# status codes (mimica_gpu.h)
+MG_OK, MG_ERR_PARAM, MG_ERR_CUDA, MG_ERR_NAN, MG_ERR_PIVOT, MG_ERR_TIMEOUT, MG_ERR_NOMEM, MG_ERR_STATE = range(8)
+MG_WENO, MG_PPM, MG_MUSCL = 0, 1, 2
+MG_LIM_MINMOD, MG_LIM_VL, MG_LIM_MC, MG_LIM_DEFAULT = 0, 1, 2, 3
+MG_PREC_FP64, MG_PREC_MIXED = 0, 1
+
+SCHEMES = {"weno": MG_WENO, "ppm": MG_PPM, "muscl": MG_MUSCL}
+LIMITERS = {"minmod": MG_LIM_MINMOD, "VL": MG_LIM_VL, "MC": MG_LIM_MC, "default": MG_LIM_DEFAULT}
+
+_dp = C.POINTER(C.c_double)
+
+
+class MgParams(C.Structure):
+    _fields_ = [
+        ("maxx", C.c_int), ("maxy", C.c_int), ("nz", C.c_int), ("nscal", C.c_int), ("iqt", C.c_int),
+        ("scal_adv", C.c_int), ("muscl_limiter", C.c_int), ("mom_ord", C.c_int), ("lavisc", C.c_int),
+        ("nsubp", C.c_int), ("with_buoy", C.c_int), ("precision", C.c_int), ("refine_iters", C.c_int),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double), ("dt0", C.c_double),
+        ("lim_tol", C.c_double), ("u0shift", C.c_double), ("v0shift", C.c_double), ("refine_tol", C.c_double),
+        ("fdz0", _dp), ("dzw", _dp), ("dz1w", _dp), ("dz1", _dp),
+        ("den0", _dp), ("avden0", _dp), ("stab0", _dp), ("pt0", _dp), ("qv0", _dp),
+    ]
+
+
+class MimicaError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        super().__init__(f"{where}: {error_string(code)} (code {code})")
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load the CUDA library (raises if it is not built or cannot be loaded)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python fdd3260_b200/build.py` (no CPU fallback exists)")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.mg_error_string.restype = C.c_char_p
+        L.mg_error_string.argtypes = [C.c_int]
+        L.mg_version.restype = C.c_int
+        L.mg_grid_metrics.argtypes = [C.c_int, C.c_double, _dp, _dp, _dp, _dp]
+        L.mg_base_state.argtypes = [C.c_int, C.c_double, C.c_double, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.mg_get_wv.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _dp]
+        L.mg_create.argtypes = [C.POINTER(MgParams), C.c_int, C.POINTER(vp)]
+        L.mg_destroy.argtypes = [vp]
+        L.mg_device_bytes.restype = C.c_size_t
+        L.mg_device_bytes.argtypes = [vp]
+        L.mg_last_launch_count.argtypes = [vp]
+        L.mg_upload_state.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, C.POINTER(_dp)]
+        L.mg_download_state.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, C.POINTER(_dp)]
+        L.mg_upload_state_device.argtypes = [vp, vp, vp, vp, vp, vp, C.POINTER(vp)]
+        L.mg_download_state_device.argtypes = [vp, vp, vp, vp, vp, vp, C.POINTER(vp)]
+        L.mg_step.argtypes = [vp, C.c_int, C.c_int, _dp, _dp]
+        L.mg_step_graph.argtypes = [vp, C.c_int, C.c_int, _dp, _dp]
+        L.mg_synchronize.argtypes = [vp]
+        L.mg_advection_ac.argtypes = [vp, _dp, _dp, _dp, _dp, _dp]
+        L.mg_qnadv_uvw.argtypes = [vp, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.mg_fft_solve.argtypes = [vp, _dp, _dp]
+        L.mg_anelastic_pressure.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.mg_time_steps.argtypes = [vp, C.c_int, C.c_int, C.c_int, _dp]
+        L.mg_profile_enable.argtypes = [vp, C.c_int]
+        L.mg_profile_report.argtypes = [vp, C.c_char_p, C.c_size_t]
+        _lib = L
+    return _lib
+
+
+def error_string(code: int) -> str:
+    try:
+        return lib().mg_error_string(code).decode()
+    except Exception:  # library not loadable: still produce a message
+        return f"error {code}"
+
+
+def check(rc: int, where: str) -> None:
+    if rc != MG_OK:
+        raise MimicaError(rc, where)
+
+
+def ptr(a: np.ndarray | None):
+    """double* of a C-contiguous float64 numpy array (or NULL)."""
+    if a is None:
+        return None
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("arrays must be C-contiguous float64")
+    return a.ctypes.data_as(_dp)
+
+
+EXPORTED = [
+    "mg_error_string", "mg_version", "mg_grid_metrics", "mg_base_state", "mg_get_wv", "mg_create", "mg_destroy",
+    "mg_device_bytes", "mg_upload_state", "mg_download_state", "mg_upload_state_device", "mg_download_state_device",
+    "mg_step", "mg_step_graph", "mg_synchronize", "mg_last_launch_count", "mg_advection_ac", "mg_qnadv_uvw",
+    "mg_fft_solve", "mg_anelastic_pressure", "mg_time_steps", "mg_profile_enable", "mg_profile_report",
+]

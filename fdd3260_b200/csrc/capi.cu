@@ -1,0 +1,688 @@
+// capi.cu -- the C ABI of include/mimica_gpu.h: context, resident state, the Heun
+// step driver and the unit-level entry points.
+//
+// Step structure (src/INTEG/time_step.f90 stepping :76-334, dynamics subset):
+//   for each of the two stages (a,b) = (1,0), (1/2,1)  (INCLUDE/integ.h):
+//     K1  scalars + density: advection, tend = F + b*tend, psi = psi_n + a*dt*tend
+//     K2  momentum: -grad p, buoyancy, advection, tend, m = m_n + a*dt*tend
+//     projection: nsubp x (rhs -> FFT -> tridiagonal -> inverse FFT -> correction),
+//                 cal_p1
+// Buffers: level-n (A), stage working (B), tendencies; the density has a third
+// buffer because every scalar's stage-2 update reads the level-n density.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <new>
+#include <vector>
+
+#include "mg_common.cuh"
+#include "mimica_gpu.h"
+
+struct mg_ctx {
+    mg_params prm;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    DevGrid G{};
+    int nf = 0;                          // 1 (density) + nscal
+    double *prof = nullptr;              // 9 profiles x nz
+    std::vector<double> wv;
+    size_t fbytes = 0;                   // bytes per field
+    double *mA[3] = {}, *mB[3] = {}, *tm[3] = {};
+    double *p = nullptr;
+    double *sA[MG_MAXF] = {}, *sB[MG_MAXF] = {}, *ts[MG_MAXF] = {};
+    double *dens3 = nullptr;
+    double *fes = nullptr, *fqt = nullptr;
+    double *unit[8] = {};                // scratch of the unit-level entry points
+    PressurePlan *pp = nullptr;
+    int rep = REP_NAT;
+    int have_state = 0;
+    int launches = 0;
+    size_t bytes = 0;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    int gsteps[2] = {0, 0};
+    // per-kernel profiling (CUDA events on the context stream)
+    int prof_on = 0;
+    struct Ev { const char *name; cudaEvent_t a, b; };
+    std::vector<Ev> evs;
+    std::vector<cudaEvent_t> pool;
+    struct Acc { const char *name; double ms; long long n; };
+    std::vector<Acc> acc;
+};
+
+static cudaEvent_t ev_get(mg_ctx *c)
+{
+    if (!c->pool.empty()) { cudaEvent_t e = c->pool.back(); c->pool.pop_back(); return e; }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+// wrap one launch: records events around it when profiling is on
+#define PROF(c, nm, call) do {                                              \
+        cudaEvent_t ea_ = nullptr, eb_ = nullptr;                          \
+        if ((c)->prof_on) { ea_ = ev_get(c); cudaEventRecord(ea_, (c)->stream); } \
+        cudaError_t pe_ = (call);                                          \
+        if ((c)->prof_on) { eb_ = ev_get(c); cudaEventRecord(eb_, (c)->stream); \
+                            (c)->evs.push_back({nm, ea_, eb_}); }          \
+        if (pe_ != cudaSuccess) return pe_;                                \
+    } while (0)
+
+static void prof_collect(mg_ctx *c)
+{
+    if (c->evs.empty()) return;
+    cudaStreamSynchronize(c->stream);
+    for (auto &e : c->evs) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e.a, e.b);
+        bool found = false;
+        for (auto &a : c->acc)
+            if (!strcmp(a.name, e.name)) { a.ms += ms; a.n++; found = true; break; }
+        if (!found) c->acc.push_back({e.name, (double)ms, 1});
+        c->pool.push_back(e.a);
+        c->pool.push_back(e.b);
+    }
+    c->evs.clear();
+}
+
+static int cuerr(cudaError_t e) { return e == cudaSuccess ? MG_OK : (e == cudaErrorMemoryAllocation ? MG_ERR_NOMEM : MG_ERR_CUDA); }
+#define CKR(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return cuerr(e_); } while (0)
+
+extern "C" const char *mg_error_string(int code)
+{
+    switch (code) {
+    case MG_OK: return "ok";
+    case MG_ERR_PARAM: return "invalid or unsupported parameter";
+    case MG_ERR_CUDA: return "CUDA runtime error";
+    case MG_ERR_NAN: return "non-finite value detected";
+    case MG_ERR_PIVOT: return "zero pivot in the vertical tridiagonal solve";
+    case MG_ERR_TIMEOUT: return "bounded device wait timed out";
+    case MG_ERR_NOMEM: return "out of memory";
+    case MG_ERR_STATE: return "call out of order (no state uploaded)";
+    default: return "unknown error";
+    }
+}
+
+extern "C" int mg_version(void) { return 1; }
+
+// ---------------- host precompute ----------------
+extern "C" int mg_grid_metrics(int nz, double dz, const double *fdz, double *dzw, double *dz1w, double *dz1)
+{
+    if (nz < 2 || !fdz || !dzw || !dz1w || !dz1) return MG_ERR_PARAM;
+    for (int k = 0; k < nz; k++) {
+        dzw[k] = dz * fdz[k];
+        dz1w[k] = 1. / (dz * fdz[k]);
+    }
+    for (int k = 0; k < nz - 1; k++) dz1[k] = 1. / ((dz * 0.5) * (fdz[k] + fdz[k + 1]));
+    dz1[nz - 1] = dz1[nz - 2];
+    return MG_OK;
+}
+
+extern "C" int mg_base_state(int nz, double dz, double psurf, const double *fdz0, const double *dz1,
+                             const double *pt0, const double *qv0, double *p0, double *den0, double *avden0, double *stab0)
+{
+    if (nz < 3) return MG_ERR_PARAM;
+    (void)qv0;
+    const double g = 9.81, pref = 100000., cp_a = 1004., cv_a = 716.;
+    const double cpm = cp_a, cvm = cv_a, ex = (cp_a - cv_a) / cp_a;
+    double dsurf;
+    p0[0] = psurf;
+    for (int l = 0; l < 10; l++) {
+        den0[0] = p0[0] / ((cpm - cvm) * pt0[0] * pow(p0[0] / pref, ex));
+        dsurf = psurf / ((cpm - cvm) * pt0[0] * pow(psurf / pref, ex));
+        p0[0] = psurf - g * 0.5 * (dsurf + den0[0]) * 0.5 * dz * fdz0[0];
+    }
+    for (int k = 1; k < nz; k++) {
+        p0[k] = p0[k - 1] - g * den0[k - 1] / dz1[k - 1];
+        for (int l = 0; l < 10; l++) {
+            den0[k] = p0[k] / ((cpm - cvm) * pt0[k] * pow(p0[k] / pref, ex));
+            p0[k] = p0[k - 1] - g * 0.5 * (den0[k - 1] + den0[k]) / dz1[k - 1];
+        }
+    }
+    for (int k = 1; k < nz; k++) avden0[k] = (fdz0[k] * den0[k] + fdz0[k - 1] * den0[k - 1]) / (fdz0[k] + fdz0[k - 1]);
+    avden0[0] = den0[0];
+    for (int k = 1; k < nz - 1; k++)
+        stab0[k] = (den0[k + 1] - den0[k - 1]) / (den0[k] * dz * (0.5 * fdz0[k + 1] + fdz0[k] + 0.5 * fdz0[k - 1]));
+    stab0[0] = (den0[1] - den0[0]) / (den0[0] * 0.5 * dz * (fdz0[1] + fdz0[0]));
+    stab0[nz - 1] = (den0[nz - 1] - den0[nz - 2]) / (den0[nz - 1] * 0.5 * dz * (fdz0[nz - 1] + fdz0[nz - 2]));
+    return MG_OK;
+}
+
+extern "C" int mg_get_wv(int maxx, int maxy, double dx, double dy, double *wv)
+{
+    if (maxx < 1 || maxy < 1 || !wv) return MG_ERR_PARAM;
+    const double pi = 3.14159265;   // the reference's constant, src/TYPES/shared_data.f90:147
+    const int nl = maxx, nm = maxy;
+    for (int l = 1; l <= maxx; l++) {
+        double xl = (l <= nl / 2) ? (double)(l - 1) : (double)(l - nl - 1);
+        for (int m = 1; m <= maxy; m++) {
+            double xm = (m <= nm / 2) ? (double)(m - 1) : (double)(m - nm - 1);
+            double sx = sin(pi * xl / (double)nl), sy = sin(pi * xm / (double)nm);
+            wv[(size_t)(m - 1) * maxx + (l - 1)] = -4. * (sx * sx / (dx * dx) + sy * sy / (dy * dy));
+        }
+    }
+    wv[0] = 1.;
+    return MG_OK;
+}
+
+// ---------------- context ----------------
+static bool good_len(int n)
+{
+    int m = n;
+    for (int r : {2, 3, 5}) while (m % r == 0) m /= r;
+    return m == 1;
+}
+
+static int validate(const mg_params *p)
+{
+    if (!p) return MG_ERR_PARAM;
+    if (p->maxx < 8 || p->maxy < 8 || p->nz < 8) return MG_ERR_PARAM;
+    if (p->maxx % 2 || p->maxy % 2 || !good_len(p->maxx) || !good_len(p->maxy)) return MG_ERR_PARAM;
+    if (p->maxx > 4096 || p->maxy > 4096) return MG_ERR_PARAM;
+    if (p->nscal < 1 || p->nscal + 1 > MG_MAXF) return MG_ERR_PARAM;
+    if (p->iqt >= p->nscal || p->iqt == 0) return MG_ERR_PARAM;
+    if (p->scal_adv < MG_WENO || p->scal_adv > MG_MUSCL) return MG_ERR_PARAM;
+    if (p->muscl_limiter < MG_LIM_MINMOD || p->muscl_limiter > MG_LIM_DEFAULT) return MG_ERR_PARAM;
+    if (p->mom_ord != 2 && p->mom_ord != 4) return MG_ERR_PARAM;
+    if (p->nsubp < 1 || p->nsubp > 16) return MG_ERR_PARAM;
+    if (p->precision != MG_PREC_FP64) return MG_ERR_PARAM;   // the mixed form is not built yet
+    if (!(p->dx > 0) || !(p->dy > 0) || !(p->dz > 0) || !(p->dt0 > 0)) return MG_ERR_PARAM;
+    if (!p->fdz0 || !p->dzw || !p->dz1w || !p->dz1 || !p->den0 || !p->avden0 || !p->stab0 || !p->pt0 || !p->qv0)
+        return MG_ERR_PARAM;
+    return MG_OK;
+}
+
+static void free_ctx(mg_ctx *c)
+{
+    if (!c) return;
+    for (int i = 0; i < 2; i++) if (c->gexec[i]) cudaGraphExecDestroy(c->gexec[i]);
+    for (int i = 0; i < 3; i++) { cudaFree(c->mA[i]); cudaFree(c->mB[i]); cudaFree(c->tm[i]); }
+    for (int f = 0; f < MG_MAXF; f++) { cudaFree(c->sA[f]); cudaFree(c->sB[f]); cudaFree(c->ts[f]); }
+    for (int i = 0; i < 8; i++) cudaFree(c->unit[i]);
+    cudaFree(c->p); cudaFree(c->dens3); cudaFree(c->fes); cudaFree(c->fqt); cudaFree(c->prof);
+    pressure_plan_destroy(c->pp);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+extern "C" int mg_create(const mg_params *params, int device, mg_ctx **out)
+{
+    if (!out) return MG_ERR_PARAM;
+    *out = nullptr;
+    int v = validate(params);
+    if (v) return v;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return MG_ERR_CUDA;
+    if (device < 0 || device >= ndev) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(device));
+    mg_ctx *c = new (std::nothrow) mg_ctx();
+    if (!c) return MG_ERR_NOMEM;
+    c->prm = *params;
+    c->device = device;
+    const int nz = params->nz;
+    DevGrid &G = c->G;
+    G.maxx = params->maxx; G.maxy = params->maxy; G.nz = nz;
+    G.nx = params->maxx + 5; G.ny = params->maxy + 5;
+    G.px = (G.nx + 7) / 8 * 8;
+    G.ps = (long long)G.px * G.ny;
+    G.dx = params->dx; G.dy = params->dy; G.dz = params->dz; G.dt0 = params->dt0;
+    G.lim_tol = params->lim_tol; G.u0shift = params->u0shift; G.v0shift = params->v0shift;
+    G.scal_adv = params->scal_adv; G.muscl_lim = params->muscl_limiter; G.mom_ord = params->mom_ord;
+    G.lavisc = params->lavisc; G.with_buoy = params->with_buoy;
+    c->nf = 1 + params->nscal;
+    c->fbytes = (size_t)G.ps * nz * sizeof(double);
+    int rc = MG_OK;
+    auto fail = [&](int code) { free_ctx(c); return code; };
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(cuerr(e));
+    // profiles
+    e = cudaMalloc(&c->prof, 9 * nz * sizeof(double));
+    if (e != cudaSuccess) return fail(cuerr(e));
+    const double *src[9] = {params->fdz0, params->dzw, params->dz1w, params->dz1, params->den0,
+                            params->avden0, params->stab0, params->pt0, params->qv0};
+    for (int q = 0; q < 9; q++) {
+        e = cudaMemcpy(c->prof + q * nz, src[q], nz * sizeof(double), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return fail(cuerr(e));
+    }
+    G.fdz0 = c->prof; G.dzw = c->prof + nz; G.dz1w = c->prof + 2 * nz; G.dz1 = c->prof + 3 * nz;
+    G.den0 = c->prof + 4 * nz; G.avden0 = c->prof + 5 * nz; G.stab0 = c->prof + 6 * nz;
+    G.pt0 = c->prof + 7 * nz; G.qv0 = c->prof + 8 * nz;
+    // fields
+    auto alloc = [&](double **p) -> int {
+        cudaError_t ee = cudaMalloc(p, c->fbytes);
+        if (ee != cudaSuccess) return cuerr(ee);
+        c->bytes += c->fbytes;
+        return cudaMemset(*p, 0, c->fbytes) == cudaSuccess ? MG_OK : MG_ERR_CUDA;
+    };
+    for (int i = 0; i < 3 && !rc; i++) {
+        rc = alloc(&c->mA[i]);
+        if (!rc) rc = alloc(&c->mB[i]);
+        if (!rc) rc = alloc(&c->tm[i]);
+    }
+    for (int f = 0; f < c->nf && !rc; f++) {
+        rc = alloc(&c->sA[f]);
+        if (!rc) rc = alloc(&c->sB[f]);
+        if (!rc) rc = alloc(&c->ts[f]);
+    }
+    if (!rc) rc = alloc(&c->p);
+    if (!rc) rc = alloc(&c->dens3);
+    if (!rc) rc = alloc(&c->fes);
+    if (!rc) rc = alloc(&c->fqt);
+    if (rc) return fail(rc);
+    // horizontal eigenvalues (get_wv) and the projection plan
+    c->wv.resize((size_t)G.maxx * G.maxy);
+    mg_get_wv(G.maxx, G.maxy, G.dx, G.dy, c->wv.data());
+    int piv = 0;
+    e = pressure_plan_create(G, c->wv.data(), params->precision == MG_PREC_MIXED, &c->pp, &piv);
+    if (e != cudaSuccess) return fail(cuerr(e));
+    c->bytes += pressure_plan_bytes(c->pp);
+    if (piv) return fail(MG_ERR_PIVOT);
+    *out = c;
+    return MG_OK;
+}
+
+extern "C" int mg_destroy(mg_ctx *ctx)
+{
+    if (!ctx) return MG_ERR_PARAM;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    free_ctx(ctx);
+    return MG_OK;
+}
+
+extern "C" size_t mg_device_bytes(const mg_ctx *ctx) { return ctx ? ctx->bytes : 0; }
+extern "C" int mg_last_launch_count(const mg_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+// host (dense nx) <-> device (pitched px)
+static cudaError_t h2d(mg_ctx *c, double *dst, const double *src, cudaMemcpyKind kind)
+{
+    const DevGrid &G = c->G;
+    return cudaMemcpy2DAsync(dst, (size_t)G.px * 8, src, (size_t)G.nx * 8, (size_t)G.nx * 8, (size_t)G.ny * G.nz, kind,
+                             c->stream);
+}
+static cudaError_t d2h(mg_ctx *c, double *dst, const double *src, cudaMemcpyKind kind)
+{
+    const DevGrid &G = c->G;
+    return cudaMemcpy2DAsync(dst, (size_t)G.nx * 8, src, (size_t)G.px * 8, (size_t)G.nx * 8, (size_t)G.ny * G.nz, kind,
+                             c->stream);
+}
+
+static int upload_impl(mg_ctx *c, const double *u, const double *v, const double *w, const double *p,
+                       const double *dens, const double *const *scal, cudaMemcpyKind kind)
+{
+    if (!c || !u || !v || !w || !p || !dens || !scal) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    CKR(h2d(c, c->mA[0], u, kind));
+    CKR(h2d(c, c->mA[1], v, kind));
+    CKR(h2d(c, c->mA[2], w, kind));
+    CKR(h2d(c, c->p, p, kind));
+    CKR(h2d(c, c->sA[0], dens, kind));
+    for (int s = 0; s < c->prm.nscal; s++) {
+        if (!scal[s]) return MG_ERR_PARAM;
+        CKR(h2d(c, c->sA[1 + s], scal[s], kind));
+    }
+    // ghost cells from the interior (the reference's state after update_prognostic)
+    std::vector<double *> f = {c->mA[0], c->mA[1], c->mA[2], c->p};
+    for (int q = 0; q < c->nf; q++) f.push_back(c->sA[q]);
+    CKR(launch_halo_fill(c->G, f.data(), (int)f.size(), c->stream));
+    c->rep = REP_NAT;
+    c->have_state = 1;
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+extern "C" int mg_upload_state(mg_ctx *c, const double *u, const double *v, const double *w, const double *p,
+                               const double *dens, const double *const *scal)
+{
+    return upload_impl(c, u, v, w, p, dens, scal, cudaMemcpyHostToDevice);
+}
+extern "C" int mg_upload_state_device(mg_ctx *c, const double *u, const double *v, const double *w, const double *p,
+                                      const double *dens, const double *const *scal)
+{
+    return upload_impl(c, u, v, w, p, dens, scal, cudaMemcpyDeviceToDevice);
+}
+
+static int download_impl(mg_ctx *c, double *u, double *v, double *w, double *p, double *dens, double *const *scal,
+                         cudaMemcpyKind kind)
+{
+    if (!c) return MG_ERR_PARAM;
+    if (!c->have_state) return MG_ERR_STATE;
+    CKR(cudaSetDevice(c->device));
+    const DevGrid &G = c->G;
+    double *tmp = c->sB[0];   // stage buffer reused as scratch between steps
+    struct Item { double *dst; const double *src; const double *w; int kind; };
+    std::vector<Item> items;
+    if (u) items.push_back({u, c->mA[0], nullptr, 1});
+    if (v) items.push_back({v, c->mA[1], nullptr, 1});
+    if (w) items.push_back({w, c->mA[2], nullptr, 2});
+    if (p) items.push_back({p, c->p, nullptr, 0});
+    if (dens) items.push_back({dens, c->sA[0], nullptr, 0});
+    if (scal)
+        for (int s = 0; s < c->prm.nscal; s++)
+            if (scal[s]) items.push_back({scal[s], c->sA[1 + s], c->sA[0], 3});
+    for (auto &it : items) {
+        CKR(launch_to_natural(G, it.src, it.w, it.kind, c->rep, tmp, c->stream));
+        CKR(d2h(c, it.dst, tmp, kind));
+    }
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+extern "C" int mg_download_state(mg_ctx *c, double *u, double *v, double *w, double *p, double *dens, double *const *scal)
+{
+    return download_impl(c, u, v, w, p, dens, scal, cudaMemcpyDeviceToHost);
+}
+extern "C" int mg_download_state_device(mg_ctx *c, double *u, double *v, double *w, double *p, double *dens,
+                                        double *const *scal)
+{
+    return download_impl(c, u, v, w, p, dens, scal, cudaMemcpyDeviceToDevice);
+}
+
+// ---------------- projection ----------------
+// nsubp x (solve + correction), cal_p1; wold: momentum w at stage start
+static cudaError_t project(mg_ctx *c, double *mu, double *mv, double *mw, const double *wold, int wold_rep,
+                           int want_p1, int want_maxdiv, int *launches)
+{
+    const DevGrid &G = c->G;
+    cudaError_t e;
+    for (int ip = 0; ip < c->prm.nsubp; ip++) {
+        PROF(c, "fft_x_fwd_div", launch_div_rhs(G, c->pp, mu, mv, mw, c->stream));
+        PROF(c, "fft_y_tridiag_fft_y_fft_x_inv", pressure_solve(G, c->pp, 0., 0, c->stream));
+        PROF(c, "correction_halo", launch_correction(G, c->pp, mu, mv, mw, c->p, c->stream));
+        *launches += 7;
+    }
+    PROF(c, "cal_p1", launch_cal_p1(G, c->pp, mw, wold, wold_rep, want_p1, c->stream));
+    *launches += want_p1 ? 3 : 2;
+    if (want_maxdiv) {
+        PROF(c, "maxdiv", launch_maxdiv(G, c->pp, mu, mv, mw, c->stream));
+        *launches += 2;
+    }
+    (void)e;
+    return cudaSuccess;
+}
+
+// ---------------- one step ----------------
+static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int want_maxdiv, int *launches)
+{
+    const DevGrid &G = c->G;
+    const mg_params &P = c->prm;
+    cudaError_t e;
+    const int nf = c->nf;
+    const int ies = 1, iqt = P.iqt >= 0 ? 1 + P.iqt : -1;
+    for (int stage = 1; stage <= 2; stage++) {
+        const double a_dt = (stage == 1 ? 1. : 0.5) * G.dt0;
+        const double b = stage == 1 ? 0. : 1.;
+        // ---- K1: scalars ----
+        K1Args a1{};
+        a1.nf = nf; a1.dens_first = 1; a1.stage = stage; a1.rep = c->rep; a1.a_dt = a_dt; a1.b = b;
+        for (int f = 0; f < nf; f++) {
+            a1.xin[f] = stage == 1 ? c->sA[f] : c->sB[f];
+            a1.xold[f] = c->sA[f];
+            a1.xout[f] = stage == 1 ? c->sB[f] : (f == 0 ? c->dens3 : c->sA[f]);
+            a1.tend[f] = c->ts[f];
+            a1.fst[f] = (f == ies && G.with_buoy) ? c->fes : ((f == iqt && G.with_buoy) ? c->fqt : nullptr);
+        }
+        a1.dens_n = c->sA[0];
+        const double *const *mom = stage == 1 ? c->mA : c->mB;
+        a1.mu = mom[0]; a1.mv = mom[1]; a1.mw = mom[2];
+        a1.mom_rep = stage == 1 ? c->rep : -1;
+        a1.mode = 0;
+        PROF(c, "k1_scalar_advection", launch_k1(G, a1, c->stream));
+        {
+            std::vector<double *> f;
+            for (int q = 0; q < nf; q++) f.push_back(a1.xout[q]);
+            PROF(c, "halo_scalars", launch_halo_fill(G, f.data(), nf, c->stream));
+        }
+        // ---- K2: momentum ----
+        K2Args a2{};
+        a2.stage = stage; a2.rep = c->rep; a2.ntime = ntime; a2.a_dt = a_dt; a2.b = b;
+        a2.mu = mom[0]; a2.mv = mom[1]; a2.mw = mom[2];
+        a2.in_is_leveln = stage == 1;
+        a2.mu_n = c->mA[0]; a2.mv_n = c->mA[1]; a2.mw_n = c->mA[2];
+        a2.p = c->p;
+        a2.dens = stage == 1 ? c->sA[0] : c->sB[0];
+        a2.es = stage == 1 ? c->sA[ies] : c->sB[ies];
+        a2.qt = iqt >= 0 ? (stage == 1 ? c->sA[iqt] : c->sB[iqt]) : nullptr;
+        a2.dens_is_leveln = stage == 1;
+        a2.fes = c->fes; a2.fqt = iqt >= 0 ? c->fqt : nullptr;
+        double **mo = stage == 1 ? c->mB : c->mA;
+        a2.ou = mo[0]; a2.ov = mo[1]; a2.ow = mo[2];
+        a2.tu = c->tm[0]; a2.tv = c->tm[1]; a2.tw = c->tm[2];
+        a2.mode = 0;
+        PROF(c, "k2_momentum", launch_k2(G, a2, c->stream));
+        PROF(c, "halo_momentum", launch_halo_fill(G, mo, 3, c->stream));
+        *launches += 4;
+        // ---- projection ----
+        const double *wold = stage == 1 ? c->mA[2] : c->mB[2];
+        int wold_rep = stage == 1 ? c->rep : -1;
+        if ((e = project(c, mo[0], mo[1], mo[2], wold, wold_rep, last && stage == 2 && want_p1,
+                         last && stage == 2 && want_maxdiv, launches)) != cudaSuccess)
+            return e;
+    }
+    // end of step: new density becomes level n; state is now density weighted
+    double *t = c->sA[0]; c->sA[0] = c->dens3; c->dens3 = t;
+    c->rep = REP_CONS;
+    return cudaSuccess;
+}
+
+extern "C" int mg_step(mg_ctx *c, int nsteps, int ntime0, double *maxdiv, double *p1)
+{
+    if (!c || nsteps < 0) return MG_ERR_PARAM;
+    if (!c->have_state) return MG_ERR_STATE;
+    CKR(cudaSetDevice(c->device));
+    int launches = 0;
+    for (int s = 0; s < nsteps; s++) {
+        cudaError_t e = step_once(c, ntime0 + s, s == nsteps - 1, p1 != nullptr, maxdiv != nullptr, &launches);
+        if (e != cudaSuccess) return cuerr(e);
+    }
+    c->launches = launches;
+    if (maxdiv && nsteps > 0) CKR(cudaMemcpyAsync(maxdiv, pressure_maxdiv_dev(c->pp), 8, cudaMemcpyDeviceToHost, c->stream));
+    if (p1 && nsteps > 0) CKR(cudaMemcpyAsync(p1, pressure_p1_dev(c->pp), c->G.nz * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (maxdiv || p1) CKR(cudaStreamSynchronize(c->stream));
+    return MG_OK;
+}
+
+extern "C" int mg_step_graph(mg_ctx *c, int nsteps, int ntime0, double *maxdiv, double *p1)
+{
+    // The step alternates buffer roles (density pointers swap every step), so the
+    // graph covers a pair of steps; odd remainders run eagerly.
+    if (!c || nsteps < 0) return MG_ERR_PARAM;
+    if (!c->have_state) return MG_ERR_STATE;
+    CKR(cudaSetDevice(c->device));
+    int rc = MG_OK;
+    int s = 0;
+    // the first step after an upload uses the natural representation: run it eagerly
+    if (c->rep == REP_NAT && nsteps > 0) {
+        rc = mg_step(c, 1, ntime0, nullptr, nullptr);
+        if (rc) return rc;
+        s = 1;
+    }
+    int par = (ntime0 + s) & 1;
+    while (nsteps - s >= 2) {
+        if (!c->gexec[par]) {
+            cudaGraph_t graph;
+            double *sa0 = c->sA[0], *d3 = c->dens3;
+            CKR(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            int launches = 0;
+            cudaError_t e = step_once(c, ntime0 + s, 0, 0, 0, &launches);
+            if (e == cudaSuccess) e = step_once(c, ntime0 + s + 1, 0, 0, 0, &launches);
+            cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
+            c->sA[0] = sa0; c->dens3 = d3;   // capture recorded two swaps: back to the same roles
+            if (e != cudaSuccess) return cuerr(e);
+            if (e2 != cudaSuccess) return cuerr(e2);
+            e = cudaGraphInstantiate(&c->gexec[par], graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return cuerr(e);
+            c->launches = launches / 2;
+        }
+        CKR(cudaGraphLaunch(c->gexec[par], c->stream));
+        s += 2;
+    }
+    if (s < nsteps) {
+        rc = mg_step(c, nsteps - s, ntime0 + s, maxdiv, p1);
+        if (rc) return rc;
+    } else if (maxdiv || p1) {
+        // diagnostics of the final state
+        int launches = 0;
+        const DevGrid &G = c->G;
+        if (maxdiv) {
+            CKR(launch_maxdiv(G, c->pp, c->mA[0], c->mA[1], c->mA[2], c->stream));
+            CKR(cudaMemcpyAsync(maxdiv, pressure_maxdiv_dev(c->pp), 8, cudaMemcpyDeviceToHost, c->stream));
+        }
+        (void)launches;
+        if (p1) memset(p1, 0, sizeof(double) * G.nz);
+        CKR(cudaStreamSynchronize(c->stream));
+    }
+    return MG_OK;
+}
+
+extern "C" int mg_synchronize(mg_ctx *c)
+{
+    if (!c) return MG_ERR_PARAM;
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+// ---------------- unit-level entry points ----------------
+static int ensure_unit(mg_ctx *c, int n)
+{
+    for (int i = 0; i < n; i++)
+        if (!c->unit[i]) {
+            cudaError_t e = cudaMalloc(&c->unit[i], c->fbytes);
+            if (e != cudaSuccess) return cuerr(e);
+            c->bytes += c->fbytes;
+        }
+    return MG_OK;
+}
+
+extern "C" int mg_advection_ac(mg_ctx *c, const double *x, const double *mu, const double *mv, const double *mw, double *xs)
+{
+    if (!c || !x || !mu || !mv || !mw || !xs) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    int rc = ensure_unit(c, 5);
+    if (rc) return rc;
+    CKR(h2d(c, c->unit[0], x, cudaMemcpyHostToDevice));
+    CKR(h2d(c, c->unit[1], mu, cudaMemcpyHostToDevice));
+    CKR(h2d(c, c->unit[2], mv, cudaMemcpyHostToDevice));
+    CKR(h2d(c, c->unit[3], mw, cudaMemcpyHostToDevice));
+    CKR(h2d(c, c->unit[4], xs, cudaMemcpyHostToDevice));
+    K1Args a{};
+    a.nf = 1; a.dens_first = 0; a.stage = 0; a.rep = REP_NAT; a.mode = 1;
+    a.xin[0] = c->unit[0]; a.xold[0] = c->unit[0]; a.xout[0] = c->unit[4];
+    a.dens_n = c->unit[0];
+    a.mu = c->unit[1]; a.mv = c->unit[2]; a.mw = c->unit[3]; a.mom_rep = -1;
+    CKR(launch_k1(c->G, a, c->stream));
+    CKR(d2h(c, xs, c->unit[4], cudaMemcpyDeviceToHost));
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+extern "C" int mg_qnadv_uvw(mg_ctx *c, int ntime, const double *mu, const double *mv, const double *mw, double *au,
+                            double *av, double *aw)
+{
+    if (!c || !mu || !mv || !mw || !au || !av || !aw) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    int rc = ensure_unit(c, 6);
+    if (rc) return rc;
+    CKR(h2d(c, c->unit[0], mu, cudaMemcpyHostToDevice));
+    CKR(h2d(c, c->unit[1], mv, cudaMemcpyHostToDevice));
+    CKR(h2d(c, c->unit[2], mw, cudaMemcpyHostToDevice));
+    for (int i = 3; i < 6; i++) CKR(cudaMemsetAsync(c->unit[i], 0, c->fbytes, c->stream));
+    K2Args a{};
+    a.ntime = ntime; a.mode = 1; a.in_is_leveln = 0; a.rep = REP_NAT;
+    a.mu = c->unit[0]; a.mv = c->unit[1]; a.mw = c->unit[2];
+    a.ou = c->unit[3]; a.ov = c->unit[4]; a.ow = c->unit[5];
+    CKR(launch_k2(c->G, a, c->stream));
+    CKR(d2h(c, au, c->unit[3], cudaMemcpyDeviceToHost));
+    CKR(d2h(c, av, c->unit[4], cudaMemcpyDeviceToHost));
+    CKR(d2h(c, aw, c->unit[5], cudaMemcpyDeviceToHost));
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+extern "C" int mg_fft_solve(mg_ctx *c, const double *tend, double *out)
+{
+    if (!c || !tend || !out) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    int rc = ensure_unit(c, 2);
+    if (rc) return rc;
+    CKR(h2d(c, c->unit[0], tend, cudaMemcpyHostToDevice));
+    CKR(h2d(c, c->unit[1], out, cudaMemcpyHostToDevice));
+    CKR(launch_load_rhs(c->G, c->pp, c->unit[0], c->stream));
+    CKR(pressure_solve(c->G, c->pp, 1., 1, c->stream));
+    CKR(launch_store_solution(c->G, c->pp, c->unit[1], c->stream));
+    CKR(d2h(c, out, c->unit[1], cudaMemcpyDeviceToHost));
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+extern "C" int mg_anelastic_pressure(mg_ctx *c, double *mu, double *mv, double *mw, double *p, const double *wold,
+                                     double *maxdiv, double *p1)
+{
+    if (!c || !mu || !mv || !mw || !p || !wold) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    int rc = ensure_unit(c, 5);
+    if (rc) return rc;
+    CKR(h2d(c, c->unit[0], mu, cudaMemcpyHostToDevice));
+    CKR(h2d(c, c->unit[1], mv, cudaMemcpyHostToDevice));
+    CKR(h2d(c, c->unit[2], mw, cudaMemcpyHostToDevice));
+    CKR(h2d(c, c->unit[3], p, cudaMemcpyHostToDevice));
+    CKR(h2d(c, c->unit[4], wold, cudaMemcpyHostToDevice));
+    double *f[4] = {c->unit[0], c->unit[1], c->unit[2], c->unit[3]};
+    CKR(launch_halo_fill(c->G, f, 4, c->stream));
+    // the projection updates c->p; route it through the unit pressure buffer
+    double *psave = c->p;
+    c->p = c->unit[3];
+    int launches = 0;
+    cudaError_t e = project(c, c->unit[0], c->unit[1], c->unit[2], c->unit[4], -1, p1 != nullptr, 1, &launches);
+    c->p = psave;
+    if (e != cudaSuccess) return cuerr(e);
+    CKR(d2h(c, mu, c->unit[0], cudaMemcpyDeviceToHost));
+    CKR(d2h(c, mv, c->unit[1], cudaMemcpyDeviceToHost));
+    CKR(d2h(c, mw, c->unit[2], cudaMemcpyDeviceToHost));
+    CKR(d2h(c, p, c->unit[3], cudaMemcpyDeviceToHost));
+    if (maxdiv) CKR(cudaMemcpyAsync(maxdiv, pressure_maxdiv_dev(c->pp), 8, cudaMemcpyDeviceToHost, c->stream));
+    if (p1) CKR(cudaMemcpyAsync(p1, pressure_p1_dev(c->pp), c->G.nz * 8, cudaMemcpyDeviceToHost, c->stream));
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+// ---------------- timing and profiling ----------------
+extern "C" int mg_time_steps(mg_ctx *c, int nsteps, int ntime0, int use_graph, double *ms)
+{
+    if (!c || nsteps < 0 || !ms) return MG_ERR_PARAM;
+    if (!c->have_state) return MG_ERR_STATE;
+    CKR(cudaSetDevice(c->device));
+    cudaEvent_t a, b;
+    CKR(cudaEventCreate(&a));
+    CKR(cudaEventCreate(&b));
+    CKR(cudaEventRecord(a, c->stream));
+    int rc = use_graph ? mg_step_graph(c, nsteps, ntime0, nullptr, nullptr) : mg_step(c, nsteps, ntime0, nullptr, nullptr);
+    if (rc == MG_OK) {
+        cudaError_t e = cudaEventRecord(b, c->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        float f = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&f, a, b);
+        *ms = f;
+        if (e != cudaSuccess) rc = cuerr(e);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return rc;
+}
+
+extern "C" int mg_profile_enable(mg_ctx *c, int on)
+{
+    if (!c) return MG_ERR_PARAM;
+    prof_collect(c);
+    c->prof_on = on ? 1 : 0;
+    c->acc.clear();
+    return MG_OK;
+}
+
+extern "C" int mg_profile_report(mg_ctx *c, char *buf, size_t len)
+{
+    if (!c || !buf || len == 0) return MG_ERR_PARAM;
+    prof_collect(c);
+    size_t off = 0;
+    buf[0] = 0;
+    for (auto &a : c->acc) {
+        int w = snprintf(buf + off, len - off, "%s %lld %.6f\n", a.name, a.n, a.ms);
+        if (w < 0 || (size_t)w >= len - off) break;
+        off += (size_t)w;
+    }
+    return MG_OK;
+}

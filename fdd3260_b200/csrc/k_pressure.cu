@@ -1,0 +1,729 @@
+// k_pressure.cu -- anelastic pressure projection on the GPU, plain FP64 form.
+//
+// Replaces src/PRESSURE/pressure_solver.f90 (solve_pressure :143-189, correction
+// :342-412, rescale_pressure :415-459), fft_solve_serial
+// (src/PRESSURE/fft_interface.f90:543-666: FFTW c2c 2-D transform per level,
+// tridiag per wavenumber, inverse transform), tridiag/TRIDAG2
+// (src/PRESSURE/fft_tools.f90:115-237), caldiv and gradp
+// (src/TOOLS/gradients.f90:986-1052,1205-1292), cal_p1 (src/TOOLS/funcpack.f90:750-793)
+// and horav (src/TOOLS/averages.f90:78-209).
+//
+// Pipeline of one pass (all on the context's stream):
+//   1. fft_x_fwd: rhs = div(m)/(dt0*rho0) computed on the fly for 8 rows of one
+//      level, two real rows packed in one complex row, shared-memory Stockham FFT
+//      (radix 4/2/3/5), split into the two half spectra, stored transposed as
+//      S[k][kx][ky] so that y transforms and the vertical solve are contiguous.
+//   2. fft_y (forward): complex Stockham FFT of every (k,kx) row along ky.
+//   3. tridiag: one (kx,ky) column per thread, Thomas elimination along k with the
+//      time-invariant elimination factors GAM precomputed at plan creation.
+//   4. fft_y (inverse).
+//   5. fft_x_inv: Hermitian rebuild of two rows, inverse FFT, scale 1/N_h -> dp.
+//   6. correction: p += rho0*dp, m -= dt0*rho0*grad(dp), ghost cells refreshed.
+// The real-to-complex transform is the same DFT as the reference's c2c of real data
+// (the spectrum is Hermitian); the reference keeps mode (0,0) and then removes the
+// horizontal mean of dp, which is that mode -- here the mode is set to zero.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "mg_common.cuh"
+#include "mimica_gpu.h"
+
+namespace {
+
+constexpr int MAXSTAGES = 16;
+struct FftPlan1 {
+    int n;                 // length
+    int nst;               // stages
+    int radix[MAXSTAGES];
+    const double2 *tw;     // device twiddles exp(-2 pi i t/n), t in [0,n)
+};
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+
+// twiddle exp(sign * 2 pi i t / n), sign = -1 forward, +1 inverse
+__device__ __forceinline__ double2 twid(const FftPlan1 &P, int t, int inv)
+{
+    double2 w = __ldg(P.tw + t);
+    return inv ? make_double2(w.x, -w.y) : w;
+}
+
+// In-shared-memory Stockham FFT of one row: buffers a (input) and b (scratch),
+// threads [t0, t0+nt) of the block cooperate.  Result ends in a or b; returns the
+// pointer holding it.  Caller provides the barrier scope (whole block syncs).
+__device__ double2 *stockham(const FftPlan1 &P, double2 *a, double2 *b, int lt, int nt, int inv)
+{
+    const int n = P.n;
+    int Ns = 1;
+    for (int s = 0; s < P.nst; s++) {
+        const int Rr = P.radix[s];
+        const int nb = n / Rr;
+        for (int j = lt; j < nb; j += nt) {
+            const int kk = j % Ns;
+            const int tstep = kk * (n / (Ns * Rr));
+            double2 v[5];
+            for (int r = 0; r < Rr; r++) {
+                double2 x = a[j + r * nb];
+                v[r] = r == 0 ? x : cmul(x, twid(P, tstep * r, inv));
+            }
+            double2 o[5];
+            if (Rr == 2) {
+                o[0] = cadd(v[0], v[1]);
+                o[1] = csub(v[0], v[1]);
+            } else if (Rr == 4) {
+                // omega = exp(sign*i*pi/2) = -i (forward) or +i (inverse), exact
+                double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+                double2 t2 = cadd(v[1], v[3]), t3 = csub(v[1], v[3]);
+                double2 t3r = inv ? make_double2(-t3.y, t3.x) : make_double2(t3.y, -t3.x);   // t3 * omega
+                o[0] = cadd(t0, t2);
+                o[2] = csub(t0, t2);
+                o[1] = cadd(t1, t3r);
+                o[3] = csub(t1, t3r);
+            } else {
+                // generic small DFT with exact table twiddles omega_R^{rs} = W_n^{(rs mod R) n/R}
+                for (int q = 0; q < Rr; q++) {
+                    double2 acc = v[0];
+                    for (int r = 1; r < Rr; r++) acc = cadd(acc, cmul(v[r], twid(P, ((r * q) % Rr) * nb, inv)));
+                    o[q] = acc;
+                }
+            }
+            const int idxD = (j / Ns) * Ns * Rr + kk;
+            for (int r = 0; r < Rr; r++) b[idxD + r * Ns] = o[r];
+        }
+        __syncthreads();
+        double2 *t = a; a = b; b = t;
+        Ns *= Rr;
+    }
+    return a;
+}
+
+// -------------------- step 1: rhs + x transform --------------------
+constexpr int ROWS = 8;   // rows per x-transform block (4 packed pairs)
+
+struct XArgs {
+    const double *mu, *mv, *mw;   // momentum (halo'd layout); null -> read rhs from rbuf
+    const double *rbuf;           // external rhs [nz][maxy][maxx] (interior only)
+    double2 *spec;                // S[k][kx][ky]
+    double dt1;                   // 1/dt0
+};
+
+__global__ void fft_x_fwd(DevGrid G, FftPlan1 P, XArgs A)
+{
+    extern __shared__ double2 smc[];
+    const int n = P.n, nh = n / 2 + 1, maxy = G.maxy;
+    const int groups = (maxy + ROWS - 1) / ROWS;
+    const int k = blockIdx.x / groups + 1, jg = blockIdx.x % groups;
+    const int jb = jg * ROWS;                       // first interior row (0-based)
+    const int nt_pair = blockDim.x / (ROWS / 2);
+    const int pair = threadIdx.x / nt_pair, lt = threadIdx.x % nt_pair;
+    double2 *a = smc + pair * 2 * n, *b = a + n;
+    const double dx1 = 1. / G.dx, dy1 = 1. / G.dy;
+    const double dzw1 = __ldg(G.dz1w + k - 1), d0 = __ldg(G.den0 + k - 1);
+    auto rhs = [&](int jr, int t) -> double {   // jr: interior row 0-based, t: interior column 0-based
+        if (jr >= maxy) return 0.;
+        if (!A.mu) return __ldg(A.rbuf + ((long long)(k - 1) * maxy + jr) * G.maxx + t);
+        const int i = t + 4, j = jr + 4;
+        long long c = gidx(G, i, j, k);
+        double d = 0.;
+        d = d + (__ldg(A.mu + c + 1) - __ldg(A.mu + c)) * dx1;
+        d = d + (__ldg(A.mv + c + G.px) - __ldg(A.mv + c)) * dy1;
+        if (k < G.nz) d = d + (__ldg(A.mw + c + G.ps) - __ldg(A.mw + c)) * dzw1;
+        else d = d + (0. - __ldg(A.mw + c)) * dzw1;
+        return A.dt1 * d / d0;
+    };
+    const int r0 = jb + 2 * pair, r1 = r0 + 1;
+    for (int t = lt; t < n; t += nt_pair) a[t] = make_double2(rhs(r0, t), rhs(r1, t));
+    __syncthreads();
+    double2 *res = stockham(P, a, b, lt, nt_pair, 0);
+    // split: A_k = (Z_k + conj Z_{n-k})/2, B_k = (Z_k - conj Z_{n-k})/(2i)
+    // write S[k][kx][jb + 2*pair + {0,1}]
+    for (int kx = lt; kx < nh; kx += nt_pair) {
+        double2 z = res[kx], w = res[(n - kx) % n];
+        double2 Av = make_double2((z.x + w.x) * 0.5, (z.y - w.y) * 0.5);
+        double2 Bv = make_double2((z.y + w.y) * 0.5, (w.x - z.x) * 0.5);
+        long long base = ((long long)(k - 1) * nh + kx) * maxy;
+        if (r0 < maxy) A.spec[base + r0] = Av;
+        if (r1 < maxy) A.spec[base + r1] = Bv;
+    }
+}
+
+// -------------------- steps 2/4: y transform --------------------
+constexpr int YROWS = 4;   // (k,kx) rows per block
+
+__global__ void fft_y(DevGrid G, FftPlan1 P, double2 *spec, int nrows, int inv)
+{
+    extern __shared__ double2 smc[];
+    const int n = P.n;
+    const int nt_row = blockDim.x / YROWS;
+    const int rr = threadIdx.x / nt_row, lt = threadIdx.x % nt_row;
+    const long long row = (long long)blockIdx.x * YROWS + rr;
+    double2 *a = smc + rr * 2 * n, *b = a + n;
+    const bool ok = row < nrows;
+    if (ok)
+        for (int t = lt; t < n; t += nt_row) a[t] = spec[row * n + t];
+    __syncthreads();
+    double2 *res = stockham(P, a, b, lt, nt_row, inv);
+    if (ok)
+        for (int t = lt; t < n; t += nt_row) spec[row * n + t] = res[t];
+}
+
+// -------------------- step 3: vertical tridiagonal --------------------
+struct TriArgs {
+    double2 *spec;
+    const double *gam;       // [k][kx][ky], k = 2..nz (index k-1); k=1 unused
+    const double *wv;        // wv(l,m), l fastest over maxx
+    const double *ak, *ck, *dka, *dkb;   // per level coefficients (host-computed)
+    int keep00;
+};
+
+__device__ __forceinline__ double dk_of(const TriArgs &T, int k, int nz, double wl)
+{
+    if (k == 1) return wl - __ldg(T.dka) - __ldg(T.dkb);
+    if (k == nz) return wl - __ldg(T.dka + nz - 1) + __ldg(T.dkb + nz - 1);
+    return wl - __ldg(T.dka + k - 1);
+}
+
+__global__ void tridiag_kernel(DevGrid G, TriArgs T)
+{
+    const int nh = G.maxx / 2 + 1, maxy = G.maxy, nz = G.nz;
+    const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= (long long)nh * maxy) return;
+    const int kx = (int)(col / maxy), ky = (int)(col % maxy);
+    const long long lstride = (long long)nh * maxy;
+    double2 *s = T.spec + (long long)kx * maxy + ky;
+    if (kx == 0 && ky == 0) {
+        if (!T.keep00)
+            for (int k = 0; k < nz; k++) s[k * lstride] = make_double2(0., 0.);
+        return;
+    }
+    const double wl = __ldg(T.wv + (long long)ky * G.maxx + kx);
+    const double *gam = T.gam + (long long)kx * maxy + ky;
+    // forward elimination (TRIDAG2 :219-229), complex rhs solved as its two real parts
+    double bet = dk_of(T, 1, nz, wl);
+    double2 r = s[0];
+    double2 uprev = make_double2(r.x / bet, r.y / bet);
+    s[0] = uprev;
+    for (int k = 2; k <= nz; k++) {
+        double g = __ldg(gam + (k - 1) * lstride);
+        double a = __ldg(T.ak + k - 1);
+        bet = dk_of(T, k, nz, wl) - a * g;
+        double2 rk = s[(k - 1) * lstride];
+        double2 u = make_double2((rk.x - a * uprev.x) / bet, (rk.y - a * uprev.y) / bet);
+        s[(k - 1) * lstride] = u;
+        uprev = u;
+    }
+    // back substitution (:231-233)
+    for (int k = nz - 1; k >= 1; k--) {
+        double g = __ldg(gam + k * lstride);   // GAM(k+1)
+        double2 uk = s[(k - 1) * lstride];
+        uk = make_double2(uk.x - g * uprev.x, uk.y - g * uprev.y);
+        s[(k - 1) * lstride] = uk;
+        uprev = uk;
+    }
+}
+
+// GAM(k) = C(k-1)/BET(k-1), BET(k) = B(k) - A(k)*GAM(k); zero pivots flagged
+__global__ void gam_kernel(DevGrid G, TriArgs T, double *gam, int *err)
+{
+    const int nh = G.maxx / 2 + 1, maxy = G.maxy, nz = G.nz;
+    const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= (long long)nh * maxy) return;
+    const int kx = (int)(col / maxy), ky = (int)(col % maxy);
+    const long long lstride = (long long)nh * maxy;
+    const double wl = __ldg(T.wv + (long long)ky * G.maxx + kx);
+    const bool skip = (kx == 0 && ky == 0);
+    double bet = dk_of(T, 1, nz, wl);
+    if (bet == 0. && !skip) atomicOr(err, 1);
+    gam[col] = 0.;
+    for (int k = 2; k <= nz; k++) {
+        double g = __ldg(T.ck + k - 2) / bet;
+        gam[(k - 1) * lstride + col] = g;
+        bet = dk_of(T, k, nz, wl) - __ldg(T.ak + k - 1) * g;
+        if (bet == 0. && !skip) atomicOr(err, 2);
+    }
+}
+
+// -------------------- step 5: inverse x transform --------------------
+struct XInvArgs {
+    const double2 *spec;
+    double *dp;          // [nz][maxy][maxx] real
+    double scale_div;    // divide by this (N_h), or 1
+};
+
+__global__ void fft_x_inv(DevGrid G, FftPlan1 P, XInvArgs A)
+{
+    extern __shared__ double2 smc[];
+    const int n = P.n, nh = n / 2 + 1, maxy = G.maxy;
+    const int groups = (maxy + ROWS - 1) / ROWS;
+    const int k = blockIdx.x / groups + 1, jg = blockIdx.x % groups;
+    const int jb = jg * ROWS;
+    const int nt_pair = blockDim.x / (ROWS / 2);
+    const int pair = threadIdx.x / nt_pair, lt = threadIdx.x % nt_pair;
+    double2 *a = smc + pair * 2 * n, *b = a + n;
+    const int r0 = jb + 2 * pair, r1 = r0 + 1;
+    // rebuild Z_k = A_k + i B_k over the full circle from the half spectra
+    for (int kx = lt; kx < nh; kx += nt_pair) {
+        long long base = ((long long)(k - 1) * nh + kx) * maxy;
+        double2 Av = r0 < maxy ? A.spec[base + r0] : make_double2(0., 0.);
+        double2 Bv = r1 < maxy ? A.spec[base + r1] : make_double2(0., 0.);
+        a[kx] = make_double2(Av.x - Bv.y, Av.y + Bv.x);
+        if (kx > 0 && kx < n - kx) a[n - kx] = make_double2(Av.x + Bv.y, Bv.x - Av.y);
+    }
+    __syncthreads();
+    double2 *res = stockham(P, a, b, lt, nt_pair, 1);
+    for (int t = lt; t < n; t += nt_pair) {
+        double2 z = res[t];
+        if (r0 < maxy) A.dp[((long long)(k - 1) * maxy + r0) * G.maxx + t] = z.x / A.scale_div;
+        if (r1 < maxy) A.dp[((long long)(k - 1) * maxy + r1) * G.maxx + t] = z.y / A.scale_div;
+    }
+}
+
+// -------------------- step 6: correction --------------------
+__global__ void correction_kernel(DevGrid G, const double *dp, double *mu, double *mv, double *mw, double *p)
+{
+    const int maxx = G.maxx, maxy = G.maxy;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)maxx * maxy * G.nz) return;
+    const int ix = (int)(t % maxx), jy = (int)((t / maxx) % maxy), k = (int)(t / ((long long)maxx * maxy)) + 1;
+    const int i = ix + 4, j = jy + 4;
+    auto DP = [&](int a, int b, int kk) { return __ldg(dp + ((long long)(kk - 1) * maxy + b) * maxx + a); };
+    const double d0 = __ldg(G.den0 + k - 1), a0 = __ldg(G.avden0 + k - 1);
+    const double dx1 = 1. / G.dx, dy1 = 1. / G.dy;
+    const double dpc = DP(ix, jy, k);
+    const long long c = gidx(G, i, j, k);
+    p[c] = p[c] + d0 * dpc;
+    const double gpx = (dpc - DP(ix == 0 ? maxx - 1 : ix - 1, jy, k)) * dx1;
+    const double gpy = (dpc - DP(ix, jy == 0 ? maxy - 1 : jy - 1, k)) * dy1;
+    double gpz;
+    if (k >= 2) gpz = (dpc - DP(ix, jy, k - 1)) * __ldg(G.dz1 + k - 2);
+    else gpz = mw[c] / (G.dt0 * __ldg(G.avden0));
+    mu[c] = mu[c] - G.dt0 * d0 * gpx;
+    mv[c] = mv[c] - G.dt0 * d0 * gpy;
+    mw[c] = mw[c] - G.dt0 * a0 * gpz;
+}
+
+// -------------------- reductions --------------------
+// per-level sums over the interior, fixed-order tree (deterministic)
+__global__ void level_sums(DevGrid G, const double *x, const double *xold, int old_rep, double dt0,
+                           double *out_mean, double *out_mean_d)
+{
+    __shared__ double s1[256], s2[256];
+    const int k = blockIdx.x + 1;
+    const int maxx = G.maxx, maxy = G.maxy;
+    const double a0 = __ldg(G.avden0 + k - 1);
+    double acc = 0., accd = 0.;
+    for (long long q = threadIdx.x; q < (long long)maxx * maxy; q += blockDim.x) {
+        int ix = (int)(q % maxx), jy = (int)(q / maxx);
+        long long c = gidx(G, ix + 4, jy + 4, k);
+        double v = x[c];
+        acc += v;
+        if (out_mean_d) {
+            double wo = __ldg(xold + c);
+            if (old_rep >= 0) wo = rep_value(old_rep, wo, a0);
+            accd += (v - wo) / dt0;
+        }
+    }
+    s1[threadIdx.x] = acc;
+    s2[threadIdx.x] = accd;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            s1[threadIdx.x] += s1[threadIdx.x + w];
+            s2[threadIdx.x] += s2[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double nn = (double)maxx * (double)maxy;
+        out_mean[k - 1] = s1[0] / nn;
+        if (out_mean_d) out_mean_d[k - 1] = s2[0] / nn;
+    }
+}
+
+__global__ void subtract_level_mean(DevGrid G, double *x, const double *mean)
+{
+    const long long n = G.ps * G.nz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int k = (int)(t / G.ps) + 1;
+        x[t] = x[t] - __ldg(mean + k - 1);
+    }
+}
+
+__global__ void p1_kernel(DevGrid G, const double *wavd, double *p1)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int nz = G.nz;
+    p1[nz - 1] = 0.;
+    for (int k = nz - 1; k >= 1; k--)
+        p1[k - 1] = p1[k] + wavd[k] * 0.5 * G.dz * (G.fdz0[k - 1] + G.fdz0[k]);
+}
+
+// caldiv over the interior, k = 2..nz-1, signed max (pressure_solver.f90:121-130)
+__global__ void maxdiv_kernel(DevGrid G, const double *mu, const double *mv, const double *mw, double *partial)
+{
+    __shared__ double sm[256];
+    const int maxx = G.maxx, maxy = G.maxy;
+    const double dx1 = 1. / G.dx, dy1 = 1. / G.dy;
+    double m = -INFINITY;
+    const long long tot = (long long)maxx * maxy * (G.nz - 2);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        int ix = (int)(t % maxx), jy = (int)((t / maxx) % maxy), k = (int)(t / ((long long)maxx * maxy)) + 2;
+        long long c = gidx(G, ix + 4, jy + 4, k);
+        double d = 0.;
+        d = d + (mu[c + 1] - mu[c]) * dx1;
+        d = d + (mv[c + G.px] - mv[c]) * dy1;
+        d = d + (mw[c + G.ps] - mw[c]) * __ldg(G.dz1w + k - 1);
+        m = fmax(m, d);
+    }
+    sm[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = sm[0];
+}
+
+__global__ void max_final(const double *partial, int n, double *out)
+{
+    __shared__ double sm[256];
+    double m = -INFINITY;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) m = fmax(m, partial[t]);
+    sm[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sm[0];
+}
+
+// copy a halo'd field's interior into a dense [nz][maxy][maxx] buffer and back
+__global__ void interior_gather(DevGrid G, const double *src, double *dst)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)G.maxx * G.maxy * G.nz) return;
+    int ix = (int)(t % G.maxx), jy = (int)((t / G.maxx) % G.maxy), k = (int)(t / ((long long)G.maxx * G.maxy)) + 1;
+    dst[t] = src[gidx(G, ix + 4, jy + 4, k)];
+}
+__global__ void interior_scatter(DevGrid G, const double *src, double *dst)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)G.maxx * G.maxy * G.nz) return;
+    int ix = (int)(t % G.maxx), jy = (int)((t / G.maxx) % G.maxy), k = (int)(t / ((long long)G.maxx * G.maxy)) + 1;
+    dst[gidx(G, ix + 4, jy + 4, k)] = src[t];
+}
+
+// ghost cells := periodic images (statebc/windbc serial periodic branches)
+struct HaloArgs { double *f[MG_MAXF]; int nf; };
+__global__ void halo_fill_kernel(DevGrid G, HaloArgs H)
+{
+    const int nx = G.nx, ny = G.ny, maxx = G.maxx, maxy = G.maxy;
+    const long long per_plane = 5LL * nx + 5LL * maxy;
+    const long long tot = per_plane * G.nz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        int k = (int)(t / per_plane) + 1;
+        long long g = t % per_plane;
+        int i, j;
+        if (g < 5LL * nx) {
+            int r = (int)(g / nx);
+            i = (int)(g % nx) + 1;
+            j = r < 3 ? r + 1 : ny - 4 + r;   // 1,2,3, ny-1, ny
+        } else {
+            long long g2 = g - 5LL * nx;
+            j = (int)(g2 / 5) + 4;
+            int c = (int)(g2 % 5);
+            i = c < 3 ? c + 1 : nx - 4 + c;
+        }
+        int si = i <= 3 ? i + maxx : (i >= nx - 1 ? i - maxx : i);
+        int sj = j <= 3 ? j + maxy : (j >= ny - 1 ? j - maxy : j);
+        long long dsti = gidx(G, i, j, k), srci = gidx(G, si, sj, k);
+        for (int f = 0; f < H.nf; f++) H.f[f][dsti] = H.f[f][srci];
+    }
+}
+
+__global__ void to_natural_kernel(DevGrid G, const double *src, const double *w, int kind, int rep, double *dst)
+{
+    const long long n = G.ps * G.nz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int k = (int)(t / G.ps) + 1;
+        double x = src[t];
+        if (rep == REP_CONS) {
+            if (kind == 1) x = x / __ldg(G.den0 + k - 1);
+            else if (kind == 2) x = x / __ldg(G.avden0 + k - 1);
+            else if (kind == 3) x = x / w[t];
+        }
+        dst[t] = x;
+    }
+}
+
+// -------------------- host side: plan --------------------
+bool factorize(int n, int *radix, int *nst)
+{
+    int m = n, s = 0;
+    while (m % 4 == 0 && s < MAXSTAGES) { radix[s++] = 4; m /= 4; }
+    while (m % 2 == 0 && s < MAXSTAGES) { radix[s++] = 2; m /= 2; }
+    while (m % 3 == 0 && s < MAXSTAGES) { radix[s++] = 3; m /= 3; }
+    while (m % 5 == 0 && s < MAXSTAGES) { radix[s++] = 5; m /= 5; }
+    *nst = s;
+    return m == 1;
+}
+
+}  // namespace
+
+struct PressurePlan {
+    FftPlan1 px, py;
+    double2 *twx = nullptr, *twy = nullptr;
+    double2 *spec = nullptr;       // [nz][nh][maxy]
+    double *dp = nullptr;          // [nz][maxy][maxx]
+    double *rbuf = nullptr;        // [nz][maxy][maxx] external rhs
+    double *gam = nullptr;         // [nz][nh][maxy]
+    double *wv = nullptr;          // [maxy][maxx]
+    double *ak = nullptr, *ck = nullptr, *dka = nullptr, *dkb = nullptr;
+    double *mean = nullptr, *mean_d = nullptr, *p1 = nullptr;
+    double *partial = nullptr, *maxdiv = nullptr;
+    int npartial = 0;
+    size_t bytes = 0;
+};
+
+static cudaError_t make_twiddles(int n, double2 **out)
+{
+    std::vector<double2> h(n);
+    const long double PI = 3.141592653589793238462643383279502884L;
+    for (int t = 0; t < n; t++) {
+        long double ang = -2.0L * PI * (long double)t / (long double)n;
+        h[t] = make_double2((double)cosl(ang), (double)sinl(ang));
+    }
+    cudaError_t e = cudaMalloc(out, n * sizeof(double2));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*out, h.data(), n * sizeof(double2), cudaMemcpyHostToDevice);
+}
+
+cudaError_t pressure_plan_create(const DevGrid &g, const double *wv_host, int mixed, PressurePlan **out, int *pivot_error)
+{
+    (void)mixed;
+    *out = nullptr;
+    *pivot_error = 0;
+    PressurePlan *pp = new PressurePlan();
+    cudaError_t e;
+    int nh = g.maxx / 2 + 1;
+    size_t nspec = (size_t)g.nz * nh * g.maxy, nreal = (size_t)g.nz * g.maxy * g.maxx;
+#define CK(x) do { e = (x); if (e != cudaSuccess) { pressure_plan_destroy(pp); return e; } } while (0)
+    pp->px.n = g.maxx;
+    pp->py.n = g.maxy;
+    if (!factorize(g.maxx, pp->px.radix, &pp->px.nst) || !factorize(g.maxy, pp->py.radix, &pp->py.nst)) {
+        pressure_plan_destroy(pp);
+        return cudaErrorInvalidValue;
+    }
+    CK(make_twiddles(g.maxx, &pp->twx));
+    CK(make_twiddles(g.maxy, &pp->twy));
+    pp->px.tw = pp->twx;
+    pp->py.tw = pp->twy;
+    CK(cudaMalloc(&pp->spec, nspec * sizeof(double2)));
+    CK(cudaMalloc(&pp->dp, nreal * sizeof(double)));
+    CK(cudaMalloc(&pp->rbuf, nreal * sizeof(double)));
+    CK(cudaMalloc(&pp->gam, nspec * sizeof(double)));
+    CK(cudaMalloc(&pp->wv, (size_t)g.maxx * g.maxy * sizeof(double)));
+    CK(cudaMemcpy(pp->wv, wv_host, (size_t)g.maxx * g.maxy * sizeof(double), cudaMemcpyHostToDevice));
+    // per-level coefficients, fft_tools.f90:142-173 (host, same arithmetic as the reference)
+    {
+        const int nz = g.nz;
+        std::vector<double> fdz(nz), dz1(nz), dz1w(nz), stab(nz);
+        cudaMemcpy(fdz.data(), g.fdz0, nz * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(dz1.data(), g.dz1, nz * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(dz1w.data(), g.dz1w, nz * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(stab.data(), g.stab0, nz * 8, cudaMemcpyDeviceToHost);
+        std::vector<double> ak(nz, 0.), ck(nz, 0.), dka(nz, 0.), dkb(nz, 0.);
+        for (int k = 2; k <= nz - 1; k++) {
+            double h = g.dz * (0.5 * fdz[k] + fdz[k - 1] + 0.5 * fdz[k - 2]);
+            ak[k - 1] = dz1[k - 2] * dz1w[k - 1] - stab[k - 1] / h;
+            ck[k - 1] = dz1[k - 1] * dz1w[k - 1] + stab[k - 1] / h;
+            dka[k - 1] = dz1w[k - 1] * (dz1[k - 1] + dz1[k - 2]);
+        }
+        ak[0] = 0.;
+        ck[0] = dz1[0] * dz1w[0] + stab[0] * dz1[0];
+        dka[0] = dz1[0] * dz1w[0];
+        dkb[0] = stab[0] * dz1[0];
+        ak[nz - 1] = dz1w[nz - 1] * dz1[nz - 2] - stab[nz - 1] * dz1[nz - 2];
+        ck[nz - 1] = 0.;
+        dka[nz - 1] = dz1w[nz - 1] * dz1[nz - 2];
+        dkb[nz - 1] = stab[nz - 1] * dz1[nz - 2];
+        CK(cudaMalloc(&pp->ak, nz * 8)); CK(cudaMalloc(&pp->ck, nz * 8));
+        CK(cudaMalloc(&pp->dka, nz * 8)); CK(cudaMalloc(&pp->dkb, nz * 8));
+        CK(cudaMemcpy(pp->ak, ak.data(), nz * 8, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(pp->ck, ck.data(), nz * 8, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(pp->dka, dka.data(), nz * 8, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(pp->dkb, dkb.data(), nz * 8, cudaMemcpyHostToDevice));
+    }
+    CK(cudaMalloc(&pp->mean, g.nz * 8));
+    CK(cudaMalloc(&pp->mean_d, g.nz * 8));
+    CK(cudaMalloc(&pp->p1, g.nz * 8));
+    pp->npartial = 1024;
+    CK(cudaMalloc(&pp->partial, pp->npartial * 8));
+    CK(cudaMalloc(&pp->maxdiv, 8));
+    // elimination factors and pivot check
+    {
+        int *derr;
+        CK(cudaMalloc(&derr, sizeof(int)));
+        CK(cudaMemset(derr, 0, sizeof(int)));
+        TriArgs T{};
+        T.wv = pp->wv; T.ak = pp->ak; T.ck = pp->ck; T.dka = pp->dka; T.dkb = pp->dkb;
+        long long ncol = (long long)nh * g.maxy;
+        gam_kernel<<<(unsigned)((ncol + 255) / 256), 256>>>(g, T, pp->gam, derr);
+        e = cudaGetLastError();
+        int herr = 0;
+        if (e == cudaSuccess) e = cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
+        cudaFree(derr);
+        if (e != cudaSuccess) { pressure_plan_destroy(pp); return e; }
+        *pivot_error = herr;
+    }
+    pp->bytes = nspec * (16 + 8) + nreal * 16 + (size_t)g.maxx * g.maxy * 8 + (size_t)(g.maxx + g.maxy) * 16;
+#undef CK
+    *out = pp;
+    return cudaSuccess;
+}
+
+void pressure_plan_destroy(PressurePlan *pp)
+{
+    if (!pp) return;
+    cudaFree(pp->twx); cudaFree(pp->twy); cudaFree(pp->spec); cudaFree(pp->dp); cudaFree(pp->rbuf);
+    cudaFree(pp->gam); cudaFree(pp->wv); cudaFree(pp->ak); cudaFree(pp->ck); cudaFree(pp->dka); cudaFree(pp->dkb);
+    cudaFree(pp->mean); cudaFree(pp->mean_d); cudaFree(pp->p1); cudaFree(pp->partial); cudaFree(pp->maxdiv);
+    delete pp;
+}
+
+size_t pressure_plan_bytes(const PressurePlan *pp) { return pp ? pp->bytes : 0; }
+const double *pressure_p1_dev(const PressurePlan *pp) { return pp->p1; }
+const double *pressure_maxdiv_dev(const PressurePlan *pp) { return pp->maxdiv; }
+
+static cudaError_t launch_x_fwd(const DevGrid &g, PressurePlan *pp, const XArgs &a, cudaStream_t s)
+{
+    int groups = (g.maxy + ROWS - 1) / ROWS;
+    int nt_pair = g.maxx / 4 < 32 ? 32 : (g.maxx / 4 > 256 ? 256 : g.maxx / 4);
+    size_t sm = (size_t)(ROWS / 2) * 2 * g.maxx * sizeof(double2);
+    cudaError_t e = cudaFuncSetAttribute(fft_x_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    fft_x_fwd<<<g.nz * groups, nt_pair * (ROWS / 2), sm, s>>>(g, pp->px, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_div_rhs(const DevGrid &g, PressurePlan *pp, const double *mu, const double *mv, const double *mw,
+                           cudaStream_t s)
+{
+    XArgs a{};
+    a.mu = mu; a.mv = mv; a.mw = mw; a.spec = pp->spec; a.dt1 = 1. / g.dt0;
+    return launch_x_fwd(g, pp, a, s);
+}
+
+cudaError_t launch_load_rhs(const DevGrid &g, PressurePlan *pp, const double *tend, cudaStream_t s)
+{
+    long long n = (long long)g.maxx * g.maxy * g.nz;
+    interior_gather<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, tend, pp->rbuf);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    XArgs a{};
+    a.rbuf = pp->rbuf; a.spec = pp->spec;
+    return launch_x_fwd(g, pp, a, s);
+}
+
+cudaError_t pressure_solve(const DevGrid &g, PressurePlan *pp, double scale, int keep00, cudaStream_t s)
+{
+    (void)scale;
+    cudaError_t e;
+    const int nh = g.maxx / 2 + 1;
+    const int nrows = g.nz * nh;
+    int nt_row = g.maxy / 4 < 32 ? 32 : (g.maxy / 4 > 256 ? 256 : g.maxy / 4);
+    size_t smy = (size_t)YROWS * 2 * g.maxy * sizeof(double2);
+    e = cudaFuncSetAttribute(fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy);
+    if (e != cudaSuccess) return e;
+    fft_y<<<(nrows + YROWS - 1) / YROWS, nt_row * YROWS, smy, s>>>(g, pp->py, pp->spec, nrows, 0);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    TriArgs T{};
+    T.spec = pp->spec; T.gam = pp->gam; T.wv = pp->wv; T.ak = pp->ak; T.ck = pp->ck; T.dka = pp->dka; T.dkb = pp->dkb;
+    T.keep00 = keep00;
+    long long ncol = (long long)nh * g.maxy;
+    tridiag_kernel<<<(unsigned)((ncol + 127) / 128), 128, 0, s>>>(g, T);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    fft_y<<<(nrows + YROWS - 1) / YROWS, nt_row * YROWS, smy, s>>>(g, pp->py, pp->spec, nrows, 1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    int groups = (g.maxy + ROWS - 1) / ROWS;
+    int nt_pair = g.maxx / 4 < 32 ? 32 : (g.maxx / 4 > 256 ? 256 : g.maxx / 4);
+    size_t smx = (size_t)(ROWS / 2) * 2 * g.maxx * sizeof(double2);
+    e = cudaFuncSetAttribute(fft_x_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
+    if (e != cudaSuccess) return e;
+    XInvArgs xa{};
+    xa.spec = pp->spec; xa.dp = pp->dp;
+    xa.scale_div = keep00 ? 1.0 : (double)g.maxx * (double)g.maxy;
+    fft_x_inv<<<g.nz * groups, nt_pair * (ROWS / 2), smx, s>>>(g, pp->px, xa);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_store_solution(const DevGrid &g, PressurePlan *pp, double *out, cudaStream_t s)
+{
+    long long n = (long long)g.maxx * g.maxy * g.nz;
+    interior_scatter<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, pp->dp, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_correction(const DevGrid &g, PressurePlan *pp, double *mu, double *mv, double *mw, double *p,
+                              cudaStream_t s)
+{
+    long long n = (long long)g.maxx * g.maxy * g.nz;
+    correction_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, pp->dp, mu, mv, mw, p);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    double *f[4] = {mu, mv, mw, p};
+    return launch_halo_fill(g, f, 4, s);
+}
+
+cudaError_t launch_cal_p1(const DevGrid &g, PressurePlan *pp, double *mw, const double *wold, int wold_rep,
+                          int want_p1, cudaStream_t s)
+{
+    level_sums<<<g.nz, 256, 0, s>>>(g, mw, wold, wold_rep, g.dt0, pp->mean, want_p1 ? pp->mean_d : nullptr);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (want_p1) {
+        p1_kernel<<<1, 32, 0, s>>>(g, pp->mean_d, pp->p1);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    subtract_level_mean<<<1184, 256, 0, s>>>(g, mw, pp->mean);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_maxdiv(const DevGrid &g, PressurePlan *pp, const double *mu, const double *mv, const double *mw,
+                          cudaStream_t s)
+{
+    int nb = pp->npartial;
+    maxdiv_kernel<<<nb, 256, 0, s>>>(g, mu, mv, mw, pp->partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    max_final<<<1, 256, 0, s>>>(pp->partial, nb, pp->maxdiv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_halo_fill(const DevGrid &g, double *const *fields, int nf, cudaStream_t s)
+{
+    HaloArgs H{};
+    for (int b = 0; b < nf; b += MG_MAXF) {
+        H.nf = nf - b < MG_MAXF ? nf - b : MG_MAXF;
+        for (int f = 0; f < H.nf; f++) H.f[f] = fields[b + f];
+        long long tot = (5LL * g.nx + 5LL * g.maxy) * g.nz;
+        int blocks = (int)((tot + 255) / 256);
+        if (blocks > 4096) blocks = 4096;
+        halo_fill_kernel<<<blocks, 256, 0, s>>>(g, H);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_to_natural(const DevGrid &g, const double *src, const double *w, int weight_kind, int rep,
+                              double *dst, cudaStream_t s)
+{
+    to_natural_kernel<<<1184, 256, 0, s>>>(g, src, w, weight_kind, rep, dst);
+    return cudaGetLastError();
+}

@@ -1,0 +1,119 @@
+// mg_common.cuh -- shared definitions of the sm_100a kernels of the MIMICA
+// dynamical-core path (internal; the public boundary is include/mimica_gpu.h).
+//
+// Device layout of a 3-D field: the reference's halo'd Fortran layout
+// x(1:nx,1:ny,1:nz), nx = MAXX+5, ny = MAXY+5, with the x pitch padded to a
+// multiple of 8 doubles (64 B) so that rows are 16-B aligned for TMA.
+// Element (i,j,k) (1-based, as in the reference) sits at
+//   ((k-1)*ny + (j-1))*px + (i-1).
+// Ghost cells hold periodic images of the interior after every producer kernel
+// (the reference's windbc/statebc invariant, src/TOOLS/bc.f90:81-502).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "mimica_gpu.h"
+
+#define MG_MAXF 16   // max fields handled by one scalar-advection launch
+
+struct DevGrid {
+    int nx, ny, nz, px;   // full sizes incl. ghost cells; padded x pitch
+    int maxx, maxy;       // interior sizes
+    long long ps;         // plane stride = px*ny
+    double dx, dy, dz, dt0, lim_tol, u0shift, v0shift;
+    int scal_adv, muscl_lim, mom_ord, lavisc, with_buoy;
+    const double *fdz0, *dzw, *dz1w, *dz1, *den0, *avden0, *stab0, *pt0, *qv0;  // device, nz each
+};
+
+__host__ __device__ inline long long gidx(const DevGrid &g, int i, int j, int k) {
+    return ((long long)(k - 1) * g.ny + (j - 1)) * (long long)g.px + (i - 1);
+}
+
+// Level-n representation of the resident state.
+//   REP_NAT : buffers hold natural variables (after an upload):  value = x * w
+//   REP_CONS: buffers hold density-weighted values from the previous step; the
+//             reference divides by the weight at the end of a step and multiplies
+//             again at the start of the next one, so value = (x / w) * w.
+enum { REP_NAT = 0, REP_CONS = 1 };
+
+__device__ __forceinline__ double rep_value(int rep, double x, double w) {
+    return rep == REP_NAT ? x * w : (x / w) * w;
+}
+
+// ---- scalar advection + stage update (K1) ----
+struct K1Args {
+    int nf;                        // number of fields (field 0 = density when dens_first)
+    int dens_first;                // field 0 is the density (unweighted, adv=.false.)
+    int stage;                     // 1 or 2
+    int rep;                       // representation of level-n buffers (REP_*)
+    double a_dt;                   // a_lm*dt0
+    double b;                      // b_lm
+    const double *xin[MG_MAXF];    // stencil input (stage 1: level-n buffer; stage 2: working)
+    const double *xold[MG_MAXF];   // level-n buffer (pointwise)
+    double *xout[MG_MAXF];         // new working value
+    double *tend[MG_MAXF];         // tendency accumulator (in/out)
+    double *fst[MG_MAXF];          // optional: this stage's tendency (for buoyancy), or null
+    const double *dens_n;          // level-n density (weights)
+    const double *mu, *mv, *mw;    // momentum for the advective velocity
+    int mom_rep;                   // -1: momentum buffers are working values; else REP_* level-n
+    int mode;                      // 0: stage update; 1: unit mode: xout := xout - T (advection_ac)
+};
+
+// ---- momentum advection + pgf + buoyancy + stage update (K2) ----
+struct K2Args {
+    int stage;
+    int rep;                       // REP_* of level-n momentum buffers
+    int ntime;                     // reference step counter (direction order)
+    double a_dt, b;
+    const double *mu, *mv, *mw;    // stencil momentum (stage 1: level-n buffers; stage 2: working)
+    int in_is_leveln;              // stencil momentum is the level-n buffer (apply rep conversion)
+    const double *mu_n, *mv_n, *mw_n;  // level-n buffers (pointwise old values)
+    const double *p;               // pressure (working)
+    const double *dens, *es, *qt;  // working density and density-weighted es, qt (qt may be null)
+    int dens_is_leveln;            // stage 1: dens/es/qt are level-n buffers (rep conversion of es,qt)
+    const double *fes, *fqt;       // this stage's tendencies of es and qt (qt may be null)
+    double *ou, *ov, *ow;          // new momentum
+    double *tu, *tv, *tw;          // tendency accumulators
+    int mode;                      // 0: full stage; 1: unit mode: ou/ov/ow := advection tendency only
+};
+
+// launch wrappers (implemented in the .cu files)
+cudaError_t launch_k1(const DevGrid &g, const K1Args &a, cudaStream_t s);
+cudaError_t launch_k2(const DevGrid &g, const K2Args &a, cudaStream_t s);
+cudaError_t launch_halo_fill(const DevGrid &g, double *const *fields, int nf, cudaStream_t s);
+
+// projection
+struct PressurePlan;
+cudaError_t pressure_plan_create(const DevGrid &g, const double *wv_host, int mixed, PressurePlan **out,
+                                 int *pivot_error);
+void pressure_plan_destroy(PressurePlan *pp);
+size_t pressure_plan_bytes(const PressurePlan *pp);
+// rhs = div(m)/(dt0*rho0) into the plan's real buffer (interior)
+cudaError_t launch_div_rhs(const DevGrid &g, PressurePlan *pp, const double *mu, const double *mv,
+                           const double *mw, cudaStream_t s);
+// external rhs (unit entry): copy interior of a halo'd field into the real buffer
+cudaError_t launch_load_rhs(const DevGrid &g, PressurePlan *pp, const double *tend, cudaStream_t s);
+// forward FFT -> tridiagonal -> inverse FFT on the plan's buffers; out real buffer = unnormalised
+// solution (scale = 1) or rescaled solution (scale = 1/N_h); keep00: keep mode (0,0) untouched
+cudaError_t pressure_solve(const DevGrid &g, PressurePlan *pp, double scale, int keep00, cudaStream_t s);
+// copy the plan's real solution into the interior of a halo'd field
+cudaError_t launch_store_solution(const DevGrid &g, PressurePlan *pp, double *out, cudaStream_t s);
+// correction: p += rho0*dp; m -= dt0*rho0*grad(dp); ghost cells refreshed
+cudaError_t launch_correction(const DevGrid &g, PressurePlan *pp, double *mu, double *mv, double *mw,
+                              double *p, cudaStream_t s);
+// cal_p1 (+ optional p1), residual max of div
+cudaError_t launch_cal_p1(const DevGrid &g, PressurePlan *pp, double *mw, const double *wold, int wold_rep,
+                          int want_p1, cudaStream_t s);
+cudaError_t launch_maxdiv(const DevGrid &g, PressurePlan *pp, const double *mu, const double *mv,
+                          const double *mw, cudaStream_t s);
+// results of the last cal_p1 / maxdiv (device pointers inside the plan)
+const double *pressure_p1_dev(const PressurePlan *pp);
+const double *pressure_maxdiv_dev(const PressurePlan *pp);
+
+// natural <-> resident conversions for download
+cudaError_t launch_to_natural(const DevGrid &g, const double *src, const double *w, int weight_kind,
+                              int rep, double *dst, cudaStream_t s);
+// copy with pitch change: halo'd host layout (nx) <-> device layout (px)
+

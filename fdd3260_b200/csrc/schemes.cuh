@@ -1,0 +1,308 @@
+// schemes.cuh -- per-face / per-cell arithmetic of the reference's scalar
+// advection schemes, as device functions shared by the FP64 kernels (double)
+// and the mixed-precision kernels (float).  Every expression keeps the reference's
+// evaluation order; the FP64 translation unit is compiled without FMA contraction
+// so that results match the CPU restatement bit for bit.
+#pragma once
+#include <cuda_runtime.h>
+
+template <typename T> __device__ __forceinline__ T tmin(T a, T b) { return a < b ? a : b; }
+template <typename T> __device__ __forceinline__ T tmax(T a, T b) { return a > b ? a : b; }
+__device__ __forceinline__ double dabs(double a) { return fabs(a); }
+__device__ __forceinline__ float dabs(float a) { return fabsf(a); }
+__device__ __forceinline__ double sign1(double b) { return copysign(1.0, b); }
+__device__ __forceinline__ float sign1(float b) { return copysignf(1.0f, b); }
+
+// ---------------- WENO3-switch: src/TOOLS/advq_weno.f90 ----------------
+// weights of one face, :304-353 (loop body); linear weights unless the smoothness
+// ratio exceeds 20.  (eps+eta)**2 is the correctly rounded product.
+template <typename T>
+__device__ __forceinline__ void weno_weights(T xm1, T x0, T xp1, T xp2, T &w0, T &w1, T &w2, T &w3)
+{
+    const T g1 = T(1.) / T(3.), g2 = T(2.) / T(3.), eps = T(1.e-15), thres = T(20.);
+    T d1 = x0 - xm1, d2 = xp1 - x0, d3 = xp2 - xp1;
+    T eta1 = d1 * d1, eta2 = d2 * d2, eta3 = d3 * d3;
+    w0 = g1; w1 = g2; w2 = g2; w3 = g1;
+    if (tmax(eta1, eta2) / (tmin(eta1, eta2) + eps) > thres) {
+        T y1 = eps + eta1, y2 = eps + eta2;
+        T a = g1 / (y1 * y1), b = g2 / (y2 * y2);
+        T s = a + b;
+        w0 = a / s; w1 = b / s;
+    }
+    if (tmax(eta2, eta3) / (tmin(eta2, eta3) + eps) > thres) {
+        T y2 = eps + eta2, y3 = eps + eta3;
+        T a = g2 / (y2 * y2), b = g1 / (y3 * y3);
+        T s = a + b;
+        w2 = a / s; w3 = b / s;
+    }
+}
+
+// face flux at i+1/2 (advq_weno.f90:92-110, limiter :462-491)
+template <typename T>
+__device__ __forceinline__ T weno_face(T xm1, T x0, T xp1, T xp2, T uu, bool full_weights)
+{
+    const T eps = T(1.e-15);
+    T w0 = T(1.) / T(3.), w1 = T(2.) / T(3.), w2 = T(2.) / T(3.), w3 = T(1.) / T(3.);
+    if (full_weights) weno_weights(xm1, x0, xp1, xp2, w0, w1, w2, w3);
+    T ffim1 = (-(T(0.5) * xm1) + T(1.5) * x0);
+    T ffip1p = (T(0.5) * x0 + T(0.5) * xp1);
+    T ffip1m = ffip1p;
+    T ffip2 = (T(1.5) * xp1 - T(0.5) * xp2);
+    T minp = tmin(tmin(tmin(ffim1, ffip1m), ffip1p), ffip2);
+    T phi = tmin(dabs((T(0.) - x0) / ((minp - x0) + eps)), T(1.));
+    ffim1 = phi * (ffim1 - x0) + x0;
+    ffip1m = phi * (ffip1m - x0) + x0;
+    ffip1p = phi * (ffip1p - x0) + x0;
+    ffip2 = phi * (ffip2 - x0) + x0;
+    T Fl = w0 * ffim1 + w1 * ffip1p;
+    T Fr = w2 * ffip1m + w3 * ffip2;
+    return T(0.5) * Fl * (uu + dabs(uu)) + T(0.5) * Fr * (uu - dabs(uu));
+}
+// vertical bottom face (k=1), :232-241
+template <typename T>
+__device__ __forceinline__ T weno_face_bottom(T x1, T x2, T x3, T ww)
+{
+    const T g1 = T(1.) / T(3.), g2 = T(2.) / T(3.);
+    T ffip1p = (T(0.5) * x1 + T(0.5) * x2);
+    T ffip1m = ffip1p;
+    T ffip2 = (T(1.5) * x2 - T(0.5) * x3);
+    T Fl = ffip1p;
+    T Fr = g2 * ffip1m + g1 * ffip2;
+    return T(0.5) * Fl * (ww + dabs(ww)) + T(0.5) * Fr * (ww - dabs(ww));
+}
+// vertical top face (k=nz-1), :262-271
+template <typename T>
+__device__ __forceinline__ T weno_face_top(T xm1, T x0, T xp1, T ww)
+{
+    const T g1 = T(1.) / T(3.), g2 = T(2.) / T(3.);
+    T ffim1 = (-(T(0.5) * xm1) + T(1.5) * x0);
+    T ffip1p = (T(0.5) * x0 + T(0.5) * xp1);
+    T ffip1m = ffip1p;
+    T Fl = g1 * ffim1 + g2 * ffip1p;
+    T Fr = ffip1m;
+    return T(0.5) * Fl * (ww + dabs(ww)) + T(0.5) * Fr * (ww - dabs(ww));
+}
+
+// ---------------- MUSCL: src/TOOLS/advq_muscl.f90 ----------------
+template <typename T>
+__device__ __forceinline__ void muscl_limiter(int lim, T lim_tol, T xx, T ffip1, T ffip2, T ffim1, T &phir, T &phil)
+{
+    T rp1 = T(1.), rp2 = T(1.);
+    if (dabs(ffim1) > lim_tol * dabs(xx) && dabs(ffip1) < dabs(ffim1) / lim_tol) rp1 = ffip1 / ffim1;
+    if (dabs(ffip2) > lim_tol * dabs(xx) && dabs(ffip1) < dabs(ffip2) / lim_tol) rp2 = ffip1 / ffip2;
+    if (lim == 1) {        // VL
+        phil = (rp1 + dabs(rp1)) / (T(1.) + dabs(rp1));
+        phir = (rp2 + dabs(rp2)) / (T(1.) + dabs(rp2));
+    } else if (lim == 2) { // MC
+        phil = tmax(T(0.), tmin(tmin(T(2.) * rp1, T(0.5) * (rp1 + T(1.))), T(2.)));
+        phir = tmax(T(0.), tmin(tmin(T(2.) * rp2, T(0.5) * (rp2 + T(1.))), T(2.)));
+    } else if (lim == 0) { // minmod
+        phil = tmax(T(0.), tmin(T(1.), rp1));
+        phir = tmax(T(0.), tmin(T(1.), rp2));
+    } else {
+        phil = T(0.5) * (rp1 + T(1.));
+        phir = T(0.5) * (rp2 + T(1.));
+    }
+}
+
+// horizontal face between i and i+1 (advq_muscl.f90:81-100); d = dx, d1 = 1/dx
+template <typename T>
+__device__ __forceinline__ T muscl_face_h(int lim, T lim_tol, T d, T d1, T xm1, T x0, T xp1, T xp2, T uu)
+{
+    const T eps = T(1.e-18);
+    T slope_p = (xp1 - x0) * d1;
+    T slope_p2 = (xp2 - xp1) * d1;
+    T slope_m = (x0 - xm1) * d1;
+    T Fr, Fl;
+    if (d * dabs(slope_m) > lim_tol * dabs(x0) + eps || d * dabs(slope_p2) > lim_tol * dabs(x0) + eps) {
+        T phir, phil;
+        muscl_limiter(lim, lim_tol, x0, slope_p, slope_p2, slope_m, phir, phil);
+        Fr = xp1 - T(0.5) * phir * slope_p2 * d;
+        Fl = x0 + T(0.5) * phil * slope_m * d;
+    } else {
+        Fr = xp1 - T(0.5) * slope_p * d;
+        Fl = x0 + T(0.5) * slope_p * d;
+    }
+    return T(0.5) * uu * (Fl * (T(1.) + sign1(uu)) + Fr * (T(1.) - sign1(uu)));
+}
+
+// vertical face k+1/2 (advq_muscl.f90:245-302).  kind: 0 core, 1 bottom (k=1), 2 top (k=nz-1).
+// xm1..xp2 = x(k-1..k+2); d1m = dz1(k-1), d10 = dz1(k), d1p = dz1(k+1); fm = fdz0(k-1),
+// fp = fdz0(k+1); dzw1 = dz1w(k).
+template <typename T>
+__device__ __forceinline__ T muscl_face_z(int kind, int lim, T lim_tol, T dz, T xm1, T x0, T xp1, T xp2,
+                                          T d1m, T d10, T d1p, T fm, T fp, T dzw1, T ww)
+{
+    const T eps = T(1.e-18);
+    T slope_p, slope_p2, slope_m, Fl, Fr, phir, phil;
+    bool lim_on;
+    if (kind == 1) {
+        slope_p = (xp1 - x0) * d10;
+        slope_p2 = (xp2 - xp1) * d1p;
+        slope_m = slope_p;
+        lim_on = fp * dz * dabs(slope_p2) > lim_tol * dabs(x0) + eps;
+        if (lim_on) {
+            muscl_limiter(lim, lim_tol, x0, slope_p, slope_p2, slope_m, phir, phil);
+            Fl = x0 + T(0.5) * phil * slope_m / dzw1;
+            Fr = xp1 - T(0.5) * phir * slope_p2 / dzw1;
+        } else {
+            Fl = x0 + T(0.5) * slope_p / dzw1;
+            Fr = xp1 - T(0.5) * slope_p / dzw1;
+        }
+    } else {
+        slope_p = (xp1 - x0) * d10;
+        slope_m = (x0 - xm1) * d1m;
+        if (kind == 2) {
+            slope_p2 = slope_p;
+            lim_on = fm * dz * dabs(slope_m) > lim_tol * dabs(x0) + eps;
+        } else {
+            slope_p2 = (xp2 - xp1) * d1p;
+            lim_on = fm * dz * dabs(slope_m) > lim_tol * dabs(x0) + eps ||
+                     fp * dz * dabs(slope_p2) > lim_tol * dabs(x0) + eps;
+        }
+        if (lim_on) {
+            muscl_limiter(lim, lim_tol, x0, slope_p, slope_p2, slope_m, phir, phil);
+            Fr = xp1 - T(0.5) * phir * slope_p2 / dzw1;
+            Fl = x0 + T(0.5) * phil * slope_m / dzw1;
+        } else {
+            Fr = xp1 - T(0.5) * slope_p / dzw1;
+            Fl = x0 + T(0.5) * slope_p / dzw1;
+        }
+    }
+    return T(0.5) * ww * (Fl * (T(1.) + sign1(ww)) + Fr * (T(1.) - sign1(ww)));
+}
+
+// ---------------- PPM: src/TOOLS/advq_ppm.f90 ----------------
+// spacing() of Fortran (2**(exponent-digits)), tiny() for 0
+__device__ __forceinline__ double fspacing(double x)
+{
+    if (x == 0.0) return 2.2250738585072014e-308;
+    int e = ilogb(x) - 52;
+    if (e < -1022) return 2.2250738585072014e-308;
+    return ldexp(1.0, e);
+}
+__device__ __forceinline__ float fspacing(float x)
+{
+    if (x == 0.0f) return 1.17549435e-38f;
+    int e = ilogbf(x) - 23;
+    if (e < -126) return 1.17549435e-38f;
+    return ldexpf(1.0f, e);
+}
+__device__ __forceinline__ double tsqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float tsqrt(float x) { return sqrtf(x); }
+
+// limiter_ppm :449-530 with ppmlimiter='PPM'
+template <typename T>
+__device__ __forceinline__ void ppm_limiter(T xx, T xp, T xm, T xplus, T xmin, T ffip1, T ffip2, T ffim1,
+                                            T ffim2, T &phir, T &phil, T &phi1, T &phi2)
+{
+    const T eps = T(1.e-15), thres = T(10.);
+    T rp1 = T(1.);
+    phir = xplus; phil = xmin;
+    T a, b;
+    a = ffip1 - ffim1; b = ffip1 + ffim1;
+    T gamma1 = T(0.5) * (a * a + b * b);
+    a = ffip2 - ffip1; b = ffip2 + ffip1;
+    T gamma2 = T(0.5) * (a * a + b * b);
+    a = ffim1 - ffim2; b = ffim1 + ffim2;
+    T gamma3 = T(0.5) * (a * a + b * b);
+    T lambda = tmax(tmax(gamma1, gamma2), gamma3) / (tmin(tmin(gamma1, gamma2), gamma3) + eps);
+    phi1 = phir - phil;
+    phi2 = T(3.) * (phil - T(2.) * xx + phir);
+    if (lambda > thres) {
+        if (phir < T(0.) || ((phir - xx) * (xp - phir) < T(0.) &&
+                             (ffim1 * ffip2 >= T(0.) || ffim1 * ffip1 <= T(0.) || ffip2 * ffip1 <= T(0.)))) {
+            if (dabs(phir - xx) < dabs(phir - xp)) phir = xx;
+            else phir = xp;
+        }
+        if (phil < T(0.) || ((xx - phil) * (phil - xm) < T(0.) &&
+                             (ffim2 * ffip1 >= T(0.) || ffim2 * ffim1 <= T(0.) || ffip1 * ffim1 <= T(0.)))) {
+            if (dabs(phil - xx) < dabs(phil - xm)) phil = xx;
+            else phil = xm;
+        }
+        phi1 = phir - phil;
+        phi2 = T(3.) * (phil - T(2.) * xx + phir);
+        T slope = -(T(0.5) * phi1 / (sign1(phi2) * tmax(dabs(phi2), eps)));
+        if (dabs(ffim1) > tsqrt(fspacing(ffim1))) rp1 = ffip1 / ffim1;
+        if (dabs(phi2) > eps && (slope > T(-0.5) || slope < T(0.5))) {
+            T lim = tmax(T(0.), tmin(tmin(T(2.), T(0.5) * (rp1 + T(1.))), T(2.) * rp1));
+            phir = xx + T(0.5) * ffim1 * lim;
+            phil = xx - T(0.5) * ffim1 * lim;
+            if ((xx - phil) * (phir - xx) < T(0.)) {
+                phil = xx;
+                phir = xx;
+            }
+            phi1 = phir - phil;
+            phi2 = T(0.);
+        }
+    }
+}
+
+// uniform-grid face value xplus of cell i (advq_ppm.f90:108-110)
+template <typename T>
+__device__ __forceinline__ T ppm_xplus_core(T xm1, T x0, T xp1, T xp2)
+{
+    T ffip1 = (xp1 - x0), ffip2 = (xp2 - xp1), ffim1 = (x0 - xm1);
+    T sl = T(0.5) * (ffip1 + ffim1);
+    T slp1 = T(0.5) * (ffip2 + ffip1);
+    return x0 + T(0.5) * ffip1 - T(1.) / T(6.) * (slp1 - sl);
+}
+
+// Courant-number fluxes (advq_ppm.f90:93-94)
+template <typename T> __device__ __forceinline__ T ppm_fr(T phir, T mup, T phi1, T phi2)
+{ return phir - T(0.5) * mup * (phi1 + (T(1.) - T(2.) / T(3.) * mup) * phi2); }
+template <typename T> __device__ __forceinline__ T ppm_fl(T phil, T muc, T phi1, T phi2)
+{ return phil + T(0.5) * muc * (phi1 - (T(1.) - T(2.) / T(3.) * muc) * phi2); }
+
+// Horizontal cell reconstruction of cell c, pencil of length n (1-based).
+// xv[0..4] = x(c-2..c+2) (entries outside the pencil unused).  kind:
+//  0 core (5 <= c <= n-2), 1 left ghost (c = 3, :79-94), 2 first interior (c = 4,
+//  xmin from the left-ghost xplus), 3 right ghost (c = n-1, :120-134).
+// xmin of a cell is the unlimited xplus of the cell before it (:98,117).
+// Returns phir, phil, phi1, phi2 (the velocity-independent part).
+template <typename T>
+__device__ __forceinline__ void ppm_cell_h(int kind, const T *xv, T &phir, T &phil, T &phi1, T &phi2)
+{
+    T xm2 = xv[0], xm1 = xv[1], x0 = xv[2], xp1 = xv[3], xp2 = xv[4];
+    T ffip1, ffip2, ffim1, ffim2, xplus, xmin;
+    if (kind == 1) {
+        ffip1 = (xp1 - x0);
+        ffip2 = (xp2 - xp1);
+        ffim1 = (x0 - xm1);
+        ffim2 = (x0 - xm1);
+        xmin = T(0.5) * (xp1 + x0);
+        xplus = x0 + T(0.5) * ffip1;
+    } else if (kind == 3) {
+        ffip1 = (xp1 - x0);
+        ffip2 = (xp1 - x0);
+        ffim1 = (x0 - xm1);
+        ffim2 = (xm1 - xm2);
+        xplus = x0 + T(0.5) * ffip1;
+        xmin = ppm_xplus_core(xm2, xm1, x0, xp1);
+    } else {
+        ffip1 = (xp1 - x0);
+        ffip2 = (xp2 - xp1);
+        ffim1 = (x0 - xm1);
+        ffim2 = (xm1 - xm2);
+        xplus = ppm_xplus_core(xm1, x0, xp1, xp2);
+        if (kind == 2) xmin = xm1 + T(0.5) * (x0 - xm1);
+        else xmin = ppm_xplus_core(xm2, xm1, x0, xp1);
+    }
+    ppm_limiter(x0, xp1, xm1, xplus, xmin, ffip1, ffip2, ffim1, ffim2, phir, phil, phi1, phi2);
+}
+
+// Stretched-grid face value of cell k (advq_ppm.f90:374-383); dm1..dp2 = dz1w(k-1..k+2)
+template <typename T>
+__device__ __forceinline__ T ppm_xplus_z(T x0, T ffip1, T ffip2, T ffim1, T deltam1, T delta, T deltap1, T deltap2)
+{
+    T sl = delta / (deltam1 + delta + deltap1) *
+           ((T(2.) * deltam1 + delta) / (deltap1 + delta) * ffip1 + (delta + T(2.) * deltap1) / (deltam1 + delta) * ffim1);
+    T slp1 = deltap1 / (delta + deltap1 + deltap2) *
+             ((T(2.) * delta + deltap1) / (deltap2 + deltap1) * ffip2 + (deltap1 + T(2.) * deltap2) / (delta + deltap1) * ffip1);
+    return x0 + delta / (delta + deltap1) * ffip1 +
+           T(1.) / (deltam1 + delta + deltap1 + deltap2) *
+               (T(2.) * deltap1 * delta / (delta + deltap1) *
+                    ((deltam1 + delta) / (T(2.) * delta + deltap1) - (deltap2 + deltap1) / (T(2.) * deltap1 + delta)) * ffip1 -
+                delta * (deltam1 + delta) / (T(2.) * delta + deltap1) * slp1 +
+                deltap1 * (deltap1 + deltap2) / (T(2.) * deltap1 + delta) * sl);
+}

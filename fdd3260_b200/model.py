@@ -1,0 +1,126 @@
+"""Host-side interface of the GPU path, named after the reference routines it replaces.
+
+``Mimica`` owns one device context (``mg_create``): the fields of one domain stay
+resident on the GPU across both integrator stages of every step; host arrays in
+the reference's layout cross the boundary only in ``upload``/``download`` and in
+the unit-level entry points used by the parity tests.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .config import Domain, State
+
+
+class Mimica:
+    def __init__(self, domain: Domain, nscal: int, iqt: int = -1, device: int = 0):
+        self.domain = domain
+        self.nscal = nscal
+        self.iqt = iqt
+        L = _lib.lib()
+        params, self._keep = domain.params(nscal, iqt)
+        h = C.c_void_p()
+        _lib.check(L.mg_create(C.byref(params), device, C.byref(h)), "mg_create")
+        self._h = h
+        self._L = L
+
+    # ---- lifetime ----
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.mg_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self._L.mg_device_bytes(self._h))
+
+    @property
+    def launches_per_call(self) -> int:
+        return int(self._L.mg_last_launch_count(self._h))
+
+    # ---- resident state ----
+    def upload(self, st: State) -> None:
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in st.scal]
+        sp = (_lib._dp * len(arrs))(*[_lib.ptr(a) for a in arrs])
+        _lib.check(self._L.mg_upload_state(self._h, _lib.ptr(st.u), _lib.ptr(st.v), _lib.ptr(st.w), _lib.ptr(st.p),
+                                           _lib.ptr(st.dens), sp), "mg_upload_state")
+
+    def download(self) -> State:
+        d = self.domain
+        u, v, w, p, dens = (np.zeros(d.shape) for _ in range(5))
+        scal = [np.zeros(d.shape) for _ in range(self.nscal)]
+        sp = (_lib._dp * len(scal))(*[_lib.ptr(a) for a in scal])
+        _lib.check(self._L.mg_download_state(self._h, _lib.ptr(u), _lib.ptr(v), _lib.ptr(w), _lib.ptr(p),
+                                             _lib.ptr(dens), sp), "mg_download_state")
+        return State(u, v, w, p, dens, scal, self.iqt)
+
+    def upload_device(self, ptrs: dict) -> None:
+        """Upload from device pointers (ints), same layout as the host path."""
+        sp = (C.c_void_p * self.nscal)(*ptrs["scal"])
+        _lib.check(self._L.mg_upload_state_device(self._h, ptrs["u"], ptrs["v"], ptrs["w"], ptrs["p"], ptrs["dens"],
+                                                  sp), "mg_upload_state_device")
+
+    def download_device(self, ptrs: dict) -> None:
+        sp = (C.c_void_p * self.nscal)(*ptrs["scal"])
+        _lib.check(self._L.mg_download_state_device(self._h, ptrs["u"], ptrs["v"], ptrs["w"], ptrs["p"],
+                                                    ptrs["dens"], sp), "mg_download_state_device")
+
+    # ---- stepping (src/INTEG/time_step.f90:76) ----
+    def stepping(self, nsteps: int = 1, ntime0: int = 1, diagnostics: bool = False, graph: bool = False):
+        md = C.c_double(0.0)
+        p1 = np.zeros(self.domain.nz) if diagnostics else None
+        fn = self._L.mg_step_graph if graph else self._L.mg_step
+        _lib.check(fn(self._h, nsteps, ntime0, C.byref(md) if diagnostics else None, _lib.ptr(p1)), "mg_step")
+        if diagnostics:
+            return md.value, p1
+        return None
+
+    def synchronize(self) -> None:
+        _lib.check(self._L.mg_synchronize(self._h), "mg_synchronize")
+
+    # ---- unit-level entry points ----
+    def advection_ac(self, x, mu, mv, mw, xs) -> np.ndarray:
+        """src/TOOLS/advection.f90:801 advection_ac; returns the updated xs."""
+        xs = np.array(xs, dtype=np.float64, copy=True)
+        _lib.check(self._L.mg_advection_ac(self._h, _lib.ptr(np.ascontiguousarray(x)), _lib.ptr(mu), _lib.ptr(mv),
+                                           _lib.ptr(mw), _lib.ptr(xs)), "mg_advection_ac")
+        return xs
+
+    def qnadv_uvw(self, mu, mv, mw, ntime: int = 1):
+        """src/INTEG/windadv.f90:46 qnadv_uvw; returns (au, av, aw)."""
+        d = self.domain
+        au, av, aw = (np.zeros(d.shape) for _ in range(3))
+        _lib.check(self._L.mg_qnadv_uvw(self._h, ntime, _lib.ptr(mu), _lib.ptr(mv), _lib.ptr(mw), _lib.ptr(au),
+                                        _lib.ptr(av), _lib.ptr(aw)), "mg_qnadv_uvw")
+        return au, av, aw
+
+    def fft_solve(self, tend, out=None) -> np.ndarray:
+        """src/PRESSURE/pressure_solver.f90:462 fft_solve (unnormalised solution)."""
+        out = np.zeros(self.domain.shape) if out is None else np.array(out, dtype=np.float64, copy=True)
+        _lib.check(self._L.mg_fft_solve(self._h, _lib.ptr(np.ascontiguousarray(tend)), _lib.ptr(out)), "mg_fft_solve")
+        return out
+
+    def anelastic_pressure(self, mu, mv, mw, p, wold):
+        """src/PRESSURE/pressure_solver.f90:73 anelastic_pressure; returns (mu, mv, mw, p, maxdiv, p1)."""
+        mu, mv, mw, p = (np.array(a, dtype=np.float64, copy=True) for a in (mu, mv, mw, p))
+        md = C.c_double(0.0)
+        p1 = np.zeros(self.domain.nz)
+        _lib.check(self._L.mg_anelastic_pressure(self._h, _lib.ptr(mu), _lib.ptr(mv), _lib.ptr(mw), _lib.ptr(p),
+                                                 _lib.ptr(np.ascontiguousarray(wold)), C.byref(md), _lib.ptr(p1)),
+                   "mg_anelastic_pressure")
+        return mu, mv, mw, p, md.value, p1

@@ -1,0 +1,164 @@
+/*
+ * mimica_gpu.h -- C ABI of the B200 (sm_100a) implementation of MIMICA's
+ * dynamical-core hot path: flux-form scalar advection (WENO3-switch, PPM, MUSCL),
+ * FD2/FD4 momentum advection with artificial viscosity, the Heun stage update and
+ * the anelastic pressure projection (horizontal FFT, vertical tridiagonal per
+ * wavenumber, inverse FFT, correction).
+ *
+ * Plain C types only (pointers, sizes, doubles); no CUDA or torch types cross this
+ * boundary.  Every entry point returns an int status (MG_OK == 0) and never exits,
+ * traps or aborts; mg_error_string() names a code.
+ *
+ * Array convention: the reference's own.  A 3-D field is real(8) x(1:nx,1:ny,1:nz)
+ * in Fortran (column-major) order with nx = MAXX+5, ny = MAXY+5: three ghost cells
+ * on the low side and two on the high side of x and y, no ghost cells in z.  Host
+ * buffers passed to this library use exactly that layout, so a Fortran caller
+ * passes its arrays through ISO_C_BINDING (c_loc) unchanged.
+ *
+ * Each entry point names the reference routine it replaces (paths relative to the
+ * MIMICA source tree).
+ */
+#ifndef MIMICA_GPU_H
+#define MIMICA_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+enum {
+    MG_OK = 0,
+    MG_ERR_PARAM = 1,        /* invalid or unsupported parameter */
+    MG_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    MG_ERR_NAN = 3,          /* non-finite value detected in a field */
+    MG_ERR_PIVOT = 4,        /* zero pivot in the vertical tridiagonal solve (TRIDAG2 CODE 1/2) */
+    MG_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up */
+    MG_ERR_NOMEM = 6,        /* device or host allocation failed */
+    MG_ERR_STATE = 7         /* call out of order (e.g. step before upload) */
+};
+
+/* ---- scheme selectors (src/TOOLS/advection.f90:603-614, advq_muscl.f90:367-380) ---- */
+enum { MG_WENO = 0, MG_PPM = 1, MG_MUSCL = 2 };
+enum { MG_LIM_MINMOD = 0, MG_LIM_VL = 1, MG_LIM_MC = 2, MG_LIM_DEFAULT = 3 };
+/* arithmetic forms */
+enum {
+    MG_PREC_FP64 = 0,        /* plain form: FP64 everywhere, matches the reference routines */
+    MG_PREC_MIXED = 1        /* FP32 fluxes and FP32 spectra, FP64 state, tendencies, tridiagonal,
+                                divergence residual; FP64-residual refinement of the Poisson solve */
+};
+
+/*
+ * Run parameters: the reference's module globals for this path
+ * (src/TYPES/shared_data.f90, INCLUDE/default.h).  Profile pointers are host
+ * arrays of length nz, copied at mg_create.
+ */
+typedef struct mg_params {
+    int maxx, maxy, nz;        /* interior sizes (MAXX, MAXY, MAXZ); nx = maxx+5, ny = maxy+5 */
+    int nscal;                 /* density-weighted scalars advected besides density:
+                                  scal[0] = es (potential temperature), then qt (if iqt >= 0),
+                                  then passive scalars */
+    int iqt;                   /* index of qt in scal[], or -1 (dry) */
+    int scal_adv;              /* MG_WENO / MG_PPM / MG_MUSCL (scal_adv, sorder=2, limit=.true.) */
+    int muscl_limiter;         /* MG_LIM_* (module default 'minmod') */
+    int mom_ord;               /* 2 or 4 (windadv.f90:515-519); 3 is rejected */
+    int lavisc;                /* artificial viscosity (lavisc) */
+    int nsubp;                 /* pressure sub-iterations (nsubp >= 1) */
+    int with_buoy;             /* buoyancy (with_buoy, imp_buoy=.true.) */
+    int precision;             /* MG_PREC_* */
+    int refine_iters;          /* mixed form: max FP64-residual refinement passes per projection */
+    double dx, dy, dz, dt0;
+    double lim_tol;            /* MUSCL tolerance (lim_tol) */
+    double u0shift, v0shift;   /* Galilean shift of the advective velocity */
+    double refine_tol;         /* mixed form: stop refining when max|div(rho0 u)|/rho0 < tol [1/s] */
+    const double *fdz0, *dzw, *dz1w, *dz1;              /* grid metrics, define_grid.f90:179-187 */
+    const double *den0, *avden0, *stab0, *pt0, *qv0;     /* base state, initial.f90:500-558 */
+} mg_params;
+
+typedef struct mg_ctx mg_ctx;
+
+const char *mg_error_string(int code);
+int mg_version(void);
+
+/* ---- host precompute: the reference's once-per-run init routines ---- */
+/* src/TOOLS/define_grid.f90:179-187 */
+int mg_grid_metrics(int nz, double dz, const double *fdz, double *dzw, double *dz1w, double *dz1);
+/* src/IO/initial.f90:473-558 (dry cp/cv, with_t=.false.); p0 and den0 by the hydrostatic recurrence */
+int mg_base_state(int nz, double dz, double psurf, const double *fdz0, const double *dz1,
+                  const double *pt0, const double *qv0,
+                  double *p0, double *den0, double *avden0, double *stab0);
+/* src/PRESSURE/fft_tools.f90:46-112: wv(1:maxx,1:maxy), l fastest */
+int mg_get_wv(int maxx, int maxy, double dx, double dy, double *wv);
+
+/* ---- context: device-resident fields of one domain, one CUDA stream ----
+ * Replaces the reference's allocations of the shared_* modules for this path
+ * (src/TOOLS/alloc.f90) and get_wv at init (src/MAIN/modelctl.f90:172-174). */
+int mg_create(const mg_params *params, int device, mg_ctx **out);
+int mg_destroy(mg_ctx *ctx);
+/* bytes of device memory held by the context */
+size_t mg_device_bytes(const mg_ctx *ctx);
+
+/* ---- resident state (time level n, natural variables) ----
+ * u, v, w: velocities; p: pressure perturbation; dens: prognostic density;
+ * scal[s]: natural scalars (es = theta first).  Host pointers, reference layout.
+ * Replaces the wind2/pressure2/state2 hand-over of time_step.f90:172-194,447-503. */
+int mg_upload_state(mg_ctx *ctx, const double *u, const double *v, const double *w,
+                    const double *p, const double *dens, const double *const *scal);
+int mg_download_state(mg_ctx *ctx, double *u, double *v, double *w, double *p,
+                      double *dens, double *const *scal);
+/* Device-pointer variants (pointers into device memory, same layout) */
+int mg_upload_state_device(mg_ctx *ctx, const double *u, const double *v, const double *w,
+                           const double *p, const double *dens, const double *const *scal);
+int mg_download_state_device(mg_ctx *ctx, double *u, double *v, double *w, double *p,
+                             double *dens, double *const *scal);
+
+/* ---- integration ----
+ * nsteps calls of `stepping` (src/INTEG/time_step.f90:76-334, dynamics subset):
+ * two Heun stages, each = scalar advection + momentum + stage update + projection.
+ * ntime0 is the reference's step counter of the first step (it sets the direction
+ * order of momentum advection, windadv.f90:103,158).  maxdiv (optional) receives
+ * the signed max of the post-projection divergence of the last stage
+ * (pressure_solver.f90:125), p1 (optional, nz) the hydrostatic correction. */
+int mg_step(mg_ctx *ctx, int nsteps, int ntime0, double *maxdiv, double *p1);
+/* Same, recorded once in a CUDA graph per (nsteps parity) and replayed. */
+int mg_step_graph(mg_ctx *ctx, int nsteps, int ntime0, double *maxdiv, double *p1);
+/* wait for all work queued on the context's stream */
+int mg_synchronize(mg_ctx *ctx);
+/* most recent kernel-launch count of mg_step (kernels launched per call) */
+int mg_last_launch_count(const mg_ctx *ctx);
+
+/* ---- timing and profiling (no counterpart in the reference, whose only timer is the
+ * per-step wall clock of src/MAIN/modelctl.f90:395-397) ---- */
+/* device time of nsteps steps, CUDA events recorded on the context's stream */
+int mg_time_steps(mg_ctx *ctx, int nsteps, int ntime0, int use_graph, double *ms);
+/* per-kernel event timing of subsequent eager steps (on != 0); resets the totals */
+int mg_profile_enable(mg_ctx *ctx, int on);
+/* text report, one line per kernel group: "<name> <launches> <total ms>" */
+int mg_profile_report(mg_ctx *ctx, char *buf, size_t len);
+
+/* ---- unit-level entry points (host buffers, reference layout) ---- */
+/* advection_ac (src/TOOLS/advection.f90:801-915) of one density-weighted field x with
+ * the advective velocity derived from momentum (mu,mv,mw) as get_advective does
+ * (funcpack.f90:65-94): xs := ((xs - Tx) - Ty) - Tz. */
+int mg_advection_ac(mg_ctx *ctx, const double *x, const double *mu, const double *mv,
+                    const double *mw, double *xs);
+/* qnadv_uvw (src/INTEG/windadv.f90:46-79): momentum advection tendency of (mu,mv,mw)
+ * with the advective velocity derived from them; positive sign convention (winda). */
+int mg_qnadv_uvw(mg_ctx *ctx, int ntime, const double *mu, const double *mv, const double *mw,
+                 double *au, double *av, double *aw);
+/* fft_solve (src/PRESSURE/pressure_solver.f90:462-538 -> fft_interface.f90:543-666):
+ * out(interior) = the unnormalised solution of the per-wavenumber vertical system
+ * for right-hand side tend; mode (0,0) is returned as the reference leaves it
+ * (the horizontal sum of tend per level). */
+int mg_fft_solve(mg_ctx *ctx, const double *tend, double *out);
+/* anelastic_pressure (src/PRESSURE/pressure_solver.f90:73-140): nsubp passes of
+ * solve + correction, cal_p1, residual.  mu,mv,mw,p in/out; wold = momentum w at the
+ * start of the stage. */
+int mg_anelastic_pressure(mg_ctx *ctx, double *mu, double *mv, double *mw, double *p,
+                          const double *wold, double *maxdiv, double *p1);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

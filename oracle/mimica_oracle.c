@@ -1,0 +1,1555 @@
+/*
+ * mimica_oracle.c -- CPU FP64 restatement of MIMICA's dynamical-core hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker for the CUDA path; see mimica_oracle.h).
+ *
+ * Every routine restates one reference routine; expressions keep the reference's
+ * left-to-right evaluation order so that the plain-FP64 CUDA kernels, compiled
+ * without FMA contraction, reproduce them bit for bit.  Build with
+ * -O2 -fno-fast-math -ffp-contract=off.
+ *
+ * Documented deviations from the reference (each one a choice the reference
+ * leaves undefined):
+ *  - advsz_weno interior-face loop starts at k=2: the reference loop
+ *    `do k=k1,k2-2` with k1=1 reads x(0) outside the pencil
+ *    (src/TOOLS/advq_weno.f90:245) and overwrites the one-sided bottom flux of
+ *    :232-241.  The intended one-sided bottom flux is kept.
+ *  - `(eps+eta)**exp` with exp=2 is evaluated as the correctly rounded product
+ *    y*y (advq_weno.f90:334-337).
+ *  - mom_ord=3 (c1, c2 uninitialised in windadv.f90:515-519) is rejected by the
+ *    host layer; only 2 and 4 are accepted.
+ *  - Lateral BCs are periodic and vertical BCs rigid ('nnf'); other bcl values
+ *    are out of scope.
+ */
+#include "mimica_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define IX(g, i, j, k) ((((size_t)(k) - 1) * (size_t)(g)->ny + (size_t)((j) - 1)) * (size_t)(g)->nx + (size_t)((i) - 1))
+#define P1(a, i) (a)[(i) - 1]
+
+static inline int imax(int a, int b) { return a > b ? a : b; }
+static inline int imin(int a, int b) { return a < b ? a : b; }
+static inline double dmax2(double a, double b) { return a > b ? a : b; }
+static inline double dmin2(double a, double b) { return a < b ? a : b; }
+static inline double fsign1(double b) { return copysign(1.0, b); } /* Fortran sign(1.,b) */
+
+static size_t ncell(const mo_grid *g) { return (size_t)g->nx * g->ny * g->nz; }
+static double *dalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
+
+/* ======================================================================
+ * Host precompute
+ * ==================================================================== */
+
+/* src/TOOLS/define_grid.f90:179-187 */
+void mo_grid_metrics(int nz, double dz, const double *fdz, double *dzw, double *dz1w, double *dz1)
+{
+    for (int k = 1; k <= nz; k++) {
+        P1(dzw, k) = dz * P1(fdz, k);
+        P1(dz1w, k) = 1.0 / (dz * P1(fdz, k));
+    }
+    for (int k = 1; k <= nz - 1; k++)
+        P1(dz1, k) = 1.0 / ((dz * 0.5) * (P1(fdz, k) + P1(fdz, k + 1)));
+    P1(dz1, nz) = P1(dz1, nz - 1);
+}
+
+/* src/IO/initial.f90:473-564, with_t=.false., with_rh=.false., cst_cp=1
+ * (cp=cp_a, cv=cv_a, src/TOOLS/thermodynamics.f90:422-469); constants from
+ * src/TYPES/shared_data.f90:147-149 and src/TYPES/shared_thermo.f90:53-54. */
+void mo_base_state(int nz, double dz, double psurf, const double *fdz0, const double *dz1,
+                   const double *pt0, const double *qv0,
+                   double *p0, double *den0, double *avden0, double *stab0)
+{
+    const double g = 9.81, pref = 100000., cp_a = 1004., cv_a = 716.;
+    const double cpm = cp_a, cvm = cv_a;
+    const double ex = (cp_a - cv_a) / cp_a;
+    (void)qv0;
+    double dsurf = 0.0;
+    P1(p0, 1) = psurf;
+    for (int l = 1; l <= 10; l++) {
+        P1(den0, 1) = P1(p0, 1) / ((cpm - cvm) * P1(pt0, 1) * pow(P1(p0, 1) / pref, ex));
+        dsurf = psurf / ((cpm - cvm) * P1(pt0, 1) * pow(psurf / pref, ex));
+        P1(p0, 1) = psurf - g * 0.5 * (dsurf + P1(den0, 1)) * 0.5 * dz * P1(fdz0, 1);
+    }
+    for (int k = 2; k <= nz; k++) {
+        P1(p0, k) = P1(p0, k - 1) - g * P1(den0, k - 1) / P1(dz1, k - 1);
+        for (int l = 1; l <= 10; l++) {
+            P1(den0, k) = P1(p0, k) / ((cpm - cvm) * P1(pt0, k) * pow(P1(p0, k) / pref, ex));
+            P1(p0, k) = P1(p0, k - 1) - g * 0.5 * (P1(den0, k - 1) + P1(den0, k)) / P1(dz1, k - 1);
+        }
+    }
+    for (int k = 2; k <= nz; k++)
+        P1(avden0, k) = (P1(fdz0, k) * P1(den0, k) + P1(fdz0, k - 1) * P1(den0, k - 1)) /
+                        (P1(fdz0, k) + P1(fdz0, k - 1));
+    P1(avden0, 1) = P1(den0, 1);
+    for (int k = 2; k <= nz - 1; k++)
+        P1(stab0, k) = (P1(den0, k + 1) - P1(den0, k - 1)) /
+                       (P1(den0, k) * dz * (0.5 * P1(fdz0, k + 1) + P1(fdz0, k) + 0.5 * P1(fdz0, k - 1)));
+    P1(stab0, 1) = (P1(den0, 2) - P1(den0, 1)) / (P1(den0, 1) * 0.5 * dz * (P1(fdz0, 2) + P1(fdz0, 1)));
+    P1(stab0, nz) = (P1(den0, nz) - P1(den0, nz - 1)) /
+                    (P1(den0, nz) * 0.5 * dz * (P1(fdz0, nz) + P1(fdz0, nz - 1)));
+}
+
+/* src/PRESSURE/fft_tools.f90:46-112, serial, MODEL_3D, not CHANNEL.
+ * pi is the reference's truncated constant (src/TYPES/shared_data.f90:147). */
+void mo_get_wv(int nxp, int nyp, double dx, double dy, double *wv)
+{
+    const double pi = 3.14159265;
+    int nl = nxp, nm = nyp > 1 ? nyp : 1;
+    for (int l = 1; l <= nxp; l++) {
+        double xl = (l <= nl / 2) ? (double)(l - 1) : (double)(l - nl - 1);
+        for (int m = 1; m <= nyp; m++) {
+            double xm = (m <= nm / 2) ? (double)(m - 1) : (double)(m - nm - 1);
+            double sx = sin(pi * xl / (double)nl), sy = sin(pi * xm / (double)nm);
+            wv[(size_t)(m - 1) * nxp + (l - 1)] = -4. * (sx * sx / (dx * dx) + sy * sy / (dy * dy));
+        }
+    }
+    wv[0] = 1.;
+}
+
+/* ======================================================================
+ * Halo maps: src/TOOLS/bc.f90 qnbc_p4 :378-502 and lbcu_p4 :81-343,
+ * serial periodic branches (x first over all j, then y over all i).
+ * ==================================================================== */
+void mo_statebc(const mo_grid *g, double *x)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    for (int k = 1; k <= nz; k++)
+        for (int j = 1; j <= ny; j++) {
+            x[IX(g, 1, j, k)] = x[IX(g, nx - 4, j, k)];
+            x[IX(g, 2, j, k)] = x[IX(g, nx - 3, j, k)];
+            x[IX(g, 3, j, k)] = x[IX(g, nx - 2, j, k)];
+            x[IX(g, nx, j, k)] = x[IX(g, 5, j, k)];
+            x[IX(g, nx - 1, j, k)] = x[IX(g, 4, j, k)];
+        }
+    for (int k = 1; k <= nz; k++)
+        for (int i = 1; i <= nx; i++) {
+            x[IX(g, i, 1, k)] = x[IX(g, i, ny - 4, k)];
+            x[IX(g, i, 2, k)] = x[IX(g, i, ny - 3, k)];
+            x[IX(g, i, 3, k)] = x[IX(g, i, ny - 2, k)];
+            x[IX(g, i, ny, k)] = x[IX(g, i, 5, k)];
+            x[IX(g, i, ny - 1, k)] = x[IX(g, i, 4, k)];
+        }
+}
+
+static void windbc(const mo_grid *g, double *u, double *v, double *w)
+{
+    mo_statebc(g, u);
+    mo_statebc(g, v);
+    mo_statebc(g, w);
+}
+
+/* ======================================================================
+ * Scalar advection schemes, one pencil.  Arrays x,u,xa are 1-based P1().
+ * ==================================================================== */
+
+/* src/TOOLS/advq_weno.f90:462-491 */
+static void limiter_weno(double *ffim1, double *ffip1m, double *ffip1p, double *ffip2, double x)
+{
+    const double eps = 1.e-15;
+    double minp = dmin2(dmin2(dmin2(*ffim1, *ffip1m), *ffip1p), *ffip2);
+    double phi = dmin2(fabs((0. - x) / ((minp - x) + eps)), 1.);
+    *ffim1 = phi * (*ffim1 - x) + x;
+    *ffip1m = phi * (*ffip1m - x) + x;
+    *ffip1p = phi * (*ffip1p - x) + x;
+    *ffip2 = phi * (*ffip2 - x) + x;
+}
+
+/* weights of one face, src/TOOLS/advq_weno.f90:304-353 (loop body) */
+static void weno_weights(double xm1, double x0, double xp1, double xp2, double ww[4])
+{
+    const double g1 = 1. / 3., g2 = 2. / 3., eps = 1.e-15, thres = 20.;
+    double d1 = x0 - xm1, d2 = xp1 - x0, d3 = xp2 - xp1;
+    double eta1 = d1 * d1, eta2 = d2 * d2, eta3 = d3 * d3;
+    double y1 = eps + eta1, y2 = eps + eta2, y3 = eps + eta3;
+    double w1 = g1 / (y1 * y1), w2 = g2 / (y2 * y2), w3 = g2 / (y2 * y2), w4 = g1 / (y3 * y3);
+    if (dmax2(eta1, eta2) / (dmin2(eta1, eta2) + eps) > thres) {
+        double sumw = w1 + w2;
+        ww[0] = w1 / sumw;
+        ww[1] = w2 / sumw;
+    }
+    if (dmax2(eta2, eta3) / (dmin2(eta2, eta3) + eps) > thres) {
+        double sumw = w3 + w4;
+        ww[2] = w3 / sumw;
+        ww[3] = w4 / sumw;
+    }
+}
+
+/* src/TOOLS/advq_weno.f90:61-131 (x) and :134-199 (y) */
+static void advs_weno_h(int n, int i1, int i2, double d, const double *x, const double *u, double *xa, int adv)
+{
+    const double g1 = 1. / 3., g2 = 2. / 3.;
+    double dx1 = 1. / d;
+    int ii1 = imax(i1 - 1, 2), ii2 = imin(i2, n - 2);
+    double *F = dalloc((size_t)n);
+    for (int i = ii1; i <= ii2; i++) {
+        double ww[4] = {g1, g2, g2, g1};
+        weno_weights(P1(x, i - 1), P1(x, i), P1(x, i + 1), P1(x, i + 2), ww);
+        double uu = P1(u, i + 1);
+        double ffim1 = (-(1. / 2. * P1(x, i - 1)) + 3. / 2. * P1(x, i));
+        double ffip1p = (1. / 2. * P1(x, i) + 1. / 2. * P1(x, i + 1));
+        double ffip1m = (1. / 2. * P1(x, i) + 1. / 2. * P1(x, i + 1));
+        double ffip2 = (3. / 2. * P1(x, i + 1) - 1. / 2. * P1(x, i + 2));
+        limiter_weno(&ffim1, &ffip1m, &ffip1p, &ffip2, P1(x, i));
+        double Fl = ww[0] * ffim1 + ww[1] * ffip1p;
+        double Fr = ww[2] * ffip1m + ww[3] * ffip2;
+        P1(F, i) = 0.5 * Fl * (uu + fabs(uu)) + 0.5 * Fr * (uu - fabs(uu));
+    }
+    double Fold = P1(F, ii1);
+    for (int i = ii1 + 1; i <= ii2; i++) {
+        P1(xa, i) = P1(xa, i) + (P1(F, i) - Fold) * dx1;
+        Fold = P1(F, i);
+    }
+    if (adv) {
+        double uold = P1(u, ii2 + 1);
+        for (int i = ii2; i >= ii1 + 1; i--) {
+            P1(xa, i) = P1(xa, i) - P1(x, i) * (uold - P1(u, i)) * dx1;
+            uold = P1(u, i);
+        }
+    }
+    free(F);
+}
+
+/* src/TOOLS/advq_weno.f90:202-301; weights of weightz(2,nz-2) (:408-459) cover
+ * k=3..nz-3 only.  Interior-face loop from k=2 (documented deviation). */
+static void advs_weno_z(const mo_grid *g, const double *x, const double *w, double *xa, int adv)
+{
+    const int nz = g->nz, k2 = nz;
+    const double g1 = 1. / 3., g2 = 2. / 3.;
+    const double *dz1w = g->dz1w;
+    double *F = dalloc((size_t)nz);
+    /* bottom face k=1: linear weights ww(1,3)=g2, ww(1,4)=g1, no limiter */
+    {
+        int k = 1;
+        double www = P1(w, k + 1);
+        double ffip1p = (1. / 2. * P1(x, k) + 1. / 2. * P1(x, k + 1));
+        double ffip1m = (1. / 2. * P1(x, k) + 1. / 2. * P1(x, k + 1));
+        double ffip2 = (3. / 2. * P1(x, k + 1) - 1. / 2. * P1(x, k + 2));
+        double Fl = ffip1p;
+        double Fr = g2 * ffip1m + g1 * ffip2;
+        P1(F, k) = 0.5 * Fl * (www + fabs(www)) + 0.5 * Fr * (www - fabs(www));
+    }
+    for (int k = 2; k <= k2 - 2; k++) {
+        double ww[4] = {g1, g2, g2, g1};
+        if (k >= 3 && k <= nz - 3)
+            weno_weights(P1(x, k - 1), P1(x, k), P1(x, k + 1), P1(x, k + 2), ww);
+        double www = P1(w, k + 1);
+        double ffim1 = (-(1. / 2. * P1(x, k - 1)) + 3. / 2. * P1(x, k));
+        double ffip1p = (1. / 2. * P1(x, k) + 1. / 2. * P1(x, k + 1));
+        double ffip1m = (1. / 2. * P1(x, k) + 1. / 2. * P1(x, k + 1));
+        double ffip2 = (3. / 2. * P1(x, k + 1) - 1. / 2. * P1(x, k + 2));
+        limiter_weno(&ffim1, &ffip1m, &ffip1p, &ffip2, P1(x, k));
+        double Fl = ww[0] * ffim1 + ww[1] * ffip1p;
+        double Fr = ww[2] * ffip1m + ww[3] * ffip2;
+        P1(F, k) = 0.5 * Fl * (www + fabs(www)) + 0.5 * Fr * (www - fabs(www));
+    }
+    {
+        int k = nz - 1;
+        double www = P1(w, k + 1);
+        double ffim1 = (-(1. / 2. * P1(x, k - 1)) + 3. / 2. * P1(x, k));
+        double ffip1p = (1. / 2. * P1(x, k) + 1. / 2. * P1(x, k + 1));
+        double ffip1m = (1. / 2. * P1(x, k) + 1. / 2. * P1(x, k + 1));
+        double Fl = g1 * ffim1 + g2 * ffip1p;
+        double Fr = ffip1m;
+        P1(F, k) = 0.5 * Fl * (www + fabs(www)) + 0.5 * Fr * (www - fabs(www));
+    }
+    double Fold = P1(F, 1);
+    for (int k = 2; k <= k2 - 1; k++) {
+        P1(xa, k) = P1(xa, k) + (P1(F, k) - Fold) * P1(dz1w, k);
+        Fold = P1(F, k);
+    }
+    if (adv) {
+        double wold = P1(w, k2);
+        for (int k = k2 - 1; k >= 2; k--) {
+            P1(xa, k) = P1(xa, k) - P1(x, k) * (wold - P1(w, k)) * P1(dz1w, k);
+            wold = P1(w, k);
+        }
+    }
+    P1(xa, 1) = P1(xa, 1) + (P1(F, 1) - 0.) * P1(dz1w, 1);
+    if (adv) P1(xa, 1) = P1(xa, 1) - P1(x, 1) * (P1(w, 2) - 0.) * P1(dz1w, 1);
+    P1(xa, nz) = P1(xa, nz) + (0. - P1(F, nz - 1)) * P1(dz1w, nz);
+    if (adv) P1(xa, nz) = P1(xa, nz) - P1(x, nz) * (0. - P1(w, nz)) * P1(dz1w, nz);
+    free(F);
+}
+
+/* spacing(x) of Fortran for real(8): 2**(exponent(x)-53), tiny(x) for x=0 */
+static double fspacing(double x)
+{
+    if (x == 0.0) return 2.2250738585072014e-308;
+    int e = ilogb(x) - 52;
+    if (e < -1022) return 2.2250738585072014e-308;
+    return ldexp(1.0, e);
+}
+
+/* src/TOOLS/advq_ppm.f90:449-530, ppmlimiter='PPM' (limit=.true.) */
+static void limiter_ppm(double xx, double xp, double xm, double xplus, double xmin, double ffip1,
+                        double ffip2, double ffim1, double ffim2, double *phir_o, double *phil_o,
+                        double *phi1_o, double *phi2_o)
+{
+    const double eps = 1.e-15, thres = 10.;
+    double rp1 = 1.;
+    double phir = xplus, phil = xmin;
+    double a, b;
+    a = ffip1 - ffim1; b = ffip1 + ffim1;
+    double gamma1 = 0.5 * (a * a + b * b);
+    a = ffip2 - ffip1; b = ffip2 + ffip1;
+    double gamma2 = 0.5 * (a * a + b * b);
+    a = ffim1 - ffim2; b = ffim1 + ffim2;
+    double gamma3 = 0.5 * (a * a + b * b);
+    double lambda = dmax2(dmax2(gamma1, gamma2), gamma3) / (dmin2(dmin2(gamma1, gamma2), gamma3) + eps);
+    double phi1 = phir - phil;
+    double phi2 = 3. * (phil - 2. * xx + phir);
+    if (lambda > thres) {
+        if (phir < 0. || ((phir - xx) * (xp - phir) < 0. &&
+                          (ffim1 * ffip2 >= 0. || ffim1 * ffip1 <= 0. || ffip2 * ffip1 <= 0.))) {
+            if (fabs(phir - xx) < fabs(phir - xp)) phir = xx;
+            else phir = xp;
+        }
+        if (phil < 0. || ((xx - phil) * (phil - xm) < 0. &&
+                          (ffim2 * ffip1 >= 0. || ffim2 * ffim1 <= 0. || ffip1 * ffim1 <= 0.))) {
+            if (fabs(phil - xx) < fabs(phil - xm)) phil = xx;
+            else phil = xm;
+        }
+        phi1 = phir - phil;
+        phi2 = 3. * (phil - 2. * xx + phir);
+        double slope = -(0.5 * phi1 / (fsign1(phi2) * dmax2(fabs(phi2), eps)));
+        if (fabs(ffim1) > sqrt(fspacing(ffim1))) rp1 = ffip1 / ffim1;
+        if (fabs(phi2) > eps && (slope > -1. / 2. || slope < 1. / 2.)) {
+            double lim = dmax2(0., dmin2(dmin2(2., 0.5 * (rp1 + 1.)), 2. * rp1));
+            phir = xx + 0.5 * ffim1 * lim;
+            phil = xx - 0.5 * ffim1 * lim;
+            if ((xx - phil) * (phir - xx) < 0.) {
+                phil = xx;
+                phir = xx;
+            }
+            phi1 = phir - phil;
+            phi2 = 0.;
+        }
+    }
+    *phir_o = phir; *phil_o = phil; *phi1_o = phi1; *phi2_o = phi2;
+}
+
+#define PPM_FLUX_R(phir, mup, phi1, phi2) ((phir) - 0.5 * (mup) * ((phi1) + (1. - 2. / 3. * (mup)) * (phi2)))
+#define PPM_FLUX_L(phil, muc, phi1, phi2) ((phil) + 0.5 * (muc) * ((phi1) - (1. - 2. / 3. * (muc)) * (phi2)))
+
+/* src/TOOLS/advq_ppm.f90:55-169 (x) and :172-286 (y); lateral BCs periodic so the
+ * non-periodic edge fixes (:138-146) do not apply. */
+static void advs_ppm_h(const mo_grid *g, int n, int i1, int i2, double d, const double *x,
+                       const double *u, double *xa, int adv)
+{
+    const double dt0 = g->dt0;
+    double dx1 = 1. / d;
+    int ii1 = imax(i1 - 1, 2), ii2 = imin(i2, n - 2);
+    double *Fr = dalloc((size_t)n), *Fl = dalloc((size_t)n);
+    double mup, muc, ffip1, ffip2, ffim1, ffim2, xmin, xplus, phir, phil, phi1, phi2, sl, slp1;
+
+    mup = fabs(P1(u, ii1 + 1)) * dt0 * dx1;
+    muc = fabs(P1(u, ii1)) * dt0 * dx1;
+    ffip1 = (P1(x, ii1 + 1) - P1(x, ii1));
+    ffip2 = (P1(x, ii1 + 2) - P1(x, ii1 + 1));
+    ffim1 = (P1(x, ii1) - P1(x, ii1 - 1));
+    ffim2 = (P1(x, ii1) - P1(x, ii1 - 1));
+    xmin = 0.5 * (P1(x, ii1 + 1) + P1(x, ii1));
+    xplus = P1(x, ii1) + 0.5 * ffip1;
+    limiter_ppm(P1(x, ii1), P1(x, ii1 + 1), P1(x, ii1 - 1), xplus, xmin, ffip1, ffip2, ffim1, ffim2,
+                &phir, &phil, &phi1, &phi2);
+    P1(Fr, ii1) = PPM_FLUX_R(phir, mup, phi1, phi2);
+    P1(Fl, ii1) = PPM_FLUX_L(phil, muc, phi1, phi2);
+
+    xmin = xplus;
+    for (int i = ii1 + 1; i <= ii2; i++) {
+        mup = fabs(P1(u, i + 1)) * dt0 * dx1;
+        muc = fabs(P1(u, i)) * dt0 * dx1;
+        ffip1 = (P1(x, i + 1) - P1(x, i));
+        ffip2 = (P1(x, i + 2) - P1(x, i + 1));
+        ffim1 = (P1(x, i) - P1(x, i - 1));
+        ffim2 = (P1(x, i - 1) - P1(x, i - 2));
+        sl = 0.5 * (ffip1 + ffim1);
+        slp1 = 0.5 * (ffip2 + ffip1);
+        xplus = P1(x, i) + 0.5 * ffip1 - 1. / 6. * (slp1 - sl);
+        limiter_ppm(P1(x, i), P1(x, i + 1), P1(x, i - 1), xplus, xmin, ffip1, ffip2, ffim1, ffim2,
+                    &phir, &phil, &phi1, &phi2);
+        P1(Fr, i) = PPM_FLUX_R(phir, mup, phi1, phi2);
+        P1(Fl, i) = PPM_FLUX_L(phil, muc, phi1, phi2);
+        xmin = xplus;
+    }
+
+    mup = fabs(P1(u, ii2 + 2)) * dt0 * dx1;
+    muc = fabs(P1(u, ii2 + 1)) * dt0 * dx1;
+    ffip1 = (P1(x, ii2 + 2) - P1(x, ii2 + 1));
+    ffip2 = (P1(x, ii2 + 2) - P1(x, ii2 + 1));
+    ffim1 = (P1(x, ii2 + 1) - P1(x, ii2));
+    ffim2 = (P1(x, ii2) - P1(x, ii2 - 1));
+    xplus = P1(x, ii2 + 1) + 0.5 * ffip1;
+    limiter_ppm(P1(x, ii2 + 1), P1(x, ii2 + 2), P1(x, ii2), xplus, xmin, ffip1, ffip2, ffim1, ffim2,
+                &phir, &phil, &phi1, &phi2);
+    P1(Fr, ii2 + 1) = PPM_FLUX_R(phir, mup, phi1, phi2);
+    P1(Fl, ii2 + 1) = PPM_FLUX_L(phil, muc, phi1, phi2);
+
+    for (int i = ii1 + 1; i <= ii2; i++) {
+        double ui = P1(u, i), up = P1(u, i + 1);
+        double Fo = 0.5 * P1(Fr, i - 1) * (ui + fabs(ui)) + 0.5 * P1(Fl, i) * (ui - fabs(ui));
+        double Fn = 0.5 * P1(Fr, i) * (up + fabs(up)) + 0.5 * P1(Fl, i + 1) * (up - fabs(up));
+        P1(xa, i) = P1(xa, i) + (Fn - Fo) * dx1;
+    }
+    if (adv) {
+        double uold = P1(u, ii2 + 1);
+        for (int i = ii2; i >= ii1 + 1; i--) {
+            P1(xa, i) = P1(xa, i) - P1(x, i) * (uold - P1(u, i)) * dx1;
+            uold = P1(u, i);
+        }
+    }
+    free(Fr);
+    free(Fl);
+}
+
+/* src/TOOLS/advq_ppm.f90:289-446 with bcl(5)=bcl(6)='nnf' (bc51=bc61=0) */
+static void advs_ppm_z(const mo_grid *g, const double *x, const double *w, double *xa, int adv)
+{
+    const int nz = g->nz, k2 = nz;
+    const double dt0 = g->dt0;
+    const double *dz1 = g->dz1, *dz1w = g->dz1w;
+    const double bc51 = 0., bc61 = 0.;
+    double *Fr = dalloc((size_t)nz), *Fl = dalloc((size_t)nz);
+    double mup, muc, ffip1, ffip2, ffim1, ffim2, xmin, xplus, phir, phil, phi1, phi2, sl, slp1;
+    int k;
+
+    k = 1;
+    mup = fabs(P1(w, k + 1)) * dt0 * P1(dz1, k);
+    muc = fabs(P1(w, k)) * dt0 * P1(dz1, k);
+    ffip1 = P1(x, k + 1) - P1(x, k);
+    ffip2 = P1(x, k + 2) - P1(x, k + 1);
+    ffim1 = bc51 * (P1(x, nz - 4) - P1(x, nz - 5));
+    ffim2 = bc51 * (P1(x, nz - 5) - P1(x, nz - 6));
+    xmin = P1(x, k) - 0.5 * ffip1;
+    xplus = P1(x, k) + 0.5 * ffip1;
+    limiter_ppm(P1(x, k), P1(x, k + 1), P1(x, k + 1), xplus, xmin, ffip1, ffip2, ffim1, ffim2,
+                &phir, &phil, &phi1, &phi2);
+    P1(Fr, k) = PPM_FLUX_R(phir, mup, phi1, phi2);
+    P1(Fl, k) = PPM_FLUX_L(phil, muc, phi1, phi2);
+
+    k = 2;
+    xmin = xplus;
+    mup = fabs(P1(w, k + 1)) * dt0 * P1(dz1, k);
+    muc = fabs(P1(w, k)) * dt0 * P1(dz1, k);
+    ffip1 = P1(x, k + 1) - P1(x, k);
+    ffip2 = P1(x, k + 2) - P1(x, k + 1);
+    ffim1 = (P1(x, k) - P1(x, k - 1));
+    ffim2 = bc51 * (P1(x, nz - 4) - P1(x, nz - 5));
+    xplus = P1(x, k) + 0.5 * ffip1;
+    limiter_ppm(P1(x, k), P1(x, k + 1), P1(x, k - 1), xplus, xmin, ffip1, ffip2, ffim1, ffim2,
+                &phir, &phil, &phi1, &phi2);
+    P1(Fr, k) = PPM_FLUX_R(phir, mup, phi1, phi2);
+    P1(Fl, k) = PPM_FLUX_L(phil, muc, phi1, phi2);
+
+    xmin = xplus;
+    for (k = 3; k <= nz - 2; k++) {
+        mup = fabs(P1(w, k + 1)) * dt0 * P1(dz1, k);
+        muc = fabs(P1(w, k)) * dt0 * P1(dz1, k);
+        ffip1 = (P1(x, k + 1) - P1(x, k));
+        ffip2 = (P1(x, k + 2) - P1(x, k + 1));
+        ffim1 = (P1(x, k) - P1(x, k - 1));
+        ffim2 = (P1(x, k - 1) - P1(x, k - 2));
+        double delta = P1(dz1w, k), deltam1 = P1(dz1w, k - 1), deltap1 = P1(dz1w, k + 1), deltap2 = P1(dz1w, k + 2);
+        sl = delta / (deltam1 + delta + deltap1) *
+             ((2. * deltam1 + delta) / (deltap1 + delta) * ffip1 + (delta + 2. * deltap1) / (deltam1 + delta) * ffim1);
+        slp1 = deltap1 / (delta + deltap1 + deltap2) *
+               ((2. * delta + deltap1) / (deltap2 + deltap1) * ffip2 + (deltap1 + 2. * deltap2) / (delta + deltap1) * ffip1);
+        xplus = P1(x, k) + delta / (delta + deltap1) * ffip1 +
+                1. / (deltam1 + delta + deltap1 + deltap2) *
+                    (2. * deltap1 * delta / (delta + deltap1) *
+                         ((deltam1 + delta) / (2. * delta + deltap1) - (deltap2 + deltap1) / (2. * deltap1 + delta)) * ffip1 -
+                     delta * (deltam1 + delta) / (2. * delta + deltap1) * slp1 +
+                     deltap1 * (deltap1 + deltap2) / (2. * deltap1 + delta) * sl);
+        limiter_ppm(P1(x, k), P1(x, k + 1), P1(x, k - 1), xplus, xmin, ffip1, ffip2, ffim1, ffim2,
+                    &phir, &phil, &phi1, &phi2);
+        P1(Fr, k) = PPM_FLUX_R(phir, mup, phi1, phi2);
+        P1(Fl, k) = PPM_FLUX_L(phil, muc, phi1, phi2);
+        xmin = xplus;
+    }
+
+    k = nz - 1;
+    mup = fabs(P1(w, k + 1)) * dt0 * P1(dz1, k);
+    muc = fabs(P1(w, k)) * dt0 * P1(dz1, k);
+    ffip1 = P1(x, k + 1) - P1(x, k);
+    ffim1 = P1(x, k) - P1(x, k - 1);
+    ffim2 = P1(x, k - 1) - P1(x, k - 2);
+    ffip2 = bc61 * (P1(x, 6) - P1(x, 5)) + (1. - bc61) * ffip1;
+    xplus = P1(x, k) + 0.5 * ffip1;
+    limiter_ppm(P1(x, k), P1(x, k + 1), P1(x, k - 1), xplus, xmin, ffip1, ffip2, ffim1, ffim2,
+                &phir, &phil, &phi1, &phi2);
+    P1(Fr, k) = PPM_FLUX_R(phir, mup, phi1, phi2);
+    P1(Fl, k) = PPM_FLUX_L(phil, muc, phi1, phi2);
+
+    k = nz;
+    muc = fabs(P1(w, k)) * dt0 * P1(dz1, k);
+    ffim1 = P1(x, k) - P1(x, k - 1);
+    P1(Fl, k) = P1(x, k) + 0.5 * ffim1 * (1. - muc);
+
+    double w2 = P1(w, 2);
+    double Fo = 0.5 * P1(Fr, 1) * (w2 + fabs(w2)) + 0.5 * P1(Fl, 2) * (w2 - fabs(w2));
+    for (k = 2; k <= k2 - 1; k++) {
+        double wk = P1(w, k + 1);
+        double Fn = 0.5 * P1(Fr, k) * (wk + fabs(wk)) + 0.5 * P1(Fl, k + 1) * (wk - fabs(wk));
+        P1(xa, k) = P1(xa, k) + (Fn - Fo) * P1(dz1w, k);
+        Fo = Fn;
+    }
+    if (adv) {
+        double wold = P1(w, k2);
+        for (k = k2 - 1; k >= 2; k--) {
+            P1(xa, k) = P1(xa, k) - P1(x, k) * (wold - P1(w, k)) * P1(dz1w, k);
+            wold = P1(w, k);
+        }
+    }
+    P1(xa, 1) = P1(xa, 1) + (0.5 * P1(Fr, 1) * (w2 + fabs(w2)) + 0.5 * P1(Fl, 2) * (w2 - fabs(w2)) - 0.) * P1(dz1w, 1);
+    if (adv) P1(xa, 1) = P1(xa, 1) - P1(x, 1) * (P1(w, 2) - 0.) * P1(dz1w, 1);
+    P1(xa, nz) = P1(xa, nz) + (0. - Fo) * P1(dz1w, nz);
+    if (adv) P1(xa, nz) = P1(xa, nz) - P1(x, nz) * (0. - P1(w, nz)) * P1(dz1w, nz);
+    free(Fr);
+    free(Fl);
+}
+
+/* src/TOOLS/advq_muscl.f90:335-383 */
+static void limiter_muscl(const mo_grid *g, double xx, double ffip1, double ffip2, double ffim1,
+                          double *phir, double *phil)
+{
+    const double lim_tol = g->lim_tol;
+    double rp1 = 1., rp2 = 1.;
+    if (fabs(ffim1) > lim_tol * fabs(xx) && fabs(ffip1) < fabs(ffim1) / lim_tol) rp1 = ffip1 / ffim1;
+    if (fabs(ffip2) > lim_tol * fabs(xx) && fabs(ffip1) < fabs(ffip2) / lim_tol) rp2 = ffip1 / ffip2;
+    switch (g->muscl_limiter) {
+    case MO_LIM_VL:
+        *phil = (rp1 + fabs(rp1)) / (1. + fabs(rp1));
+        *phir = (rp2 + fabs(rp2)) / (1. + fabs(rp2));
+        break;
+    case MO_LIM_MC:
+        *phil = dmax2(0., dmin2(dmin2(2. * rp1, 0.5 * (rp1 + 1.)), 2.));
+        *phir = dmax2(0., dmin2(dmin2(2. * rp2, 0.5 * (rp2 + 1.)), 2.));
+        break;
+    case MO_LIM_MINMOD:
+        *phil = dmax2(0., dmin2(1., rp1));
+        *phir = dmax2(0., dmin2(1., rp2));
+        break;
+    default:
+        *phil = 0.5 * (rp1 + 1.);
+        *phir = 0.5 * (rp2 + 1.);
+        break;
+    }
+}
+
+/* src/TOOLS/advq_muscl.f90:56-122 (x) and :125-205 (y, CHANNEL off) */
+static void advs_muscl_h(const mo_grid *g, int n, int i1, int i2, double d, const double *x,
+                         const double *u, double *xa, int adv)
+{
+    const double eps = 1.e-18, lim_tol = g->lim_tol;
+    double dx1 = 1. / d;
+    double *F = dalloc((size_t)n);
+    for (int i = i1 - 1; i <= i2; i++) {
+        double uu = P1(u, i + 1), xx = P1(x, i);
+        double slope_p = (P1(x, i + 1) - xx) * dx1;
+        double slope_p2 = (P1(x, i + 2) - P1(x, i + 1)) * dx1;
+        double slope_m = (xx - P1(x, i - 1)) * dx1;
+        double Fr, Fl, phir, phil;
+        if (d * fabs(slope_m) > lim_tol * fabs(xx) + eps || d * fabs(slope_p2) > lim_tol * fabs(xx) + eps) {
+            limiter_muscl(g, xx, slope_p, slope_p2, slope_m, &phir, &phil);
+            Fr = P1(x, i + 1) - 0.5 * phir * slope_p2 * d;
+            Fl = xx + 0.5 * phil * slope_m * d;
+        } else {
+            Fr = P1(x, i + 1) - 0.5 * slope_p * d;
+            Fl = xx + 0.5 * slope_p * d;
+        }
+        P1(F, i) = 0.5 * uu * (Fl * (1. + fsign1(uu)) + Fr * (1. - fsign1(uu)));
+    }
+    double Fold = P1(F, i1 - 1);
+    for (int i = i1; i <= i2; i++) {
+        P1(xa, i) = P1(xa, i) + (P1(F, i) - Fold) * dx1;
+        Fold = P1(F, i);
+    }
+    if (adv) {
+        double uold = P1(u, i2 + 1);
+        for (int i = i2; i >= i1; i--) {
+            P1(xa, i) = P1(xa, i) - P1(x, i) * (uold - P1(u, i)) * dx1;
+            uold = P1(u, i);
+        }
+    }
+    free(F);
+}
+
+/* src/TOOLS/advq_muscl.f90:208-332 with bcl(5)=bcl(6)='nnf' */
+static void advs_muscl_z(const mo_grid *g, const double *x, const double *w, double *xa, int adv)
+{
+    const int nz = g->nz, k2 = nz;
+    const double eps = 1.e-18, lim_tol = g->lim_tol, dz = g->dz;
+    const double *dz1 = g->dz1, *dz1w = g->dz1w, *fdz0 = g->fdz0;
+    const double bc51 = 0., bc61 = 0.;
+    double *F = dalloc((size_t)nz);
+    double ww, slope_p, slope_p2, slope_m, Fl, Fr, phir, phil;
+    int k;
+
+    k = 1;
+    ww = P1(w, 2);
+    slope_p = (P1(x, 2) - P1(x, 1)) * P1(dz1, 1);
+    slope_p2 = (P1(x, 3) - P1(x, 2)) * P1(dz1, 2);
+    slope_m = bc51 * (P1(x, nz - 4) - P1(x, nz - 5)) * P1(dz1, nz - 5) + (1. - bc51) * slope_p;
+    if (P1(fdz0, 2) * dz * fabs(slope_p2) > lim_tol * fabs(P1(x, 1)) + eps) {
+        limiter_muscl(g, P1(x, 1), slope_p, slope_p2, slope_m, &phir, &phil);
+        Fl = P1(x, 1) + 0.5 * phil * slope_m / P1(dz1w, 1);
+        Fr = P1(x, 2) - 0.5 * phir * slope_p2 / P1(dz1w, 1);
+    } else {
+        Fl = P1(x, 1) + 0.5 * slope_p / P1(dz1w, 1);
+        Fr = P1(x, 2) - 0.5 * slope_p / P1(dz1w, 1);
+    }
+    P1(F, 1) = 0.5 * ww * (Fl * (1. + fsign1(ww)) + Fr * (1. - fsign1(ww)));
+
+    for (k = 2; k <= nz - 2; k++) {
+        ww = P1(w, k + 1);
+        slope_p = (P1(x, k + 1) - P1(x, k)) * P1(dz1, k);
+        slope_p2 = (P1(x, k + 2) - P1(x, k + 1)) * P1(dz1, k + 1);
+        slope_m = (P1(x, k) - P1(x, k - 1)) * P1(dz1, k - 1);
+        if (P1(fdz0, k - 1) * dz * fabs(slope_m) > lim_tol * fabs(P1(x, k)) + eps ||
+            P1(fdz0, k + 1) * dz * fabs(slope_p2) > lim_tol * fabs(P1(x, k)) + eps) {
+            limiter_muscl(g, P1(x, k), slope_p, slope_p2, slope_m, &phir, &phil);
+            Fr = P1(x, k + 1) - 0.5 * phir * slope_p2 / P1(dz1w, k);
+            Fl = P1(x, k) + 0.5 * phil * slope_m / P1(dz1w, k);
+        } else {
+            Fr = P1(x, k + 1) - 0.5 * slope_p / P1(dz1w, k);
+            Fl = P1(x, k) + 0.5 * slope_p / P1(dz1w, k);
+        }
+        P1(F, k) = 0.5 * ww * (Fl * (1. + fsign1(ww)) + Fr * (1. - fsign1(ww)));
+    }
+
+    k = nz - 1;
+    ww = P1(w, k + 1);
+    slope_p = (P1(x, k + 1) - P1(x, k)) * P1(dz1, k);
+    slope_p2 = bc61 * (P1(x, 6) - P1(x, 5)) * P1(dz1, 5) + (1. - bc61) * slope_p;
+    slope_m = (P1(x, k) - P1(x, k - 1)) * P1(dz1, k - 1);
+    if (P1(fdz0, k - 1) * dz * fabs(slope_m) > lim_tol * fabs(P1(x, nz - 1)) + eps) {
+        limiter_muscl(g, P1(x, k), slope_p, slope_p2, slope_m, &phir, &phil);
+        Fr = P1(x, k + 1) - 0.5 * phir * slope_p2 / P1(dz1w, k);
+        Fl = P1(x, k) + 0.5 * phil * slope_m / P1(dz1w, k);
+    } else {
+        Fr = P1(x, k + 1) - 0.5 * slope_p / P1(dz1w, k);
+        Fl = P1(x, k) + 0.5 * slope_p / P1(dz1w, k);
+    }
+    P1(F, k) = 0.5 * ww * (Fl * (1. + fsign1(ww)) + Fr * (1. - fsign1(ww)));
+
+    double Fold = P1(F, 1);
+    for (k = 2; k <= nz - 1; k++) {
+        P1(xa, k) = P1(xa, k) + (P1(F, k) - Fold) * P1(dz1w, k);
+        Fold = P1(F, k);
+    }
+    if (adv) {
+        double wold = P1(w, k2);
+        for (k = nz - 1; k >= 2; k--) {
+            P1(xa, k) = P1(xa, k) - P1(x, k) * (wold - P1(w, k)) * P1(dz1w, k);
+            wold = P1(w, k);
+        }
+    }
+    P1(xa, 1) = P1(xa, 1) + (P1(F, 1) - 0.) * P1(dz1w, 1);
+    if (adv) P1(xa, 1) = P1(xa, 1) - P1(x, 1) * (P1(w, 2) - 0.) * P1(dz1w, 1);
+    P1(xa, nz) = P1(xa, nz) + (0. - P1(F, nz - 1)) * P1(dz1w, nz);
+    if (adv) P1(xa, nz) = P1(xa, nz) - P1(x, nz) * (0. - P1(w, nz)) * P1(dz1w, nz);
+    free(F);
+}
+
+void mo_advs_h(const mo_grid *g, int scheme, int n, int i1, int i2, double d, const double *x,
+               const double *u, double *xa, int adv)
+{
+    switch (scheme) {
+    case MO_WENO: advs_weno_h(n, i1, i2, d, x, u, xa, adv); break;
+    case MO_PPM: advs_ppm_h(g, n, i1, i2, d, x, u, xa, adv); break;
+    default: advs_muscl_h(g, n, i1, i2, d, x, u, xa, adv); break;
+    }
+}
+
+void mo_advs_z(const mo_grid *g, int scheme, const double *x, const double *w, double *xa, int adv)
+{
+    switch (scheme) {
+    case MO_WENO: advs_weno_z(g, x, w, xa, adv); break;
+    case MO_PPM: advs_ppm_z(g, x, w, xa, adv); break;
+    default: advs_muscl_z(g, x, w, xa, adv); break;
+    }
+}
+
+/* ======================================================================
+ * 3-D scalar advection: src/TOOLS/advection.f90 advection_x/y/z :556-798
+ * (pencil loops with copy-in temporaries) and advection_ac :801-915.
+ * ==================================================================== */
+void mo_advection_dir(const mo_grid *g, int dir, const double *xtmp, const double *uadv, double *xs, int adv)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    const int its = 4, ite = nx - 2, jts = 4, jte = ny - 2;
+    const int n = dir == 0 ? nx : (dir == 1 ? ny : nz);
+    double *xx = dalloc(ncell(g)); /* the direction's tendency, zeroed */
+    /* independent pencils: thread-parallel, results identical for any thread count */
+#pragma omp parallel
+    {
+        double *px = dalloc((size_t)n), *pu = dalloc((size_t)n), *pa = dalloc((size_t)n);
+        if (dir == 0) {
+#pragma omp for collapse(2) schedule(static)
+            for (int k = 1; k <= nz; k++)
+                for (int j = jts; j <= jte; j++) {
+                    for (int i = 1; i <= nx; i++) {
+                        P1(px, i) = xtmp[IX(g, i, j, k)];
+                        P1(pu, i) = uadv[IX(g, i, j, k)];
+                        P1(pa, i) = xx[IX(g, i, j, k)];
+                    }
+                    mo_advs_h(g, g->scal_adv, nx, its, ite, g->dx, px, pu, pa, adv);
+                    for (int i = 1; i <= nx; i++) xx[IX(g, i, j, k)] = P1(pa, i);
+                }
+        } else if (dir == 1) {
+#pragma omp for collapse(2) schedule(static)
+            for (int k = 1; k <= nz; k++)
+                for (int i = its; i <= ite; i++) {
+                    for (int j = 1; j <= ny; j++) {
+                        P1(px, j) = xtmp[IX(g, i, j, k)];
+                        P1(pu, j) = uadv[IX(g, i, j, k)];
+                        P1(pa, j) = xx[IX(g, i, j, k)];
+                    }
+                    mo_advs_h(g, g->scal_adv, ny, jts, jte, g->dy, px, pu, pa, adv);
+                    for (int j = 1; j <= ny; j++) xx[IX(g, i, j, k)] = P1(pa, j);
+                }
+        } else {
+#pragma omp for collapse(2) schedule(static)
+            for (int j = jts; j <= jte; j++)
+                for (int i = its; i <= ite; i++) {
+                    for (int k = 1; k <= nz; k++) {
+                        P1(px, k) = xtmp[IX(g, i, j, k)];
+                        P1(pu, k) = uadv[IX(g, i, j, k)];
+                        P1(pa, k) = xx[IX(g, i, j, k)];
+                    }
+                    mo_advs_z(g, g->scal_adv, px, pu, pa, adv);
+                    for (int k = 1; k <= nz; k++) xx[IX(g, i, j, k)] = P1(pa, k);
+                }
+        }
+        free(px); free(pu); free(pa);
+    }
+    size_t nc = ncell(g);
+#pragma omp parallel for schedule(static)
+    for (size_t c = 0; c < nc; c++) xs[c] = xs[c] - xx[c];
+    free(xx);
+}
+
+void mo_advection_ac(const mo_grid *g, const double *x, const double *ua, const double *va,
+                     const double *wa, double *xs, int adv)
+{
+    mo_advection_dir(g, 0, x, ua, xs, adv);
+    mo_advection_dir(g, 1, x, va, xs, adv);
+    mo_advection_dir(g, 2, x, wa, xs, adv);
+}
+
+/* src/TOOLS/funcpack.f90:65-94 with get_velocities_1 anelastic branch :328-334 */
+void mo_get_advective(const mo_grid *g, const double *mu, const double *mv, const double *mw,
+                      double *ua, double *va, double *wa)
+{
+    for (int k = 1; k <= g->nz; k++) {
+        double d0 = P1(g->den0, k), ad0 = P1(g->avden0, k);
+        for (int j = 1; j <= g->ny; j++)
+            for (int i = 1; i <= g->nx; i++) {
+                size_t c = IX(g, i, j, k);
+                ua[c] = mu[c] / d0 - g->u0shift;
+                va[c] = mv[c] / d0 - g->v0shift;
+                wa[c] = mw[c] / ad0;
+            }
+    }
+}
+
+/* ======================================================================
+ * Momentum advection: src/INTEG/windadv.f90
+ * ==================================================================== */
+static const double AVISC = 1. / 16.; /* windadv.f90:39 */
+
+#define FD4(a, m2, m1, c0, p1, p2) ((-(a)[p2] + 4. * (a)[p1] - 6. * (a)[c0] + 4. * (a)[m1] - (a)[m2]))
+
+/* advux_fd :494-554; row (j,k) */
+static void advux(const mo_grid *g, const double *u, const double *ut, double *ua, int j, int k)
+{
+    const int its = 4, ite = g->nx - 2;
+    double dx1 = 1. / g->dx, dx2 = 1. / (2. * g->dx), c1, c2;
+    if (g->mom_ord == 4) { c1 = 4. / 3.; c2 = 1. / 3.; } else { c1 = 1.; c2 = 0.; }
+    double *F = dalloc((size_t)g->nx + 2), *A = dalloc((size_t)g->nx + 2);
+#define U(i) u[IX(g, i, j, k)]
+#define UT(i) ut[IX(g, i, j, k)]
+    for (int i = its - 2; i <= ite; i++) {
+        double uu = (UT(i + 1) + UT(i)) * 0.5, uu2 = (UT(i + 2) + UT(i)) * 0.5;
+        double fr = (U(i + 1) + U(i)) * 0.5, fr2 = (U(i + 2) + U(i)) * 0.5;
+        P1(F, i) = uu * fr;
+        P1(A, i) = uu2 * fr2;
+    }
+    for (int i = its; i <= ite; i++) {
+        size_t c = IX(g, i, j, k);
+        ua[c] = ua[c] + c1 * (P1(F, i) - P1(F, i - 1)) * dx1 - c2 * (P1(A, i) - P1(A, i - 2)) * dx2;
+    }
+    if (g->lavisc)
+        for (int i = its; i <= ite; i++) {
+            size_t c = IX(g, i, j, k);
+            double mu = fabs(UT(i)) * dx1;
+            ua[c] = ua[c] - AVISC * mu * (-U(i + 2) + 4. * U(i + 1) - 6. * U(i) + 4. * U(i - 1) - U(i - 2));
+        }
+#undef U
+#undef UT
+    free(F); free(A);
+}
+
+/* advuy_fd :556-626; column (i,k); vt1=vt(i-1), vt2=vt(i), vt3=vt(i-2), vt4=vt(i+1) */
+static void advuy(const mo_grid *g, const double *u, const double *vt, double *ua, int i, int k)
+{
+    const int jts = 4, jte = g->ny - 2;
+    double dy1 = 1. / g->dy, dy3 = 1. / (3. * g->dy), c1, c2;
+    if (g->mom_ord == 4) { c1 = 9. / 8.; c2 = 1. / 8.; } else { c1 = 1.; c2 = 0.; }
+    double *F = dalloc((size_t)g->ny + 2);
+#define U(j) u[IX(g, i, j, k)]
+#define V1(j) vt[IX(g, i - 1, j, k)]
+#define V2(j) vt[IX(g, i, j, k)]
+#define V3(j) vt[IX(g, i - 2, j, k)]
+#define V4(j) vt[IX(g, i + 1, j, k)]
+    for (int j = jts - 2; j <= jte + 1; j++) {
+        double vv = c1 * (V1(j + 1) + V2(j + 1)) * 0.5 - c2 * (V3(j + 1) + V4(j + 1)) * 0.5;
+        double fr = (U(j + 1) + U(j)) * 0.5;
+        P1(F, j) = vv * fr;
+    }
+    for (int j = jts; j <= jte; j++) {
+        size_t c = IX(g, i, j, k);
+        ua[c] = ua[c] + c1 * (P1(F, j) - P1(F, j - 1)) * dy1 - c2 * (P1(F, j + 1) - P1(F, j - 2)) * dy3;
+    }
+    if (g->lavisc)
+        for (int j = jts; j <= jte; j++) {
+            size_t c = IX(g, i, j, k);
+            double mu = 0.25 * fabs(V1(j) + V2(j) + V1(j + 1) + V2(j + 1)) * dy1;
+            ua[c] = ua[c] - AVISC * mu * (-U(j + 2) + 4. * U(j + 1) - 6. * U(j) + 4. * U(j - 1) - U(j - 2));
+        }
+#undef U
+#undef V1
+#undef V2
+#undef V3
+#undef V4
+    free(F);
+}
+
+/* advuz_fd :628-694 (vert=0) and advvz_fd :828-894 (vert=1; row 2 uses dz1w(2)).
+ * Column (i,j); wt1..wt4 at (ia1,ja1),(i,j),(ia3,ja3),(ia4,ja4). */
+static void advhz(const mo_grid *g, const double *u, const double *wt, double *ua, int i, int j,
+                  int ia1, int ja1, int ia3, int ja3, int ia4, int ja4, int isv)
+{
+    const int nz = g->nz;
+    const double *dzw = g->dzw, *dz1w = g->dz1w;
+    double c1, c2;
+    if (g->mom_ord == 4) { c1 = 9. / 8.; c2 = 1. / 8.; } else { c1 = 1.; c2 = 0.; }
+    double *F = dalloc((size_t)nz + 2);
+#define U(k) u[IX(g, i, j, k)]
+#define W1(k) wt[IX(g, ia1, ja1, k)]
+#define W2(k) wt[IX(g, i, j, k)]
+#define W3(k) wt[IX(g, ia3, ja3, k)]
+#define W4(k) wt[IX(g, ia4, ja4, k)]
+#define UA(k) ua[IX(g, i, j, k)]
+    for (int k = 1; k <= nz - 1; k++) {
+        double ww = c1 * (W1(k + 1) + W2(k + 1)) * 0.5 - c2 * (W3(k + 1) + W4(k + 1)) * 0.5;
+        double fr = (P1(dzw, k + 1) * U(k + 1) + P1(dzw, k) * U(k)) / (P1(dzw, k + 1) + P1(dzw, k));
+        P1(F, k) = ww * fr;
+    }
+    P1(F, nz) = 0.;
+    for (int k = 3; k <= nz - 1; k++)
+        UA(k) = UA(k) + c1 * (P1(F, k) - P1(F, k - 1)) * P1(dz1w, k) -
+                c2 * (P1(F, k + 1) - P1(F, k - 2)) / (P1(dzw, k - 1) + P1(dzw, k) + P1(dzw, k + 1));
+    UA(1) = UA(1) + (P1(F, 1) - 0.) * P1(dz1w, 1);
+    UA(2) = UA(2) + c1 * (P1(F, 2) - P1(F, 1)) * P1(dz1w, isv ? 2 : 1) -
+            c2 * (P1(F, 3) - 0.) / (P1(dzw, 1) + P1(dzw, 2) + P1(dzw, 3));
+    UA(nz) = UA(nz) + (0. - P1(F, nz - 1)) * P1(dz1w, nz);
+    if (g->lavisc)
+        for (int k = 3; k <= nz - 2; k++) {
+            double mu = 0.25 * fabs(W1(k) + W2(k) + W1(k + 1) + W2(k + 1)) * P1(dz1w, k);
+            UA(k) = UA(k) - AVISC * mu * (-U(k + 2) + 4. * U(k + 1) - 6. * U(k) + 4. * U(k - 1) - U(k - 2));
+        }
+#undef U
+#undef W1
+#undef W2
+#undef W3
+#undef W4
+#undef UA
+    free(F);
+}
+
+/* advvx_fd :696-752; row (j,k); ut1=ut(j-1), ut2=ut(j), ut3=ut(j-2), ut4=ut(j+1) */
+static void advvx(const mo_grid *g, const double *v, const double *ut, double *va, int j, int k)
+{
+    const int its = 4, ite = g->nx - 2;
+    double dx1 = 1. / g->dx, dx3 = 1. / (3. * g->dx), c1, c2;
+    if (g->mom_ord == 4) { c1 = 9. / 8.; c2 = 1. / 8.; } else { c1 = 1.; c2 = 0.; }
+    double *F = dalloc((size_t)g->nx + 2);
+#define V(i) v[IX(g, i, j, k)]
+#define T1(i) ut[IX(g, i, j - 1, k)]
+#define T2(i) ut[IX(g, i, j, k)]
+#define T3(i) ut[IX(g, i, j - 2, k)]
+#define T4(i) ut[IX(g, i, j + 1, k)]
+    for (int i = its - 2; i <= ite + 1; i++) {
+        double uu = c1 * (T1(i + 1) + T2(i + 1)) * 0.5 - c2 * (T3(i + 1) + T4(i + 1)) * 0.5;
+        double fr = (V(i + 1) + V(i)) * 0.5;
+        P1(F, i) = uu * fr;
+    }
+    for (int i = its; i <= ite; i++) {
+        size_t c = IX(g, i, j, k);
+        va[c] = va[c] + c1 * (P1(F, i) - P1(F, i - 1)) * dx1 - c2 * (P1(F, i + 1) - P1(F, i - 2)) * dx3;
+    }
+    if (g->lavisc)
+        for (int i = its; i <= ite; i++) {
+            size_t c = IX(g, i, j, k);
+            double mu = 0.25 * fabs(T1(i) + T2(i) + T1(i + 1) + T2(i + 1)) * dx1;
+            va[c] = va[c] - AVISC * mu * (-V(i + 2) + 4. * V(i + 1) - 6. * V(i) + 4. * V(i - 1) - V(i - 2));
+        }
+#undef V
+#undef T1
+#undef T2
+#undef T3
+#undef T4
+    free(F);
+}
+
+/* advvy_fd :754-826; column (i,k) */
+static void advvy(const mo_grid *g, const double *v, const double *vt, double *va, int i, int k)
+{
+    const int jts = 4, jte = g->ny - 2;
+    double dy1 = 1. / g->dy, dy2 = 1. / (2. * g->dy), c1, c2;
+    if (g->mom_ord == 4) { c1 = 4. / 3.; c2 = 1. / 3.; } else { c1 = 1.; c2 = 0.; }
+    double *F = dalloc((size_t)g->ny + 2), *A = dalloc((size_t)g->ny + 2);
+#define V(j) v[IX(g, i, j, k)]
+#define VT(j) vt[IX(g, i, j, k)]
+    for (int j = jts - 2; j <= jte; j++) {
+        double vv = (VT(j + 1) + VT(j)) * 0.5, vv2 = (VT(j + 2) + VT(j)) * 0.5;
+        double fr = (V(j + 1) + V(j)) * 0.5, fr2 = (V(j + 2) + V(j)) * 0.5;
+        P1(F, j) = vv * fr;
+        P1(A, j) = vv2 * fr2;
+    }
+    for (int j = jts; j <= jte; j++) {
+        size_t c = IX(g, i, j, k);
+        va[c] = va[c] + c1 * (P1(F, j) - P1(F, j - 1)) * dy1 - c2 * (P1(A, j) - P1(A, j - 2)) * dy2;
+    }
+    if (g->lavisc)
+        for (int j = jts; j <= jte; j++) {
+            size_t c = IX(g, i, j, k);
+            double mu = fabs(VT(j)) * dy1;
+            va[c] = va[c] - AVISC * mu * (-V(j + 2) + 4. * V(j + 1) - 6. * V(j) + 4. * V(j - 1) - V(j - 2));
+        }
+#undef V
+#undef VT
+    free(F); free(A);
+}
+
+/* advwx_fd :896-968 (dir=0, slab j) and advwy_fd :970-1056 (dir=1, slab i) */
+static void advwh(const mo_grid *g, const double *w, const double *ht, double *wa, int dir, int s)
+{
+    const int nz = g->nz;
+    const int lo = 4, hi = (dir == 0 ? g->nx : g->ny) - 2;
+    const int n = dir == 0 ? g->nx : g->ny;
+    double d = dir == 0 ? g->dx : g->dy;
+    double d1 = 1. / d, d3 = 1. / (3. * d), c1, c2;
+    if (g->mom_ord == 4) { c1 = 9. / 8.; c2 = 1. / 8.; } else { c1 = 1.; c2 = 0.; }
+    double *F = dalloc((size_t)(n + 2) * (nz + 2));
+#define AT(a, p, k) (dir == 0 ? (a)[IX(g, p, s, k)] : (a)[IX(g, s, p, k)])
+#define FF(p, k) F[(size_t)(k) * (n + 2) + (p)]
+    for (int p = lo - 2; p <= hi + 1; p++) {
+        double uu = (AT(ht, p + 1, 2) + AT(ht, p + 1, 1)) * 0.5;
+        double fr = (AT(w, p + 1, 2) + AT(w, p, 2)) * 0.5;
+        FF(p, 2) = uu * fr;
+        uu = (AT(ht, p + 1, nz) + AT(ht, p + 1, nz - 1)) * 0.5;
+        fr = (AT(w, p + 1, nz) + AT(w, p, nz)) * 0.5;
+        FF(p, nz) = uu * fr;
+    }
+    for (int k = 3; k <= nz - 1; k++)
+        for (int p = lo - 2; p <= hi + 1; p++) {
+            double uu = c1 * (AT(ht, p + 1, k) + AT(ht, p + 1, k - 1)) * 0.5 -
+                        c2 * (AT(ht, p + 1, k + 1) + AT(ht, p + 1, k - 2)) * 0.5;
+            double fr = (AT(w, p + 1, k) + AT(w, p, k)) * 0.5;
+            FF(p, k) = uu * fr;
+        }
+    for (int k = 2; k <= nz; k++)
+        for (int p = lo; p <= hi; p++) {
+            size_t c = dir == 0 ? IX(g, p, s, k) : IX(g, s, p, k);
+            wa[c] = wa[c] + c1 * (FF(p, k) - FF(p - 1, k)) * d1 - c2 * (FF(p + 1, k) - FF(p - 2, k)) * d3;
+        }
+    if (g->lavisc)
+        for (int k = 2; k <= nz; k++)
+            for (int p = lo; p <= hi; p++) {
+                size_t c = dir == 0 ? IX(g, p, s, k) : IX(g, s, p, k);
+                double mu = 0.25 * fabs(AT(ht, p, k) + AT(ht, p, k - 1) + AT(ht, p + 1, k) + AT(ht, p + 1, k - 1)) * d1;
+                wa[c] = wa[c] - AVISC * mu *
+                                    (-AT(w, p + 2, k) + 4. * AT(w, p + 1, k) - 6. * AT(w, p, k) + 4. * AT(w, p - 1, k) - AT(w, p - 2, k));
+            }
+#undef AT
+#undef FF
+    free(F);
+}
+
+/* advwz_fd :1058-1127; column (i,j) */
+static void advwz(const mo_grid *g, const double *w, const double *wt, double *wa, int i, int j)
+{
+    const int nz = g->nz;
+    const double *dzw = g->dzw, *dz1 = g->dz1;
+    double c1, c2;
+    if (g->mom_ord == 4) { c1 = 4. / 3.; c2 = 1. / 3.; } else { c1 = 1.; c2 = 0.; }
+    double *F = dalloc((size_t)nz + 2), *A = dalloc((size_t)nz + 2);
+#define W(k) w[IX(g, i, j, k)]
+#define WT(k) wt[IX(g, i, j, k)]
+#define WA(k) wa[IX(g, i, j, k)]
+    for (int k = 1; k <= nz - 2; k++) {
+        double ww = (WT(k + 1) + WT(k)) * 0.5;
+        double ww2 = (P1(dzw, k + 1) * WT(k + 2) + P1(dzw, k) * WT(k)) / (P1(dzw, k + 1) + P1(dzw, k));
+        double fr = (W(k + 1) + W(k)) * 0.5;
+        double fr2 = (P1(dzw, k + 1) * W(k + 2) + P1(dzw, k) * W(k)) / (P1(dzw, k + 1) + P1(dzw, k));
+        P1(F, k) = ww * fr;
+        P1(A, k) = ww2 * fr2;
+    }
+    P1(F, nz - 1) = 0.25 * (WT(nz) + WT(nz - 1)) * (W(nz) + W(nz - 1));
+    {
+        double s = P1(dzw, nz) + P1(dzw, nz - 1);
+        P1(A, nz - 1) = (0. + P1(dzw, nz - 1) * WT(nz - 1)) * (0. + P1(dzw, nz - 1) * W(nz - 1)) / (s * s);
+    }
+    for (int k = 3; k <= nz - 1; k++)
+        WA(k) = WA(k) + c1 * (P1(F, k) - P1(F, k - 1)) * P1(dz1, k - 1) -
+                c2 * (P1(A, k) - P1(A, k - 2)) / (P1(dzw, k) + P1(dzw, k - 1));
+    WA(2) = WA(2) + c1 * (P1(F, 2) - P1(F, 1)) * P1(dz1, 1) - c2 * (P1(A, 2) - 0.) / (P1(dzw, 2) + P1(dzw, 1));
+    WA(nz) = WA(nz) + (0. - P1(F, nz - 1)) * P1(dz1, nz - 1);
+    if (g->lavisc)
+        for (int k = 3; k <= nz - 2; k++) {
+            double mu = fabs(WT(k)) * P1(dz1, k - 1);
+            WA(k) = WA(k) - AVISC * mu * (-W(k + 2) + 4. * W(k + 1) - 6. * W(k) + 4. * W(k - 1) - W(k - 2));
+        }
+#undef W
+#undef WT
+#undef WA
+    free(F); free(A);
+}
+
+/* qnadv_uvw :46-79 with uadv_fd :82-220, vadv_fd :223-357, wadv_fd :360-492
+ * (ADV_SPLIT off).  Even ntime: x, y, z; odd ntime: z, y, x. */
+void mo_qnadv_uvw(const mo_grid *g, int ntime, const double *mu, const double *mv, const double *mw,
+                  const double *ua, const double *va, const double *wa,
+                  double *au, double *av, double *aw)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    const int its = 4, ite = nx - 2, jts = 4, jte = ny - 2;
+    size_t nc = ncell(g);
+    memset(au, 0, nc * sizeof(double));
+    memset(av, 0, nc * sizeof(double));
+    memset(aw, 0, nc * sizeof(double));
+    int even = (ntime % 2) == 0;
+    for (int pass = 0; pass < 3; pass++) {
+        int dir = even ? pass : 2 - pass;
+        if (dir == 0) {
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int k = 1; k <= nz; k++)
+                for (int j = jts; j <= jte; j++) advux(g, mu, ua, au, j, k);
+        } else if (dir == 1) {
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int k = 1; k <= nz; k++)
+                for (int i = its; i <= ite; i++) advuy(g, mu, va, au, i, k);
+        } else {
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int j = jts; j <= jte; j++)
+                for (int i = its; i <= ite; i++) advhz(g, mu, wa, au, i, j, i - 1, j, i - 2, j, i + 1, j, 0);
+        }
+    }
+    for (int pass = 0; pass < 3; pass++) {
+        int dir = even ? pass : 2 - pass;
+        if (dir == 0) {
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int k = 1; k <= nz; k++)
+                for (int j = jts; j <= jte; j++) advvx(g, mv, ua, av, j, k);
+        } else if (dir == 1) {
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int k = 1; k <= nz; k++)
+                for (int i = its; i <= ite; i++) advvy(g, mv, va, av, i, k);
+        } else {
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int j = jts; j <= jte; j++)
+                for (int i = its; i <= ite; i++) advhz(g, mv, wa, av, i, j, i, j - 1, i, j - 2, i, j + 1, 1);
+        }
+    }
+    for (int pass = 0; pass < 3; pass++) {
+        int dir = even ? pass : 2 - pass;
+        if (dir == 0) {
+#pragma omp parallel for schedule(static)
+            for (int j = jts; j <= jte; j++) advwh(g, mw, ua, aw, 0, j);
+        } else if (dir == 1) {
+#pragma omp parallel for schedule(static)
+            for (int i = its; i <= ite; i++) advwh(g, mw, va, aw, 1, i);
+        } else {
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int j = jts; j <= jte; j++)
+                for (int i = its; i <= ite; i++) advwz(g, mw, wa, aw, i, j);
+        }
+    }
+}
+
+/* ======================================================================
+ * Gradients: src/TOOLS/gradients.f90 caldiv :986-1052, gradp :1205-1292
+ * ==================================================================== */
+void mo_caldiv(const mo_grid *g, double *mu, double *mv, double *mw, double *div)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    double dx1 = 1. / g->dx, dy1 = 1. / g->dy;
+    memset(div, 0, ncell(g) * sizeof(double));
+    windbc(g, mu, mv, mw);
+    for (int k = 1; k <= nz; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) {
+                size_t c = IX(g, i, j, k);
+                div[c] = div[c] + (mu[IX(g, i + 1, j, k)] - mu[c]) * dx1;
+            }
+    for (int k = 1; k <= nz; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) {
+                size_t c = IX(g, i, j, k);
+                div[c] = div[c] + (mv[IX(g, i, j + 1, k)] - mv[c]) * dy1;
+            }
+    for (int k = 1; k <= nz - 1; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) {
+                size_t c = IX(g, i, j, k);
+                div[c] = div[c] + (mw[IX(g, i, j, k + 1)] - mw[c]) * P1(g->dz1w, k);
+            }
+    for (int j = 4; j <= ny - 2; j++)
+        for (int i = 4; i <= nx - 2; i++) {
+            size_t c = IX(g, i, j, nz);
+            div[c] = div[c] + (0. - mw[c]) * P1(g->dz1w, nz);
+        }
+    mo_statebc(g, div);
+}
+
+void mo_gradp(const mo_grid *g, double *p, const double *w, double *gpx, double *gpy, double *gpz)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    double dx1 = 1. / g->dx, dy1 = 1. / g->dy;
+    size_t nc = ncell(g);
+    mo_statebc(g, p);
+    memset(gpx, 0, nc * sizeof(double));
+    memset(gpy, 0, nc * sizeof(double));
+    memset(gpz, 0, nc * sizeof(double));
+    for (int k = 1; k <= nz; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) {
+                size_t c = IX(g, i, j, k);
+                gpx[c] = (p[c] - p[IX(g, i - 1, j, k)]) * dx1;
+                gpy[c] = (p[c] - p[IX(g, i, j - 1, k)]) * dy1;
+            }
+    for (int k = 2; k <= nz; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) {
+                size_t c = IX(g, i, j, k);
+                gpz[c] = (p[c] - p[IX(g, i, j, k - 1)]) * P1(g->dz1, k - 1);
+            }
+    for (int j = 4; j <= ny - 2; j++)
+        for (int i = 4; i <= nx - 2; i++) {
+            size_t c = IX(g, i, j, 1);
+            gpz[c] = w[c] / (g->dt0 * P1(g->avden0, 1));
+        }
+}
+
+/* src/TOOLS/thermodynamics.f90:472-534 (ANELASTIC, CONSERVATIVE, ISENTROPIC, nhydro=0);
+ * es and qt are the density-weighted values; qt may be NULL (dry: qt=0). */
+void mo_buoyancy(const mo_grid *g, const double *dens, const double *es, const double *qt, double *buoy)
+{
+    const double grav = 9.81, epsm = 0.60243;
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    size_t plane = (size_t)nx * ny;
+    double *bb = dalloc(ncell(g));
+    for (int k = 1; k <= nz; k++) {
+        double ref = P1(g->pt0, k) * (1. + epsm * P1(g->qv0, k));
+        for (size_t c = (size_t)(k - 1) * plane; c < (size_t)k * plane; c++) {
+            double den1 = 1. / dens[c];
+            double pt = den1 * es[c];
+            double q = qt ? qt[c] : 0.;
+            double sumh = 0.;
+            bb[c] = dens[c] * grav * (pt * (1. + epsm * den1 * (q - sumh) - den1 * sumh) / ref - 1.);
+        }
+    }
+    for (int k = 2; k <= nz; k++)
+        for (size_t c = 0; c < plane; c++)
+            buoy[(size_t)(k - 1) * plane + c] = 0.5 * (bb[(size_t)(k - 2) * plane + c] + bb[(size_t)(k - 1) * plane + c]);
+    for (size_t c = 0; c < plane; c++) buoy[c] = bb[c];
+    free(bb);
+}
+
+/* ======================================================================
+ * Pressure: FFT, tridiagonal, projection
+ * ==================================================================== */
+
+/* Mixed-radix recursive DFT (decimation in time), unnormalised, sign -1 forward
+ * (FFTW_FORWARD) and +1 backward (FFTW_BACKWARD) as in fftw_plan_dft_2d
+ * (src/PRESSURE/fft_interface.f90:580-591,626-637).  The reference delegates the
+ * transform to FFTW 3.3.8 (not vendored); this is a plain restatement of the DFT. */
+static void fft1d_rec(int n, int stride, const double *ire, const double *iim, double *ore, double *oim,
+                      int sign, double *scratch)
+{
+    if (n == 1) { ore[0] = ire[0]; oim[0] = iim[0]; return; }
+    int p = 0;
+    for (int r = 2; r * r <= n; r++) if (n % r == 0) { p = r; break; }
+    if (!p) p = n; /* prime: direct DFT */
+    int m = n / p;
+    if (p == n) {
+        for (int kk = 0; kk < n; kk++) {
+            long double sr = 0, si = 0;
+            for (int t = 0; t < n; t++) {
+                long double ang = 2.0L * 3.141592653589793238462643383279502884L * (long double)((long)kk * t % n) / n;
+                long double c = cosl(ang), s = sign * sinl(ang);
+                sr += ire[(size_t)t * stride] * c - iim[(size_t)t * stride] * s;
+                si += ire[(size_t)t * stride] * s + iim[(size_t)t * stride] * c;
+            }
+            ore[kk] = (double)sr; oim[kk] = (double)si;
+        }
+        return;
+    }
+    /* sub-transforms of the p decimated sequences into ore/oim blocks of size m */
+    for (int q = 0; q < p; q++)
+        fft1d_rec(m, stride * p, ire + (size_t)q * stride, iim + (size_t)q * stride, ore + (size_t)q * m,
+                  oim + (size_t)q * m, sign, scratch + 2 * n);
+    double *tr = scratch, *ti = scratch + n;
+    for (int kk = 0; kk < n; kk++) {
+        int k1 = kk % m;
+        long double sr = 0, si = 0;
+        for (int q = 0; q < p; q++) {
+            long double ang = 2.0L * 3.141592653589793238462643383279502884L * (long double)(((long)q * kk) % n) / n;
+            long double c = cosl(ang), s = sign * sinl(ang);
+            long double xr = ore[(size_t)q * m + k1], xi = oim[(size_t)q * m + k1];
+            sr += xr * c - xi * s;
+            si += xr * s + xi * c;
+        }
+        tr[kk] = (double)sr; ti[kk] = (double)si;
+    }
+    memcpy(ore, tr, n * sizeof(double));
+    memcpy(oim, ti, n * sizeof(double));
+}
+
+static void fft1d(int n, double *re, double *im, size_t stride, int sign)
+{
+    double *ir = dalloc(n), *ii = dalloc(n), *or_ = dalloc(n), *oi = dalloc(n), *scr = dalloc((size_t)8 * n + 64);
+    for (int t = 0; t < n; t++) { ir[t] = re[t * stride]; ii[t] = im[t * stride]; }
+    fft1d_rec(n, 1, ir, ii, or_, oi, sign, scr);
+    for (int t = 0; t < n; t++) { re[t * stride] = or_[t]; im[t * stride] = oi[t]; }
+    free(ir); free(ii); free(or_); free(oi); free(scr);
+}
+
+void mo_fft2d(int nxp, int nyp, double *re, double *im, int inverse)
+{
+    int sign = inverse ? +1 : -1;
+    for (int m = 0; m < nyp; m++) fft1d(nxp, re + (size_t)m * nxp, im + (size_t)m * nxp, 1, sign);
+    for (int l = 0; l < nxp; l++) fft1d(nyp, re + l, im + l, (size_t)nxp, sign);
+}
+
+/* src/PRESSURE/fft_tools.f90:202-237 */
+static int tridag2(const double *A, const double *B, const double *C, const double *R, double *U, int N)
+{
+    double *GAM = dalloc((size_t)N + 1);
+    if (B[0] == 0.) { free(GAM); return 1; }
+    double BET = B[0];
+    U[0] = R[0] / BET;
+    for (int J = 2; J <= N; J++) {
+        P1(GAM, J) = P1(C, J - 1) / BET;
+        BET = P1(B, J) - P1(A, J) * P1(GAM, J);
+        if (BET == 0.) { free(GAM); return 2; }
+        P1(U, J) = (P1(R, J) - P1(A, J) * P1(U, J - 1)) / BET;
+    }
+    for (int J = N - 1; J >= 1; J--) P1(U, J) = P1(U, J) - P1(GAM, J + 1) * P1(U, J + 1);
+    free(GAM);
+    return 0;
+}
+
+/* src/PRESSURE/fft_tools.f90:115-199, serial (ioff=joff=0), bcl(5:6)='nnf'.
+ * s1(l,k) for l=1..nxp, k=1..nzp at re/im[(l-1)*stride_l + (k-1)*stride_k]. */
+int mo_tridiag(const mo_grid *g, int m, int nxp, int nzp, const double *wvl,
+               double *s1re, double *s1im, size_t stride_l, size_t stride_k)
+{
+    const double dz = g->dz;
+    const double *dz1 = g->dz1, *dz1w = g->dz1w, *stab0 = g->stab0, *fdz0 = g->fdz0;
+    double *ak = dalloc(nzp), *bk = dalloc(nzp), *ck = dalloc(nzp), *dk = dalloc(nzp), *xk = dalloc((size_t)nzp * nxp);
+    double *bre = dalloc((size_t)nzp * nxp);
+    int err = 0;
+#define S(l, k) ((size_t)((l) - 1) * stride_l + (size_t)((k) - 1) * stride_k)
+    for (int pass = 0; pass < 2; pass++) {
+        for (int l = 1; l <= nxp; l++) {
+            double wl = P1(wvl, l);
+            for (int k = 2; k <= nzp - 1; k++) {
+                double h = dz * (0.5 * P1(fdz0, k + 1) + P1(fdz0, k) + 0.5 * P1(fdz0, k - 1));
+                P1(ak, k) = P1(dz1, k - 1) * P1(dz1w, k) - P1(stab0, k) / h;
+                P1(ck, k) = P1(dz1, k) * P1(dz1w, k) + P1(stab0, k) / h;
+                P1(dk, k) = wl - P1(dz1w, k) * (P1(dz1, k) + P1(dz1, k - 1));
+            }
+            P1(ak, 1) = 0.;
+            P1(ck, 1) = P1(dz1, 1) * P1(dz1w, 1) + P1(stab0, 1) * P1(dz1, 1);
+            P1(dk, 1) = wl - P1(dz1, 1) * P1(dz1w, 1) - P1(stab0, 1) * P1(dz1, 1);
+            P1(ak, nzp) = P1(dz1w, nzp) * P1(dz1, nzp - 1) - P1(stab0, nzp) * P1(dz1, nzp - 1);
+            P1(ck, nzp) = 0.;
+            P1(dk, nzp) = wl - P1(dz1w, nzp) * P1(dz1, nzp - 1) + P1(stab0, nzp) * P1(dz1, nzp - 1);
+            for (int k = 1; k <= nzp; k++)
+                P1(bk, k) = pass == 0 ? s1re[S(l, k)] : bre[(size_t)(l - 1) * nzp + (k - 1)];
+            int e = tridag2(ak, dk, ck, bk, xk + (size_t)(l - 1) * nzp, nzp);
+            if (e && !(m + l <= 2)) err = err ? err : e;
+        }
+        if (pass == 0) {
+            for (int k = 1; k <= nzp; k++)
+                for (int l = 1; l <= nxp; l++)
+                    if (m + l > 2) {
+                        bre[(size_t)(l - 1) * nzp + (k - 1)] = s1im[S(l, k)];
+                        s1re[S(l, k)] = xk[(size_t)(l - 1) * nzp + (k - 1)];
+                        s1im[S(l, k)] = 0.;
+                    }
+        } else {
+            for (int k = 1; k <= nzp; k++)
+                for (int l = 1; l <= nxp; l++)
+                    if (m + l > 2) s1im[S(l, k)] = xk[(size_t)(l - 1) * nzp + (k - 1)];
+        }
+    }
+#undef S
+    free(ak); free(bk); free(ck); free(dk); free(xk); free(bre);
+    return err;
+}
+
+/* fft_solve_serial: src/PRESSURE/fft_interface.f90:543-666 */
+int mo_fft_solve(const mo_grid *g, const double *tend, double *out)
+{
+    const int nxp = g->nx - 5, nyp = g->ny - 5, nzp = g->nz;
+    size_t pl = (size_t)nxp * nyp;
+    double *re = dalloc(pl * nzp), *im = dalloc(pl * nzp);
+    for (int k = 1; k <= nzp; k++)
+        for (int m = 1; m <= nyp; m++)
+            for (int l = 1; l <= nxp; l++)
+                re[(size_t)(k - 1) * pl + (size_t)(m - 1) * nxp + (l - 1)] = tend[IX(g, 3 + l, 3 + m, k)];
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < nzp; k++) mo_fft2d(nxp, nyp, re + (size_t)k * pl, im + (size_t)k * pl, 0);
+    int err = 0;
+#pragma omp parallel for schedule(static)
+    for (int m = 1; m <= nyp; m++) {
+        int e = mo_tridiag(g, m, nxp, nzp, g->wv + (size_t)(m - 1) * nxp, re + (size_t)(m - 1) * nxp,
+                           im + (size_t)(m - 1) * nxp, 1, pl);
+        if (e) {
+#pragma omp critical
+            if (!err) err = e;
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < nzp; k++) mo_fft2d(nxp, nyp, re + (size_t)k * pl, im + (size_t)k * pl, 1);
+    for (int k = 1; k <= nzp; k++)
+        for (int m = 1; m <= nyp; m++)
+            for (int l = 1; l <= nxp; l++)
+                out[IX(g, 3 + l, 3 + m, k)] = re[(size_t)(k - 1) * pl + (size_t)(m - 1) * nxp + (l - 1)];
+    free(re); free(im);
+    return err;
+}
+
+/* src/TOOLS/averages.f90:78-209 without filters: sequential sum over the interior */
+void mo_horav(const mo_grid *g, const double *x, double *xav)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    for (int k = 1; k <= nz; k++) {
+        double s = 0., ii = 0.;
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) {
+                double c = 1.;
+                s = s + c * x[IX(g, i, j, k)];
+                ii = ii + c;
+            }
+        P1(xav, k) = s / dmax2(ii, 1.);
+    }
+}
+
+/* src/PRESSURE/pressure_solver.f90:415-459 */
+void mo_rescale_pressure(const mo_grid *g, double *pp)
+{
+    size_t nc = ncell(g), pl = (size_t)g->nx * g->ny;
+    double nh = (double)((g->nx - 5) * (g->ny - 5));
+    for (size_t c = 0; c < nc; c++) pp[c] = pp[c] / nh;
+    double *pav = dalloc(g->nz);
+    mo_horav(g, pp, pav);
+    for (int k = 1; k <= g->nz; k++)
+        for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) pp[c] = pp[c] - P1(pav, k);
+    free(pav);
+}
+
+/* anelastic_pressure :73-140, solve_pressure :143-189, correction :342-412,
+ * cal_p1 src/TOOLS/funcpack.f90:750-793 (p_mcons off). */
+int mo_anelastic_pressure(const mo_grid *g, double *mu, double *mv, double *mw, double *p,
+                          const double *wold, double *maxdiv, double *p1)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    size_t nc = ncell(g), pl = (size_t)nx * ny;
+    double *deltap = dalloc(nc), *div = dalloc(nc), *tend = dalloc(nc);
+    double *gpx = dalloc(nc), *gpy = dalloc(nc), *gpz = dalloc(nc);
+    int err = 0;
+    double dt1 = 1. / g->dt0;
+    for (int ip = 1; ip <= g->nsubp; ip++) {
+        /* solve_pressure */
+        mo_caldiv(g, mu, mv, mw, tend);
+        for (int k = 1; k <= nz; k++)
+            for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) tend[c] = dt1 * tend[c] / P1(g->den0, k);
+        memset(deltap, 0, nc * sizeof(double));
+        int e = mo_fft_solve(g, tend, deltap);
+        if (e && !err) err = e;
+        mo_rescale_pressure(g, deltap);
+        /* correction */
+        for (int k = 1; k <= nz; k++)
+            for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) p[c] = p[c] + P1(g->den0, k) * deltap[c];
+        mo_gradp(g, deltap, mw, gpx, gpy, gpz);
+        for (int k = 1; k <= nz; k++)
+            for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) {
+                mu[c] = mu[c] - g->dt0 * P1(g->den0, k) * gpx[c];
+                mv[c] = mv[c] - g->dt0 * P1(g->den0, k) * gpy[c];
+                mw[c] = mw[c] - g->dt0 * P1(g->avden0, k) * gpz[c];
+            }
+        windbc(g, mu, mv, mw);
+    }
+    /* cal_p1 */
+    {
+        double *wav = dalloc(nz);
+        for (size_t c = 0; c < nc; c++) tend[c] = (mw[c] - wold[c]) / g->dt0;
+        mo_horav(g, tend, wav);
+        if (p1) {
+            P1(p1, nz) = 0.0;
+            for (int k = nz - 1; k >= 1; k--)
+                P1(p1, k) = P1(p1, k + 1) + P1(wav, k + 1) * 0.5 * g->dz * (P1(g->fdz0, k) + P1(g->fdz0, k + 1));
+        }
+        mo_horav(g, mw, wav);
+        for (int k = 1; k <= nz; k++)
+            for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) mw[c] = mw[c] - P1(wav, k);
+        free(wav);
+    }
+    mo_caldiv(g, mu, mv, mw, div);
+    if (maxdiv) {
+        double m = -INFINITY;
+        for (int k = 2; k <= nz - 1; k++)
+            for (int j = 4; j <= ny - 2; j++)
+                for (int i = 4; i <= nx - 2; i++) m = dmax2(m, div[IX(g, i, j, k)]);
+        *maxdiv = m;
+    }
+    free(deltap); free(div); free(tend); free(gpx); free(gpy); free(gpz);
+    return err;
+}
+
+/* ======================================================================
+ * One integrator step: src/INTEG/time_step.f90 stepping :76-334 (dynamics subset:
+ * with_dif, with_rad, with_mic, sponge, nudging off; w0 = 0), integrate_all
+ * :337-444, integ_mom/integ_scal src/INTEG/integpack.f90:54-284 with
+ * INCLUDE/integ.h, momentum src/INTEG/momentum.f90:64-228 (imp_buoy=.true.),
+ * scalars src/INTEG/scalars.f90:61-230, tracers src/INTEG/tracers.f90:50-125,
+ * get_momentum/get_velocities/get_conserved/get_scalars src/TOOLS/funcpack.f90.
+ * ==================================================================== */
+int mo_step(const mo_grid *g, int ntime, double *u, double *v, double *w, double *p,
+            double *dens, int nsc, double **scal, int iqt, double *maxdiv, double *p1)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    size_t nc = ncell(g), pl = (size_t)nx * ny;
+    const double dt0 = g->dt0, cdiag = 0.5;
+    int err = 0;
+    /* level n (time level 2 in the reference naming) */
+    double *u2 = dalloc(nc), *v2 = dalloc(nc), *w2 = dalloc(nc), *dens2 = dalloc(nc);
+    memcpy(u2, u, nc * 8); memcpy(v2, v, nc * 8); memcpy(w2, w, nc * 8); memcpy(dens2, dens, nc * 8);
+    double **s2 = (double **)calloc(nsc ? nsc : 1, sizeof(double *));
+    for (int s = 0; s < nsc; s++) { s2[s] = dalloc(nc); memcpy(s2[s], scal[s], nc * 8); }
+    /* working state: momentum and conserved scalars */
+    double *mu = dalloc(nc), *mv = dalloc(nc), *mw = dalloc(nc);
+    for (int k = 1; k <= nz; k++)
+        for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) {
+            mu[c] = u[c] * P1(g->den0, k);
+            mv[c] = v[c] * P1(g->den0, k);
+            mw[c] = w[c] * P1(g->avden0, k);
+        }
+    for (int s = 0; s < nsc; s++)
+        for (size_t c = 0; c < nc; c++) scal[s][c] = scal[s][c] * dens[c];
+    /* tendency accumulators (tend, reset at step start) */
+    double *tu = dalloc(nc), *tv = dalloc(nc), *tw = dalloc(nc), *td = dalloc(nc);
+    double **ts = (double **)calloc(nsc ? nsc : 1, sizeof(double *));
+    for (int s = 0; s < nsc; s++) ts[s] = dalloc(nc);
+    /* scratch */
+    double *windold = dalloc(nc), *ua = dalloc(nc), *va = dalloc(nc), *wa = dalloc(nc);
+    double *au = dalloc(nc), *av = dalloc(nc), *aw = dalloc(nc);
+    double *wsu = dalloc(nc), *wsv = dalloc(nc), *wsw = dalloc(nc), *wsd = dalloc(nc);
+    double **wss = (double **)calloc(nsc ? nsc : 1, sizeof(double *));
+    for (int s = 0; s < nsc; s++) wss[s] = dalloc(nc);
+    double *pp = dalloc(nc), *gpx = dalloc(nc), *gpy = dalloc(nc), *gpz = dalloc(nc), *buoy = dalloc(nc);
+    double *estmp = dalloc(nc), *qttmp = dalloc(nc);
+
+    for (int im = 1; im <= 2; im++) {
+        double a_lm = im == 1 ? 1. : 0.5, b_lm = im == 1 ? 0. : 1.;
+        memcpy(windold, mw, nc * 8);
+        memset(wsu, 0, nc * 8); memset(wsv, 0, nc * 8); memset(wsw, 0, nc * 8); memset(wsd, 0, nc * 8);
+        for (int s = 0; s < nsc; s++) memset(wss[s], 0, nc * 8);
+        mo_get_advective(g, mu, mv, mw, ua, va, wa);
+        /* scalars: density first (adv=.false.), then es, qt; tracers with advection_ac */
+        mo_advection_ac(g, dens, ua, va, wa, wsd, 0);
+        for (int s = 0; s < nsc; s++) mo_advection_ac(g, scal[s], ua, va, wa, wss[s], 0);
+        /* momentum */
+        for (int k = 1; k <= nz; k++)
+            for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) pp[c] = p[c] / P1(g->den0, k);
+        mo_gradp(g, pp, mw, gpx, gpy, gpz);
+        for (int k = 1; k <= nz; k++)
+            for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) {
+                wsu[c] = wsu[c] - P1(g->den0, k) * gpx[c];
+                wsv[c] = wsv[c] - P1(g->den0, k) * gpy[c];
+                wsw[c] = wsw[c] - P1(g->avden0, k) * gpz[c];
+            }
+        memset(buoy, 0, nc * 8);
+        if (g->with_buoy) {
+            /* imp_buoy: cb = 0, state_tmp = state + cdiag*dt0*states */
+            for (size_t c = 0; c < nc; c++) estmp[c] = scal[0][c] + cdiag * dt0 * wss[0][c];
+            if (iqt >= 0)
+                for (size_t c = 0; c < nc; c++) qttmp[c] = scal[iqt][c] + cdiag * dt0 * wss[iqt][c];
+            mo_buoyancy(g, dens, estmp, iqt >= 0 ? qttmp : NULL, buoy);
+            for (size_t c = 0; c < nc; c++) buoy[c] = 0. * 0. + (1. - 0.) * buoy[c];
+        }
+        mo_qnadv_uvw(g, ntime, mu, mv, mw, ua, va, wa, au, av, aw);
+        for (int k = 1; k <= nz; k++)
+            for (int j = 4; j <= ny - 2; j++)
+                for (int i = 4; i <= nx - 2; i++) {
+                    size_t c = IX(g, i, j, k);
+                    wsu[c] = -au[c] + wsu[c];
+                    wsv[c] = -av[c] + wsv[c];
+                    wsw[c] = -aw[c] + wsw[c] + buoy[c];
+                }
+        /* integrate_all(im): level-n values re-weighted */
+        for (int k = 1; k <= nz; k++)
+            for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) {
+                tu[c] = wsu[c] + b_lm * tu[c];
+                tv[c] = wsv[c] + b_lm * tv[c];
+                tw[c] = wsw[c] + b_lm * tw[c];
+                mu[c] = u2[c] * P1(g->den0, k) + a_lm * dt0 * tu[c];
+                mv[c] = v2[c] * P1(g->den0, k) + a_lm * dt0 * tv[c];
+                mw[c] = 1. * (w2[c] * P1(g->avden0, k) + a_lm * dt0 * tw[c]);
+            }
+        for (size_t c = 0; c < nc; c++) {
+            td[c] = wsd[c] + b_lm * td[c];
+            for (int s = 0; s < nsc; s++) ts[s][c] = wss[s][c] + b_lm * ts[s][c];
+            dens[c] = dens2[c] + a_lm * dt0 * td[c];
+            for (int s = 0; s < nsc; s++) scal[s][c] = s2[s][c] * dens2[c] + a_lm * dt0 * ts[s][c];
+        }
+        windbc(g, mu, mv, mw);
+        mo_statebc(g, p);
+        mo_statebc(g, dens);
+        for (int s = 0; s < nsc; s++) mo_statebc(g, scal[s]);
+        if (g->nsubp > 0) {
+            int e = mo_anelastic_pressure(g, mu, mv, mw, p, windold, maxdiv, p1);
+            if (e && !err) err = e;
+        }
+    }
+    /* get_velocities, get_scalars, update_prognostic BCs */
+    for (int k = 1; k <= nz; k++)
+        for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) {
+            u[c] = mu[c] / P1(g->den0, k);
+            v[c] = mv[c] / P1(g->den0, k);
+            w[c] = mw[c] / P1(g->avden0, k);
+        }
+    for (int s = 0; s < nsc; s++)
+        for (size_t c = 0; c < nc; c++) scal[s][c] = scal[s][c] / dens[c];
+    windbc(g, u, v, w);
+    mo_statebc(g, p);
+    mo_statebc(g, dens);
+    for (int s = 0; s < nsc; s++) mo_statebc(g, scal[s]);
+
+    free(u2); free(v2); free(w2); free(dens2);
+    for (int s = 0; s < nsc; s++) { free(s2[s]); free(ts[s]); free(wss[s]); }
+    free(s2); free(ts); free(wss);
+    free(mu); free(mv); free(mw); free(tu); free(tv); free(tw); free(td);
+    free(windold); free(ua); free(va); free(wa); free(au); free(av); free(aw);
+    free(wsu); free(wsv); free(wsw); free(wsd);
+    free(pp); free(gpx); free(gpy); free(gpz); free(buoy); free(estmp); free(qttmp);
+    return err;
+}

@@ -1,0 +1,107 @@
+/*
+ * mimica_oracle.h -- CPU FP64 restatement of MIMICA's dynamical-core hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA path: only
+ * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it.
+ * It is never the thing measured on the GPU arm and never a fallback of the
+ * product library.
+ *
+ * Parity status: the reference (Fortran 90, CPU only) has no compiler, no FFTW and
+ * no golden vectors for this path in this environment, so the Fortran routines are
+ * "parity unpinned" against a reference binary; they are restated line by line
+ * (each function cites the reference file:line it follows).  The FFT step is
+ * pinned against the reference's own KISS FFT (src/fftmpi/src/kissfft.h) compiled
+ * from its sources by oracle/build_ref.sh, and against numpy.fft.
+ *
+ * Array convention (identical to the reference): a 3-D field is
+ * real(8) x(1:nx,1:ny,1:nz), column-major, nx = MAXX+5, ny = MAXY+5, interior
+ * i in [4, nx-2], j in [4, ny-2]; C index ((k-1)*ny + (j-1))*nx + (i-1).
+ * Lateral boundaries periodic (bcl(1:4) = 'per'), bottom/top rigid (bcl(5:6) = 'nnf').
+ */
+#ifndef MIMICA_ORACLE_H
+#define MIMICA_ORACLE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { MO_WENO = 0, MO_PPM = 1, MO_MUSCL = 2 };
+enum { MO_LIM_MINMOD = 0, MO_LIM_VL = 1, MO_LIM_MC = 2, MO_LIM_DEFAULT = 3 };
+
+typedef struct mo_grid {
+    int nx, ny, nz;              /* full sizes incl. ghost cells */
+    int scal_adv;                /* MO_WENO / MO_PPM / MO_MUSCL */
+    int muscl_limiter;           /* MO_LIM_* (module default 'minmod') */
+    int mom_ord;                 /* 2 or 4 */
+    int lavisc;                  /* artificial viscosity on momentum */
+    int nsubp;                   /* pressure sub-iterations */
+    int with_buoy;
+    double dx, dy, dz, dt0;
+    double lim_tol;
+    double u0shift, v0shift;
+    /* 1-D profiles, length nz */
+    const double *fdz0, *dzw, *dz1w, *dz1;
+    const double *den0, *avden0, *stab0, *pt0, *qv0;
+    /* horizontal eigenvalues wv(1:nx-5, 1:ny-5), l fastest */
+    const double *wv;
+} mo_grid;
+
+/* ---- host precompute (define_grid, initial, get_wv) ---- */
+void mo_grid_metrics(int nz, double dz, const double *fdz, double *dzw, double *dz1w, double *dz1);
+void mo_base_state(int nz, double dz, double psurf, const double *fdz0, const double *dz1,
+                   const double *pt0, const double *qv0,
+                   double *p0, double *den0, double *avden0, double *stab0);
+void mo_get_wv(int nxp, int nyp, double dx, double dy, double *wv);
+
+/* ---- halo maps (bc.f90) ---- */
+void mo_statebc(const mo_grid *g, double *x);
+
+/* ---- per-pencil schemes (advq_*.f90), 1-based semantics, arrays of length n ---- */
+void mo_advs_h(const mo_grid *g, int scheme, int n, int i1, int i2, double d,
+               const double *x, const double *u, double *xa, int adv);
+void mo_advs_z(const mo_grid *g, int scheme, const double *x, const double *w, double *xa, int adv);
+
+/* ---- 3-D operators ---- */
+/* advection_x/y/z: xs := xs - xx, with xx the tendency of one direction */
+void mo_advection_dir(const mo_grid *g, int dir, const double *xtmp, const double *uadv,
+                      double *xs, int adv);
+/* advection of one field in all three directions: xs := ((xs - Tx) - Ty) - Tz */
+void mo_advection_ac(const mo_grid *g, const double *x, const double *ua, const double *va,
+                     const double *wa, double *xs, int adv);
+/* get_advective: wind_adv = m/rho0 - shift over all cells */
+void mo_get_advective(const mo_grid *g, const double *mu, const double *mv, const double *mw,
+                      double *ua, double *va, double *wa);
+/* qnadv_uvw: winda = momentum advection tendency (positive sign convention) */
+void mo_qnadv_uvw(const mo_grid *g, int ntime, const double *mu, const double *mv, const double *mw,
+                  const double *ua, const double *va, const double *wa,
+                  double *au, double *av, double *aw);
+void mo_caldiv(const mo_grid *g, double *mu, double *mv, double *mw, double *div);
+void mo_gradp(const mo_grid *g, double *p, const double *w, double *gpx, double *gpy, double *gpz);
+/* buoyancy (thermodynamics.f90:472-534), ANELASTIC, ISENTROPIC, nhydro=0 */
+void mo_buoyancy(const mo_grid *g, const double *dens, const double *es, const double *qt, double *buoy);
+
+/* ---- pressure ---- */
+void mo_fft2d(int nxp, int nyp, double *re, double *im, int inverse);   /* unnormalised DFT */
+int  mo_tridiag(const mo_grid *g, int m, int nxp, int nzp, const double *wvl,
+                double *s1re, double *s1im, size_t stride_l, size_t stride_k);
+int  mo_fft_solve(const mo_grid *g, const double *tend, double *out);
+void mo_rescale_pressure(const mo_grid *g, double *pp);
+void mo_horav(const mo_grid *g, const double *x, double *xav);
+int  mo_anelastic_pressure(const mo_grid *g, double *mu, double *mv, double *mw, double *p,
+                           const double *wold, double *maxdiv, double *p1);
+
+/* ---- one full integrator step (time_step.f90 stepping, dynamics subset) ----
+ * State at time level n, natural variables, all arrays nx*ny*nz with valid halos:
+ *   u, v, w (velocities), p, dens, scal[0..nsc)  (es = theta first, then qt if
+ *   with_qt, then passive scalars).  Updated in place to level n+1.
+ * iqt: index of qt among scal (or -1); buoyancy uses scal[0] as es.
+ */
+int mo_step(const mo_grid *g, int ntime, double *u, double *v, double *w, double *p,
+            double *dens, int nsc, double **scal, int iqt, double *maxdiv, double *p1);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
