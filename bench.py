@@ -206,6 +206,8 @@ def main():
     cfg = {"workload": f"shallow-cumulus domain {args.maxx}x{args.maxx}x{args.nz}, dx=dy=25 m, stretched dz 10->100 m, "
                        f"3 momentum + density + 5 scalars, {args.scheme.upper()} (reference scheme), FD4 momentum, "
                        f"dt=1 s, nsubp=1",
+           "fields": "theta_l 298->310 K, qt 17->4 g/kg, qr/nr/aerosol smooth decreasing profiles; "
+                     "seeded Gaussian perturbations below 500 m; u=-8+N(0,0.5), v=N(0,0.5) m/s",
            "form": "plain FP64", "scheme": args.scheme, "interior_cells": d.cells,
            "l2": "inputs larger than L2 (~16 GB working set)", "parallelism": f"replicas x{ws}"}
 

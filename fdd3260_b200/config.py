@@ -216,9 +216,11 @@ def cumulus_domain(maxx=512, maxy=512, nz=256, dx=25.0, dy=25.0, dt0=1.0, scheme
     return d.finish()
 
 
-def cumulus_state(d: Domain, seed: int = 1000, n_extra: int = 3) -> State:
+def cumulus_state(d: Domain, seed: int = 1000, n_extra: int = 3, lognormal_extras: bool = False) -> State:
     """theta_l, qt from the base profiles plus N(0,0.1 K / 0.1 g/kg) below 500 m; u = -8 + N(0,0.5);
-    v = N(0,0.5); w = 0; extra passive scalars (qr, nr, aerosol number) lognormal positive."""
+    v = N(0,0.5); w = 0.  Extra scalars (qr, nr, aerosol number): smooth positive profiles
+    decreasing with height with 1 % seeded Gaussian perturbations below 500 m, or, with
+    lognormal_extras, independent lognormal values (sigma_log = 1) in every cell."""
     rng = np.random.Generator(np.random.PCG64(seed))
     zc = d.zc()
     sh = (d.nz, d.maxy, d.maxx)
@@ -236,8 +238,12 @@ def cumulus_state(d: Domain, seed: int = 1000, n_extra: int = 3) -> State:
     w = _new(d)
     scal = [th, qt]
     scales = [1e-4, 1e5, 1e8]
+    prof = np.exp(-zc / 1500.0)[:, None, None]
     for e in range(n_extra):
-        scal.append(field3(scales[e % 3] * np.exp(rng.normal(0.0, 1.0, sh))))
+        if lognormal_extras:
+            scal.append(field3(scales[e % 3] * np.exp(rng.normal(0.0, 1.0, sh))))
+        else:
+            scal.append(field3(scales[e % 3] * prof * (1.0 + np.where(low, rng.normal(0, 0.01, sh), 0.0))))
     dens = np.broadcast_to(d.den0[:, None, None], d.shape).copy()
     return State(u, v, w, _new(d), dens, scal, iqt=1)
 

@@ -7,8 +7,8 @@
 //     K2  momentum: -grad p, buoyancy, advection, tend, m = m_n + a*dt*tend
 //     projection: nsubp x (rhs -> FFT -> tridiagonal -> inverse FFT -> correction),
 //                 cal_p1
-// Buffers: level-n (A), stage working (B), tendencies; the density has a third
-// buffer because every scalar's stage-2 update reads the level-n density.
+// Buffers: level n (A, natural variables between steps), stage working (B, density
+// weighted), tendencies.  Stage 2 writes the new level-n values into A in place.
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -36,6 +36,8 @@ struct mg_ctx {
     double *fes = nullptr, *fqt = nullptr;
     double *unit[8] = {};                // scratch of the unit-level entry points
     PressurePlan *pp = nullptr;
+    K1Maps maps1, maps2;                 // TMA descriptors: stage-1 inputs (level n), stage-2 inputs (working)
+    int *derr = nullptr;                 // device error flag of bounded waits
     int rep = REP_NAT;
     int have_state = 0;
     int launches = 0;
@@ -165,6 +167,24 @@ extern "C" int mg_get_wv(int maxx, int maxy, double dx, double dy, double *wv)
     return MG_OK;
 }
 
+// ---------------- TMA descriptors ----------------
+#include "tma.cuh"
+int make_field_map(const DevGrid &g, const double *base, int boxx, int boxy, CUtensorMap *map)
+{
+    CUresult r = mg_encode_field_map(map, base, g.nx, g.ny, g.nz, g.px, boxx, boxy);
+    return r == CUDA_SUCCESS ? MG_OK : MG_ERR_CUDA;
+}
+
+static int build_maps(mg_ctx *c, const double *const *x, int nf, const double *mu, const double *mv, K1Maps *m)
+{
+    memset(m, 0, sizeof(*m));
+    for (int f = 0; f < nf; f++)
+        if (make_field_map(c->G, x[f], 38, 14, &m->x[f])) return MG_ERR_CUDA;
+    if (make_field_map(c->G, mu, 34, 9, &m->mu)) return MG_ERR_CUDA;
+    if (make_field_map(c->G, mv, 34, 9, &m->mv)) return MG_ERR_CUDA;
+    return MG_OK;
+}
+
 // ---------------- context ----------------
 static bool good_len(int n)
 {
@@ -199,7 +219,7 @@ static void free_ctx(mg_ctx *c)
     for (int i = 0; i < 3; i++) { cudaFree(c->mA[i]); cudaFree(c->mB[i]); cudaFree(c->tm[i]); }
     for (int f = 0; f < MG_MAXF; f++) { cudaFree(c->sA[f]); cudaFree(c->sB[f]); cudaFree(c->ts[f]); }
     for (int i = 0; i < 8; i++) cudaFree(c->unit[i]);
-    cudaFree(c->p); cudaFree(c->dens3); cudaFree(c->fes); cudaFree(c->fqt); cudaFree(c->prof);
+    cudaFree(c->p); cudaFree(c->dens3); cudaFree(c->fes); cudaFree(c->fqt); cudaFree(c->prof); cudaFree(c->derr);
     pressure_plan_destroy(c->pp);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -265,10 +285,16 @@ extern "C" int mg_create(const mg_params *params, int device, mg_ctx **out)
         if (!rc) rc = alloc(&c->ts[f]);
     }
     if (!rc) rc = alloc(&c->p);
-    if (!rc) rc = alloc(&c->dens3);
     if (!rc) rc = alloc(&c->fes);
     if (!rc) rc = alloc(&c->fqt);
     if (rc) return fail(rc);
+    e = cudaMalloc(&c->derr, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(c->derr, 0, sizeof(int));
+    if (e == cudaSuccess) e = k1_init();
+    if (e != cudaSuccess) return fail(cuerr(e));
+    if (build_maps(c, c->sA, c->nf, c->mA[0], c->mA[1], &c->maps1) ||
+        build_maps(c, c->sB, c->nf, c->mB[0], c->mB[1], &c->maps2))
+        return fail(MG_ERR_CUDA);
     // horizontal eigenvalues (get_wv) and the projection plan
     c->wv.resize((size_t)G.maxx * G.maxy);
     mg_get_wv(G.maxx, G.maxy, G.dx, G.dy, c->wv.data());
@@ -377,25 +403,30 @@ extern "C" int mg_download_state_device(mg_ctx *c, double *u, double *v, double 
 }
 
 // ---------------- projection ----------------
-// nsubp x (solve + correction), cal_p1; wold: momentum w at stage start
+// nsubp x (solve + correction), cal_p1; wold: momentum w at stage start.
+// finalize: end of a step -- leave natural velocities (get_velocities) in mu, mv, mw.
 static cudaError_t project(mg_ctx *c, double *mu, double *mv, double *mw, const double *wold, int wold_rep,
-                           int want_p1, int want_maxdiv, int *launches)
+                           int want_p1, int want_maxdiv, int finalize, int *launches)
 {
     const DevGrid &G = c->G;
-    cudaError_t e;
+    const int fuse = finalize && !want_maxdiv;   // maxdiv needs the momentum after cal_p1
     for (int ip = 0; ip < c->prm.nsubp; ip++) {
+        const int last = ip == c->prm.nsubp - 1;
         PROF(c, "fft_x_fwd_div", launch_div_rhs(G, c->pp, mu, mv, mw, c->stream));
         PROF(c, "fft_y_tridiag_fft_y_fft_x_inv", pressure_solve(G, c->pp, 0., 0, c->stream));
-        PROF(c, "correction_halo", launch_correction(G, c->pp, mu, mv, mw, c->p, c->stream));
+        PROF(c, "correction_halo", launch_correction(G, c->pp, mu, mv, mw, c->p, fuse && last, c->stream));
         *launches += 7;
     }
-    PROF(c, "cal_p1", launch_cal_p1(G, c->pp, mw, wold, wold_rep, want_p1, c->stream));
+    PROF(c, "cal_p1", launch_cal_p1(G, c->pp, mw, wold, wold_rep, want_p1, fuse, c->stream));
     *launches += want_p1 ? 3 : 2;
     if (want_maxdiv) {
         PROF(c, "maxdiv", launch_maxdiv(G, c->pp, mu, mv, mw, c->stream));
         *launches += 2;
+        if (finalize) {
+            PROF(c, "to_velocity", launch_to_velocity(G, mu, mv, mw, c->stream));
+            *launches += 1;
+        }
     }
-    (void)e;
     return cudaSuccess;
 }
 
@@ -404,28 +435,25 @@ static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int wa
 {
     const DevGrid &G = c->G;
     const mg_params &P = c->prm;
-    cudaError_t e;
     const int nf = c->nf;
     const int ies = 1, iqt = P.iqt >= 0 ? 1 + P.iqt : -1;
     for (int stage = 1; stage <= 2; stage++) {
         const double a_dt = (stage == 1 ? 1. : 0.5) * G.dt0;
         const double b = stage == 1 ? 0. : 1.;
-        // ---- K1: scalars ----
+        // ---- K1: density + scalars (level-n buffers hold natural variables) ----
         K1Args a1{};
-        a1.nf = nf; a1.dens_first = 1; a1.stage = stage; a1.rep = c->rep; a1.a_dt = a_dt; a1.b = b;
+        a1.nf = nf; a1.dens_first = 1; a1.stage = stage; a1.a_dt = a_dt; a1.b = b; a1.mode = 0;
+        a1.err = c->derr;
         for (int f = 0; f < nf; f++) {
             a1.xin[f] = stage == 1 ? c->sA[f] : c->sB[f];
             a1.xold[f] = c->sA[f];
-            a1.xout[f] = stage == 1 ? c->sB[f] : (f == 0 ? c->dens3 : c->sA[f]);
+            a1.xout[f] = stage == 1 ? c->sB[f] : c->sA[f];
             a1.tend[f] = c->ts[f];
             a1.fst[f] = (f == ies && G.with_buoy) ? c->fes : ((f == iqt && G.with_buoy) ? c->fqt : nullptr);
         }
-        a1.dens_n = c->sA[0];
         const double *const *mom = stage == 1 ? c->mA : c->mB;
-        a1.mu = mom[0]; a1.mv = mom[1]; a1.mw = mom[2];
-        a1.mom_rep = stage == 1 ? c->rep : -1;
-        a1.mode = 0;
-        PROF(c, "k1_scalar_advection", launch_k1(G, a1, c->stream));
+        a1.mw = mom[2];
+        PROF(c, "k1_scalar_advection", launch_k1(G, a1, stage == 1 ? c->maps1 : c->maps2, c->stream));
         {
             std::vector<double *> f;
             for (int q = 0; q < nf; q++) f.push_back(a1.xout[q]);
@@ -433,11 +461,13 @@ static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int wa
         }
         // ---- K2: momentum ----
         K2Args a2{};
-        a2.stage = stage; a2.rep = c->rep; a2.ntime = ntime; a2.a_dt = a_dt; a2.b = b;
+        a2.stage = stage; a2.rep = REP_NAT; a2.ntime = ntime; a2.a_dt = a_dt; a2.b = b;
         a2.mu = mom[0]; a2.mv = mom[1]; a2.mw = mom[2];
         a2.in_is_leveln = stage == 1;
         a2.mu_n = c->mA[0]; a2.mv_n = c->mA[1]; a2.mw_n = c->mA[2];
         a2.p = c->p;
+        // buoyancy reads the stage's input density and scalars: level n in stage 1 (natural,
+        // unchanged by K1 stage 1), the working values in stage 2
         a2.dens = stage == 1 ? c->sA[0] : c->sB[0];
         a2.es = stage == 1 ? c->sA[ies] : c->sB[ies];
         a2.qt = iqt >= 0 ? (stage == 1 ? c->sA[iqt] : c->sB[iqt]) : nullptr;
@@ -452,15 +482,26 @@ static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int wa
         *launches += 4;
         // ---- projection ----
         const double *wold = stage == 1 ? c->mA[2] : c->mB[2];
-        int wold_rep = stage == 1 ? c->rep : -1;
-        if ((e = project(c, mo[0], mo[1], mo[2], wold, wold_rep, last && stage == 2 && want_p1,
-                         last && stage == 2 && want_maxdiv, launches)) != cudaSuccess)
-            return e;
+        const int wold_rep = stage == 1 ? REP_NAT : -1;
+        cudaError_t e = project(c, mo[0], mo[1], mo[2], wold, wold_rep, last && stage == 2 && want_p1,
+                                last && stage == 2 && want_maxdiv, stage == 2, launches);
+        if (e != cudaSuccess) return e;
     }
-    // end of step: new density becomes level n; state is now density weighted
-    double *t = c->sA[0]; c->sA[0] = c->dens3; c->dens3 = t;
-    c->rep = REP_CONS;
+    c->rep = REP_NAT;
     return cudaSuccess;
+}
+
+static int check_err(mg_ctx *c)
+{
+    int h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, c->derr, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuerr(e);
+    if (h) {
+        cudaMemsetAsync(c->derr, 0, sizeof(int), c->stream);
+        return MG_ERR_TIMEOUT;
+    }
+    return MG_OK;
 }
 
 extern "C" int mg_step(mg_ctx *c, int nsteps, int ntime0, double *maxdiv, double *p1)
@@ -476,36 +517,27 @@ extern "C" int mg_step(mg_ctx *c, int nsteps, int ntime0, double *maxdiv, double
     c->launches = launches;
     if (maxdiv && nsteps > 0) CKR(cudaMemcpyAsync(maxdiv, pressure_maxdiv_dev(c->pp), 8, cudaMemcpyDeviceToHost, c->stream));
     if (p1 && nsteps > 0) CKR(cudaMemcpyAsync(p1, pressure_p1_dev(c->pp), c->G.nz * 8, cudaMemcpyDeviceToHost, c->stream));
-    if (maxdiv || p1) CKR(cudaStreamSynchronize(c->stream));
-    return MG_OK;
+    return check_err(c);
 }
 
 extern "C" int mg_step_graph(mg_ctx *c, int nsteps, int ntime0, double *maxdiv, double *p1)
 {
-    // The step alternates buffer roles (density pointers swap every step), so the
-    // graph covers a pair of steps; odd remainders run eagerly.
+    // The graph covers a pair of steps (the momentum direction order alternates with
+    // the step counter's parity); odd remainders run eagerly.
     if (!c || nsteps < 0) return MG_ERR_PARAM;
     if (!c->have_state) return MG_ERR_STATE;
     CKR(cudaSetDevice(c->device));
     int rc = MG_OK;
     int s = 0;
-    // the first step after an upload uses the natural representation: run it eagerly
-    if (c->rep == REP_NAT && nsteps > 0) {
-        rc = mg_step(c, 1, ntime0, nullptr, nullptr);
-        if (rc) return rc;
-        s = 1;
-    }
     int par = (ntime0 + s) & 1;
     while (nsteps - s >= 2) {
         if (!c->gexec[par]) {
             cudaGraph_t graph;
-            double *sa0 = c->sA[0], *d3 = c->dens3;
             CKR(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
             int launches = 0;
             cudaError_t e = step_once(c, ntime0 + s, 0, 0, 0, &launches);
             if (e == cudaSuccess) e = step_once(c, ntime0 + s + 1, 0, 0, 0, &launches);
             cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
-            c->sA[0] = sa0; c->dens3 = d3;   // capture recorded two swaps: back to the same roles
             if (e != cudaSuccess) return cuerr(e);
             if (e2 != cudaSuccess) return cuerr(e2);
             e = cudaGraphInstantiate(&c->gexec[par], graph, 0);
@@ -516,6 +548,8 @@ extern "C" int mg_step_graph(mg_ctx *c, int nsteps, int ntime0, double *maxdiv, 
         CKR(cudaGraphLaunch(c->gexec[par], c->stream));
         s += 2;
     }
+    rc = check_err(c);
+    if (rc) return rc;
     if (s < nsteps) {
         rc = mg_step(c, nsteps - s, ntime0 + s, maxdiv, p1);
         if (rc) return rc;
@@ -564,13 +598,16 @@ extern "C" int mg_advection_ac(mg_ctx *c, const double *x, const double *mu, con
     CKR(h2d(c, c->unit[3], mw, cudaMemcpyHostToDevice));
     CKR(h2d(c, c->unit[4], xs, cudaMemcpyHostToDevice));
     K1Args a{};
-    a.nf = 1; a.dens_first = 0; a.stage = 0; a.rep = REP_NAT; a.mode = 1;
+    a.nf = 1; a.dens_first = 0; a.stage = 0; a.mode = 1; a.err = c->derr;
     a.xin[0] = c->unit[0]; a.xold[0] = c->unit[0]; a.xout[0] = c->unit[4];
-    a.dens_n = c->unit[0];
-    a.mu = c->unit[1]; a.mv = c->unit[2]; a.mw = c->unit[3]; a.mom_rep = -1;
-    CKR(launch_k1(c->G, a, c->stream));
+    a.mw = c->unit[3];
+    K1Maps maps;
+    const double *xv[1] = {c->unit[0]};
+    rc = build_maps(c, xv, 1, c->unit[1], c->unit[2], &maps);
+    if (rc) return rc;
+    CKR(launch_k1(c->G, a, maps, c->stream));
     CKR(d2h(c, xs, c->unit[4], cudaMemcpyDeviceToHost));
-    return cuerr(cudaStreamSynchronize(c->stream));
+    return check_err(c);
 }
 
 extern "C" int mg_qnadv_uvw(mg_ctx *c, int ntime, const double *mu, const double *mv, const double *mw, double *au,
@@ -628,7 +665,7 @@ extern "C" int mg_anelastic_pressure(mg_ctx *c, double *mu, double *mv, double *
     double *psave = c->p;
     c->p = c->unit[3];
     int launches = 0;
-    cudaError_t e = project(c, c->unit[0], c->unit[1], c->unit[2], c->unit[4], -1, p1 != nullptr, 1, &launches);
+    cudaError_t e = project(c, c->unit[0], c->unit[1], c->unit[2], c->unit[4], -1, p1 != nullptr, 1, 0, &launches);
     c->p = psave;
     if (e != cudaSuccess) return cuerr(e);
     CKR(d2h(c, mu, c->unit[0], cudaMemcpyDeviceToHost));

@@ -69,9 +69,12 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
             ring_a[(slot * 3 + arr) * PL + o] = av;
         }
     };
-    // accessors: component c (0 u, 1 v, 2 w), level l, offsets di, dj
-#define MM(c, l, di, dj) ring_m[(((l) % NSLOT) * 3 + (c)) * PL + (ty + R + (dj)) * PW + (tx + R + (di))]
-#define AA(c, l, di, dj) ring_a[(((l) % NSLOT) * 3 + (c)) * PL + (ty + R + (dj)) * PW + (tx + R + (di))]
+    // Per level k: lb[d+2] = this thread's element of ring slot (k+d) mod 5, d = -2..2.
+    // MM/AA(c, d, di, dj): momentum / advective velocity of component c (0 u, 1 v, 2 w)
+    // at (i+di, j+dj, k+d); d, di, dj are compile-time constants at every use.
+    const double *lb[5];
+#define MM(c, d, di, dj) lb[(d) + 2][(c) * PL + (dj) * PW + (di)]
+#define AA(c, d, di, dj) lb[(d) + 2][NSLOT * 3 * PL + (c) * PL + (dj) * PW + (di)]
 #define ZW(l) ldg(dzw, (l) - 1)
 #define ZW1(l) ldg(dz1w, (l) - 1)
 #define Z1(l) ldg(dz1, (l) - 1)
@@ -80,56 +83,102 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
     if (nz >= 2) load_level(2);
 
     double bb_prev = 0.;   // buoyancy at level k-1 (cell centre)
+    // vertical fluxes carried up the column (each computed once):
+    //   fzu/fzv[m] = Flux(k-2+m) of advuz/advvz, m = 0..3;  fzw[m] = Flux(k-1+m) and
+    //   azw[m] = Adv(k-2+m) of advwz;  pp_below = p(k-1)/rho0(k-1)
+    double fzu0 = 0., fzu1 = 0., fzu2 = 0., fzu3 = 0., fzv0 = 0., fzv1 = 0., fzv2 = 0., fzv3 = 0.;
+    double fzw0 = 0., fzw1 = 0., azw0 = 0., azw1 = 0., azw2 = 0.;
+    double pp_below = 0.;
     const bool even = (A.ntime % 2) == 0;
     const double grav = 9.81, epsm = 0.60243, cdiag = 0.5;
+    const int own = (ty + R) * PW + (tx + R);
 
     for (int k = 1; k <= nz; k++) {
         __syncthreads();
         if (k + 2 <= nz) load_level(k + 2);
         __syncthreads();
         if (!act) continue;   // no further barriers in this iteration
+#pragma unroll
+        for (int d = -2; d <= 2; d++) lb[d + 2] = ring_m + (((k + d + NSLOT) % NSLOT) * 3) * PL + own;
+
+        // ---- advance the carried vertical fluxes ----
+        {
+            // advuz_fd/advvz_fd Flux(k+1) (windadv.f90:656-663): levels k+1, k+2; Flux(nz) = 0
+            double fu = 0., fv = 0.;
+            if (k + 1 <= nz - 1) {
+                const double zp = ZW(k + 2), zc = ZW(k + 1), zs = zp + zc;
+                double ww = c1b * (AA(2, 2, -1, 0) + AA(2, 2, 0, 0)) * 0.5 - c2b * (AA(2, 2, -2, 0) + AA(2, 2, 1, 0)) * 0.5;
+                double fr = (zp * MM(0, 2, 0, 0) + zc * MM(0, 1, 0, 0)) / zs;
+                fu = ww * fr;
+                ww = c1b * (AA(2, 2, 0, -1) + AA(2, 2, 0, 0)) * 0.5 - c2b * (AA(2, 2, 0, -2) + AA(2, 2, 0, 1)) * 0.5;
+                fr = (zp * MM(1, 2, 0, 0) + zc * MM(1, 1, 0, 0)) / zs;
+                fv = ww * fr;
+            }
+            if (k == 1) {   // Flux(1): levels 1, 2
+                const double zp = ZW(2), zc = ZW(1), zs = zp + zc;
+                double ww = c1b * (AA(2, 1, -1, 0) + AA(2, 1, 0, 0)) * 0.5 - c2b * (AA(2, 1, -2, 0) + AA(2, 1, 1, 0)) * 0.5;
+                double fr = (zp * MM(0, 1, 0, 0) + zc * MM(0, 0, 0, 0)) / zs;
+                fzu3 = ww * fr;
+                ww = c1b * (AA(2, 1, 0, -1) + AA(2, 1, 0, 0)) * 0.5 - c2b * (AA(2, 1, 0, -2) + AA(2, 1, 0, 1)) * 0.5;
+                fr = (zp * MM(1, 1, 0, 0) + zc * MM(1, 0, 0, 0)) / zs;
+                fzv3 = ww * fr;
+            }
+            fzu0 = fzu1; fzu1 = fzu2; fzu2 = fzu3; fzu3 = fu;
+            fzv0 = fzv1; fzv1 = fzv2; fzv2 = fzv3; fzv3 = fv;
+            // advwz_fd Flux(k), Adv(k) (:1087-1098)
+            double fw = 0., aw_ = 0.;
+            if (k <= nz - 2) {
+                double ww = (AA(2, 1, 0, 0) + AA(2, 0, 0, 0)) * 0.5;
+                double fr = (MM(2, 1, 0, 0) + MM(2, 0, 0, 0)) * 0.5;
+                fw = ww * fr;
+                const double zp = ZW(k + 1), zc = ZW(k), zs = zp + zc;
+                double ww2 = (zp * AA(2, 2, 0, 0) + zc * AA(2, 0, 0, 0)) / zs;
+                double fr2 = (zp * MM(2, 2, 0, 0) + zc * MM(2, 0, 0, 0)) / zs;
+                aw_ = ww2 * fr2;
+            } else if (k == nz - 1) {
+                fw = 0.25 * (AA(2, 1, 0, 0) + AA(2, 0, 0, 0)) * (MM(2, 1, 0, 0) + MM(2, 0, 0, 0));
+                const double s2 = ZW(nz) + ZW(nz - 1);
+                aw_ = (0. + ZW(nz - 1) * AA(2, 0, 0, 0)) * (0. + ZW(nz - 1) * MM(2, 0, 0, 0)) / (s2 * s2);
+            }
+            fzw0 = fzw1; fzw1 = fw;
+            azw0 = azw1; azw1 = azw2; azw2 = aw_;
+        }
 
         // ---------------- u component ----------------
         double au = 0.;
         for (int pass = 0; pass < 3; pass++) {
             int dir = even ? pass : 2 - pass;
             if (dir == 0) {   // advux_fd
-                auto Fx = [&](int p) { return ((AA(0, k, p + 1, 0) + AA(0, k, p, 0)) * 0.5) * ((MM(0, k, p + 1, 0) + MM(0, k, p, 0)) * 0.5); };
-                auto Ax = [&](int p) { return ((AA(0, k, p + 2, 0) + AA(0, k, p, 0)) * 0.5) * ((MM(0, k, p + 2, 0) + MM(0, k, p, 0)) * 0.5); };
-                au = au + c1a * (Fx(0) - Fx(-1)) * dx1 - c2a * (Ax(0) - Ax(-2)) * dx2;
+#define FX(p) (((AA(0, 0, (p) + 1, 0) + AA(0, 0, (p), 0)) * 0.5) * ((MM(0, 0, (p) + 1, 0) + MM(0, 0, (p), 0)) * 0.5))
+#define AX(p) (((AA(0, 0, (p) + 2, 0) + AA(0, 0, (p), 0)) * 0.5) * ((MM(0, 0, (p) + 2, 0) + MM(0, 0, (p), 0)) * 0.5))
+                au = au + c1a * (FX(0) - FX(-1)) * dx1 - c2a * (AX(0) - AX(-2)) * dx2;
+#undef FX
+#undef AX
                 if (G.lavisc) {
-                    double mu = fabs(AA(0, k, 0, 0)) * dx1;
-                    au = au - AVISC * mu * (-MM(0, k, 2, 0) + 4. * MM(0, k, 1, 0) - 6. * MM(0, k, 0, 0) + 4. * MM(0, k, -1, 0) - MM(0, k, -2, 0));
+                    double mu = fabs(AA(0, 0, 0, 0)) * dx1;
+                    au = au - AVISC * mu * (-MM(0, 0, 2, 0) + 4. * MM(0, 0, 1, 0) - 6. * MM(0, 0, 0, 0) + 4. * MM(0, 0, -1, 0) - MM(0, 0, -2, 0));
                 }
             } else if (dir == 1) {   // advuy_fd: vt1=vt(i-1), vt2=vt(i), vt3=vt(i-2), vt4=vt(i+1)
-                auto Fy = [&](int p) {
-                    double vv = c1b * (AA(1, k, -1, p + 1) + AA(1, k, 0, p + 1)) * 0.5 - c2b * (AA(1, k, -2, p + 1) + AA(1, k, 1, p + 1)) * 0.5;
-                    double fr = (MM(0, k, 0, p + 1) + MM(0, k, 0, p)) * 0.5;
-                    return vv * fr;
-                };
-                au = au + c1b * (Fy(0) - Fy(-1)) * dy1 - c2b * (Fy(1) - Fy(-2)) * dy3;
+#define FY(p) ((c1b * (AA(1, 0, -1, (p) + 1) + AA(1, 0, 0, (p) + 1)) * 0.5 - c2b * (AA(1, 0, -2, (p) + 1) + AA(1, 0, 1, (p) + 1)) * 0.5) * \
+               ((MM(0, 0, 0, (p) + 1) + MM(0, 0, 0, (p))) * 0.5))
+                au = au + c1b * (FY(0) - FY(-1)) * dy1 - c2b * (FY(1) - FY(-2)) * dy3;
+#undef FY
                 if (G.lavisc) {
-                    double mu = 0.25 * fabs(AA(1, k, -1, 0) + AA(1, k, 0, 0) + AA(1, k, -1, 1) + AA(1, k, 0, 1)) * dy1;
-                    au = au - AVISC * mu * (-MM(0, k, 0, 2) + 4. * MM(0, k, 0, 1) - 6. * MM(0, k, 0, 0) + 4. * MM(0, k, 0, -1) - MM(0, k, 0, -2));
+                    double mu = 0.25 * fabs(AA(1, 0, -1, 0) + AA(1, 0, 0, 0) + AA(1, 0, -1, 1) + AA(1, 0, 0, 1)) * dy1;
+                    au = au - AVISC * mu * (-MM(0, 0, 0, 2) + 4. * MM(0, 0, 0, 1) - 6. * MM(0, 0, 0, 0) + 4. * MM(0, 0, 0, -1) - MM(0, 0, 0, -2));
                 }
-            } else {   // advuz_fd
-                auto Fz = [&](int l) -> double {
-                    if (l >= nz || l < 1) return 0.;
-                    double ww = c1b * (AA(2, l + 1, -1, 0) + AA(2, l + 1, 0, 0)) * 0.5 - c2b * (AA(2, l + 1, -2, 0) + AA(2, l + 1, 1, 0)) * 0.5;
-                    double fr = (ZW(l + 1) * MM(0, l + 1, 0, 0) + ZW(l) * MM(0, l, 0, 0)) / (ZW(l + 1) + ZW(l));
-                    return ww * fr;
-                };
+            } else {   // advuz_fd, Flux(k-2..k+1) = fzu0..fzu3
                 if (k >= 3 && k <= nz - 1)
-                    au = au + c1b * (Fz(k) - Fz(k - 1)) * ZW1(k) - c2b * (Fz(k + 1) - Fz(k - 2)) / (ZW(k - 1) + ZW(k) + ZW(k + 1));
+                    au = au + c1b * (fzu2 - fzu1) * ZW1(k) - c2b * (fzu3 - fzu0) / (ZW(k - 1) + ZW(k) + ZW(k + 1));
                 else if (k == 1)
-                    au = au + (Fz(1) - 0.) * ZW1(1);
+                    au = au + (fzu2 - 0.) * ZW1(1);
                 else if (k == 2)
-                    au = au + c1b * (Fz(2) - Fz(1)) * ZW1(1) - c2b * (Fz(3) - 0.) / (ZW(1) + ZW(2) + ZW(3));
+                    au = au + c1b * (fzu2 - fzu1) * ZW1(1) - c2b * (fzu3 - 0.) / (ZW(1) + ZW(2) + ZW(3));
                 else
-                    au = au + (0. - Fz(nz - 1)) * ZW1(nz);
+                    au = au + (0. - fzu1) * ZW1(nz);
                 if (G.lavisc && k >= 3 && k <= nz - 2) {
-                    double mu = 0.25 * fabs(AA(2, k, -1, 0) + AA(2, k, 0, 0) + AA(2, k + 1, -1, 0) + AA(2, k + 1, 0, 0)) * ZW1(k);
-                    au = au - AVISC * mu * (-MM(0, k + 2, 0, 0) + 4. * MM(0, k + 1, 0, 0) - 6. * MM(0, k, 0, 0) + 4. * MM(0, k - 1, 0, 0) - MM(0, k - 2, 0, 0));
+                    double mu = 0.25 * fabs(AA(2, 0, -1, 0) + AA(2, 0, 0, 0) + AA(2, 1, -1, 0) + AA(2, 1, 0, 0)) * ZW1(k);
+                    au = au - AVISC * mu * (-MM(0, 2, 0, 0) + 4. * MM(0, 1, 0, 0) - 6. * MM(0, 0, 0, 0) + 4. * MM(0, -1, 0, 0) - MM(0, -2, 0, 0));
                 }
             }
         }
@@ -139,42 +188,36 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
         for (int pass = 0; pass < 3; pass++) {
             int dir = even ? pass : 2 - pass;
             if (dir == 0) {   // advvx_fd: ut1=ut(j-1), ut2=ut(j), ut3=ut(j-2), ut4=ut(j+1)
-                auto Fx = [&](int p) {
-                    double uu = c1b * (AA(0, k, p + 1, -1) + AA(0, k, p + 1, 0)) * 0.5 - c2b * (AA(0, k, p + 1, -2) + AA(0, k, p + 1, 1)) * 0.5;
-                    double fr = (MM(1, k, p + 1, 0) + MM(1, k, p, 0)) * 0.5;
-                    return uu * fr;
-                };
-                av = av + c1b * (Fx(0) - Fx(-1)) * dx1 - c2b * (Fx(1) - Fx(-2)) * dx3;
+#define FX(p) ((c1b * (AA(0, 0, (p) + 1, -1) + AA(0, 0, (p) + 1, 0)) * 0.5 - c2b * (AA(0, 0, (p) + 1, -2) + AA(0, 0, (p) + 1, 1)) * 0.5) * \
+               ((MM(1, 0, (p) + 1, 0) + MM(1, 0, (p), 0)) * 0.5))
+                av = av + c1b * (FX(0) - FX(-1)) * dx1 - c2b * (FX(1) - FX(-2)) * dx3;
+#undef FX
                 if (G.lavisc) {
-                    double mu = 0.25 * fabs(AA(0, k, 0, -1) + AA(0, k, 0, 0) + AA(0, k, 1, -1) + AA(0, k, 1, 0)) * dx1;
-                    av = av - AVISC * mu * (-MM(1, k, 2, 0) + 4. * MM(1, k, 1, 0) - 6. * MM(1, k, 0, 0) + 4. * MM(1, k, -1, 0) - MM(1, k, -2, 0));
+                    double mu = 0.25 * fabs(AA(0, 0, 0, -1) + AA(0, 0, 0, 0) + AA(0, 0, 1, -1) + AA(0, 0, 1, 0)) * dx1;
+                    av = av - AVISC * mu * (-MM(1, 0, 2, 0) + 4. * MM(1, 0, 1, 0) - 6. * MM(1, 0, 0, 0) + 4. * MM(1, 0, -1, 0) - MM(1, 0, -2, 0));
                 }
             } else if (dir == 1) {   // advvy_fd
-                auto Fy = [&](int p) { return ((AA(1, k, 0, p + 1) + AA(1, k, 0, p)) * 0.5) * ((MM(1, k, 0, p + 1) + MM(1, k, 0, p)) * 0.5); };
-                auto Ay = [&](int p) { return ((AA(1, k, 0, p + 2) + AA(1, k, 0, p)) * 0.5) * ((MM(1, k, 0, p + 2) + MM(1, k, 0, p)) * 0.5); };
-                av = av + c1a * (Fy(0) - Fy(-1)) * dy1 - c2a * (Ay(0) - Ay(-2)) * dy2;
+#define FY(p) (((AA(1, 0, 0, (p) + 1) + AA(1, 0, 0, (p))) * 0.5) * ((MM(1, 0, 0, (p) + 1) + MM(1, 0, 0, (p))) * 0.5))
+#define AY(p) (((AA(1, 0, 0, (p) + 2) + AA(1, 0, 0, (p))) * 0.5) * ((MM(1, 0, 0, (p) + 2) + MM(1, 0, 0, (p))) * 0.5))
+                av = av + c1a * (FY(0) - FY(-1)) * dy1 - c2a * (AY(0) - AY(-2)) * dy2;
+#undef FY
+#undef AY
                 if (G.lavisc) {
-                    double mu = fabs(AA(1, k, 0, 0)) * dy1;
-                    av = av - AVISC * mu * (-MM(1, k, 0, 2) + 4. * MM(1, k, 0, 1) - 6. * MM(1, k, 0, 0) + 4. * MM(1, k, 0, -1) - MM(1, k, 0, -2));
+                    double mu = fabs(AA(1, 0, 0, 0)) * dy1;
+                    av = av - AVISC * mu * (-MM(1, 0, 0, 2) + 4. * MM(1, 0, 0, 1) - 6. * MM(1, 0, 0, 0) + 4. * MM(1, 0, 0, -1) - MM(1, 0, 0, -2));
                 }
-            } else {   // advvz_fd: wt1=wt(j-1), wt2=wt(j), wt3=wt(j-2), wt4=wt(j+1)
-                auto Fz = [&](int l) -> double {
-                    if (l >= nz || l < 1) return 0.;
-                    double ww = c1b * (AA(2, l + 1, 0, -1) + AA(2, l + 1, 0, 0)) * 0.5 - c2b * (AA(2, l + 1, 0, -2) + AA(2, l + 1, 0, 1)) * 0.5;
-                    double fr = (ZW(l + 1) * MM(1, l + 1, 0, 0) + ZW(l) * MM(1, l, 0, 0)) / (ZW(l + 1) + ZW(l));
-                    return ww * fr;
-                };
+            } else {   // advvz_fd, Flux(k-2..k+1) = fzv0..fzv3
                 if (k >= 3 && k <= nz - 1)
-                    av = av + c1b * (Fz(k) - Fz(k - 1)) * ZW1(k) - c2b * (Fz(k + 1) - Fz(k - 2)) / (ZW(k - 1) + ZW(k) + ZW(k + 1));
+                    av = av + c1b * (fzv2 - fzv1) * ZW1(k) - c2b * (fzv3 - fzv0) / (ZW(k - 1) + ZW(k) + ZW(k + 1));
                 else if (k == 1)
-                    av = av + (Fz(1) - 0.) * ZW1(1);
+                    av = av + (fzv2 - 0.) * ZW1(1);
                 else if (k == 2)
-                    av = av + c1b * (Fz(2) - Fz(1)) * ZW1(2) - c2b * (Fz(3) - 0.) / (ZW(1) + ZW(2) + ZW(3));
+                    av = av + c1b * (fzv2 - fzv1) * ZW1(2) - c2b * (fzv3 - 0.) / (ZW(1) + ZW(2) + ZW(3));
                 else
-                    av = av + (0. - Fz(nz - 1)) * ZW1(nz);
+                    av = av + (0. - fzv1) * ZW1(nz);
                 if (G.lavisc && k >= 3 && k <= nz - 2) {
-                    double mu = 0.25 * fabs(AA(2, k, 0, -1) + AA(2, k, 0, 0) + AA(2, k + 1, 0, -1) + AA(2, k + 1, 0, 0)) * ZW1(k);
-                    av = av - AVISC * mu * (-MM(1, k + 2, 0, 0) + 4. * MM(1, k + 1, 0, 0) - 6. * MM(1, k, 0, 0) + 4. * MM(1, k - 1, 0, 0) - MM(1, k - 2, 0, 0));
+                    double mu = 0.25 * fabs(AA(2, 0, 0, -1) + AA(2, 0, 0, 0) + AA(2, 1, 0, -1) + AA(2, 1, 0, 0)) * ZW1(k);
+                    av = av - AVISC * mu * (-MM(1, 2, 0, 0) + 4. * MM(1, 1, 0, 0) - 6. * MM(1, 0, 0, 0) + 4. * MM(1, -1, 0, 0) - MM(1, -2, 0, 0));
                 }
             }
         }
@@ -184,51 +227,42 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
         if (k >= 2) {
             for (int pass = 0; pass < 3; pass++) {
                 int dir = even ? pass : 2 - pass;
-                if (dir == 0 || dir == 1) {   // advwx_fd / advwy_fd
-                    const int c = dir;   // transport component
-                    auto hv = [&](int p, int l) { return dir == 0 ? AA(c, l, p, 0) : AA(c, l, 0, p); };
-                    auto wv = [&](int p) { return dir == 0 ? MM(2, k, p, 0) : MM(2, k, 0, p); };
-                    auto Fh = [&](int p) -> double {
-                        double uu;
-                        if (k == 2) uu = (hv(p + 1, 2) + hv(p + 1, 1)) * 0.5;
-                        else if (k == nz) uu = (hv(p + 1, nz) + hv(p + 1, nz - 1)) * 0.5;
-                        else uu = c1b * (hv(p + 1, k) + hv(p + 1, k - 1)) * 0.5 - c2b * (hv(p + 1, k + 1) + hv(p + 1, k - 2)) * 0.5;
-                        double fr = (wv(p + 1) + wv(p)) * 0.5;
-                        return uu * fr;
-                    };
-                    const double d1 = dir == 0 ? dx1 : dy1, d3 = dir == 0 ? dx3 : dy3;
-                    aw = aw + c1b * (Fh(0) - Fh(-1)) * d1 - c2b * (Fh(1) - Fh(-2)) * d3;
+                if (dir == 0) {   // advwx_fd
+#define HV(p, d) AA(0, d, p, 0)
+#define WV(p) MM(2, 0, p, 0)
+#define FH(p) ((k == 2 ? (HV((p) + 1, 0) + HV((p) + 1, -1)) * 0.5                                            \
+                       : (k == nz ? (HV((p) + 1, 0) + HV((p) + 1, -1)) * 0.5                                  \
+                                  : c1b * (HV((p) + 1, 0) + HV((p) + 1, -1)) * 0.5 -                          \
+                                        c2b * (HV((p) + 1, 1) + HV((p) + 1, -2)) * 0.5)) *                    \
+                ((WV((p) + 1) + WV(p)) * 0.5))
+                    aw = aw + c1b * (FH(0) - FH(-1)) * dx1 - c2b * (FH(1) - FH(-2)) * dx3;
                     if (G.lavisc) {
-                        double mu = 0.25 * fabs(hv(0, k) + hv(0, k - 1) + hv(1, k) + hv(1, k - 1)) * d1;
-                        aw = aw - AVISC * mu * (-wv(2) + 4. * wv(1) - 6. * wv(0) + 4. * wv(-1) - wv(-2));
+                        double mu = 0.25 * fabs(HV(0, 0) + HV(0, -1) + HV(1, 0) + HV(1, -1)) * dx1;
+                        aw = aw - AVISC * mu * (-WV(2) + 4. * WV(1) - 6. * WV(0) + 4. * WV(-1) - WV(-2));
                     }
-                } else {   // advwz_fd
-                    auto Fz = [&](int l) -> double {
-                        if (l < 1 || l >= nz) return 0.;
-                        if (l == nz - 1) return 0.25 * (AA(2, nz, 0, 0) + AA(2, nz - 1, 0, 0)) * (MM(2, nz, 0, 0) + MM(2, nz - 1, 0, 0));
-                        double ww = (AA(2, l + 1, 0, 0) + AA(2, l, 0, 0)) * 0.5;
-                        double fr = (MM(2, l + 1, 0, 0) + MM(2, l, 0, 0)) * 0.5;
-                        return ww * fr;
-                    };
-                    auto Az = [&](int l) -> double {
-                        if (l < 1 || l >= nz) return 0.;
-                        if (l == nz - 1) {
-                            double s = ZW(nz) + ZW(nz - 1);
-                            return (0. + ZW(nz - 1) * AA(2, nz - 1, 0, 0)) * (0. + ZW(nz - 1) * MM(2, nz - 1, 0, 0)) / (s * s);
-                        }
-                        double ww2 = (ZW(l + 1) * AA(2, l + 2, 0, 0) + ZW(l) * AA(2, l, 0, 0)) / (ZW(l + 1) + ZW(l));
-                        double fr2 = (ZW(l + 1) * MM(2, l + 2, 0, 0) + ZW(l) * MM(2, l, 0, 0)) / (ZW(l + 1) + ZW(l));
-                        return ww2 * fr2;
-                    };
+#undef HV
+#undef WV
+                } else if (dir == 1) {   // advwy_fd
+#define HV(p, d) AA(1, d, 0, p)
+#define WV(p) MM(2, 0, 0, p)
+                    aw = aw + c1b * (FH(0) - FH(-1)) * dy1 - c2b * (FH(1) - FH(-2)) * dy3;
+                    if (G.lavisc) {
+                        double mu = 0.25 * fabs(HV(0, 0) + HV(0, -1) + HV(1, 0) + HV(1, -1)) * dy1;
+                        aw = aw - AVISC * mu * (-WV(2) + 4. * WV(1) - 6. * WV(0) + 4. * WV(-1) - WV(-2));
+                    }
+#undef HV
+#undef WV
+#undef FH
+                } else {   // advwz_fd, Flux(k-1..k) = fzw0..1, Adv(k-2..k) = azw0..2
                     if (k >= 3 && k <= nz - 1)
-                        aw = aw + c1a * (Fz(k) - Fz(k - 1)) * Z1(k - 1) - c2a * (Az(k) - Az(k - 2)) / (ZW(k) + ZW(k - 1));
+                        aw = aw + c1a * (fzw1 - fzw0) * Z1(k - 1) - c2a * (azw2 - azw0) / (ZW(k) + ZW(k - 1));
                     else if (k == 2)
-                        aw = aw + c1a * (Fz(2) - Fz(1)) * Z1(1) - c2a * (Az(2) - 0.) / (ZW(2) + ZW(1));
+                        aw = aw + c1a * (fzw1 - fzw0) * Z1(1) - c2a * (azw2 - 0.) / (ZW(2) + ZW(1));
                     else
-                        aw = aw + (0. - Fz(nz - 1)) * Z1(nz - 1);
+                        aw = aw + (0. - fzw0) * Z1(nz - 1);
                     if (G.lavisc && k >= 3 && k <= nz - 2) {
-                        double mu = fabs(AA(2, k, 0, 0)) * Z1(k - 1);
-                        aw = aw - AVISC * mu * (-MM(2, k + 2, 0, 0) + 4. * MM(2, k + 1, 0, 0) - 6. * MM(2, k, 0, 0) + 4. * MM(2, k - 1, 0, 0) - MM(2, k - 2, 0, 0));
+                        double mu = fabs(AA(2, 0, 0, 0)) * Z1(k - 1);
+                        aw = aw - AVISC * mu * (-MM(2, 2, 0, 0) + 4. * MM(2, 1, 0, 0) - 6. * MM(2, 0, 0, 0) + 4. * MM(2, -1, 0, 0) - MM(2, -2, 0, 0));
                     }
                 }
             }
@@ -248,8 +282,9 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
         const double gpx = (ppc - ldg(A.p, gidx(G, i - 1, j, k)) / d0) * dx1;
         const double gpy = (ppc - ldg(A.p, gidx(G, i, j - 1, k)) / d0) * dy1;
         double gpz;
-        if (k >= 2) gpz = (ppc - ldg(A.p, gidx(G, i, j, k - 1)) / ldg(G.den0, k - 2)) * Z1(k - 1);
-        else gpz = MM(2, 1, 0, 0) / (dt0 * ldg(G.avden0, 0));
+        if (k >= 2) gpz = (ppc - pp_below) * Z1(k - 1);
+        else gpz = MM(2, 0, 0, 0) / (dt0 * ldg(G.avden0, 0));
+        pp_below = ppc;
         double wsu = 0. - d0 * gpx;
         double wsv = 0. - d0 * gpy;
         double wsw = 0. - a0 * gpz;

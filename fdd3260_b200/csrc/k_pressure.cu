@@ -283,7 +283,8 @@ __global__ void fft_x_inv(DevGrid G, FftPlan1 P, XInvArgs A)
 }
 
 // -------------------- step 6: correction --------------------
-__global__ void correction_kernel(DevGrid G, const double *dp, double *mu, double *mv, double *mw, double *p)
+__global__ void correction_kernel(DevGrid G, const double *dp, double *mu, double *mv, double *mw, double *p,
+                                  int natural_uv)
 {
     const int maxx = G.maxx, maxy = G.maxy;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -301,9 +302,12 @@ __global__ void correction_kernel(DevGrid G, const double *dp, double *mu, doubl
     double gpz;
     if (k >= 2) gpz = (dpc - DP(ix, jy, k - 1)) * __ldg(G.dz1 + k - 2);
     else gpz = mw[c] / (G.dt0 * __ldg(G.avden0));
-    mu[c] = mu[c] - G.dt0 * d0 * gpx;
-    mv[c] = mv[c] - G.dt0 * d0 * gpy;
+    const double mun = mu[c] - G.dt0 * d0 * gpx;
+    const double mvn = mv[c] - G.dt0 * d0 * gpy;
     mw[c] = mw[c] - G.dt0 * a0 * gpz;
+    // last correction of a step: get_velocities (funcpack.f90:328-334) fused for u, v
+    mu[c] = natural_uv ? mun / d0 : mun;
+    mv[c] = natural_uv ? mvn / d0 : mvn;
 }
 
 // -------------------- reductions --------------------
@@ -344,12 +348,26 @@ __global__ void level_sums(DevGrid G, const double *x, const double *xold, int o
     }
 }
 
-__global__ void subtract_level_mean(DevGrid G, double *x, const double *mean)
+// w -= <w>_k over all cells (cal_p1 :786-790); natural_w: then w/avden0 (get_velocities)
+__global__ void subtract_level_mean(DevGrid G, double *x, const double *mean, int natural_w)
 {
     const long long n = G.ps * G.nz;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         int k = (int)(t / G.ps) + 1;
-        x[t] = x[t] - __ldg(mean + k - 1);
+        const double v = x[t] - __ldg(mean + k - 1);
+        x[t] = natural_w ? v / __ldg(G.avden0 + k - 1) : v;
+    }
+}
+
+__global__ void to_velocity_kernel(DevGrid G, double *mu, double *mv, double *mw)
+{
+    const long long n = G.ps * G.nz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int k = (int)(t / G.ps) + 1;
+        const double d0 = __ldg(G.den0 + k - 1), a0 = __ldg(G.avden0 + k - 1);
+        mu[t] = mu[t] / d0;
+        mv[t] = mv[t] / d0;
+        mw[t] = mw[t] / a0;
     }
 }
 
@@ -670,10 +688,10 @@ cudaError_t launch_store_solution(const DevGrid &g, PressurePlan *pp, double *ou
 }
 
 cudaError_t launch_correction(const DevGrid &g, PressurePlan *pp, double *mu, double *mv, double *mw, double *p,
-                              cudaStream_t s)
+                              int natural_uv, cudaStream_t s)
 {
     long long n = (long long)g.maxx * g.maxy * g.nz;
-    correction_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, pp->dp, mu, mv, mw, p);
+    correction_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, pp->dp, mu, mv, mw, p, natural_uv);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     double *f[4] = {mu, mv, mw, p};
@@ -681,7 +699,7 @@ cudaError_t launch_correction(const DevGrid &g, PressurePlan *pp, double *mu, do
 }
 
 cudaError_t launch_cal_p1(const DevGrid &g, PressurePlan *pp, double *mw, const double *wold, int wold_rep,
-                          int want_p1, cudaStream_t s)
+                          int want_p1, int natural_w, cudaStream_t s)
 {
     level_sums<<<g.nz, 256, 0, s>>>(g, mw, wold, wold_rep, g.dt0, pp->mean, want_p1 ? pp->mean_d : nullptr);
     cudaError_t e = cudaGetLastError();
@@ -690,7 +708,13 @@ cudaError_t launch_cal_p1(const DevGrid &g, PressurePlan *pp, double *mw, const 
         p1_kernel<<<1, 32, 0, s>>>(g, pp->mean_d, pp->p1);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    subtract_level_mean<<<1184, 256, 0, s>>>(g, mw, pp->mean);
+    subtract_level_mean<<<1184, 256, 0, s>>>(g, mw, pp->mean, natural_w);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_to_velocity(const DevGrid &g, double *mu, double *mv, double *mw, cudaStream_t s)
+{
+    to_velocity_kernel<<<1184, 256, 0, s>>>(g, mu, mv, mw);
     return cudaGetLastError();
 }
 

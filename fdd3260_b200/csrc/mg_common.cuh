@@ -10,6 +10,7 @@
 // (the reference's windbc/statebc invariant, src/TOOLS/bc.f90:81-502).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
@@ -46,19 +47,22 @@ __device__ __forceinline__ double rep_value(int rep, double x, double w) {
 struct K1Args {
     int nf;                        // number of fields (field 0 = density when dens_first)
     int dens_first;                // field 0 is the density (unweighted, adv=.false.)
-    int stage;                     // 1 or 2
-    int rep;                       // representation of level-n buffers (REP_*)
+    int stage;                     // 1 or 2 (0: unit mode, inputs used as given)
     double a_dt;                   // a_lm*dt0
     double b;                      // b_lm
-    const double *xin[MG_MAXF];    // stencil input (stage 1: level-n buffer; stage 2: working)
-    const double *xold[MG_MAXF];   // level-n buffer (pointwise)
-    double *xout[MG_MAXF];         // new working value
-    double *tend[MG_MAXF];         // tendency accumulator (in/out)
+    const double *xin[MG_MAXF];    // stencil input (stage 1: level-n natural; stage 2: working)
+    double *xold[MG_MAXF];         // level-n natural buffer (pointwise; stage 2 writes it in place)
+    double *xout[MG_MAXF];         // stage 1: working buffers; stage 2: the level-n buffers
+    double *tend[MG_MAXF];         // tendency accumulator (stage 1 writes, stage 2 reads)
     double *fst[MG_MAXF];          // optional: this stage's tendency (for buoyancy), or null
-    const double *dens_n;          // level-n density (weights)
-    const double *mu, *mv, *mw;    // momentum for the advective velocity
-    int mom_rep;                   // -1: momentum buffers are working values; else REP_* level-n
-    int mode;                      // 0: stage update; 1: unit mode: xout := xout - T (advection_ac)
+    const double *mw;              // momentum w (stage 1: natural w) for the vertical face velocity
+    int mode;                      // 0: stage update; 1: unit mode: xout := ((xout - Tx) - Ty) - Tz
+    int *err;                      // device error flag (bounded waits)
+};
+// TMA descriptors of the K1 inputs: haloed planes (38 x 14) of every field, momentum boxes (34 x 9)
+struct alignas(64) K1Maps {
+    CUtensorMap x[MG_MAXF];
+    CUtensorMap mu, mv;
 };
 
 // ---- momentum advection + pgf + buoyancy + stage update (K2) ----
@@ -80,7 +84,11 @@ struct K2Args {
 };
 
 // launch wrappers (implemented in the .cu files)
-cudaError_t launch_k1(const DevGrid &g, const K1Args &a, cudaStream_t s);
+cudaError_t launch_k1(const DevGrid &g, const K1Args &a, const K1Maps &maps, cudaStream_t s);
+cudaError_t k1_init();
+size_t k1_smem_bytes(int scheme, int nf);
+// TMA descriptor of one field buffer (box in doubles)
+int make_field_map(const DevGrid &g, const double *base, int boxx, int boxy, CUtensorMap *map);
 cudaError_t launch_k2(const DevGrid &g, const K2Args &a, cudaStream_t s);
 cudaError_t launch_halo_fill(const DevGrid &g, double *const *fields, int nf, cudaStream_t s);
 
@@ -102,10 +110,12 @@ cudaError_t pressure_solve(const DevGrid &g, PressurePlan *pp, double scale, int
 cudaError_t launch_store_solution(const DevGrid &g, PressurePlan *pp, double *out, cudaStream_t s);
 // correction: p += rho0*dp; m -= dt0*rho0*grad(dp); ghost cells refreshed
 cudaError_t launch_correction(const DevGrid &g, PressurePlan *pp, double *mu, double *mv, double *mw,
-                              double *p, cudaStream_t s);
+                              double *p, int natural_uv, cudaStream_t s);
 // cal_p1 (+ optional p1), residual max of div
 cudaError_t launch_cal_p1(const DevGrid &g, PressurePlan *pp, double *mw, const double *wold, int wold_rep,
-                          int want_p1, cudaStream_t s);
+                          int want_p1, int natural_w, cudaStream_t s);
+// momentum -> natural velocities over all cells (get_velocities, funcpack.f90:265-344)
+cudaError_t launch_to_velocity(const DevGrid &g, double *mu, double *mv, double *mw, cudaStream_t s);
 cudaError_t launch_maxdiv(const DevGrid &g, PressurePlan *pp, const double *mu, const double *mv,
                           const double *mw, cudaStream_t s);
 // results of the last cal_p1 / maxdiv (device pointers inside the plan)

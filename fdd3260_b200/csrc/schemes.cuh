@@ -13,6 +13,34 @@ __device__ __forceinline__ float dabs(float a) { return fabsf(a); }
 __device__ __forceinline__ double sign1(double b) { return copysign(1.0, b); }
 __device__ __forceinline__ float sign1(float b) { return copysignf(1.0f, b); }
 
+// RN(a/b) > thr for b > 0, decided without the division when a lies clearly on one
+// side of thr*b (a relative band of 1e-7 around thr); bit-identical to the division.
+template <typename T> __device__ __forceinline__ bool ratio_gt(T a, T b, T thr);
+template <> __device__ __forceinline__ bool ratio_gt<double>(double a, double b, double thr)
+{
+    if (a > b * (thr * 1.0000001)) return true;
+    if (a < b * (thr * 0.9999999)) return false;
+    return a / b > thr;
+}
+template <> __device__ __forceinline__ bool ratio_gt<float>(float a, float b, float thr) { return a > thr * b; }
+
+// min(|num/den|, 1) of the positivity limiters: 1 exactly whenever |num| >= |den|
+// (then |num/den| >= 1 and its rounding too, or the quotient is inf/NaN and min()
+// returns 1), so the division is only evaluated when it can matter.
+template <typename T> __device__ __forceinline__ T min_abs_ratio_1(T num, T den);
+template <> __device__ __forceinline__ double min_abs_ratio_1<double>(double num, double den)
+{
+    if (fabs(num) >= fabs(den)) return 1.;
+    const double q = fabs(num / den);
+    return q < 1. ? q : 1.;
+}
+template <> __device__ __forceinline__ float min_abs_ratio_1<float>(float num, float den)
+{
+    if (fabsf(num) >= fabsf(den)) return 1.f;
+    const float q = fabsf(num / den);
+    return q < 1.f ? q : 1.f;
+}
+
 // ---------------- WENO3-switch: src/TOOLS/advq_weno.f90 ----------------
 // weights of one face, :304-353 (loop body); linear weights unless the smoothness
 // ratio exceeds 20.  (eps+eta)**2 is the correctly rounded product.
@@ -23,13 +51,13 @@ __device__ __forceinline__ void weno_weights(T xm1, T x0, T xp1, T xp2, T &w0, T
     T d1 = x0 - xm1, d2 = xp1 - x0, d3 = xp2 - xp1;
     T eta1 = d1 * d1, eta2 = d2 * d2, eta3 = d3 * d3;
     w0 = g1; w1 = g2; w2 = g2; w3 = g1;
-    if (tmax(eta1, eta2) / (tmin(eta1, eta2) + eps) > thres) {
+    if (ratio_gt(tmax(eta1, eta2), tmin(eta1, eta2) + eps, thres)) {
         T y1 = eps + eta1, y2 = eps + eta2;
         T a = g1 / (y1 * y1), b = g2 / (y2 * y2);
         T s = a + b;
         w0 = a / s; w1 = b / s;
     }
-    if (tmax(eta2, eta3) / (tmin(eta2, eta3) + eps) > thres) {
+    if (ratio_gt(tmax(eta2, eta3), tmin(eta2, eta3) + eps, thres)) {
         T y2 = eps + eta2, y3 = eps + eta3;
         T a = g2 / (y2 * y2), b = g1 / (y3 * y3);
         T s = a + b;
@@ -49,7 +77,7 @@ __device__ __forceinline__ T weno_face(T xm1, T x0, T xp1, T xp2, T uu, bool ful
     T ffip1m = ffip1p;
     T ffip2 = (T(1.5) * xp1 - T(0.5) * xp2);
     T minp = tmin(tmin(tmin(ffim1, ffip1m), ffip1p), ffip2);
-    T phi = tmin(dabs((T(0.) - x0) / ((minp - x0) + eps)), T(1.));
+    T phi = min_abs_ratio_1(T(0.) - x0, (minp - x0) + eps);
     ffim1 = phi * (ffim1 - x0) + x0;
     ffip1m = phi * (ffip1m - x0) + x0;
     ffip1p = phi * (ffip1p - x0) + x0;
@@ -206,10 +234,10 @@ __device__ __forceinline__ void ppm_limiter(T xx, T xp, T xm, T xplus, T xmin, T
     T gamma2 = T(0.5) * (a * a + b * b);
     a = ffim1 - ffim2; b = ffim1 + ffim2;
     T gamma3 = T(0.5) * (a * a + b * b);
-    T lambda = tmax(tmax(gamma1, gamma2), gamma3) / (tmin(tmin(gamma1, gamma2), gamma3) + eps);
+    const bool sel = ratio_gt(tmax(tmax(gamma1, gamma2), gamma3), tmin(tmin(gamma1, gamma2), gamma3) + eps, thres);
     phi1 = phir - phil;
     phi2 = T(3.) * (phil - T(2.) * xx + phir);
-    if (lambda > thres) {
+    if (sel) {
         if (phir < T(0.) || ((phir - xx) * (xp - phir) < T(0.) &&
                              (ffim1 * ffip2 >= T(0.) || ffim1 * ffip1 <= T(0.) || ffip2 * ffip1 <= T(0.)))) {
             if (dabs(phir - xx) < dabs(phir - xp)) phir = xx;
