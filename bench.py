@@ -195,6 +195,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"],
+                    help="fp64: plain FP64 form; mixed: FP32 stencils/fluxes with FP64 state and accumulation")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -202,13 +204,17 @@ def main():
     ws, rank, local = dist_init()
     from fdd3260_b200 import Mimica, config
     d = config.cumulus_domain(args.maxx, args.maxx, args.nz, scheme=args.scheme)
+    if args.form == "mixed":
+        from fdd3260_b200 import _lib
+        d.precision = _lib.MG_PREC_MIXED
     metric = "Mcell-updates/s per integrator step (2-stage Heun + projection)"
     cfg = {"workload": f"shallow-cumulus domain {args.maxx}x{args.maxx}x{args.nz}, dx=dy=25 m, stretched dz 10->100 m, "
                        f"3 momentum + density + 5 scalars, {args.scheme.upper()} (reference scheme), FD4 momentum, "
                        f"dt=1 s, nsubp=1",
            "fields": "theta_l 298->310 K, qt 17->4 g/kg, qr/nr/aerosol smooth decreasing profiles; "
                      "seeded Gaussian perturbations below 500 m; u=-8+N(0,0.5), v=N(0,0.5) m/s",
-           "form": "plain FP64", "scheme": args.scheme, "interior_cells": d.cells,
+           "form": "plain FP64" if args.form == "fp64" else "mixed (FP32 stencils and fluxes, FP64 state)",
+           "scheme": args.scheme, "interior_cells": d.cells,
            "l2": "inputs larger than L2 (~16 GB working set)", "parallelism": f"replicas x{ws}"}
 
     if args.impl == "reference":

@@ -31,8 +31,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # (source, extra flags)
 SOURCES = [
     ("k_scalar.cu", ["-fmad=false"]),
-    ("k_scalar_mixed.cu", []),
+    ("k_scalar_mixed.cu", ["-use_fast_math"]),
     ("k_momentum.cu", ["-fmad=false"]),
+    ("k_momentum_mixed.cu", []),
     ("k_pressure.cu", ["-fmad=false"]),
     ("k_pressure_mixed.cu", []),
     ("capi.cu", []),

@@ -205,7 +205,7 @@ static int validate(const mg_params *p)
     if (p->muscl_limiter < MG_LIM_MINMOD || p->muscl_limiter > MG_LIM_DEFAULT) return MG_ERR_PARAM;
     if (p->mom_ord != 2 && p->mom_ord != 4) return MG_ERR_PARAM;
     if (p->nsubp < 1 || p->nsubp > 16) return MG_ERR_PARAM;
-    if (p->precision != MG_PREC_FP64) return MG_ERR_PARAM;   // the mixed form is not built yet
+    if (p->precision != MG_PREC_FP64 && p->precision != MG_PREC_MIXED) return MG_ERR_PARAM;
     if (!(p->dx > 0) || !(p->dy > 0) || !(p->dz > 0) || !(p->dt0 > 0)) return MG_ERR_PARAM;
     if (!p->fdz0 || !p->dzw || !p->dz1w || !p->dz1 || !p->den0 || !p->avden0 || !p->stab0 || !p->pt0 || !p->qv0)
         return MG_ERR_PARAM;
@@ -291,6 +291,7 @@ extern "C" int mg_create(const mg_params *params, int device, mg_ctx **out)
     e = cudaMalloc(&c->derr, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(c->derr, 0, sizeof(int));
     if (e == cudaSuccess) e = k1_init();
+    if (e == cudaSuccess) e = k1_mixed_init();
     if (e != cudaSuccess) return fail(cuerr(e));
     if (build_maps(c, c->sA, c->nf, c->mA[0], c->mA[1], &c->maps1) ||
         build_maps(c, c->sB, c->nf, c->mB[0], c->mB[1], &c->maps2))
@@ -453,7 +454,10 @@ static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int wa
         }
         const double *const *mom = stage == 1 ? c->mA : c->mB;
         a1.mw = mom[2];
-        PROF(c, "k1_scalar_advection", launch_k1(G, a1, stage == 1 ? c->maps1 : c->maps2, c->stream));
+        if (P.precision == MG_PREC_MIXED)
+            PROF(c, "k1_scalar_advection", launch_k1_mixed(G, a1, stage == 1 ? c->maps1 : c->maps2, c->stream));
+        else
+            PROF(c, "k1_scalar_advection", launch_k1(G, a1, stage == 1 ? c->maps1 : c->maps2, c->stream));
         {
             std::vector<double *> f;
             for (int q = 0; q < nf; q++) f.push_back(a1.xout[q]);
@@ -477,7 +481,10 @@ static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int wa
         a2.ou = mo[0]; a2.ov = mo[1]; a2.ow = mo[2];
         a2.tu = c->tm[0]; a2.tv = c->tm[1]; a2.tw = c->tm[2];
         a2.mode = 0;
-        PROF(c, "k2_momentum", launch_k2(G, a2, c->stream));
+        if (P.precision == MG_PREC_MIXED)
+            PROF(c, "k2_momentum", launch_k2_mixed(G, a2, c->stream));
+        else
+            PROF(c, "k2_momentum", launch_k2(G, a2, c->stream));
         PROF(c, "halo_momentum", launch_halo_fill(G, mo, 3, c->stream));
         *launches += 4;
         // ---- projection ----

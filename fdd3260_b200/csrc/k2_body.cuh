@@ -1,0 +1,340 @@
+// k2_body.cuh -- body of the K2 kernel (momentum tendency + stage update), templated
+// on the arithmetic form; instantiated by k_momentum.cu (plain FP64, no FMA
+// contraction: bit-identical to the CPU restatement) and k_momentum_mixed.cu (FP32
+// stencils and fluxes, FP64 accumulation, pressure gradient, buoyancy and state).
+#pragma once
+#include <type_traits>
+#include "mg_common.cuh"
+#include "mimica_gpu.h"
+
+namespace {
+
+constexpr int TX = 32, TY = 8, RH = 2;
+constexpr int PW = TX + 2 * RH, PH = TY + 2 * RH, PL = PW * PH;
+constexpr int NSLOT = 5;
+constexpr double AVISC = 1. / 16.;   // windadv.f90:39
+
+__device__ __forceinline__ double ldg(const double *p, long long i) { return __ldg(p + i); }
+__device__ __forceinline__ double abs_r(double x) { return fabs(x); }
+__device__ __forceinline__ float abs_r(float x) { return fabsf(x); }
+
+template <bool MIXED>
+__global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
+{
+    // R: type of the stencil arithmetic (FP64 plain form, FP32 mixed form)
+    using R = typename std::conditional<MIXED, float, double>::type;
+    extern __shared__ double sm_raw[];
+    R *sm = reinterpret_cast<R *>(sm_raw);
+    R *ring_m = sm;                            // [slot][3][PL] momentum (stencil values)
+    R *ring_a = sm + NSLOT * 3 * PL;           // [slot][3][PL] advective velocity
+
+    const int ntx = (G.maxx + TX - 1) / TX;
+    const int ti = blockIdx.x % ntx, tj = blockIdx.x / ntx;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const int i0 = 4 + ti * TX, j0 = 4 + tj * TY;
+    const int i = i0 + tx, j = j0 + ty;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const bool act = (i <= nx - 2) && (j <= ny - 2);
+    const double dx1d = 1. / G.dx, dy1d = 1. / G.dy, dt0 = G.dt0;
+    const R dx1 = (R)dx1d, dy1 = (R)dy1d;
+    const R dx2 = (R)(1. / (2. * G.dx)), dy2 = (R)(1. / (2. * G.dy));
+    const R dx3 = (R)(1. / (3. * G.dx)), dy3 = (R)(1. / (3. * G.dy));
+    R c1a, c2a, c1b, c2b;   // a: 4/3,1/3 (self-advection); b: 9/8,1/8 (cross terms)
+    if (G.mom_ord == 4) { c1a = (R)(4. / 3.); c2a = (R)(1. / 3.); c1b = (R)(9. / 8.); c2b = (R)(1. / 8.); }
+    else { c1a = 1; c2a = 0; c1b = 1; c2b = 0; }
+    const R AVR = (R)AVISC, HALF = (R)0.5, QUART = (R)0.25, FOUR = (R)4., SIX = (R)6.;
+    const double *dzw = G.dzw, *dz1w = G.dz1w, *dz1 = G.dz1;
+
+    auto load_level = [&](int l) {
+        const int slot = l % NSLOT;
+        const double d0 = ldg(G.den0, l - 1), a0 = ldg(G.avden0, l - 1);
+        for (int q = tid; q < 3 * PL; q += TX * TY) {
+            int arr = q / PL, o = q - arr * PL;
+            int r = o / PW, c = o - r * PW;
+            int ii = i0 - RH + c, jj = j0 - RH + r;
+            double mv = 0., av = 0.;
+            if (ii >= 1 && ii <= nx && jj >= 1 && jj <= ny) {
+                long long idx = gidx(G, ii, jj, l);
+                const double *src = arr == 0 ? A.mu : (arr == 1 ? A.mv : A.mw);
+                double w = arr == 2 ? a0 : d0;
+                double x = ldg(src, idx);
+                mv = A.in_is_leveln ? rep_value(A.rep, x, w) : x;
+                av = mv / w;
+                if (arr == 0) av = av - G.u0shift;
+                else if (arr == 1) av = av - G.v0shift;
+            }
+            ring_m[(slot * 3 + arr) * PL + o] = (R)mv;
+            ring_a[(slot * 3 + arr) * PL + o] = (R)av;
+        }
+    };
+    // Per level k: lb[d+2] = this thread's element of ring slot (k+d) mod 5, d = -2..2.
+    // MM/AA(c, d, di, dj): momentum / advective velocity of component c (0 u, 1 v, 2 w)
+    // at (i+di, j+dj, k+d); d, di, dj are compile-time constants at every use.
+    const R *lb[5];
+#define MM(c, d, di, dj) lb[(d) + 2][(c) * PL + (dj) * PW + (di)]
+#define AA(c, d, di, dj) lb[(d) + 2][NSLOT * 3 * PL + (c) * PL + (dj) * PW + (di)]
+#define ZW(l) ((R)ldg(dzw, (l) - 1))
+#define ZW1(l) ((R)ldg(dz1w, (l) - 1))
+#define Z1(l) ((R)ldg(dz1, (l) - 1))
+// accumulation of one direction's contribution: (acc + a) - b in the plain form (the
+// reference's order), acc + (a - b) evaluated in R and added in FP64 in the mixed form
+#define ACC2(acc, a, b) do { if constexpr (MIXED) acc = acc + (double)((a) - (b)); else acc = acc + (a) - (b); } while (0)
+#define ACC1(acc, a) do { acc = acc + (a); } while (0)
+#define SUB1(acc, a) do { acc = acc - (a); } while (0)
+
+    load_level(1);
+    if (nz >= 2) load_level(2);
+
+    double bb_prev = 0.;   // buoyancy at level k-1 (cell centre)
+    // vertical fluxes carried up the column (each computed once):
+    //   fzu/fzv[m] = Flux(k-2+m) of advuz/advvz, m = 0..3;  fzw[m] = Flux(k-1+m) and
+    //   azw[m] = Adv(k-2+m) of advwz;  pp_below = p(k-1)/rho0(k-1)
+    R fzu0 = 0, fzu1 = 0, fzu2 = 0, fzu3 = 0, fzv0 = 0, fzv1 = 0, fzv2 = 0, fzv3 = 0;
+    R fzw0 = 0, fzw1 = 0, azw0 = 0, azw1 = 0, azw2 = 0;
+    double pp_below = 0.;
+    const bool even = (A.ntime % 2) == 0;
+    const double grav = 9.81, epsm = 0.60243, cdiag = 0.5;
+    const int own = (ty + RH) * PW + (tx + RH);
+
+    for (int k = 1; k <= nz; k++) {
+        __syncthreads();
+        if (k + 2 <= nz) load_level(k + 2);
+        __syncthreads();
+        if (!act) continue;   // no further barriers in this iteration
+#pragma unroll
+        for (int d = -2; d <= 2; d++) lb[d + 2] = ring_m + (((k + d + NSLOT) % NSLOT) * 3) * PL + own;
+
+        // ---- advance the carried vertical fluxes ----
+        {
+            // advuz_fd/advvz_fd Flux(k+1) (windadv.f90:656-663): levels k+1, k+2; Flux(nz) = 0
+            R fu = 0, fv = 0;
+            if (k + 1 <= nz - 1) {
+                const R zp = ZW(k + 2), zc = ZW(k + 1), zs = zp + zc;
+                R ww = c1b * (AA(2, 2, -1, 0) + AA(2, 2, 0, 0)) * HALF - c2b * (AA(2, 2, -2, 0) + AA(2, 2, 1, 0)) * HALF;
+                R fr = (zp * MM(0, 2, 0, 0) + zc * MM(0, 1, 0, 0)) / zs;
+                fu = ww * fr;
+                ww = c1b * (AA(2, 2, 0, -1) + AA(2, 2, 0, 0)) * HALF - c2b * (AA(2, 2, 0, -2) + AA(2, 2, 0, 1)) * HALF;
+                fr = (zp * MM(1, 2, 0, 0) + zc * MM(1, 1, 0, 0)) / zs;
+                fv = ww * fr;
+            }
+            if (k == 1) {   // Flux(1): levels 1, 2
+                const R zp = ZW(2), zc = ZW(1), zs = zp + zc;
+                R ww = c1b * (AA(2, 1, -1, 0) + AA(2, 1, 0, 0)) * HALF - c2b * (AA(2, 1, -2, 0) + AA(2, 1, 1, 0)) * HALF;
+                R fr = (zp * MM(0, 1, 0, 0) + zc * MM(0, 0, 0, 0)) / zs;
+                fzu3 = ww * fr;
+                ww = c1b * (AA(2, 1, 0, -1) + AA(2, 1, 0, 0)) * HALF - c2b * (AA(2, 1, 0, -2) + AA(2, 1, 0, 1)) * HALF;
+                fr = (zp * MM(1, 1, 0, 0) + zc * MM(1, 0, 0, 0)) / zs;
+                fzv3 = ww * fr;
+            }
+            fzu0 = fzu1; fzu1 = fzu2; fzu2 = fzu3; fzu3 = fu;
+            fzv0 = fzv1; fzv1 = fzv2; fzv2 = fzv3; fzv3 = fv;
+            // advwz_fd Flux(k), Adv(k) (:1087-1098)
+            R fw = 0, aw_ = 0;
+            if (k <= nz - 2) {
+                R ww = (AA(2, 1, 0, 0) + AA(2, 0, 0, 0)) * HALF;
+                R fr = (MM(2, 1, 0, 0) + MM(2, 0, 0, 0)) * HALF;
+                fw = ww * fr;
+                const R zp = ZW(k + 1), zc = ZW(k), zs = zp + zc;
+                R ww2 = (zp * AA(2, 2, 0, 0) + zc * AA(2, 0, 0, 0)) / zs;
+                R fr2 = (zp * MM(2, 2, 0, 0) + zc * MM(2, 0, 0, 0)) / zs;
+                aw_ = ww2 * fr2;
+            } else if (k == nz - 1) {
+                fw = QUART * (AA(2, 1, 0, 0) + AA(2, 0, 0, 0)) * (MM(2, 1, 0, 0) + MM(2, 0, 0, 0));
+                const R s2 = ZW(nz) + ZW(nz - 1);
+                aw_ = ((R)0 + ZW(nz - 1) * AA(2, 0, 0, 0)) * ((R)0 + ZW(nz - 1) * MM(2, 0, 0, 0)) / (s2 * s2);
+            }
+            fzw0 = fzw1; fzw1 = fw;
+            azw0 = azw1; azw1 = azw2; azw2 = aw_;
+        }
+
+        // ---------------- u component ----------------
+        double au = 0.;
+        for (int pass = 0; pass < 3; pass++) {
+            int dir = even ? pass : 2 - pass;
+            if (dir == 0) {   // advux_fd
+#define FX(p) (((AA(0, 0, (p) + 1, 0) + AA(0, 0, (p), 0)) * HALF) * ((MM(0, 0, (p) + 1, 0) + MM(0, 0, (p), 0)) * HALF))
+#define AX(p) (((AA(0, 0, (p) + 2, 0) + AA(0, 0, (p), 0)) * HALF) * ((MM(0, 0, (p) + 2, 0) + MM(0, 0, (p), 0)) * HALF))
+                ACC2(au, c1a * (FX(0) - FX(-1)) * dx1, c2a * (AX(0) - AX(-2)) * dx2);
+#undef FX
+#undef AX
+                if (G.lavisc) {
+                    const R mu = abs_r(AA(0, 0, 0, 0)) * dx1;
+                    SUB1(au, AVR * mu * (-MM(0, 0, 2, 0) + FOUR * MM(0, 0, 1, 0) - SIX * MM(0, 0, 0, 0) + FOUR * MM(0, 0, -1, 0) - MM(0, 0, -2, 0)));
+                }
+            } else if (dir == 1) {   // advuy_fd: vt1=vt(i-1), vt2=vt(i), vt3=vt(i-2), vt4=vt(i+1)
+#define FY(p) ((c1b * (AA(1, 0, -1, (p) + 1) + AA(1, 0, 0, (p) + 1)) * HALF - c2b * (AA(1, 0, -2, (p) + 1) + AA(1, 0, 1, (p) + 1)) * HALF) * \
+               ((MM(0, 0, 0, (p) + 1) + MM(0, 0, 0, (p))) * HALF))
+                ACC2(au, c1b * (FY(0) - FY(-1)) * dy1, c2b * (FY(1) - FY(-2)) * dy3);
+#undef FY
+                if (G.lavisc) {
+                    const R mu = QUART * abs_r(AA(1, 0, -1, 0) + AA(1, 0, 0, 0) + AA(1, 0, -1, 1) + AA(1, 0, 0, 1)) * dy1;
+                    SUB1(au, AVR * mu * (-MM(0, 0, 0, 2) + FOUR * MM(0, 0, 0, 1) - SIX * MM(0, 0, 0, 0) + FOUR * MM(0, 0, 0, -1) - MM(0, 0, 0, -2)));
+                }
+            } else {   // advuz_fd, Flux(k-2..k+1) = fzu0..fzu3
+                if (k >= 3 && k <= nz - 1)
+                    ACC2(au, c1b * (fzu2 - fzu1) * ZW1(k), c2b * (fzu3 - fzu0) / (ZW(k - 1) + ZW(k) + ZW(k + 1)));
+                else if (k == 1)
+                    ACC1(au, (fzu2 - (R)0) * ZW1(1));
+                else if (k == 2)
+                    ACC2(au, c1b * (fzu2 - fzu1) * ZW1(1), c2b * (fzu3 - (R)0) / (ZW(1) + ZW(2) + ZW(3)));
+                else
+                    ACC1(au, ((R)0 - fzu1) * ZW1(nz));
+                if (G.lavisc && k >= 3 && k <= nz - 2) {
+                    const R mu = QUART * abs_r(AA(2, 0, -1, 0) + AA(2, 0, 0, 0) + AA(2, 1, -1, 0) + AA(2, 1, 0, 0)) * ZW1(k);
+                    SUB1(au, AVR * mu * (-MM(0, 2, 0, 0) + FOUR * MM(0, 1, 0, 0) - SIX * MM(0, 0, 0, 0) + FOUR * MM(0, -1, 0, 0) - MM(0, -2, 0, 0)));
+                }
+            }
+        }
+
+        // ---------------- v component ----------------
+        double av = 0.;
+        for (int pass = 0; pass < 3; pass++) {
+            int dir = even ? pass : 2 - pass;
+            if (dir == 0) {   // advvx_fd: ut1=ut(j-1), ut2=ut(j), ut3=ut(j-2), ut4=ut(j+1)
+#define FX(p) ((c1b * (AA(0, 0, (p) + 1, -1) + AA(0, 0, (p) + 1, 0)) * HALF - c2b * (AA(0, 0, (p) + 1, -2) + AA(0, 0, (p) + 1, 1)) * HALF) * \
+               ((MM(1, 0, (p) + 1, 0) + MM(1, 0, (p), 0)) * HALF))
+                ACC2(av, c1b * (FX(0) - FX(-1)) * dx1, c2b * (FX(1) - FX(-2)) * dx3);
+#undef FX
+                if (G.lavisc) {
+                    const R mu = QUART * abs_r(AA(0, 0, 0, -1) + AA(0, 0, 0, 0) + AA(0, 0, 1, -1) + AA(0, 0, 1, 0)) * dx1;
+                    SUB1(av, AVR * mu * (-MM(1, 0, 2, 0) + FOUR * MM(1, 0, 1, 0) - SIX * MM(1, 0, 0, 0) + FOUR * MM(1, 0, -1, 0) - MM(1, 0, -2, 0)));
+                }
+            } else if (dir == 1) {   // advvy_fd
+#define FY(p) (((AA(1, 0, 0, (p) + 1) + AA(1, 0, 0, (p))) * HALF) * ((MM(1, 0, 0, (p) + 1) + MM(1, 0, 0, (p))) * HALF))
+#define AY(p) (((AA(1, 0, 0, (p) + 2) + AA(1, 0, 0, (p))) * HALF) * ((MM(1, 0, 0, (p) + 2) + MM(1, 0, 0, (p))) * HALF))
+                ACC2(av, c1a * (FY(0) - FY(-1)) * dy1, c2a * (AY(0) - AY(-2)) * dy2);
+#undef FY
+#undef AY
+                if (G.lavisc) {
+                    const R mu = abs_r(AA(1, 0, 0, 0)) * dy1;
+                    SUB1(av, AVR * mu * (-MM(1, 0, 0, 2) + FOUR * MM(1, 0, 0, 1) - SIX * MM(1, 0, 0, 0) + FOUR * MM(1, 0, 0, -1) - MM(1, 0, 0, -2)));
+                }
+            } else {   // advvz_fd, Flux(k-2..k+1) = fzv0..fzv3
+                if (k >= 3 && k <= nz - 1)
+                    ACC2(av, c1b * (fzv2 - fzv1) * ZW1(k), c2b * (fzv3 - fzv0) / (ZW(k - 1) + ZW(k) + ZW(k + 1)));
+                else if (k == 1)
+                    ACC1(av, (fzv2 - (R)0) * ZW1(1));
+                else if (k == 2)
+                    ACC2(av, c1b * (fzv2 - fzv1) * ZW1(2), c2b * (fzv3 - (R)0) / (ZW(1) + ZW(2) + ZW(3)));
+                else
+                    ACC1(av, ((R)0 - fzv1) * ZW1(nz));
+                if (G.lavisc && k >= 3 && k <= nz - 2) {
+                    const R mu = QUART * abs_r(AA(2, 0, 0, -1) + AA(2, 0, 0, 0) + AA(2, 1, 0, -1) + AA(2, 1, 0, 0)) * ZW1(k);
+                    SUB1(av, AVR * mu * (-MM(1, 2, 0, 0) + FOUR * MM(1, 1, 0, 0) - SIX * MM(1, 0, 0, 0) + FOUR * MM(1, -1, 0, 0) - MM(1, -2, 0, 0)));
+                }
+            }
+        }
+
+        // ---------------- w component (k >= 2) ----------------
+        double aw = 0.;
+        if (k >= 2) {
+            for (int pass = 0; pass < 3; pass++) {
+                int dir = even ? pass : 2 - pass;
+                if (dir == 0) {   // advwx_fd
+#define HV(p, d) AA(0, d, p, 0)
+#define WV(p) MM(2, 0, p, 0)
+#define FH(p) ((k == 2 ? (HV((p) + 1, 0) + HV((p) + 1, -1)) * HALF                                            \
+                       : (k == nz ? (HV((p) + 1, 0) + HV((p) + 1, -1)) * HALF                                  \
+                                  : c1b * (HV((p) + 1, 0) + HV((p) + 1, -1)) * HALF -                          \
+                                        c2b * (HV((p) + 1, 1) + HV((p) + 1, -2)) * HALF)) *                    \
+                ((WV((p) + 1) + WV(p)) * HALF))
+                    ACC2(aw, c1b * (FH(0) - FH(-1)) * dx1, c2b * (FH(1) - FH(-2)) * dx3);
+                    if (G.lavisc) {
+                        const R mu = QUART * abs_r(HV(0, 0) + HV(0, -1) + HV(1, 0) + HV(1, -1)) * dx1;
+                        SUB1(aw, AVR * mu * (-WV(2) + FOUR * WV(1) - SIX * WV(0) + FOUR * WV(-1) - WV(-2)));
+                    }
+#undef HV
+#undef WV
+                } else if (dir == 1) {   // advwy_fd
+#define HV(p, d) AA(1, d, 0, p)
+#define WV(p) MM(2, 0, 0, p)
+                    ACC2(aw, c1b * (FH(0) - FH(-1)) * dy1, c2b * (FH(1) - FH(-2)) * dy3);
+                    if (G.lavisc) {
+                        const R mu = QUART * abs_r(HV(0, 0) + HV(0, -1) + HV(1, 0) + HV(1, -1)) * dy1;
+                        SUB1(aw, AVR * mu * (-WV(2) + FOUR * WV(1) - SIX * WV(0) + FOUR * WV(-1) - WV(-2)));
+                    }
+#undef HV
+#undef WV
+#undef FH
+                } else {   // advwz_fd, Flux(k-1..k) = fzw0..1, Adv(k-2..k) = azw0..2
+                    if (k >= 3 && k <= nz - 1)
+                        ACC2(aw, c1a * (fzw1 - fzw0) * Z1(k - 1), c2a * (azw2 - azw0) / (ZW(k) + ZW(k - 1)));
+                    else if (k == 2)
+                        ACC2(aw, c1a * (fzw1 - fzw0) * Z1(1), c2a * (azw2 - (R)0) / (ZW(2) + ZW(1)));
+                    else
+                        ACC1(aw, ((R)0 - fzw0) * Z1(nz - 1));
+                    if (G.lavisc && k >= 3 && k <= nz - 2) {
+                        const R mu = abs_r(AA(2, 0, 0, 0)) * Z1(k - 1);
+                        SUB1(aw, AVR * mu * (-MM(2, 2, 0, 0) + FOUR * MM(2, 1, 0, 0) - SIX * MM(2, 0, 0, 0) + FOUR * MM(2, -1, 0, 0) - MM(2, -2, 0, 0)));
+                    }
+                }
+            }
+        }
+
+        const long long idx = gidx(G, i, j, k);
+        if (A.mode == 1) {
+            A.ou[idx] = au;
+            A.ov[idx] = av;
+            A.ow[idx] = aw;
+            continue;
+        }
+
+        // ---------------- explicit pressure gradient (gradp on p/rho0) ----------------
+        const double d0 = ldg(G.den0, k - 1), a0 = ldg(G.avden0, k - 1);
+        const double ppc = ldg(A.p, idx) / d0;
+        const double gpx = (ppc - ldg(A.p, gidx(G, i - 1, j, k)) / d0) * dx1d;
+        const double gpy = (ppc - ldg(A.p, gidx(G, i, j - 1, k)) / d0) * dy1d;
+        double gpz;
+        if (k >= 2) gpz = (ppc - pp_below) * ldg(dz1, k - 2);
+        else gpz = (double)MM(2, 0, 0, 0) / (dt0 * ldg(G.avden0, 0));
+        pp_below = ppc;
+        double wsu = 0. - d0 * gpx;
+        double wsv = 0. - d0 * gpy;
+        double wsw = 0. - a0 * gpz;
+
+        // ---------------- buoyancy (imp_buoy: state + cdiag*dt0*states) ----------------
+        double buoy = 0.;
+        if (G.with_buoy) {
+            double dn = ldg(A.dens, idx);
+            double esv = ldg(A.es, idx), qtv = A.qt ? ldg(A.qt, idx) : 0.;
+            if (A.dens_is_leveln) {
+                esv = rep_value(A.rep, esv, dn);
+                if (A.qt) qtv = rep_value(A.rep, qtv, dn);
+            }
+            double est = esv + cdiag * dt0 * ldg(A.fes, idx);
+            double qtt = A.qt ? qtv + cdiag * dt0 * ldg(A.fqt, idx) : 0.;
+            double den1 = 1. / dn;
+            double pt = den1 * est;
+            double sumh = 0.;
+            double ref = ldg(G.pt0, k - 1) * (1. + epsm * ldg(G.qv0, k - 1));
+            double bb = dn * grav * (pt * (1. + epsm * den1 * (qtt - sumh) - den1 * sumh) / ref - 1.);
+            buoy = k >= 2 ? 0.5 * (bb_prev + bb) : bb;
+            bb_prev = bb;
+        }
+
+        // ---------------- assembly and integ_mom ----------------
+        wsu = -au + wsu;
+        wsv = -av + wsv;
+        wsw = -aw + wsw + buoy;
+        double tu_o = A.stage == 1 ? 0. : A.tu[idx];
+        double tv_o = A.stage == 1 ? 0. : A.tv[idx];
+        double tw_o = A.stage == 1 ? 0. : A.tw[idx];
+        double tu = wsu + A.b * tu_o, tv = wsv + A.b * tv_o, tw = wsw + A.b * tw_o;
+        double un = rep_value(A.rep, ldg(A.mu_n, idx), d0);
+        double vn = rep_value(A.rep, ldg(A.mv_n, idx), d0);
+        double wn = rep_value(A.rep, ldg(A.mw_n, idx), a0);
+        A.ou[idx] = un + A.a_dt * tu;
+        A.ov[idx] = vn + A.a_dt * tv;
+        A.ow[idx] = 1. * (wn + A.a_dt * tw);
+        A.tu[idx] = tu;
+        A.tv[idx] = tv;
+        A.tw[idx] = tw;
+    }
+#undef MM
+#undef AA
+#undef ZW
+#undef ZW1
+#undef Z1
+}
+
+}  // namespace

@@ -1,375 +1,7 @@
-// k_scalar.cu -- K1: flux-form advection of the density and of all density-weighted
-// scalars, fused with the Heun stage update; plain FP64 form.
-//
-// Replaces, per stage, src/TOOLS/advection.f90 advect/advection_ac ->
-// advection_x/y/z (:556-798) -> advs{x,y,z}_{weno,ppm,muscl}
-// (src/TOOLS/advq_weno.f90, advq_ppm.f90, advq_muscl.f90), integ_scal
-// (src/INTEG/integpack.f90:137-261) and, at the end of a step, get_scalars
-// (src/TOOLS/funcpack.f90:488-542).
-//
-// One block owns a 32x8 column tile and all fields, and marches k = 1..nz:
-//  * the haloed plane (38x14, three ghost cells each side) of field f at level k is
-//    staged into shared memory by TMA (cp.async.bulk.tensor.3d), two-slot ring,
-//    prefetched one (k,f) item ahead, completion on an mbarrier (bounded waits);
-//  * the momentum boxes of level k (34x9) for the x/y face velocities, TMA as well;
-//  * each thread's own column window x(k-1..k+L) of every field (and w) is
-//    prefetched with cp.async one level ahead into a shared-memory ring;
-//  * per item: x and y face fluxes in shared memory (552 faces over 288 threads =
-//    two rounds, face arrays double-buffered so one barrier per item suffices), then
-//    the z face of the thread's column, T = ((0-Tx)-Ty)-Tz (the reference's
-//    accumulation order), stage update, store.
-// Level-n buffers hold natural variables (the reference's state2 after
-// get_scalars), so stage-1 inputs are psi = s*rho (one multiply), and the stage-2
-// update writes s_new = psi_new/rho_new in place.
-//
-// Compiled with -fmad=false: bit-identical to the CPU restatement.
-#include "mg_common.cuh"
-#include "schemes.cuh"
-#include "tma.cuh"
-
-namespace {
-
-constexpr int TX = 32, TY = 8, H = 3;
-constexpr int SW = TX + 2 * H, SH = TY + 2 * H;   // haloed plane box 38 x 14
-constexpr int NT = TX * (TY + 1);                 // 288 threads: 8 cell warps + 1 helper warp
-constexpr int PLANE_BYTES = SW * SH * 8;          // 4256
-constexpr int PLANE_SLOT = 4352;                  // 128-byte multiple
-constexpr int VW = 34, VH = 9;                    // momentum box (x from i0-1, y from j0)
-constexpr int VBOX_BYTES = VW * VH * 8;           // 2448
-constexpr int VBOX_SLOT = 2560;
-constexpr int NCELL = TX * TY;
-
-struct Layout {
-    int zs;             // z-ring slots
-    size_t planes, vbu, vbv, densp, su, sv, fx, fy, mbar, zring, wring, zf, chain, crx, cry, total;
-};
-
-__host__ __device__ inline Layout make_layout(int scheme, int nf)
-{
-    Layout L;
-    L.zs = scheme == MG_PPM ? 5 : 4;   // window x(k-1..k+L), L = 3 (PPM) or 2
-    size_t o = 0;
-    L.planes = o; o += 2 * PLANE_SLOT;
-    L.vbu = o; o += VBOX_SLOT;
-    L.vbv = o; o += VBOX_SLOT;
-    L.densp = o; o += PLANE_SLOT;
-    L.su = o; o += TY * (TX + 1) * 8;
-    L.sv = o; o += (TY + 1) * TX * 8;
-    L.fx = o; o += 2 * TY * (TX + 1) * 8;   // double-buffered by item parity
-    L.fy = o; o += 2 * (TY + 1) * TX * 8;
-    o = (o + 127) / 128 * 128;
-    L.mbar = o; o += 128;
-    L.zring = o; o += (size_t)nf * L.zs * NCELL * 8;
-    L.wring = o; o += (size_t)L.zs * NCELL * 8;
-    L.zf = o; o += (size_t)nf * NCELL * 8;
-    L.chain = o;
-    L.crx = o;
-    L.cry = o;
-    if (scheme == MG_PPM) {
-        o += (size_t)2 * nf * NCELL * 8;
-        L.crx = o; o += 2 * 4 * TY * (TX + 2) * 8;   // double-buffered by item parity
-        L.cry = o; o += 2 * 4 * (TY + 2) * TX * 8;
-    }
-    L.total = o + 128;   // slack for 128-byte alignment of the base
-    return L;
-}
-
-__device__ __forceinline__ double ldg(const double *p, long long i) { return __ldg(p + i); }
-
-template <int SCHEME>
-__global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __grid_constant__ K1Maps M)
-{
-    extern __shared__ unsigned char smraw[];
-    unsigned char *sm = (unsigned char *)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
-    const int F = A.nf;
-    const Layout Ly = make_layout(SCHEME, F);
-    constexpr int ZS = SCHEME == MG_PPM ? 5 : 4;   // z-ring slots
-    constexpr int L = SCHEME == MG_PPM ? 3 : 2;    // window x(k-1 .. k+L)
-    double *planes = (double *)(sm + Ly.planes);
-    double *vbu = (double *)(sm + Ly.vbu), *vbv = (double *)(sm + Ly.vbv);
-    double *densp = (double *)(sm + Ly.densp);
-    double *su = (double *)(sm + Ly.su), *sv = (double *)(sm + Ly.sv);
-    double *fx = (double *)(sm + Ly.fx), *fy = (double *)(sm + Ly.fy);
-    uint64_t *mb = (uint64_t *)(sm + Ly.mbar);    // [0],[1] planes, [2] momentum boxes
-    double *zring = (double *)(sm + Ly.zring), *wring = (double *)(sm + Ly.wring);
-    double *zf = (double *)(sm + Ly.zf);
-    double *chain = (double *)(sm + Ly.chain);   // PPM: [0][f] Fr of the cell below, [1][f] its xplus
-    double *crx = (double *)(sm + Ly.crx), *cry = (double *)(sm + Ly.cry);
-
-    const int ntx = (G.maxx + TX - 1) / TX;
-    const int ti = blockIdx.x % ntx, tj = blockIdx.x / ntx;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int i0 = 4 + ti * TX, j0 = 4 + tj * TY;
-    const int nx = G.nx, ny = G.ny, nz = G.nz;
-    const bool cellt = ty < TY;
-    const int i = i0 + tx, j = j0 + ty;
-    const bool act = cellt && (i <= nx - 2) && (j <= ny - 2);
-    const int ic = min(i, nx - 2), jc = min(j, ny - 2);
-    const int cid = ty * TX + tx;   // cell slot (valid for cell threads)
-    const double dx1 = 1. / G.dx, dy1 = 1. / G.dy, dt0 = G.dt0;
-    const bool conv1 = (A.stage == 1);   // stage-1 inputs are natural: psi = s * rho
-    const int total_items = nz * F;
-
-    if (tid == 0) {
-        mbar_init(&mb[0], 1);
-        mbar_init(&mb[1], 1);
-        mbar_init(&mb[2], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-
-    auto issue_plane = [&](int q) {   // item q = (k-1)*F + f
-        const int k = q / F + 1, f = q % F;
-        double *dst = planes + (q & 1) * (PLANE_SLOT / 8);
-        fence_proxy_async_shared();
-        mbar_arrive_expect_tx(&mb[q & 1], PLANE_BYTES);
-        tma_load_3d(dst, &M.x[f], i0 - 4, j0 - 4, k - 1, &mb[q & 1]);
-    };
-    auto issue_vel = [&](int k) {
-        fence_proxy_async_shared();
-        mbar_arrive_expect_tx(&mb[2], 2 * VBOX_BYTES);
-        tma_load_3d(vbu, &M.mu, i0 - 2, j0 - 1, k - 1, &mb[2]);
-        tma_load_3d(vbv, &M.mv, i0 - 2, j0 - 1, k - 1, &mb[2]);
-    };
-    auto issue_z = [&](int l) {   // own-column values of every field and w at level l
-        if (cellt && l <= nz) {
-            const long long idx = gidx(G, ic, jc, l);
-            const int s = l % ZS;
-            for (int f = 0; f < F; f++) cp_async_8(&zring[(f * ZS + s) * NCELL + cid], A.xin[f] + idx);
-            cp_async_8(&wring[s * NCELL + cid], A.mw + idx);
-        }
-        cp_async_commit();
-    };
-
-    if (tid == 0) {
-        issue_plane(0);
-        issue_vel(1);
-    }
-    for (int l = 1; l <= L + 1; l++) issue_z(l);
-
-    double dn_old = 0., dn_new = 0.;   // density of the own cell: level n and new (stage 2)
-    int k_cur = 1;
-    // per-field vertical state
-    if (cellt)
-        for (int f = 0; f < F; f++) zf[f * NCELL + cid] = 0.;
-
-    int zsl[L + 2];   // z-ring slot of level k-1+m, refreshed per level
-    // stencil value of a field at level l = k-1+m of the own column
-#define ZVAL(f, m) (zring[((f) * ZS + zsl[(m)]) * NCELL + cid] * ((conv1 && A.dens_first && (f) > 0) ? zring[zsl[(m)] * NCELL + cid] : 1.))
-    auto wval = [&](int m) -> double {   // w_adv at level k-1+m of the own column
-        const double a0 = ldg(G.avden0, k_cur - 2 + m);
-        double x = wring[zsl[m] * NCELL + cid];
-        if (conv1) x = x * a0;
-        return x / a0;
-    };
-
-    for (int k = 1; k <= nz; k++) {
-        k_cur = k;
-#pragma unroll
-        for (int m = 0; m < L + 2; m++) zsl[m] = (k - 1 + m) % ZS;
-        const double d0 = ldg(G.den0, k - 1);
-        // momentum boxes of level k -> face velocities.  Previous readers of su/sv (the
-        // faces of iteration k-1) passed that iteration's last face barrier.
-        mbar_wait_bounded(&mb[2], (uint32_t)((k - 1) & 1), A.err);
-        for (int q = tid; q < TY * (TX + 1) + (TY + 1) * TX; q += NT) {
-            if (q < TY * (TX + 1)) {
-                int r = q / (TX + 1), c = q - r * (TX + 1);
-                double m = vbu[r * VW + c + 1];
-                if (conv1) m = m * d0;
-                su[q] = m / d0 - G.u0shift;
-            } else {
-                int qq = q - TY * (TX + 1);
-                int r = qq / TX, c = qq - r * TX;
-                double m = vbv[r * VW + c + 1];
-                if (conv1) m = m * d0;
-                sv[qq] = m / d0 - G.v0shift;
-            }
-        }
-        __syncthreads();   // su/sv complete; the momentum boxes are free again
-        if (tid == 0 && k + 1 <= nz) issue_vel(k + 1);
-        for (int f = 0; f < F; f++) {
-            const int q = (k - 1) * F + f;
-            // slot (q+1)&1 last held item q-1, whose faces all threads finished before
-            // the face barrier of item q-1
-            if (tid == 0 && q + 1 < total_items) issue_plane(q + 1);
-            mbar_wait_bounded(&mb[q & 1], (uint32_t)((q >> 1) & 1), A.err);
-            const double *pl = planes + (q & 1) * (PLANE_SLOT / 8);
-            const bool wconv = conv1 && A.dens_first && f > 0;
-            // the density plane of level k, read by the other fields' faces after this
-            // item's face barrier
-            if (conv1 && A.dens_first && f == 0)
-                for (int e = tid; e < SW * SH; e += NT) densp[e] = pl[e];
-            double *fxq = fx + (q & 1) * TY * (TX + 1), *fyq = fy + (q & 1) * (TY + 1) * TX;
-            double *crxq = crx + (q & 1) * 4 * TY * (TX + 2), *cryq = cry + (q & 1) * 4 * (TY + 2) * TX;
-            auto V = [&](int e) -> double { return wconv ? pl[e] * densp[e] : pl[e]; };
-            if (SCHEME == MG_PPM) {
-                for (int qq = tid; qq < TY * (TX + 2) + (TY + 2) * TX; qq += NT) {
-                    double xv[5], pr = 0., pL = 0., p1 = 0., p2 = 0.;
-                    if (qq < TY * (TX + 2)) {
-                        int r = qq / (TX + 2), c = qq - r * (TX + 2);
-                        int cell = i0 - 1 + c;
-                        for (int m = 0; m < 5; m++) xv[m] = V((r + H) * SW + c + m);
-                        int kind = cell == 3 ? 1 : (cell == 4 ? 2 : (cell == nx - 1 ? 3 : 0));
-                        if (cell <= nx - 1) ppm_cell_h(kind, xv, pr, pL, p1, p2);
-                        const int o = r * (TX + 2) + c, S = TY * (TX + 2);
-                        crxq[o] = pr; crxq[S + o] = pL; crxq[2 * S + o] = p1; crxq[3 * S + o] = p2;
-                    } else {
-                        int q2 = qq - TY * (TX + 2);
-                        int r = q2 / TX, c = q2 - r * TX;
-                        int cell = j0 - 1 + r;
-                        for (int m = 0; m < 5; m++) xv[m] = V((r + m) * SW + c + H);
-                        int kind = cell == 3 ? 1 : (cell == 4 ? 2 : (cell == ny - 1 ? 3 : 0));
-                        if (cell <= ny - 1) ppm_cell_h(kind, xv, pr, pL, p1, p2);
-                        const int o = r * TX + c, S = (TY + 2) * TX;
-                        cryq[o] = pr; cryq[S + o] = pL; cryq[2 * S + o] = p1; cryq[3 * S + o] = p2;
-                    }
-                }
-                __syncthreads();
-            }
-            // x face (threads 0..263: (TX+1)*TY faces) and y face (all 288 threads:
-            // TX*(TY+1) faces), written as two independent chains for instruction-level
-            // parallelism
-            {
-                const bool hasx = tid < TY * (TX + 1);
-                const int rx = hasx ? tid / (TX + 1) : 0, cx = hasx ? tid - rx * (TX + 1) : 0;
-                const int ry = tid / TX, cy = tid - ry * TX;
-                const double uu = su[hasx ? tid : 0], vv = sv[tid];
-                const int bx = (rx + H) * SW + H + cx - 1;   // x(i0 + cx - 1) in row rx
-                const int by = (ry - 1 + H) * SW + H + cy;   // x(j0 + ry - 1) in column cy
-                double Fx, Fy;
-                if (SCHEME == MG_WENO) {
-                    Fx = weno_face(V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu, true);
-                    Fy = weno_face(V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv, true);
-                } else if (SCHEME == MG_MUSCL) {
-                    Fx = muscl_face_h(G.muscl_lim, G.lim_tol, G.dx, dx1, V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu);
-                    Fy = muscl_face_h(G.muscl_lim, G.lim_tol, G.dy, dy1, V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv);
-                } else {
-                    const double mux = fabs(uu) * dt0 * dx1;
-                    const int o0 = rx * (TX + 2) + cx, o1 = o0 + 1, S = TY * (TX + 2);
-                    const double frx = ppm_fr(crxq[o0], mux, crxq[2 * S + o0], crxq[3 * S + o0]);
-                    const double flx = ppm_fl(crxq[S + o1], mux, crxq[2 * S + o1], crxq[3 * S + o1]);
-                    Fx = 0.5 * frx * (uu + fabs(uu)) + 0.5 * flx * (uu - fabs(uu));
-                    const double muy = fabs(vv) * dt0 * dy1;
-                    const int p0 = ry * TX + cy, p1 = p0 + TX, Sy = (TY + 2) * TX;
-                    const double fry = ppm_fr(cryq[p0], muy, cryq[2 * Sy + p0], cryq[3 * Sy + p0]);
-                    const double fly = ppm_fl(cryq[Sy + p1], muy, cryq[2 * Sy + p1], cryq[3 * Sy + p1]);
-                    Fy = 0.5 * fry * (vv + fabs(vv)) + 0.5 * fly * (vv - fabs(vv));
-                }
-                if (hasx) fxq[tid] = Fx;
-                fyq[tid] = Fy;
-            }
-            __syncthreads();   // faces of item q complete
-            if (!cellt) continue;
-
-            const double Tx = (fxq[ty * (TX + 1) + tx + 1] - fxq[ty * (TX + 1) + tx]) * dx1;
-            const double Ty = (fyq[(ty + 1) * TX + tx] - fyq[ty * TX + tx]) * dy1;
-
-            // ---- vertical face k+1/2 of the own column ----
-            if (f == 0) cp_async_wait_all();
-            const double dzw1 = ldg(G.dz1w, k - 1);
-            double Fzn = 0.;
-            double *zfo = &zf[f * NCELL + cid];
-            if (k <= nz - 1) {
-                const double ww = wval(2);
-                if (SCHEME == MG_WENO) {
-                    if (k == 1) Fzn = weno_face_bottom(ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww);
-                    else if (k == nz - 1) Fzn = weno_face_top(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ww);
-                    else Fzn = weno_face(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww,
-                                         (k >= 3 && k <= nz - 3));
-                } else if (SCHEME == MG_MUSCL) {
-                    const int kind = k == 1 ? 1 : (k == nz - 1 ? 2 : 0);
-                    const double d1m = k >= 2 ? ldg(G.dz1, k - 2) : 0., d10 = ldg(G.dz1, k - 1), d1p = ldg(G.dz1, k);
-                    const double fm = k >= 2 ? ldg(G.fdz0, k - 2) : 0., fp = ldg(G.fdz0, k);
-                    const double xm1 = k >= 2 ? ZVAL(f, 0) : 0.;
-                    const double xp2 = k + 2 <= nz ? ZVAL(f, 3) : 0.;
-                    Fzn = muscl_face_z(kind, G.muscl_lim, G.lim_tol, G.dz, xm1, ZVAL(f, 1), ZVAL(f, 2), xp2, d1m, d10,
-                                       d1p, fm, fp, dzw1, ww);
-                } else {
-                    double *prfr = &chain[f * NCELL + cid], *prxp = &chain[(F + f) * NCELL + cid];
-                    if (k == 1) {
-                        // cell 1 (advq_ppm.f90:328-343): bottom special, bc51 = 0
-                        const double x1 = ZVAL(f, 1), x2 = ZVAL(f, 2), x3 = ZVAL(f, 3);
-                        const double mup = fabs(wval(2)) * dt0 * ldg(G.dz1, 0);   // w(2) at k = 1
-                        const double ffip1 = x2 - x1, ffip2 = x3 - x2;
-                        const double xmin = x1 - 0.5 * ffip1, xplus = x1 + 0.5 * ffip1;
-                        double phir, phil, phi1, phi2;
-                        ppm_limiter(x1, x2, x2, xplus, xmin, ffip1, ffip2, 0., 0., phir, phil, phi1, phi2);
-                        *prfr = ppm_fr(phir, mup, phi1, phi2);
-                        *prxp = xplus;
-                    }
-                    // reconstruction of cell c = k+1 (:345-414)
-                    const int c = k + 1;
-                    const double xm2 = k >= 2 ? ZVAL(f, 0) : 0., xm1 = ZVAL(f, 1), x0 = ZVAL(f, 2);
-                    const double xp1 = c + 1 <= nz ? ZVAL(f, 3) : 0., xp2 = c + 2 <= nz ? ZVAL(f, 4) : 0.;
-                    const double d1c = ldg(G.dz1, c - 1);
-                    const double muc = fabs(ww) * dt0 * d1c;
-                    if (c == nz) {
-                        const double fl = x0 + 0.5 * (x0 - xm1) * (1. - muc);
-                        Fzn = 0.5 * (*prfr) * (ww + fabs(ww)) + 0.5 * fl * (ww - fabs(ww));
-                    } else {
-                        const double mup = fabs(wval(3)) * dt0 * d1c;
-                        double ffip1, ffip2, ffim1, ffim2, xplus;
-                        const double xmin = *prxp;
-                        if (c == 2) {
-                            ffip1 = xp1 - x0; ffip2 = xp2 - xp1; ffim1 = (x0 - xm1); ffim2 = 0.;
-                            xplus = x0 + 0.5 * ffip1;
-                        } else if (c == nz - 1) {
-                            ffip1 = xp1 - x0; ffim1 = x0 - xm1; ffim2 = xm1 - xm2; ffip2 = ffip1;
-                            xplus = x0 + 0.5 * ffip1;
-                        } else {
-                            ffip1 = (xp1 - x0); ffip2 = (xp2 - xp1); ffim1 = (x0 - xm1); ffim2 = (xm1 - xm2);
-                            xplus = ppm_xplus_z(x0, ffip1, ffip2, ffim1, ldg(G.dz1w, c - 2), ldg(G.dz1w, c - 1),
-                                                ldg(G.dz1w, c), ldg(G.dz1w, c + 1));
-                        }
-                        double phir, phil, phi1, phi2;
-                        ppm_limiter(x0, xp1, xm1, xplus, xmin, ffip1, ffip2, ffim1, ffim2, phir, phil, phi1, phi2);
-                        const double fl = ppm_fl(phil, muc, phi1, phi2);
-                        Fzn = 0.5 * (*prfr) * (ww + fabs(ww)) + 0.5 * fl * (ww - fabs(ww));
-                        *prfr = ppm_fr(phir, mup, phi1, phi2);
-                        *prxp = xplus;
-                    }
-                }
-            }
-            double Tz;
-            if (k == 1) Tz = (Fzn - 0.) * dzw1;
-            else if (k == nz) Tz = (0. - *zfo) * dzw1;
-            else Tz = (Fzn - *zfo) * dzw1;
-            *zfo = Fzn;
-
-            // ---- epilogue ----
-            if (act) {
-                const long long idx = gidx(G, i, j, k);
-                if (A.mode == 1) {
-                    double *xs = A.xout[f];
-                    xs[idx] = ((xs[idx] - Tx) - Ty) - Tz;
-                } else {
-                    const double T = ((0. - Tx) - Ty) - Tz;
-                    const double told = A.stage == 1 ? 0. : A.tend[f][idx];
-                    const double tn = T + A.b * told;
-                    const bool weighted = A.dens_first && f > 0;
-                    const double xo = A.xold[f][idx];   // level n (natural); stage 2 overwrites it in place
-                    if (A.dens_first && f == 0) dn_old = xo;
-                    const double old = weighted ? xo * dn_old : xo;
-                    const double xnew = old + A.a_dt * tn;
-                    if (A.stage == 2 && A.dens_first) {
-                        // get_scalars (funcpack.f90:488-542): natural value with the new density
-                        if (f == 0) dn_new = xnew;
-                        A.xout[f][idx] = weighted ? xnew / dn_new : xnew;
-                    } else {
-                        A.xout[f][idx] = xnew;
-                        A.tend[f][idx] = tn;
-                    }
-                    if (A.fst[f]) A.fst[f][idx] = T;
-                }
-            }
-        }
-        if (cellt) issue_z(k + L + 1);
-        else cp_async_commit();
-    }
-    cp_async_wait_all();
-}
-
-}  // namespace
+// k_scalar.cu -- K1 (scalar advection fused with the Heun stage update), plain FP64
+// form.  The kernel body is in k1_body.cuh.  This translation unit is compiled
+// with -fmad=false: bit-identical to the CPU restatement.
+#include "k1_body.cuh"
 
 size_t k1_smem_bytes(int scheme, int nf) { return make_layout(scheme, nf).total; }
 
@@ -381,9 +13,9 @@ cudaError_t launch_k1(const DevGrid &g, const K1Args &a, const K1Maps &maps, cud
     const size_t sm = make_layout(g.scal_adv, a.nf).total;
     if (sm > 232448) return cudaErrorInvalidValue;
     switch (g.scal_adv) {
-    case MG_WENO: k1_kernel<MG_WENO><<<grid, block, sm, s>>>(g, a, maps); break;
-    case MG_PPM: k1_kernel<MG_PPM><<<grid, block, sm, s>>>(g, a, maps); break;
-    default: k1_kernel<MG_MUSCL><<<grid, block, sm, s>>>(g, a, maps); break;
+    case MG_WENO: k1_kernel<MG_WENO, false><<<grid, block, sm, s>>>(g, a, maps); break;
+    case MG_PPM: k1_kernel<MG_PPM, false><<<grid, block, sm, s>>>(g, a, maps); break;
+    default: k1_kernel<MG_MUSCL, false><<<grid, block, sm, s>>>(g, a, maps); break;
     }
     return cudaGetLastError();
 }
@@ -391,7 +23,7 @@ cudaError_t launch_k1(const DevGrid &g, const K1Args &a, const K1Maps &maps, cud
 cudaError_t k1_init()
 {
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k1_kernel<MG_WENO>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k1_kernel<MG_PPM>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448)) != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k1_kernel<MG_MUSCL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+    if ((e = cudaFuncSetAttribute(k1_kernel<MG_WENO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k1_kernel<MG_PPM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k1_kernel<MG_MUSCL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
 }

@@ -86,10 +86,13 @@ struct K2Args {
 // launch wrappers (implemented in the .cu files)
 cudaError_t launch_k1(const DevGrid &g, const K1Args &a, const K1Maps &maps, cudaStream_t s);
 cudaError_t k1_init();
+cudaError_t launch_k1_mixed(const DevGrid &g, const K1Args &a, const K1Maps &maps, cudaStream_t s);
+cudaError_t k1_mixed_init();
 size_t k1_smem_bytes(int scheme, int nf);
 // TMA descriptor of one field buffer (box in doubles)
 int make_field_map(const DevGrid &g, const double *base, int boxx, int boxy, CUtensorMap *map);
 cudaError_t launch_k2(const DevGrid &g, const K2Args &a, cudaStream_t s);
+cudaError_t launch_k2_mixed(const DevGrid &g, const K2Args &a, cudaStream_t s);
 cudaError_t launch_halo_fill(const DevGrid &g, double *const *fields, int nf, cudaStream_t s);
 
 // projection

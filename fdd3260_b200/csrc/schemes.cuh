@@ -334,3 +334,181 @@ __device__ __forceinline__ T ppm_xplus_z(T x0, T ffip1, T ffip2, T ffim1, T delt
                 delta * (deltam1 + delta) / (T(2.) * delta + deltap1) * slp1 +
                 deltap1 * (deltap1 + deltap2) / (T(2.) * deltap1 + delta) * sl);
 }
+
+// =====================================================================================
+// Mixed form: the scheme logic in FP32 on differences relative to the upwind cell
+// value, the face flux u*(x_upwind + delta) in FP64.  Same algorithm as above
+// (identical in exact arithmetic); FP32 only ever holds perturbations, so the
+// cancellation in the flux differences costs no digits of the FP64 state.
+// =====================================================================================
+
+// WENO3-switch face i+1/2: returns the flux in FP64
+__device__ __forceinline__ double weno_face_mixed(double xm1, double x0, double xp1, double xp2, double uu,
+                                                  bool full_weights)
+{
+    const float eps = 1.e-15f, thres = 20.f, g1 = 1.f / 3.f, g2 = 2.f / 3.f;
+    const float a = (float)(xm1 - x0), b = (float)(xp1 - x0), c = (float)(xp2 - x0);
+    float w0 = g1, w1 = g2, w2 = g2, w3 = g1;
+    if (full_weights) {
+        const float d3 = c - b;
+        const float eta1 = a * a, eta2 = b * b, eta3 = d3 * d3;
+        if (fmaxf(eta1, eta2) > thres * (fminf(eta1, eta2) + eps)) {
+            const float y1 = eps + eta1, y2 = eps + eta2;
+            // w0 = g1/y1^2 / (g1/y1^2 + g2/y2^2) = g1 y2^2 / (g1 y2^2 + g2 y1^2)
+            const float p = g1 * (y2 * y2), q = g2 * (y1 * y1), r = __frcp_rn(p + q);
+            w0 = p * r; w1 = q * r;
+        }
+        if (fmaxf(eta2, eta3) > thres * (fminf(eta2, eta3) + eps)) {
+            const float y2 = eps + eta2, y3 = eps + eta3;
+            const float p = g2 * (y3 * y3), q = g1 * (y2 * y2), r = __frcp_rn(p + q);
+            w2 = p * r; w3 = q * r;
+        }
+    }
+    float d1 = -0.5f * a, d2 = 0.5f * b, dd3 = 1.5f * b - 0.5f * c;   // reconstructions minus x0
+    const float mind = fminf(fminf(d1, d2), dd3);
+    const float x0f = (float)x0;
+    const float den = mind + eps;
+    const float phi = fabsf(x0f) >= fabsf(den) ? 1.f : fabsf(x0f / den);
+    d1 *= phi; d2 *= phi; dd3 *= phi;
+    const float dl = w0 * d1 + w1 * d2, dr = w2 * d2 + w3 * dd3;
+    return uu > 0. ? uu * (x0 + (double)dl) : (uu < 0. ? uu * (x0 + (double)dr) : 0.);
+}
+__device__ __forceinline__ double weno_face_bottom_mixed(double x1, double x2, double x3, double ww)
+{
+    // Fl = (x1+x2)/2; Fr = g2 (x1+x2)/2 + g1 (1.5 x2 - 0.5 x3), relative to x1
+    const float b = (float)(x2 - x1), c = (float)(x3 - x1);
+    const float dl = 0.5f * b, dr = (2.f / 3.f) * (0.5f * b) + (1.f / 3.f) * (1.5f * b - 0.5f * c);
+    return ww > 0. ? ww * (x1 + (double)dl) : (ww < 0. ? ww * (x1 + (double)dr) : 0.);
+}
+__device__ __forceinline__ double weno_face_top_mixed(double xm1, double x0, double xp1, double ww)
+{
+    const float a = (float)(xm1 - x0), b = (float)(xp1 - x0);
+    const float dl = (1.f / 3.f) * (-0.5f * a) + (2.f / 3.f) * (0.5f * b), dr = 0.5f * b;
+    return ww > 0. ? ww * (x0 + (double)dl) : (ww < 0. ? ww * (x0 + (double)dr) : 0.);
+}
+
+// MUSCL horizontal face between i and i+1, relative to x0 (upwind for u > 0) and xp1
+__device__ __forceinline__ double muscl_face_h_mixed(int lim, float lim_tol, float d, float d1, double xm1, double x0,
+                                                     double xp1, double xp2, double uu)
+{
+    const float eps = 1.e-18f;
+    const float sp = (float)(xp1 - x0) * d1, sp2 = (float)(xp2 - xp1) * d1, sm = (float)(x0 - xm1) * d1;
+    const float ax = fabsf((float)x0);
+    float dr, dl;
+    if (d * fabsf(sm) > lim_tol * ax + eps || d * fabsf(sp2) > lim_tol * ax + eps) {
+        float phir, phil;
+        muscl_limiter(lim, lim_tol, (float)x0, sp, sp2, sm, phir, phil);
+        dr = -0.5f * phir * sp2 * d;   // Flux_r - x(i+1)
+        dl = 0.5f * phil * sm * d;     // Flux_l - x(i)
+    } else {
+        dr = -0.5f * sp * d;
+        dl = 0.5f * sp * d;
+    }
+    return uu >= 0. ? uu * (x0 + (double)dl) : uu * (xp1 + (double)dr);
+}
+// MUSCL vertical face (kind: 0 core, 1 bottom, 2 top), same argument meaning as muscl_face_z
+__device__ __forceinline__ double muscl_face_z_mixed(int kind, int lim, float lim_tol, float dz, double xm1, double x0,
+                                                     double xp1, double xp2, float d1m, float d10, float d1p, float fm,
+                                                     float fp, float dzw1, double ww)
+{
+    const float eps = 1.e-18f;
+    const float ax = fabsf((float)x0);
+    const float sp = (float)(xp1 - x0) * d10;
+    float sp2, sm;
+    bool lim_on;
+    if (kind == 1) {
+        sp2 = (float)(xp2 - xp1) * d1p;
+        sm = sp;
+        lim_on = fp * dz * fabsf(sp2) > lim_tol * ax + eps;
+    } else {
+        sm = (float)(x0 - xm1) * d1m;
+        if (kind == 2) {
+            sp2 = sp;
+            lim_on = fm * dz * fabsf(sm) > lim_tol * ax + eps;
+        } else {
+            sp2 = (float)(xp2 - xp1) * d1p;
+            lim_on = fm * dz * fabsf(sm) > lim_tol * ax + eps || fp * dz * fabsf(sp2) > lim_tol * ax + eps;
+        }
+    }
+    const float h = 0.5f / dzw1;
+    float dr, dl;
+    if (lim_on) {
+        float phir, phil;
+        muscl_limiter(lim, lim_tol, (float)x0, sp, sp2, sm, phir, phil);
+        dl = phil * sm * h;
+        dr = -(phir * sp2 * h);
+    } else {
+        dl = sp * h;
+        dr = -(sp * h);
+    }
+    return ww >= 0. ? ww * (x0 + (double)dl) : ww * (xp1 + (double)dr);
+}
+
+// PPM: reconstruction of a cell relative to its own value x0; xv[] holds
+// differences x(c-2..c+2) - x0 in FP32 and x0f the value itself (positivity tests).
+// Outputs dr = phir - x0, dl = phil - x0, phi1, phi2.
+__device__ __forceinline__ void ppm_limiter_rel(float x0f, float dp, float dm, float dplus, float dmin, float ffip1,
+                                                float ffip2, float ffim1, float ffim2, float &dr, float &dl, float &phi1,
+                                                float &phi2)
+{
+    // same logic as ppm_limiter with xx -> 0 (values relative to x0) and the
+    // positivity tests phir < 0  <=>  dr < -x0
+    const float eps = 1.e-15f, thres = 10.f;
+    float rp1 = 1.f;
+    dr = dplus; dl = dmin;
+    float a, b;
+    a = ffip1 - ffim1; b = ffip1 + ffim1;
+    const float gamma1 = 0.5f * (a * a + b * b);
+    a = ffip2 - ffip1; b = ffip2 + ffip1;
+    const float gamma2 = 0.5f * (a * a + b * b);
+    a = ffim1 - ffim2; b = ffim1 + ffim2;
+    const float gamma3 = 0.5f * (a * a + b * b);
+    const bool sel = fmaxf(fmaxf(gamma1, gamma2), gamma3) > thres * (fminf(fminf(gamma1, gamma2), gamma3) + eps);
+    phi1 = dr - dl;
+    phi2 = 3.f * (dl + dr);
+    if (sel) {
+        if (dr < -x0f || ((dr) * (dp - dr) < 0.f && (ffim1 * ffip2 >= 0.f || ffim1 * ffip1 <= 0.f || ffip2 * ffip1 <= 0.f))) {
+            if (fabsf(dr) < fabsf(dr - dp)) dr = 0.f;
+            else dr = dp;
+        }
+        if (dl < -x0f || ((-dl) * (dl - dm) < 0.f && (ffim2 * ffip1 >= 0.f || ffim2 * ffim1 <= 0.f || ffip1 * ffim1 <= 0.f))) {
+            if (fabsf(dl) < fabsf(dl - dm)) dl = 0.f;
+            else dl = dm;
+        }
+        phi1 = dr - dl;
+        phi2 = 3.f * (dl + dr);
+        const float slope = -(0.5f * phi1 / (copysignf(1.f, phi2) * fmaxf(fabsf(phi2), eps)));
+        if (fabsf(ffim1) > sqrtf(fspacing(ffim1))) rp1 = ffip1 / ffim1;
+        if (fabsf(phi2) > eps && (slope > -0.5f || slope < 0.5f)) {
+            const float lim = fmaxf(0.f, fminf(fminf(2.f, 0.5f * (rp1 + 1.f)), 2.f * rp1));
+            dr = 0.5f * ffim1 * lim;
+            dl = -(0.5f * ffim1 * lim);
+            if ((-dl) * (dr) < 0.f) { dl = 0.f; dr = 0.f; }
+            phi1 = dr - dl;
+            phi2 = 0.f;
+        }
+    }
+}
+
+// horizontal cell recon, mixed: xv = x(c-2..c+2) in FP64; outputs relative to x(c)
+__device__ __forceinline__ void ppm_cell_h_mixed(int kind, const double *xv, float &dr, float &dl, float &phi1, float &phi2)
+{
+    const double x0 = xv[2];
+    const float m2 = (float)(xv[0] - x0), m1 = (float)(xv[1] - x0), p1 = (float)(xv[3] - x0), p2 = (float)(xv[4] - x0);
+    float ffip1, ffip2, ffim1, ffim2, dplus, dmin;
+    if (kind == 1) {
+        ffip1 = p1; ffip2 = p2 - p1; ffim1 = -m1; ffim2 = -m1;
+        dmin = 0.5f * p1;
+        dplus = 0.5f * ffip1;
+    } else if (kind == 3) {
+        ffip1 = p1; ffip2 = p1; ffim1 = -m1; ffim2 = m1 - m2;
+        dplus = 0.5f * ffip1;
+        dmin = m1 + 0.5f * (-m1) - (1.f / 6.f) * (0.5f * ((p1 - 0.f) + (0.f - m1)) - 0.5f * ((0.f - m1) + (m1 - m2)));
+    } else {
+        ffip1 = p1; ffip2 = p2 - p1; ffim1 = -m1; ffim2 = m1 - m2;
+        dplus = 0.5f * ffip1 - (1.f / 6.f) * (0.5f * (ffip2 + ffip1) - 0.5f * (ffip1 + ffim1));
+        if (kind == 2) dmin = m1 + 0.5f * (-m1);
+        else dmin = m1 + 0.5f * (-m1) - (1.f / 6.f) * (0.5f * (p1 + (-m1)) - 0.5f * ((-m1) + (m1 - m2)));
+    }
+    ppm_limiter_rel((float)x0, p1, m1, dplus, dmin, ffip1, ffip2, ffim1, ffim2, dr, dl, phi1, phi2);
+}
