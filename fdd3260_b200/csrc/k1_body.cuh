@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
     }
     for (int l = 1; l <= L + 1; l++) issue_z(l);
 
-    double dn_old = 0., dn_new = 0.;   // density of the own cell: level n and new (stage 2)
+    double dn_old = 0., dn_new = 0., rdn_new = 0.;   // density of the own cell: level n and new (stage 2)
     int k_cur = 1;
     // per-field vertical state
     if (cellt)
@@ -135,7 +135,9 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
 
     int zsl[L + 2];   // z-ring slot of level k-1+m, refreshed per level
     // stencil value of a field at level l = k-1+m of the own column
-#define ZVAL(f, m) (zring[((f) * ZS + zsl[(m)]) * NCELL + cid] * ((conv1 && A.dens_first && (f) > 0) ? zring[zsl[(m)] * NCELL + cid] : 1.))
+// (stage 1 with density first: the other fields' entries are multiplied by the density
+// entry of the same level once, when the level arrives)
+#define ZVAL(f, m) (zring[((f) * ZS + zsl[(m)]) * NCELL + cid])
     auto wval = [&](int m) -> double {   // w_adv at level k-1+m of the own column
         const double a0 = ldg(G.avden0, k_cur - 2 + m);
         double x = wring[zsl[m] * NCELL + cid];
@@ -143,6 +145,7 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
         return x / a0;
     };
 
+    double wz2 = 0., wz3 = 0.;   // w_adv of the own column at levels k+1 and k+2
     for (int k = 1; k <= nz; k++) {
         k_cur = k;
 #pragma unroll
@@ -175,13 +178,20 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
             mbar_wait_bounded(&mb[q & 1], (uint32_t)((q >> 1) & 1), A.err);
             const double *pl = planes + (q & 1) * (PLANE_SLOT / 8);
             const bool wconv = conv1 && A.dens_first && f > 0;
-            // the density plane of level k, read by the other fields' faces after this
-            // item's face barrier
-            if (conv1 && A.dens_first && f == 0)
-                for (int e = tid; e < SW * SH; e += NT) densp[e] = pl[e];
+            // stage 1: the density plane of level k is kept for the other fields of the
+            // level, whose planes are turned into psi = s * rho in place, once per element
+            if (conv1 && A.dens_first) {
+                double *plw = planes + (q & 1) * (PLANE_SLOT / 8);
+                if (f == 0)
+                    for (int e = tid; e < SW * SH; e += NT) densp[e] = pl[e];
+                else
+                    for (int e = tid; e < SW * SH; e += NT) plw[e] = plw[e] * densp[e];
+                if (f > 0) __syncthreads();
+            }
             double *fxq = fx + (q & 1) * TY * (TX + 1), *fyq = fy + (q & 1) * (TY + 1) * TX;
             double *crxq = crx + (q & 1) * 4 * TY * (TX + 2), *cryq = cry + (q & 1) * 4 * (TY + 2) * TX;
-            auto V = [&](int e) -> double { return wconv ? pl[e] * densp[e] : pl[e]; };
+            (void)wconv;
+            auto V = [&](int e) -> double { return pl[e]; };
             if (SCHEME == MG_PPM) {
                 for (int qq = tid; qq < TY * (TX + 2) + (TY + 2) * TX; qq += NT) {
                     double xv[5], pr = 0., pL = 0., p1 = 0., p2 = 0.;
@@ -285,12 +295,26 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
             const double Ty = (fyq[(ty + 1) * TX + tx] - fyq[ty * TX + tx]) * dy1;
 
             // ---- vertical face k+1/2 of the own column ----
-            if (f == 0) cp_async_wait_all();
+            if (f == 0) {
+                cp_async_wait_all();
+                if (conv1 && A.dens_first) {
+                    // newly arrived levels: 1..L+1 at k = 1, else k+L
+                    const int m_lo = k == 1 ? 1 : L + 1;
+                    for (int m = m_lo; m <= L + 1; m++) {
+                        if (k - 1 + m > nz) break;
+                        const int sl = (k - 1 + m) % ZS;
+                        const double dn = zring[sl * NCELL + cid];
+                        for (int g = 1; g < F; g++) zring[(g * ZS + sl) * NCELL + cid] *= dn;
+                    }
+                }
+                wz2 = k <= nz - 1 ? wval(2) : 0.;
+                if (SCHEME == MG_PPM) wz3 = k + 2 <= nz ? wval(3) : 0.;
+            }
             const double dzw1 = ldg(G.dz1w, k - 1);
             double Fzn = 0.;
             double *zfo = &zf[f * NCELL + cid];
             if (k <= nz - 1) {
-                const double ww = wval(2);
+                const double ww = wz2;
                 if (SCHEME == MG_WENO) {
                     if constexpr (MIXED) {
                         if (k == 1) Fzn = weno_face_bottom_mixed(ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww);
@@ -319,7 +343,7 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
                     if (k == 1) {
                         const double x1 = ZVAL(f, 1);
                         const float b1 = (float)(ZVAL(f, 2) - x1), b2 = (float)(ZVAL(f, 3) - x1);
-                        const float mup = (float)(fabs(wval(2)) * dt0 * ldg(G.dz1, 0));
+                        const float mup = (float)(fabs(wz2) * dt0 * ldg(G.dz1, 0));
                         const float ffip1 = b1, ffip2 = b2 - b1;
                         float dr, dl, phi1, phi2;
                         ppm_limiter_rel((float)x1, b1, b1, 0.5f * ffip1, -0.5f * ffip1, ffip1, ffip2, 0.f, 0.f, dr, dl, phi1, phi2);
@@ -338,7 +362,7 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
                     if (c == nz) {
                         dfl = 0.5f * (-m1) * (1.f - muc);
                     } else {
-                        const float mup = (float)(fabs(wval(3)) * dt0 * d1c);
+                        const float mup = (float)(fabs(wz3) * dt0 * d1c);
                         float ffip1, ffip2, ffim1, ffim2, dplus;
                         const float dmin = (float)(*prxp) + m1;   // xplus(k) - x(k+1)
                         if (c == 2) {
@@ -366,7 +390,7 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
                     if (k == 1) {
                         // cell 1 (advq_ppm.f90:328-343): bottom special, bc51 = 0
                         const double x1 = ZVAL(f, 1), x2 = ZVAL(f, 2), x3 = ZVAL(f, 3);
-                        const double mup = fabs(wval(2)) * dt0 * ldg(G.dz1, 0);   // w(2) at k = 1
+                        const double mup = fabs(wz2) * dt0 * ldg(G.dz1, 0);   // w(2) at k = 1
                         const double ffip1 = x2 - x1, ffip2 = x3 - x2;
                         const double xmin = x1 - 0.5 * ffip1, xplus = x1 + 0.5 * ffip1;
                         double phir, phil, phi1, phi2;
@@ -384,7 +408,7 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
                         const double fl = x0 + 0.5 * (x0 - xm1) * (1. - muc);
                         Fzn = 0.5 * (*prfr) * (ww + fabs(ww)) + 0.5 * fl * (ww - fabs(ww));
                     } else {
-                        const double mup = fabs(wval(3)) * dt0 * d1c;
+                        const double mup = fabs(wz3) * dt0 * d1c;
                         double ffip1, ffip2, ffim1, ffim2, xplus;
                         const double xmin = *prxp;
                         if (c == 2) {
@@ -430,8 +454,13 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
                     const double xnew = old + A.a_dt * tn;
                     if (A.stage == 2 && A.dens_first) {
                         // get_scalars (funcpack.f90:488-542): natural value with the new density
-                        if (f == 0) dn_new = xnew;
-                        A.xout[f][idx] = weighted ? xnew / dn_new : xnew;
+                        if constexpr (MIXED) {   // one reciprocal per cell
+                            if (f == 0) { dn_new = xnew; rdn_new = 1. / xnew; }
+                            A.xout[f][idx] = weighted ? xnew * rdn_new : xnew;
+                        } else {
+                            if (f == 0) dn_new = xnew;
+                            A.xout[f][idx] = weighted ? xnew / dn_new : xnew;
+                        }
                     } else {
                         A.xout[f][idx] = xnew;
                         A.tend[f][idx] = tn;
