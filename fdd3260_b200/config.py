@@ -43,8 +43,8 @@ class Domain:
     u0shift: float = 0.0
     v0shift: float = 0.0
     precision: int = _lib.MG_PREC_FP64
-    refine_iters: int = 3
-    refine_tol: float = 1e-10
+    refine_iters: int = 2
+    refine_tol: float = 1e-13
     # derived (filled by finish())
     dzw: np.ndarray = field(default=None, repr=False)
     dz1w: np.ndarray = field(default=None, repr=False)

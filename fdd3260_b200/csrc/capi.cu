@@ -206,6 +206,9 @@ static int validate(const mg_params *p)
     if (p->mom_ord != 2 && p->mom_ord != 4) return MG_ERR_PARAM;
     if (p->nsubp < 1 || p->nsubp > 16) return MG_ERR_PARAM;
     if (p->precision != MG_PREC_FP64 && p->precision != MG_PREC_MIXED) return MG_ERR_PARAM;
+    if (p->precision == MG_PREC_MIXED &&
+        (p->refine_iters < 0 || p->nsubp * (1 + p->refine_iters) > MG_MAXPASS || !(p->refine_tol >= 0.)))
+        return MG_ERR_PARAM;
     if (!(p->dx > 0) || !(p->dy > 0) || !(p->dz > 0) || !(p->dt0 > 0)) return MG_ERR_PARAM;
     if (!p->fdz0 || !p->dzw || !p->dz1w || !p->dz1 || !p->den0 || !p->avden0 || !p->stab0 || !p->pt0 || !p->qv0)
         return MG_ERR_PARAM;
@@ -411,12 +414,27 @@ static cudaError_t project(mg_ctx *c, double *mu, double *mv, double *mw, const 
 {
     const DevGrid &G = c->G;
     const int fuse = finalize && !want_maxdiv;   // maxdiv needs the momentum after cal_p1
-    for (int ip = 0; ip < c->prm.nsubp; ip++) {
-        const int last = ip == c->prm.nsubp - 1;
-        PROF(c, "fft_x_fwd_div", launch_div_rhs(G, c->pp, mu, mv, mw, c->stream));
-        PROF(c, "fft_y_tridiag_fft_y_fft_x_inv", pressure_solve(G, c->pp, 0., 0, c->stream));
+    // each of the nsubp sub-iterations: solve (+ in the mixed form up to refine_iters
+    // refinement passes on the FP64 residual of the Poisson system), then the correction
+    const int nsub = c->prm.nsubp;
+    const int nref = c->prm.precision == MG_PREC_MIXED ? c->prm.refine_iters : 0;
+    cudaError_t er = pressure_resid_reset(c->pp, c->stream);
+    if (er != cudaSuccess) return er;
+    for (int ip = 0; ip < nsub; ip++) {
+        const int last = ip == nsub - 1;
+        const int slot0 = ip * (1 + nref);
+        const PassCtl p0 = {slot0, 0, 0, nref > 0, c->prm.refine_tol};
+        PROF(c, "fft_x_fwd_div", launch_div_rhs(G, c->pp, mu, mv, mw, p0, c->stream));
+        PROF(c, "fft_y_tridiag_fft_y_fft_x_inv", pressure_solve(G, c->pp, 0., 0, p0, c->stream));
+        *launches += 5;
+        for (int r = 0; r < nref; r++) {
+            const PassCtl pr = {slot0 + 1 + r, 1, r > 0, 0, c->prm.refine_tol};
+            PROF(c, "refine_residual_fft_x", launch_resid_rhs(G, c->pp, pr, c->stream));
+            PROF(c, "refine_solve", pressure_solve(G, c->pp, 0., 0, pr, c->stream));
+            *launches += 5;
+        }
         PROF(c, "correction_halo", launch_correction(G, c->pp, mu, mv, mw, c->p, fuse && last, c->stream));
-        *launches += 7;
+        *launches += 2;
     }
     PROF(c, "cal_p1", launch_cal_p1(G, c->pp, mw, wold, wold_rep, want_p1, fuse, c->stream));
     *launches += want_p1 ? 3 : 2;
@@ -648,7 +666,7 @@ extern "C" int mg_fft_solve(mg_ctx *c, const double *tend, double *out)
     CKR(h2d(c, c->unit[0], tend, cudaMemcpyHostToDevice));
     CKR(h2d(c, c->unit[1], out, cudaMemcpyHostToDevice));
     CKR(launch_load_rhs(c->G, c->pp, c->unit[0], c->stream));
-    CKR(pressure_solve(c->G, c->pp, 1., 1, c->stream));
+    CKR(pressure_solve(c->G, c->pp, 1., 1, kNoPassCtl, c->stream));
     CKR(launch_store_solution(c->G, c->pp, c->unit[1], c->stream));
     CKR(d2h(c, out, c->unit[1], cudaMemcpyDeviceToHost));
     return cuerr(cudaStreamSynchronize(c->stream));

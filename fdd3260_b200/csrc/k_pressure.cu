@@ -37,95 +37,254 @@ constexpr int MAXSTAGES = 16;
 struct FftPlan1 {
     int n;                 // length
     int nst;               // stages
-    int radix[MAXSTAGES];
+    unsigned long long rpack;   // radix of stage s in bits [4s, 4s+4)
     const double2 *tw;     // device twiddles exp(-2 pi i t/n), t in [0,n)
+    const float2 *twf;     // the same twiddles rounded to FP32 (mixed form)
 };
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// complex arithmetic on double2 (plain form) and float2 (mixed form: FP32 spectra)
+template <typename C> struct CT;
+template <> struct CT<double2> { using R = double; };
+template <> struct CT<float2> { using R = float; };
+template <typename C> __device__ __forceinline__ C mkc(typename CT<C>::R x, typename CT<C>::R y) { C c; c.x = x; c.y = y; return c; }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) { return mkc<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return mkc<C>(a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mkc<C>(a.x - b.x, a.y - b.y); }
 
 // twiddle exp(sign * 2 pi i t / n), sign = -1 forward, +1 inverse
-__device__ __forceinline__ double2 twid(const FftPlan1 &P, int t, int inv)
+template <typename C> __device__ __forceinline__ C twid(const FftPlan1 &P, int t, int inv);
+template <> __device__ __forceinline__ double2 twid<double2>(const FftPlan1 &P, int t, int inv)
 {
     double2 w = __ldg(P.tw + t);
     return inv ? make_double2(w.x, -w.y) : w;
 }
-
-// In-shared-memory Stockham FFT of one row: buffers a (input) and b (scratch),
-// threads [t0, t0+nt) of the block cooperate.  Result ends in a or b; returns the
-// pointer holding it.  Caller provides the barrier scope (whole block syncs).
-__device__ double2 *stockham(const FftPlan1 &P, double2 *a, double2 *b, int lt, int nt, int inv)
+template <> __device__ __forceinline__ float2 twid<float2>(const FftPlan1 &P, int t, int inv)
 {
-    const int n = P.n;
+    float2 w = __ldg(P.twf + t);
+    return inv ? make_float2(w.x, -w.y) : w;
+}
+
+// multiply by -i (forward, sign = -1) or +i (inverse): the exact quarter-turn
+template <typename C> __device__ __forceinline__ C rot(C v, int inv) { return inv ? mkc<C>(-v.y, v.x) : mkc<C>(v.y, -v.x); }
+
+// DFT of R values in registers, o[q] = sum_r v[r] w^{rq}, w = exp(-+2 pi i / R); R = 2, 3, 4, 5, 8
+template <typename C, int R> __device__ __forceinline__ void dft_small(C *v, int inv);
+template <typename C> __device__ __forceinline__ void dft_small2(C &a, C &b)
+{
+    const C t = a;
+    a = cadd(t, b);
+    b = csub(t, b);
+}
+template <> __device__ __forceinline__ void dft_small<double2, 2>(double2 *v, int) { dft_small2(v[0], v[1]); }
+template <> __device__ __forceinline__ void dft_small<float2, 2>(float2 *v, int) { dft_small2(v[0], v[1]); }
+template <typename C> __device__ __forceinline__ void dft4(C *v, int inv)
+{
+    const C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    const C t2 = cadd(v[1], v[3]), t3 = rot(csub(v[1], v[3]), inv);
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[3] = csub(t1, t3);
+}
+template <> __device__ __forceinline__ void dft_small<double2, 4>(double2 *v, int inv) { dft4(v, inv); }
+template <> __device__ __forceinline__ void dft_small<float2, 4>(float2 *v, int inv) { dft4(v, inv); }
+template <typename C> __device__ __forceinline__ void dft8(C *v, int inv)
+{
+    using R = typename CT<C>::R;
+    const R h = (R)0.70710678118654752440084436210485;   // sqrt(1/2)
+    // radix-2 over (r, r+4), then twiddles w8^{r}, then two radix-4 transforms
+    C a[4], b[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        a[r] = cadd(v[r], v[r + 4]);
+        b[r] = csub(v[r], v[r + 4]);
+    }
+    // b[r] *= w8^r:  w8 = (h, -+h)
+    const R sg = inv ? (R)1 : (R)-1;
+    b[1] = mkc<C>(h * (b[1].x - sg * b[1].y), h * (b[1].y + sg * b[1].x));
+    b[2] = rot(b[2], inv);
+    b[3] = mkc<C>(-h * (b[3].x + sg * b[3].y), h * (sg * b[3].x - b[3].y));
+    dft4(a, inv);
+    dft4(b, inv);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        v[2 * q] = a[q];
+        v[2 * q + 1] = b[q];
+    }
+}
+template <> __device__ __forceinline__ void dft_small<double2, 8>(double2 *v, int inv) { dft8(v, inv); }
+template <> __device__ __forceinline__ void dft_small<float2, 8>(float2 *v, int inv) { dft8(v, inv); }
+template <typename C> __device__ __forceinline__ void dft3(C *v, int inv)
+{
+    using R = typename CT<C>::R;
+    const R s3 = (R)0.86602540378443864676372317075294;   // sin(2 pi/3)
+    const C t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+    const C m = mkc<C>(v[0].x - (R)0.5 * t1.x, v[0].y - (R)0.5 * t1.y);
+    const C r = rot(mkc<C>(s3 * t2.x, s3 * t2.y), inv);
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(m, r);
+    v[2] = csub(m, r);
+}
+template <> __device__ __forceinline__ void dft_small<double2, 3>(double2 *v, int inv) { dft3(v, inv); }
+template <> __device__ __forceinline__ void dft_small<float2, 3>(float2 *v, int inv) { dft3(v, inv); }
+template <typename C> __device__ __forceinline__ void dft5(C *v, int inv)
+{
+    using R = typename CT<C>::R;
+    const R c1 = (R)0.30901699437494742410229341718282, c2 = (R)-0.80901699437494742410229341718282;
+    const R s1 = (R)0.95105651629515357211643933337938, s2 = (R)0.58778525229247312916870595463907;
+    const C t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]), t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+    const C a1 = mkc<C>(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+    const C a2 = mkc<C>(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+    const C b1 = rot(mkc<C>(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y), inv);
+    const C b2 = rot(mkc<C>(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y), inv);
+    v[0] = cadd(v[0], cadd(t1, t2));
+    v[1] = cadd(a1, b1);
+    v[4] = csub(a1, b1);
+    v[2] = cadd(a2, b2);
+    v[3] = csub(a2, b2);
+}
+template <> __device__ __forceinline__ void dft_small<double2, 5>(double2 *v, int inv) { dft5(v, inv); }
+template <> __device__ __forceinline__ void dft_small<float2, 5>(float2 *v, int inv) { dft5(v, inv); }
+
+// one Stockham stage of radix R: butterflies j = lt, lt+nt, ... < n/R; Ns = product of
+// the earlier radices (ns_shift = log2 Ns when Ns is a power of two, else -1)
+template <typename C, int R>
+__device__ __forceinline__ void stockham_stage(const FftPlan1 &P, const C *a, C *b, int lt, int nt, int inv,
+                                               int Ns, int ns_shift)
+{
+    const int n = P.n, nb = n / R;
+    const int tmul = n / (Ns * R);
+    for (int j = lt; j < nb; j += nt) {
+        const int jq = ns_shift >= 0 ? (j >> ns_shift) : j / Ns;
+        const int kk = j - jq * Ns;
+        const int tstep = kk * tmul;
+        C v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = a[j + r * nb];
+        if (tstep != 0) {
+#pragma unroll
+            for (int r = 1; r < R; r++) v[r] = cmul(v[r], twid<C>(P, tstep * r, inv));
+        }
+        dft_small<C, R>(v, inv);
+        const int idxD = jq * Ns * R + kk;
+#pragma unroll
+        for (int r = 0; r < R; r++) b[idxD + r * Ns] = v[r];
+    }
+}
+
+// In-shared-memory Stockham FFT of one row: buffers a (input) and b (scratch), threads
+// [0, nt) of a row group cooperate (lt = thread within the group).  Every stage ends in a
+// block barrier.  Returns the buffer holding the result.
+template <typename C>
+__device__ C *stockham(const FftPlan1 &P, C *a, C *b, int lt, int nt, int inv)
+{
     int Ns = 1;
     for (int s = 0; s < P.nst; s++) {
-        const int Rr = P.radix[s];
-        const int nb = n / Rr;
-        for (int j = lt; j < nb; j += nt) {
-            const int kk = j % Ns;
-            const int tstep = kk * (n / (Ns * Rr));
-            double2 v[5];
-            for (int r = 0; r < Rr; r++) {
-                double2 x = a[j + r * nb];
-                v[r] = r == 0 ? x : cmul(x, twid(P, tstep * r, inv));
-            }
-            double2 o[5];
-            if (Rr == 2) {
-                o[0] = cadd(v[0], v[1]);
-                o[1] = csub(v[0], v[1]);
-            } else if (Rr == 4) {
-                // omega = exp(sign*i*pi/2) = -i (forward) or +i (inverse), exact
-                double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
-                double2 t2 = cadd(v[1], v[3]), t3 = csub(v[1], v[3]);
-                double2 t3r = inv ? make_double2(-t3.y, t3.x) : make_double2(t3.y, -t3.x);   // t3 * omega
-                o[0] = cadd(t0, t2);
-                o[2] = csub(t0, t2);
-                o[1] = cadd(t1, t3r);
-                o[3] = csub(t1, t3r);
-            } else {
-                // generic small DFT with exact table twiddles omega_R^{rs} = W_n^{(rs mod R) n/R}
-                for (int q = 0; q < Rr; q++) {
-                    double2 acc = v[0];
-                    for (int r = 1; r < Rr; r++) acc = cadd(acc, cmul(v[r], twid(P, ((r * q) % Rr) * nb, inv)));
-                    o[q] = acc;
-                }
-            }
-            const int idxD = (j / Ns) * Ns * Rr + kk;
-            for (int r = 0; r < Rr; r++) b[idxD + r * Ns] = o[r];
+        const int Rr = (int)((P.rpack >> (4 * s)) & 15ull);
+        const int sh = (Ns & (Ns - 1)) == 0 ? __ffs(Ns) - 1 : -1;
+        switch (Rr) {
+        case 8: stockham_stage<C, 8>(P, a, b, lt, nt, inv, Ns, sh); break;
+        case 4: stockham_stage<C, 4>(P, a, b, lt, nt, inv, Ns, sh); break;
+        case 2: stockham_stage<C, 2>(P, a, b, lt, nt, inv, Ns, sh); break;
+        case 3: stockham_stage<C, 3>(P, a, b, lt, nt, inv, Ns, sh); break;
+        default: stockham_stage<C, 5>(P, a, b, lt, nt, inv, Ns, sh); break;
         }
         __syncthreads();
-        double2 *t = a; a = b; b = t;
+        C *t = a; a = b; b = t;
         Ns *= Rr;
     }
     return a;
+}
+
+// -------------------- refinement control --------------------
+struct Skip {
+    const unsigned long long *flag;   // residual slot checked, or null (never skip)
+    double tol;
+};
+__device__ __forceinline__ bool converged(const Skip &k)
+{
+    if (!k.flag) return false;
+    const unsigned long long v = *(volatile const unsigned long long *)k.flag;
+    return __longlong_as_double((long long)v) < k.tol;
 }
 
 // -------------------- step 1: rhs + x transform --------------------
 constexpr int ROWS = 8;   // rows per x-transform block (4 packed pairs)
 
 struct XArgs {
-    const double *mu, *mv, *mw;   // momentum (halo'd layout); null -> read rhs from rbuf
-    const double *rbuf;           // external rhs [nz][maxy][maxx] (interior only)
-    double2 *spec;                // S[k][kx][ky]
+    int mode;                     // 0: rhs = div(m)/(dt0*rho0) from momentum; 1: external rhs in rbuf;
+                                  // 2: refinement residual r = (b - <b>_k) - A dp
+    const double *mu, *mv, *mw;   // mode 0: momentum (halo'd layout)
+    double *rbuf;                 // [nz][maxy][maxx]: mode 1/2 read; mode 0 writes b when store_b
+    double *bsum;                 // [nz][groups] row-group sums of b (mode 0 writes when store_b, mode 2 reads)
+    int store_b;
+    const double *dp;             // mode 2: current solution [nz][maxy][maxx]
+    const double *ak, *ck, *dka, *dkb;   // mode 2: vertical coefficients of the Poisson system
+    void *spec;                   // S[k][kx][ky], complex of the form's precision
     double dt1;                   // 1/dt0
+    unsigned long long *resid;    // this pass's residual slot (max |rhs|*dt0), or null
+    Skip prev;                    // skip the pass when the previous pass's residual converged
 };
 
+// (A x) at one cell of the Poisson system solved by the transforms and the tridiagonal:
+// the periodic 5-point horizontal Laplacian (whose DFT eigenvalues are wv, get_wv
+// fft_tools.f90:82-107) plus the vertical rows of tridiag (fft_tools.f90:142-173).
+__device__ __forceinline__ double poisson_apply(const DevGrid &G, const XArgs &A, int k, int jr, int t)
+{
+    const int maxx = G.maxx, maxy = G.maxy, nz = G.nz;
+    const long long lev = (long long)maxx * maxy;
+    const double *pl = A.dp + (long long)(k - 1) * lev;
+    const long long o = (long long)jr * maxx + t;
+    const double x = __ldg(pl + o);
+    const double xw = __ldg(pl + (long long)jr * maxx + (t == 0 ? maxx - 1 : t - 1));
+    const double xe = __ldg(pl + (long long)jr * maxx + (t == maxx - 1 ? 0 : t + 1));
+    const double xs = __ldg(pl + (long long)(jr == 0 ? maxy - 1 : jr - 1) * maxx + t);
+    const double xn = __ldg(pl + (long long)(jr == maxy - 1 ? 0 : jr + 1) * maxx + t);
+    const double idx2 = 1. / (G.dx * G.dx), idy2 = 1. / (G.dy * G.dy);
+    double v = (xe - 2. * x + xw) * idx2 + (xn - 2. * x + xs) * idy2;
+    double dv;
+    if (k == 1) dv = -__ldg(A.dka) - __ldg(A.dkb);
+    else if (k == nz) dv = -__ldg(A.dka + nz - 1) + __ldg(A.dkb + nz - 1);
+    else dv = -__ldg(A.dka + k - 1);
+    v += dv * x;
+    if (k > 1) v += __ldg(A.ak + k - 1) * __ldg(pl + o - lev);
+    if (k < nz) v += __ldg(A.ck + k - 1) * __ldg(pl + o + lev);
+    return v;
+}
+
+template <typename C>
 __global__ void fft_x_fwd(DevGrid G, FftPlan1 P, XArgs A)
 {
-    extern __shared__ double2 smc[];
+    using R = typename CT<C>::R;
+    extern __shared__ double2 smraw_x[];
+    C *smc = reinterpret_cast<C *>(smraw_x);
+    C *spec = reinterpret_cast<C *>(A.spec);
     const int n = P.n, nh = n / 2 + 1, maxy = G.maxy;
     const int groups = (maxy + ROWS - 1) / ROWS;
     const int k = blockIdx.x / groups + 1, jg = blockIdx.x % groups;
     const int jb = jg * ROWS;                       // first interior row (0-based)
     const int nt_pair = blockDim.x / (ROWS / 2);
     const int pair = threadIdx.x / nt_pair, lt = threadIdx.x % nt_pair;
-    double2 *a = smc + pair * 2 * n, *b = a + n;
+    C *a = smc + pair * 2 * n, *b = a + n;
+    __shared__ unsigned long long bmax;
+    __shared__ double wsum[32];
+    if (converged(A.prev)) {   // uniform over the grid: nothing left to refine
+        if (blockIdx.x == 0 && threadIdx.x == 0 && A.resid) *A.resid = *A.prev.flag;
+        return;
+    }
+    if (threadIdx.x == 0) bmax = 0ull;
     const double dx1 = 1. / G.dx, dy1 = 1. / G.dy;
     const double dzw1 = __ldg(G.dz1w + k - 1), d0 = __ldg(G.den0 + k - 1);
+    double bmean = 0.;
+    if (A.mode == 2) {   // level mean of b from the row-group sums, fixed order
+        for (int g = 0; g < groups; g++) bmean += A.bsum[(k - 1) * groups + g];
+        bmean /= (double)G.maxx * (double)maxy;
+    }
     auto rhs = [&](int jr, int t) -> double {   // jr: interior row 0-based, t: interior column 0-based
         if (jr >= maxy) return 0.;
-        if (!A.mu) return __ldg(A.rbuf + ((long long)(k - 1) * maxy + jr) * G.maxx + t);
+        const long long o = ((long long)(k - 1) * maxy + jr) * G.maxx + t;
+        if (A.mode == 1) return __ldg(A.rbuf + o);
+        if (A.mode == 2) return (A.rbuf[o] - bmean) - poisson_apply(G, A, k, jr, t);
         const int i = t + 4, j = jr + 4;
         long long c = gidx(G, i, j, k);
         double d = 0.;
@@ -133,51 +292,79 @@ __global__ void fft_x_fwd(DevGrid G, FftPlan1 P, XArgs A)
         d = d + (__ldg(A.mv + c + G.px) - __ldg(A.mv + c)) * dy1;
         if (k < G.nz) d = d + (__ldg(A.mw + c + G.ps) - __ldg(A.mw + c)) * dzw1;
         else d = d + (0. - __ldg(A.mw + c)) * dzw1;
-        return A.dt1 * d / d0;
+        const double bv = A.dt1 * d / d0;
+        if (A.store_b) A.rbuf[o] = bv;
+        return bv;
     };
     const int r0 = jb + 2 * pair, r1 = r0 + 1;
-    for (int t = lt; t < n; t += nt_pair) a[t] = make_double2(rhs(r0, t), rhs(r1, t));
-    __syncthreads();
-    double2 *res = stockham(P, a, b, lt, nt_pair, 0);
+    double mx = 0., sm = 0.;
+    for (int t = lt; t < n; t += nt_pair) {
+        const double v0 = rhs(r0, t), v1 = rhs(r1, t);
+        mx = fmax(mx, fmax(fabs(v0), fabs(v1)));
+        sm += v0 + v1;
+        a[t] = mkc<C>((R)v0, (R)v1);
+    }
+    if (A.store_b) {   // deterministic block sum of b: fixed shuffle tree, warps in order
+        for (int o = 16; o > 0; o >>= 1) sm += __shfl_xor_sync(0xffffffffu, sm, o);
+        if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = sm;
+    }
+    __syncthreads();   // a[] complete, bmax initialised, warp sums written
+    if (A.store_b && threadIdx.x == 0) {
+        double t = 0.;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += wsum[w];
+        A.bsum[(k - 1) * groups + jg] = t;
+    }
+    if (A.resid) {
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if ((threadIdx.x & 31) == 0) atomicMax(&bmax, (unsigned long long)__double_as_longlong(mx * G.dt0));
+    }
+    C *res = stockham<C>(P, a, b, lt, nt_pair, 0);   // ends with a barrier
+    if (A.resid && threadIdx.x == 0) atomicMax(A.resid, bmax);
     // split: A_k = (Z_k + conj Z_{n-k})/2, B_k = (Z_k - conj Z_{n-k})/(2i)
     // write S[k][kx][jb + 2*pair + {0,1}]
     for (int kx = lt; kx < nh; kx += nt_pair) {
-        double2 z = res[kx], w = res[(n - kx) % n];
-        double2 Av = make_double2((z.x + w.x) * 0.5, (z.y - w.y) * 0.5);
-        double2 Bv = make_double2((z.y + w.y) * 0.5, (w.x - z.x) * 0.5);
+        C z = res[kx], w = res[(n - kx) % n];
+        C Av = mkc<C>((z.x + w.x) * (R)0.5, (z.y - w.y) * (R)0.5);
+        C Bv = mkc<C>((z.y + w.y) * (R)0.5, (w.x - z.x) * (R)0.5);
         long long base = ((long long)(k - 1) * nh + kx) * maxy;
-        if (r0 < maxy) A.spec[base + r0] = Av;
-        if (r1 < maxy) A.spec[base + r1] = Bv;
+        if (r0 < maxy) spec[base + r0] = Av;
+        if (r1 < maxy) spec[base + r1] = Bv;
     }
 }
 
 // -------------------- steps 2/4: y transform --------------------
 constexpr int YROWS = 4;   // (k,kx) rows per block
 
-__global__ void fft_y(DevGrid G, FftPlan1 P, double2 *spec, int nrows, int inv)
+template <typename C>
+__global__ void fft_y(DevGrid G, FftPlan1 P, void *spec_v, int nrows, int inv, Skip sk)
 {
-    extern __shared__ double2 smc[];
+    if (converged(sk)) return;
+    extern __shared__ double2 smraw_y[];
+    C *smc = reinterpret_cast<C *>(smraw_y);
+    C *spec = reinterpret_cast<C *>(spec_v);
     const int n = P.n;
     const int nt_row = blockDim.x / YROWS;
     const int rr = threadIdx.x / nt_row, lt = threadIdx.x % nt_row;
     const long long row = (long long)blockIdx.x * YROWS + rr;
-    double2 *a = smc + rr * 2 * n, *b = a + n;
+    C *a = smc + rr * 2 * n, *b = a + n;
     const bool ok = row < nrows;
     if (ok)
         for (int t = lt; t < n; t += nt_row) a[t] = spec[row * n + t];
     __syncthreads();
-    double2 *res = stockham(P, a, b, lt, nt_row, inv);
+    C *res = stockham<C>(P, a, b, lt, nt_row, inv);
     if (ok)
         for (int t = lt; t < n; t += nt_row) spec[row * n + t] = res[t];
 }
 
 // -------------------- step 3: vertical tridiagonal --------------------
 struct TriArgs {
-    double2 *spec;
+    void *spec;
+    double2 *scratch;        // mixed form: FP64 forward values [k][kx][ky]; null in the plain form
     const double *gam;       // [k][kx][ky], k = 2..nz (index k-1); k=1 unused
     const double *wv;        // wv(l,m), l fastest over maxx
     const double *ak, *ck, *dka, *dkb;   // per level coefficients (host-computed)
     int keep00;
+    Skip sk;
 };
 
 __device__ __forceinline__ double dk_of(const TriArgs &T, int k, int nz, double wl)
@@ -187,41 +374,56 @@ __device__ __forceinline__ double dk_of(const TriArgs &T, int k, int nz, double 
     return wl - __ldg(T.dka + k - 1);
 }
 
+// The elimination runs in FP64 in both forms, including the values carried between the
+// sweeps: the near-singular low-wavenumber columns amplify any rounding of them, and the
+// divergence residual barely sees errors in those modes, so refinement could not repair
+// them.  The mixed form reads its FP32 right-hand side, keeps the forward values in an
+// FP64 scratch spectrum and writes the FP32 solution.
+__device__ __forceinline__ double2 ld_spec(const double2 *s) { return *s; }
+__device__ __forceinline__ double2 ld_spec(const float2 *s) { float2 v = *s; return make_double2(v.x, v.y); }
+__device__ __forceinline__ void st_spec(double2 *s, double2 v) { *s = v; }
+__device__ __forceinline__ void st_spec(float2 *s, double2 v) { *s = make_float2((float)v.x, (float)v.y); }
+
+template <typename C>
 __global__ void tridiag_kernel(DevGrid G, TriArgs T)
 {
+    if (converged(T.sk)) return;
     const int nh = G.maxx / 2 + 1, maxy = G.maxy, nz = G.nz;
     const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= (long long)nh * maxy) return;
     const int kx = (int)(col / maxy), ky = (int)(col % maxy);
     const long long lstride = (long long)nh * maxy;
-    double2 *s = T.spec + (long long)kx * maxy + ky;
+    C *s = reinterpret_cast<C *>(T.spec) + (long long)kx * maxy + ky;
+    // forward values: in place (plain form) or in the FP64 scratch (mixed form)
+    double2 *u64 = T.scratch ? T.scratch + (long long)kx * maxy + ky : reinterpret_cast<double2 *>(s);
     if (kx == 0 && ky == 0) {
         if (!T.keep00)
-            for (int k = 0; k < nz; k++) s[k * lstride] = make_double2(0., 0.);
+            for (int k = 0; k < nz; k++) st_spec(s + k * lstride, make_double2(0., 0.));
         return;
     }
     const double wl = __ldg(T.wv + (long long)ky * G.maxx + kx);
     const double *gam = T.gam + (long long)kx * maxy + ky;
     // forward elimination (TRIDAG2 :219-229), complex rhs solved as its two real parts
     double bet = dk_of(T, 1, nz, wl);
-    double2 r = s[0];
+    double2 r = ld_spec(s);
     double2 uprev = make_double2(r.x / bet, r.y / bet);
-    s[0] = uprev;
+    u64[0] = uprev;
     for (int k = 2; k <= nz; k++) {
         double g = __ldg(gam + (k - 1) * lstride);
         double a = __ldg(T.ak + k - 1);
         bet = dk_of(T, k, nz, wl) - a * g;
-        double2 rk = s[(k - 1) * lstride];
+        double2 rk = ld_spec(s + (k - 1) * lstride);
         double2 u = make_double2((rk.x - a * uprev.x) / bet, (rk.y - a * uprev.y) / bet);
-        s[(k - 1) * lstride] = u;
+        u64[(k - 1) * lstride] = u;
         uprev = u;
     }
     // back substitution (:231-233)
+    st_spec(s + (nz - 1) * lstride, uprev);
     for (int k = nz - 1; k >= 1; k--) {
         double g = __ldg(gam + k * lstride);   // GAM(k+1)
-        double2 uk = s[(k - 1) * lstride];
+        double2 uk = u64[(k - 1) * lstride];
         uk = make_double2(uk.x - g * uprev.x, uk.y - g * uprev.y);
-        s[(k - 1) * lstride] = uk;
+        st_spec(s + (k - 1) * lstride, uk);
         uprev = uk;
     }
 }
@@ -249,37 +451,51 @@ __global__ void gam_kernel(DevGrid G, TriArgs T, double *gam, int *err)
 
 // -------------------- step 5: inverse x transform --------------------
 struct XInvArgs {
-    const double2 *spec;
+    const void *spec;
     double *dp;          // [nz][maxy][maxx] real
     double scale_div;    // divide by this (N_h), or 1
+    int accumulate;      // refinement pass: dp += solution
+    Skip sk;
 };
 
+template <typename C>
 __global__ void fft_x_inv(DevGrid G, FftPlan1 P, XInvArgs A)
 {
-    extern __shared__ double2 smc[];
+    if (converged(A.sk)) return;
+    using R = typename CT<C>::R;
+    extern __shared__ double2 smraw_xi[];
+    C *smc = reinterpret_cast<C *>(smraw_xi);
+    const C *spec = reinterpret_cast<const C *>(A.spec);
     const int n = P.n, nh = n / 2 + 1, maxy = G.maxy;
     const int groups = (maxy + ROWS - 1) / ROWS;
     const int k = blockIdx.x / groups + 1, jg = blockIdx.x % groups;
     const int jb = jg * ROWS;
     const int nt_pair = blockDim.x / (ROWS / 2);
     const int pair = threadIdx.x / nt_pair, lt = threadIdx.x % nt_pair;
-    double2 *a = smc + pair * 2 * n, *b = a + n;
+    C *a = smc + pair * 2 * n, *b = a + n;
     const int r0 = jb + 2 * pair, r1 = r0 + 1;
     // rebuild Z_k = A_k + i B_k over the full circle from the half spectra
     for (int kx = lt; kx < nh; kx += nt_pair) {
         long long base = ((long long)(k - 1) * nh + kx) * maxy;
-        double2 Av = r0 < maxy ? A.spec[base + r0] : make_double2(0., 0.);
-        double2 Bv = r1 < maxy ? A.spec[base + r1] : make_double2(0., 0.);
-        a[kx] = make_double2(Av.x - Bv.y, Av.y + Bv.x);
-        if (kx > 0 && kx < n - kx) a[n - kx] = make_double2(Av.x + Bv.y, Bv.x - Av.y);
+        C Av = r0 < maxy ? spec[base + r0] : mkc<C>(0, 0);
+        C Bv = r1 < maxy ? spec[base + r1] : mkc<C>(0, 0);
+        a[kx] = mkc<C>(Av.x - Bv.y, Av.y + Bv.x);
+        if (kx > 0 && kx < n - kx) a[n - kx] = mkc<C>(Av.x + Bv.y, Bv.x - Av.y);
     }
     __syncthreads();
-    double2 *res = stockham(P, a, b, lt, nt_pair, 1);
+    C *res = stockham<C>(P, a, b, lt, nt_pair, 1);
     for (int t = lt; t < n; t += nt_pair) {
-        double2 z = res[t];
-        if (r0 < maxy) A.dp[((long long)(k - 1) * maxy + r0) * G.maxx + t] = z.x / A.scale_div;
-        if (r1 < maxy) A.dp[((long long)(k - 1) * maxy + r1) * G.maxx + t] = z.y / A.scale_div;
+        C z = res[t];
+        const long long o0 = ((long long)(k - 1) * maxy + r0) * G.maxx + t, o1 = o0 + G.maxx;
+        if (A.accumulate) {
+            if (r0 < maxy) A.dp[o0] = A.dp[o0] + (double)z.x / A.scale_div;
+            if (r1 < maxy) A.dp[o1] = A.dp[o1] + (double)z.y / A.scale_div;
+        } else {
+            if (r0 < maxy) A.dp[o0] = (double)z.x / A.scale_div;
+            if (r1 < maxy) A.dp[o1] = (double)z.y / A.scale_div;
+        }
     }
+    (void)sizeof(R);
 }
 
 // -------------------- step 6: correction --------------------
@@ -480,14 +696,18 @@ __global__ void to_natural_kernel(DevGrid G, const double *src, const double *w,
 }
 
 // -------------------- host side: plan --------------------
-bool factorize(int n, int *radix, int *nst)
+bool factorize(int n, FftPlan1 *P)
 {
     int m = n, s = 0;
-    while (m % 4 == 0 && s < MAXSTAGES) { radix[s++] = 4; m /= 4; }
-    while (m % 2 == 0 && s < MAXSTAGES) { radix[s++] = 2; m /= 2; }
-    while (m % 3 == 0 && s < MAXSTAGES) { radix[s++] = 3; m /= 3; }
-    while (m % 5 == 0 && s < MAXSTAGES) { radix[s++] = 5; m /= 5; }
-    *nst = s;
+    unsigned long long pk = 0;
+    auto put = [&](int r) { pk |= (unsigned long long)r << (4 * s); s++; m /= r; };
+    while (m % 8 == 0 && s < MAXSTAGES) put(8);
+    while (m % 4 == 0 && s < MAXSTAGES) put(4);
+    while (m % 2 == 0 && s < MAXSTAGES) put(2);
+    while (m % 3 == 0 && s < MAXSTAGES) put(3);
+    while (m % 5 == 0 && s < MAXSTAGES) put(5);
+    P->nst = s;
+    P->rpack = pk;
     return m == 1;
 }
 
@@ -496,6 +716,9 @@ bool factorize(int n, int *radix, int *nst)
 struct PressurePlan {
     FftPlan1 px, py;
     double2 *twx = nullptr, *twy = nullptr;
+    float2 *twxf = nullptr, *twyf = nullptr;
+    int mixed = 0;                 // FP32 spectra and transforms
+    double2 *tri = nullptr;        // mixed form: FP64 values between the tridiagonal sweeps
     double2 *spec = nullptr;       // [nz][nh][maxy]
     double *dp = nullptr;          // [nz][maxy][maxx]
     double *rbuf = nullptr;        // [nz][maxy][maxx] external rhs
@@ -504,6 +727,8 @@ struct PressurePlan {
     double *ak = nullptr, *ck = nullptr, *dka = nullptr, *dkb = nullptr;
     double *mean = nullptr, *mean_d = nullptr, *p1 = nullptr;
     double *partial = nullptr, *maxdiv = nullptr;
+    unsigned long long *resid = nullptr;   // [MG_MAXPASS] residual per pass of the current projection
+    double *bsum = nullptr;                // [nz][row groups] sums of b (refined projection)
     int npartial = 0;
     size_t bytes = 0;
 };
@@ -521,9 +746,21 @@ static cudaError_t make_twiddles(int n, double2 **out)
     return cudaMemcpy(*out, h.data(), n * sizeof(double2), cudaMemcpyHostToDevice);
 }
 
+static cudaError_t make_twiddles_f(int n, float2 **out)
+{
+    std::vector<float2> h(n);
+    const long double PI = 3.141592653589793238462643383279502884L;
+    for (int t = 0; t < n; t++) {
+        long double ang = -2.0L * PI * (long double)t / (long double)n;
+        h[t] = make_float2((float)cosl(ang), (float)sinl(ang));
+    }
+    cudaError_t e = cudaMalloc(out, n * sizeof(float2));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*out, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice);
+}
+
 cudaError_t pressure_plan_create(const DevGrid &g, const double *wv_host, int mixed, PressurePlan **out, int *pivot_error)
 {
-    (void)mixed;
     *out = nullptr;
     *pivot_error = 0;
     PressurePlan *pp = new PressurePlan();
@@ -533,15 +770,22 @@ cudaError_t pressure_plan_create(const DevGrid &g, const double *wv_host, int mi
 #define CK(x) do { e = (x); if (e != cudaSuccess) { pressure_plan_destroy(pp); return e; } } while (0)
     pp->px.n = g.maxx;
     pp->py.n = g.maxy;
-    if (!factorize(g.maxx, pp->px.radix, &pp->px.nst) || !factorize(g.maxy, pp->py.radix, &pp->py.nst)) {
+    if (!factorize(g.maxx, &pp->px) || !factorize(g.maxy, &pp->py)) {
         pressure_plan_destroy(pp);
         return cudaErrorInvalidValue;
     }
+    pp->mixed = mixed ? 1 : 0;
     CK(make_twiddles(g.maxx, &pp->twx));
     CK(make_twiddles(g.maxy, &pp->twy));
+    CK(make_twiddles_f(g.maxx, &pp->twxf));
+    CK(make_twiddles_f(g.maxy, &pp->twyf));
     pp->px.tw = pp->twx;
     pp->py.tw = pp->twy;
-    CK(cudaMalloc(&pp->spec, nspec * sizeof(double2)));
+    pp->px.twf = pp->twxf;
+    pp->py.twf = pp->twyf;
+    const size_t cbytes = pp->mixed ? sizeof(float2) : sizeof(double2);
+    CK(cudaMalloc(&pp->spec, nspec * cbytes));
+    if (pp->mixed) CK(cudaMalloc(&pp->tri, nspec * sizeof(double2)));
     CK(cudaMalloc(&pp->dp, nreal * sizeof(double)));
     CK(cudaMalloc(&pp->rbuf, nreal * sizeof(double)));
     CK(cudaMalloc(&pp->gam, nspec * sizeof(double)));
@@ -583,6 +827,9 @@ cudaError_t pressure_plan_create(const DevGrid &g, const double *wv_host, int mi
     pp->npartial = 1024;
     CK(cudaMalloc(&pp->partial, pp->npartial * 8));
     CK(cudaMalloc(&pp->maxdiv, 8));
+    CK(cudaMalloc(&pp->resid, MG_MAXPASS * sizeof(unsigned long long)));
+    CK(cudaMalloc(&pp->bsum, (size_t)g.nz * ((g.maxy + ROWS - 1) / ROWS) * sizeof(double)));
+    CK(cudaMemset(pp->resid, 0, MG_MAXPASS * sizeof(unsigned long long)));
     // elimination factors and pivot check
     {
         int *derr;
@@ -599,7 +846,7 @@ cudaError_t pressure_plan_create(const DevGrid &g, const double *wv_host, int mi
         if (e != cudaSuccess) { pressure_plan_destroy(pp); return e; }
         *pivot_error = herr;
     }
-    pp->bytes = nspec * (16 + 8) + nreal * 16 + (size_t)g.maxx * g.maxy * 8 + (size_t)(g.maxx + g.maxy) * 16;
+    pp->bytes = nspec * (cbytes + 8 + (pp->mixed ? 16 : 0)) + nreal * 16 + (size_t)g.maxx * g.maxy * 8 + (size_t)(g.maxx + g.maxy) * 16;
 #undef CK
     *out = pp;
     return cudaSuccess;
@@ -608,32 +855,71 @@ cudaError_t pressure_plan_create(const DevGrid &g, const double *wv_host, int mi
 void pressure_plan_destroy(PressurePlan *pp)
 {
     if (!pp) return;
-    cudaFree(pp->twx); cudaFree(pp->twy); cudaFree(pp->spec); cudaFree(pp->dp); cudaFree(pp->rbuf);
+    cudaFree(pp->twx); cudaFree(pp->twy); cudaFree(pp->twxf); cudaFree(pp->twyf); cudaFree(pp->spec); cudaFree(pp->tri); cudaFree(pp->dp); cudaFree(pp->rbuf);
     cudaFree(pp->gam); cudaFree(pp->wv); cudaFree(pp->ak); cudaFree(pp->ck); cudaFree(pp->dka); cudaFree(pp->dkb);
     cudaFree(pp->mean); cudaFree(pp->mean_d); cudaFree(pp->p1); cudaFree(pp->partial); cudaFree(pp->maxdiv);
+    cudaFree(pp->resid); cudaFree(pp->bsum);
     delete pp;
 }
 
 size_t pressure_plan_bytes(const PressurePlan *pp) { return pp ? pp->bytes : 0; }
 const double *pressure_p1_dev(const PressurePlan *pp) { return pp->p1; }
 const double *pressure_maxdiv_dev(const PressurePlan *pp) { return pp->maxdiv; }
+const unsigned long long *pressure_resid_dev(const PressurePlan *pp) { return pp->resid; }
+cudaError_t pressure_resid_reset(PressurePlan *pp, cudaStream_t s)
+{
+    return cudaMemsetAsync(pp->resid, 0, MG_MAXPASS * sizeof(unsigned long long), s);
+}
+static Skip skip_self(const PressurePlan *pp, const PassCtl &pc)
+{
+    Skip k{nullptr, pc.tol};
+    if (pc.slot >= 0 && pc.refine) k.flag = pp->resid + pc.slot;
+    return k;
+}
 
-static cudaError_t launch_x_fwd(const DevGrid &g, PressurePlan *pp, const XArgs &a, cudaStream_t s)
+template <typename C>
+static cudaError_t launch_x_fwd_t(const DevGrid &g, PressurePlan *pp, const XArgs &a, cudaStream_t s)
 {
     int groups = (g.maxy + ROWS - 1) / ROWS;
-    int nt_pair = g.maxx / 4 < 32 ? 32 : (g.maxx / 4 > 256 ? 256 : g.maxx / 4);
-    size_t sm = (size_t)(ROWS / 2) * 2 * g.maxx * sizeof(double2);
-    cudaError_t e = cudaFuncSetAttribute(fft_x_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int nt_pair = g.maxx / 8 < 32 ? 32 : (g.maxx / 8 > 256 ? 256 : g.maxx / 8);
+    size_t sm = (size_t)(ROWS / 2) * 2 * g.maxx * sizeof(C);
+    cudaError_t e = cudaFuncSetAttribute(fft_x_fwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    fft_x_fwd<<<g.nz * groups, nt_pair * (ROWS / 2), sm, s>>>(g, pp->px, a);
+    fft_x_fwd<C><<<g.nz * groups, nt_pair * (ROWS / 2), sm, s>>>(g, pp->px, a);
     return cudaGetLastError();
+}
+static cudaError_t launch_x_fwd(const DevGrid &g, PressurePlan *pp, const XArgs &a, cudaStream_t s)
+{
+    return pp->mixed ? launch_x_fwd_t<float2>(g, pp, a, s) : launch_x_fwd_t<double2>(g, pp, a, s);
+}
+
+static void set_resid(const PressurePlan *pp, const PassCtl &pc, XArgs &a)
+{
+    if (pc.slot >= 0 && pc.slot < MG_MAXPASS) {
+        a.resid = pp->resid + pc.slot;
+        if (pc.skip_prev && pc.slot > 0) a.prev = Skip{pp->resid + pc.slot - 1, pc.tol};
+    }
 }
 
 cudaError_t launch_div_rhs(const DevGrid &g, PressurePlan *pp, const double *mu, const double *mv, const double *mw,
-                           cudaStream_t s)
+                           const PassCtl &pc, cudaStream_t s)
 {
     XArgs a{};
+    a.mode = 0;
     a.mu = mu; a.mv = mv; a.mw = mw; a.spec = pp->spec; a.dt1 = 1. / g.dt0;
+    if (pc.store_b) { a.store_b = 1; a.rbuf = pp->rbuf; a.bsum = pp->bsum; }
+    set_resid(pp, pc, a);
+    return launch_x_fwd(g, pp, a, s);
+}
+
+cudaError_t launch_resid_rhs(const DevGrid &g, PressurePlan *pp, const PassCtl &pc, cudaStream_t s)
+{
+    XArgs a{};
+    a.mode = 2;
+    a.rbuf = pp->rbuf; a.bsum = pp->bsum; a.dp = pp->dp;
+    a.ak = pp->ak; a.ck = pp->ck; a.dka = pp->dka; a.dkb = pp->dkb;
+    a.spec = pp->spec; a.dt1 = 1. / g.dt0;
+    set_resid(pp, pc, a);
     return launch_x_fwd(g, pp, a, s);
 }
 
@@ -644,40 +930,55 @@ cudaError_t launch_load_rhs(const DevGrid &g, PressurePlan *pp, const double *te
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     XArgs a{};
+    a.mode = 1;
     a.rbuf = pp->rbuf; a.spec = pp->spec;
     return launch_x_fwd(g, pp, a, s);
 }
 
-cudaError_t pressure_solve(const DevGrid &g, PressurePlan *pp, double scale, int keep00, cudaStream_t s)
+template <typename C>
+static cudaError_t pressure_solve_t(const DevGrid &g, PressurePlan *pp, int keep00, Skip sk, int accumulate,
+                                    cudaStream_t s)
 {
-    (void)scale;
     cudaError_t e;
     const int nh = g.maxx / 2 + 1;
     const int nrows = g.nz * nh;
-    int nt_row = g.maxy / 4 < 32 ? 32 : (g.maxy / 4 > 256 ? 256 : g.maxy / 4);
-    size_t smy = (size_t)YROWS * 2 * g.maxy * sizeof(double2);
-    e = cudaFuncSetAttribute(fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy);
+    int nt_row = g.maxy / 8 < 32 ? 32 : (g.maxy / 8 > 256 ? 256 : g.maxy / 8);
+    size_t smy = (size_t)YROWS * 2 * g.maxy * sizeof(C);
+    e = cudaFuncSetAttribute(fft_y<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy);
     if (e != cudaSuccess) return e;
-    fft_y<<<(nrows + YROWS - 1) / YROWS, nt_row * YROWS, smy, s>>>(g, pp->py, pp->spec, nrows, 0);
+    fft_y<C><<<(nrows + YROWS - 1) / YROWS, nt_row * YROWS, smy, s>>>(g, pp->py, pp->spec, nrows, 0, sk);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     TriArgs T{};
     T.spec = pp->spec; T.gam = pp->gam; T.wv = pp->wv; T.ak = pp->ak; T.ck = pp->ck; T.dka = pp->dka; T.dkb = pp->dkb;
     T.keep00 = keep00;
+    T.sk = sk;
+    T.scratch = pp->tri;
     long long ncol = (long long)nh * g.maxy;
-    tridiag_kernel<<<(unsigned)((ncol + 127) / 128), 128, 0, s>>>(g, T);
+    tridiag_kernel<C><<<(unsigned)((ncol + 127) / 128), 128, 0, s>>>(g, T);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    fft_y<<<(nrows + YROWS - 1) / YROWS, nt_row * YROWS, smy, s>>>(g, pp->py, pp->spec, nrows, 1);
+    fft_y<C><<<(nrows + YROWS - 1) / YROWS, nt_row * YROWS, smy, s>>>(g, pp->py, pp->spec, nrows, 1, sk);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     int groups = (g.maxy + ROWS - 1) / ROWS;
-    int nt_pair = g.maxx / 4 < 32 ? 32 : (g.maxx / 4 > 256 ? 256 : g.maxx / 4);
-    size_t smx = (size_t)(ROWS / 2) * 2 * g.maxx * sizeof(double2);
-    e = cudaFuncSetAttribute(fft_x_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
+    int nt_pair = g.maxx / 8 < 32 ? 32 : (g.maxx / 8 > 256 ? 256 : g.maxx / 8);
+    size_t smx = (size_t)(ROWS / 2) * 2 * g.maxx * sizeof(C);
+    e = cudaFuncSetAttribute(fft_x_inv<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
     if (e != cudaSuccess) return e;
     XInvArgs xa{};
     xa.spec = pp->spec; xa.dp = pp->dp;
     xa.scale_div = keep00 ? 1.0 : (double)g.maxx * (double)g.maxy;
-    fft_x_inv<<<g.nz * groups, nt_pair * (ROWS / 2), smx, s>>>(g, pp->px, xa);
+    xa.sk = sk;
+    xa.accumulate = accumulate;
+    fft_x_inv<C><<<g.nz * groups, nt_pair * (ROWS / 2), smx, s>>>(g, pp->px, xa);
     return cudaGetLastError();
+}
+
+cudaError_t pressure_solve(const DevGrid &g, PressurePlan *pp, double scale, int keep00, const PassCtl &pc,
+                           cudaStream_t s)
+{
+    (void)scale;
+    const Skip sk = skip_self(pp, pc);
+    return pp->mixed ? pressure_solve_t<float2>(g, pp, keep00, sk, pc.refine, s)
+                     : pressure_solve_t<double2>(g, pp, keep00, sk, pc.refine, s);
 }
 
 cudaError_t launch_store_solution(const DevGrid &g, PressurePlan *pp, double *out, cudaStream_t s)

@@ -101,14 +101,37 @@ cudaError_t pressure_plan_create(const DevGrid &g, const double *wv_host, int mi
                                  int *pivot_error);
 void pressure_plan_destroy(PressurePlan *pp);
 size_t pressure_plan_bytes(const PressurePlan *pp);
+// Refinement control of one projection pass.  The mixed form solves the Poisson system
+// A dp = b of the reference (b = div(m)/(dt0*rho0); A: periodic 5-point horizontal
+// Laplacian plus the vertical tridiagonal rows) with FP32 transforms, then refines:
+// r = (b - <b>_k) - A dp in FP64, solve A e = r with FP32 transforms, dp += e.  The plan
+// keeps, per pass, the residual max|rhs|*dt0 [1/s] seen by that pass (as the bit pattern
+// of a non-negative double).  A refinement pass is skipped on the device -- its kernels
+// return at entry -- once that residual is below tol, so a captured graph keeps a fixed
+// launch sequence while the work stops at convergence.
+struct PassCtl {
+    int slot;        // residual slot of this pass, or -1 (no bookkeeping)
+    int refine;      // refinement pass (residual rhs, dp += solution, skipped once converged)
+    int skip_prev;   // refinement pass after another: skip entirely once that one had converged
+    int store_b;     // first pass of a refined projection: keep b and its level sums
+    double tol;
+};
+constexpr PassCtl kNoPassCtl = {-1, 0, 0, 0, 0.};
+constexpr int MG_MAXPASS = 64;
+// zero the residual slots before a projection
+cudaError_t pressure_resid_reset(PressurePlan *pp, cudaStream_t s);
+const unsigned long long *pressure_resid_dev(const PressurePlan *pp);
+// refinement pass right-hand side: r = (b - <b>_k) - A dp into the spectrum (FP64 residual)
+cudaError_t launch_resid_rhs(const DevGrid &g, PressurePlan *pp, const PassCtl &pc, cudaStream_t s);
 // rhs = div(m)/(dt0*rho0) into the plan's real buffer (interior)
 cudaError_t launch_div_rhs(const DevGrid &g, PressurePlan *pp, const double *mu, const double *mv,
-                           const double *mw, cudaStream_t s);
+                           const double *mw, const PassCtl &pc, cudaStream_t s);
 // external rhs (unit entry): copy interior of a halo'd field into the real buffer
 cudaError_t launch_load_rhs(const DevGrid &g, PressurePlan *pp, const double *tend, cudaStream_t s);
 // forward FFT -> tridiagonal -> inverse FFT on the plan's buffers; out real buffer = unnormalised
 // solution (scale = 1) or rescaled solution (scale = 1/N_h); keep00: keep mode (0,0) untouched
-cudaError_t pressure_solve(const DevGrid &g, PressurePlan *pp, double scale, int keep00, cudaStream_t s);
+cudaError_t pressure_solve(const DevGrid &g, PressurePlan *pp, double scale, int keep00, const PassCtl &pc,
+                           cudaStream_t s);
 // copy the plan's real solution into the interior of a halo'd field
 cudaError_t launch_store_solution(const DevGrid &g, PressurePlan *pp, double *out, cudaStream_t s);
 // correction: p += rho0*dp; m -= dt0*rho0*grad(dp); ghost cells refreshed

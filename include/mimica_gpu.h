@@ -67,11 +67,13 @@ typedef struct mg_params {
     int nsubp;                 /* pressure sub-iterations (nsubp >= 1) */
     int with_buoy;             /* buoyancy (with_buoy, imp_buoy=.true.) */
     int precision;             /* MG_PREC_* */
-    int refine_iters;          /* mixed form: max FP64-residual refinement passes per projection */
+    int refine_iters;          /* mixed form: max refinement passes per pressure solve, each on the
+                                  FP64 residual r = b - A dp of the Poisson system; nsubp*(1+refine_iters) <= 64 */
     double dx, dy, dz, dt0;
     double lim_tol;            /* MUSCL tolerance (lim_tol) */
     double u0shift, v0shift;   /* Galilean shift of the advective velocity */
-    double refine_tol;         /* mixed form: stop refining when max|div(rho0 u)|/rho0 < tol [1/s] */
+    double refine_tol;         /* mixed form: skip further refinement once max|r|*dt0 < tol [1/s]
+                                  (r in the units of b = div(rho0 u)/(dt0 rho0)) */
     const double *fdz0, *dzw, *dz1w, *dz1;              /* grid metrics, define_grid.f90:179-187 */
     const double *den0, *avden0, *stab0, *pt0, *qv0;     /* base state, initial.f90:500-558 */
 } mg_params;
