@@ -37,6 +37,7 @@ SOURCES = [
     ("k_pressure.cu", ["-fmad=false"]),
     ("k_pressure_mixed.cu", []),
     ("capi.cu", []),
+    ("noalloc.cu", ["-fmad=false"]),
 ]
 
 

@@ -160,6 +160,20 @@ int mg_fft_solve(mg_ctx *ctx, const double *tend, double *out);
 int mg_anelastic_pressure(mg_ctx *ctx, double *mu, double *mv, double *mw, double *p,
                           const double *wold, double *maxdiv, double *p1);
 
+/* ---- allocation-free entry (no counterpart in the reference) ----
+ * The projection residual of pressure_solver.f90:121-130 (signed max of the
+ * divergence over the interior, k = 2..nz-1), computed without a context and without
+ * allocating: its block partials live in a fixed 8 KiB device array of the library.
+ * mu, mv, mw: device pointers to momentum in the reference layout (nx = maxx+5,
+ * ny = maxy+5, nz); dz1w: device pointer (nz); maxdiv: device pointer receiving the
+ * result; stream: a cudaStream_t (or NULL for the legacy default stream).
+ * Limits: maxx, maxy <= 4096, 3 <= nz <= 4096 (MG_ERR_PARAM beyond).  The first call
+ * on a device resolves the scratch address and must precede any stream capture that
+ * is to contain the call; calls in flight together on one device race on the scratch. */
+int mg_maxdiv_noalloc(int maxx, int maxy, int nz, double dx, double dy, const double *dz1w,
+                      const double *mu, const double *mv, const double *mw, double *maxdiv,
+                      void *stream);
+
 #ifdef __cplusplus
 }
 #endif
