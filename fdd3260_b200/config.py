@@ -43,7 +43,7 @@ class Domain:
     u0shift: float = 0.0
     v0shift: float = 0.0
     precision: int = _lib.MG_PREC_FP64
-    refine_iters: int = 2
+    refine_iters: int = 1
     refine_tol: float = 1e-13
     # derived (filled by finish())
     dzw: np.ndarray = field(default=None, repr=False)

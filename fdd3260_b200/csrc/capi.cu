@@ -466,6 +466,7 @@ static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int wa
         for (int f = 0; f < nf; f++) {
             a1.xin[f] = stage == 1 ? c->sA[f] : c->sB[f];
             a1.xold[f] = c->sA[f];
+            a1.xold_is_xin = stage == 1;
             a1.xout[f] = stage == 1 ? c->sB[f] : c->sA[f];
             a1.tend[f] = c->ts[f];
             a1.fst[f] = (f == ies && G.with_buoy) ? c->fes : ((f == iqt && G.with_buoy) ? c->fqt : nullptr);

@@ -14,6 +14,8 @@ constexpr int SW = TX + 2 * H, SH = TY + 2 * H;   // haloed plane box 38 x 14
 constexpr int NT = TX * (TY + 1);                 // 288 threads: 8 cell warps + 1 helper warp
 constexpr int PLANE_BYTES = SW * SH * 8;          // 4256
 constexpr int PLANE_SLOT = 4352;                  // 128-byte multiple
+constexpr int NP = 4;                             // plane slots: NP-1 items of TMA look-ahead
+constexpr int MB_VEL = NP;                        // mbarrier of the momentum boxes
 constexpr int VW = 34, VH = 9;                    // momentum box (x from i0-1, y from j0)
 constexpr int VBOX_BYTES = VW * VH * 8;           // 2448
 constexpr int VBOX_SLOT = 2560;
@@ -29,7 +31,7 @@ __host__ __device__ inline Layout make_layout(int scheme, int nf)
     Layout L;
     L.zs = scheme == MG_PPM ? 5 : 4;   // window x(k-1..k+L), L = 3 (PPM) or 2
     size_t o = 0;
-    L.planes = o; o += 2 * PLANE_SLOT;
+    L.planes = o; o += NP * PLANE_SLOT;
     L.vbu = o; o += VBOX_SLOT;
     L.vbv = o; o += VBOX_SLOT;
     L.densp = o; o += PLANE_SLOT;
@@ -70,7 +72,7 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
     double *densp = (double *)(sm + Ly.densp);
     double *su = (double *)(sm + Ly.su), *sv = (double *)(sm + Ly.sv);
     double *fx = (double *)(sm + Ly.fx), *fy = (double *)(sm + Ly.fy);
-    uint64_t *mb = (uint64_t *)(sm + Ly.mbar);    // [0],[1] planes, [2] momentum boxes
+    uint64_t *mb = (uint64_t *)(sm + Ly.mbar);    // [0, NP) planes, [NP] momentum boxes
     double *zring = (double *)(sm + Ly.zring), *wring = (double *)(sm + Ly.wring);
     double *zf = (double *)(sm + Ly.zf);
     double *chain = (double *)(sm + Ly.chain);   // PPM: [0][f] Fr of the cell below, [1][f] its xplus
@@ -91,25 +93,23 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
     const int total_items = nz * F;
 
     if (tid == 0) {
-        mbar_init(&mb[0], 1);
-        mbar_init(&mb[1], 1);
-        mbar_init(&mb[2], 1);
+        for (int b = 0; b <= NP; b++) mbar_init(&mb[b], 1);
         fence_mbar_init();
     }
     __syncthreads();
 
     auto issue_plane = [&](int q) {   // item q = (k-1)*F + f
         const int k = q / F + 1, f = q % F;
-        double *dst = planes + (q & 1) * (PLANE_SLOT / 8);
+        double *dst = planes + (q % NP) * (PLANE_SLOT / 8);
         fence_proxy_async_shared();
-        mbar_arrive_expect_tx(&mb[q & 1], PLANE_BYTES);
-        tma_load_3d(dst, &M.x[f], i0 - 4, j0 - 4, k - 1, &mb[q & 1]);
+        mbar_arrive_expect_tx(&mb[q % NP], PLANE_BYTES);
+        tma_load_3d(dst, &M.x[f], i0 - 4, j0 - 4, k - 1, &mb[q % NP]);
     };
     auto issue_vel = [&](int k) {
         fence_proxy_async_shared();
-        mbar_arrive_expect_tx(&mb[2], 2 * VBOX_BYTES);
-        tma_load_3d(vbu, &M.mu, i0 - 2, j0 - 1, k - 1, &mb[2]);
-        tma_load_3d(vbv, &M.mv, i0 - 2, j0 - 1, k - 1, &mb[2]);
+        mbar_arrive_expect_tx(&mb[MB_VEL], 2 * VBOX_BYTES);
+        tma_load_3d(vbu, &M.mu, i0 - 2, j0 - 1, k - 1, &mb[MB_VEL]);
+        tma_load_3d(vbv, &M.mv, i0 - 2, j0 - 1, k - 1, &mb[MB_VEL]);
     };
     auto issue_z = [&](int l) {   // own-column values of every field and w at level l
         if (cellt && l <= nz) {
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
     };
 
     if (tid == 0) {
-        issue_plane(0);
+        for (int q0 = 0; q0 < NP - 1 && q0 < total_items; q0++) issue_plane(q0);
         issue_vel(1);
     }
     for (int l = 1; l <= L + 1; l++) issue_z(l);
@@ -146,6 +146,14 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
     };
 
     double wz2 = 0., wz3 = 0.;   // w_adv of the own column at levels k+1 and k+2
+    // register prefetch of the epilogue operands (stage 2 / unit mode), one item ahead
+    const long long idx0 = gidx(G, ic, jc, 1);
+    const bool pf_loads = A.mode == 0 && (!A.xold_is_xin || A.stage == 2);
+    double nx_xold = 0., nx_tend = 0.;
+    if (pf_loads && act) {
+        if (!A.xold_is_xin) nx_xold = ldg(A.xold[0], idx0);
+        if (A.stage == 2) nx_tend = ldg(A.tend[0], idx0);
+    }
     for (int k = 1; k <= nz; k++) {
         k_cur = k;
 #pragma unroll
@@ -153,7 +161,7 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
         const double d0 = ldg(G.den0, k - 1);
         // momentum boxes of level k -> face velocities.  Previous readers of su/sv (the
         // faces of iteration k-1) passed that iteration's last face barrier.
-        mbar_wait_bounded(&mb[2], (uint32_t)((k - 1) & 1), A.err);
+        mbar_wait_bounded(&mb[MB_VEL], (uint32_t)((k - 1) & 1), A.err);
         for (int q = tid; q < TY * (TX + 1) + (TY + 1) * TX; q += NT) {
             if (q < TY * (TX + 1)) {
                 int r = q / (TX + 1), c = q - r * (TX + 1);
@@ -172,21 +180,47 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
         if (tid == 0 && k + 1 <= nz) issue_vel(k + 1);
         for (int f = 0; f < F; f++) {
             const int q = (k - 1) * F + f;
-            // slot (q+1)&1 last held item q-1, whose faces all threads finished before
-            // the face barrier of item q-1
-            if (tid == 0 && q + 1 < total_items) issue_plane(q + 1);
-            mbar_wait_bounded(&mb[q & 1], (uint32_t)((q >> 1) & 1), A.err);
-            const double *pl = planes + (q & 1) * (PLANE_SLOT / 8);
+            // epilogue operands of this item (loaded one item ahead), then the loads of the
+            // next item's, which complete while this item's faces are computed
+            const double cur_xold = nx_xold, cur_tend = nx_tend;
+            if (pf_loads && act && q + 1 < total_items) {
+                const int fn = f + 1 < F ? f + 1 : 0, kn = f + 1 < F ? k : k + 1;
+                const long long idn = idx0 + (long long)(kn - 1) * G.ps;
+                if (!A.xold_is_xin) nx_xold = ldg(A.xold[fn], idn);
+                if (A.stage == 2) nx_tend = ldg(A.tend[fn], idn);
+            }
+            // slot (q+NP-1)%NP last held item q-1, whose faces all threads finished
+            // before the face barrier of item q-1
+            if (tid == 0 && q + NP - 1 < total_items) issue_plane(q + NP - 1);
+            mbar_wait_bounded(&mb[q % NP], (uint32_t)((q / NP) & 1), A.err);
+            const double *pl = planes + (q % NP) * (PLANE_SLOT / 8);
+            // level-n value of the own cell when it is the plane's.  Stage 1 then turns
+            // the plane into psi = s * rho in place (the density plane of the level is kept
+            // for the other fields): each cell thread scales its own element right after
+            // reading it, the 276 halo elements are shared out, one barrier follows.
+            const int own_e = (ty + H) * SW + tx + H;
+            const double plane_xo = cellt ? pl[own_e] : 0.;
             const bool wconv = conv1 && A.dens_first && f > 0;
-            // stage 1: the density plane of level k is kept for the other fields of the
-            // level, whose planes are turned into psi = s * rho in place, once per element
             if (conv1 && A.dens_first) {
-                double *plw = planes + (q & 1) * (PLANE_SLOT / 8);
-                if (f == 0)
+                double *plw = planes + (q % NP) * (PLANE_SLOT / 8);
+                if (f == 0) {
                     for (int e = tid; e < SW * SH; e += NT) densp[e] = pl[e];
-                else
-                    for (int e = tid; e < SW * SH; e += NT) plw[e] = plw[e] * densp[e];
-                if (f > 0) __syncthreads();
+                } else {
+                    if (cellt) plw[own_e] = plane_xo * densp[own_e];
+                    constexpr int NHALO = SW * SH - TX * TY;   // 276
+                    for (int h = tid; h < NHALO; h += NT) {
+                        int e;
+                        if (h < 2 * H * SW) {   // halo rows 0..2 and 11..13
+                            const int r = h / SW, c = h - r * SW;
+                            e = (r < H ? r : r + TY) * SW + c;
+                        } else {                 // halo columns of the cell rows
+                            const int h2 = h - 2 * H * SW, r = h2 / (2 * H), cc = h2 - r * (2 * H);
+                            e = (r + H) * SW + (cc < H ? cc : cc + TX);
+                        }
+                        plw[e] = plw[e] * densp[e];
+                    }
+                    __syncthreads();
+                }
             }
             double *fxq = fx + (q & 1) * TY * (TX + 1), *fyq = fy + (q & 1) * (TY + 1) * TX;
             double *crxq = crx + (q & 1) * 4 * TY * (TX + 2), *cryq = cry + (q & 1) * 4 * (TY + 2) * TX;
@@ -445,10 +479,11 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
                     xs[idx] = ((xs[idx] - Tx) - Ty) - Tz;
                 } else {
                     const double T = ((0. - Tx) - Ty) - Tz;
-                    const double told = A.stage == 1 ? 0. : A.tend[f][idx];
+                    const double told = A.stage == 1 ? 0. : cur_tend;
                     const double tn = T + A.b * told;
                     const bool weighted = A.dens_first && f > 0;
-                    const double xo = A.xold[f][idx];   // level n (natural); stage 2 overwrites it in place
+                    // level n (natural); stage 2 overwrites it in place
+                    const double xo = A.xold_is_xin ? plane_xo : cur_xold;
                     if (A.dens_first && f == 0) dn_old = xo;
                     const double old = weighted ? xo * dn_old : xo;
                     const double xnew = old + A.a_dt * tn;

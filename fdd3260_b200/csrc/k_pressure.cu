@@ -252,8 +252,13 @@ __device__ __forceinline__ double poisson_apply(const DevGrid &G, const XArgs &A
     return v;
 }
 
+// The x-transform kernels keep the rows' buffers as two halves, [a_0..a_3 | b_0..b_3],
+// so that one half is free when the other holds data: the half spectra move between
+// shared memory and S[k][kx][ky] through a [kx][8 rows] staging tile in the free half,
+// 8 consecutive ky (one 64/128-byte segment) per kx instead of 2 scattered values.
+constexpr int XT_THREADS = 256;
 template <typename C>
-__global__ void fft_x_fwd(DevGrid G, FftPlan1 P, XArgs A)
+__global__ void __launch_bounds__(XT_THREADS, 3) fft_x_fwd(DevGrid G, FftPlan1 P, XArgs A)
 {
     using R = typename CT<C>::R;
     extern __shared__ double2 smraw_x[];
@@ -265,7 +270,8 @@ __global__ void fft_x_fwd(DevGrid G, FftPlan1 P, XArgs A)
     const int jb = jg * ROWS;                       // first interior row (0-based)
     const int nt_pair = blockDim.x / (ROWS / 2);
     const int pair = threadIdx.x / nt_pair, lt = threadIdx.x % nt_pair;
-    C *a = smc + pair * 2 * n, *b = a + n;
+    C *ahalf = smc, *bhalf = smc + (ROWS / 2) * n;
+    C *a = ahalf + pair * n, *b = bhalf + pair * n;
     __shared__ unsigned long long bmax;
     __shared__ double wsum[32];
     if (converged(A.prev)) {   // uniform over the grid: nothing left to refine
@@ -275,6 +281,7 @@ __global__ void fft_x_fwd(DevGrid G, FftPlan1 P, XArgs A)
     if (threadIdx.x == 0) bmax = 0ull;
     const double dx1 = 1. / G.dx, dy1 = 1. / G.dy;
     const double dzw1 = __ldg(G.dz1w + k - 1), d0 = __ldg(G.den0 + k - 1);
+    const double rfac = A.dt1 / d0;   // rhs = div(m) * dt1 / rho0
     double bmean = 0.;
     if (A.mode == 2) {   // level mean of b from the row-group sums, fixed order
         for (int g = 0; g < groups; g++) bmean += A.bsum[(k - 1) * groups + g];
@@ -292,7 +299,7 @@ __global__ void fft_x_fwd(DevGrid G, FftPlan1 P, XArgs A)
         d = d + (__ldg(A.mv + c + G.px) - __ldg(A.mv + c)) * dy1;
         if (k < G.nz) d = d + (__ldg(A.mw + c + G.ps) - __ldg(A.mw + c)) * dzw1;
         else d = d + (0. - __ldg(A.mw + c)) * dzw1;
-        const double bv = A.dt1 * d / d0;
+        const double bv = d * rfac;
         if (A.store_b) A.rbuf[o] = bv;
         return bv;
     };
@@ -320,15 +327,28 @@ __global__ void fft_x_fwd(DevGrid G, FftPlan1 P, XArgs A)
     }
     C *res = stockham<C>(P, a, b, lt, nt_pair, 0);   // ends with a barrier
     if (A.resid && threadIdx.x == 0) atomicMax(A.resid, bmax);
-    // split: A_k = (Z_k + conj Z_{n-k})/2, B_k = (Z_k - conj Z_{n-k})/(2i)
-    // write S[k][kx][jb + 2*pair + {0,1}]
+    // split: A_k = (Z_k + conj Z_{n-k})/2, B_k = (Z_k - conj Z_{n-k})/(2i), rows r0 and r1;
+    // kx < n/2 through the staging tile T[kx][8] in the free half, the Nyquist kx = n/2
+    // directly
+    const int hn = n / 2;
+    C *T = (res == a) ? bhalf : ahalf;
     for (int kx = lt; kx < nh; kx += nt_pair) {
         C z = res[kx], w = res[(n - kx) % n];
         C Av = mkc<C>((z.x + w.x) * (R)0.5, (z.y - w.y) * (R)0.5);
         C Bv = mkc<C>((z.y + w.y) * (R)0.5, (w.x - z.x) * (R)0.5);
-        long long base = ((long long)(k - 1) * nh + kx) * maxy;
-        if (r0 < maxy) spec[base + r0] = Av;
-        if (r1 < maxy) spec[base + r1] = Bv;
+        if (kx < hn) {
+            T[kx * ROWS + 2 * pair] = Av;
+            T[kx * ROWS + 2 * pair + 1] = Bv;
+        } else {
+            const long long base = ((long long)(k - 1) * nh + kx) * maxy;
+            if (r0 < maxy) spec[base + r0] = Av;
+            if (r1 < maxy) spec[base + r1] = Bv;
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < hn * ROWS; e += blockDim.x) {
+        const int kx = e / ROWS, jr = jb + (e - kx * ROWS);
+        if (jr < maxy) spec[((long long)(k - 1) * nh + kx) * maxy + jr] = T[e];
     }
 }
 
@@ -403,28 +423,55 @@ __global__ void tridiag_kernel(DevGrid G, TriArgs T)
     }
     const double wl = __ldg(T.wv + (long long)ky * G.maxx + kx);
     const double *gam = T.gam + (long long)kx * maxy + ky;
-    // forward elimination (TRIDAG2 :219-229), complex rhs solved as its two real parts
-    double bet = dk_of(T, 1, nz, wl);
-    double2 r = ld_spec(s);
-    double2 uprev = make_double2(r.x / bet, r.y / bet);
-    u64[0] = uprev;
-    for (int k = 2; k <= nz; k++) {
-        double g = __ldg(gam + (k - 1) * lstride);
-        double a = __ldg(T.ak + k - 1);
-        bet = dk_of(T, k, nz, wl) - a * g;
-        double2 rk = ld_spec(s + (k - 1) * lstride);
-        double2 u = make_double2((rk.x - a * uprev.x) / bet, (rk.y - a * uprev.y) / bet);
-        u64[(k - 1) * lstride] = u;
-        uprev = u;
+    // forward elimination (TRIDAG2 :219-229), complex rhs solved as its two real parts;
+    // the loads of TB levels are issued together ahead of their dependent chain
+    constexpr int TB = 8;
+    double2 uprev = make_double2(0., 0.);
+    for (int k0 = 1; k0 <= nz; k0 += TB) {
+        double2 rr[TB];
+        double gg[TB];
+#pragma unroll
+        for (int u = 0; u < TB; u++) {
+            const int k = k0 + u;
+            if (k <= nz) {
+                rr[u] = ld_spec(s + (k - 1) * lstride);
+                gg[u] = k >= 2 ? __ldg(gam + (k - 1) * lstride) : 0.;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < TB; u++) {
+            const int k = k0 + u;
+            if (k <= nz) {
+                const double a = k >= 2 ? __ldg(T.ak + k - 1) : 0.;
+                const double bet = k >= 2 ? dk_of(T, k, nz, wl) - a * gg[u] : dk_of(T, 1, nz, wl);
+                const double2 uk = make_double2((rr[u].x - a * uprev.x) / bet, (rr[u].y - a * uprev.y) / bet);
+                u64[(k - 1) * lstride] = uk;
+                uprev = uk;
+            }
+        }
     }
-    // back substitution (:231-233)
+    // back substitution (:231-233), TB levels of loads at a time
     st_spec(s + (nz - 1) * lstride, uprev);
-    for (int k = nz - 1; k >= 1; k--) {
-        double g = __ldg(gam + k * lstride);   // GAM(k+1)
-        double2 uk = u64[(k - 1) * lstride];
-        uk = make_double2(uk.x - g * uprev.x, uk.y - g * uprev.y);
-        st_spec(s + (k - 1) * lstride, uk);
-        uprev = uk;
+    for (int k0 = nz - 1; k0 >= 1; k0 -= TB) {
+        double2 uu[TB];
+        double gg[TB];
+#pragma unroll
+        for (int u = 0; u < TB; u++) {
+            const int k = k0 - u;
+            if (k >= 1) {
+                uu[u] = u64[(k - 1) * lstride];
+                gg[u] = __ldg(gam + k * lstride);   // GAM(k+1)
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < TB; u++) {
+            const int k = k0 - u;
+            if (k >= 1) {
+                const double2 uk = make_double2(uu[u].x - gg[u] * uprev.x, uu[u].y - gg[u] * uprev.y);
+                st_spec(s + (k - 1) * lstride, uk);
+                uprev = uk;
+            }
+        }
     }
 }
 
@@ -459,7 +506,7 @@ struct XInvArgs {
 };
 
 template <typename C>
-__global__ void fft_x_inv(DevGrid G, FftPlan1 P, XInvArgs A)
+__global__ void __launch_bounds__(XT_THREADS, 3) fft_x_inv(DevGrid G, FftPlan1 P, XInvArgs A)
 {
     if (converged(A.sk)) return;
     using R = typename CT<C>::R;
@@ -472,17 +519,31 @@ __global__ void fft_x_inv(DevGrid G, FftPlan1 P, XInvArgs A)
     const int jb = jg * ROWS;
     const int nt_pair = blockDim.x / (ROWS / 2);
     const int pair = threadIdx.x / nt_pair, lt = threadIdx.x % nt_pair;
-    C *a = smc + pair * 2 * n, *b = a + n;
+    C *ahalf = smc, *bhalf = smc + (ROWS / 2) * n;
+    C *a = ahalf + pair * n, *b = bhalf + pair * n;
     const int r0 = jb + 2 * pair, r1 = r0 + 1;
+    // the block's half spectra for kx < n/2, 8 consecutive ky per kx, staged in the b half
+    const int hn = n / 2;
+    for (int e = threadIdx.x; e < hn * ROWS; e += blockDim.x) {
+        const int kx = e / ROWS, jr = jb + (e - kx * ROWS);
+        bhalf[e] = jr < maxy ? spec[((long long)(k - 1) * nh + kx) * maxy + jr] : mkc<C>(0, 0);
+    }
+    __syncthreads();
     // rebuild Z_k = A_k + i B_k over the full circle from the half spectra
     for (int kx = lt; kx < nh; kx += nt_pair) {
-        long long base = ((long long)(k - 1) * nh + kx) * maxy;
-        C Av = r0 < maxy ? spec[base + r0] : mkc<C>(0, 0);
-        C Bv = r1 < maxy ? spec[base + r1] : mkc<C>(0, 0);
+        C Av, Bv;
+        if (kx < hn) {
+            Av = bhalf[kx * ROWS + 2 * pair];
+            Bv = bhalf[kx * ROWS + 2 * pair + 1];
+        } else {
+            const long long base = ((long long)(k - 1) * nh + kx) * maxy;
+            Av = r0 < maxy ? spec[base + r0] : mkc<C>(0, 0);
+            Bv = r1 < maxy ? spec[base + r1] : mkc<C>(0, 0);
+        }
         a[kx] = mkc<C>(Av.x - Bv.y, Av.y + Bv.x);
         if (kx > 0 && kx < n - kx) a[n - kx] = mkc<C>(Av.x + Bv.y, Bv.x - Av.y);
     }
-    __syncthreads();
+    __syncthreads();   // the b half is scratch for the transform from here on
     C *res = stockham<C>(P, a, b, lt, nt_pair, 1);
     for (int t = lt; t < n; t += nt_pair) {
         C z = res[t];
@@ -881,7 +942,7 @@ template <typename C>
 static cudaError_t launch_x_fwd_t(const DevGrid &g, PressurePlan *pp, const XArgs &a, cudaStream_t s)
 {
     int groups = (g.maxy + ROWS - 1) / ROWS;
-    int nt_pair = g.maxx / 8 < 32 ? 32 : (g.maxx / 8 > 256 ? 256 : g.maxx / 8);
+    int nt_pair = g.maxx / 8 < 32 ? 32 : (g.maxx / 8 > XT_THREADS / (ROWS / 2) ? XT_THREADS / (ROWS / 2) : g.maxx / 8);
     size_t sm = (size_t)(ROWS / 2) * 2 * g.maxx * sizeof(C);
     cudaError_t e = cudaFuncSetAttribute(fft_x_fwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
@@ -959,7 +1020,7 @@ static cudaError_t pressure_solve_t(const DevGrid &g, PressurePlan *pp, int keep
     fft_y<C><<<(nrows + YROWS - 1) / YROWS, nt_row * YROWS, smy, s>>>(g, pp->py, pp->spec, nrows, 1, sk);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     int groups = (g.maxy + ROWS - 1) / ROWS;
-    int nt_pair = g.maxx / 8 < 32 ? 32 : (g.maxx / 8 > 256 ? 256 : g.maxx / 8);
+    int nt_pair = g.maxx / 8 < 32 ? 32 : (g.maxx / 8 > XT_THREADS / (ROWS / 2) ? XT_THREADS / (ROWS / 2) : g.maxx / 8);
     size_t smx = (size_t)(ROWS / 2) * 2 * g.maxx * sizeof(C);
     e = cudaFuncSetAttribute(fft_x_inv<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
     if (e != cudaSuccess) return e;

@@ -58,6 +58,7 @@ struct K1Args {
     const double *mw;              // momentum w (stage 1: natural w) for the vertical face velocity
     int mode;                      // 0: stage update; 1: unit mode: xout := ((xout - Tx) - Ty) - Tz
     int *err;                      // device error flag (bounded waits)
+    int xold_is_xin;               // xold[f] == xin[f]: the level-n value is the plane's own cell
 };
 // TMA descriptors of the K1 inputs: haloed planes (38 x 14) of every field, momentum boxes (34 x 9)
 struct alignas(64) K1Maps {
