@@ -37,6 +37,7 @@ struct mg_ctx {
     double *unit[8] = {};                // scratch of the unit-level entry points
     PressurePlan *pp = nullptr;
     K1Maps maps1, maps2;                 // TMA descriptors: stage-1 inputs (level n), stage-2 inputs (working)
+    K2Maps mmaps1, mmaps2;               // TMA descriptors of the K2 stencil momentum, per stage
     int *derr = nullptr;                 // device error flag of bounded waits
     int rep = REP_NAT;
     int have_state = 0;
@@ -175,6 +176,13 @@ int make_field_map(const DevGrid &g, const double *base, int boxx, int boxy, CUt
     return r == CUDA_SUCCESS ? MG_OK : MG_ERR_CUDA;
 }
 
+static int build_mom_maps(mg_ctx *c, const double *const *m3, K2Maps *m)
+{
+    for (int q = 0; q < 3; q++)
+        if (make_field_map(c->G, m3[q], 38, 12, &m->m[q])) return MG_ERR_CUDA;
+    return MG_OK;
+}
+
 static int build_maps(mg_ctx *c, const double *const *x, int nf, const double *mu, const double *mv, K1Maps *m)
 {
     memset(m, 0, sizeof(*m));
@@ -297,7 +305,8 @@ extern "C" int mg_create(const mg_params *params, int device, mg_ctx **out)
     if (e == cudaSuccess) e = k1_mixed_init();
     if (e != cudaSuccess) return fail(cuerr(e));
     if (build_maps(c, c->sA, c->nf, c->mA[0], c->mA[1], &c->maps1) ||
-        build_maps(c, c->sB, c->nf, c->mB[0], c->mB[1], &c->maps2))
+        build_maps(c, c->sB, c->nf, c->mB[0], c->mB[1], &c->maps2) ||
+        build_mom_maps(c, c->mA, &c->mmaps1) || build_mom_maps(c, c->mB, &c->mmaps2))
         return fail(MG_ERR_CUDA);
     // horizontal eigenvalues (get_wv) and the projection plan
     c->wv.resize((size_t)G.maxx * G.maxy);
@@ -500,10 +509,12 @@ static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int wa
         a2.ou = mo[0]; a2.ov = mo[1]; a2.ow = mo[2];
         a2.tu = c->tm[0]; a2.tv = c->tm[1]; a2.tw = c->tm[2];
         a2.mode = 0;
+        a2.err = c->derr;
+        const K2Maps &mm = stage == 1 ? c->mmaps1 : c->mmaps2;
         if (P.precision == MG_PREC_MIXED)
-            PROF(c, "k2_momentum", launch_k2_mixed(G, a2, c->stream));
+            PROF(c, "k2_momentum", launch_k2_mixed(G, a2, mm, c->stream));
         else
-            PROF(c, "k2_momentum", launch_k2(G, a2, c->stream));
+            PROF(c, "k2_momentum", launch_k2(G, a2, mm, c->stream));
         PROF(c, "halo_momentum", launch_halo_fill(G, mo, 3, c->stream));
         *launches += 4;
         // ---- projection ----
@@ -651,7 +662,11 @@ extern "C" int mg_qnadv_uvw(mg_ctx *c, int ntime, const double *mu, const double
     a.ntime = ntime; a.mode = 1; a.in_is_leveln = 0; a.rep = REP_NAT;
     a.mu = c->unit[0]; a.mv = c->unit[1]; a.mw = c->unit[2];
     a.ou = c->unit[3]; a.ov = c->unit[4]; a.ow = c->unit[5];
-    CKR(launch_k2(c->G, a, c->stream));
+    a.err = c->derr;
+    K2Maps mm;
+    const double *m3[3] = {c->unit[0], c->unit[1], c->unit[2]};
+    if (build_mom_maps(c, m3, &mm)) return MG_ERR_CUDA;
+    CKR(c->prm.precision == MG_PREC_MIXED ? launch_k2_mixed(c->G, a, mm, c->stream) : launch_k2(c->G, a, mm, c->stream));
     CKR(d2h(c, au, c->unit[3], cudaMemcpyDeviceToHost));
     CKR(d2h(c, av, c->unit[4], cudaMemcpyDeviceToHost));
     CKR(d2h(c, aw, c->unit[5], cudaMemcpyDeviceToHost));

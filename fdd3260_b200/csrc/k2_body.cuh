@@ -6,12 +6,21 @@
 #include <type_traits>
 #include "mg_common.cuh"
 #include "mimica_gpu.h"
+#include "tma.cuh"
 
 namespace {
 
 constexpr int TX = 32, TY = 8, RH = 2;
 constexpr int PW = TX + 2 * RH, PH = TY + 2 * RH, PL = PW * PH;
 constexpr int NSLOT = 5;
+// raw momentum of one level, three TMA boxes of 38 x 12 doubles: x from cell i0-3 (an
+// even 0-based start, as TMA requires), y from j0-2; ring column c is box column c+1
+constexpr int SBW = TX + 2 * RH + 2, SBH = TY + 2 * RH;
+constexpr int STG_BYTES = SBW * SBH * 8;   // 3648
+constexpr int STG_SLOT = 3712;              // 128-byte multiple
+
+template <typename R> __host__ __device__ constexpr size_t k2_ring_bytes() { return ((size_t)2 * NSLOT * 3 * PL * sizeof(R) + 127) / 128 * 128; }
+template <typename R> __host__ __device__ constexpr size_t k2_smem_bytes() { return k2_ring_bytes<R>() + 3 * STG_SLOT + 128 + 128; }
 constexpr double AVISC = 1. / 16.;   // windadv.f90:39
 
 __device__ __forceinline__ double ldg(const double *p, long long i) { return __ldg(p + i); }
@@ -19,14 +28,17 @@ __device__ __forceinline__ double abs_r(double x) { return fabs(x); }
 __device__ __forceinline__ float abs_r(float x) { return fabsf(x); }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
+__global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const __grid_constant__ K2Maps M)
 {
     // R: type of the stencil arithmetic (FP64 plain form, FP32 mixed form)
     using R = typename std::conditional<MIXED, float, double>::type;
-    extern __shared__ double sm_raw[];
-    R *sm = reinterpret_cast<R *>(sm_raw);
+    extern __shared__ unsigned char sm_raw[];
+    unsigned char *smb = (unsigned char *)(((uintptr_t)sm_raw + 127) & ~(uintptr_t)127);
+    R *sm = reinterpret_cast<R *>(smb);
     R *ring_m = sm;                            // [slot][3][PL] momentum (stencil values)
     R *ring_a = sm + NSLOT * 3 * PL;           // [slot][3][PL] advective velocity
+    double *stg = reinterpret_cast<double *>(smb + k2_ring_bytes<R>());   // [3][SBH][SBW] raw level
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smb + k2_ring_bytes<R>() + 3 * STG_SLOT);
 
     const int ntx = (G.maxx + TX - 1) / TX;
     const int ti = blockIdx.x % ntx, tj = blockIdx.x / ntx;
@@ -45,7 +57,22 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
     const R AVR = (R)AVISC, HALF = (R)0.5, QUART = (R)0.25, FOUR = (R)4., SIX = (R)6.;
     const double *dzw = G.dzw, *dz1w = G.dz1w, *dz1 = G.dz1;
 
-    auto load_level = [&](int l) {
+    if (tid == 0) {
+        mbar_init(mbar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    // raw level l -> staging (single slot; the l-th copy completes phase (l-1)&1)
+    auto issue_raw = [&](int l) {
+        fence_proxy_async_shared();
+        mbar_arrive_expect_tx(mbar, 3 * STG_BYTES);
+        for (int c = 0; c < 3; c++)
+            tma_load_3d(stg + c * (STG_SLOT / 8), &M.m[c], i0 - 4, j0 - 3, l - 1, mbar);
+    };
+    // staging -> ring slot of level l: stencil momentum and advective velocity (zero
+    // outside the domain, as the reference's arrays are read there)
+    auto convert_level = [&](int l) {
+        mbar_wait_bounded(mbar, (uint32_t)((l - 1) & 1), A.err);
         const int slot = l % NSLOT;
         const double d0 = ldg(G.den0, l - 1), a0 = ldg(G.avden0, l - 1);
         for (int q = tid; q < 3 * PL; q += TX * TY) {
@@ -54,10 +81,8 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
             int ii = i0 - RH + c, jj = j0 - RH + r;
             double mv = 0., av = 0.;
             if (ii >= 1 && ii <= nx && jj >= 1 && jj <= ny) {
-                long long idx = gidx(G, ii, jj, l);
-                const double *src = arr == 0 ? A.mu : (arr == 1 ? A.mv : A.mw);
                 double w = arr == 2 ? a0 : d0;
-                double x = ldg(src, idx);
+                double x = stg[arr * (STG_SLOT / 8) + r * SBW + c + 1];
                 mv = A.in_is_leveln ? rep_value(A.rep, x, w) : x;
                 av = mv / w;
                 if (arr == 0) av = av - G.u0shift;
@@ -82,8 +107,15 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
 #define ACC1(acc, a) do { acc = acc + (a); } while (0)
 #define SUB1(acc, a) do { acc = acc - (a); } while (0)
 
-    load_level(1);
-    if (nz >= 2) load_level(2);
+    if (tid == 0) issue_raw(1);
+    convert_level(1);
+    __syncthreads();
+    if (nz >= 2) {
+        if (tid == 0) issue_raw(2);
+        convert_level(2);
+        __syncthreads();
+    }
+    if (tid == 0 && nz >= 3) issue_raw(3);
 
     double bb_prev = 0.;   // buoyancy at level k-1 (cell centre)
     // vertical fluxes carried up the column (each computed once):
@@ -97,10 +129,30 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
     const int own = (ty + RH) * PW + (tx + RH);
 
     for (int k = 1; k <= nz; k++) {
-        __syncthreads();
-        if (k + 2 <= nz) load_level(k + 2);
-        __syncthreads();
+        __syncthreads();   // ring slot (k+2)%5 (level k-3) no longer read
+        if (k + 2 <= nz) convert_level(k + 2);
+        __syncthreads();   // ring complete for level k; the staging slot is free
+        if (tid == 0 && k + 3 <= nz) issue_raw(k + 3);
         if (!act) continue;   // no further barriers in this iteration
+        // epilogue operands of this level, issued before the stencil arithmetic
+        const long long idx = gidx(G, i, j, k);
+        double e_p = 0., e_pw = 0., e_ps = 0., e_dn = 0., e_es = 0., e_qt = 0., e_fes = 0., e_fqt = 0.;
+        double e_tu = 0., e_tv = 0., e_tw = 0., e_un = 0., e_vn = 0., e_wn = 0.;
+        if (A.mode != 1) {
+            e_p = ldg(A.p, idx);
+            e_pw = ldg(A.p, idx - 1);
+            e_ps = ldg(A.p, idx - G.px);
+            if (G.with_buoy) {
+                e_dn = ldg(A.dens, idx);
+                e_es = ldg(A.es, idx);
+                e_fes = ldg(A.fes, idx);
+                if (A.qt) { e_qt = ldg(A.qt, idx); e_fqt = ldg(A.fqt, idx); }
+            }
+            if (A.stage != 1) { e_tu = A.tu[idx]; e_tv = A.tv[idx]; e_tw = A.tw[idx]; }
+            e_un = ldg(A.mu_n, idx);
+            e_vn = ldg(A.mv_n, idx);
+            e_wn = ldg(A.mw_n, idx);
+        }
 #pragma unroll
         for (int d = -2; d <= 2; d++) lb[d + 2] = ring_m + (((k + d + NSLOT) % NSLOT) * 3) * PL + own;
 
@@ -271,7 +323,6 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
             }
         }
 
-        const long long idx = gidx(G, i, j, k);
         if (A.mode == 1) {
             A.ou[idx] = au;
             A.ov[idx] = av;
@@ -281,9 +332,9 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
 
         // ---------------- explicit pressure gradient (gradp on p/rho0) ----------------
         const double d0 = ldg(G.den0, k - 1), a0 = ldg(G.avden0, k - 1);
-        const double ppc = ldg(A.p, idx) / d0;
-        const double gpx = (ppc - ldg(A.p, gidx(G, i - 1, j, k)) / d0) * dx1d;
-        const double gpy = (ppc - ldg(A.p, gidx(G, i, j - 1, k)) / d0) * dy1d;
+        const double ppc = e_p / d0;
+        const double gpx = (ppc - e_pw / d0) * dx1d;
+        const double gpy = (ppc - e_ps / d0) * dy1d;
         double gpz;
         if (k >= 2) gpz = (ppc - pp_below) * ldg(dz1, k - 2);
         else gpz = (double)MM(2, 0, 0, 0) / (dt0 * ldg(G.avden0, 0));
@@ -295,14 +346,14 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
         // ---------------- buoyancy (imp_buoy: state + cdiag*dt0*states) ----------------
         double buoy = 0.;
         if (G.with_buoy) {
-            double dn = ldg(A.dens, idx);
-            double esv = ldg(A.es, idx), qtv = A.qt ? ldg(A.qt, idx) : 0.;
+            double dn = e_dn;
+            double esv = e_es, qtv = A.qt ? e_qt : 0.;
             if (A.dens_is_leveln) {
                 esv = rep_value(A.rep, esv, dn);
                 if (A.qt) qtv = rep_value(A.rep, qtv, dn);
             }
-            double est = esv + cdiag * dt0 * ldg(A.fes, idx);
-            double qtt = A.qt ? qtv + cdiag * dt0 * ldg(A.fqt, idx) : 0.;
+            double est = esv + cdiag * dt0 * e_fes;
+            double qtt = A.qt ? qtv + cdiag * dt0 * e_fqt : 0.;
             double den1 = 1. / dn;
             double pt = den1 * est;
             double sumh = 0.;
@@ -316,13 +367,13 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A)
         wsu = -au + wsu;
         wsv = -av + wsv;
         wsw = -aw + wsw + buoy;
-        double tu_o = A.stage == 1 ? 0. : A.tu[idx];
-        double tv_o = A.stage == 1 ? 0. : A.tv[idx];
-        double tw_o = A.stage == 1 ? 0. : A.tw[idx];
+        double tu_o = A.stage == 1 ? 0. : e_tu;
+        double tv_o = A.stage == 1 ? 0. : e_tv;
+        double tw_o = A.stage == 1 ? 0. : e_tw;
         double tu = wsu + A.b * tu_o, tv = wsv + A.b * tv_o, tw = wsw + A.b * tw_o;
-        double un = rep_value(A.rep, ldg(A.mu_n, idx), d0);
-        double vn = rep_value(A.rep, ldg(A.mv_n, idx), d0);
-        double wn = rep_value(A.rep, ldg(A.mw_n, idx), a0);
+        double un = rep_value(A.rep, e_un, d0);
+        double vn = rep_value(A.rep, e_vn, d0);
+        double wn = rep_value(A.rep, e_wn, a0);
         A.ou[idx] = un + A.a_dt * tu;
         A.ov[idx] = vn + A.a_dt * tv;
         A.ow[idx] = 1. * (wn + A.a_dt * tw);

@@ -3,12 +3,12 @@
 // k2_body.cuh.
 #include "k2_body.cuh"
 
-cudaError_t launch_k2_mixed(const DevGrid &g, const K2Args &a, cudaStream_t s)
+cudaError_t launch_k2_mixed(const DevGrid &g, const K2Args &a, const K2Maps &maps, cudaStream_t s)
 {
     int ntx = (g.maxx + TX - 1) / TX, nty = (g.maxy + TY - 1) / TY;
-    size_t sm = (size_t)2 * NSLOT * 3 * PL * sizeof(float);
+    const size_t sm = k2_smem_bytes<float>();
     cudaError_t e = cudaFuncSetAttribute(k2_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    k2_kernel<true><<<ntx * nty, dim3(TX, TY), sm, s>>>(g, a);
+    k2_kernel<true><<<ntx * nty, dim3(TX, TY), sm, s>>>(g, a, maps);
     return cudaGetLastError();
 }

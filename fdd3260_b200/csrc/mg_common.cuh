@@ -82,6 +82,11 @@ struct K2Args {
     double *ou, *ov, *ow;          // new momentum
     double *tu, *tv, *tw;          // tendency accumulators
     int mode;                      // 0: full stage; 1: unit mode: ou/ov/ow := advection tendency only
+    int *err;                      // device error flag (bounded waits)
+};
+// TMA descriptors of the K2 stencil momentum (boxes of 38 x 12 doubles)
+struct alignas(64) K2Maps {
+    CUtensorMap m[3];
 };
 
 // launch wrappers (implemented in the .cu files)
@@ -92,8 +97,8 @@ cudaError_t k1_mixed_init();
 size_t k1_smem_bytes(int scheme, int nf);
 // TMA descriptor of one field buffer (box in doubles)
 int make_field_map(const DevGrid &g, const double *base, int boxx, int boxy, CUtensorMap *map);
-cudaError_t launch_k2(const DevGrid &g, const K2Args &a, cudaStream_t s);
-cudaError_t launch_k2_mixed(const DevGrid &g, const K2Args &a, cudaStream_t s);
+cudaError_t launch_k2(const DevGrid &g, const K2Args &a, const K2Maps &maps, cudaStream_t s);
+cudaError_t launch_k2_mixed(const DevGrid &g, const K2Args &a, const K2Maps &maps, cudaStream_t s);
 cudaError_t launch_halo_fill(const DevGrid &g, double *const *fields, int nf, cudaStream_t s);
 
 // projection
