@@ -1,7 +1,14 @@
 // k1_body.cuh -- body of the K1 kernel (scalar advection + stage update), templated
-// on the scheme and on the arithmetic form; instantiated by k_scalar.cu (plain FP64,
-// compiled without FMA contraction) and k_scalar_mixed.cu (FP32 scheme logic on
+// on the scheme, the arithmetic form and the stage; instantiated by k_scalar.cu (plain
+// FP64, compiled without FMA contraction) and k_scalar_mixed.cu (FP32 scheme logic on
 // differences, FP64 fluxes and state).
+//
+// One CTA (288 threads: 8 cell warps + 1 helper warp) owns a 32 x 8 column tile and
+// marches up k.  Per level, the fields are processed in groups of PF (2 for WENO and
+// MUSCL, 1 for PPM, whose per-field reconstruction arrays are large): the haloed planes
+// of a group arrive by TMA (NPS group slots in flight), their x/y faces are computed as
+// independent chains, one barrier publishes them, then each cell thread finishes the
+// vertical face and the stage update of every field of the group.
 #pragma once
 #include "mg_common.cuh"
 #include "schemes.cuh"
@@ -14,12 +21,18 @@ constexpr int SW = TX + 2 * H, SH = TY + 2 * H;   // haloed plane box 38 x 14
 constexpr int NT = TX * (TY + 1);                 // 288 threads: 8 cell warps + 1 helper warp
 constexpr int PLANE_BYTES = SW * SH * 8;          // 4256
 constexpr int PLANE_SLOT = 4352;                  // 128-byte multiple
-constexpr int NP = 4;                             // plane slots: NP-1 items of TMA look-ahead
-constexpr int MB_VEL = NP;                        // mbarrier of the momentum boxes
 constexpr int VW = 34, VH = 9;                    // momentum box (x from i0-1, y from j0)
 constexpr int VBOX_BYTES = VW * VH * 8;           // 2448
 constexpr int VBOX_SLOT = 2560;
 constexpr int NCELL = TX * TY;
+constexpr int FXN = TY * (TX + 1), FYN = (TY + 1) * TX;   // x faces, y faces of one field
+constexpr int NHALO = SW * SH - TX * TY;          // 276 plane elements outside the cells
+
+// fields per group, group slots of planes in flight, face buffers (parity-double-buffered
+// when a group is one field, single otherwise: an extra barrier then guards reuse)
+__host__ __device__ constexpr int k1_pf(int scheme) { return scheme == MG_PPM ? 1 : 2; }
+__host__ __device__ constexpr int k1_nps(int scheme) { return scheme == MG_PPM ? 4 : 2; }
+__host__ __device__ constexpr int k1_nfb(int scheme) { return k1_pf(scheme) == 1 ? 2 : 1; }
 
 struct Layout {
     int zs;             // z-ring slots
@@ -29,16 +42,17 @@ struct Layout {
 __host__ __device__ inline Layout make_layout(int scheme, int nf)
 {
     Layout L;
+    const int PF = k1_pf(scheme), NPS = k1_nps(scheme), NFB = k1_nfb(scheme);
     L.zs = scheme == MG_PPM ? 5 : 4;   // window x(k-1..k+L), L = 3 (PPM) or 2
     size_t o = 0;
-    L.planes = o; o += NP * PLANE_SLOT;
+    L.planes = o; o += (size_t)NPS * PF * PLANE_SLOT;
     L.vbu = o; o += VBOX_SLOT;
     L.vbv = o; o += VBOX_SLOT;
     L.densp = o; o += PLANE_SLOT;
     L.su = o; o += TY * (TX + 1) * 8;
     L.sv = o; o += (TY + 1) * TX * 8;
-    L.fx = o; o += 2 * TY * (TX + 1) * 8;   // double-buffered by item parity
-    L.fy = o; o += 2 * (TY + 1) * TX * 8;
+    L.fx = o; o += (size_t)NFB * PF * FXN * 8;
+    L.fy = o; o += (size_t)NFB * PF * FYN * 8;
     o = (o + 127) / 128 * 128;
     L.mbar = o; o += 128;
     L.zring = o; o += (size_t)nf * L.zs * NCELL * 8;
@@ -49,8 +63,8 @@ __host__ __device__ inline Layout make_layout(int scheme, int nf)
     L.cry = o;
     if (scheme == MG_PPM) {
         o += (size_t)2 * nf * NCELL * 8;
-        L.crx = o; o += 2 * 4 * TY * (TX + 2) * 8;   // double-buffered by item parity
-        L.cry = o; o += 2 * 4 * (TY + 2) * TX * 8;
+        L.crx = o; o += (size_t)NFB * 4 * TY * (TX + 2) * 8;
+        L.cry = o; o += (size_t)NFB * 4 * (TY + 2) * TX * 8;
     }
     L.total = o + 128;   // slack for 128-byte alignment of the base
     return L;
@@ -58,9 +72,25 @@ __host__ __device__ inline Layout make_layout(int scheme, int nf)
 
 __device__ __forceinline__ double ldg(const double *p, long long i) { return __ldg(p + i); }
 
-template <int SCHEME, bool MIXED>
-__global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __grid_constant__ K1Maps M)
+// plane element of halo index h in [0, NHALO): rows 0..2 and 11..13, then the halo
+// columns of the cell rows
+__device__ __forceinline__ int halo_elem(int h)
 {
+    if (h < 2 * H * SW) {
+        const int r = h / SW, c = h - r * SW;
+        return (r < H ? r : r + TY) * SW + c;
+    }
+    const int h2 = h - 2 * H * SW, r = h2 / (2 * H), cc = h2 - r * (2 * H);
+    return (r + H) * SW + (cc < H ? cc : cc + TX);
+}
+
+// STAGE 1, 2: Heun stage update of density + density-weighted scalars (field 0 is the
+// density); STAGE 0: unit mode (advection_ac of one field, xout := ((xout-Tx)-Ty)-Tz)
+template <int SCHEME, bool MIXED, int STAGE>
+__global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __grid_constant__ K1Maps M)
+{
+    constexpr int PF = k1_pf(SCHEME), NPS = k1_nps(SCHEME), NFB = k1_nfb(SCHEME);
+    constexpr bool CONV1 = STAGE == 1;   // stage-1 inputs are natural: psi = s * rho
     extern __shared__ unsigned char smraw[];
     unsigned char *sm = (unsigned char *)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
     const int F = A.nf;
@@ -72,7 +102,7 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
     double *densp = (double *)(sm + Ly.densp);
     double *su = (double *)(sm + Ly.su), *sv = (double *)(sm + Ly.sv);
     double *fx = (double *)(sm + Ly.fx), *fy = (double *)(sm + Ly.fy);
-    uint64_t *mb = (uint64_t *)(sm + Ly.mbar);    // [0, NP) planes, [NP] momentum boxes
+    uint64_t *mb = (uint64_t *)(sm + Ly.mbar);    // [0, NPS) plane groups, [NPS] momentum boxes
     double *zring = (double *)(sm + Ly.zring), *wring = (double *)(sm + Ly.wring);
     double *zf = (double *)(sm + Ly.zf);
     double *chain = (double *)(sm + Ly.chain);   // PPM: [0][f] Fr of the cell below, [1][f] its xplus
@@ -88,22 +118,28 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
     const bool act = cellt && (i <= nx - 2) && (j <= ny - 2);
     const int ic = min(i, nx - 2), jc = min(j, ny - 2);
     const int cid = ty * TX + tx;   // cell slot (valid for cell threads)
+    const int own_e = (ty + H) * SW + tx + H;   // own cell in a plane (cell threads)
     const double dx1 = 1. / G.dx, dy1 = 1. / G.dy, dt0 = G.dt0;
-    const bool conv1 = (A.stage == 1);   // stage-1 inputs are natural: psi = s * rho
-    const int total_items = nz * F;
+    const bool conv1 = CONV1;
+    const int NG = (F + PF - 1) / PF;      // field groups per level
+    const int total_groups = nz * NG;
+    const int MB_VEL = NPS;
 
     if (tid == 0) {
-        for (int b = 0; b <= NP; b++) mbar_init(&mb[b], 1);
+        for (int b = 0; b <= NPS; b++) mbar_init(&mb[b], 1);
         fence_mbar_init();
     }
     __syncthreads();
 
-    auto issue_plane = [&](int q) {   // item q = (k-1)*F + f
-        const int k = q / F + 1, f = q % F;
-        double *dst = planes + (q % NP) * (PLANE_SLOT / 8);
+    auto issue_group = [&](int qg) {   // group qg = (k-1)*NG + g: planes of fields g*PF ..
+        const int k = qg / NG + 1, g = qg - (k - 1) * NG;
+        const int slot = qg % NPS;
+        const int nfg = min(PF, F - g * PF);
         fence_proxy_async_shared();
-        mbar_arrive_expect_tx(&mb[q % NP], PLANE_BYTES);
-        tma_load_3d(dst, &M.x[f], i0 - 4, j0 - 4, k - 1, &mb[q % NP]);
+        mbar_arrive_expect_tx(&mb[slot], nfg * PLANE_BYTES);
+        for (int u = 0; u < nfg; u++)
+            tma_load_3d(planes + (size_t)(slot * PF + u) * (PLANE_SLOT / 8), &M.x[g * PF + u], i0 - 4, j0 - 4, k - 1,
+                        &mb[slot]);
     };
     auto issue_vel = [&](int k) {
         fence_proxy_async_shared();
@@ -122,7 +158,7 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
     };
 
     if (tid == 0) {
-        for (int q0 = 0; q0 < NP - 1 && q0 < total_items; q0++) issue_plane(q0);
+        for (int q0 = 0; q0 < NPS - 1 && q0 < total_groups; q0++) issue_group(q0);
         issue_vel(1);
     }
     for (int l = 1; l <= L + 1; l++) issue_z(l);
@@ -134,25 +170,29 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
         for (int f = 0; f < F; f++) zf[f * NCELL + cid] = 0.;
 
     int zsl[L + 2];   // z-ring slot of level k-1+m, refreshed per level
-    // stencil value of a field at level l = k-1+m of the own column
-// (stage 1 with density first: the other fields' entries are multiplied by the density
-// entry of the same level once, when the level arrives)
+    // stencil value of a field at level l = k-1+m of the own column (stage 1: the other
+    // fields' entries are multiplied by the density entry of the same level once, when
+    // the level arrives)
 #define ZVAL(f, m) (zring[((f) * ZS + zsl[(m)]) * NCELL + cid])
     auto wval = [&](int m) -> double {   // w_adv at level k-1+m of the own column
         const double a0 = ldg(G.avden0, k_cur - 2 + m);
-        double x = wring[zsl[m] * NCELL + cid];
+        double x = wring[((k_cur - 1 + m) % ZS) * NCELL + cid];
         if (conv1) x = x * a0;
         return x / a0;
     };
 
     double wz2 = 0., wz3 = 0.;   // w_adv of the own column at levels k+1 and k+2
-    // register prefetch of the epilogue operands (stage 2 / unit mode), one item ahead
+    // stage 2: level-n value and tendency of the group's fields, loaded one group ahead
     const long long idx0 = gidx(G, ic, jc, 1);
-    const bool pf_loads = A.mode == 0 && (!A.xold_is_xin || A.stage == 2);
-    double nx_xold = 0., nx_tend = 0.;
-    if (pf_loads && act) {
-        if (!A.xold_is_xin) nx_xold = ldg(A.xold[0], idx0);
-        if (A.stage == 2) nx_tend = ldg(A.tend[0], idx0);
+    double nx_xold[PF], nx_tend[PF];
+#pragma unroll
+    for (int u = 0; u < PF; u++) {
+        nx_xold[u] = 0.;
+        nx_tend[u] = 0.;
+        if (STAGE == 2 && act && u < F) {
+            nx_xold[u] = ldg(A.xold[u], idx0);
+            nx_tend[u] = ldg(A.tend[u], idx0);
+        }
     }
     for (int k = 1; k <= nz; k++) {
         k_cur = k;
@@ -178,55 +218,65 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
         }
         __syncthreads();   // su/sv complete; the momentum boxes are free again
         if (tid == 0 && k + 1 <= nz) issue_vel(k + 1);
-        for (int f = 0; f < F; f++) {
-            const int q = (k - 1) * F + f;
-            // epilogue operands of this item (loaded one item ahead), then the loads of the
-            // next item's, which complete while this item's faces are computed
-            const double cur_xold = nx_xold, cur_tend = nx_tend;
-            if (pf_loads && act && q + 1 < total_items) {
-                const int fn = f + 1 < F ? f + 1 : 0, kn = f + 1 < F ? k : k + 1;
-                const long long idn = idx0 + (long long)(kn - 1) * G.ps;
-                if (!A.xold_is_xin) nx_xold = ldg(A.xold[fn], idn);
-                if (A.stage == 2) nx_tend = ldg(A.tend[fn], idn);
+        for (int g = 0; g < NG; g++) {
+            const int qg = (k - 1) * NG + g, gb = g * PF;
+            // this group's stage-2 operands, then the next group's loads (they complete
+            // while this group's faces are computed)
+            double cur_xold[PF], cur_tend[PF];
+#pragma unroll
+            for (int u = 0; u < PF; u++) {
+                cur_xold[u] = nx_xold[u];
+                cur_tend[u] = nx_tend[u];
             }
-            // slot (q+NP-1)%NP last held item q-1, whose faces all threads finished
-            // before the face barrier of item q-1
-            if (tid == 0 && q + NP - 1 < total_items) issue_plane(q + NP - 1);
-            mbar_wait_bounded(&mb[q % NP], (uint32_t)((q / NP) & 1), A.err);
-            const double *pl = planes + (q % NP) * (PLANE_SLOT / 8);
-            // level-n value of the own cell when it is the plane's.  Stage 1 then turns
-            // the plane into psi = s * rho in place (the density plane of the level is kept
-            // for the other fields): each cell thread scales its own element right after
-            // reading it, the 276 halo elements are shared out, one barrier follows.
-            const int own_e = (ty + H) * SW + tx + H;
-            const double plane_xo = cellt ? pl[own_e] : 0.;
-            const bool wconv = conv1 && A.dens_first && f > 0;
-            if (conv1 && A.dens_first) {
-                double *plw = planes + (q % NP) * (PLANE_SLOT / 8);
-                if (f == 0) {
-                    for (int e = tid; e < SW * SH; e += NT) densp[e] = pl[e];
-                } else {
-                    if (cellt) plw[own_e] = plane_xo * densp[own_e];
-                    constexpr int NHALO = SW * SH - TX * TY;   // 276
-                    for (int h = tid; h < NHALO; h += NT) {
-                        int e;
-                        if (h < 2 * H * SW) {   // halo rows 0..2 and 11..13
-                            const int r = h / SW, c = h - r * SW;
-                            e = (r < H ? r : r + TY) * SW + c;
-                        } else {                 // halo columns of the cell rows
-                            const int h2 = h - 2 * H * SW, r = h2 / (2 * H), cc = h2 - r * (2 * H);
-                            e = (r + H) * SW + (cc < H ? cc : cc + TX);
-                        }
-                        plw[e] = plw[e] * densp[e];
+            if (STAGE == 2 && act && qg + 1 < total_groups) {
+                const int gn = g + 1 < NG ? g + 1 : 0, kn = g + 1 < NG ? k : k + 1;
+                const long long idn = idx0 + (long long)(kn - 1) * G.ps;
+#pragma unroll
+                for (int u = 0; u < PF; u++)
+                    if (gn * PF + u < F) {
+                        nx_xold[u] = ldg(A.xold[gn * PF + u], idn);
+                        nx_tend[u] = ldg(A.tend[gn * PF + u], idn);
                     }
-                    __syncthreads();
+            }
+            // slot (qg+NPS-1)%NPS last held group qg-1, whose faces all threads finished
+            // before the face barrier of group qg-1
+            if (tid == 0 && qg + NPS - 1 < total_groups) issue_group(qg + NPS - 1);
+            mbar_wait_bounded(&mb[qg % NPS], (uint32_t)((qg / NPS) & 1), A.err);
+            double *plq = planes + (size_t)(qg % NPS) * PF * (PLANE_SLOT / 8);
+            // level-n values of the own cell (stage 1: they are the planes' own elements,
+            // read before the density products below)
+            double plane_xo[PF];
+#pragma unroll
+            for (int u = 0; u < PF; u++) plane_xo[u] = (cellt && gb + u < F) ? plq[u * (PLANE_SLOT / 8) + own_e] : 0.;
+            if constexpr (CONV1) {
+                // psi = s * rho in place, once per element: each cell thread scales its own
+                // element, the halo elements are shared out.  Group 0 holds the density
+                // (field 0), which is kept in densp for the later groups of the level.
+#pragma unroll
+                for (int u = 0; u < PF; u++) {
+                    const int f = gb + u;
+                    if (f >= F) continue;
+                    double *plw = plq + u * (PLANE_SLOT / 8);
+                    if (f == 0) {
+                        for (int e = tid; e < SW * SH; e += NT) densp[e] = plw[e];
+                    } else {
+                        const double *dsrc = g == 0 ? plq : densp;   // group 0: the density plane itself
+                        if (cellt) plw[own_e] = plane_xo[u] * dsrc[own_e];
+                        for (int h = tid; h < NHALO; h += NT) {
+                            const int e = halo_elem(h);
+                            plw[e] = plw[e] * dsrc[e];
+                        }
+                    }
                 }
             }
-            double *fxq = fx + (q & 1) * TY * (TX + 1), *fyq = fy + (q & 1) * (TY + 1) * TX;
-            double *crxq = crx + (q & 1) * 4 * TY * (TX + 2), *cryq = cry + (q & 1) * 4 * (TY + 2) * TX;
-            (void)wconv;
-            auto V = [&](int e) -> double { return pl[e]; };
-            if (SCHEME == MG_PPM) {
+            if ((CONV1 && (PF == 2 || g > 0)) || NFB == 1) __syncthreads();
+            double *fxb = fx + (NFB == 2 ? (qg & 1) : 0) * PF * FXN;
+            double *fyb = fy + (NFB == 2 ? (qg & 1) : 0) * PF * FYN;
+            double *crxq = crx + (NFB == 2 ? (qg & 1) : 0) * 4 * TY * (TX + 2);
+            double *cryq = cry + (NFB == 2 ? (qg & 1) : 0) * 4 * (TY + 2) * TX;
+            if constexpr (SCHEME == MG_PPM) {
+                const double *pl = plq;
+                auto V = [&](int e) -> double { return pl[e]; };
                 for (int qq = tid; qq < TY * (TX + 2) + (TY + 2) * TX; qq += NT) {
                     double xv[5], pr = 0., pL = 0., p1 = 0., p2 = 0.;
                     if (qq < TY * (TX + 2)) {
@@ -266,241 +316,253 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
                 }
                 __syncthreads();
             }
-            // x face (threads 0..263: (TX+1)*TY faces) and y face (all 288 threads:
-            // TX*(TY+1) faces), written as two independent chains for instruction-level
-            // parallelism
-            {
-                const bool hasx = tid < TY * (TX + 1);
-                const int rx = hasx ? tid / (TX + 1) : 0, cx = hasx ? tid - rx * (TX + 1) : 0;
-                const int ry = tid / TX, cy = tid - ry * TX;
-                const double uu = su[hasx ? tid : 0], vv = sv[tid];
-                const int bx = (rx + H) * SW + H + cx - 1;   // x(i0 + cx - 1) in row rx
-                const int by = (ry - 1 + H) * SW + H + cy;   // x(j0 + ry - 1) in column cy
-                double Fx, Fy;
-                if (SCHEME == MG_WENO) {
-                    if constexpr (MIXED) {
-                        Fx = weno_face_mixed(V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu, true);
-                        Fy = weno_face_mixed(V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv, true);
-                    } else {
-                        Fx = weno_face(V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu, true);
-                        Fy = weno_face(V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv, true);
+#pragma unroll
+            for (int u = 0; u < PF; u++) {
+                if (PF > 1 && gb + u >= F) continue;
+                const double *pl = plq + u * (PLANE_SLOT / 8);
+                auto V = [&](int e) -> double { return pl[e]; };
+                double *fxq = fxb + u * FXN, *fyq = fyb + u * FYN;
+                    // x face (threads 0..263: (TX+1)*TY faces) and y face (all 288 threads:
+                    // TX*(TY+1) faces), written as two independent chains for instruction-level
+                    // parallelism
+                    {
+                        const bool hasx = tid < TY * (TX + 1);
+                        const int rx = hasx ? tid / (TX + 1) : 0, cx = hasx ? tid - rx * (TX + 1) : 0;
+                        const int ry = tid / TX, cy = tid - ry * TX;
+                        const double uu = su[hasx ? tid : 0], vv = sv[tid];
+                        const int bx = (rx + H) * SW + H + cx - 1;   // x(i0 + cx - 1) in row rx
+                        const int by = (ry - 1 + H) * SW + H + cy;   // x(j0 + ry - 1) in column cy
+                        double Fx, Fy;
+                        if (SCHEME == MG_WENO) {
+                            if constexpr (MIXED) {
+                                Fx = weno_face_mixed(V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu, true);
+                                Fy = weno_face_mixed(V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv, true);
+                            } else {
+                                Fx = weno_face(V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu, true);
+                                Fy = weno_face(V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv, true);
+                            }
+                        } else if (SCHEME == MG_MUSCL) {
+                            if constexpr (MIXED) {
+                                Fx = muscl_face_h_mixed(G.muscl_lim, (float)G.lim_tol, (float)G.dx, (float)dx1, V(bx - 1), V(bx),
+                                                        V(bx + 1), V(bx + 2), uu);
+                                Fy = muscl_face_h_mixed(G.muscl_lim, (float)G.lim_tol, (float)G.dy, (float)dy1, V(by - SW), V(by),
+                                                        V(by + SW), V(by + 2 * SW), vv);
+                            } else {
+                                Fx = muscl_face_h(G.muscl_lim, G.lim_tol, G.dx, dx1, V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu);
+                                Fy = muscl_face_h(G.muscl_lim, G.lim_tol, G.dy, dy1, V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv);
+                            }
+                        } else if constexpr (MIXED) {
+                            // relative reconstructions: cell base values from the plane
+                            const double mux = fabs(uu) * dt0 * dx1;
+                            const int o0 = rx * (TX + 2) + cx, o1 = o0 + 1, S = TY * (TX + 2);
+                            const float frx = ppm_fr((float)crxq[o0], (float)mux, (float)crxq[2 * S + o0], (float)crxq[3 * S + o0]);
+                            const float flx = ppm_fl((float)crxq[S + o1], (float)mux, (float)crxq[2 * S + o1], (float)crxq[3 * S + o1]);
+                            Fx = uu > 0. ? uu * (V(bx) + (double)frx) : (uu < 0. ? uu * (V(bx + 1) + (double)flx) : 0.);
+                            const double muy = fabs(vv) * dt0 * dy1;
+                            const int p0 = ry * TX + cy, p1 = p0 + TX, Sy = (TY + 2) * TX;
+                            const float fry = ppm_fr((float)cryq[p0], (float)muy, (float)cryq[2 * Sy + p0], (float)cryq[3 * Sy + p0]);
+                            const float fly = ppm_fl((float)cryq[Sy + p1], (float)muy, (float)cryq[2 * Sy + p1], (float)cryq[3 * Sy + p1]);
+                            Fy = vv > 0. ? vv * (V(by) + (double)fry) : (vv < 0. ? vv * (V(by + SW) + (double)fly) : 0.);
+                        } else {
+                            const double mux = fabs(uu) * dt0 * dx1;
+                            const int o0 = rx * (TX + 2) + cx, o1 = o0 + 1, S = TY * (TX + 2);
+                            const double frx = ppm_fr(crxq[o0], mux, crxq[2 * S + o0], crxq[3 * S + o0]);
+                            const double flx = ppm_fl(crxq[S + o1], mux, crxq[2 * S + o1], crxq[3 * S + o1]);
+                            Fx = 0.5 * frx * (uu + fabs(uu)) + 0.5 * flx * (uu - fabs(uu));
+                            const double muy = fabs(vv) * dt0 * dy1;
+                            const int p0 = ry * TX + cy, p1 = p0 + TX, Sy = (TY + 2) * TX;
+                            const double fry = ppm_fr(cryq[p0], muy, cryq[2 * Sy + p0], cryq[3 * Sy + p0]);
+                            const double fly = ppm_fl(cryq[Sy + p1], muy, cryq[2 * Sy + p1], cryq[3 * Sy + p1]);
+                            Fy = 0.5 * fry * (vv + fabs(vv)) + 0.5 * fly * (vv - fabs(vv));
+                        }
+                        if (hasx) fxq[tid] = Fx;
+                        fyq[tid] = Fy;
                     }
-                } else if (SCHEME == MG_MUSCL) {
-                    if constexpr (MIXED) {
-                        Fx = muscl_face_h_mixed(G.muscl_lim, (float)G.lim_tol, (float)G.dx, (float)dx1, V(bx - 1), V(bx),
-                                                V(bx + 1), V(bx + 2), uu);
-                        Fy = muscl_face_h_mixed(G.muscl_lim, (float)G.lim_tol, (float)G.dy, (float)dy1, V(by - SW), V(by),
-                                                V(by + SW), V(by + 2 * SW), vv);
-                    } else {
-                        Fx = muscl_face_h(G.muscl_lim, G.lim_tol, G.dx, dx1, V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu);
-                        Fy = muscl_face_h(G.muscl_lim, G.lim_tol, G.dy, dy1, V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv);
-                    }
-                } else if constexpr (MIXED) {
-                    // relative reconstructions: cell base values from the plane
-                    const double mux = fabs(uu) * dt0 * dx1;
-                    const int o0 = rx * (TX + 2) + cx, o1 = o0 + 1, S = TY * (TX + 2);
-                    const float frx = ppm_fr((float)crxq[o0], (float)mux, (float)crxq[2 * S + o0], (float)crxq[3 * S + o0]);
-                    const float flx = ppm_fl((float)crxq[S + o1], (float)mux, (float)crxq[2 * S + o1], (float)crxq[3 * S + o1]);
-                    Fx = uu > 0. ? uu * (V(bx) + (double)frx) : (uu < 0. ? uu * (V(bx + 1) + (double)flx) : 0.);
-                    const double muy = fabs(vv) * dt0 * dy1;
-                    const int p0 = ry * TX + cy, p1 = p0 + TX, Sy = (TY + 2) * TX;
-                    const float fry = ppm_fr((float)cryq[p0], (float)muy, (float)cryq[2 * Sy + p0], (float)cryq[3 * Sy + p0]);
-                    const float fly = ppm_fl((float)cryq[Sy + p1], (float)muy, (float)cryq[2 * Sy + p1], (float)cryq[3 * Sy + p1]);
-                    Fy = vv > 0. ? vv * (V(by) + (double)fry) : (vv < 0. ? vv * (V(by + SW) + (double)fly) : 0.);
-                } else {
-                    const double mux = fabs(uu) * dt0 * dx1;
-                    const int o0 = rx * (TX + 2) + cx, o1 = o0 + 1, S = TY * (TX + 2);
-                    const double frx = ppm_fr(crxq[o0], mux, crxq[2 * S + o0], crxq[3 * S + o0]);
-                    const double flx = ppm_fl(crxq[S + o1], mux, crxq[2 * S + o1], crxq[3 * S + o1]);
-                    Fx = 0.5 * frx * (uu + fabs(uu)) + 0.5 * flx * (uu - fabs(uu));
-                    const double muy = fabs(vv) * dt0 * dy1;
-                    const int p0 = ry * TX + cy, p1 = p0 + TX, Sy = (TY + 2) * TX;
-                    const double fry = ppm_fr(cryq[p0], muy, cryq[2 * Sy + p0], cryq[3 * Sy + p0]);
-                    const double fly = ppm_fl(cryq[Sy + p1], muy, cryq[2 * Sy + p1], cryq[3 * Sy + p1]);
-                    Fy = 0.5 * fry * (vv + fabs(vv)) + 0.5 * fly * (vv - fabs(vv));
-                }
-                if (hasx) fxq[tid] = Fx;
-                fyq[tid] = Fy;
             }
-            __syncthreads();   // faces of item q complete
+            __syncthreads();   // faces of group qg complete
             if (!cellt) continue;
 
-            const double Tx = (fxq[ty * (TX + 1) + tx + 1] - fxq[ty * (TX + 1) + tx]) * dx1;
-            const double Ty = (fyq[(ty + 1) * TX + tx] - fyq[ty * TX + tx]) * dy1;
-
-            // ---- vertical face k+1/2 of the own column ----
-            if (f == 0) {
+            // ---- vertical faces k+1/2 of the own column ----
+            if (g == 0) {
                 cp_async_wait_all();
-                if (conv1 && A.dens_first) {
+                if (conv1) {
                     // newly arrived levels: 1..L+1 at k = 1, else k+L
                     const int m_lo = k == 1 ? 1 : L + 1;
                     for (int m = m_lo; m <= L + 1; m++) {
                         if (k - 1 + m > nz) break;
                         const int sl = (k - 1 + m) % ZS;
                         const double dn = zring[sl * NCELL + cid];
-                        for (int g = 1; g < F; g++) zring[(g * ZS + sl) * NCELL + cid] *= dn;
+                        for (int gg = 1; gg < F; gg++) zring[(gg * ZS + sl) * NCELL + cid] *= dn;
                     }
                 }
                 wz2 = k <= nz - 1 ? wval(2) : 0.;
                 if (SCHEME == MG_PPM) wz3 = k + 2 <= nz ? wval(3) : 0.;
             }
-            const double dzw1 = ldg(G.dz1w, k - 1);
-            double Fzn = 0.;
-            double *zfo = &zf[f * NCELL + cid];
-            if (k <= nz - 1) {
-                const double ww = wz2;
-                if (SCHEME == MG_WENO) {
-                    if constexpr (MIXED) {
-                        if (k == 1) Fzn = weno_face_bottom_mixed(ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww);
-                        else if (k == nz - 1) Fzn = weno_face_top_mixed(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ww);
-                        else Fzn = weno_face_mixed(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww, (k >= 3 && k <= nz - 3));
-                    } else {
-                        if (k == 1) Fzn = weno_face_bottom(ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww);
-                        else if (k == nz - 1) Fzn = weno_face_top(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ww);
-                        else Fzn = weno_face(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww, (k >= 3 && k <= nz - 3));
-                    }
-                } else if (SCHEME == MG_MUSCL) {
-                    const int kind = k == 1 ? 1 : (k == nz - 1 ? 2 : 0);
-                    const double d1m = k >= 2 ? ldg(G.dz1, k - 2) : 0., d10 = ldg(G.dz1, k - 1), d1p = ldg(G.dz1, k);
-                    const double fm = k >= 2 ? ldg(G.fdz0, k - 2) : 0., fp = ldg(G.fdz0, k);
-                    const double xm1 = k >= 2 ? ZVAL(f, 0) : 0.;
-                    const double xp2 = k + 2 <= nz ? ZVAL(f, 3) : 0.;
-                    if constexpr (MIXED)
-                        Fzn = muscl_face_z_mixed(kind, G.muscl_lim, (float)G.lim_tol, (float)G.dz, xm1, ZVAL(f, 1), ZVAL(f, 2), xp2,
-                                                 (float)d1m, (float)d10, (float)d1p, (float)fm, (float)fp, (float)dzw1, ww);
-                    else
-                        Fzn = muscl_face_z(kind, G.muscl_lim, G.lim_tol, G.dz, xm1, ZVAL(f, 1), ZVAL(f, 2), xp2, d1m, d10,
-                                           d1p, fm, fp, dzw1, ww);
-                } else if constexpr (MIXED) {
-                    // chain values relative: prfr = Fr(k) - x(k), prxp = xplus(k) - x(k)
-                    double *prfr = &chain[f * NCELL + cid], *prxp = &chain[(F + f) * NCELL + cid];
-                    if (k == 1) {
-                        const double x1 = ZVAL(f, 1);
-                        const float b1 = (float)(ZVAL(f, 2) - x1), b2 = (float)(ZVAL(f, 3) - x1);
-                        const float mup = (float)(fabs(wz2) * dt0 * ldg(G.dz1, 0));
-                        const float ffip1 = b1, ffip2 = b2 - b1;
-                        float dr, dl, phi1, phi2;
-                        ppm_limiter_rel((float)x1, b1, b1, 0.5f * ffip1, -0.5f * ffip1, ffip1, ffip2, 0.f, 0.f, dr, dl, phi1, phi2);
-                        *prfr = ppm_fr(dr, mup, phi1, phi2);
-                        *prxp = 0.5f * ffip1;
-                    }
-                    const int c = k + 1;
-                    const double x0 = ZVAL(f, 2), xkm = ZVAL(f, 1);
-                    const float m1 = (float)(xkm - x0);
-                    const float m2 = k >= 2 ? (float)(ZVAL(f, 0) - x0) : 0.f;
-                    const float p1 = c + 1 <= nz ? (float)(ZVAL(f, 3) - x0) : 0.f;
-                    const float p2 = c + 2 <= nz ? (float)(ZVAL(f, 4) - x0) : 0.f;
-                    const double d1c = ldg(G.dz1, c - 1);
-                    const float muc = (float)(fabs(ww) * dt0 * d1c);
-                    float dfl;
-                    if (c == nz) {
-                        dfl = 0.5f * (-m1) * (1.f - muc);
-                    } else {
-                        const float mup = (float)(fabs(wz3) * dt0 * d1c);
-                        float ffip1, ffip2, ffim1, ffim2, dplus;
-                        const float dmin = (float)(*prxp) + m1;   // xplus(k) - x(k+1)
-                        if (c == 2) {
-                            ffip1 = p1; ffip2 = p2 - p1; ffim1 = -m1; ffim2 = 0.f;
-                            dplus = 0.5f * ffip1;
-                        } else if (c == nz - 1) {
-                            ffip1 = p1; ffim1 = -m1; ffim2 = m1 - m2; ffip2 = ffip1;
-                            dplus = 0.5f * ffip1;
+#pragma unroll
+            for (int u = 0; u < PF; u++) {
+                const int f = gb + u;
+                if (PF > 1 && f >= F) continue;
+                const double *fxq = fxb + u * FXN, *fyq = fyb + u * FYN;
+                const double Tx = (fxq[ty * (TX + 1) + tx + 1] - fxq[ty * (TX + 1) + tx]) * dx1;
+                const double Ty = (fyq[(ty + 1) * TX + tx] - fyq[ty * TX + tx]) * dy1;
+                    const double dzw1 = ldg(G.dz1w, k - 1);
+                    double Fzn = 0.;
+                    double *zfo = &zf[f * NCELL + cid];
+                    if (k <= nz - 1) {
+                        const double ww = wz2;
+                        if (SCHEME == MG_WENO) {
+                            if constexpr (MIXED) {
+                                if (k == 1) Fzn = weno_face_bottom_mixed(ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww);
+                                else if (k == nz - 1) Fzn = weno_face_top_mixed(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ww);
+                                else Fzn = weno_face_mixed(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww, (k >= 3 && k <= nz - 3));
+                            } else {
+                                if (k == 1) Fzn = weno_face_bottom(ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww);
+                                else if (k == nz - 1) Fzn = weno_face_top(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ww);
+                                else Fzn = weno_face(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww, (k >= 3 && k <= nz - 3));
+                            }
+                        } else if (SCHEME == MG_MUSCL) {
+                            const int kind = k == 1 ? 1 : (k == nz - 1 ? 2 : 0);
+                            const double d1m = k >= 2 ? ldg(G.dz1, k - 2) : 0., d10 = ldg(G.dz1, k - 1), d1p = ldg(G.dz1, k);
+                            const double fm = k >= 2 ? ldg(G.fdz0, k - 2) : 0., fp = ldg(G.fdz0, k);
+                            const double xm1 = k >= 2 ? ZVAL(f, 0) : 0.;
+                            const double xp2 = k + 2 <= nz ? ZVAL(f, 3) : 0.;
+                            if constexpr (MIXED)
+                                Fzn = muscl_face_z_mixed(kind, G.muscl_lim, (float)G.lim_tol, (float)G.dz, xm1, ZVAL(f, 1), ZVAL(f, 2), xp2,
+                                                         (float)d1m, (float)d10, (float)d1p, (float)fm, (float)fp, (float)dzw1, ww);
+                            else
+                                Fzn = muscl_face_z(kind, G.muscl_lim, G.lim_tol, G.dz, xm1, ZVAL(f, 1), ZVAL(f, 2), xp2, d1m, d10,
+                                                   d1p, fm, fp, dzw1, ww);
+                        } else if constexpr (MIXED) {
+                            // chain values relative: prfr = Fr(k) - x(k), prxp = xplus(k) - x(k)
+                            double *prfr = &chain[f * NCELL + cid], *prxp = &chain[(F + f) * NCELL + cid];
+                            if (k == 1) {
+                                const double x1 = ZVAL(f, 1);
+                                const float b1 = (float)(ZVAL(f, 2) - x1), b2 = (float)(ZVAL(f, 3) - x1);
+                                const float mup = (float)(fabs(wz2) * dt0 * ldg(G.dz1, 0));
+                                const float ffip1 = b1, ffip2 = b2 - b1;
+                                float dr, dl, phi1, phi2;
+                                ppm_limiter_rel((float)x1, b1, b1, 0.5f * ffip1, -0.5f * ffip1, ffip1, ffip2, 0.f, 0.f, dr, dl, phi1, phi2);
+                                *prfr = ppm_fr(dr, mup, phi1, phi2);
+                                *prxp = 0.5f * ffip1;
+                            }
+                            const int c = k + 1;
+                            const double x0 = ZVAL(f, 2), xkm = ZVAL(f, 1);
+                            const float m1 = (float)(xkm - x0);
+                            const float m2 = k >= 2 ? (float)(ZVAL(f, 0) - x0) : 0.f;
+                            const float p1 = c + 1 <= nz ? (float)(ZVAL(f, 3) - x0) : 0.f;
+                            const float p2 = c + 2 <= nz ? (float)(ZVAL(f, 4) - x0) : 0.f;
+                            const double d1c = ldg(G.dz1, c - 1);
+                            const float muc = (float)(fabs(ww) * dt0 * d1c);
+                            float dfl;
+                            if (c == nz) {
+                                dfl = 0.5f * (-m1) * (1.f - muc);
+                            } else {
+                                const float mup = (float)(fabs(wz3) * dt0 * d1c);
+                                float ffip1, ffip2, ffim1, ffim2, dplus;
+                                const float dmin = (float)(*prxp) + m1;   // xplus(k) - x(k+1)
+                                if (c == 2) {
+                                    ffip1 = p1; ffip2 = p2 - p1; ffim1 = -m1; ffim2 = 0.f;
+                                    dplus = 0.5f * ffip1;
+                                } else if (c == nz - 1) {
+                                    ffip1 = p1; ffim1 = -m1; ffim2 = m1 - m2; ffip2 = ffip1;
+                                    dplus = 0.5f * ffip1;
+                                } else {
+                                    ffip1 = p1; ffip2 = p2 - p1; ffim1 = -m1; ffim2 = m1 - m2;
+                                    dplus = ppm_xplus_z(0.f, ffip1, ffip2, ffim1, (float)ldg(G.dz1w, c - 2), (float)ldg(G.dz1w, c - 1),
+                                                        (float)ldg(G.dz1w, c), (float)ldg(G.dz1w, c + 1));
+                                }
+                                float dr, dl, phi1, phi2;
+                                ppm_limiter_rel((float)x0, p1, m1, dplus, dmin, ffip1, ffip2, ffim1, ffim2, dr, dl, phi1, phi2);
+                                dfl = ppm_fl(dl, muc, phi1, phi2);
+                                const double fzn_up = ww > 0. ? ww * (xkm + *prfr) : (ww < 0. ? ww * (x0 + (double)dfl) : 0.);
+                                *prfr = ppm_fr(dr, mup, phi1, phi2);
+                                *prxp = dplus;
+                                Fzn = fzn_up;
+                            }
+                            if (c == nz) Fzn = ww > 0. ? ww * (xkm + *prfr) : (ww < 0. ? ww * (x0 + (double)dfl) : 0.);
                         } else {
-                            ffip1 = p1; ffip2 = p2 - p1; ffim1 = -m1; ffim2 = m1 - m2;
-                            dplus = ppm_xplus_z(0.f, ffip1, ffip2, ffim1, (float)ldg(G.dz1w, c - 2), (float)ldg(G.dz1w, c - 1),
-                                                (float)ldg(G.dz1w, c), (float)ldg(G.dz1w, c + 1));
+                            double *prfr = &chain[f * NCELL + cid], *prxp = &chain[(F + f) * NCELL + cid];
+                            if (k == 1) {
+                                // cell 1 (advq_ppm.f90:328-343): bottom special, bc51 = 0
+                                const double x1 = ZVAL(f, 1), x2 = ZVAL(f, 2), x3 = ZVAL(f, 3);
+                                const double mup = fabs(wz2) * dt0 * ldg(G.dz1, 0);   // w(2) at k = 1
+                                const double ffip1 = x2 - x1, ffip2 = x3 - x2;
+                                const double xmin = x1 - 0.5 * ffip1, xplus = x1 + 0.5 * ffip1;
+                                double phir, phil, phi1, phi2;
+                                ppm_limiter(x1, x2, x2, xplus, xmin, ffip1, ffip2, 0., 0., phir, phil, phi1, phi2);
+                                *prfr = ppm_fr(phir, mup, phi1, phi2);
+                                *prxp = xplus;
+                            }
+                            // reconstruction of cell c = k+1 (:345-414)
+                            const int c = k + 1;
+                            const double xm2 = k >= 2 ? ZVAL(f, 0) : 0., xm1 = ZVAL(f, 1), x0 = ZVAL(f, 2);
+                            const double xp1 = c + 1 <= nz ? ZVAL(f, 3) : 0., xp2 = c + 2 <= nz ? ZVAL(f, 4) : 0.;
+                            const double d1c = ldg(G.dz1, c - 1);
+                            const double muc = fabs(ww) * dt0 * d1c;
+                            if (c == nz) {
+                                const double fl = x0 + 0.5 * (x0 - xm1) * (1. - muc);
+                                Fzn = 0.5 * (*prfr) * (ww + fabs(ww)) + 0.5 * fl * (ww - fabs(ww));
+                            } else {
+                                const double mup = fabs(wz3) * dt0 * d1c;
+                                double ffip1, ffip2, ffim1, ffim2, xplus;
+                                const double xmin = *prxp;
+                                if (c == 2) {
+                                    ffip1 = xp1 - x0; ffip2 = xp2 - xp1; ffim1 = (x0 - xm1); ffim2 = 0.;
+                                    xplus = x0 + 0.5 * ffip1;
+                                } else if (c == nz - 1) {
+                                    ffip1 = xp1 - x0; ffim1 = x0 - xm1; ffim2 = xm1 - xm2; ffip2 = ffip1;
+                                    xplus = x0 + 0.5 * ffip1;
+                                } else {
+                                    ffip1 = (xp1 - x0); ffip2 = (xp2 - xp1); ffim1 = (x0 - xm1); ffim2 = (xm1 - xm2);
+                                    xplus = ppm_xplus_z(x0, ffip1, ffip2, ffim1, ldg(G.dz1w, c - 2), ldg(G.dz1w, c - 1),
+                                                        ldg(G.dz1w, c), ldg(G.dz1w, c + 1));
+                                }
+                                double phir, phil, phi1, phi2;
+                                ppm_limiter(x0, xp1, xm1, xplus, xmin, ffip1, ffip2, ffim1, ffim2, phir, phil, phi1, phi2);
+                                const double fl = ppm_fl(phil, muc, phi1, phi2);
+                                Fzn = 0.5 * (*prfr) * (ww + fabs(ww)) + 0.5 * fl * (ww - fabs(ww));
+                                *prfr = ppm_fr(phir, mup, phi1, phi2);
+                                *prxp = xplus;
+                            }
                         }
-                        float dr, dl, phi1, phi2;
-                        ppm_limiter_rel((float)x0, p1, m1, dplus, dmin, ffip1, ffip2, ffim1, ffim2, dr, dl, phi1, phi2);
-                        dfl = ppm_fl(dl, muc, phi1, phi2);
-                        const double fzn_up = ww > 0. ? ww * (xkm + *prfr) : (ww < 0. ? ww * (x0 + (double)dfl) : 0.);
-                        *prfr = ppm_fr(dr, mup, phi1, phi2);
-                        *prxp = dplus;
-                        Fzn = fzn_up;
                     }
-                    if (c == nz) Fzn = ww > 0. ? ww * (xkm + *prfr) : (ww < 0. ? ww * (x0 + (double)dfl) : 0.);
-                } else {
-                    double *prfr = &chain[f * NCELL + cid], *prxp = &chain[(F + f) * NCELL + cid];
-                    if (k == 1) {
-                        // cell 1 (advq_ppm.f90:328-343): bottom special, bc51 = 0
-                        const double x1 = ZVAL(f, 1), x2 = ZVAL(f, 2), x3 = ZVAL(f, 3);
-                        const double mup = fabs(wz2) * dt0 * ldg(G.dz1, 0);   // w(2) at k = 1
-                        const double ffip1 = x2 - x1, ffip2 = x3 - x2;
-                        const double xmin = x1 - 0.5 * ffip1, xplus = x1 + 0.5 * ffip1;
-                        double phir, phil, phi1, phi2;
-                        ppm_limiter(x1, x2, x2, xplus, xmin, ffip1, ffip2, 0., 0., phir, phil, phi1, phi2);
-                        *prfr = ppm_fr(phir, mup, phi1, phi2);
-                        *prxp = xplus;
-                    }
-                    // reconstruction of cell c = k+1 (:345-414)
-                    const int c = k + 1;
-                    const double xm2 = k >= 2 ? ZVAL(f, 0) : 0., xm1 = ZVAL(f, 1), x0 = ZVAL(f, 2);
-                    const double xp1 = c + 1 <= nz ? ZVAL(f, 3) : 0., xp2 = c + 2 <= nz ? ZVAL(f, 4) : 0.;
-                    const double d1c = ldg(G.dz1, c - 1);
-                    const double muc = fabs(ww) * dt0 * d1c;
-                    if (c == nz) {
-                        const double fl = x0 + 0.5 * (x0 - xm1) * (1. - muc);
-                        Fzn = 0.5 * (*prfr) * (ww + fabs(ww)) + 0.5 * fl * (ww - fabs(ww));
-                    } else {
-                        const double mup = fabs(wz3) * dt0 * d1c;
-                        double ffip1, ffip2, ffim1, ffim2, xplus;
-                        const double xmin = *prxp;
-                        if (c == 2) {
-                            ffip1 = xp1 - x0; ffip2 = xp2 - xp1; ffim1 = (x0 - xm1); ffim2 = 0.;
-                            xplus = x0 + 0.5 * ffip1;
-                        } else if (c == nz - 1) {
-                            ffip1 = xp1 - x0; ffim1 = x0 - xm1; ffim2 = xm1 - xm2; ffip2 = ffip1;
-                            xplus = x0 + 0.5 * ffip1;
-                        } else {
-                            ffip1 = (xp1 - x0); ffip2 = (xp2 - xp1); ffim1 = (x0 - xm1); ffim2 = (xm1 - xm2);
-                            xplus = ppm_xplus_z(x0, ffip1, ffip2, ffim1, ldg(G.dz1w, c - 2), ldg(G.dz1w, c - 1),
-                                                ldg(G.dz1w, c), ldg(G.dz1w, c + 1));
-                        }
-                        double phir, phil, phi1, phi2;
-                        ppm_limiter(x0, xp1, xm1, xplus, xmin, ffip1, ffip2, ffim1, ffim2, phir, phil, phi1, phi2);
-                        const double fl = ppm_fl(phil, muc, phi1, phi2);
-                        Fzn = 0.5 * (*prfr) * (ww + fabs(ww)) + 0.5 * fl * (ww - fabs(ww));
-                        *prfr = ppm_fr(phir, mup, phi1, phi2);
-                        *prxp = xplus;
-                    }
-                }
-            }
-            double Tz;
-            if (k == 1) Tz = (Fzn - 0.) * dzw1;
-            else if (k == nz) Tz = (0. - *zfo) * dzw1;
-            else Tz = (Fzn - *zfo) * dzw1;
-            *zfo = Fzn;
+                    double Tz;
+                    if (k == 1) Tz = (Fzn - 0.) * dzw1;
+                    else if (k == nz) Tz = (0. - *zfo) * dzw1;
+                    else Tz = (Fzn - *zfo) * dzw1;
+                    *zfo = Fzn;
 
-            // ---- epilogue ----
-            if (act) {
-                const long long idx = gidx(G, i, j, k);
-                if (A.mode == 1) {
-                    double *xs = A.xout[f];
-                    xs[idx] = ((xs[idx] - Tx) - Ty) - Tz;
-                } else {
-                    const double T = ((0. - Tx) - Ty) - Tz;
-                    const double told = A.stage == 1 ? 0. : cur_tend;
-                    const double tn = T + A.b * told;
-                    const bool weighted = A.dens_first && f > 0;
-                    // level n (natural); stage 2 overwrites it in place
-                    const double xo = A.xold_is_xin ? plane_xo : cur_xold;
-                    if (A.dens_first && f == 0) dn_old = xo;
-                    const double old = weighted ? xo * dn_old : xo;
-                    const double xnew = old + A.a_dt * tn;
-                    if (A.stage == 2 && A.dens_first) {
-                        // get_scalars (funcpack.f90:488-542): natural value with the new density
-                        if constexpr (MIXED) {   // one reciprocal per cell
-                            if (f == 0) { dn_new = xnew; rdn_new = 1. / xnew; }
-                            A.xout[f][idx] = weighted ? xnew * rdn_new : xnew;
-                        } else {
-                            if (f == 0) dn_new = xnew;
-                            A.xout[f][idx] = weighted ? xnew / dn_new : xnew;
-                        }
+                // ---- epilogue ----
+                if (act) {
+                    const long long idx = idx0 + (long long)(k - 1) * G.ps;
+                    if constexpr (STAGE == 0) {
+                        double *xs = A.xout[f];
+                        xs[idx] = ((xs[idx] - Tx) - Ty) - Tz;
                     } else {
-                        A.xout[f][idx] = xnew;
-                        A.tend[f][idx] = tn;
+                        const double T = ((0. - Tx) - Ty) - Tz;
+                        const double told = STAGE == 1 ? 0. : cur_tend[u];
+                        const double tn = T + A.b * told;
+                        const bool weighted = f > 0;
+                        // level n (natural); stage 2 overwrites it in place
+                        const double xo = STAGE == 1 ? plane_xo[u] : cur_xold[u];
+                        if (f == 0) dn_old = xo;
+                        const double old = weighted ? xo * dn_old : xo;
+                        const double xnew = old + A.a_dt * tn;
+                        if constexpr (STAGE == 2) {
+                            // get_scalars (funcpack.f90:488-542): natural value with the new density
+                            if constexpr (MIXED) {   // one reciprocal per cell
+                                if (f == 0) { dn_new = xnew; rdn_new = 1. / xnew; }
+                                A.xout[f][idx] = weighted ? xnew * rdn_new : xnew;
+                            } else {
+                                if (f == 0) dn_new = xnew;
+                                A.xout[f][idx] = weighted ? xnew / dn_new : xnew;
+                            }
+                        } else {
+                            A.xout[f][idx] = xnew;
+                            A.tend[f][idx] = tn;
+                        }
+                        if (A.fst[f]) A.fst[f][idx] = T;
                     }
-                    if (A.fst[f]) A.fst[f][idx] = T;
                 }
             }
         }
@@ -508,6 +570,7 @@ __global__ void __launch_bounds__(NT) k1_kernel(DevGrid G, K1Args A, const __gri
         else cp_async_commit();
     }
     cp_async_wait_all();
+#undef ZVAL
 }
 
 }  // namespace

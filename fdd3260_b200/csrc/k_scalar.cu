@@ -5,25 +5,48 @@
 
 size_t k1_smem_bytes(int scheme, int nf) { return make_layout(scheme, nf).total; }
 
+namespace {
+template <int SCHEME, int STAGE>
+cudaError_t launch_one(const DevGrid &g, const K1Args &a, const K1Maps &maps, size_t sm, cudaStream_t s)
+{
+    const int ntx = (g.maxx + TX - 1) / TX, nty = (g.maxy + TY - 1) / TY;
+    k1_kernel<SCHEME, false, STAGE><<<dim3(ntx * nty), dim3(TX, TY + 1), sm, s>>>(g, a, maps);
+    return cudaGetLastError();
+}
+template <int SCHEME>
+cudaError_t launch_scheme(const DevGrid &g, const K1Args &a, const K1Maps &maps, size_t sm, cudaStream_t s)
+{
+    if (a.mode == 1) return launch_one<SCHEME, 0>(g, a, maps, sm, s);
+    if (a.stage == 1) return launch_one<SCHEME, 1>(g, a, maps, sm, s);
+    return launch_one<SCHEME, 2>(g, a, maps, sm, s);
+}
+template <int SCHEME>
+cudaError_t init_scheme()
+{
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k1_kernel<SCHEME, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k1_kernel<SCHEME, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k1_kernel<SCHEME, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+}
+}  // namespace
+
 cudaError_t launch_k1(const DevGrid &g, const K1Args &a, const K1Maps &maps, cudaStream_t s)
 {
     if (a.nf <= 0 || a.nf > MG_MAXF) return cudaErrorInvalidValue;
-    const int ntx = (g.maxx + TX - 1) / TX, nty = (g.maxy + TY - 1) / TY;
-    const dim3 grid(ntx * nty), block(TX, TY + 1);
+    if (a.mode != 1 && a.stage != 1 && a.stage != 2) return cudaErrorInvalidValue;
     const size_t sm = make_layout(g.scal_adv, a.nf).total;
     if (sm > 232448) return cudaErrorInvalidValue;
     switch (g.scal_adv) {
-    case MG_WENO: k1_kernel<MG_WENO, false><<<grid, block, sm, s>>>(g, a, maps); break;
-    case MG_PPM: k1_kernel<MG_PPM, false><<<grid, block, sm, s>>>(g, a, maps); break;
-    default: k1_kernel<MG_MUSCL, false><<<grid, block, sm, s>>>(g, a, maps); break;
+    case MG_WENO: return launch_scheme<MG_WENO>(g, a, maps, sm, s);
+    case MG_PPM: return launch_scheme<MG_PPM>(g, a, maps, sm, s);
+    default: return launch_scheme<MG_MUSCL>(g, a, maps, sm, s);
     }
-    return cudaGetLastError();
 }
 
 cudaError_t k1_init()
 {
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k1_kernel<MG_WENO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k1_kernel<MG_PPM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448)) != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k1_kernel<MG_MUSCL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+    if ((e = init_scheme<MG_WENO>()) != cudaSuccess) return e;
+    if ((e = init_scheme<MG_PPM>()) != cudaSuccess) return e;
+    return init_scheme<MG_MUSCL>();
 }
