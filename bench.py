@@ -13,6 +13,13 @@ WENO3-switch), FD4 momentum, dt = 1 s, plain FP64 form.  Synthetic seeded inputs
 (no dataset exists for this benchmark); the working set (~16 GB) exceeds the
 126 MB L2, so no flush is needed between timed steps.
 
+Both arithmetic forms are measured by default: the plain FP64 form is the headline
+(`value`, bit-exact with the CPU restatement of the reference routines), and the mixed
+form (FP32 stencils, fluxes and spectra; FP64 state, tendencies, tridiagonal elimination
+and divergence residual, with refinement of the Poisson solve) is reported in the
+`mixed` object: its throughput, roofline, and its per-field relative L2 error against the
+FP64 form after `--err-steps` steps from the same initial state.
+
 `python bench.py --gpus N --steps K --warmup W` prints one JSON line.
 `--impl reference` times the reference's algorithm on the host cores instead
 (the CPU restatement, OpenMP over all cores, bounded sample).
@@ -195,8 +202,12 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
-    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"],
-                    help="fp64: plain FP64 form; mixed: FP32 stencils/fluxes with FP64 state and accumulation")
+    ap.add_argument("--form", default="both", choices=["both", "fp64", "mixed"],
+                    help="both (default): the plain FP64 form is the headline, the mixed form (FP32 "
+                         "stencils/fluxes/spectra, FP64 state) is reported beside it with its error against "
+                         "the FP64 form; fp64 / mixed: one form only")
+    ap.add_argument("--err-steps", type=int, default=10,
+                    help="steps of the accuracy leg (mixed vs FP64 fields from the same initial state)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -204,16 +215,15 @@ def main():
     ws, rank, local = dist_init()
     from fdd3260_b200 import Mimica, config
     d = config.cumulus_domain(args.maxx, args.maxx, args.nz, scheme=args.scheme)
-    if args.form == "mixed":
-        from fdd3260_b200 import _lib
-        d.precision = _lib.MG_PREC_MIXED
+    from fdd3260_b200 import _lib
     metric = "Mcell-updates/s per integrator step (2-stage Heun + projection)"
     cfg = {"workload": f"shallow-cumulus domain {args.maxx}x{args.maxx}x{args.nz}, dx=dy=25 m, stretched dz 10->100 m, "
                        f"3 momentum + density + 5 scalars, {args.scheme.upper()} (reference scheme), FD4 momentum, "
                        f"dt=1 s, nsubp=1",
            "fields": "theta_l 298->310 K, qt 17->4 g/kg, qr/nr/aerosol smooth decreasing profiles; "
                      "seeded Gaussian perturbations below 500 m; u=-8+N(0,0.5), v=N(0,0.5) m/s",
-           "form": "plain FP64" if args.form == "fp64" else "mixed (FP32 stencils and fluxes, FP64 state)",
+           "form": {"both": "plain FP64 (headline) + mixed", "fp64": "plain FP64",
+                    "mixed": "mixed (FP32 stencils, fluxes and spectra; FP64 state)"}[args.form],
            "scheme": args.scheme, "interior_cells": d.cells,
            "l2": "inputs larger than L2 (~16 GB working set)", "parallelism": f"replicas x{ws}"}
 
@@ -235,11 +245,102 @@ def main():
         return
 
     st = config.cumulus_state(d, seed=1000 + rank, n_extra=3)
-    m = Mimica(d, nscal=len(st.scal), iqt=st.iqt, device=local if ws > 1 else 0)
-    m.upload(st)
-    L = m._L
     use_graph = not args.no_graph
-    # warm-up
+    dev = local if ws > 1 else 0
+    forms = ["fp64", "mixed"] if args.form == "both" else [args.form]
+    res = {}
+    ref_fields = None
+    for form in forms:
+        d.precision = _lib.MG_PREC_MIXED if form == "mixed" else _lib.MG_PREC_FP64
+        m = Mimica(d, nscal=len(st.scal), iqt=st.iqt, device=dev)
+        r = {}
+        # accuracy leg: err_steps steps from the initial state, fields downloaded; the mixed
+        # form is compared with the plain FP64 form (bit-exact with the CPU restatement of
+        # the reference routines)
+        if args.err_steps > 0 and len(forms) == 2:
+            m.upload(st)
+            md, _ = m.stepping(args.err_steps, ntime0=1, diagnostics=True, graph=use_graph)
+            out = m.download()
+            r["maxdiv"] = md
+            if form == "fp64":
+                ref_fields = out
+                # FP64 twin: the same run from u perturbed by 1e-9 relative (seeded).  The
+                # reference's WENO3 switch is discontinuous, so any perturbation of about
+                # this size flips faces and the trajectories separate along the flow's own
+                # sensitivity; this is the floor against which the mixed error is read.
+                tw = config.State(st.u * (1.0 + 1e-9 * np.random.default_rng(99).standard_normal(st.u.shape)),
+                                  st.v, st.w, st.p, st.dens, st.scal, st.iqt)
+                m.upload(tw)
+                del tw
+                m.stepping(args.err_steps, ntime0=1, graph=use_graph)
+                twin = m.download()
+                r["twin_error"] = field_errors(twin, ref_fields, st, args.err_steps)
+                del twin
+            else:
+                r["error_vs_fp64"] = field_errors(out, ref_fields, st, args.err_steps)
+            del out
+        m.upload(st)
+        r.update(time_form(args, m, d, st, use_graph, ws, local))
+        if form == forms[0]:
+            r.update(e2e_leg(args, m, d, st, ws))
+        r["device_bytes"] = m.device_bytes
+        m.close()
+        res[form] = r
+    ref_fields = None
+
+    cpu = None
+    if rank == 0 and not args.skip_cpu:
+        try:
+            v, cores, sample = cpu_reference(args, d, args.scheme, nsamp_steps=1)
+            cpu = {"value": v, "unit": "Mcell-updates/s", "cores": cores, "kind": "port", "sample": sample}
+        except Exception as e:  # pragma: no cover
+            cpu = {"value": None, "unit": "Mcell-updates/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        head = res[forms[0]]
+        line = {"metric": metric, "value": head["value"], "unit": "Mcell-updates/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if forms[0] == "fp64" else "f32 fluxes/spectra, f64 state",
+                "data": "synthetic (seeded PCG64)", "config": cfg,
+                "clocks": head["clocks"], "gpu_launches": head["gpu_launches"],
+                "e2e": head["e2e"], "roofline": head["roofline"], "kernel_share": head["kernel_share"],
+                "cpu_baseline": cpu, "graph": use_graph, "device_bytes": head["device_bytes"]}
+        if "mixed" in res and forms[0] != "mixed":
+            mx = res["mixed"]
+            line["mixed"] = {"form": "FP32 stencils, fluxes and spectra; FP64 state, tendencies, tridiagonal, "
+                                     f"residual; refinement passes <= {d.refine_iters}, tol {d.refine_tol} 1/s",
+                             "value": mx["value"], "unit": "Mcell-updates/s", "ms_per_step": mx["ms_per_step"],
+                             "speedup_vs_fp64": mx["value"] / head["value"], "roofline": mx["roofline"],
+                             "kernel_share": mx["kernel_share"], "clocks": mx["clocks"],
+                             "gpu_launches": mx["gpu_launches"]}
+            if "error_vs_fp64" in mx:
+                line["mixed"]["error_vs_fp64"] = mx["error_vs_fp64"]
+                line["mixed"]["fp64_twin_1e-9_error"] = head.get("twin_error")
+                line["mixed"]["maxdiv"] = mx["maxdiv"]
+                line["mixed"]["maxdiv_fp64"] = head.get("maxdiv")
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def field_errors(out, ref, st0, nsteps: int) -> dict:
+    """Per-field relative L2 error over the interior: against the FP64 field, and against
+    the change the FP64 form made over the run."""
+    rel, relc = {}, {}
+    names = [("u", out.u, ref.u, st0.u), ("v", out.v, ref.v, st0.v), ("w", out.w, ref.w, st0.w),
+             ("p", out.p, ref.p, st0.p), ("dens", out.dens, ref.dens, st0.dens)]
+    names += [(f"s{i}", a, b, c) for i, (a, b, c) in enumerate(zip(out.scal, ref.scal, st0.scal))]
+    for name, a, b, c in names:
+        a, b, c = a[:, 3:-2, 3:-2], b[:, 3:-2, 3:-2], c[:, 3:-2, 3:-2]
+        e = float(np.linalg.norm(a - b))
+        rel[name] = e / max(float(np.linalg.norm(b)), 1e-300)
+        relc[name] = e / max(float(np.linalg.norm(b - c)), 1e-300)
+    return {"steps": nsteps, "rel_l2": rel, "rel_l2_of_change": relc}
+
+
+def time_form(args, m, d, st, use_graph, ws, local) -> dict:
+    L = m._L
     m.stepping(args.warmup, ntime0=1, graph=use_graph)
     m.synchronize()
     # timed region (device time, CUDA events on the library stream), clocks sampled meanwhile
@@ -250,14 +351,12 @@ def main():
     if rc:
         raise RuntimeError(f"mg_time_steps failed: {rc}")
     t_ms = dist_max(ms.value, ws)
-    per_rank_rate = d.cells * args.steps / (t_ms / 1e3) / 1e6
-    value = per_rank_rate * ws
+    value = d.cells * args.steps / (t_ms / 1e3) / 1e6 * ws
     launches_per_step = m.launches_per_call
 
     # per-kernel device times (separate eager pass, events around each launch group)
     L.mg_profile_enable(m._h, 1)
-    nprof = 2
-    m.stepping(nprof, ntime0=1 + args.warmup + args.steps)
+    m.stepping(2, ntime0=1 + args.warmup + args.steps)
     buf = C.create_string_buffer(8192)
     L.mg_profile_report(m._h, buf, 8192)
     L.mg_profile_enable(m._h, 0)
@@ -269,16 +368,21 @@ def main():
     pk, pk_src = peaks()
     dom = max((k for k in kern if k in ab), key=lambda k: kern[k]["total_ms"])
     avg_ms = kern[dom]["total_ms"] / kern[dom]["launches"]
-    alg = ab[dom] * d.cells
-    achieved = alg / (avg_ms / 1e3) / 1e9
+    achieved = ab[dom] * d.cells / (avg_ms / 1e3) / 1e9
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_source": pk_src,
             "algorithmic_bytes_per_cell": ab[dom], "avg_launch_ms": avg_ms,
             "step_alg_bytes_per_cell": ab["step"],
             "step_frac": ab["step"] * d.cells * args.steps / (t_ms / 1e3) / 1e9 / pk["hbm_gbs"]}
     kshare = {k: round(v["total_ms"] / sum(x["total_ms"] for x in kern.values()), 4) for k, v in kern.items()}
+    return {"value": value, "ms_per_step": t_ms / args.steps, "clocks": clk.summary(),
+            "gpu_launches": launches_per_step * args.steps, "roofline": roof, "kernel_share": kshare}
 
-    # end-to-end through the public API with pinned host buffers: upload state, one step, download state
+
+def e2e_leg(args, m, d, st, ws) -> dict:
+    """End to end through the public API with pinned host buffers: upload the state, one
+    step, download the state, per step."""
+    from fdd3260_b200 import config
     host = {n: pinned_like(d.shape) for n in ("u", "v", "w", "p", "dens")}
     hscal = [pinned_like(d.shape) for _ in st.scal]
     for n in ("u", "v", "w", "p", "dens"):
@@ -294,35 +398,13 @@ def main():
     for s in range(args.e2e_steps):
         m.upload(hstate)
         m.stepping(1, ntime0=2 + s)
-        out = m.download()
-        hstate = out
+        hstate = m.download()
     m.synchronize()
     e2e_s = dist_max(time.perf_counter() - t0, ws)
-    e2e_val = d.cells * args.e2e_steps * ws / e2e_s / 1e6
     nbytes = (5 + len(st.scal)) * d.nx * d.ny * d.nz * 8
-
-    cpu = None
-    if rank == 0 and not args.skip_cpu:
-        try:
-            v, cores, sample = cpu_reference(args, d, args.scheme, nsamp_steps=1)
-            cpu = {"value": v, "unit": "Mcell-updates/s", "cores": cores, "kind": "port", "sample": sample}
-        except Exception as e:  # pragma: no cover
-            cpu = {"value": None, "unit": "Mcell-updates/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
-
-    if rank == 0:
-        line = {"metric": metric, "value": value, "unit": "Mcell-updates/s", "n_gpus": ws, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)", "config": cfg,
-                "clocks": clk.summary(), "gpu_launches": launches_per_step * args.steps,
-                "e2e": {"value": e2e_val, "unit": "Mcell-updates/s", "h2d_bytes_per_step": nbytes,
-                        "d2h_bytes_per_step": nbytes, "timing": "host wall clock, synchronised, pinned buffers"},
-                "roofline": roof, "kernel_share": kshare, "cpu_baseline": cpu,
-                "graph": use_graph, "device_bytes": m.device_bytes}
-        print(json.dumps(line), flush=True)
-    m.close()
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    return {"e2e": {"value": d.cells * args.e2e_steps * ws / e2e_s / 1e6, "unit": "Mcell-updates/s",
+                    "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                    "timing": "host wall clock, synchronised, pinned buffers"}}
 
 
 if __name__ == "__main__":

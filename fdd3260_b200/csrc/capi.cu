@@ -642,7 +642,7 @@ extern "C" int mg_advection_ac(mg_ctx *c, const double *x, const double *mu, con
     const double *xv[1] = {c->unit[0]};
     rc = build_maps(c, xv, 1, c->unit[1], c->unit[2], &maps);
     if (rc) return rc;
-    CKR(launch_k1(c->G, a, maps, c->stream));
+    CKR(c->prm.precision == MG_PREC_MIXED ? launch_k1_mixed(c->G, a, maps, c->stream) : launch_k1(c->G, a, maps, c->stream));
     CKR(d2h(c, xs, c->unit[4], cudaMemcpyDeviceToHost));
     return check_err(c);
 }
