@@ -352,23 +352,12 @@ __device__ __forceinline__ double weno_face_mixed(double xm1, double x0, double 
     if (full_weights) {
         const float d3 = c - b;
         const float eta1 = a * a, eta2 = b * b, eta3 = d3 * d3;
-        // The switch to nonlinear weights is discontinuous: where the FP32 smoothness
-        // ratio is within its rounding band (4e-6 relative) of the threshold, the
-        // decision is taken in FP64 from the FP64 differences, as the plain form does,
-        // so that FP32 rounding never flips a face between the two reconstructions.
-        bool nl1, nl2;
-        {
-            const float r1 = fmaxf(eta1, eta2) - thres * (fminf(eta1, eta2) + eps);
-            const float r2 = fmaxf(eta2, eta3) - thres * (fminf(eta2, eta3) + eps);
-            nl1 = r1 > 0.f;
-            nl2 = r2 > 0.f;
-            const float band1 = 4e-6f * fmaxf(eta1, eta2), band2 = 4e-6f * fmaxf(eta2, eta3);
-            if (fabsf(r1) <= band1 || fabsf(r2) <= band2) {
-                const double e1 = (x0 - xm1) * (x0 - xm1), e2 = (xp1 - x0) * (xp1 - x0), e3 = (xp2 - xp1) * (xp2 - xp1);
-                if (fabsf(r1) <= band1) nl1 = ratio_gt(fmax(e1, e2), fmin(e1, e2) + 1.e-15, 20.);
-                if (fabsf(r2) <= band2) nl2 = ratio_gt(fmax(e2, e3), fmin(e2, e3) + 1.e-15, 20.);
-            }
-        }
+        // The switch is decided on the FP32 smoothness indicators.  Being discontinuous,
+        // it can differ from the plain form's decision where the ratio lies within the
+        // FP32 rounding band (~1e-6 relative) of the threshold; the plain form itself
+        // flips such faces under perturbations of ~1e-9 of its state.
+        const bool nl1 = fmaxf(eta1, eta2) > thres * (fminf(eta1, eta2) + eps);
+        const bool nl2 = fmaxf(eta2, eta3) > thres * (fminf(eta2, eta3) + eps);
         if (nl1) {
             const float y1 = eps + eta1, y2 = eps + eta2;
             // w0 = g1/y1^2 / (g1/y1^2 + g2/y2^2) = g1 y2^2 / (g1 y2^2 + g2 y1^2)
