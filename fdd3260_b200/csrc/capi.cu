@@ -605,6 +605,137 @@ extern "C" int mg_step_graph(mg_ctx *c, int nsteps, int ntime0, double *maxdiv, 
     return MG_OK;
 }
 
+// ---------------- ensembles of independent domains ----------------
+// The members are contexts of their own (sizes, parameters, streams).  A pair of steps
+// of all members is recorded once per parity into one CUDA graph that forks from the
+// ensemble's stream to every member's stream and joins back, so that the launches of
+// small members run concurrently and one graph launch advances the whole ensemble.
+struct mg_ens {
+    std::vector<mg_ctx *> m;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    int launches = 0;
+};
+
+extern "C" int mg_ensemble_create(mg_ctx *const *members, int n, mg_ens **out)
+{
+    if (!members || n < 1 || !out) return MG_ERR_PARAM;
+    *out = nullptr;
+    for (int i = 0; i < n; i++) {
+        if (!members[i]) return MG_ERR_PARAM;
+        if (members[i]->device != members[0]->device) return MG_ERR_PARAM;
+        for (int j = 0; j < i; j++) if (members[j] == members[i]) return MG_ERR_PARAM;
+    }
+    CKR(cudaSetDevice(members[0]->device));
+    mg_ens *e = new mg_ens();
+    e->device = members[0]->device;
+    e->m.assign(members, members + n);
+    cudaError_t er = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    if (er == cudaSuccess) er = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+    e->join.resize(n, nullptr);
+    for (int i = 0; i < n && er == cudaSuccess; i++) er = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming);
+    if (er != cudaSuccess) {
+        mg_ensemble_destroy(e);
+        return cuerr(er);
+    }
+    *out = e;
+    return MG_OK;
+}
+
+extern "C" int mg_ensemble_destroy(mg_ens *e)
+{
+    if (!e) return MG_ERR_PARAM;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    for (int i = 0; i < 2; i++) if (e->gexec[i]) cudaGraphExecDestroy(e->gexec[i]);
+    for (cudaEvent_t ev : e->join) if (ev) cudaEventDestroy(ev);
+    if (e->fork) cudaEventDestroy(e->fork);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return MG_OK;
+}
+
+// steps [ntime, ntime+nst) of every member, forked from and joined back to e->stream
+static cudaError_t ens_issue(mg_ens *e, int ntime, int nst, int *launches)
+{
+    cudaError_t er = cudaEventRecord(e->fork, e->stream);
+    for (size_t i = 0; i < e->m.size() && er == cudaSuccess; i++) {
+        mg_ctx *c = e->m[i];
+        er = cudaStreamWaitEvent(c->stream, e->fork, 0);
+        for (int s = 0; s < nst && er == cudaSuccess; s++) er = step_once(c, ntime + s, 0, 0, 0, launches);
+        if (er == cudaSuccess) er = cudaEventRecord(e->join[i], c->stream);
+        if (er == cudaSuccess) er = cudaStreamWaitEvent(e->stream, e->join[i], 0);
+    }
+    return er;
+}
+
+extern "C" int mg_ensemble_step(mg_ens *e, int nsteps, int ntime0)
+{
+    if (!e || nsteps < 0) return MG_ERR_PARAM;
+    for (mg_ctx *c : e->m) {
+        if (!c->have_state) return MG_ERR_STATE;
+        if (c->prof_on) return MG_ERR_STATE;   // per-kernel events cannot be recorded into the graph
+    }
+    CKR(cudaSetDevice(e->device));
+    int s = 0;
+    while (nsteps - s >= 2) {
+        const int par = (ntime0 + s) & 1;
+        if (!e->gexec[par]) {
+            cudaGraph_t graph;
+            CKR(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+            int launches = 0;
+            cudaError_t er = ens_issue(e, ntime0 + s, 2, &launches);
+            cudaError_t er2 = cudaStreamEndCapture(e->stream, &graph);
+            if (er != cudaSuccess) return cuerr(er);
+            if (er2 != cudaSuccess) return cuerr(er2);
+            er = cudaGraphInstantiate(&e->gexec[par], graph, 0);
+            cudaGraphDestroy(graph);
+            if (er != cudaSuccess) return cuerr(er);
+            e->launches = launches / 2;
+        }
+        CKR(cudaGraphLaunch(e->gexec[par], e->stream));
+        s += 2;
+    }
+    if (s < nsteps) {
+        int launches = 0;
+        CKR(ens_issue(e, ntime0 + s, nsteps - s, &launches));
+    }
+    CKR(cudaStreamSynchronize(e->stream));
+    for (mg_ctx *c : e->m) {
+        int rc = check_err(c);
+        if (rc) return rc;
+    }
+    return MG_OK;
+}
+
+extern "C" int mg_ensemble_time_steps(mg_ens *e, int nsteps, int ntime0, double *ms)
+{
+    if (!e || nsteps < 0 || !ms) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(e->device));
+    cudaEvent_t a, b;
+    CKR(cudaEventCreate(&a));
+    CKR(cudaEventCreate(&b));
+    cudaError_t er = cudaEventRecord(a, e->stream);
+    int rc = er == cudaSuccess ? mg_ensemble_step(e, nsteps, ntime0) : cuerr(er);
+    if (rc == MG_OK) {
+        // mg_ensemble_step synchronised its stream; b closes the interval there
+        er = cudaEventRecord(b, e->stream);
+        if (er == cudaSuccess) er = cudaEventSynchronize(b);
+        float f = 0.f;
+        if (er == cudaSuccess) er = cudaEventElapsedTime(&f, a, b);
+        *ms = f;
+        if (er != cudaSuccess) rc = cuerr(er);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return rc;
+}
+
+extern "C" int mg_ensemble_launch_count(const mg_ens *e) { return e ? e->launches : -1; }
+
 extern "C" int mg_synchronize(mg_ctx *c)
 {
     if (!c) return MG_ERR_PARAM;

@@ -130,6 +130,23 @@ int mg_synchronize(mg_ctx *ctx);
 /* most recent kernel-launch count of mg_step (kernels launched per call) */
 int mg_last_launch_count(const mg_ctx *ctx);
 
+/* ---- ensembles of independent domains (no counterpart in the reference, which runs one
+ * domain per job) ----
+ * The members are contexts from mg_create on one device, each with its own sizes and
+ * parameters and already holding a state (mg_upload_state).  mg_ensemble_step advances
+ * every member by nsteps steps: a pair of steps of all members is recorded once per step
+ * parity into one CUDA graph that forks to the members' streams and joins back, so the
+ * launches of small members run concurrently.  The members stay owned by the caller and
+ * must outlive the ensemble; their states are read with mg_download_state. */
+typedef struct mg_ens mg_ens;
+int mg_ensemble_create(mg_ctx *const *members, int n, mg_ens **out);
+int mg_ensemble_destroy(mg_ens *ens);
+int mg_ensemble_step(mg_ens *ens, int nsteps, int ntime0);
+/* device time of nsteps ensemble steps (CUDA events on the ensemble's stream) */
+int mg_ensemble_time_steps(mg_ens *ens, int nsteps, int ntime0, double *ms);
+/* kernels launched per ensemble step (all members) */
+int mg_ensemble_launch_count(const mg_ens *ens);
+
 /* ---- timing and profiling (no counterpart in the reference, whose only timer is the
  * per-step wall clock of src/MAIN/modelctl.f90:395-397) ---- */
 /* device time of nsteps steps, CUDA events recorded on the context's stream */
