@@ -1,0 +1,41 @@
+"""Forward/backward pairs shaped like an autograd Function, over the C-ABI.
+
+``AdvectionFunction.forward(ctx, x, mu, mv, mw)`` returns the advective tendency
+A(x, m) = -(Tx + Ty + Tz) of one density-weighted field (WENO, the plain FP64 form) and
+saves its inputs; ``backward(ctx, abar)`` returns the vector-Jacobian products
+(xbar, mubar, mvbar, mwbar).  ``jvp`` gives the tangent-linear product.  Arrays are host
+float64 arrays in the reference layout with periodic ghosts filled.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .model import Mimica
+
+
+class FnContext:
+    """Holds what forward saves for backward (the role of autograd's ctx)."""
+
+    def __init__(self, model: Mimica):
+        self.model = model
+        self.saved: tuple = ()
+
+    def save_for_backward(self, *arrays):
+        self.saved = arrays
+
+
+class AdvectionFunction:
+    @staticmethod
+    def forward(ctx: FnContext, x, mu, mv, mw) -> np.ndarray:
+        ctx.save_for_backward(x, mu, mv, mw)
+        return ctx.model.advection_ac(x, mu, mv, mw, np.zeros_like(x))
+
+    @staticmethod
+    def backward(ctx: FnContext, abar):
+        x, mu, mv, mw = ctx.saved
+        return ctx.model.advection_ad(x, mu, mv, mw, abar)
+
+    @staticmethod
+    def jvp(ctx: FnContext, dx, dmu, dmv, dmw) -> np.ndarray:
+        x, mu, mv, mw = ctx.saved
+        return ctx.model.advection_tl(x, mu, mv, mw, dx, dmu, dmv, dmw)

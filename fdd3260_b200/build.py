@@ -38,6 +38,7 @@ SOURCES = [
     ("k_pressure_mixed.cu", []),
     ("capi.cu", []),
     ("noalloc.cu", ["-fmad=false"]),
+    ("k_adjoint.cu", ["-fmad=false"]),
 ]
 
 

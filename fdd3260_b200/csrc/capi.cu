@@ -34,7 +34,7 @@ struct mg_ctx {
     double *sA[MG_MAXF] = {}, *sB[MG_MAXF] = {}, *ts[MG_MAXF] = {};
     double *dens3 = nullptr;
     double *fes = nullptr, *fqt = nullptr;
-    double *unit[8] = {};                // scratch of the unit-level entry points
+    double *unit[16] = {};               // scratch of the unit-level entry points
     PressurePlan *pp = nullptr;
     K1Maps maps1, maps2;                 // TMA descriptors: stage-1 inputs (level n), stage-2 inputs (working)
     K2Maps mmaps1, mmaps2;               // TMA descriptors of the K2 stencil momentum, per stage
@@ -776,6 +776,42 @@ extern "C" int mg_advection_ac(mg_ctx *c, const double *x, const double *mu, con
     CKR(c->prm.precision == MG_PREC_MIXED ? launch_k1_mixed(c->G, a, maps, c->stream) : launch_k1(c->G, a, maps, c->stream));
     CKR(d2h(c, xs, c->unit[4], cudaMemcpyDeviceToHost));
     return check_err(c);
+}
+
+// ---- tangent linear and adjoint of the scalar advection operator (WENO) ----
+extern "C" int mg_advection_tl(mg_ctx *c, const double *x, const double *mu, const double *mv, const double *mw,
+                               const double *dx, const double *dmu, const double *dmv, const double *dmw, double *dA)
+{
+    if (!c || !x || !mu || !mv || !mw || !dx || !dmu || !dmv || !dmw || !dA) return MG_ERR_PARAM;
+    if (c->prm.scal_adv != MG_WENO) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    int rc = ensure_unit(c, 9);
+    if (rc) return rc;
+    const double *in[8] = {x, mu, mv, mw, dx, dmu, dmv, dmw};
+    for (int q = 0; q < 8; q++) CKR(h2d(c, c->unit[q], in[q], cudaMemcpyHostToDevice));
+    CKR(cudaMemsetAsync(c->unit[8], 0, c->fbytes, c->stream));
+    CKR(launch_advection_tl(c->G, c->unit[0], c->unit[1], c->unit[2], c->unit[3], c->unit[4], c->unit[5], c->unit[6],
+                            c->unit[7], c->unit[8], c->stream));
+    CKR(d2h(c, dA, c->unit[8], cudaMemcpyDeviceToHost));
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+extern "C" int mg_advection_ad(mg_ctx *c, const double *x, const double *mu, const double *mv, const double *mw,
+                               const double *Abar, double *xbar, double *mubar, double *mvbar, double *mwbar)
+{
+    if (!c || !x || !mu || !mv || !mw || !Abar || !xbar || !mubar || !mvbar || !mwbar) return MG_ERR_PARAM;
+    if (c->prm.scal_adv != MG_WENO) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    int rc = ensure_unit(c, 14);
+    if (rc) return rc;
+    const double *in[5] = {x, mu, mv, mw, Abar};
+    for (int q = 0; q < 5; q++) CKR(h2d(c, c->unit[q], in[q], cudaMemcpyHostToDevice));
+    double *scratch[5] = {c->unit[9], c->unit[10], c->unit[11], c->unit[12], c->unit[13]};
+    CKR(launch_advection_ad(c->G, c->unit[0], c->unit[1], c->unit[2], c->unit[3], c->unit[4], c->unit[5], c->unit[6],
+                            c->unit[7], c->unit[8], scratch, c->stream));
+    double *outs[4] = {xbar, mubar, mvbar, mwbar};
+    for (int q = 0; q < 4; q++) CKR(d2h(c, outs[q], c->unit[5 + q], cudaMemcpyDeviceToHost));
+    return cuerr(cudaStreamSynchronize(c->stream));
 }
 
 extern "C" int mg_qnadv_uvw(mg_ctx *c, int ntime, const double *mu, const double *mv, const double *mw, double *au,

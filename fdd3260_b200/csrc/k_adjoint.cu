@@ -1,0 +1,239 @@
+// k_adjoint.cu -- tangent-linear and adjoint of the scalar advection operator.
+//
+// The operator is the advective tendency of one density-weighted field x,
+//     A(x, m) = -(Tx + Ty + Tz),  Tx = (F(i+1/2) - F(i-1/2)) * dx1, ...
+// with the WENO3-switch face fluxes of src/TOOLS/advq_weno.f90 (x :61-131, y :134-199,
+// z :202-301) and the advective velocity u = m/rho0 - shift of
+// src/TOOLS/funcpack.f90:65-94 -- the tendency mg_advection_ac adds to xs.
+//
+// The Jacobian of every face flux with respect to its four stencil values and its
+// velocity is obtained by evaluating the forward scheme templates on dual numbers
+// (dual.cuh): the switch to nonlinear weights and the positivity limiter follow the
+// branch the FP64 form takes, and the smoothness weights are differentiated.
+//   TL: dA = J (dx, dm), one thread per cell, both faces of each direction.
+//   AD: (xbar, mbar) = J^T Abar, deterministic two-pass form per direction: a face pass
+//       stores Fbar * J per face, a gather pass sums the four faces that read each
+//       cell; the adjoints of the periodic ghost cells are then folded onto the cells
+//       they are images of.
+#include "dual.cuh"
+#include "mg_common.cuh"
+#include "mimica_gpu.h"
+
+namespace {
+
+using D5 = D<5>;
+
+struct AdvIn {
+    const double *x, *mu, *mv, *mw;
+};
+
+// partials of the face flux of direction dir whose lower cell is (i,j,k):
+// J[m] with respect to the stencil cell (lower - 1 + m) along dir, m = 0..3, and
+// Jv with respect to the momentum that carries the face velocity; returns false when
+// the face does not exist (z faces k+1/2 with k outside 1..nz-1)
+__device__ bool face_jac(const DevGrid &G, int dir, const AdvIn &in, int i, int j, int k, double J[4], double &Jv)
+{
+    const int nz = G.nz;
+    if (dir == 2 && (k < 1 || k > nz - 1)) return false;
+    for (int m = 0; m < 4; m++) J[m] = 0.;
+    Jv = 0.;
+    if (dir == 0 || dir == 1) {
+        const long long st = dir == 0 ? 1 : G.px;
+        const long long c = gidx(G, i, j, k);
+        const double d0 = __ldg(G.den0 + k - 1);
+        const double mom = dir == 0 ? __ldg(in.mu + c + 1) : __ldg(in.mv + c + G.px);
+        const double shift = dir == 0 ? G.u0shift : G.v0shift;
+        const D5 v = D5::var(mom / d0 - shift, 4);
+        const D5 a = D5::var(__ldg(in.x + c - st), 0), b = D5::var(__ldg(in.x + c), 1);
+        const D5 cc = D5::var(__ldg(in.x + c + st), 2), e = D5::var(__ldg(in.x + c + 2 * st), 3);
+        const D5 F = weno_face<D5>(a, b, cc, e, v, true);
+        for (int m = 0; m < 4; m++) J[m] = F.d[m];
+        Jv = F.d[4] / d0;
+        return true;
+    }
+    const long long c = gidx(G, i, j, k);
+    const long long st = G.ps;
+    const double a1 = __ldg(G.avden0 + k);   // w(k+1) carries face k+1/2
+    const D5 w = D5::var(__ldg(in.mw + c + st) / a1, 4);
+    D5 F;
+    if (k == 1) {   // bottom face: x(1), x(2), x(3) at stencil positions 1..3
+        const D5 x1 = D5::var(__ldg(in.x + c), 1), x2 = D5::var(__ldg(in.x + c + st), 2);
+        const D5 x3 = D5::var(__ldg(in.x + c + 2 * st), 3);
+        F = weno_face_bottom<D5>(x1, x2, x3, w);
+    } else if (k == nz - 1) {   // top face: x(nz-2), x(nz-1), x(nz) at positions 0..2
+        const D5 a = D5::var(__ldg(in.x + c - st), 0), b = D5::var(__ldg(in.x + c), 1);
+        const D5 cc = D5::var(__ldg(in.x + c + st), 2);
+        F = weno_face_top<D5>(a, b, cc, w);
+    } else {
+        const D5 a = D5::var(__ldg(in.x + c - st), 0), b = D5::var(__ldg(in.x + c), 1);
+        const D5 cc = D5::var(__ldg(in.x + c + st), 2), e = D5::var(__ldg(in.x + c + 2 * st), 3);
+        F = weno_face<D5>(a, b, cc, e, w, k >= 3 && k <= nz - 3);
+    }
+    for (int m = 0; m < 4; m++) J[m] = F.d[m];
+    Jv = F.d[4] / a1;
+    return true;
+}
+
+__device__ __forceinline__ double face_metric(const DevGrid &G, int dir, int k)
+{
+    return dir == 0 ? 1. / G.dx : (dir == 1 ? 1. / G.dy : __ldg(G.dz1w + k - 1));
+}
+
+// ---- tangent linear: dA over the interior ----
+__global__ void adv_tl_kernel(DevGrid G, AdvIn in, AdvIn d, double *dA)
+{
+    const int maxx = G.maxx, maxy = G.maxy;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)maxx * maxy * G.nz) return;
+    const int i = (int)(t % maxx) + 4, j = (int)((t / maxx) % maxy) + 4, k = (int)(t / ((long long)maxx * maxy)) + 1;
+    double acc = 0.;
+    for (int dir = 0; dir < 3; dir++) {
+        const long long st = dir == 0 ? 1 : (dir == 1 ? G.px : G.ps);
+        const double *dm = dir == 0 ? d.mu : (dir == 1 ? d.mv : d.mw);
+        double dF[2] = {0., 0.};
+        for (int s = 0; s < 2; s++) {   // faces c-1/2 (lower cell c-1) and c+1/2 (lower cell c)
+            const int li = dir == 0 ? i - 1 + s : i, lj = dir == 1 ? j - 1 + s : j, lk = dir == 2 ? k - 1 + s : k;
+            double J[4], Jv;
+            if (!face_jac(G, dir, in, li, lj, lk, J, Jv)) continue;
+            const long long lc = gidx(G, li, lj, lk);
+            double v = 0.;
+            for (int m = 0; m < 4; m++)
+                if (J[m] != 0.) v += J[m] * __ldg(d.x + lc + (m - 1) * st);
+            v += Jv * __ldg(dm + lc + st);
+            dF[s] = v;
+        }
+        acc += (dF[1] - dF[0]) * face_metric(G, dir, k);
+    }
+    dA[gidx(G, i, j, k)] = -acc;
+}
+
+// ---- adjoint, face pass of one direction: g[m][face] = Fbar * J[m], gv[face] = Fbar * Jv ----
+__global__ void adv_ad_face_kernel(DevGrid G, int dir, AdvIn in, const double *Abar, double *g0, double *g1,
+                                   double *g2, double *g3, double *gv)
+{
+    // faces indexed by their lower cell: x: i in [3, nx-2] (j, k interior); y: j in
+    // [3, ny-2]; z: k in [1, nz-1]
+    const int maxx = G.maxx, maxy = G.maxy, nz = G.nz;
+    const int ni = dir == 0 ? maxx + 1 : maxx, nj = dir == 1 ? maxy + 1 : maxy, nk = dir == 2 ? nz - 1 : nz;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ni * nj * nk) return;
+    const int i = (int)(t % ni) + (dir == 0 ? 3 : 4), j = (int)((t / ni) % nj) + (dir == 1 ? 3 : 4);
+    const int k = (int)(t / ((long long)ni * nj)) + 1;
+    const long long c = gidx(G, i, j, k);
+    const long long st = dir == 0 ? 1 : (dir == 1 ? G.px : G.ps);
+    auto interior = [&](int ii, int jj, int kk) { return ii >= 4 && ii <= G.nx - 2 && jj >= 4 && jj <= G.ny - 2 && kk >= 1 && kk <= nz; };
+    // A(lower) has -F*metric(lower), A(upper) has +F*metric(upper)
+    const int ui = dir == 0 ? i + 1 : i, uj = dir == 1 ? j + 1 : j, uk = dir == 2 ? k + 1 : k;
+    double Fbar = 0.;
+    if (interior(i, j, k)) Fbar -= Abar[c] * face_metric(G, dir, k);
+    if (interior(ui, uj, uk)) Fbar += Abar[c + st] * face_metric(G, dir, uk);
+    double J[4], Jv;
+    if (!face_jac(G, dir, in, i, j, k, J, Jv)) {
+        J[0] = J[1] = J[2] = J[3] = Jv = 0.;
+    }
+    g0[c] = Fbar * J[0];
+    g1[c] = Fbar * J[1];
+    g2[c] = Fbar * J[2];
+    g3[c] = Fbar * J[3];
+    gv[c] = Fbar * Jv;
+}
+
+// ---- adjoint, gather pass of one direction over every cell (ghosts included) ----
+__global__ void adv_ad_gather_kernel(DevGrid G, int dir, const double *g0, const double *g1, const double *g2,
+                                     const double *g3, const double *gv, double *xbar, double *mbar)
+{
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nx * ny * nz) return;
+    const int i = (int)(t % nx) + 1, j = (int)((t / nx) % ny) + 1, k = (int)(t / ((long long)nx * ny)) + 1;
+    const long long c = gidx(G, i, j, k);
+    const long long st = dir == 0 ? 1 : (dir == 1 ? G.px : G.ps);
+    // face with lower cell l exists for: x: l in [3, nx-2], j, k interior; y likewise; z: l in [1, nz-1]
+    auto face_ok = [&](int l) {
+        if (dir == 0) return l >= 3 && l <= nx - 2 && j >= 4 && j <= ny - 2;
+        if (dir == 1) return l >= 3 && l <= ny - 2 && i >= 4 && i <= nx - 2;
+        return l >= 1 && l <= nz - 1 && i >= 4 && i <= nx - 2 && j >= 4 && j <= ny - 2;
+    };
+    const int p = dir == 0 ? i : (dir == 1 ? j : k);
+    double s = 0.;
+    // cell p is stencil position m of the face with lower cell p + 1 - m
+    if (face_ok(p + 1)) s += g0[c + st];
+    if (face_ok(p)) s += g1[c];
+    if (face_ok(p - 1)) s += g2[c - st];
+    if (face_ok(p - 2)) s += g3[c - 2 * st];
+    xbar[c] += s;
+    // the face with lower cell p-1 is carried by the velocity at index p
+    if (face_ok(p - 1)) mbar[c] += gv[c - st];
+}
+
+// adjoint of the periodic ghost images: ghost columns then ghost rows are added onto
+// the cells they copy, then zeroed (each destination receives from one ghost per pass)
+__global__ void fold_x_kernel(DevGrid G, double *f)
+{
+    const int ny = G.ny, nz = G.nz, maxx = G.maxx;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 5LL * ny * nz) return;
+    const int q = (int)(t % 5), j = (int)((t / 5) % ny) + 1, k = (int)(t / (5LL * ny)) + 1;
+    const int gi = q < 3 ? q + 1 : G.nx - 4 + q;   // 1,2,3, nx-1, nx
+    const int si = gi <= 3 ? gi + maxx : gi - maxx;
+    const long long gc = gidx(G, gi, j, k);
+    f[gidx(G, si, j, k)] += f[gc];
+    f[gc] = 0.;
+}
+__global__ void fold_y_kernel(DevGrid G, double *f)
+{
+    const int nx = G.nx, nz = G.nz, maxy = G.maxy;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 5LL * nx * nz) return;
+    const int i = (int)(t % nx) + 1, q = (int)((t / nx) % 5), k = (int)(t / (5LL * nx)) + 1;
+    const int gj = q < 3 ? q + 1 : G.ny - 4 + q;
+    const int sj = gj <= 3 ? gj + maxy : gj - maxy;
+    const long long gc = gidx(G, i, gj, k);
+    f[gidx(G, i, sj, k)] += f[gc];
+    f[gc] = 0.;
+}
+
+inline unsigned nblk(long long n) { return (unsigned)((n + 255) / 256); }
+
+}  // namespace
+
+cudaError_t launch_advection_tl(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
+                                const double *dx, const double *dmu, const double *dmv, const double *dmw, double *dA,
+                                cudaStream_t s)
+{
+    const long long n = (long long)g.maxx * g.maxy * g.nz;
+    adv_tl_kernel<<<nblk(n), 256, 0, s>>>(g, AdvIn{x, mu, mv, mw}, AdvIn{dx, dmu, dmv, dmw}, dA);
+    return cudaGetLastError();
+}
+
+// xbar, mubar, mvbar, mwbar are overwritten; scratch: 5 fields
+cudaError_t launch_advection_ad(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
+                                const double *Abar, double *xbar, double *mubar, double *mvbar, double *mwbar,
+                                double *const *scratch, cudaStream_t s)
+{
+    const size_t fbytes = (size_t)g.ps * g.nz * 8;
+    cudaError_t e;
+    double *outs[4] = {xbar, mubar, mvbar, mwbar};
+    for (int q = 0; q < 4; q++)
+        if ((e = cudaMemsetAsync(outs[q], 0, fbytes, s)) != cudaSuccess) return e;
+    const AdvIn in{x, mu, mv, mw};
+    const long long ncell = (long long)g.nx * g.ny * g.nz;
+    for (int dir = 0; dir < 3; dir++) {
+        for (int q = 0; q < 5; q++)
+            if ((e = cudaMemsetAsync(scratch[q], 0, fbytes, s)) != cudaSuccess) return e;
+        const long long nf = (long long)(dir == 0 ? g.maxx + 1 : g.maxx) * (dir == 1 ? g.maxy + 1 : g.maxy) *
+                             (dir == 2 ? g.nz - 1 : g.nz);
+        adv_ad_face_kernel<<<nblk(nf), 256, 0, s>>>(g, dir, in, Abar, scratch[0], scratch[1], scratch[2], scratch[3],
+                                                    scratch[4]);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        double *mb = dir == 0 ? mubar : (dir == 1 ? mvbar : mwbar);
+        adv_ad_gather_kernel<<<nblk(ncell), 256, 0, s>>>(g, dir, scratch[0], scratch[1], scratch[2], scratch[3],
+                                                         scratch[4], xbar, mb);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    for (int q = 0; q < 4; q++) {
+        fold_x_kernel<<<nblk(5LL * g.ny * g.nz), 256, 0, s>>>(g, outs[q]);
+        fold_y_kernel<<<nblk(5LL * g.nx * g.nz), 256, 0, s>>>(g, outs[q]);
+    }
+    return cudaGetLastError();
+}

@@ -101,6 +101,14 @@ cudaError_t launch_k2(const DevGrid &g, const K2Args &a, const K2Maps &maps, cud
 cudaError_t launch_k2_mixed(const DevGrid &g, const K2Args &a, const K2Maps &maps, cudaStream_t s);
 cudaError_t launch_halo_fill(const DevGrid &g, double *const *fields, int nf, cudaStream_t s);
 
+// tangent linear / adjoint of the scalar advection operator (k_adjoint.cu)
+cudaError_t launch_advection_tl(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
+                                const double *dx, const double *dmu, const double *dmv, const double *dmw, double *dA,
+                                cudaStream_t s);
+cudaError_t launch_advection_ad(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
+                                const double *Abar, double *xbar, double *mubar, double *mvbar, double *mwbar,
+                                double *const *scratch, cudaStream_t s);
+
 // projection
 struct PressurePlan;
 cudaError_t pressure_plan_create(const DevGrid &g, const double *wv_host, int mixed, PressurePlan **out,

@@ -101,6 +101,21 @@ class Mimica:
                                            _lib.ptr(mw), _lib.ptr(xs)), "mg_advection_ac")
         return xs
 
+    def advection_tl(self, x, mu, mv, mw, dx, dmu, dmv, dmw) -> np.ndarray:
+        """Tangent linear of the advective tendency A(x, m) = -(Tx+Ty+Tz) (WENO)."""
+        out = np.zeros(self.domain.shape)
+        args = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, mu, mv, mw, dx, dmu, dmv, dmw)]
+        _lib.check(self._L.mg_advection_tl(self._h, *[_lib.ptr(a) for a in args], _lib.ptr(out)), "mg_advection_tl")
+        return out
+
+    def advection_ad(self, x, mu, mv, mw, abar):
+        """Adjoint of the advective tendency: returns (xbar, mubar, mvbar, mwbar)."""
+        outs = [np.zeros(self.domain.shape) for _ in range(4)]
+        args = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, mu, mv, mw, abar)]
+        _lib.check(self._L.mg_advection_ad(self._h, *[_lib.ptr(a) for a in args], *[_lib.ptr(o) for o in outs]),
+                   "mg_advection_ad")
+        return tuple(outs)
+
     def qnadv_uvw(self, mu, mv, mw, ntime: int = 1):
         """src/INTEG/windadv.f90:46 qnadv_uvw; returns (au, av, aw)."""
         d = self.domain

@@ -177,6 +177,22 @@ int mg_fft_solve(mg_ctx *ctx, const double *tend, double *out);
 int mg_anelastic_pressure(mg_ctx *ctx, double *mu, double *mv, double *mw, double *p,
                           const double *wold, double *maxdiv, double *p1);
 
+/* ---- tangent linear and adjoint of the scalar advection operator (WENO; no counterpart
+ * in the reference, whose adjoint does not exist) ----
+ * The operator is the advective tendency A(x, m) = -(Tx + Ty + Tz) that mg_advection_ac
+ * adds to xs, as a function of the density-weighted field x and of the momentum
+ * (mu, mv, mw) that carries the face velocities.  The face Jacobians include the
+ * differentiated smoothness weights and positivity limiter, along the branches the FP64
+ * form takes.  Host arrays, reference layout, periodic ghosts filled by the caller.
+ *   mg_advection_tl: dA = dA/dx . dx + dA/dm . dm     (interior; ghosts of dA are 0)
+ *   mg_advection_ad: xbar = (dA/dx)^T Abar, mbar = (dA/dm)^T Abar (outputs overwritten;
+ *                    the adjoints of the periodic ghost images are folded onto the
+ *                    interior cells they copy, so ghost entries are 0) */
+int mg_advection_tl(mg_ctx *ctx, const double *x, const double *mu, const double *mv, const double *mw,
+                    const double *dx, const double *dmu, const double *dmv, const double *dmw, double *dA);
+int mg_advection_ad(mg_ctx *ctx, const double *x, const double *mu, const double *mv, const double *mw,
+                    const double *Abar, double *xbar, double *mubar, double *mvbar, double *mwbar);
+
 /* ---- allocation-free entry (no counterpart in the reference) ----
  * The projection residual of pressure_solver.f90:121-130 (signed max of the
  * divergence over the interior, k = 2..nz-1), computed without a context and without
