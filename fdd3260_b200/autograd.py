@@ -39,3 +39,23 @@ class AdvectionFunction:
     def jvp(ctx: FnContext, dx, dmu, dmv, dmw) -> np.ndarray:
         x, mu, mv, mw = ctx.saved
         return ctx.model.advection_tl(x, mu, mv, mw, dx, dmu, dmv, dmw)
+
+
+class ProjectionFunction:
+    """anelastic_pressure as a map of (mu, mv, mw, p): affine, linear in the momentum."""
+
+    @staticmethod
+    def forward(ctx: FnContext, mu, mv, mw, p):
+        ctx.save_for_backward()
+        z = np.zeros_like(mw)
+        out = ctx.model.anelastic_pressure(mu, mv, mw, p, z)
+        return out[:4]
+
+    @staticmethod
+    def backward(ctx: FnContext, mub, mvb, mwb, pb):
+        return ctx.model.anelastic_pressure_ad(mub, mvb, mwb, pb)
+
+    @staticmethod
+    def jvp(ctx: FnContext, dmu, dmv, dmw, dp):
+        z = np.zeros_like(dmw)
+        return ctx.model.anelastic_pressure(dmu, dmv, dmw, dp, z)[:4]

@@ -814,6 +814,21 @@ extern "C" int mg_advection_ad(mg_ctx *c, const double *x, const double *mu, con
     return cuerr(cudaStreamSynchronize(c->stream));
 }
 
+// ---- adjoint of the projection (anelastic_pressure, FP64 contexts) ----
+extern "C" int mg_anelastic_pressure_ad(mg_ctx *c, double *mub, double *mvb, double *mwb, double *pb)
+{
+    if (!c || !mub || !mvb || !mwb || !pb) return MG_ERR_PARAM;
+    if (c->prm.precision != MG_PREC_FP64) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    int rc = ensure_unit(c, 4);
+    if (rc) return rc;
+    double *io[4] = {mub, mvb, mwb, pb};
+    for (int q = 0; q < 4; q++) CKR(h2d(c, c->unit[q], io[q], cudaMemcpyHostToDevice));
+    CKR(pressure_adjoint(c->G, c->pp, c->prm.nsubp, c->unit[0], c->unit[1], c->unit[2], c->unit[3], c->stream));
+    for (int q = 0; q < 4; q++) CKR(d2h(c, io[q], c->unit[q], cudaMemcpyDeviceToHost));
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
 extern "C" int mg_qnadv_uvw(mg_ctx *c, int ntime, const double *mu, const double *mv, const double *mw, double *au,
                             double *av, double *aw)
 {

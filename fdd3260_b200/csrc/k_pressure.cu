@@ -790,6 +790,7 @@ struct PressurePlan {
     double *partial = nullptr, *maxdiv = nullptr;
     unsigned long long *resid = nullptr;   // [MG_MAXPASS] residual per pass of the current projection
     double *bsum = nullptr;                // [nz][row groups] sums of b (refined projection)
+    double *gamT = nullptr, *akT = nullptr, *ckT = nullptr;   // transposed system (adjoint), built on first use
     int npartial = 0;
     size_t bytes = 0;
 };
@@ -920,6 +921,7 @@ void pressure_plan_destroy(PressurePlan *pp)
     cudaFree(pp->gam); cudaFree(pp->wv); cudaFree(pp->ak); cudaFree(pp->ck); cudaFree(pp->dka); cudaFree(pp->dkb);
     cudaFree(pp->mean); cudaFree(pp->mean_d); cudaFree(pp->p1); cudaFree(pp->partial); cudaFree(pp->maxdiv);
     cudaFree(pp->resid); cudaFree(pp->bsum);
+    cudaFree(pp->gamT); cudaFree(pp->akT); cudaFree(pp->ckT);
     delete pp;
 }
 
@@ -998,7 +1000,7 @@ cudaError_t launch_load_rhs(const DevGrid &g, PressurePlan *pp, const double *te
 
 template <typename C>
 static cudaError_t pressure_solve_t(const DevGrid &g, PressurePlan *pp, int keep00, Skip sk, int accumulate,
-                                    cudaStream_t s)
+                                    cudaStream_t s, int transposed = 0)
 {
     cudaError_t e;
     const int nh = g.maxx / 2 + 1;
@@ -1011,6 +1013,7 @@ static cudaError_t pressure_solve_t(const DevGrid &g, PressurePlan *pp, int keep
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     TriArgs T{};
     T.spec = pp->spec; T.gam = pp->gam; T.wv = pp->wv; T.ak = pp->ak; T.ck = pp->ck; T.dka = pp->dka; T.dkb = pp->dkb;
+    if (transposed) { T.gam = pp->gamT; T.ak = pp->akT; T.ck = pp->ckT; }
     T.keep00 = keep00;
     T.sk = sk;
     T.scratch = pp->tri;
@@ -1112,4 +1115,124 @@ cudaError_t launch_to_natural(const DevGrid &g, const double *src, const double 
 {
     to_natural_kernel<<<1184, 256, 0, s>>>(g, src, w, weight_kind, rep, dst);
     return cudaGetLastError();
+}
+
+// ======================== adjoint of the projection ========================
+// One projection pass maps (m, p) to
+//   m' = m - dt0 * R * G(dp),  p' = p + rho0 * dp,  dp = S(b),  b = D(m) * dt1 / rho0,
+// with G the backward-difference gradient of correction_kernel (the bottom w row is set
+// to zero from m_w(1) itself), S the transforms + tridiagonal solve (mode (0,0) zero,
+// 1/N_h), D the divergence of fft_x_fwd, R = rho0 (u, v) or avden0 (w); cal_p1 then
+// removes the level mean of w.  Its adjoint, pass by pass in reverse:
+//   dpbar = rho0 * pbar - dt0 * G^T(R mbar),  bbar = S^T(dpbar),  mbar <- Z mbar + D^T(bbar dt1/rho0)
+// where S^T has the same transforms around the transposed tridiagonal and Z zeroes the
+// bottom w row.  Arrays: halo'd layout, interior adjoints, ghosts zero.
+namespace {
+
+__global__ void adj_sub_level_mean_kernel(DevGrid G, double *x, const double *mean)
+{
+    const int maxx = G.maxx, maxy = G.maxy;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)maxx * maxy * G.nz) return;
+    const int ix = (int)(t % maxx), jy = (int)((t / maxx) % maxy), k = (int)(t / ((long long)maxx * maxy)) + 1;
+    const long long c = gidx(G, ix + 4, jy + 4, k);
+    x[c] = x[c] - mean[k - 1];
+}
+
+// dpbar (dense interior [nz][maxy][maxx]) = rho0 pbar - dt0 G^T(R mbar)
+__global__ void adj_rhs_kernel(DevGrid G, const double *mub, const double *mvb, const double *mwb, const double *pb,
+                               double *out)
+{
+    const int maxx = G.maxx, maxy = G.maxy, nz = G.nz;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)maxx * maxy * nz) return;
+    const int ix = (int)(t % maxx), jy = (int)((t / maxx) % maxy), k = (int)(t / ((long long)maxx * maxy)) + 1;
+    const int i = ix + 4, j = jy + 4;
+    const long long c = gidx(G, i, j, k);
+    const double d0 = __ldg(G.den0 + k - 1);
+    const double dx1 = 1. / G.dx, dy1 = 1. / G.dy;
+    // G_x dp(i) = (dp(i) - dp(i-1)) dx1 (periodic): G_x^T q(i) = (q(i) - q(i+1)) dx1
+    const long long ce = gidx(G, ix == maxx - 1 ? 4 : i + 1, j, k);
+    const long long cn = gidx(G, i, jy == maxy - 1 ? 4 : j + 1, k);
+    double gt = (d0 * mub[c] - d0 * mub[ce]) * dx1 + (d0 * mvb[c] - d0 * mvb[cn]) * dy1;
+    // G_z dp(k) = (dp(k) - dp(k-1)) dz1(k-1), k >= 2
+    if (k >= 2) gt += __ldg(G.avden0 + k - 1) * mwb[c] * __ldg(G.dz1 + k - 2);
+    if (k + 1 <= nz) gt -= __ldg(G.avden0 + k) * mwb[c + G.ps] * __ldg(G.dz1 + k - 1);
+    out[t] = d0 * pb[c] - G.dt0 * gt;
+}
+
+// mbar <- Z mbar + D^T(q), q = bbar * dt1 / rho0 (dense interior bbar = dp)
+__global__ void adj_div_kernel(DevGrid G, const double *bbar, double *mub, double *mvb, double *mwb)
+{
+    const int maxx = G.maxx, maxy = G.maxy, nz = G.nz;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)maxx * maxy * nz) return;
+    const int ix = (int)(t % maxx), jy = (int)((t / maxx) % maxy), k = (int)(t / ((long long)maxx * maxy)) + 1;
+    const int i = ix + 4, j = jy + 4;
+    const long long c = gidx(G, i, j, k);
+    const double dt1 = 1. / G.dt0, dx1 = 1. / G.dx, dy1 = 1. / G.dy;
+    auto Q = [&](int a, int b, int kk) {
+        return bbar[((long long)(kk - 1) * maxy + b) * maxx + a] * (dt1 / __ldg(G.den0 + kk - 1));
+    };
+    const double q = Q(ix, jy, k);
+    // D: (mu(i+1) - mu(i)) dx1 + (mv(j+1) - mv(j)) dy1 + (mw(k+1) - mw(k)) dzw1(k), mw(nz+1) = 0
+    mub[c] += (Q(ix == 0 ? maxx - 1 : ix - 1, jy, k) - q) * dx1;
+    mvb[c] += (Q(ix, jy == 0 ? maxy - 1 : jy - 1, k) - q) * dy1;
+    double wz = -q * __ldg(G.dz1w + k - 1);
+    if (k >= 2) wz += Q(ix, jy, k - 1) * __ldg(G.dz1w + k - 2);
+    mwb[c] = (k == 1 ? 0. : mwb[c]) + wz;
+}
+
+}  // namespace
+
+cudaError_t pressure_adjoint(const DevGrid &g, PressurePlan *pp, int nsubp, double *mub, double *mvb, double *mwb,
+                             double *pb, cudaStream_t s)
+{
+    if (pp->mixed) return cudaErrorInvalidValue;   // the adjoint runs in FP64
+    cudaError_t e;
+    const int nz = g.nz, nh = g.maxx / 2 + 1;
+    const long long ncol = (long long)nh * g.maxy;
+    if (!pp->gamT) {   // transposed system: sub-diagonal c(k-1), super-diagonal a(k+1)
+        std::vector<double> ak(nz), ck(nz), akT(nz, 0.), ckT(nz, 0.);
+        if ((e = cudaMemcpy(ak.data(), pp->ak, nz * 8, cudaMemcpyDeviceToHost)) != cudaSuccess) return e;
+        if ((e = cudaMemcpy(ck.data(), pp->ck, nz * 8, cudaMemcpyDeviceToHost)) != cudaSuccess) return e;
+        for (int k = 2; k <= nz; k++) akT[k - 1] = ck[k - 2];
+        for (int k = 1; k <= nz - 1; k++) ckT[k - 1] = ak[k];
+        if ((e = cudaMalloc(&pp->akT, nz * 8)) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&pp->ckT, nz * 8)) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&pp->gamT, (size_t)nz * ncol * 8)) != cudaSuccess) return e;
+        if ((e = cudaMemcpy(pp->akT, akT.data(), nz * 8, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+        if ((e = cudaMemcpy(pp->ckT, ckT.data(), nz * 8, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+        int *derr;
+        if ((e = cudaMalloc(&derr, sizeof(int))) != cudaSuccess) return e;
+        cudaMemset(derr, 0, sizeof(int));
+        TriArgs T{};
+        T.wv = pp->wv; T.ak = pp->akT; T.ck = pp->ckT; T.dka = pp->dka; T.dkb = pp->dkb;
+        gam_kernel<<<(unsigned)((ncol + 255) / 256), 256>>>(g, T, pp->gamT, derr);
+        e = cudaGetLastError();
+        int herr = 0;
+        if (e == cudaSuccess) e = cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
+        cudaFree(derr);
+        if (e != cudaSuccess) return e;
+        if (herr) return cudaErrorInvalidValue;
+    }
+    const long long n = (long long)g.maxx * g.maxy * nz;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    // cal_p1^T: remove the level mean of wbar (interior)
+    level_sums<<<nz, 256, 0, s>>>(g, mwb, mwb, -1, g.dt0, pp->mean, nullptr);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    adj_sub_level_mean_kernel<<<nb, 256, 0, s>>>(g, mwb, pp->mean);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    for (int ip = 0; ip < nsubp; ip++) {
+        adj_rhs_kernel<<<nb, 256, 0, s>>>(g, mub, mvb, mwb, pb, pp->rbuf);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        XArgs a{};
+        a.mode = 1;
+        a.rbuf = pp->rbuf; a.spec = pp->spec;
+        if ((e = launch_x_fwd(g, pp, a, s)) != cudaSuccess) return e;
+        if ((e = pressure_solve_t<double2>(g, pp, 0, Skip{nullptr, 0.}, 0, s, 1)) != cudaSuccess) return e;
+        adj_div_kernel<<<nb, 256, 0, s>>>(g, pp->dp, mub, mvb, mwb);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }

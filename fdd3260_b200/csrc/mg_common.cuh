@@ -162,6 +162,10 @@ cudaError_t launch_maxdiv(const DevGrid &g, PressurePlan *pp, const double *mu, 
 const double *pressure_p1_dev(const PressurePlan *pp);
 const double *pressure_maxdiv_dev(const PressurePlan *pp);
 
+// adjoint of anelastic_pressure (nsubp passes + cal_p1) on interior adjoints, in place
+cudaError_t pressure_adjoint(const DevGrid &g, PressurePlan *pp, int nsubp, double *mub, double *mvb, double *mwb,
+                             double *pb, cudaStream_t s);
+
 // natural <-> resident conversions for download
 cudaError_t launch_to_natural(const DevGrid &g, const double *src, const double *w, int weight_kind,
                               int rep, double *dst, cudaStream_t s);

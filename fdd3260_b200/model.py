@@ -116,6 +116,12 @@ class Mimica:
                    "mg_advection_ad")
         return tuple(outs)
 
+    def anelastic_pressure_ad(self, mub, mvb, mwb, pb):
+        """Adjoint of anelastic_pressure (the momentum/pressure map): returns (mub, mvb, mwb, pb)."""
+        io = [np.array(a, dtype=np.float64, copy=True) for a in (mub, mvb, mwb, pb)]
+        _lib.check(self._L.mg_anelastic_pressure_ad(self._h, *[_lib.ptr(a) for a in io]), "mg_anelastic_pressure_ad")
+        return tuple(io)
+
     def qnadv_uvw(self, mu, mv, mw, ntime: int = 1):
         """src/INTEG/windadv.f90:46 qnadv_uvw; returns (au, av, aw)."""
         d = self.domain

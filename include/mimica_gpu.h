@@ -193,6 +193,13 @@ int mg_advection_tl(mg_ctx *ctx, const double *x, const double *mu, const double
 int mg_advection_ad(mg_ctx *ctx, const double *x, const double *mu, const double *mv, const double *mw,
                     const double *Abar, double *xbar, double *mubar, double *mvbar, double *mwbar);
 
+/* Adjoint of anelastic_pressure (pressure_solver.f90:73-140: nsubp passes of solve +
+ * correction, then the level-mean removal of w) as a map of the momentum and pressure;
+ * the map is affine (linear in m), so its tangent linear is mg_anelastic_pressure itself.
+ * In place: (mubar, mvbar, mwbar, pbar) := adjoint applied to them (interior values;
+ * ghosts 0).  FP64 contexts only. */
+int mg_anelastic_pressure_ad(mg_ctx *ctx, double *mubar, double *mvbar, double *mwbar, double *pbar);
+
 /* ---- allocation-free entry (no counterpart in the reference) ----
  * The projection residual of pressure_solver.f90:121-130 (signed max of the
  * divergence over the interior, k = 2..nz-1), computed without a context and without

@@ -120,3 +120,32 @@ def test_taylor():
     ratios = [rem[q] / rem[q + 1] for q in range(len(rem) - 1)]
     assert all(80.0 < rt < 125.0 for rt in ratios), (rem, ratios)
     assert rem[-1] < 1e-6 * first[-1]
+
+
+@pytest.mark.parametrize("nsubp", [1, 2])
+def test_projection_dot_product(nsubp):
+    """<P(dm, dp), (mbar, pbar)> = <(dm, dp), P^T(mbar, pbar)> over the interior."""
+    from fdd3260_b200.autograd import ProjectionFunction
+    d = config.cumulus_domain(32, 32, 24, nsubp=nsubp)
+    rng = np.random.default_rng(40 + nsubp)
+
+    def field(scale, bottom_zero=False):
+        a = np.zeros(d.shape)
+        a[:, 3:-2, 3:-2] = scale * rng.standard_normal(_interior(a).shape)
+        if bottom_zero:
+            a[0] = 0.0
+        return config.periodic_fill(a)
+
+    dm = [field(1.0), field(1.0), field(0.5, bottom_zero=True)]
+    dp = field(10.0)
+    bars = [field(1.0), field(1.0), field(0.5), field(1.0)]
+    for b in bars:   # adjoint inputs live on the interior
+        b[:, :3, :] = 0.0; b[:, -2:, :] = 0.0; b[:, :, :3] = 0.0; b[:, :, -2:] = 0.0
+    with Mimica(d, nscal=2) as m:
+        ctx = FnContext(m)
+        out = ProjectionFunction.jvp(ctx, *dm, dp)
+        back = ProjectionFunction.backward(ctx, *bars)
+    lhs = sum(float(np.sum(_interior(o) * _interior(b))) for o, b in zip(out, bars))
+    rhs = sum(float(np.sum(_interior(x) * _interior(y))) for x, y in zip(dm + [dp], back))
+    scale = sum(float(np.sum(np.abs(_interior(o) * _interior(b)))) for o, b in zip(out, bars))
+    assert abs(lhs - rhs) <= 1e-12 * scale, (lhs, rhs, scale)
