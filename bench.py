@@ -297,6 +297,8 @@ def main():
             del out
         m.upload(st)
         r.update(time_form(args, m, d, st, use_graph, ws, local))
+        if form == "fp64" and args.scheme == "weno":
+            r["adjoint"] = adjoint_leg(m)
         if form == forms[0]:
             r.update(e2e_leg(args, m, d, st, ws))
         r["device_bytes"] = m.device_bytes
@@ -334,6 +336,8 @@ def main():
                 line["mixed"]["fp64_twin_1e-9_error"] = head.get("twin_error")
                 line["mixed"]["maxdiv"] = mx["maxdiv"]
                 line["mixed"]["maxdiv_fp64"] = head.get("maxdiv")
+        if "adjoint" in head:
+            line["adjoint"] = head["adjoint"]
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
@@ -437,6 +441,20 @@ def run_ensemble(args, ws, rank, local):
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def adjoint_leg(m, reps: int = 3) -> dict:
+    """Device time of the hand-written tangent-linear and adjoint kernels against their
+    forward operators, on copies of the resident state (mg_time_adjoint)."""
+    out = (C.c_double * 5)()
+    rc = m._L.mg_time_adjoint(m._h, reps, out)
+    if rc:
+        return {"error": rc}
+    f = list(out)
+    return {"advection_fwd_ms": f[0], "advection_tl_ms": f[1], "advection_ad_ms": f[2],
+            "advection_ad_over_fwd": f[2] / f[0], "projection_fwd_ms": f[3], "projection_ad_ms": f[4],
+            "projection_ad_over_fwd": f[4] / f[3],
+            "note": "operator level: one density-weighted field (WENO) and one anelastic_pressure call"}
 
 
 def field_errors(out, ref, st0, nsteps: int) -> dict:

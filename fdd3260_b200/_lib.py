@@ -82,6 +82,7 @@ def lib() -> C.CDLL:
         L.mg_advection_tl.argtypes = [vp] + [_dp] * 9
         L.mg_advection_ad.argtypes = [vp] + [_dp] * 9
         L.mg_anelastic_pressure_ad.argtypes = [vp] + [_dp] * 4
+        L.mg_time_adjoint.argtypes = [vp, C.c_int, _dp]
         L.mg_ensemble_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
         L.mg_ensemble_destroy.argtypes = [vp]
         L.mg_ensemble_step.argtypes = [vp, C.c_int, C.c_int]
@@ -117,5 +118,5 @@ EXPORTED = [
     "mg_device_bytes", "mg_upload_state", "mg_download_state", "mg_upload_state_device", "mg_download_state_device",
     "mg_step", "mg_step_graph", "mg_synchronize", "mg_last_launch_count", "mg_advection_ac", "mg_qnadv_uvw",
     "mg_fft_solve", "mg_anelastic_pressure", "mg_time_steps", "mg_profile_enable", "mg_profile_report",
-    "mg_advection_tl", "mg_advection_ad", "mg_anelastic_pressure_ad", "mg_ensemble_create", "mg_ensemble_destroy", "mg_ensemble_step", "mg_ensemble_time_steps", "mg_ensemble_launch_count",
+    "mg_advection_tl", "mg_advection_ad", "mg_anelastic_pressure_ad", "mg_time_adjoint", "mg_ensemble_create", "mg_ensemble_destroy", "mg_ensemble_step", "mg_ensemble_time_steps", "mg_ensemble_launch_count",
 ]

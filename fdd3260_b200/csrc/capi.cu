@@ -829,6 +829,63 @@ extern "C" int mg_anelastic_pressure_ad(mg_ctx *c, double *mub, double *mvb, dou
     return cuerr(cudaStreamSynchronize(c->stream));
 }
 
+// ---- device time of the operators and their adjoints on the resident state ----
+// out[0]: advection (unit K1 on one field), out[1]: its tangent linear, out[2]: its
+// adjoint, out[3]: anelastic_pressure (nsubp passes + cal_p1), out[4]: its adjoint; ms per
+// call, averaged over reps after one untimed call of each.  The operands are copies of
+// the resident state (density-weighted first scalar, momentum); FP64 contexts, WENO.
+extern "C" int mg_time_adjoint(mg_ctx *c, int reps, double *out)
+{
+    if (!c || reps < 1 || !out) return MG_ERR_PARAM;
+    if (!c->have_state) return MG_ERR_STATE;
+    if (c->prm.precision != MG_PREC_FP64 || c->prm.scal_adv != MG_WENO) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    int rc = ensure_unit(c, 14);
+    if (rc) return rc;
+    const size_t fb = c->fbytes;
+    double **u = c->unit;
+    // x, mu, mv, mw from the state; dx, dm = the same fields (any perturbation costs the same)
+    CKR(cudaMemcpyAsync(u[0], c->sA[c->nf > 1 ? 1 : 0], fb, cudaMemcpyDeviceToDevice, c->stream));
+    for (int q = 0; q < 3; q++) CKR(cudaMemcpyAsync(u[1 + q], c->mA[q], fb, cudaMemcpyDeviceToDevice, c->stream));
+    for (int q = 0; q < 4; q++) CKR(cudaMemcpyAsync(u[4 + q], u[q], fb, cudaMemcpyDeviceToDevice, c->stream));
+    K1Args a{};
+    a.nf = 1; a.stage = 0; a.mode = 1; a.err = c->derr;
+    a.xin[0] = u[0]; a.xold[0] = u[0]; a.xout[0] = u[8]; a.mw = u[3];
+    K1Maps maps;
+    const double *xv[1] = {u[0]};
+    rc = build_maps(c, xv, 1, u[1], u[2], &maps);
+    if (rc) return rc;
+    double *scratch[5] = {u[9], u[10], u[11], u[12], u[13]};
+    auto run = [&](int which) -> cudaError_t {
+        int launches = 0;
+        switch (which) {
+        case 0: return launch_k1(c->G, a, maps, c->stream);
+        case 1: return launch_advection_tl(c->G, u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7], u[8], c->stream);
+        case 2: return launch_advection_ad(c->G, u[0], u[1], u[2], u[3], u[8], u[4], u[5], u[6], u[7], scratch, c->stream);
+        case 3: return project(c, u[4], u[5], u[6], u[7], -1, 0, 0, 0, &launches);
+        default: return pressure_adjoint(c->G, c->pp, c->prm.nsubp, u[4], u[5], u[6], u[7], c->stream);
+        }
+    };
+    cudaEvent_t e0, e1;
+    CKR(cudaEventCreate(&e0));
+    CKR(cudaEventCreate(&e1));
+    cudaError_t er = cudaSuccess;
+    for (int w = 0; w < 5 && er == cudaSuccess; w++) {
+        er = run(w);   // untimed (the adjoint of the projection builds its transposed system here)
+        if (er == cudaSuccess) er = cudaEventRecord(e0, c->stream);
+        for (int r = 0; r < reps && er == cudaSuccess; r++) er = run(w);
+        if (er == cudaSuccess) er = cudaEventRecord(e1, c->stream);
+        if (er == cudaSuccess) er = cudaEventSynchronize(e1);
+        float f = 0.f;
+        if (er == cudaSuccess) er = cudaEventElapsedTime(&f, e0, e1);
+        out[w] = f / reps;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (er != cudaSuccess) return cuerr(er);
+    return check_err(c);
+}
+
 extern "C" int mg_qnadv_uvw(mg_ctx *c, int ntime, const double *mu, const double *mv, const double *mw, double *au,
                             double *av, double *aw)
 {

@@ -219,8 +219,7 @@ cudaError_t launch_advection_ad(const DevGrid &g, const double *x, const double 
     const AdvIn in{x, mu, mv, mw};
     const long long ncell = (long long)g.nx * g.ny * g.nz;
     for (int dir = 0; dir < 3; dir++) {
-        for (int q = 0; q < 5; q++)
-            if ((e = cudaMemsetAsync(scratch[q], 0, fbytes, s)) != cudaSuccess) return e;
+        // every face entry the gather reads is written by the face pass: no clearing
         const long long nf = (long long)(dir == 0 ? g.maxx + 1 : g.maxx) * (dir == 1 ? g.maxy + 1 : g.maxy) *
                              (dir == 2 ? g.nz - 1 : g.nz);
         adv_ad_face_kernel<<<nblk(nf), 256, 0, s>>>(g, dir, in, Abar, scratch[0], scratch[1], scratch[2], scratch[3],

@@ -200,6 +200,11 @@ int mg_advection_ad(mg_ctx *ctx, const double *x, const double *mu, const double
  * ghosts 0).  FP64 contexts only. */
 int mg_anelastic_pressure_ad(mg_ctx *ctx, double *mubar, double *mvbar, double *mwbar, double *pbar);
 
+/* device time (ms per call) of, on copies of the resident state: [0] the advection
+ * operator, [1] its tangent linear, [2] its adjoint, [3] anelastic_pressure, [4] its
+ * adjoint; averaged over reps.  FP64 contexts, WENO.  No counterpart in the reference. */
+int mg_time_adjoint(mg_ctx *ctx, int reps, double *out5);
+
 /* ---- allocation-free entry (no counterpart in the reference) ----
  * The projection residual of pressure_solver.f90:121-130 (signed max of the
  * divergence over the interior, k = 2..nz-1), computed without a context and without
