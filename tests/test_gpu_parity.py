@@ -156,3 +156,17 @@ def test_deterministic_reruns():
             res.append(m.download())
     for x, y in zip([res[0].u, res[0].p, *res[0].scal], [res[1].u, res[1].p, *res[1].scal]):
         assert np.array_equal(x, y)
+
+
+def test_step_parity_many_lognormal_tracers():
+    """Capacity-run field set at a small size: theta_l, qt and 10 lognormal tracers
+    (sigma_log = 1), 13 advected fields with density, on the stretched grid."""
+    d = config.cumulus_domain(32, 32, 24, scheme="weno", dt0=0.5)
+    st = config.cumulus_state(d, seed=4000, n_extra=10, lognormal_extras=True)
+    assert len(st.scal) == 12
+    with Mimica(d, nscal=len(st.scal), iqt=1) as m:
+        m.upload(st)
+        m.stepping(2, ntime0=1)
+        g = m.download()
+    r, _, _ = O.Oracle(d).stepping(st, nsteps=2, ntime0=1)
+    _compare_states(g, r)
