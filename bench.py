@@ -205,7 +205,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mimica", choices=["mimica", "reference"])
-    ap.add_argument("--scheme", default="weno", choices=["weno", "ppm", "muscl"])
+    ap.add_argument("--scheme", default="weno", choices=["weno", "ppm", "muscl", "lw", "quick"])
     ap.add_argument("--maxx", type=int, default=512)
     ap.add_argument("--nz", type=int, default=256)
     ap.add_argument("--cpu-sample-xy", type=int, default=64)

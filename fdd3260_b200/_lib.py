@@ -15,11 +15,11 @@ LIB_PATH = os.path.join(HERE, "libmimica_gpu.so")
 
 # status codes (mimica_gpu.h)
 MG_OK, MG_ERR_PARAM, MG_ERR_CUDA, MG_ERR_NAN, MG_ERR_PIVOT, MG_ERR_TIMEOUT, MG_ERR_NOMEM, MG_ERR_STATE = range(8)
-MG_WENO, MG_PPM, MG_MUSCL = 0, 1, 2
+MG_WENO, MG_PPM, MG_MUSCL, MG_LW, MG_QUICK = 0, 1, 2, 3, 4
 MG_LIM_MINMOD, MG_LIM_VL, MG_LIM_MC, MG_LIM_DEFAULT = 0, 1, 2, 3
 MG_PREC_FP64, MG_PREC_MIXED = 0, 1
 
-SCHEMES = {"weno": MG_WENO, "ppm": MG_PPM, "muscl": MG_MUSCL}
+SCHEMES = {"weno": MG_WENO, "ppm": MG_PPM, "muscl": MG_MUSCL, "lw": MG_LW, "quick": MG_QUICK}
 LIMITERS = {"minmod": MG_LIM_MINMOD, "VL": MG_LIM_VL, "MC": MG_LIM_MC, "default": MG_LIM_DEFAULT}
 
 _dp = C.POINTER(C.c_double)

@@ -209,7 +209,7 @@ static int validate(const mg_params *p)
     if (p->maxx > 4096 || p->maxy > 4096) return MG_ERR_PARAM;
     if (p->nscal < 1 || p->nscal + 1 > MG_MAXF) return MG_ERR_PARAM;
     if (p->iqt >= p->nscal || p->iqt == 0) return MG_ERR_PARAM;
-    if (p->scal_adv < MG_WENO || p->scal_adv > MG_MUSCL) return MG_ERR_PARAM;
+    if (p->scal_adv < MG_WENO || p->scal_adv > MG_QUICK) return MG_ERR_PARAM;
     if (p->muscl_limiter < MG_LIM_MINMOD || p->muscl_limiter > MG_LIM_DEFAULT) return MG_ERR_PARAM;
     if (p->mom_ord != 2 && p->mom_ord != 4) return MG_ERR_PARAM;
     if (p->nsubp < 1 || p->nsubp > 16) return MG_ERR_PARAM;

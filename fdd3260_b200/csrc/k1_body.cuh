@@ -351,6 +351,23 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
                                 Fx = muscl_face_h(G.muscl_lim, G.lim_tol, G.dx, dx1, V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu);
                                 Fy = muscl_face_h(G.muscl_lim, G.lim_tol, G.dy, dy1, V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv);
                             }
+                        } else if (SCHEME == MG_LW) {
+                            if constexpr (MIXED) {
+                                Fx = lw_face_h_mixed((float)G.lim_tol, (float)dt0, (float)dx1, V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu);
+                                Fy = lw_face_h_mixed((float)G.lim_tol, (float)dt0, (float)dy1, V(by - SW), V(by), V(by + SW),
+                                                     V(by + 2 * SW), vv);
+                            } else {
+                                Fx = lw_face_h(G.lim_tol, dt0, dx1, V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu);
+                                Fy = lw_face_h(G.lim_tol, dt0, dy1, V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv);
+                            }
+                        } else if (SCHEME == MG_QUICK) {
+                            if constexpr (MIXED) {
+                                Fx = quick_face_h_mixed((float)G.lim_tol, V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu);
+                                Fy = quick_face_h_mixed((float)G.lim_tol, V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv);
+                            } else {
+                                Fx = quick_face_h(G.lim_tol, V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu);
+                                Fy = quick_face_h(G.lim_tol, V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv);
+                            }
                         } else if constexpr (MIXED) {
                             // relative reconstructions: cell base values from the plane
                             const double mux = fabs(uu) * dt0 * dx1;
@@ -432,6 +449,24 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
                             else
                                 Fzn = muscl_face_z(kind, G.muscl_lim, G.lim_tol, G.dz, xm1, ZVAL(f, 1), ZVAL(f, 2), xp2, d1m, d10,
                                                    d1p, fm, fp, dzw1, ww);
+                        } else if (SCHEME == MG_LW || SCHEME == MG_QUICK) {
+                            const int kind = k == 1 ? 1 : (k == nz - 1 ? 2 : 0);
+                            const double d1m = k >= 2 ? ldg(G.dz1, k - 2) : 0., d10 = ldg(G.dz1, k - 1), d1p = ldg(G.dz1, k);
+                            const double xm1 = k >= 2 ? ZVAL(f, 0) : 0.;
+                            const double xp2 = k + 2 <= nz ? ZVAL(f, 3) : 0.;
+                            if constexpr (MIXED) {
+                                if constexpr (SCHEME == MG_LW)
+                                    Fzn = lw_face_z_mixed(kind, (float)G.lim_tol, (float)G.dz, (float)dt0, xm1, ZVAL(f, 1), ZVAL(f, 2), xp2,
+                                                          (float)d1m, (float)d10, (float)d1p, (float)dzw1, ww);
+                                else
+                                    Fzn = quick_face_z_mixed(kind, (float)G.lim_tol, (float)G.dz, xm1, ZVAL(f, 1), ZVAL(f, 2), xp2,
+                                                             (float)d1m, (float)d10, (float)d1p, (float)dzw1, ww);
+                            } else {
+                                if constexpr (SCHEME == MG_LW)
+                                    Fzn = lw_face_z(kind, G.lim_tol, G.dz, dt0, xm1, ZVAL(f, 1), ZVAL(f, 2), xp2, d1m, d10, d1p, dzw1, ww);
+                                else
+                                    Fzn = quick_face_z(kind, G.lim_tol, G.dz, xm1, ZVAL(f, 1), ZVAL(f, 2), xp2, d1m, d10, d1p, dzw1, ww);
+                            }
                         } else if constexpr (MIXED) {
                             // chain values relative: prfr = Fr(k) - x(k), prxp = xplus(k) - x(k)
                             double *prfr = &chain[f * NCELL + cid], *prxp = &chain[(F + f) * NCELL + cid];

@@ -37,6 +37,8 @@ cudaError_t launch_k1_mixed(const DevGrid &g, const K1Args &a, const K1Maps &map
     switch (g.scal_adv) {
     case MG_WENO: return launch_scheme<MG_WENO>(g, a, maps, sm, s);
     case MG_PPM: return launch_scheme<MG_PPM>(g, a, maps, sm, s);
+    case MG_LW: return launch_scheme<MG_LW>(g, a, maps, sm, s);
+    case MG_QUICK: return launch_scheme<MG_QUICK>(g, a, maps, sm, s);
     default: return launch_scheme<MG_MUSCL>(g, a, maps, sm, s);
     }
 }
@@ -46,5 +48,7 @@ cudaError_t k1_mixed_init()
     cudaError_t e;
     if ((e = init_scheme<MG_WENO>()) != cudaSuccess) return e;
     if ((e = init_scheme<MG_PPM>()) != cudaSuccess) return e;
+    if ((e = init_scheme<MG_LW>()) != cudaSuccess) return e;
+    if ((e = init_scheme<MG_QUICK>()) != cudaSuccess) return e;
     return init_scheme<MG_MUSCL>();
 }

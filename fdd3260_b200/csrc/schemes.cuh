@@ -200,6 +200,111 @@ __device__ __forceinline__ T muscl_face_z(int kind, int lim, T lim_tol, T dz, T 
     return T(0.5) * ww * (Fl * (T(1.) + sign1(ww)) + Fr * (T(1.) - sign1(ww)));
 }
 
+// ---------------- lw: src/TOOLS/advq_lw.f90 (limiter 'MC', the module constant) ----------------
+template <typename T>
+__device__ __forceinline__ void lw_limiter(T lim_tol, T xx, T ffip1, T ffip2, T ffim1, T &phir, T &phil)
+{
+    const T eps = T(1.e-18);
+    T rp1 = T(1.), rp2 = T(1.);
+    if (dabs(ffim1) > lim_tol * dabs(xx) + eps) rp1 = ffip1 / ffim1;
+    if (dabs(ffip2) > lim_tol * dabs(xx) + eps) rp2 = ffip1 / ffip2;
+    phil = tmax(tmin(tmin(T(2.) * rp1, T(0.5) * (rp1 + T(1.))), T(2.)), T(0.));
+    phir = tmax(tmin(tmin(T(2.) * rp2, T(0.5) * (rp2 + T(1.))), T(2.)), T(0.));
+}
+
+// horizontal face between i and i+1 (advq_lw.f90:82-101); d1 = 1/dx
+template <typename T>
+__device__ __forceinline__ T lw_face_h(T lim_tol, T dt0, T d1, T xm1, T x0, T xp1, T xp2, T uu)
+{
+    const T eps = T(1.e-18);
+    const T ffip1 = xp1 - x0, ffim1 = x0 - xm1, ffip2 = xp2 - xp1;
+    const T mu = dabs(uu) * dt0 * d1;
+    T fl, fr;
+    if (dabs(ffim1) > lim_tol * dabs(x0) + eps || dabs(ffip2) > lim_tol * dabs(x0) + eps) {
+        T phir, phil;
+        lw_limiter(lim_tol, x0, ffip1, ffip2, ffim1, phir, phil);
+        fl = x0 + T(0.5) * phil * ffim1 * (T(1.) - mu);
+        fr = xp1 - T(0.5) * phir * ffip2 * (T(1.) - mu);
+    } else {
+        fl = x0 + T(0.5) * ffip1 * (T(1.) - mu);
+        fr = xp1 - T(0.5) * ffip1 * (T(1.) - mu);
+    }
+    return T(0.5) * uu * (fl * (sign1(uu) + T(1.)) - fr * (sign1(uu) - T(1.)));
+}
+
+// vertical face k+1/2 (advq_lw.f90:246-311).  kind: 0 core, 1 bottom (k=1, ffim1 = ffip1),
+// 2 top (k=nz-1, ffip2 = ffip1).  d1m, d10, d1p = dz1(k-1), dz1(k), dz1(k+1); dzw1 = dz1w(k).
+template <typename T>
+__device__ __forceinline__ T lw_face_z(int kind, T lim_tol, T dz, T dt0, T xm1, T x0, T xp1, T xp2,
+                                       T d1m, T d10, T d1p, T dzw1, T ww)
+{
+    const T eps = T(1.e-18);
+    const T ffip1 = (xp1 - x0) * d10;
+    const T ffim1 = kind == 1 ? ffip1 : (x0 - xm1) * d1m;
+    const T ffip2 = kind == 2 ? ffip1 : (xp2 - xp1) * d1p;
+    const T mu = dabs(ww) * dt0 * d10;
+    T fl, fr;
+    if (dz * dabs(ffim1) > lim_tol * dabs(x0) + eps || dz * dabs(ffip2) > lim_tol * dabs(x0) + eps) {
+        T phir, phil;
+        lw_limiter(lim_tol, x0, ffip1, ffip2, ffim1, phir, phil);
+        fl = x0 + T(0.5) * phil * ffim1 * (T(1.) - mu) / dzw1;
+        fr = xp1 - T(0.5) * phir * ffip2 * (T(1.) - mu) / dzw1;
+    } else {
+        fl = x0 + T(0.5) * ffip1 * (T(1.) - mu) / dzw1;
+        fr = xp1 - T(0.5) * ffip1 * (T(1.) - mu) / dzw1;
+    }
+    return T(0.5) * ww * (fl * (sign1(ww) + T(1.)) - fr * (sign1(ww) - T(1.)));
+}
+
+// ---------------- QUICK: src/TOOLS/advq_quick.f90 ----------------
+template <typename T>
+__device__ __forceinline__ void quick_limiter(T lim_tol, T phic, T ffip1, T ffip2, T ffim1, T &phil, T &phir)
+{
+    const T eps = T(1.e-18);
+    const T c1 = T(1.) / T(3.);
+    const T thr = lim_tol * dabs(phic) + eps;
+    T rp1 = T(1.), rp2 = T(1.), rp11 = T(1.), rp21 = T(1.);
+    if (dabs(ffim1) > thr) rp1 = ffip1 / ffim1;
+    if (dabs(ffip2) > thr) rp2 = ffip1 / ffip2;
+    if (dabs(ffip1) > thr) {
+        rp11 = ffim1 / ffip1;
+        rp21 = ffip2 / ffip1;
+    }
+    phil = rp1 * (T(1.) - c1 * (T(1.) - rp11));
+    phir = rp2 * (T(1.) - c1 * (T(1.) - rp21));
+    if (dabs(ffim1) > thr || dabs(ffip2) > thr) {
+        phil = tmax(T(0.), tmin(T(2.) * rp1, tmin(phil, T(2.))));
+        phir = tmax(T(0.), tmin(T(2.) * rp2, tmin(phir, T(2.))));
+    }
+}
+
+// horizontal face between i and i+1 (advq_quick.f90:79-93)
+template <typename T>
+__device__ __forceinline__ T quick_face_h(T lim_tol, T xm1, T x0, T xp1, T xp2, T uu)
+{
+    const T ffip1 = xp1 - x0, ffip2 = xp2 - xp1, ffim1 = x0 - xm1;
+    T phil, phir;
+    quick_limiter(lim_tol, x0, ffip1, ffip2, ffim1, phil, phir);
+    const T Fl = x0 + T(0.5) * phil * ffim1;
+    const T Fr = xp1 - T(0.5) * phir * ffip2;
+    return T(0.5) * Fl * (uu + dabs(uu)) + T(0.5) * Fr * (uu - dabs(uu));
+}
+
+// vertical face k+1/2 (advq_quick.f90:235-279), kinds and arguments as lw_face_z
+template <typename T>
+__device__ __forceinline__ T quick_face_z(int kind, T lim_tol, T dz, T xm1, T x0, T xp1, T xp2, T d1m, T d10,
+                                          T d1p, T dzw1, T ww)
+{
+    const T ffip1 = (xp1 - x0) * d10;
+    const T ffip2 = kind == 2 ? ffip1 : (xp2 - xp1) * d1p;
+    const T ffim1 = kind == 1 ? ffip1 : (x0 - xm1) * d1m;
+    T phil, phir;
+    quick_limiter(lim_tol, x0 / dz, ffip1, ffip2, ffim1, phil, phir);
+    const T Fl = x0 + T(0.5) * phil * ffim1 / dzw1;
+    const T Fr = xp1 - T(0.5) * phir * ffip2 / dzw1;
+    return T(0.5) * Fl * (ww + dabs(ww)) + T(0.5) * Fr * (ww - dabs(ww));
+}
+
 // ---------------- PPM: src/TOOLS/advq_ppm.f90 ----------------
 // spacing() of Fortran (2**(exponent-digits)), tiny() for 0
 __device__ __forceinline__ double fspacing(double x)
@@ -448,6 +553,73 @@ __device__ __forceinline__ double muscl_face_z_mixed(int kind, int lim, float li
         dr = -(sp * h);
     }
     return ww >= 0. ? ww * (x0 + (double)dl) : ww * (xp1 + (double)dr);
+}
+
+// lw faces in the mixed form: FP32 slopes of differences relative to the upwind cell,
+// FP64 flux (same switch structure as lw_face_h / lw_face_z)
+__device__ __forceinline__ double lw_face_h_mixed(float lim_tol, float dt0, float d1, double xm1, double x0,
+                                                  double xp1, double xp2, double uu)
+{
+    const float eps = 1.e-18f;
+    const float sp = (float)(xp1 - x0), sp2 = (float)(xp2 - xp1), sm = (float)(x0 - xm1);
+    const float ax = fabsf((float)x0);
+    const float om = 1.f - fabsf((float)uu) * dt0 * d1;
+    float dr, dl;
+    if (fabsf(sm) > lim_tol * ax + eps || fabsf(sp2) > lim_tol * ax + eps) {
+        float phir, phil;
+        lw_limiter(lim_tol, (float)x0, sp, sp2, sm, phir, phil);
+        dl = 0.5f * phil * sm * om;
+        dr = -(0.5f * phir * sp2 * om);
+    } else {
+        dl = 0.5f * sp * om;
+        dr = -dl;
+    }
+    return uu >= 0. ? uu * (x0 + (double)dl) : uu * (xp1 + (double)dr);
+}
+__device__ __forceinline__ double lw_face_z_mixed(int kind, float lim_tol, float dz, float dt0, double xm1, double x0,
+                                                  double xp1, double xp2, float d1m, float d10, float d1p, float dzw1,
+                                                  double ww)
+{
+    const float eps = 1.e-18f;
+    const float sp = (float)(xp1 - x0) * d10;
+    const float sm = kind == 1 ? sp : (float)(x0 - xm1) * d1m;
+    const float sp2 = kind == 2 ? sp : (float)(xp2 - xp1) * d1p;
+    const float ax = fabsf((float)x0);
+    const float h = 0.5f * (1.f - fabsf((float)ww) * dt0 * d10) / dzw1;
+    float dr, dl;
+    if (dz * fabsf(sm) > lim_tol * ax + eps || dz * fabsf(sp2) > lim_tol * ax + eps) {
+        float phir, phil;
+        lw_limiter(lim_tol, (float)x0, sp, sp2, sm, phir, phil);
+        dl = phil * sm * h;
+        dr = -(phir * sp2 * h);
+    } else {
+        dl = sp * h;
+        dr = -dl;
+    }
+    return ww >= 0. ? ww * (x0 + (double)dl) : ww * (xp1 + (double)dr);
+}
+// QUICK faces in the mixed form
+__device__ __forceinline__ double quick_face_h_mixed(float lim_tol, double xm1, double x0, double xp1, double xp2,
+                                                     double uu)
+{
+    const float sp = (float)(xp1 - x0), sp2 = (float)(xp2 - xp1), sm = (float)(x0 - xm1);
+    float phil, phir;
+    quick_limiter(lim_tol, (float)x0, sp, sp2, sm, phil, phir);
+    const float dl = 0.5f * phil * sm, dr = -(0.5f * phir * sp2);
+    return uu > 0. ? uu * (x0 + (double)dl) : (uu < 0. ? uu * (xp1 + (double)dr) : 0.);
+}
+__device__ __forceinline__ double quick_face_z_mixed(int kind, float lim_tol, float dz, double xm1, double x0,
+                                                     double xp1, double xp2, float d1m, float d10, float d1p,
+                                                     float dzw1, double ww)
+{
+    const float sp = (float)(xp1 - x0) * d10;
+    const float sp2 = kind == 2 ? sp : (float)(xp2 - xp1) * d1p;
+    const float sm = kind == 1 ? sp : (float)(x0 - xm1) * d1m;
+    float phil, phir;
+    quick_limiter(lim_tol, (float)x0 / dz, sp, sp2, sm, phil, phir);
+    const float h = 0.5f / dzw1;
+    const float dl = phil * sm * h, dr = -(phir * sp2 * h);
+    return ww > 0. ? ww * (x0 + (double)dl) : (ww < 0. ? ww * (xp1 + (double)dr) : 0.);
 }
 
 // PPM: reconstruction of a cell relative to its own value x0; xv[] holds

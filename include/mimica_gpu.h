@@ -39,8 +39,10 @@ enum {
     MG_ERR_STATE = 7         /* call out of order (e.g. step before upload) */
 };
 
-/* ---- scheme selectors (src/TOOLS/advection.f90:603-614, advq_muscl.f90:367-380) ---- */
-enum { MG_WENO = 0, MG_PPM = 1, MG_MUSCL = 2 };
+/* ---- scheme selectors (src/TOOLS/advection.f90:603-614, advq_muscl.f90:367-380) ----
+ * MG_LW is the dispatcher's `case default` (advq_lw.f90) with the module's 'MC'
+ * limiter (lwlimiter, advq_lw.f90:50, is in no namelist); MG_QUICK is advq_quick.f90. */
+enum { MG_WENO = 0, MG_PPM = 1, MG_MUSCL = 2, MG_LW = 3, MG_QUICK = 4 };
 enum { MG_LIM_MINMOD = 0, MG_LIM_VL = 1, MG_LIM_MC = 2, MG_LIM_DEFAULT = 3 };
 /* arithmetic forms */
 enum {
@@ -60,7 +62,8 @@ typedef struct mg_params {
                                   scal[0] = es (potential temperature), then qt (if iqt >= 0),
                                   then passive scalars */
     int iqt;                   /* index of qt in scal[], or -1 (dry) */
-    int scal_adv;              /* MG_WENO / MG_PPM / MG_MUSCL (scal_adv, sorder=2, limit=.true.) */
+    int scal_adv;              /* MG_WENO / MG_PPM / MG_MUSCL / MG_LW / MG_QUICK
+                                  (scal_adv, sorder=2, limit=.true.) */
     int muscl_limiter;         /* MG_LIM_* (module default 'minmod') */
     int mom_ord;               /* 2 or 4 (windadv.f90:515-519); 3 is rejected */
     int lavisc;                /* artificial viscosity (lavisc) */
@@ -70,7 +73,7 @@ typedef struct mg_params {
     int refine_iters;          /* mixed form: max refinement passes per pressure solve, each on the
                                   FP64 residual r = b - A dp of the Poisson system; nsubp*(1+refine_iters) <= 64 */
     double dx, dy, dz, dt0;
-    double lim_tol;            /* MUSCL tolerance (lim_tol) */
+    double lim_tol;            /* flux-limiter tolerance of MUSCL, lw and QUICK (lim_tol) */
     double u0shift, v0shift;   /* Galilean shift of the advective velocity */
     double refine_tol;         /* mixed form: skip further refinement once max|r|*dt0 < tol [1/s]
                                   (r in the units of b = div(rho0 u)/(dt0 rho0)) */

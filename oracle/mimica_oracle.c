@@ -654,12 +654,246 @@ static void advs_muscl_z(const mo_grid *g, const double *x, const double *w, dou
     free(F);
 }
 
+/* src/TOOLS/advq_lw.f90:343-420, limiter 'MC' (lwlimiter is a module constant, :50) */
+static void limiter_lw(const mo_grid *g, double xx, double ffip1, double ffip2, double ffim1,
+                       double *phir, double *phil)
+{
+    const double eps = 1.e-18, lim_tol = g->lim_tol;
+    double rp1 = 1., rp2 = 1.;
+    if (fabs(ffim1) > lim_tol * fabs(xx) + eps) rp1 = ffip1 / ffim1;
+    if (fabs(ffip2) > lim_tol * fabs(xx) + eps) rp2 = ffip1 / ffip2;
+    *phil = dmax2(dmin2(dmin2(2. * rp1, 0.5 * (rp1 + 1.)), 2.), 0.);
+    *phir = dmax2(dmin2(dmin2(2. * rp2, 0.5 * (rp2 + 1.)), 2.), 0.);
+}
+
+/* src/TOOLS/advq_lw.f90:57-123 (x) and :126-206 (y, CHANNEL off) */
+static void advs_lw_h(const mo_grid *g, int n, int i1, int i2, double d, const double *x,
+                      const double *u, double *xa, int adv)
+{
+    const double eps = 1.e-18, lim_tol = g->lim_tol, dt0 = g->dt0;
+    double dx1 = 1. / d;
+    double *F = dalloc((size_t)n);
+    for (int i = i1 - 1; i <= i2; i++) {
+        double uu = P1(u, i + 1), xx = P1(x, i);
+        double ffip1 = P1(x, i + 1) - xx;
+        double ffim1 = xx - P1(x, i - 1);
+        double ffip2 = P1(x, i + 2) - P1(x, i + 1);
+        double mu = fabs(uu) * dt0 * dx1;
+        double fl, fr, phir, phil;
+        if (fabs(ffim1) > lim_tol * fabs(xx) + eps || fabs(ffip2) > lim_tol * fabs(xx) + eps) {
+            limiter_lw(g, xx, ffip1, ffip2, ffim1, &phir, &phil);
+            fl = xx + 0.5 * phil * ffim1 * (1. - mu);
+            fr = P1(x, i + 1) - 0.5 * phir * ffip2 * (1. - mu);
+        } else {
+            fl = xx + 0.5 * ffip1 * (1. - mu);
+            fr = P1(x, i + 1) - 0.5 * ffip1 * (1. - mu);
+        }
+        P1(F, i) = 0.5 * uu * (fl * (fsign1(uu) + 1.) - fr * (fsign1(uu) - 1.));
+    }
+    double Fold = P1(F, i1 - 1);
+    for (int i = i1; i <= i2; i++) {
+        P1(xa, i) = P1(xa, i) + (P1(F, i) - Fold) * dx1;
+        Fold = P1(F, i);
+    }
+    if (adv) {
+        double uold = P1(u, i2 + 1);
+        for (int i = i2; i >= i1; i--) {
+            P1(xa, i) = P1(xa, i) - P1(x, i) * (uold - P1(u, i)) * dx1;
+            uold = P1(u, i);
+        }
+    }
+    free(F);
+}
+
+/* One vertical lw face k+1/2 given its three slopes (advq_lw.f90:253-263, 278-288, 301-311) */
+static double lw_face_z(const mo_grid *g, int k, double xx, double xp1, double ffim1, double ffip1,
+                        double ffip2, double ww)
+{
+    const double eps = 1.e-18, lim_tol = g->lim_tol, dz = g->dz;
+    double mu = fabs(ww) * g->dt0 * P1(g->dz1, k);
+    double fl, fr, phir, phil;
+    if (dz * fabs(ffim1) > lim_tol * fabs(xx) + eps || dz * fabs(ffip2) > lim_tol * fabs(xx) + eps) {
+        limiter_lw(g, xx, ffip1, ffip2, ffim1, &phir, &phil);
+        fl = xx + 0.5 * phil * ffim1 * (1. - mu) / P1(g->dz1w, k);
+        fr = xp1 - 0.5 * phir * ffip2 * (1. - mu) / P1(g->dz1w, k);
+    } else {
+        fl = xx + 0.5 * ffip1 * (1. - mu) / P1(g->dz1w, k);
+        fr = xp1 - 0.5 * ffip1 * (1. - mu) / P1(g->dz1w, k);
+    }
+    return 0.5 * ww * (fl * (fsign1(ww) + 1.) - fr * (fsign1(ww) - 1.));
+}
+
+/* src/TOOLS/advq_lw.f90:209-341 with bcl(5)=bcl(6)='nnf' */
+static void advs_lw_z(const mo_grid *g, const double *x, const double *w, double *xa, int adv)
+{
+    const int nz = g->nz, k2 = nz;
+    const double *dz1 = g->dz1, *dz1w = g->dz1w;
+    const double bc51 = 0., bc61 = 0.;
+    double *F = dalloc((size_t)nz);
+    double ffip1, ffip2, ffim1;
+    int k;
+
+    k = 1;
+    ffip1 = (P1(x, 2) - P1(x, 1)) * P1(dz1, 1);
+    ffip2 = (P1(x, 3) - P1(x, 2)) * P1(dz1, 2);
+    ffim1 = bc51 * (P1(x, nz - 4) - P1(x, nz - 5)) * P1(dz1, nz - 5) + (1. - bc51) * ffip1;
+    P1(F, 1) = lw_face_z(g, 1, P1(x, 1), P1(x, 2), ffim1, ffip1, ffip2, P1(w, 2));
+
+    for (k = 2; k <= nz - 2; k++) {
+        double xx = P1(x, k), xp1 = P1(x, k + 1), xp2 = P1(x, k + 2);
+        ffim1 = (xx - P1(x, k - 1)) * P1(dz1, k - 1);
+        ffip1 = (xp1 - xx) * P1(dz1, k);
+        ffip2 = (xp2 - xp1) * P1(dz1, k + 1);
+        P1(F, k) = lw_face_z(g, k, xx, xp1, ffim1, ffip1, ffip2, P1(w, k + 1));
+    }
+
+    k = nz - 1;
+    ffim1 = (P1(x, k) - P1(x, k - 1)) * P1(dz1, k - 1);
+    ffip1 = (P1(x, k + 1) - P1(x, k)) * P1(dz1, k);
+    ffip2 = bc61 * (P1(x, 6) - P1(x, 5)) * P1(dz1, 5) + (1. - bc61) * ffip1;
+    P1(F, k) = lw_face_z(g, k, P1(x, k), P1(x, k + 1), ffim1, ffip1, ffip2, P1(w, nz));
+
+    double Fold = P1(F, 1);
+    for (k = 2; k <= nz - 1; k++) {
+        P1(xa, k) = P1(xa, k) + (P1(F, k) - Fold) * P1(dz1w, k);
+        Fold = P1(F, k);
+    }
+    if (adv) {
+        double wold = P1(w, k2);
+        for (k = nz - 1; k >= 2; k--) {
+            P1(xa, k) = P1(xa, k) - P1(x, k) * (wold - P1(w, k)) * P1(dz1w, k);
+            wold = P1(w, k);
+        }
+    }
+    P1(xa, 1) = P1(xa, 1) + (P1(F, 1) - 0.) * P1(dz1w, 1);
+    if (adv) P1(xa, 1) = P1(xa, 1) - P1(x, 1) * (P1(w, 2) - 0.) * P1(dz1w, 1);
+    P1(xa, nz) = P1(xa, nz) + (0. - P1(F, nz - 1)) * P1(dz1w, nz);
+    if (adv) P1(xa, nz) = P1(xa, nz) - P1(x, nz) * (0. - P1(w, nz)) * P1(dz1w, nz);
+    free(F);
+}
+
+/* src/TOOLS/advq_quick.f90:311-352 */
+static void limiter_quick(const mo_grid *g, double phic, double ffip1, double ffip2, double ffim1,
+                          double *phil, double *phir)
+{
+    const double eps = 1.e-18, lim_tol = g->lim_tol;
+    const double c1 = 1. / 3.;
+    double rp1 = 1., rp2 = 1., rp11 = 1., rp21 = 1.;
+    if (fabs(ffim1) > lim_tol * fabs(phic) + eps) rp1 = ffip1 / ffim1;
+    if (fabs(ffip2) > lim_tol * fabs(phic) + eps) rp2 = ffip1 / ffip2;
+    if (fabs(ffip1) > lim_tol * fabs(phic) + eps) {
+        rp11 = ffim1 / ffip1;
+        rp21 = ffip2 / ffip1;
+    }
+    *phil = rp1 * (1. - c1 * (1. - rp11));
+    *phir = rp2 * (1. - c1 * (1. - rp21));
+    if (fabs(ffim1) > lim_tol * fabs(phic) + eps || fabs(ffip2) > lim_tol * fabs(phic) + eps) {
+        *phil = dmax2(0., dmin2(2. * rp1, dmin2(*phil, 2.)));
+        *phir = dmax2(0., dmin2(2. * rp2, dmin2(*phir, 2.)));
+    }
+}
+
+/* src/TOOLS/advq_quick.f90:53-115 (x) and :118-195 (y, CHANNEL off) */
+static void advs_quick_h(const mo_grid *g, int n, int i1, int i2, double d, const double *x,
+                         const double *u, double *xa, int adv)
+{
+    double dx1 = 1. / d;
+    double *F = dalloc((size_t)n);
+    for (int i = i1 - 1; i <= i2; i++) {
+        double uu = P1(u, i + 1), xx = P1(x, i);
+        double ffip1 = P1(x, i + 1) - xx;
+        double ffip2 = P1(x, i + 2) - P1(x, i + 1);
+        double ffim1 = xx - P1(x, i - 1);
+        double phil, phir;
+        limiter_quick(g, xx, ffip1, ffip2, ffim1, &phil, &phir);
+        double Fl = xx + 0.5 * phil * ffim1;
+        double Fr = P1(x, i + 1) - 0.5 * phir * ffip2;
+        P1(F, i) = 0.5 * Fl * (uu + fabs(uu)) + 0.5 * Fr * (uu - fabs(uu));
+    }
+    double Fold = P1(F, i1 - 1);
+    for (int i = i1; i <= i2; i++) {
+        P1(xa, i) = P1(xa, i) + (P1(F, i) - Fold) * dx1;
+        Fold = P1(F, i);
+    }
+    if (adv) {
+        double uold = P1(u, i2 + 1);
+        for (int i = i2; i >= i1; i--) {
+            P1(xa, i) = P1(xa, i) - P1(x, i) * (uold - P1(u, i)) * dx1;
+            uold = P1(u, i);
+        }
+    }
+    free(F);
+}
+
+/* One vertical QUICK face k+1/2 (advq_quick.f90:241-246, 257-262, 274-279) */
+static double quick_face_z(const mo_grid *g, int k, double xx, double xp1, double ffim1, double ffip1,
+                           double ffip2, double ww)
+{
+    double phil, phir;
+    limiter_quick(g, xx / g->dz, ffip1, ffip2, ffim1, &phil, &phir);
+    double Fl = xx + 0.5 * phil * ffim1 / P1(g->dz1w, k);
+    double Fr = xp1 - 0.5 * phir * ffip2 / P1(g->dz1w, k);
+    return 0.5 * Fl * (ww + fabs(ww)) + 0.5 * Fr * (ww - fabs(ww));
+}
+
+/* src/TOOLS/advq_quick.f90:198-309 with bcl(5)=bcl(6)='nnf' */
+static void advs_quick_z(const mo_grid *g, const double *x, const double *w, double *xa, int adv)
+{
+    const int nz = g->nz, k2 = nz;
+    const double *dz1 = g->dz1, *dz1w = g->dz1w;
+    const double bc51 = 0., bc61 = 0.;
+    double *F = dalloc((size_t)nz);
+    double ffip1, ffip2, ffim1, xx;
+    int k;
+
+    xx = P1(x, 1);
+    ffip1 = (P1(x, 2) - xx) * P1(dz1, 1);
+    ffip2 = (P1(x, 3) - P1(x, 2)) * P1(dz1, 2);
+    ffim1 = bc51 * (P1(x, nz - 4) - P1(x, nz - 5)) * P1(dz1, nz - 5) + (1. - bc51) * ffip1;
+    P1(F, 1) = quick_face_z(g, 1, xx, P1(x, 2), ffim1, ffip1, ffip2, P1(w, 2));
+
+    for (k = 2; k <= nz - 2; k++) {
+        xx = P1(x, k);
+        ffip1 = (P1(x, k + 1) - xx) * P1(dz1, k);
+        ffip2 = (P1(x, k + 2) - P1(x, k + 1)) * P1(dz1, k + 1);
+        ffim1 = (xx - P1(x, k - 1)) * P1(dz1, k - 1);
+        P1(F, k) = quick_face_z(g, k, xx, P1(x, k + 1), ffim1, ffip1, ffip2, P1(w, k + 1));
+    }
+
+    k = nz - 1;
+    xx = P1(x, nz - 1);
+    ffip1 = (P1(x, k + 1) - xx) * P1(dz1, k);
+    ffim1 = (xx - P1(x, k - 1)) * P1(dz1, k - 1);
+    ffip2 = bc61 * (P1(x, 6) - P1(x, 5)) * P1(dz1, 5) + (1. - bc61) * ffip1;
+    P1(F, k) = quick_face_z(g, k, xx, P1(x, k + 1), ffim1, ffip1, ffip2, P1(w, nz));
+
+    double Fold = P1(F, 1);
+    for (k = 2; k <= nz - 1; k++) {
+        P1(xa, k) = P1(xa, k) + (P1(F, k) - Fold) * P1(dz1w, k);
+        Fold = P1(F, k);
+    }
+    if (adv) {
+        double wold = P1(w, k2);
+        for (k = nz - 1; k >= 2; k--) {
+            P1(xa, k) = P1(xa, k) - P1(x, k) * (wold - P1(w, k)) * P1(dz1w, k);
+            wold = P1(w, k);
+        }
+    }
+    P1(xa, 1) = P1(xa, 1) + (P1(F, 1) - 0.) * P1(dz1w, 1);
+    if (adv) P1(xa, 1) = P1(xa, 1) - P1(x, 1) * (P1(w, 2) - 0.) * P1(dz1w, 1);
+    P1(xa, nz) = P1(xa, nz) + (0. - P1(F, nz - 1)) * P1(dz1w, nz);
+    if (adv) P1(xa, nz) = P1(xa, nz) - P1(x, nz) * (0. - P1(w, nz)) * P1(dz1w, nz);
+    free(F);
+}
+
 void mo_advs_h(const mo_grid *g, int scheme, int n, int i1, int i2, double d, const double *x,
                const double *u, double *xa, int adv)
 {
     switch (scheme) {
     case MO_WENO: advs_weno_h(n, i1, i2, d, x, u, xa, adv); break;
     case MO_PPM: advs_ppm_h(g, n, i1, i2, d, x, u, xa, adv); break;
+    case MO_LW: advs_lw_h(g, n, i1, i2, d, x, u, xa, adv); break;
+    case MO_QUICK: advs_quick_h(g, n, i1, i2, d, x, u, xa, adv); break;
     default: advs_muscl_h(g, n, i1, i2, d, x, u, xa, adv); break;
     }
 }
@@ -669,6 +903,8 @@ void mo_advs_z(const mo_grid *g, int scheme, const double *x, const double *w, d
     switch (scheme) {
     case MO_WENO: advs_weno_z(g, x, w, xa, adv); break;
     case MO_PPM: advs_ppm_z(g, x, w, xa, adv); break;
+    case MO_LW: advs_lw_z(g, x, w, xa, adv); break;
+    case MO_QUICK: advs_quick_z(g, x, w, xa, adv); break;
     default: advs_muscl_z(g, x, w, xa, adv); break;
     }
 }

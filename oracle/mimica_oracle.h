@@ -27,12 +27,12 @@
 extern "C" {
 #endif
 
-enum { MO_WENO = 0, MO_PPM = 1, MO_MUSCL = 2 };
+enum { MO_WENO = 0, MO_PPM = 1, MO_MUSCL = 2, MO_LW = 3, MO_QUICK = 4 };
 enum { MO_LIM_MINMOD = 0, MO_LIM_VL = 1, MO_LIM_MC = 2, MO_LIM_DEFAULT = 3 };
 
 typedef struct mo_grid {
     int nx, ny, nz;              /* full sizes incl. ghost cells */
-    int scal_adv;                /* MO_WENO / MO_PPM / MO_MUSCL */
+    int scal_adv;                /* MO_WENO / MO_PPM / MO_MUSCL / MO_LW / MO_QUICK */
     int muscl_limiter;           /* MO_LIM_* (module default 'minmod') */
     int mom_ord;                 /* 2 or 4 */
     int lavisc;                  /* artificial viscosity on momentum */

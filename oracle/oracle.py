@@ -19,7 +19,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 _dp = C.POINTER(C.c_double)
 
-WENO, PPM, MUSCL = 0, 1, 2
+WENO, PPM, MUSCL, LW, QUICK = 0, 1, 2, 3, 4
 LIM = {"minmod": 0, "VL": 1, "MC": 2, "default": 3}
 
 
@@ -93,7 +93,7 @@ class Oracle:
         self.L.mo_get_wv(d.maxx, d.maxy, d.dx, d.dy, P(self.wv))
         g = MoGrid()
         g.nx, g.ny, g.nz = d.nx, d.ny, d.nz
-        g.scal_adv = {"weno": WENO, "ppm": PPM, "muscl": MUSCL}[d.scal_adv]
+        g.scal_adv = {"weno": WENO, "ppm": PPM, "muscl": MUSCL, "lw": LW, "quick": QUICK}[d.scal_adv]
         g.muscl_limiter = LIM[d.muscl_limiter]
         g.mom_ord, g.lavisc, g.nsubp, g.with_buoy = d.mom_ord, d.lavisc, d.nsubp, d.with_buoy
         g.dx, g.dy, g.dz, g.dt0 = d.dx, d.dy, d.dz, d.dt0

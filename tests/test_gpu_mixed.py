@@ -50,7 +50,7 @@ def _run_mixed(d, st, nsteps, nscal, iqt=-1):
     return field_errors(g, r, st)
 
 
-@pytest.mark.parametrize("scheme", ["weno", "ppm", "muscl"])
+@pytest.mark.parametrize("scheme", ["weno", "ppm", "muscl", "lw", "quick"])
 def test_mixed_warm_bubble(scheme):
     d = config.warm_bubble_domain(32, 32, 24, scheme=scheme)
     st = config.warm_bubble_state(d, seed=21, centre=(800.0, 800.0, 400.0), radius=400.0)

@@ -26,7 +26,7 @@ def _mom(d, st):
     return (st.u * d.den0[:, None, None], st.v * d.den0[:, None, None], st.w * d.avden0[:, None, None])
 
 
-@pytest.mark.parametrize("scheme", ["weno", "ppm", "muscl"])
+@pytest.mark.parametrize("scheme", ["weno", "ppm", "muscl", "lw", "quick"])
 @pytest.mark.parametrize("limiter", ["minmod", "VL", "MC"])
 def test_advection_ac(scheme, limiter):
     if scheme != "muscl" and limiter != "minmod":
@@ -95,7 +95,7 @@ def _compare_states(g, r, tol=TOL):
     return out
 
 
-@pytest.mark.parametrize("scheme", ["weno", "ppm", "muscl"])
+@pytest.mark.parametrize("scheme", ["weno", "ppm", "muscl", "lw", "quick"])
 def test_step_parity(scheme):
     d = config.warm_bubble_domain(32, 32, 24, scheme=scheme)
     st = config.warm_bubble_state(d, seed=21, centre=(800.0, 800.0, 400.0), radius=400.0)

@@ -85,7 +85,7 @@ def _rand_mom(d, seed):
     return st, mu, mv, mw
 
 
-@pytest.mark.parametrize("scheme", ["weno", "ppm", "muscl"])
+@pytest.mark.parametrize("scheme", ["weno", "ppm", "muscl", "lw", "quick"])
 def test_constant_field_uniform_flow_zero_tendency(scheme):
     d = config.warm_bubble_domain(16, 16, 12, scheme=scheme)
     orc = O.Oracle(d)
@@ -97,9 +97,9 @@ def test_constant_field_uniform_flow_zero_tendency(scheme):
     assert np.abs(xs).max() <= 1e-13 * 2.5 * 3.0 / d.dx
 
 
-@pytest.mark.parametrize("scheme", ["weno", "muscl"])
+@pytest.mark.parametrize("scheme", ["weno", "muscl", "lw", "quick"])
 def test_translation_invariance_bit_exact(scheme):
-    """WENO and MUSCL are translation invariant on the periodic domain (PPM is not:
+    """WENO, MUSCL, lw and QUICK are translation invariant on the periodic domain (PPM is not:
     it reconstructs the ghost cells 3 and nx-1 with one-sided formulas)."""
     d = config.warm_bubble_domain(16, 16, 10, scheme=scheme)
     orc = O.Oracle(d)
@@ -116,7 +116,7 @@ def test_translation_invariance_bit_exact(scheme):
     assert np.array_equal(shift(t0)[:, 3:-2, 3:-2], t1[:, 3:-2, 3:-2])
 
 
-@pytest.mark.parametrize("scheme", ["weno", "ppm", "muscl"])
+@pytest.mark.parametrize("scheme", ["weno", "ppm", "muscl", "lw", "quick"])
 def test_xy_symmetry_bit_exact(scheme):
     d = config.warm_bubble_domain(16, 16, 10, scheme=scheme)
     orc = O.Oracle(d)
@@ -204,7 +204,7 @@ def test_nsubp_iterations_converge():
     assert res[1] < res[0] and res[2] < res[1]
 
 
-@pytest.mark.parametrize("scheme", ["weno", "ppm", "muscl"])
+@pytest.mark.parametrize("scheme", ["weno", "ppm", "muscl", "lw", "quick"])
 def test_oracle_step_finite_and_conservative(scheme):
     d = config.warm_bubble_domain(16, 16, 12, scheme=scheme)
     st = config.warm_bubble_state(d, seed=1, centre=(400.0, 400.0, 300.0), radius=250.0)
