@@ -37,6 +37,17 @@ class MgParams(C.Structure):
     ]
 
 
+class MgSgsParams(C.Structure):
+    _fields_ = [
+        ("with_dif", C.c_int), ("anis_k", C.c_int), ("momsf", C.c_int), ("reserved", C.c_int),
+        ("diff", C.c_double), ("pran", C.c_double), ("zdec", C.c_double), ("zrough", C.c_double),
+        ("min_w", C.c_double), ("qt0", _dp),
+    ]
+
+
+SGS_NPROF = 10
+
+
 class MimicaError(RuntimeError):
     def __init__(self, code: int, where: str):
         self.code = code
@@ -88,6 +99,12 @@ def lib() -> C.CDLL:
         L.mg_ensemble_step.argtypes = [vp, C.c_int, C.c_int]
         L.mg_ensemble_time_steps.argtypes = [vp, C.c_int, C.c_int, _dp]
         L.mg_ensemble_launch_count.argtypes = [vp]
+        L.mg_set_sgs.argtypes = [vp, C.POINTER(MgSgsParams)]
+        L.mg_set_surface_fluxes.argtypes = [vp, _dp, _dp, _dp]
+        L.mg_sgs_profiles.argtypes = [C.POINTER(MgParams), C.POINTER(MgSgsParams), _dp]
+        L.mg_calc_subgrid.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.mg_efud.argtypes = [vp] + [_dp] * 8
+        L.mg_eff.argtypes = [vp, C.c_int, _dp, _dp, _dp, _dp, _dp]
         _lib = L
     return _lib
 
@@ -119,4 +136,5 @@ EXPORTED = [
     "mg_step", "mg_step_graph", "mg_synchronize", "mg_last_launch_count", "mg_advection_ac", "mg_qnadv_uvw",
     "mg_fft_solve", "mg_anelastic_pressure", "mg_time_steps", "mg_profile_enable", "mg_profile_report",
     "mg_advection_tl", "mg_advection_ad", "mg_anelastic_pressure_ad", "mg_time_adjoint", "mg_ensemble_create", "mg_ensemble_destroy", "mg_ensemble_step", "mg_ensemble_time_steps", "mg_ensemble_launch_count",
+    "mg_set_sgs", "mg_set_surface_fluxes", "mg_sgs_profiles", "mg_calc_subgrid", "mg_efud", "mg_eff",
 ]

@@ -39,6 +39,7 @@ SOURCES = [
     ("capi.cu", []),
     ("noalloc.cu", ["-fmad=false"]),
     ("k_adjoint.cu", ["-fmad=false"]),
+    ("k_sgs.cu", ["-fmad=false", "-Xcompiler", "-ffp-contract=off"]),
 ]
 
 

@@ -21,6 +21,36 @@ from . import _lib
 
 
 @dataclass
+class Sgs:
+    """SGS turbulence switches (the reference's with_dif, diff, pran, zdec, anis_k, momsf,
+    zrough, min_w; src/TYPES/shared_data.f90, defaults of INCLUDE/default.h) and the
+    surface fluxes surf%esflux, surf%qvflux, surf%mflux ((ny, nx) arrays or None)."""
+    diff: float = 0.0
+    pran: float = 0.4
+    zdec: float = 2000.0
+    anis_k: bool = False
+    momsf: int = 0
+    zrough: float = 0.01
+    min_w: float = 0.1
+    qt0: np.ndarray | None = None
+    esflux: np.ndarray | None = None
+    qvflux: np.ndarray | None = None
+    mflux: np.ndarray | None = None
+
+    def params(self, nz: int, with_dif: bool = True) -> tuple[_lib.MgSgsParams, list]:
+        keep = []
+        p = _lib.MgSgsParams()
+        p.with_dif, p.anis_k, p.momsf, p.reserved = int(with_dif), int(self.anis_k), int(self.momsf), 0
+        p.diff, p.pran, p.zdec, p.zrough, p.min_w = self.diff, self.pran, self.zdec, self.zrough, self.min_w
+        if self.qt0 is not None:
+            q = np.ascontiguousarray(self.qt0, dtype=np.float64)
+            assert q.shape == (nz,)
+            keep.append(q)
+            p.qt0 = _lib.ptr(q)
+        return p, keep
+
+
+@dataclass
 class Domain:
     maxx: int
     maxy: int
@@ -45,6 +75,7 @@ class Domain:
     precision: int = _lib.MG_PREC_FP64
     refine_iters: int = 1
     refine_tol: float = 1e-13
+    sgs: Sgs | None = None        # SGS turbulence diffusion (with_dif) when set
     # derived (filled by finish())
     dzw: np.ndarray = field(default=None, repr=False)
     dz1w: np.ndarray = field(default=None, repr=False)

@@ -17,6 +17,8 @@
 #include <new>
 #include <vector>
 
+#include <cmath>
+
 #include "mg_common.cuh"
 #include "mimica_gpu.h"
 
@@ -45,6 +47,14 @@ struct mg_ctx {
     size_t bytes = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int gsteps[2] = {0, 0};
+    // SGS diffusion (mg_set_sgs): per-level factors + qt0 on the device, the
+    // deformation tensor and eddy viscosity of level n, the stored tendencies
+    mg_sgs_params sgsp{};
+    std::vector<double> sgs_qt0;
+    int sgs_on = 0;
+    double *sgs_prof = nullptr;          // SGS_NPROF*nz factors, then qt0 (nz)
+    double *dij[6] = {}, *fkv = nullptr, *sgm[3] = {}, *sgsc[MG_MAXF] = {};
+    double *sfc[3] = {};                 // esflux, qvflux, mflux (nx*ny), zero until set
     // per-kernel profiling (CUDA events on the context stream)
     int prof_on = 0;
     struct Ev { const char *name; cudaEvent_t a, b; };
@@ -229,7 +239,11 @@ static void free_ctx(mg_ctx *c)
     for (int i = 0; i < 2; i++) if (c->gexec[i]) cudaGraphExecDestroy(c->gexec[i]);
     for (int i = 0; i < 3; i++) { cudaFree(c->mA[i]); cudaFree(c->mB[i]); cudaFree(c->tm[i]); }
     for (int f = 0; f < MG_MAXF; f++) { cudaFree(c->sA[f]); cudaFree(c->sB[f]); cudaFree(c->ts[f]); }
-    for (int i = 0; i < 8; i++) cudaFree(c->unit[i]);
+    for (int i = 0; i < 16; i++) cudaFree(c->unit[i]);
+    cudaFree(c->sgs_prof); cudaFree(c->fkv);
+    for (int q = 0; q < 6; q++) cudaFree(c->dij[q]);
+    for (int q = 0; q < 3; q++) { cudaFree(c->sgm[q]); cudaFree(c->sfc[q]); }
+    for (int f = 0; f < MG_MAXF; f++) cudaFree(c->sgsc[f]);
     cudaFree(c->p); cudaFree(c->dens3); cudaFree(c->fes); cudaFree(c->fqt); cudaFree(c->prof); cudaFree(c->derr);
     pressure_plan_destroy(c->pp);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -250,6 +264,10 @@ extern "C" int mg_create(const mg_params *params, int device, mg_ctx **out)
     if (!c) return MG_ERR_NOMEM;
     c->prm = *params;
     c->device = device;
+    // SGS switches: off, with the reference's namelist defaults (INCLUDE/default.h)
+    c->sgsp.with_dif = 0; c->sgsp.anis_k = 0; c->sgsp.momsf = 0; c->sgsp.reserved = 0;
+    c->sgsp.diff = 0.; c->sgsp.pran = 0.4; c->sgsp.zdec = 2000.; c->sgsp.zrough = 0.01; c->sgsp.min_w = 0.1;
+    c->sgsp.qt0 = nullptr;
     const int nz = params->nz;
     DevGrid &G = c->G;
     G.maxx = params->maxx; G.maxy = params->maxy; G.nz = nz;
@@ -459,12 +477,85 @@ static cudaError_t project(mg_ctx *c, double *mu, double *mv, double *mw, const 
 }
 
 // ---------------- one step ----------------
+// ---------------- SGS diffusion ----------------
+static SgsDev sgs_dev(const mg_ctx *c)
+{
+    const int nz = c->G.nz;
+    const double *P = c->sgs_prof;
+    SgsDev S{};
+    S.anis_k = c->sgsp.anis_k; S.momsf = c->sgsp.momsf; S.diff_on = c->sgsp.diff != 0.;
+    S.diff = c->sgsp.diff; S.pran = c->sgsp.pran; S.min_w = c->sgsp.min_w;
+    S.cs2d = P + nz; S.func = P + 2 * nz; S.fan = P + 3 * nz; S.n2c = P + 4 * nz; S.n2d = P + 5 * nz;
+    S.du = P + 6 * nz; S.dv = P + 7 * nz; S.dw = P + 8 * nz; S.dwt = P + 9 * nz;
+    return S;
+}
+static const double *sgs_qt0_dev(const mg_ctx *c) { return c->sgs_prof + SGS_NPROF * c->G.nz; }
+
+// allocate the SGS work fields (first use) and upload the per-level factors of sgsp
+static int ensure_sgs(mg_ctx *c)
+{
+    const DevGrid &G = c->G;
+    const int nz = G.nz;
+    auto field = [&](double **p, size_t bytes) -> int {
+        if (*p) return MG_OK;
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess) return cuerr(e);
+        c->bytes += bytes;
+        return cudaMemset(*p, 0, bytes) == cudaSuccess ? MG_OK : MG_ERR_CUDA;
+    };
+    int rc = field(&c->sgs_prof, (size_t)(SGS_NPROF + 1) * nz * sizeof(double));
+    for (int q = 0; q < 6 && !rc; q++) rc = field(&c->dij[q], c->fbytes);
+    if (!rc) rc = field(&c->fkv, c->fbytes);
+    for (int q = 0; q < 3 && !rc; q++) rc = field(&c->sgm[q], c->fbytes);
+    for (int q = 0; q < 3 && !rc; q++) rc = field(&c->sfc[q], (size_t)G.nx * G.ny * sizeof(double));
+    if (rc) return rc;
+    const mg_params &P = c->prm;
+    std::vector<double> h((size_t)(SGS_NPROF + 1) * nz);
+    sgs_host_profiles(nz, P.dx, P.dy, P.dz, P.fdz0, P.pt0, P.qv0, c->sgsp.anis_k, c->sgsp.zdec, c->sgsp.zrough, h.data());
+    for (int k = 0; k < nz; k++) h[(size_t)SGS_NPROF * nz + k] = c->sgs_qt0.empty() ? P.qv0[k] : c->sgs_qt0[k];
+    CKR(cudaMemcpyAsync(c->sgs_prof, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+// calc_subgrid, efud and eff0/effs of level n (once per step)
+static cudaError_t sgs_tendencies(mg_ctx *c, int *launches)
+{
+    const DevGrid &G = c->G;
+    const int ies = 1, iqt = c->prm.iqt >= 0 ? 1 + c->prm.iqt : -1;
+    const SgsDev S = sgs_dev(c);
+    SgsDij D{};
+    for (int q = 0; q < 6; q++) D.d[q] = c->dij[q];
+    PROF(c, "sgs_viscosity", launch_sgs_visc(G, S, c->mA[0], c->mA[1], c->mA[2], c->sA[ies], iqt >= 0 ? c->sA[iqt] : nullptr,
+                                             D, c->fkv, c->stream));
+    double *hf[7] = {c->dij[0], c->dij[1], c->dij[2], c->dij[3], c->dij[4], c->dij[5], c->fkv};
+    PROF(c, "sgs_halo", launch_halo_fill(G, hf, 7, c->stream));
+    PROF(c, "sgs_momentum", launch_sgs_mom(G, S, c->mA[0], c->mA[1], c->sA[0], c->fkv, D, c->sfc[2], nullptr, nullptr,
+                                           nullptr, c->sgm[0], c->sgm[1], c->sgm[2], c->stream));
+    SgsScal A{};
+    A.nf = c->nf - 1;
+    for (int f = 1; f < c->nf; f++) {
+        const int q = f - 1;
+        A.x[q] = c->sA[f];
+        A.out[q] = c->sgsc[f];
+        A.x0[q] = f == ies ? G.pt0 : (f == iqt ? sgs_qt0_dev(c) : nullptr);
+        A.fs[q] = f == ies ? c->sfc[0] : (f == iqt ? c->sfc[1] : nullptr);
+        A.fs_neg[q] = 1;
+    }
+    if (A.nf > 0) PROF(c, "sgs_scalars", launch_sgs_scal(G, S, c->sA[0], c->fkv, A, c->stream));
+    *launches += A.nf > 0 ? 4 : 3;
+    return cudaSuccess;
+}
+
 static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int want_maxdiv, int *launches)
 {
     const DevGrid &G = c->G;
     const mg_params &P = c->prm;
     const int nf = c->nf;
     const int ies = 1, iqt = P.iqt >= 0 ? 1 + P.iqt : -1;
+    if (c->sgs_on) {
+        cudaError_t e = sgs_tendencies(c, launches);
+        if (e != cudaSuccess) return e;
+    }
     for (int stage = 1; stage <= 2; stage++) {
         const double a_dt = (stage == 1 ? 1. : 0.5) * G.dt0;
         const double b = stage == 1 ? 0. : 1.;
@@ -479,7 +570,9 @@ static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int wa
             a1.xout[f] = stage == 1 ? c->sB[f] : c->sA[f];
             a1.tend[f] = c->ts[f];
             a1.fst[f] = (f == ies && G.with_buoy) ? c->fes : ((f == iqt && G.with_buoy) ? c->fqt : nullptr);
+            a1.sgs[f] = (c->sgs_on && f >= 1) ? c->sgsc[f] : nullptr;
         }
+        a1.sgs_post = c->sgs_on ? ((1u << ies) | (iqt >= 0 ? 1u << iqt : 0u)) : 0u;
         const double *const *mom = stage == 1 ? c->mA : c->mB;
         a1.mw = mom[2];
         if (P.precision == MG_PREC_MIXED)
@@ -510,6 +603,7 @@ static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int wa
         a2.tu = c->tm[0]; a2.tv = c->tm[1]; a2.tw = c->tm[2];
         a2.mode = 0;
         a2.err = c->derr;
+        if (c->sgs_on) { a2.su = c->sgm[0]; a2.sv = c->sgm[1]; a2.sw = c->sgm[2]; }
         const K2Maps &mm = stage == 1 ? c->mmaps1 : c->mmaps2;
         if (P.precision == MG_PREC_MIXED)
             PROF(c, "k2_momentum", launch_k2_mixed(G, a2, mm, c->stream));
@@ -776,6 +870,140 @@ extern "C" int mg_advection_ac(mg_ctx *c, const double *x, const double *mu, con
     CKR(c->prm.precision == MG_PREC_MIXED ? launch_k1_mixed(c->G, a, maps, c->stream) : launch_k1(c->G, a, maps, c->stream));
     CKR(d2h(c, xs, c->unit[4], cudaMemcpyDeviceToHost));
     return check_err(c);
+}
+
+// ---- SGS turbulence diffusion (src/PHYS/subgrid.f90) ----
+extern "C" int mg_sgs_profiles(const mg_params *p, const mg_sgs_params *s, double *prof)
+{
+    if (!p || !s || !prof || p->nz < 5 || !p->fdz0 || !p->pt0 || !p->qv0) return MG_ERR_PARAM;
+    sgs_host_profiles(p->nz, p->dx, p->dy, p->dz, p->fdz0, p->pt0, p->qv0, s->anis_k, s->zdec, s->zrough, prof);
+    return MG_OK;
+}
+
+static int sgs_validate(const mg_sgs_params *s)
+{
+    if (!s || s->reserved != 0) return MG_ERR_PARAM;
+    if (!(std::isfinite(s->diff) && std::isfinite(s->pran) && std::isfinite(s->zdec) && std::isfinite(s->zrough) &&
+          std::isfinite(s->min_w)))
+        return MG_ERR_PARAM;
+    if (s->pran == 0. || s->zdec <= 0. || s->min_w <= 0. || s->zrough < 0.) return MG_ERR_PARAM;
+    return MG_OK;
+}
+
+extern "C" int mg_set_sgs(mg_ctx *c, const mg_sgs_params *s)
+{
+    if (!c) return MG_ERR_PARAM;
+    int rc = sgs_validate(s);
+    if (rc) return rc;
+    if (c->G.nz < 5) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    c->sgsp = *s;
+    c->sgsp.qt0 = nullptr;
+    c->sgs_qt0.clear();
+    if (s->qt0) c->sgs_qt0.assign(s->qt0, s->qt0 + c->G.nz);
+    rc = ensure_sgs(c);
+    if (rc) return rc;
+    if (s->with_dif)
+        for (int f = 1; f < c->nf; f++)
+            if (!c->sgsc[f]) {
+                CKR(cudaMalloc(&c->sgsc[f], c->fbytes));
+                c->bytes += c->fbytes;
+                CKR(cudaMemset(c->sgsc[f], 0, c->fbytes));
+            }
+    c->sgs_on = s->with_dif != 0;
+    // step graphs recorded before this call no longer describe the step
+    for (int i = 0; i < 2; i++)
+        if (c->gexec[i]) { cudaGraphExecDestroy(c->gexec[i]); c->gexec[i] = nullptr; }
+    return MG_OK;
+}
+
+extern "C" int mg_set_surface_fluxes(mg_ctx *c, const double *esflux, const double *qvflux, const double *mflux)
+{
+    if (!c) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    int rc = ensure_sgs(c);
+    if (rc) return rc;
+    const size_t b = (size_t)c->G.nx * c->G.ny * sizeof(double);
+    const double *src[3] = {esflux, qvflux, mflux};
+    for (int q = 0; q < 3; q++) {
+        if (src[q]) CKR(cudaMemcpyAsync(c->sfc[q], src[q], b, cudaMemcpyHostToDevice, c->stream));
+        else CKR(cudaMemsetAsync(c->sfc[q], 0, b, c->stream));
+    }
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+extern "C" int mg_calc_subgrid(mg_ctx *c, const double *u, const double *v, const double *w, const double *es,
+                               const double *qt, double *fkv)
+{
+    if (!c || !u || !v || !w || !es || !fkv) return MG_ERR_PARAM;
+    if (c->G.nz < 5) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    int rc = ensure_sgs(c);
+    if (!rc) rc = ensure_unit(c, 5);
+    if (rc) return rc;
+    const double *in[5] = {u, v, w, es, qt};
+    for (int q = 0; q < 5; q++)
+        if (in[q]) CKR(h2d(c, c->unit[q], in[q], cudaMemcpyHostToDevice));
+    SgsDij D{};
+    for (int q = 0; q < 6; q++) D.d[q] = c->dij[q];
+    CKR(launch_sgs_visc(c->G, sgs_dev(c), c->unit[0], c->unit[1], c->unit[2], c->unit[3], qt ? c->unit[4] : nullptr, D,
+                        c->fkv, c->stream));
+    double *hf[1] = {c->fkv};
+    CKR(launch_halo_fill(c->G, hf, 1, c->stream));
+    CKR(d2h(c, fkv, c->fkv, cudaMemcpyDeviceToHost));
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+extern "C" int mg_efud(mg_ctx *c, const double *u, const double *v, const double *w, const double *dens,
+                       const double *fkv, double *su, double *sv, double *sw)
+{
+    if (!c || !u || !v || !w || !dens || !fkv || !su || !sv || !sw) return MG_ERR_PARAM;
+    if (c->G.nz < 5) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    int rc = ensure_sgs(c);
+    if (!rc) rc = ensure_unit(c, 8);
+    if (rc) return rc;
+    const double *in[8] = {u, v, w, dens, fkv, su, sv, sw};
+    for (int q = 0; q < 8; q++) CKR(h2d(c, c->unit[q], in[q], cudaMemcpyHostToDevice));
+    SgsDij D{};
+    for (int q = 0; q < 6; q++) D.d[q] = c->dij[q];
+    const SgsDev S = sgs_dev(c);
+    CKR(launch_sgs_visc(c->G, S, c->unit[0], c->unit[1], c->unit[2], nullptr, nullptr, D, nullptr, c->stream));
+    CKR(launch_halo_fill(c->G, D.d, 6, c->stream));
+    CKR(launch_sgs_mom(c->G, S, c->unit[0], c->unit[1], c->unit[3], c->unit[4], D, c->sfc[2], c->unit[5], c->unit[6],
+                       c->unit[7], c->unit[5], c->unit[6], c->unit[7], c->stream));
+    CKR(d2h(c, su, c->unit[5], cudaMemcpyDeviceToHost));
+    CKR(d2h(c, sv, c->unit[6], cudaMemcpyDeviceToHost));
+    CKR(d2h(c, sw, c->unit[7], cudaMemcpyDeviceToHost));
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+extern "C" int mg_eff(mg_ctx *c, int kind, const double *dens, const double *fkv, const double *x,
+                      const double *flux_s, double *ec)
+{
+    if (!c || kind < 1 || kind > 3 || !dens || !fkv || !x || !ec) return MG_ERR_PARAM;
+    if (c->G.nz < 5) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    int rc = ensure_sgs(c);
+    if (!rc) rc = ensure_unit(c, 5);
+    if (rc) return rc;
+    CKR(h2d(c, c->unit[0], dens, cudaMemcpyHostToDevice));
+    CKR(h2d(c, c->unit[1], fkv, cudaMemcpyHostToDevice));
+    CKR(h2d(c, c->unit[2], x, cudaMemcpyHostToDevice));
+    CKR(h2d(c, c->unit[3], ec, cudaMemcpyHostToDevice));
+    if (flux_s)
+        CKR(cudaMemcpyAsync(c->unit[4], flux_s, (size_t)c->G.nx * c->G.ny * sizeof(double), cudaMemcpyHostToDevice,
+                            c->stream));
+    SgsScal A{};
+    A.nf = 1;
+    A.x[0] = c->unit[2];
+    A.out[0] = c->unit[3];
+    A.x0[0] = kind == 1 ? c->G.pt0 : (kind == 2 ? sgs_qt0_dev(c) : nullptr);
+    A.fs[0] = flux_s ? c->unit[4] : nullptr;
+    A.fs_neg[0] = 0;
+    CKR(launch_sgs_scal(c->G, sgs_dev(c), c->unit[0], c->unit[1], A, c->stream));
+    CKR(d2h(c, ec, c->unit[3], cudaMemcpyDeviceToHost));
+    return cuerr(cudaStreamSynchronize(c->stream));
 }
 
 // ---- tangent linear and adjoint of the scalar advection operator (WENO) ----

@@ -574,7 +574,11 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
                         double *xs = A.xout[f];
                         xs[idx] = ((xs[idx] - Tx) - Ty) - Tz;
                     } else {
-                        const double T = ((0. - Tx) - Ty) - Tz;
+                        const double *sgp = A.sgs[f];
+                        const bool spost = (A.sgs_post >> f) & 1u;
+                        const double sgv = sgp ? sgp[idx] : 0.;
+                        double T = (((sgp && !spost ? 0. + sgv : 0.) - Tx) - Ty) - Tz;
+                        if (sgp && spost) T = T + sgv;
                         const double told = STAGE == 1 ? 0. : cur_tend[u];
                         const double tn = T + A.b * told;
                         const bool weighted = f > 0;

@@ -339,9 +339,9 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
         if (k >= 2) gpz = (ppc - pp_below) * ldg(dz1, k - 2);
         else gpz = (double)MM(2, 0, 0, 0) / (dt0 * ldg(G.avden0, 0));
         pp_below = ppc;
-        double wsu = 0. - d0 * gpx;
-        double wsv = 0. - d0 * gpy;
-        double wsw = 0. - a0 * gpz;
+        double wsu = (A.su ? A.su[idx] : 0.) - d0 * gpx;
+        double wsv = (A.sv ? A.sv[idx] : 0.) - d0 * gpy;
+        double wsw = (A.sw ? A.sw[idx] : 0.) - a0 * gpz;
 
         // ---------------- buoyancy (imp_buoy: state + cdiag*dt0*states) ----------------
         double buoy = 0.;

@@ -59,6 +59,11 @@ struct K1Args {
     int mode;                      // 0: stage update; 1: unit mode: xout := ((xout - Tx) - Ty) - Tz
     int *err;                      // device error flag (bounded waits)
     int xold_is_xin;               // xold[f] == xin[f]: the level-n value is the plane's own cell
+    // SGS tendency of field f (level-n, equal in both stages), or null.  Bit f of
+    // sgs_post set: T = advection + S (es, qt: scalars.f90:146-150); clear: S is the
+    // initial tendency that advection_ac then updates (tracers: tracers.f90:81-106).
+    const double *sgs[MG_MAXF];
+    unsigned sgs_post;
 };
 // TMA descriptors of the K1 inputs: haloed planes (38 x 14) of every field, momentum boxes (34 x 9)
 struct alignas(64) K1Maps {
@@ -83,6 +88,7 @@ struct K2Args {
     double *tu, *tv, *tw;          // tendency accumulators
     int mode;                      // 0: full stage; 1: unit mode: ou/ov/ow := advection tendency only
     int *err;                      // device error flag (bounded waits)
+    const double *su, *sv, *sw;    // SGS momentum tendencies (efud), or null: winds starts at S
 };
 // TMA descriptors of the K2 stencil momentum (boxes of 38 x 12 doubles)
 struct alignas(64) K2Maps {
@@ -100,6 +106,36 @@ int make_field_map(const DevGrid &g, const double *base, int boxx, int boxy, CUt
 cudaError_t launch_k2(const DevGrid &g, const K2Args &a, const K2Maps &maps, cudaStream_t s);
 cudaError_t launch_k2_mixed(const DevGrid &g, const K2Args &a, const K2Maps &maps, cudaStream_t s);
 cudaError_t launch_halo_fill(const DevGrid &g, double *const *fields, int nf, cudaStream_t s);
+
+// ---- SGS turbulence diffusion (k_sgs.cu) ----
+#define SGS_NPROF 10   // per-level factors: z0, (C_s delta)^2, func, f_an, N2 coef., N2 den., d/dz den. u, v, w, w(nz-1)
+struct SgsDev {
+    int anis_k, momsf, diff_on;
+    double diff, pran, min_w;
+    const double *cs2d, *func, *fan, *n2c, *n2d, *du, *dv, *dw, *dwt;   // device, nz each
+};
+struct SgsDij {
+    double *d[6];   // d11, d22, d33, d12, d13, d23 (cell centred, periodic ghosts)
+};
+struct SgsScal {
+    int nf;
+    const double *x[MG_MAXF];      // natural level-n scalar
+    const double *x0[MG_MAXF];     // diff != 0: base profile subtracted (pt0, qt0), or null
+    const double *fs[MG_MAXF];     // surface flux (nx*ny), or null
+    int fs_neg[MG_MAXF];           // flux_s = -fs (eff0 passes -surf%esflux, -surf%qvflux)
+    double *out[MG_MAXF];          // SGS tendency (levels 1..nz-1 written)
+};
+__host__ __device__ __forceinline__ double fmax_ref(double a, double b) { return a > b ? a : b; }
+cudaError_t launch_sgs_visc(const DevGrid &g, const SgsDev &s, const double *u, const double *v, const double *w,
+                            const double *es, const double *qt, const SgsDij &d, double *fkv, cudaStream_t st);
+cudaError_t launch_sgs_mom(const DevGrid &g, const SgsDev &s, const double *u, const double *v, const double *dens,
+                           const double *fkv, const SgsDij &d, const double *mflux, const double *in_u,
+                           const double *in_v, const double *in_w, double *out_u, double *out_v, double *out_w,
+                           cudaStream_t st);
+cudaError_t launch_sgs_scal(const DevGrid &g, const SgsDev &s, const double *dens, const double *fkv,
+                            const SgsScal &a, cudaStream_t st);
+void sgs_host_profiles(int nz, double dx, double dy, double dz, const double *fdz0, const double *pt0,
+                       const double *qv0, int anis_k, double zdec, double zrough, double *prof);
 
 // tangent linear / adjoint of the scalar advection operator (k_adjoint.cu)
 cudaError_t launch_advection_tl(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,

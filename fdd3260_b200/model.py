@@ -26,6 +26,8 @@ class Mimica:
         _lib.check(L.mg_create(C.byref(params), device, C.byref(h)), "mg_create")
         self._h = h
         self._L = L
+        if domain.sgs is not None:
+            self.set_sgs(domain.sgs)
 
     # ---- lifetime ----
     def close(self) -> None:
@@ -52,6 +54,42 @@ class Mimica:
     @property
     def launches_per_call(self) -> int:
         return int(self._L.mg_last_launch_count(self._h))
+
+    # ---- SGS turbulence diffusion (subgrid.f90) ----
+    def set_sgs(self, sgs, with_dif: bool = True) -> None:
+        """Switch SGS diffusion on (or off) for the following steps; uploads the surface
+        fluxes of ``sgs`` (``None`` = zero)."""
+        p, keep = sgs.params(self.domain.nz, with_dif)
+        _lib.check(self._L.mg_set_sgs(self._h, C.byref(p)), "mg_set_sgs")
+        self.set_surface_fluxes(sgs.esflux, sgs.qvflux, sgs.mflux)
+
+    def set_surface_fluxes(self, esflux=None, qvflux=None, mflux=None) -> None:
+        d = self.domain
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (esflux, qvflux, mflux)]
+        for a in arrs:
+            if a is not None and a.shape != (d.ny, d.nx):
+                raise ValueError(f"surface flux arrays are (ny, nx) = {(d.ny, d.nx)}")
+        _lib.check(self._L.mg_set_surface_fluxes(self._h, *[_lib.ptr(a) for a in arrs]), "mg_set_surface_fluxes")
+
+    def calc_subgrid(self, u, v, w, es, qt=None) -> np.ndarray:
+        fkv = np.zeros(self.domain.shape)
+        c = [np.ascontiguousarray(a, dtype=np.float64) if a is not None else None for a in (u, v, w, es, qt)]
+        _lib.check(self._L.mg_calc_subgrid(self._h, *[_lib.ptr(a) for a in c], _lib.ptr(fkv)), "mg_calc_subgrid")
+        return fkv
+
+    def efud(self, u, v, w, dens, fkv, su=None, sv=None, sw=None):
+        d = self.domain
+        outs = [np.zeros(d.shape) if a is None else np.array(a, dtype=np.float64, copy=True) for a in (su, sv, sw)]
+        c = [np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, w, dens, fkv)]
+        _lib.check(self._L.mg_efud(self._h, *[_lib.ptr(a) for a in c], *[_lib.ptr(a) for a in outs]), "mg_efud")
+        return tuple(outs)
+
+    def eff(self, kind: int, dens, fkv, x, flux_s=None, ec=None) -> np.ndarray:
+        out = np.zeros(self.domain.shape) if ec is None else np.array(ec, dtype=np.float64, copy=True)
+        c = [np.ascontiguousarray(a, dtype=np.float64) for a in (dens, fkv, x)]
+        fs = None if flux_s is None else np.ascontiguousarray(flux_s, dtype=np.float64)
+        _lib.check(self._L.mg_eff(self._h, kind, *[_lib.ptr(a) for a in c], _lib.ptr(fs), _lib.ptr(out)), "mg_eff")
+        return out
 
     # ---- resident state ----
     def upload(self, st: State) -> None:

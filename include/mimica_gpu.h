@@ -180,6 +180,51 @@ int mg_fft_solve(mg_ctx *ctx, const double *tend, double *out);
 int mg_anelastic_pressure(mg_ctx *ctx, double *mu, double *mv, double *mw, double *p,
                           const double *wold, double *maxdiv, double *p1);
 
+/* ---- SGS turbulence diffusion (src/PHYS/subgrid.f90) ----
+ * The Smagorinsky-Lilly closure of the build without TKE: calc_subgrid (cal_dij,
+ * stability, calc_smago with the 'Lilly' stability correction, :87-145, :793-866,
+ * :909-1001), the momentum stresses efud (:187-456) and the scalar fluxes eff0/effs/eff
+ * (:459-789, grad_quick).  Scope: diff_ord = 2, nl_sgs = .false., no microphysics
+ * (the dry N2 branch; ptv = theta (1 + epsm qt)), CONSERVATIVE, ISENTROPIC, periodic
+ * lateral and rigid ('nnf') vertical boundaries, CHANNEL off.
+ * With with_dif set, every mg_step / mg_step_graph evaluates the three once per step
+ * from the level-n state (the reference's subgrid_interface before the dynamics loop
+ * and efud/eff0/effs on wind2/state2/pressure2, time_step.f90:222, momentum.f90:104,
+ * scalars.f90:106, tracers.f90:81-85) and adds them in both Heun stages. */
+typedef struct mg_sgs_params {
+    int with_dif;              /* with_dif: 0 = off (the default of a new context) */
+    int anis_k;                /* anis_k: anisotropic viscosity, f_an = (sqrt(dx dy)/dz(k))**2 */
+    int momsf;                 /* momsf > 0: surface momentum flux from mg_set_surface_fluxes' mflux */
+    int reserved;              /* must be 0 */
+    double diff;               /* diff: 0 = Smagorinsky-Lilly; otherwise constant viscosity |diff| */
+    double pran;               /* pran (!= 0); < 0: diffusion damped above zdec, scalars by 1/|pran| */
+    double zdec;               /* zdec [m] (> 0) */
+    double zrough;             /* zrough [m], in the length scale vk (z + zrough) */
+    double min_w;              /* min_w [m/s] (> 0), floor of the surface wind in the momentum flux */
+    const double *qt0;         /* diff != 0: base-state qt profile (nz, host), NULL = qv0; copied */
+} mg_sgs_params;
+int mg_set_sgs(mg_ctx *ctx, const mg_sgs_params *sgs);
+/* surface fluxes of the reference's surf%esflux, surf%qvflux, surf%mflux (host arrays
+ * nx*ny, i fastest, the reference's 2-D layout; NULL = 0).  The SGS step reads them on
+ * the device; call again whenever the caller's surface layer updates them. */
+int mg_set_surface_fluxes(mg_ctx *ctx, const double *esflux, const double *qvflux, const double *mflux);
+/* per-level factors (host, prof[q*nz + k-1]): q = 0 z0, 1 (C_s delta)**2, 2 pran < 0
+ * damping, 3 f_an, 4 N2 coefficient, 5 N2 denominator, 6..9 the d/dz denominators of
+ * grad_wind_3d (gradients.f90:884-905) for u, v, w and w at nz-1. */
+int mg_sgs_profiles(const mg_params *p, const mg_sgs_params *sgs, double *prof);
+/* unit entries, host arrays in the reference layout with periodic ghosts:
+ *   mg_calc_subgrid: fkv := turbu%fkv from natural u, v, w, es (theta), qt (NULL = dry)
+ *   mg_efud: su, sv, sw := (s + eh) + ev (winds%u ... in efud) for dens and fkv = turbu%fkv
+ *   mg_eff: ec := the eff tendency on levels 1..nz-1 (other cells unchanged);
+ *           kind 1 = es (x0 = pt0), 2 = qt (x0 = qt0), 3 = a tracer (effs, x0 = 0);
+ *           flux_s: eff's surface flux argument (nx*ny), NULL = 0 */
+int mg_calc_subgrid(mg_ctx *ctx, const double *u, const double *v, const double *w, const double *es,
+                    const double *qt, double *fkv);
+int mg_efud(mg_ctx *ctx, const double *u, const double *v, const double *w, const double *dens,
+            const double *fkv, double *su, double *sv, double *sw);
+int mg_eff(mg_ctx *ctx, int kind, const double *dens, const double *fkv, const double *x,
+           const double *flux_s, double *ec);
+
 /* ---- tangent linear and adjoint of the scalar advection operator (WENO; no counterpart
  * in the reference, whose adjoint does not exist) ----
  * The operator is the advective tendency A(x, m) = -(Tx + Ty + Tz) that mg_advection_ac

@@ -1662,8 +1662,363 @@ int mo_anelastic_pressure(const mo_grid *g, double *mu, double *mv, double *mw, 
 }
 
 /* ======================================================================
+ * SGS turbulence: src/PHYS/subgrid.f90 (Smagorinsky-Lilly closure, TKE undefined,
+ * nl_sgs = .false., diff_ord = 2, lmicro = 0, CONSERVATIVE, ISENTROPIC) and the
+ * gradients it uses, src/TOOLS/gradients.f90 grad_wind_3d :794-983, cal_dij
+ * :476-600, grad_quick :62-187.  Constants: src/TYPES/shared_turbu.f90:47-53,
+ * src/TYPES/shared_data.f90:148 (g), src/TYPES/shared_thermo.f90:61 (epsm).
+ * ==================================================================== */
+#define SGS_CS 0.23
+#define SGS_RIC 0.25
+#define SGS_VK 0.41
+#define SGS_G 9.81
+#define SGS_EPSM 0.60243
+#define SGS_C98 (9. / 8.)
+#define SGS_C124 (1. / 24.)
+
+static const mo_sgs *sgs_of(const mo_grid *g) { return (g->sgs && g->sgs->with_dif) ? g->sgs : NULL; }
+
+/* Per-level quantities of the routines below, evaluated with the reference's
+ * expressions: z0 (define_grid.f90:132-135), length_scale :1183-1232 with l_d = 1e8
+ * (TKE off), the pran < 0 damping (subgrid.f90:234-239), f_an (:244-249), the N2
+ * coefficients (:929-963) and the d/dz denominators of grad_wind_3d (:884-905). */
+void mo_sgs_profiles(const mo_grid *g, double *prof)
+{
+    const int nz = g->nz;
+    const mo_sgs *s = g->sgs;
+    const double dx = g->dx, dy = g->dy, dz = g->dz;
+    const double *f = g->fdz0;
+    double *z0 = prof, *cs2d = prof + nz, *func = prof + 2 * nz, *fan = prof + 3 * nz;
+    double *n2c = prof + 4 * nz, *n2d = prof + 5 * nz;
+    double *du = prof + 6 * nz, *dv = prof + 7 * nz, *dw = prof + 8 * nz, *dwt = prof + 9 * nz;
+    const int anis = s ? s->anis_k : 0;
+    const double zdec = s ? s->zdec : 2000., zrough = s ? s->zrough : 0.01;
+    for (int q = 0; q < MO_SGS_NPROF * nz; q++) prof[q] = 0.;
+    P1(z0, 1) = 0.5 * dz * P1(f, 1);
+    for (int k = 2; k <= nz; k++) P1(z0, k) = P1(z0, k - 1) + 0.5 * dz * (P1(f, k - 1) + P1(f, k));
+    const double l_d = 1e8;
+    for (int k = 1; k <= nz; k++) {
+        double deltas = anis ? dz * P1(f, k) : pow(dx * dy * dz * P1(f, k), 1. / 3.);
+        double l_z = SGS_VK * (P1(z0, k) + zrough);
+        double delta = 1. / sqrt(1. / (deltas * deltas) + 1. / (l_d * l_d) + 1. / (l_z * l_z));
+        double cd = SGS_CS * delta;
+        P1(cs2d, k) = cd * cd;
+        P1(func, k) = dmax2(1. - exp(6. * (P1(z0, k) - zdec) / zdec), 0.);
+        if (anis) {
+            double t = pow(dx * dy, 1. / 2.) / (dz * P1(f, k));
+            P1(fan, k) = t * t;
+        } else {
+            P1(fan, k) = 1.;
+        }
+        double ref = g->pt0[k - 1] * (1. + SGS_EPSM * g->qv0[k - 1]);
+        P1(n2c, k) = (k == 1 || k == nz) ? 0.5 * SGS_G / ref : SGS_G / ref;
+    }
+    for (int k = 2; k <= nz - 1; k++) P1(n2d, k) = dz * (0.5 * P1(f, k + 1) + P1(f, k) + 0.5 * P1(f, k - 1));
+    P1(n2d, 1) = 0.5 * dz * (P1(f, 2) + P1(f, 1));
+    P1(n2d, nz) = 0.5 * dz * (P1(f, nz) + P1(f, nz - 1));
+    for (int k = 2; k <= nz - 2; k++) {
+        P1(du, k) = dz * (0.5 * P1(f, k + 2) + P1(f, k) + P1(f, k - 1) + 0.5 * P1(f, k - 1));
+        P1(dv, k) = dz * (0.5 * P1(f, k + 2) + P1(f, k) + P1(f, k + 1) + 0.5 * P1(f, k - 1));
+        P1(dw, k) = dz * (P1(f, k - 1) + P1(f, k) + P1(f, k + 1));
+    }
+    P1(dwt, nz - 1) = dz * (P1(f, nz) + P1(f, nz - 1) + P1(f, nz - 2));
+}
+
+/* 4th-order staggered derivative along a line: 9/8 (a1 - a0)/d - 1/24 (a2 - am1)/d */
+static double d4(double am1, double a0, double a1, double a2, double d1)
+{
+    return SGS_C98 * (a1 - a0) * d1 - SGS_C124 * (a2 - am1) * d1;
+}
+
+/* grad_wind_3d (gradients.f90:794-983), bcl(6) = 'nnf': the nine gradients, each
+ * evaluated on the interior columns and then given periodic ghosts (gradbc). */
+static void grad_wind_3d(const mo_grid *g, const double *prof, const double *u, const double *v, const double *w,
+                         double **gr)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    const double dx1 = 1. / g->dx, dy1 = 1. / g->dy;
+    const double *dz1 = g->dz1, *dz1w = g->dz1w;
+    const double *du = prof + 6 * nz, *dv = prof + 7 * nz, *dw = prof + 8 * nz, *dwt = prof + 9 * nz;
+    const double *f3[3] = {u, v, w};
+    /* gr[3*c + d] = d(f_c)/d(x_d) */
+    for (int q = 0; q < 9; q++) memset(gr[q], 0, ncell(g) * 8);
+    for (int k = 1; k <= nz; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++)
+                for (int c = 0; c < 3; c++) {
+                    const double *a = f3[c];
+                    gr[3 * c][IX(g, i, j, k)] = d4(a[IX(g, i - 1, j, k)], a[IX(g, i, j, k)], a[IX(g, i + 1, j, k)],
+                                                   a[IX(g, i + 2, j, k)], dx1);
+                    gr[3 * c + 1][IX(g, i, j, k)] = d4(a[IX(g, i, j - 1, k)], a[IX(g, i, j, k)], a[IX(g, i, j + 1, k)],
+                                                       a[IX(g, i, j + 2, k)], dy1);
+                }
+    for (int j = 4; j <= ny - 2; j++)
+        for (int i = 4; i <= nx - 2; i++) {
+#define U3(k) u[IX(g, i, j, k)]
+#define V3(k) v[IX(g, i, j, k)]
+#define W3(k) w[IX(g, i, j, k)]
+            double *gu = gr[2], *gv = gr[5], *gw = gr[8];
+            for (int k = 2; k <= nz - 2; k++) {
+                gu[IX(g, i, j, k)] = SGS_C98 * (U3(k + 1) - U3(k)) * P1(dz1, k) - 1. / 8. * (U3(k + 2) - U3(k - 1)) / P1(du, k);
+                gv[IX(g, i, j, k)] = SGS_C98 * (V3(k + 1) - V3(k)) * P1(dz1, k) - 1. / 8. * (V3(k + 2) - V3(k - 1)) / P1(dv, k);
+                gw[IX(g, i, j, k)] = SGS_C98 * (W3(k + 1) - W3(k)) * P1(dz1w, k) - 1. / 8. * (W3(k + 2) - W3(k - 1)) / P1(dw, k);
+            }
+            gu[IX(g, i, j, 1)] = (U3(2) - U3(1)) * P1(dz1, 1);
+            gv[IX(g, i, j, 1)] = (V3(2) - V3(1)) * P1(dz1, 1);
+            gw[IX(g, i, j, 1)] = (W3(2) - 0.) * P1(dz1w, 1);
+            gu[IX(g, i, j, nz - 1)] = (U3(nz) - U3(nz - 1)) * P1(dz1, nz - 1);
+            gv[IX(g, i, j, nz - 1)] = (V3(nz) - V3(nz - 1)) * P1(dz1, nz - 1);
+            gw[IX(g, i, j, nz - 1)] = SGS_C98 * (W3(nz) - W3(nz - 1)) * P1(dz1w, nz - 1) - 1. / 8. * (0. - W3(nz - 2)) / P1(dwt, nz - 1);
+            gu[IX(g, i, j, nz)] = gu[IX(g, i, j, nz - 1)];
+            gv[IX(g, i, j, nz)] = gv[IX(g, i, j, nz - 1)];
+            gw[IX(g, i, j, nz)] = (0. - W3(nz)) * P1(dz1w, nz);
+#undef U3
+#undef V3
+#undef W3
+        }
+    for (int q = 0; q < 9; q++) mo_statebc(g, gr[q]);
+}
+
+void mo_cal_dij(const mo_grid *g, const double *u, const double *v, const double *w, double *const *d)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    double *prof = dalloc((size_t)MO_SGS_NPROF * nz);
+    mo_sgs_profiles(g, prof);
+    double *gr[9];
+    for (int q = 0; q < 9; q++) gr[q] = dalloc(ncell(g));
+    grad_wind_3d(g, prof, u, v, w, gr);
+    /* gr index: u: 0 x, 1 y, 2 z; v: 3, 4, 5; w: 6, 7, 8 */
+    memcpy(d[0], gr[0], ncell(g) * 8);
+    memcpy(d[1], gr[4], ncell(g) * 8);
+    memcpy(d[2], gr[8], ncell(g) * 8);
+    for (int q = 3; q < 6; q++) memset(d[q], 0, ncell(g) * 8);
+    const double *gux = gr[0], *guy = gr[1], *guz = gr[2], *gvx = gr[3], *gvz = gr[5], *gwx = gr[6], *gwy = gr[7];
+    (void)gux;
+#define G(a, i, j, k) (a)[IX(g, i, j, k)]
+    for (int k = 2; k <= nz - 1; k++)
+        for (int j = 3; j <= ny - 1; j++)
+            for (int i = 3; i <= nx - 1; i++) {
+                d[4][IX(g, i, j, k)] = 0.5 * (0.25 * (G(guz, i, j, k) + G(guz, i + 1, j, k) + G(guz, i, j, k - 1) + G(guz, i + 1, j, k - 1)) +
+                                              0.25 * (G(gwx, i - 1, j, k + 1) + G(gwx, i, j, k + 1) + G(gwx, i - 1, j, k) + G(gwx, i, j, k)));
+                d[3][IX(g, i, j, k)] = 0.5 * (0.25 * (G(guy, i, j, k) + G(guy, i + 1, j, k) + G(guy, i, j - 1, k) + G(guy, i + 1, j - 1, k)) +
+                                              0.25 * (G(gvx, i - 1, j + 1, k) + G(gvx, i, j + 1, k) + G(gvx, i - 1, j, k) + G(gvx, i, j, k)));
+                d[5][IX(g, i, j, k)] = 0.5 * (0.25 * (G(gvz, i, j, k) + G(gvz, i, j + 1, k) + G(gvz, i, j, k - 1) + G(gvz, i, j + 1, k - 1)) +
+                                              0.25 * (G(gwy, i, j - 1, k + 1) + G(gwy, i, j, k + 1) + G(gwy, i, j - 1, k) + G(gwy, i, j, k)));
+            }
+#undef G
+    for (int q = 0; q < 9; q++) free(gr[q]);
+    free(prof);
+}
+
+/* stability (subgrid.f90:909-1001, dry branch) and calc_smago (:793-866, 'Lilly') */
+void mo_calc_subgrid(const mo_grid *g, const double *u, const double *v, const double *w,
+                     const double *es, const double *qt, double *fkv)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    const mo_sgs *s = g->sgs;
+    const size_t nc = ncell(g);
+    if (s && s->diff != 0.) {   /* fixed diffusion coefficient (:131-133) */
+        for (size_t c = 0; c < nc; c++) fkv[c] = fabs(s->diff);
+        return;
+    }
+    const double pran = s ? s->pran : 0.4;
+    double *prof = dalloc((size_t)MO_SGS_NPROF * nz);
+    mo_sgs_profiles(g, prof);
+    const double *cs2d = prof + nz, *n2c = prof + 4 * nz, *n2d = prof + 5 * nz;
+    double *d[6];
+    for (int q = 0; q < 6; q++) d[q] = dalloc(nc);
+    mo_cal_dij(g, u, v, w, d);
+    double *ptv = dalloc(nc);
+    for (size_t c = 0; c < nc; c++) ptv[c] = es[c] * (1. + SGS_EPSM * (qt ? qt[c] : 0.));
+    memset(fkv, 0, nc * 8);
+    for (int k = 1; k <= nz; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) {
+                size_t c = IX(g, i, j, k);
+                double n2;
+                if (k == 1) n2 = P1(n2c, 1) * (ptv[IX(g, i, j, 2)] - ptv[IX(g, i, j, 1)]) / P1(n2d, 1);
+                else if (k == nz) n2 = P1(n2c, nz) * (ptv[IX(g, i, j, nz)] - ptv[IX(g, i, j, nz - 1)]) / P1(n2d, nz);
+                else n2 = P1(n2c, k) * (ptv[IX(g, i, j, k + 1)] - ptv[IX(g, i, j, k - 1)]) / P1(n2d, k);
+                /* sum(dij*dij) in array element order (l fastest), dij symmetric */
+                double d11 = d[0][c], d22 = d[1][c], d33 = d[2][c], d12 = d[3][c], d13 = d[4][c], d23 = d[5][c];
+                double sm = 0.;
+                sm = sm + d11 * d11; sm = sm + d12 * d12; sm = sm + d13 * d13;
+                sm = sm + d12 * d12; sm = sm + d22 * d22; sm = sm + d23 * d23;
+                sm = sm + d13 * d13; sm = sm + d23 * d23; sm = sm + d33 * d33;
+                double s2 = dmax2(2. * sm, 1.e-12);
+                double ri = n2 / dmax2(s2, 1.e-12) / fabs(pran);
+                double fri = ri <= SGS_RIC ? sqrt(1. - dmax2(ri, -0.25) / SGS_RIC) : 0.;
+                fkv[c] = P1(cs2d, k) * sqrt(s2) * dmax2(fri, 0.);
+            }
+    mo_statebc(g, fkv);
+    for (int q = 0; q < 6; q++) free(d[q]);
+    free(ptv);
+    free(prof);
+}
+
+/* efud (subgrid.f90:187-456), nl_sgs = .false., CHANNEL off */
+void mo_efud(const mo_grid *g, const double *u, const double *v, const double *w, const double *dens,
+             const double *fkv, double *su, double *sv, double *sw)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    const mo_sgs *s = g->sgs;
+    const size_t nc = ncell(g);
+    const double dx1 = 1. / g->dx, dy1 = 1. / g->dy;
+    double *prof = dalloc((size_t)MO_SGS_NPROF * nz);
+    mo_sgs_profiles(g, prof);
+    const double *func = prof + 2 * nz, *fan = prof + 3 * nz;
+    double *d[6];
+    for (int q = 0; q < 6; q++) d[q] = dalloc(nc);
+    mo_cal_dij(g, u, v, w, d);
+    double *fe = dalloc(nc), *fh = dalloc(nc);
+    for (int k = 1; k <= nz; k++)
+        for (int j = 1; j <= ny; j++)
+            for (int i = 1; i <= nx; i++) {
+                size_t c = IX(g, i, j, k);
+                double t = dens[c] * fkv[c];
+                if (s && s->pran < 0.) t = P1(func, k) * t;
+                fe[c] = t;
+                fh[c] = (s && s->anis_k) ? P1(fan, k) * t : t;
+                for (int q = 0; q < 6; q++) d[q][c] = 2. * d[q][c];
+            }
+    /* Flux(.,.,.,l,m): F[3*l+m], zero-initialised like the reference's alloc */
+    double *F[9];
+    for (int q = 0; q < 9; q++) F[q] = dalloc(nc);
+    double *d11 = d[0], *d22 = d[1], *d33 = d[2], *d12 = d[3], *d13 = d[4], *d23 = d[5];
+#define A(a, i, j, k) (a)[IX(g, i, j, k)]
+    for (int k = 1; k <= nz - 1; k++)
+        for (int j = 3; j <= ny - 2; j++)
+            for (int i = 3; i <= nx - 2; i++) {
+                A(F[0], i + 1, j, k) = A(fh, i, j, k) * A(d11, i, j, k);
+                A(F[1], i, j + 1, k) = 0.25 * (A(fh, i, j, k) * A(d12, i, j, k) + A(fh, i, j + 1, k) * A(d12, i, j + 1, k) +
+                                               A(fh, i - 1, j, k) * A(d12, i - 1, j, k) + A(fh, i - 1, j + 1, k) * A(d12, i - 1, j + 1, k));
+                A(F[2], i, j, k + 1) = 0.25 * (A(fe, i, j, k) * A(d13, i, j, k) + A(fe, i - 1, j, k) * A(d13, i - 1, j, k) +
+                                               A(fe, i - 1, j, k + 1) * A(d13, i - 1, j, k + 1) + A(fe, i, j, k + 1) * A(d13, i, j, k + 1));
+            }
+    for (int k = 1; k <= nz - 1; k++)
+        for (int j = 3; j <= ny - 2; j++)
+            for (int i = 3; i <= nx - 2; i++) {
+                A(F[3], i + 1, j, k) = 0.25 * (A(fh, i, j, k) * A(d12, i, j, k) + A(fh, i, j - 1, k) * A(d12, i, j - 1, k) +
+                                               A(fh, i + 1, j - 1, k) * A(d12, i + 1, j - 1, k) + A(fh, i + 1, j, k) * A(d12, i + 1, j, k));
+                A(F[4], i, j + 1, k) = A(fh, i, j, k) * A(d22, i, j, k);
+                A(F[5], i, j, k + 1) = 0.25 * (A(fe, i, j, k) * A(d23, i, j, k) + A(fe, i, j - 1, k) * A(d23, i, j - 1, k) +
+                                               A(fe, i, j - 1, k + 1) * A(d23, i, j - 1, k + 1) + A(fe, i, j, k + 1) * A(d23, i, j, k + 1));
+            }
+    for (int k = 2; k <= nz - 1; k++)
+        for (int j = 3; j <= ny - 2; j++)
+            for (int i = 3; i <= nx - 2; i++) {
+                A(F[6], i + 1, j, k) = 0.25 * (A(fh, i, j, k) * A(d13, i, j, k) + A(fh, i, j, k - 1) * A(d13, i, j, k - 1) +
+                                               A(fh, i + 1, j, k - 1) * A(d13, i + 1, j, k - 1) + A(fh, i + 1, j, k) * A(d13, i + 1, j, k));
+                A(F[7], i, j + 1, k) = 0.25 * (A(fh, i, j, k) * A(d23, i, j, k) + A(fh, i, j, k - 1) * A(d23, i, j, k - 1) +
+                                               A(fh, i, j + 1, k - 1) * A(d23, i, j + 1, k - 1) + A(fh, i, j + 1, k) * A(d23, i, j + 1, k));
+                A(F[8], i, j, k + 1) = A(fe, i, j, k) * A(d33, i, j, k);
+            }
+    for (int j = 3; j <= ny - 2; j++)
+        for (int i = 3; i <= nx - 2; i++) A(F[8], i, j, 2) = A(fe, i, j, 1) * A(d33, i, j, 1);
+    if (s && s->momsf > 0) {   /* surface momentum flux (:318-333) */
+        for (int j = 3; j <= ny - 2; j++)
+            for (int i = 3; i <= nx - 2; i++) {
+                double ua = 0.5 * (A(u, i + 1, j, 1) + A(u, i, j, 1)), va = 0.5 * (A(v, i, j + 1, 1) + A(v, i, j, 1));
+                double windm = ua * ua;
+                windm = windm + va * va;
+                windm = dmax2(s->min_w, sqrt(windm));
+                double mf = s->mflux ? s->mflux[(size_t)(j - 1) * nx + (i - 1)] : 0.;
+                A(F[2], i, j, 1) = mf * 0.5 * (A(u, i + 1, j, 1) + A(u, i, j, 1)) / windm;
+                A(F[5], i, j, 1) = mf * 0.5 * (A(v, i, j + 1, 1) + A(v, i, j, 1)) / windm;
+            }
+    }
+    for (int k = 1; k <= nz - 1; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) {
+                size_t c = IX(g, i, j, k);
+                double eh = (A(F[0], i + 1, j, k) - A(F[0], i, j, k)) * dx1;
+                eh = eh + (A(F[1], i, j + 1, k) - A(F[1], i, j, k)) * dy1;
+                double ev = (A(F[2], i, j, k + 1) - A(F[2], i, j, k)) * P1(g->dz1w, k);
+                su[c] = su[c] + eh + ev;
+                eh = (A(F[3], i + 1, j, k) - A(F[3], i, j, k)) * dx1;
+                eh = eh + (A(F[4], i, j + 1, k) - A(F[4], i, j, k)) * dy1;
+                ev = (A(F[5], i, j, k + 1) - A(F[5], i, j, k)) * P1(g->dz1w, k);
+                sv[c] = sv[c] + eh + ev;
+                if (k >= 2) {
+                    eh = (A(F[6], i + 1, j, k) - A(F[6], i, j, k)) * dx1;
+                    eh = eh + (A(F[7], i, j + 1, k) - A(F[7], i, j, k)) * dy1;
+                    ev = (A(F[8], i, j, k + 1) - A(F[8], i, j, k)) * P1(g->dz1, k);
+                    sw[c] = sw[c] + eh + ev;
+                }
+            }
+#undef A
+    for (int q = 0; q < 9; q++) free(F[q]);
+    for (int q = 0; q < 6; q++) free(d[q]);
+    free(fe); free(fh); free(prof);
+}
+
+/* eff0 / effs / eff (subgrid.f90:459-789), grad_quick (gradients.f90:62-187),
+ * CONSERVATIVE (no division by the density), diff_ord = 2 */
+void mo_eff(const mo_grid *g, int kind, const double *dens, const double *fkv, const double *x, double *ec)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    const mo_sgs *s = g->sgs;
+    const size_t nc = ncell(g);
+    const double dx1 = 1. / g->dx, dy1 = 1. / g->dy;
+    double *prof = dalloc((size_t)MO_SGS_NPROF * nz);
+    mo_sgs_profiles(g, prof);
+    const double *func = prof + 2 * nz, *fan = prof + 3 * nz;
+    const double pran = s ? s->pran : 0.4;
+    double *nut = dalloc(nc), *nuh = dalloc(nc), *xs = dalloc(nc);
+    double *gx = dalloc(nc), *gy = dalloc(nc), *gz = dalloc(nc);
+    for (int k = 1; k <= nz; k++)
+        for (size_t c = IX(g, 1, 1, k); c < IX(g, 1, 1, k) + (size_t)nx * ny; c++) {
+            nut[c] = pran < 0. ? dens[c] * fkv[c] * P1(func, k) / fabs(pran) : dens[c] * fkv[c] / fabs(pran);
+            nuh[c] = (s && s->anis_k) ? P1(fan, k) * nut[c] : nut[c];
+            double x0 = 0.;
+            if (kind == 1) x0 = P1(g->pt0, k);
+            else if (kind == 2) x0 = (s && s->qt0) ? P1(s->qt0, k) : P1(g->qv0, k);
+            xs[c] = (s && s->diff != 0.) ? x[c] - x0 : x[c];
+        }
+#define A(a, i, j, k) (a)[IX(g, i, j, k)]
+    for (int k = 1; k <= nz; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 3; i <= nx - 2; i++) A(gx, i + 1, j, k) = (A(xs, i + 1, j, k) - A(xs, i, j, k)) * dx1;
+    mo_statebc(g, gx);
+    for (int k = 1; k <= nz; k++)
+        for (int j = 3; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) A(gy, i, j + 1, k) = (A(xs, i, j + 1, k) - A(xs, i, j, k)) * dy1;
+    mo_statebc(g, gy);
+    for (int k = 1; k <= nz - 1; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) A(gz, i, j, k + 1) = (A(xs, i, j, k + 1) - A(xs, i, j, k)) * P1(g->dz1, k);
+    mo_statebc(g, gz);
+    /* fluxes, stored as in the reference at the lower index of each face */
+    double *fx = dalloc(nc), *fy = dalloc(nc), *fz = dalloc(nc);
+    for (int k = 1; k <= nz - 1; k++)
+        for (int j = 3; j <= ny - 2; j++)
+            for (int i = 3; i <= nx - 2; i++) {
+                A(fx, i, j, k) = 0.5 * (A(nuh, i + 1, j, k) + A(nuh, i, j, k)) * A(gx, i + 1, j, k);
+                A(fy, i, j, k) = 0.5 * (A(nuh, i, j + 1, k) + A(nuh, i, j, k)) * A(gy, i, j + 1, k);
+                A(fz, i, j, k) = 0.5 * (A(nut, i, j, k + 1) + A(nut, i, j, k)) * A(gz, i, j, k + 1);
+            }
+    const double *fs = kind == 1 ? (s ? s->esflux : NULL) : (kind == 2 ? (s ? s->qvflux : NULL) : NULL);
+    for (int k = 1; k <= nz - 1; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) {
+                double e = (A(fx, i, j, k) - A(fx, i - 1, j, k)) * dx1;
+                e = e + (A(fy, i, j, k) - A(fy, i, j - 1, k)) * dy1;
+                double ez;
+                if (k == 1) {
+                    double flux_s = fs ? -fs[(size_t)(j - 1) * nx + (i - 1)] : 0.;
+                    ez = (A(fz, i, j, 1) - flux_s) * P1(g->dz1w, 1);
+                } else {
+                    ez = (A(fz, i, j, k) - A(fz, i, j, k - 1)) * P1(g->dz1w, k);
+                }
+                A(ec, i, j, k) = e + ez;
+            }
+#undef A
+    free(nut); free(nuh); free(xs); free(gx); free(gy); free(gz); free(fx); free(fy); free(fz); free(prof);
+}
+
+/* ======================================================================
  * One integrator step: src/INTEG/time_step.f90 stepping :76-334 (dynamics subset:
- * with_dif, with_rad, with_mic, sponge, nudging off; w0 = 0), integrate_all
+ * with_rad, with_mic, sponge, nudging off; w0 = 0; with_dif from g->sgs), integrate_all
  * :337-444, integ_mom/integ_scal src/INTEG/integpack.f90:54-284 with
  * INCLUDE/integ.h, momentum src/INTEG/momentum.f90:64-228 (imp_buoy=.true.),
  * scalars src/INTEG/scalars.f90:61-230, tracers src/INTEG/tracers.f90:50-125,
@@ -1703,16 +2058,43 @@ int mo_step(const mo_grid *g, int ntime, double *u, double *v, double *w, double
     for (int s = 0; s < nsc; s++) wss[s] = dalloc(nc);
     double *pp = dalloc(nc), *gpx = dalloc(nc), *gpy = dalloc(nc), *gpz = dalloc(nc), *buoy = dalloc(nc);
     double *estmp = dalloc(nc), *qttmp = dalloc(nc);
+    /* SGS tendencies (subgrid_interface before the dynamics loop, efud/eff0/effs in both
+     * stages): all read the level-n natural state (wind2, state2, pressure2%dens), which
+     * update_prognostic refreshes only after the loop, so they are equal in both stages */
+    const mo_sgs *sg = sgs_of(g);
+    double *sgu = NULL, *sgv = NULL, *sgw = NULL, **sgsc = NULL;
+    if (sg) {
+        double *fkv = dalloc(nc);
+        mo_calc_subgrid(g, u2, v2, w2, s2[0], iqt >= 0 ? s2[iqt] : NULL, fkv);
+        sgu = dalloc(nc); sgv = dalloc(nc); sgw = dalloc(nc);
+        mo_efud(g, u2, v2, w2, dens2, fkv, sgu, sgv, sgw);
+        sgsc = (double **)calloc(nsc ? nsc : 1, sizeof(double *));
+        for (int s = 0; s < nsc; s++) {
+            sgsc[s] = dalloc(nc);
+            mo_eff(g, s == 0 ? 1 : (s == iqt ? 2 : 3), dens2, fkv, s2[s], sgsc[s]);
+        }
+        free(fkv);
+    }
 
     for (int im = 1; im <= 2; im++) {
         double a_lm = im == 1 ? 1. : 0.5, b_lm = im == 1 ? 0. : 1.;
         memcpy(windold, mw, nc * 8);
         memset(wsu, 0, nc * 8); memset(wsv, 0, nc * 8); memset(wsw, 0, nc * 8); memset(wsd, 0, nc * 8);
         for (int s = 0; s < nsc; s++) memset(wss[s], 0, nc * 8);
+        if (sg) {   /* efud: winds = (winds + eh) + ev; effs: states%scal = states%scal + ec */
+            for (size_t c = 0; c < nc; c++) { wsu[c] = sgu[c]; wsv[c] = sgv[c]; wsw[c] = sgw[c]; }
+            for (int s = 0; s < nsc; s++)
+                if (s != 0 && s != iqt)
+                    for (size_t c = 0; c < nc; c++) wss[s][c] = 0. + sgsc[s][c];
+        }
         mo_get_advective(g, mu, mv, mw, ua, va, wa);
         /* scalars: density first (adv=.false.), then es, qt; tracers with advection_ac */
         mo_advection_ac(g, dens, ua, va, wa, wsd, 0);
         for (int s = 0; s < nsc; s++) mo_advection_ac(g, scal[s], ua, va, wa, wss[s], 0);
+        if (sg)   /* scalars.f90:146-150: states%es = statea%es + states%es (eff0 result) */
+            for (int s = 0; s < nsc; s++)
+                if (s == 0 || s == iqt)
+                    for (size_t c = 0; c < nc; c++) wss[s][c] = wss[s][c] + sgsc[s][c];
         /* momentum */
         for (int k = 1; k <= nz; k++)
             for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) pp[c] = p[c] / P1(g->den0, k);
@@ -1787,5 +2169,10 @@ int mo_step(const mo_grid *g, int ntime, double *u, double *v, double *w, double
     free(windold); free(ua); free(va); free(wa); free(au); free(av); free(aw);
     free(wsu); free(wsv); free(wsw); free(wsd);
     free(pp); free(gpx); free(gpy); free(gpz); free(buoy); free(estmp); free(qttmp);
+    if (sg) {
+        free(sgu); free(sgv); free(sgw);
+        for (int s = 0; s < nsc; s++) free(sgsc[s]);
+        free(sgsc);
+    }
     return err;
 }

@@ -30,6 +30,20 @@ extern "C" {
 enum { MO_WENO = 0, MO_PPM = 1, MO_MUSCL = 2, MO_LW = 3, MO_QUICK = 4 };
 enum { MO_LIM_MINMOD = 0, MO_LIM_VL = 1, MO_LIM_MC = 2, MO_LIM_DEFAULT = 3 };
 
+/* SGS turbulence switches (src/TYPES/shared_data.f90, INCLUDE/default.h), the
+ * Smagorinsky-Lilly build (TKE undefined), nl_sgs=.false., diff_ord=2, lmicro=0. */
+typedef struct mo_sgs {
+    int with_dif;                /* with_dif */
+    int anis_k;                  /* anis_k */
+    int momsf;                   /* momsf > 0: surface momentum flux from mflux */
+    int pad;
+    double diff;                 /* 0: Smagorinsky-Lilly; otherwise constant viscosity |diff| */
+    double pran;                 /* Prandtl number; < 0: viscosity damped above zdec */
+    double zdec, zrough, min_w;
+    const double *qt0;           /* diff != 0: base-state qt profile (nz), NULL = qv0 */
+    const double *esflux, *qvflux, *mflux;   /* surface fluxes (nx*ny) or NULL = 0 */
+} mo_sgs;
+
 typedef struct mo_grid {
     int nx, ny, nz;              /* full sizes incl. ghost cells */
     int scal_adv;                /* MO_WENO / MO_PPM / MO_MUSCL / MO_LW / MO_QUICK */
@@ -46,6 +60,7 @@ typedef struct mo_grid {
     const double *den0, *avden0, *stab0, *pt0, *qv0;
     /* horizontal eigenvalues wv(1:nx-5, 1:ny-5), l fastest */
     const double *wv;
+    const mo_sgs *sgs;           /* SGS diffusion, or NULL (with_dif = .false.) */
 } mo_grid;
 
 /* ---- host precompute (define_grid, initial, get_wv) ---- */
@@ -91,6 +106,24 @@ void mo_rescale_pressure(const mo_grid *g, double *pp);
 void mo_horav(const mo_grid *g, const double *x, double *xav);
 int  mo_anelastic_pressure(const mo_grid *g, double *mu, double *mv, double *mw, double *p,
                            const double *wold, double *maxdiv, double *p1);
+
+/* ---- SGS turbulence (src/PHYS/subgrid.f90, src/TOOLS/gradients.f90) ----
+ * Per-level profiles, prof[q*nz + k-1] for q = 0..MO_SGS_NPROF-1:
+ * 0 z0, 1 (C_s*delta)**2, 2 damping func, 3 anisotropy f_an, 4 N2 coefficient,
+ * 5 N2 denominator, 6..8 denominators of the 4th-order d/dz of u, v, w. */
+#define MO_SGS_NPROF 10
+void mo_sgs_profiles(const mo_grid *g, double *prof);
+/* cal_dij: d[0..5] = d11, d22, d33, d12, d13, d23 (cell centred, full arrays) */
+void mo_cal_dij(const mo_grid *g, const double *u, const double *v, const double *w, double *const *d);
+/* calc_subgrid: turbu%fkv from natural level-n winds, es (theta) and qt (NULL = dry) */
+void mo_calc_subgrid(const mo_grid *g, const double *u, const double *v, const double *w,
+                     const double *es, const double *qt, double *fkv);
+/* efud: su/sv/sw := (s + eh) + ev on the interior (the reference's winds%u etc.) */
+void mo_efud(const mo_grid *g, const double *u, const double *v, const double *w, const double *dens,
+             const double *fkv, double *su, double *sv, double *sw);
+/* eff: kind 1 = es (flux -esflux, x0 = pt0), 2 = qt (-qvflux, qt0), 3 = tracer (effs: 0, 0);
+ * ec := SGS tendency on the interior levels 1..nz-1 (conservative form) */
+void mo_eff(const mo_grid *g, int kind, const double *dens, const double *fkv, const double *x, double *ec);
 
 /* ---- one full integrator step (time_step.f90 stepping, dynamics subset) ----
  * State at time level n, natural variables, all arrays nx*ny*nz with valid halos:

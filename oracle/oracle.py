@@ -23,6 +23,17 @@ WENO, PPM, MUSCL, LW, QUICK = 0, 1, 2, 3, 4
 LIM = {"minmod": 0, "VL": 1, "MC": 2, "default": 3}
 
 
+class MoSgs(C.Structure):
+    _fields_ = [
+        ("with_dif", C.c_int), ("anis_k", C.c_int), ("momsf", C.c_int), ("pad", C.c_int),
+        ("diff", C.c_double), ("pran", C.c_double), ("zdec", C.c_double), ("zrough", C.c_double),
+        ("min_w", C.c_double), ("qt0", _dp), ("esflux", _dp), ("qvflux", _dp), ("mflux", _dp),
+    ]
+
+
+SGS_NPROF = 10
+
+
 class MoGrid(C.Structure):
     _fields_ = [
         ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
@@ -31,7 +42,7 @@ class MoGrid(C.Structure):
         ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double), ("dt0", C.c_double),
         ("lim_tol", C.c_double), ("u0shift", C.c_double), ("v0shift", C.c_double),
         ("fdz0", _dp), ("dzw", _dp), ("dz1w", _dp), ("dz1", _dp), ("den0", _dp), ("avden0", _dp),
-        ("stab0", _dp), ("pt0", _dp), ("qv0", _dp), ("wv", _dp),
+        ("stab0", _dp), ("pt0", _dp), ("qv0", _dp), ("wv", _dp), ("sgs", C.POINTER(MoSgs)),
     ]
 
 
@@ -70,6 +81,11 @@ def load(omp: bool = False) -> C.CDLL:
         L.mo_grid_metrics.argtypes = [C.c_int, C.c_double, _dp, _dp, _dp, _dp]
         L.mo_base_state.argtypes = [C.c_int, C.c_double, C.c_double, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         L.mo_get_wv.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _dp]
+        L.mo_sgs_profiles.argtypes = [g, _dp]
+        L.mo_cal_dij.argtypes = [g, _dp, _dp, _dp, C.POINTER(_dp)]
+        L.mo_calc_subgrid.argtypes = [g, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.mo_efud.argtypes = [g] + [_dp] * 8
+        L.mo_eff.argtypes = [g, C.c_int, _dp, _dp, _dp, _dp]
         _libs[name] = L
     return _libs[name]
 
@@ -100,6 +116,19 @@ class Oracle:
         g.lim_tol, g.u0shift, g.v0shift = d.lim_tol, d.u0shift, d.v0shift
         (g.fdz0, g.dzw, g.dz1w, g.dz1, g.den0, g.avden0, g.stab0, g.pt0, g.qv0) = [P(a) for a in self._keep]
         g.wv = P(self.wv)
+        sg = getattr(d, "sgs", None)
+        if sg is not None:
+            ms = MoSgs()
+            ms.with_dif, ms.anis_k, ms.momsf, ms.pad = 1, int(sg.anis_k), int(sg.momsf), 0
+            ms.diff, ms.pran, ms.zdec, ms.zrough, ms.min_w = sg.diff, sg.pran, sg.zdec, sg.zrough, sg.min_w
+            for name in ("qt0", "esflux", "qvflux", "mflux"):
+                a = getattr(sg, name)
+                if a is not None:
+                    a = np.ascontiguousarray(a, dtype=np.float64)
+                    self._keep.append(a)
+                    setattr(ms, name, P(a))
+            self._sgs = ms
+            g.sgs = C.pointer(ms)
         self.g = g
         self.gp = C.byref(g)
 
@@ -108,6 +137,36 @@ class Oracle:
         xs = np.array(xs, dtype=np.float64, copy=True)
         self.L.mo_advection_ac(self.gp, P(np.ascontiguousarray(x)), P(ua), P(va), P(wa), P(xs), 0)
         return xs
+
+    # ---- SGS turbulence (subgrid.f90) ----
+    def sgs_profiles(self) -> np.ndarray:
+        prof = np.zeros(SGS_NPROF * self.d.nz)
+        self.L.mo_sgs_profiles(self.gp, P(prof))
+        return prof
+
+    def cal_dij(self, u, v, w):
+        d = [np.zeros(self.d.shape) for _ in range(6)]
+        arr = (_dp * 6)(*[P(a) for a in d])
+        self.L.mo_cal_dij(self.gp, *[P(np.ascontiguousarray(a)) for a in (u, v, w)], arr)
+        return d
+
+    def calc_subgrid(self, u, v, w, es, qt=None):
+        fkv = np.zeros(self.d.shape)
+        c = [None if a is None else np.ascontiguousarray(a) for a in (u, v, w, es, qt)]
+        self.L.mo_calc_subgrid(self.gp, *[P(a) for a in c], P(fkv))
+        return fkv
+
+    def efud(self, u, v, w, dens, fkv, su=None, sv=None, sw=None):
+        outs = [np.zeros(self.d.shape) if a is None else np.array(a, dtype=np.float64, copy=True) for a in (su, sv, sw)]
+        c = [np.ascontiguousarray(a) for a in (u, v, w, dens, fkv)]
+        self.L.mo_efud(self.gp, *[P(a) for a in c], *[P(a) for a in outs])
+        return tuple(outs)
+
+    def eff(self, kind, dens, fkv, x, ec=None):
+        out = np.zeros(self.d.shape) if ec is None else np.array(ec, dtype=np.float64, copy=True)
+        c = [np.ascontiguousarray(a) for a in (dens, fkv, x)]
+        self.L.mo_eff(self.gp, kind, *[P(a) for a in c], P(out))
+        return out
 
     def get_advective(self, mu, mv, mw):
         ua, va, wa = (np.zeros(self.d.shape) for _ in range(3))
