@@ -55,7 +55,7 @@ def peaks():
 
 
 # ---------------- algorithmic bytes (FP64 state), per interior cell ----------------
-def alg_bytes(nf_scalar: int, nsubp: int) -> dict:
+def alg_bytes(nf_scalar: int, nsubp: int, sgs: bool = False) -> dict:
     """Minimal HBM traffic per interior cell of each kernel group (bytes).
 
     K1 (all scalar fields incl. density), per launch averaged over the two stages:
@@ -72,9 +72,25 @@ def alg_bytes(nf_scalar: int, nsubp: int) -> dict:
     k1 = (f * 24 + 24 + 16 + f * 32 + 24 + 16) / 2.0
     k2 = ((24 + 8 + 40 + 48) + (72 + 8 + 40 + 24)) / 2.0
     proj = 32 + 64 + 72
+    out = {"k1_scalar_advection": k1, "k2_momentum": k2, "fft_x_fwd_div": 32.0,
+           "fft_y_tridiag_fft_y_fft_x_inv": 64.0, "correction_halo": 72.0}
     step = 2 * (k1 + k2) + 2 * nsubp * proj
-    return {"k1_scalar_advection": k1, "k2_momentum": k2, "fft_x_fwd_div": 32.0,
-            "fft_y_tridiag_fft_y_fft_x_inv": 64.0, "correction_halo": 72.0, "step": step}
+    if sgs:
+        # SGS diffusion, once per step: the viscosity kernel reads u, v, w, es, qt, dens and
+        # writes the six deformation components, dens*fkv and the diffusivity; the momentum
+        # stresses read dens*fkv and dij and write 3 tendencies; the scalar fluxes read the
+        # diffusivity and f-1 scalars and write f-1 tendencies.  K1 and K2 read the stored
+        # tendencies in both stages (f-1 and 3 fields).
+        s = f - 1
+        out["sgs_viscosity"] = 48.0 + 64.0
+        out["sgs_momentum"] = 56.0 + 24.0
+        out["sgs_scalars"] = 8.0 + 16.0 * s
+        k1 += 8.0 * s
+        k2 += 24.0
+        out["k1_scalar_advection"], out["k2_momentum"] = k1, k2
+        step = 2 * (k1 + k2) + 2 * nsubp * proj + out["sgs_viscosity"] + out["sgs_momentum"] + out["sgs_scalars"]
+    out["step"] = step
+    return out
 
 
 class ClockSampler:
@@ -181,6 +197,22 @@ def dist_barrier(ws):
         dist.barrier()
 
 
+def bench_sgs(args, d):
+    """SGS settings of the --sgs option (the BOMEX template's pran, zdec, momsf; uniform
+    surface fluxes of its prescribed magnitude: 8.4 W/m2 sensible, 153 W/m2 latent heat,
+    u* = 0.28 m/s)."""
+    if args.sgs == "none":
+        return None
+    from fdd3260_b200 import config
+    one = np.ones((d.ny, d.nx))
+    return config.Sgs(pran=-0.4, zdec=2400.0, momsf=1, zrough=1.0, min_w=0.1,
+                      esflux=7.0e-3 * one, qvflux=5.2e-5 * one, mflux=-(0.28 ** 2) * one)
+
+
+def sgs_label(args):
+    return {"none": "off", "smagorinsky": "Smagorinsky-Lilly, pran=-0.4, zdec=2400 m, surface fluxes"}[args.sgs]
+
+
 def cpu_reference(args, d_full, scheme, nsamp_steps=1, omp=True):
     """The reference's algorithm timed on the host cores: the CPU restatement, bounded
     sample = a horizontally reduced domain with the same dz profile, spacing and fields."""
@@ -188,6 +220,7 @@ def cpu_reference(args, d_full, scheme, nsamp_steps=1, omp=True):
     from oracle import oracle as O
     mx = args.cpu_sample_xy
     d = config.cumulus_domain(mx, mx, d_full.nz, scheme=scheme)
+    d.sgs = bench_sgs(args, d)
     st = config.cumulus_state(d, seed=1000, n_extra=3)
     orc = O.Oracle(d, omp=omp)
     orc.stepping(st, nsteps=1, ntime0=1)   # warm-up (page faults, OpenMP pool)
@@ -219,6 +252,9 @@ def main():
     ap.add_argument("--workload", default="cumulus", choices=["cumulus", "ensemble"],
                     help="cumulus: the 512x512x256 shallow-cumulus domain (default); ensemble: 64 independent "
                          "warm-bubble domains of seeded uneven sizes, batched per GPU, sharded over ranks")
+    ap.add_argument("--sgs", default="none", choices=["none", "smagorinsky"],
+                    help="smagorinsky: SGS turbulence diffusion on (Smagorinsky-Lilly, pran=-0.4, zdec=2400 m, "
+                         "surface heat, moisture and momentum fluxes), as the BOMEX template runs it")
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--err-steps", type=int, default=10,
                     help="steps of the accuracy leg (mixed vs FP64 fields from the same initial state)")
@@ -231,6 +267,7 @@ def main():
         return run_ensemble(args, ws, rank, local)
     from fdd3260_b200 import Mimica, config
     d = config.cumulus_domain(args.maxx, args.maxx, args.nz, scheme=args.scheme)
+    d.sgs = bench_sgs(args, d)
     from fdd3260_b200 import _lib
     metric = "Mcell-updates/s per integrator step (2-stage Heun + projection)"
     cfg = {"workload": f"shallow-cumulus domain {args.maxx}x{args.maxx}x{args.nz}, dx=dy=25 m, stretched dz 10->100 m, "
@@ -240,7 +277,7 @@ def main():
                      "seeded Gaussian perturbations below 500 m; u=-8+N(0,0.5), v=N(0,0.5) m/s",
            "form": {"both": "plain FP64 (headline) + mixed", "fp64": "plain FP64",
                     "mixed": "mixed (FP32 stencils, fluxes and spectra; FP64 state)"}[args.form],
-           "scheme": args.scheme, "interior_cells": d.cells,
+           "scheme": args.scheme, "sgs": sgs_label(args), "interior_cells": d.cells,
            "l2": "inputs larger than L2 (~16 GB working set)", "parallelism": f"replicas x{ws}"}
 
     if args.impl == "reference":
@@ -497,7 +534,7 @@ def time_form(args, m, d, st, use_graph, ws, local) -> dict:
     for ln in buf.value.decode().splitlines():
         name, n, tot = ln.split()
         kern[name] = {"launches": int(n), "total_ms": float(tot)}
-    ab = alg_bytes(1 + len(st.scal), d.nsubp)
+    ab = alg_bytes(1 + len(st.scal), d.nsubp, d.sgs is not None)
     pk, pk_src = peaks()
     dom = max((k for k in kern if k in ab), key=lambda k: kern[k]["total_ms"])
     avg_ms = kern[dom]["total_ms"] / kern[dom]["launches"]

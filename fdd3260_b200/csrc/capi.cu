@@ -53,7 +53,7 @@ struct mg_ctx {
     std::vector<double> sgs_qt0;
     int sgs_on = 0;
     double *sgs_prof = nullptr;          // SGS_NPROF*nz factors, then qt0 (nz)
-    double *dij[6] = {}, *fkv = nullptr, *sgm[3] = {}, *sgsc[MG_MAXF] = {};
+    double *dij[6] = {}, *fkv = nullptr, *sfe = nullptr, *snut = nullptr, *sgm[3] = {}, *sgsc[MG_MAXF] = {};
     double *sfc[3] = {};                 // esflux, qvflux, mflux (nx*ny), zero until set
     // per-kernel profiling (CUDA events on the context stream)
     int prof_on = 0;
@@ -240,7 +240,7 @@ static void free_ctx(mg_ctx *c)
     for (int i = 0; i < 3; i++) { cudaFree(c->mA[i]); cudaFree(c->mB[i]); cudaFree(c->tm[i]); }
     for (int f = 0; f < MG_MAXF; f++) { cudaFree(c->sA[f]); cudaFree(c->sB[f]); cudaFree(c->ts[f]); }
     for (int i = 0; i < 16; i++) cudaFree(c->unit[i]);
-    cudaFree(c->sgs_prof); cudaFree(c->fkv);
+    cudaFree(c->sgs_prof); cudaFree(c->fkv); cudaFree(c->sfe); cudaFree(c->snut);
     for (int q = 0; q < 6; q++) cudaFree(c->dij[q]);
     for (int q = 0; q < 3; q++) { cudaFree(c->sgm[q]); cudaFree(c->sfc[q]); }
     for (int f = 0; f < MG_MAXF; f++) cudaFree(c->sgsc[f]);
@@ -506,6 +506,8 @@ static int ensure_sgs(mg_ctx *c)
     int rc = field(&c->sgs_prof, (size_t)(SGS_NPROF + 1) * nz * sizeof(double));
     for (int q = 0; q < 6 && !rc; q++) rc = field(&c->dij[q], c->fbytes);
     if (!rc) rc = field(&c->fkv, c->fbytes);
+    if (!rc) rc = field(&c->sfe, c->fbytes);
+    if (!rc) rc = field(&c->snut, c->fbytes);
     for (int q = 0; q < 3 && !rc; q++) rc = field(&c->sgm[q], c->fbytes);
     for (int q = 0; q < 3 && !rc; q++) rc = field(&c->sfc[q], (size_t)G.nx * G.ny * sizeof(double));
     if (rc) return rc;
@@ -525,12 +527,13 @@ static cudaError_t sgs_tendencies(mg_ctx *c, int *launches)
     const SgsDev S = sgs_dev(c);
     SgsDij D{};
     for (int q = 0; q < 6; q++) D.d[q] = c->dij[q];
+    const SgsVisc O{nullptr, c->sfe, c->snut};
     PROF(c, "sgs_viscosity", launch_sgs_visc(G, S, c->mA[0], c->mA[1], c->mA[2], c->sA[ies], iqt >= 0 ? c->sA[iqt] : nullptr,
-                                             D, c->fkv, c->stream));
-    double *hf[7] = {c->dij[0], c->dij[1], c->dij[2], c->dij[3], c->dij[4], c->dij[5], c->fkv};
-    PROF(c, "sgs_halo", launch_halo_fill(G, hf, 7, c->stream));
-    PROF(c, "sgs_momentum", launch_sgs_mom(G, S, c->mA[0], c->mA[1], c->sA[0], c->fkv, D, c->sfc[2], nullptr, nullptr,
-                                           nullptr, c->sgm[0], c->sgm[1], c->sgm[2], c->stream));
+                                             c->sA[0], D, O, c->stream));
+    double *hf[8] = {c->dij[0], c->dij[1], c->dij[2], c->dij[3], c->dij[4], c->dij[5], c->sfe, c->snut};
+    PROF(c, "sgs_halo", launch_halo_fill(G, hf, 8, c->stream));
+    PROF(c, "sgs_momentum", launch_sgs_mom(G, S, c->mA[0], c->mA[1], c->sfe, D, c->sfc[2], nullptr, nullptr, nullptr,
+                                           c->sgm[0], c->sgm[1], c->sgm[2], c->stream));
     SgsScal A{};
     A.nf = c->nf - 1;
     for (int f = 1; f < c->nf; f++) {
@@ -541,7 +544,7 @@ static cudaError_t sgs_tendencies(mg_ctx *c, int *launches)
         A.fs[q] = f == ies ? c->sfc[0] : (f == iqt ? c->sfc[1] : nullptr);
         A.fs_neg[q] = 1;
     }
-    if (A.nf > 0) PROF(c, "sgs_scalars", launch_sgs_scal(G, S, c->sA[0], c->fkv, A, c->stream));
+    if (A.nf > 0) PROF(c, "sgs_scalars", launch_sgs_scal(G, S, c->snut, A, c->stream));
     *launches += A.nf > 0 ? 4 : 3;
     return cudaSuccess;
 }
@@ -946,8 +949,9 @@ extern "C" int mg_calc_subgrid(mg_ctx *c, const double *u, const double *v, cons
         if (in[q]) CKR(h2d(c, c->unit[q], in[q], cudaMemcpyHostToDevice));
     SgsDij D{};
     for (int q = 0; q < 6; q++) D.d[q] = c->dij[q];
-    CKR(launch_sgs_visc(c->G, sgs_dev(c), c->unit[0], c->unit[1], c->unit[2], c->unit[3], qt ? c->unit[4] : nullptr, D,
-                        c->fkv, c->stream));
+    const SgsVisc O{c->fkv, nullptr, nullptr};
+    CKR(launch_sgs_visc(c->G, sgs_dev(c), c->unit[0], c->unit[1], c->unit[2], c->unit[3], qt ? c->unit[4] : nullptr,
+                        nullptr, D, O, c->stream));
     double *hf[1] = {c->fkv};
     CKR(launch_halo_fill(c->G, hf, 1, c->stream));
     CKR(d2h(c, fkv, c->fkv, cudaMemcpyDeviceToHost));
@@ -968,10 +972,11 @@ extern "C" int mg_efud(mg_ctx *c, const double *u, const double *v, const double
     SgsDij D{};
     for (int q = 0; q < 6; q++) D.d[q] = c->dij[q];
     const SgsDev S = sgs_dev(c);
-    CKR(launch_sgs_visc(c->G, S, c->unit[0], c->unit[1], c->unit[2], nullptr, nullptr, D, nullptr, c->stream));
+    CKR(launch_sgs_visc(c->G, S, c->unit[0], c->unit[1], c->unit[2], nullptr, nullptr, nullptr, D, SgsVisc{}, c->stream));
     CKR(launch_halo_fill(c->G, D.d, 6, c->stream));
-    CKR(launch_sgs_mom(c->G, S, c->unit[0], c->unit[1], c->unit[3], c->unit[4], D, c->sfc[2], c->unit[5], c->unit[6],
-                       c->unit[7], c->unit[5], c->unit[6], c->unit[7], c->stream));
+    CKR(launch_sgs_prep(c->G, S, c->unit[3], c->unit[4], c->sfe, c->snut, c->stream));
+    CKR(launch_sgs_mom(c->G, S, c->unit[0], c->unit[1], c->sfe, D, c->sfc[2], c->unit[5], c->unit[6], c->unit[7],
+                       c->unit[5], c->unit[6], c->unit[7], c->stream));
     CKR(d2h(c, su, c->unit[5], cudaMemcpyDeviceToHost));
     CKR(d2h(c, sv, c->unit[6], cudaMemcpyDeviceToHost));
     CKR(d2h(c, sw, c->unit[7], cudaMemcpyDeviceToHost));
@@ -1001,7 +1006,9 @@ extern "C" int mg_eff(mg_ctx *c, int kind, const double *dens, const double *fkv
     A.x0[0] = kind == 1 ? c->G.pt0 : (kind == 2 ? sgs_qt0_dev(c) : nullptr);
     A.fs[0] = flux_s ? c->unit[4] : nullptr;
     A.fs_neg[0] = 0;
-    CKR(launch_sgs_scal(c->G, sgs_dev(c), c->unit[0], c->unit[1], A, c->stream));
+    const SgsDev S = sgs_dev(c);
+    CKR(launch_sgs_prep(c->G, S, c->unit[0], c->unit[1], c->sfe, c->snut, c->stream));
+    CKR(launch_sgs_scal(c->G, S, c->snut, A, c->stream));
     CKR(d2h(c, ec, c->unit[3], cudaMemcpyDeviceToHost));
     return cuerr(cudaStreamSynchronize(c->stream));
 }

@@ -86,7 +86,9 @@ __device__ __forceinline__ int halo_elem(int h)
 
 // STAGE 1, 2: Heun stage update of density + density-weighted scalars (field 0 is the
 // density); STAGE 0: unit mode (advection_ac of one field, xout := ((xout-Tx)-Ty)-Tz)
-template <int SCHEME, bool MIXED, int STAGE>
+// SGS: the stage adds stored SGS tendencies (A.sgs), loaded one group ahead; a variant of
+// its own so that the kernels without SGS keep their register budget
+template <int SCHEME, bool MIXED, int STAGE, bool SGS>
 __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __grid_constant__ K1Maps M)
 {
     constexpr int PF = k1_pf(SCHEME), NPS = k1_nps(SCHEME), NFB = k1_nfb(SCHEME);
@@ -185,14 +187,17 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
     // stage 2: level-n value and tendency of the group's fields, loaded one group ahead
     const long long idx0 = gidx(G, ic, jc, 1);
     double nx_xold[PF], nx_tend[PF];
+    double nx_sgs[PF];   // SGS tendencies (both stages), loaded one group ahead as well
 #pragma unroll
     for (int u = 0; u < PF; u++) {
         nx_xold[u] = 0.;
         nx_tend[u] = 0.;
+        nx_sgs[u] = 0.;
         if (STAGE == 2 && act && u < F) {
             nx_xold[u] = ldg(A.xold[u], idx0);
             nx_tend[u] = ldg(A.tend[u], idx0);
         }
+        if (SGS && act && u < F && A.sgs[u]) nx_sgs[u] = ldg(A.sgs[u], idx0);
     }
     for (int k = 1; k <= nz; k++) {
         k_cur = k;
@@ -222,20 +227,24 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
             const int qg = (k - 1) * NG + g, gb = g * PF;
             // this group's stage-2 operands, then the next group's loads (they complete
             // while this group's faces are computed)
-            double cur_xold[PF], cur_tend[PF];
+            double cur_xold[PF], cur_tend[PF], cur_sgs[PF];
 #pragma unroll
             for (int u = 0; u < PF; u++) {
                 cur_xold[u] = nx_xold[u];
                 cur_tend[u] = nx_tend[u];
+                cur_sgs[u] = nx_sgs[u];
             }
-            if (STAGE == 2 && act && qg + 1 < total_groups) {
+            if ((STAGE == 2 || SGS) && act && qg + 1 < total_groups) {
                 const int gn = g + 1 < NG ? g + 1 : 0, kn = g + 1 < NG ? k : k + 1;
                 const long long idn = idx0 + (long long)(kn - 1) * G.ps;
 #pragma unroll
                 for (int u = 0; u < PF; u++)
                     if (gn * PF + u < F) {
-                        nx_xold[u] = ldg(A.xold[gn * PF + u], idn);
-                        nx_tend[u] = ldg(A.tend[gn * PF + u], idn);
+                        if (STAGE == 2) {
+                            nx_xold[u] = ldg(A.xold[gn * PF + u], idn);
+                            nx_tend[u] = ldg(A.tend[gn * PF + u], idn);
+                        }
+                        if (SGS) nx_sgs[u] = A.sgs[gn * PF + u] ? ldg(A.sgs[gn * PF + u], idn) : 0.;
                     }
             }
             // slot (qg+NPS-1)%NPS last held group qg-1, whose faces all threads finished
@@ -574,11 +583,15 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
                         double *xs = A.xout[f];
                         xs[idx] = ((xs[idx] - Tx) - Ty) - Tz;
                     } else {
-                        const double *sgp = A.sgs[f];
-                        const bool spost = (A.sgs_post >> f) & 1u;
-                        const double sgv = sgp ? sgp[idx] : 0.;
-                        double T = (((sgp && !spost ? 0. + sgv : 0.) - Tx) - Ty) - Tz;
-                        if (sgp && spost) T = T + sgv;
+                        double T;
+                        if constexpr (SGS) {
+                            const bool has = A.sgs[f] != nullptr, spost = (A.sgs_post >> f) & 1u;
+                            const double sgv = cur_sgs[u];
+                            T = (((has && !spost ? 0. + sgv : 0.) - Tx) - Ty) - Tz;
+                            if (has && spost) T = T + sgv;
+                        } else {
+                            T = ((0. - Tx) - Ty) - Tz;
+                        }
                         const double told = STAGE == 1 ? 0. : cur_tend[u];
                         const double tn = T + A.b * told;
                         const bool weighted = f > 0;

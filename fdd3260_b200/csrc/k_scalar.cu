@@ -10,7 +10,12 @@ template <int SCHEME, int STAGE>
 cudaError_t launch_one(const DevGrid &g, const K1Args &a, const K1Maps &maps, size_t sm, cudaStream_t s)
 {
     const int ntx = (g.maxx + TX - 1) / TX, nty = (g.maxy + TY - 1) / TY;
-    k1_kernel<SCHEME, false, STAGE><<<dim3(ntx * nty), dim3(TX, TY + 1), sm, s>>>(g, a, maps);
+    bool sgs = false;
+    for (int f = 0; f < a.nf; f++) sgs = sgs || a.sgs[f] != nullptr;
+    if (STAGE != 0 && sgs)
+        k1_kernel<SCHEME, false, STAGE, true><<<dim3(ntx * nty), dim3(TX, TY + 1), sm, s>>>(g, a, maps);
+    else
+        k1_kernel<SCHEME, false, STAGE, false><<<dim3(ntx * nty), dim3(TX, TY + 1), sm, s>>>(g, a, maps);
     return cudaGetLastError();
 }
 template <int SCHEME>
@@ -24,9 +29,12 @@ template <int SCHEME>
 cudaError_t init_scheme()
 {
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k1_kernel<SCHEME, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k1_kernel<SCHEME, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448)) != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k1_kernel<SCHEME, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+    const int mx = 232448;
+    if ((e = cudaFuncSetAttribute(k1_kernel<SCHEME, false, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k1_kernel<SCHEME, false, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k1_kernel<SCHEME, false, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k1_kernel<SCHEME, false, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k1_kernel<SCHEME, false, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
 }
 }  // namespace
 

@@ -82,13 +82,29 @@ struct Grad {
     }
 };
 
+// turbu%fkv of a cell and the two density-weighted forms the flux kernels use:
+// fe = dens*fkv, times func(k) when pran < 0 (efud, subgrid.f90:228-239), and
+// nut = fe/|pran| (eff0/effs, :489-497: ((dens*fkv)*func)/|pran| = fe/|pran|, the
+// product being commutative)
+__device__ __forceinline__ void sgs_store_visc(const SgsDev &S, const SgsVisc &O, long long c, int k, double fk,
+                                               const double *dens)
+{
+    if (O.fkv) O.fkv[c] = fk;
+    if (O.fe) {
+        const double t0 = ld(dens, c) * fk;
+        const double t = S.pran < 0. ? ld(S.func, k - 1) * t0 : t0;
+        O.fe[c] = t;
+        O.nut[c] = t / fabs(S.pran);
+    }
+}
+
 // calc_subgrid for one interior cell: cal_dij (gradients.f90:476-600), stability
 // (subgrid.f90:909-1001, dry branch, ISENTROPIC: ptv = es (1 + epsm qt)) and
 // calc_smago (:793-866, 'Lilly').  Writes d11, d22, d33, d12, d13, d23 and fkv.
 __global__ void __launch_bounds__(256) sgs_visc_kernel(DevGrid G, SgsDev S, const double *__restrict__ u,
                                                        const double *__restrict__ v, const double *__restrict__ w,
                                                        const double *__restrict__ es, const double *__restrict__ qt,
-                                                       SgsDij D, double *__restrict__ fkv)
+                                                       const double *__restrict__ dens, SgsDij D, SgsVisc O)
 {
     const int i = 4 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 4 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -111,9 +127,9 @@ __global__ void __launch_bounds__(256) sgs_visc_kernel(DevGrid G, SgsDev S, cons
     }
     D.d[0][c] = d11; D.d[1][c] = d22; D.d[2][c] = d33;
     D.d[3][c] = d12; D.d[4][c] = d13; D.d[5][c] = d23;
-    if (!fkv) return;  // deformation only (unit entry of efud)
-    if (S.diff_on) {   // fixed diffusion coefficient (subgrid.f90:131-133)
-        fkv[c] = fabs(S.diff);
+    if (!O.fkv && !O.fe) return;   // deformation only (unit entry of efud)
+    if (S.diff_on) {               // fixed diffusion coefficient (subgrid.f90:131-133)
+        sgs_store_visc(S, O, c, k, fabs(S.diff), dens);
         return;
     }
     // N2 (subgrid.f90:929-963): ptv at k-1, k, k+1 of the own column
@@ -133,14 +149,29 @@ __global__ void __launch_bounds__(256) sgs_visc_kernel(DevGrid G, SgsDev S, cons
     const double s2 = fmax_ref(2. * sm, 1.e-12);
     const double ri = n2 / fmax_ref(s2, 1.e-12) / fabs(S.pran);
     const double fri = ri <= SGS_RIC ? sqrt(1. - fmax_ref(ri, -0.25) / SGS_RIC) : 0.;
-    fkv[c] = ld(S.cs2d, k - 1) * sqrt(s2) * fmax_ref(fri, 0.);
+    sgs_store_visc(S, O, c, k, ld(S.cs2d, k - 1) * sqrt(s2) * fmax_ref(fri, 0.), dens);
+}
+
+// density-weighted viscosity and diffusivity of every cell (the unit entries, whose
+// turbu%fkv is an input): fe, nut as sgs_store_visc, over the whole allocation
+__global__ void __launch_bounds__(256) sgs_prep_kernel(DevGrid G, SgsDev S, const double *__restrict__ dens,
+                                                       const double *__restrict__ fkv, double *fe, double *nut)
+{
+    const long long n = G.ps * G.nz;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int k = 1 + (int)(q / G.ps);
+        const double t0 = ld(dens, q) * ld(fkv, q);
+        const double t = S.pran < 0. ? ld(S.func, k - 1) * t0 : t0;
+        fe[q] = t;
+        nut[q] = t / fabs(S.pran);
+    }
 }
 
 // efud (subgrid.f90:187-456): out := (in + eh) + ev for u, v (levels 1..nz-1) and
 // w (levels 2..nz-1), in = 0 when null.  fkv and the dij fields carry periodic ghosts.
 __global__ void __launch_bounds__(256) sgs_mom_kernel(DevGrid G, SgsDev S, const double *__restrict__ u,
-                                                      const double *__restrict__ v, const double *__restrict__ dens,
-                                                      const double *__restrict__ fkv, SgsDij D, const double *mflux,
+                                                      const double *__restrict__ v, const double *__restrict__ fev,
+                                                      SgsDij D, const double *mflux,
                                                       const double *in_u, const double *in_v, const double *in_w,
                                                       double *out_u, double *out_v, double *out_w)
 {
@@ -149,13 +180,8 @@ __global__ void __launch_bounds__(256) sgs_mom_kernel(DevGrid G, SgsDev S, const
     const int k = 1 + blockIdx.z;   // 1 .. nz-1
     if (i > G.nx - 2 || j > G.ny - 2) return;
     const double dx1 = 1. / G.dx, dy1 = 1. / G.dy;
-    // fkv := dens*fkv, damped by func(k) when pran < 0; fkh = f_an(k)*fkv (anis_k)
-    auto fe = [&](int ii, int jj, int kk) {
-        const long long q = gidx(G, ii, jj, kk);
-        double t = ld(dens, q) * ld(fkv, q);
-        if (S.pran < 0.) t = ld(S.func, kk - 1) * t;
-        return t;
-    };
+    // efud's fkv (dens*fkv, damped when pran < 0) and fkh = f_an(k)*fkv (anis_k)
+    auto fe = [&](int ii, int jj, int kk) { return ld(fev, gidx(G, ii, jj, kk)); };
     auto fh = [&](int ii, int jj, int kk) {
         const double t = fe(ii, jj, kk);
         return S.anis_k ? ld(S.fan, kk - 1) * t : t;
@@ -234,50 +260,52 @@ __global__ void __launch_bounds__(256) sgs_mom_kernel(DevGrid G, SgsDev S, const
 }
 
 // eff (subgrid.f90:604-789) with grad_quick (gradients.f90:62-187), CONSERVATIVE:
-// out := SGS tendency of the density-weighted scalar on levels 1..nz-1.
-// blockIdx.z = (k - 1) + (nz - 1) * field.
-__global__ void __launch_bounds__(256) sgs_scal_kernel(DevGrid G, SgsDev S, const double *__restrict__ dens,
-                                                       const double *__restrict__ fkv, SgsScal A)
+// out := SGS tendency of each density-weighted scalar on levels 1..nz-1.  One thread
+// per cell serves every field: the diffusivities of the seven points are loaded once.
+__global__ void __launch_bounds__(256) sgs_scal_kernel(DevGrid G, SgsDev S, const double *__restrict__ nutv, SgsScal A)
 {
     const int i = 4 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 4 + blockIdx.y * blockDim.y + threadIdx.y;
-    const int nz = G.nz;
-    const int f = blockIdx.z / (nz - 1);
-    const int k = 1 + blockIdx.z - f * (nz - 1);
-    if (i > G.nx - 2 || j > G.ny - 2 || f >= A.nf) return;
+    const int k = 1 + blockIdx.z;   // 1 .. nz-1
+    if (i > G.nx - 2 || j > G.ny - 2) return;
     const double dx1 = 1. / G.dx, dy1 = 1. / G.dy;
-    const double apran = fabs(S.pran);
-    auto nut = [&](long long q, int kk) {
-        return S.pran < 0. ? ld(dens, q) * ld(fkv, q) * ld(S.func, kk - 1) / apran : ld(dens, q) * ld(fkv, q) / apran;
-    };
-    auto nuh = [&](long long q, int kk) {
-        const double t = nut(q, kk);
-        return S.anis_k ? ld(S.fan, kk - 1) * t : t;
-    };
-    const double *x = A.x[f];
-    const double *x0 = A.x0[f];
-    auto xs = [&](long long q, int kk) { return (S.diff_on && x0) ? ld(x, q) - ld(x0, kk - 1) : ld(x, q); };
     const long long c = gidx(G, i, j, k), px = G.px, ps = G.ps;
-    const double fxp = 0.5 * (nuh(c + 1, k) + nuh(c, k)) * ((xs(c + 1, k) - xs(c, k)) * dx1);
-    const double fxm = 0.5 * (nuh(c, k) + nuh(c - 1, k)) * ((xs(c, k) - xs(c - 1, k)) * dx1);
-    const double fyp = 0.5 * (nuh(c + px, k) + nuh(c, k)) * ((xs(c + px, k) - xs(c, k)) * dy1);
-    const double fym = 0.5 * (nuh(c, k) + nuh(c - px, k)) * ((xs(c, k) - xs(c - px, k)) * dy1);
-    const double fzp = 0.5 * (nut(c + ps, k + 1) + nut(c, k)) * ((xs(c + ps, k + 1) - xs(c, k)) * ld(G.dz1, k - 1));
-    double e = (fxp - fxm) * dx1;
-    e = e + (fyp - fym) * dy1;
-    double ez;
-    if (k == 1) {
-        double fsv = 0.;
-        if (A.fs[f]) {
-            fsv = ld(A.fs[f], (long long)(j - 1) * G.nx + (i - 1));
-            if (A.fs_neg[f]) fsv = -fsv;
+    const double fan = S.anis_k ? ld(S.fan, k - 1) : 1.;
+    auto nuh = [&](long long q) {
+        const double t = ld(nutv, q);
+        return S.anis_k ? fan * t : t;
+    };
+    const double h0 = nuh(c), hxp = nuh(c + 1), hxm = nuh(c - 1), hyp = nuh(c + px), hym = nuh(c - px);
+    const double n0 = ld(nutv, c), nzp = ld(nutv, c + ps), nzm = k >= 2 ? ld(nutv, c - ps) : 0.;
+    const double d1k = ld(G.dz1, k - 1), d1km = k >= 2 ? ld(G.dz1, k - 2) : 0., dzw = ld(G.dz1w, k - 1);
+    for (int f = 0; f < A.nf; f++) {
+        const double *x = A.x[f];
+        const double *x0 = A.x0[f];
+        const bool sub = S.diff_on && x0;
+        const double x0k = sub ? ld(x0, k - 1) : 0., x0p = sub ? ld(x0, k) : 0., x0m = (sub && k >= 2) ? ld(x0, k - 2) : 0.;
+        auto xs = [&](long long q, double xz) { return sub ? ld(x, q) - xz : ld(x, q); };
+        const double xc = xs(c, x0k);
+        const double fxp = 0.5 * (hxp + h0) * ((xs(c + 1, x0k) - xc) * dx1);
+        const double fxm = 0.5 * (h0 + hxm) * ((xc - xs(c - 1, x0k)) * dx1);
+        const double fyp = 0.5 * (hyp + h0) * ((xs(c + px, x0k) - xc) * dy1);
+        const double fym = 0.5 * (h0 + hym) * ((xc - xs(c - px, x0k)) * dy1);
+        const double fzp = 0.5 * (nzp + n0) * ((xs(c + ps, x0p) - xc) * d1k);
+        double e = (fxp - fxm) * dx1;
+        e = e + (fyp - fym) * dy1;
+        double ez;
+        if (k == 1) {
+            double fsv = 0.;
+            if (A.fs[f]) {
+                fsv = ld(A.fs[f], (long long)(j - 1) * G.nx + (i - 1));
+                if (A.fs_neg[f]) fsv = -fsv;
+            }
+            ez = (fzp - fsv) * dzw;
+        } else {
+            const double fzm = 0.5 * (n0 + nzm) * ((xc - xs(c - ps, x0m)) * d1km);
+            ez = (fzp - fzm) * dzw;
         }
-        ez = (fzp - fsv) * ld(G.dz1w, 0);
-    } else {
-        const double fzm = 0.5 * (nut(c, k) + nut(c - ps, k - 1)) * ((xs(c, k) - xs(c - ps, k - 1)) * ld(G.dz1, k - 2));
-        ez = (fzp - fzm) * ld(G.dz1w, k - 1);
+        A.out[f][c] = e + ez;
     }
-    A.out[f][c] = e + ez;
 }
 
 inline dim3 sgs_grid(const DevGrid &g, int nzb) { return dim3((g.maxx + 31) / 32, (g.maxy + 7) / 8, nzb); }
@@ -285,29 +313,37 @@ inline dim3 sgs_grid(const DevGrid &g, int nzb) { return dim3((g.maxx + 31) / 32
 }  // namespace
 
 cudaError_t launch_sgs_visc(const DevGrid &g, const SgsDev &s, const double *u, const double *v, const double *w,
-                            const double *es, const double *qt, const SgsDij &d, double *fkv, cudaStream_t st)
+                            const double *es, const double *qt, const double *dens, const SgsDij &d,
+                            const SgsVisc &o, cudaStream_t st)
 {
     if (g.nz < 5) return cudaErrorInvalidValue;
-    sgs_visc_kernel<<<sgs_grid(g, g.nz), dim3(32, 8), 0, st>>>(g, s, u, v, w, es, qt, d, fkv);
+    if (o.fe && (!o.nut || !dens)) return cudaErrorInvalidValue;
+    if ((o.fkv || o.fe) && !s.diff_on && !es) return cudaErrorInvalidValue;
+    sgs_visc_kernel<<<sgs_grid(g, g.nz), dim3(32, 8), 0, st>>>(g, s, u, v, w, es, qt, dens, d, o);
     return cudaGetLastError();
 }
 
-cudaError_t launch_sgs_mom(const DevGrid &g, const SgsDev &s, const double *u, const double *v, const double *dens,
-                           const double *fkv, const SgsDij &d, const double *mflux, const double *in_u,
-                           const double *in_v, const double *in_w, double *out_u, double *out_v, double *out_w,
-                           cudaStream_t st)
+cudaError_t launch_sgs_prep(const DevGrid &g, const SgsDev &s, const double *dens, const double *fkv, double *fe,
+                            double *nut, cudaStream_t st)
 {
-    if (g.nz < 5) return cudaErrorInvalidValue;
-    sgs_mom_kernel<<<sgs_grid(g, g.nz - 1), dim3(32, 8), 0, st>>>(g, s, u, v, dens, fkv, d, mflux, in_u, in_v, in_w,
-                                                                   out_u, out_v, out_w);
+    sgs_prep_kernel<<<1184, 256, 0, st>>>(g, s, dens, fkv, fe, nut);
     return cudaGetLastError();
 }
 
-cudaError_t launch_sgs_scal(const DevGrid &g, const SgsDev &s, const double *dens, const double *fkv,
-                            const SgsScal &a, cudaStream_t st)
+cudaError_t launch_sgs_mom(const DevGrid &g, const SgsDev &s, const double *u, const double *v, const double *fe,
+                           const SgsDij &d, const double *mflux, const double *in_u, const double *in_v,
+                           const double *in_w, double *out_u, double *out_v, double *out_w, cudaStream_t st)
+{
+    if (g.nz < 5) return cudaErrorInvalidValue;
+    sgs_mom_kernel<<<sgs_grid(g, g.nz - 1), dim3(32, 8), 0, st>>>(g, s, u, v, fe, d, mflux, in_u, in_v, in_w, out_u,
+                                                                   out_v, out_w);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sgs_scal(const DevGrid &g, const SgsDev &s, const double *nut, const SgsScal &a, cudaStream_t st)
 {
     if (g.nz < 5 || a.nf <= 0 || a.nf > MG_MAXF) return cudaErrorInvalidValue;
-    sgs_scal_kernel<<<sgs_grid(g, (g.nz - 1) * a.nf), dim3(32, 8), 0, st>>>(g, s, dens, fkv, a);
+    sgs_scal_kernel<<<sgs_grid(g, g.nz - 1), dim3(32, 8), 0, st>>>(g, s, nut, a);
     return cudaGetLastError();
 }
 

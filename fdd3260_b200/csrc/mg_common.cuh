@@ -117,6 +117,11 @@ struct SgsDev {
 struct SgsDij {
     double *d[6];   // d11, d22, d33, d12, d13, d23 (cell centred, periodic ghosts)
 };
+struct SgsVisc {
+    double *fkv;   // turbu%fkv (interior), or null
+    double *fe;    // dens*fkv (times func(k) when pran < 0), or null (then nut null too)
+    double *nut;   // fe/|pran|, the scalar diffusivity
+};
 struct SgsScal {
     int nf;
     const double *x[MG_MAXF];      // natural level-n scalar
@@ -127,13 +132,14 @@ struct SgsScal {
 };
 __host__ __device__ __forceinline__ double fmax_ref(double a, double b) { return a > b ? a : b; }
 cudaError_t launch_sgs_visc(const DevGrid &g, const SgsDev &s, const double *u, const double *v, const double *w,
-                            const double *es, const double *qt, const SgsDij &d, double *fkv, cudaStream_t st);
-cudaError_t launch_sgs_mom(const DevGrid &g, const SgsDev &s, const double *u, const double *v, const double *dens,
-                           const double *fkv, const SgsDij &d, const double *mflux, const double *in_u,
-                           const double *in_v, const double *in_w, double *out_u, double *out_v, double *out_w,
-                           cudaStream_t st);
-cudaError_t launch_sgs_scal(const DevGrid &g, const SgsDev &s, const double *dens, const double *fkv,
-                            const SgsScal &a, cudaStream_t st);
+                            const double *es, const double *qt, const double *dens, const SgsDij &d,
+                            const SgsVisc &o, cudaStream_t st);
+cudaError_t launch_sgs_prep(const DevGrid &g, const SgsDev &s, const double *dens, const double *fkv, double *fe,
+                            double *nut, cudaStream_t st);
+cudaError_t launch_sgs_mom(const DevGrid &g, const SgsDev &s, const double *u, const double *v, const double *fe,
+                           const SgsDij &d, const double *mflux, const double *in_u, const double *in_v,
+                           const double *in_w, double *out_u, double *out_v, double *out_w, cudaStream_t st);
+cudaError_t launch_sgs_scal(const DevGrid &g, const SgsDev &s, const double *nut, const SgsScal &a, cudaStream_t st);
 void sgs_host_profiles(int nz, double dx, double dy, double dz, const double *fdz0, const double *pt0,
                        const double *qv0, int anis_k, double zdec, double zrough, double *prof);
 
