@@ -47,6 +47,26 @@ class MgSgsParams(C.Structure):
 
 SGS_NPROF = 10
 
+MG_STOP_NONE, MG_STOP_ES, MG_STOP_QT, MG_STOP_CFL, MG_STOP_DT = 0, 1, 2, 3, 4
+
+
+class MgCheckParams(C.Structure):
+    _fields_ = [
+        ("cfl_max", C.c_double), ("cfl_min", C.c_double), ("dt0_i", C.c_double), ("limit_ts", C.c_double),
+        ("es_min", C.c_double), ("es_max", C.c_double), ("qt_min", C.c_double), ("qt_max", C.c_double),
+        ("ldtfix", C.c_int), ("apply", C.c_int),
+    ]
+
+
+class MgCheckResult(C.Structure):
+    _fields_ = [
+        ("maxcfl", C.c_double), ("cfl_ijk", C.c_int * 3), ("stop", C.c_int),
+        ("dt0_old", C.c_double), ("dt0_new", C.c_double),
+        ("es_min", C.c_double), ("es_max", C.c_double), ("qt_min", C.c_double), ("qt_max", C.c_double),
+        ("es_min_ijk", C.c_int * 3), ("es_max_ijk", C.c_int * 3), ("qt_min_ijk", C.c_int * 3),
+        ("qt_max_ijk", C.c_int * 3),
+    ]
+
 
 class MimicaError(RuntimeError):
     def __init__(self, code: int, where: str):
@@ -99,6 +119,9 @@ def lib() -> C.CDLL:
         L.mg_ensemble_step.argtypes = [vp, C.c_int, C.c_int]
         L.mg_ensemble_time_steps.argtypes = [vp, C.c_int, C.c_int, _dp]
         L.mg_ensemble_launch_count.argtypes = [vp]
+        L.mg_checkall.argtypes = [vp, C.POINTER(MgCheckParams), C.POINTER(MgCheckResult)]
+        L.mg_cfl_dt.argtypes = [C.POINTER(MgCheckParams), C.c_double, C.c_double, _dp, C.POINTER(C.c_int)]
+        L.mg_set_dt.argtypes = [vp, C.c_double]
         L.mg_set_sgs.argtypes = [vp, C.POINTER(MgSgsParams)]
         L.mg_set_surface_fluxes.argtypes = [vp, _dp, _dp, _dp]
         L.mg_sgs_profiles.argtypes = [C.POINTER(MgParams), C.POINTER(MgSgsParams), _dp]
@@ -137,4 +160,5 @@ EXPORTED = [
     "mg_fft_solve", "mg_anelastic_pressure", "mg_time_steps", "mg_profile_enable", "mg_profile_report",
     "mg_advection_tl", "mg_advection_ad", "mg_anelastic_pressure_ad", "mg_time_adjoint", "mg_ensemble_create", "mg_ensemble_destroy", "mg_ensemble_step", "mg_ensemble_time_steps", "mg_ensemble_launch_count",
     "mg_set_sgs", "mg_set_surface_fluxes", "mg_sgs_profiles", "mg_calc_subgrid", "mg_efud", "mg_eff",
+    "mg_checkall", "mg_cfl_dt", "mg_set_dt",
 ]

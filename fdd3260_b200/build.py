@@ -40,6 +40,7 @@ SOURCES = [
     ("noalloc.cu", ["-fmad=false"]),
     ("k_adjoint.cu", ["-fmad=false"]),
     ("k_sgs.cu", ["-fmad=false", "-Xcompiler", "-ffp-contract=off"]),
+    ("k_check.cu", ["-fmad=false"]),
 ]
 
 

@@ -51,6 +51,27 @@ class Sgs:
 
 
 @dataclass
+class Checks:
+    """Switches of checkall (src/IO/check.f90) and the time-step control (namelist cm_num /
+    cm_run: cfl_max, cfl_min, limit_ts, ldtfix; checkx bounds of es and qt)."""
+    cfl_max: float = 0.5
+    cfl_min: float = 0.4
+    limit_ts: float = 20.0
+    ldtfix: int = 0
+    es_min: float = 200.0
+    es_max: float = 4000.0
+    qt_min: float = 1e-15
+    qt_max: float = 1.0
+
+    def params(self, dt0_i: float, apply: bool = True) -> _lib.MgCheckParams:
+        p = _lib.MgCheckParams()
+        p.cfl_max, p.cfl_min, p.dt0_i, p.limit_ts = self.cfl_max, self.cfl_min, dt0_i, self.limit_ts
+        p.es_min, p.es_max, p.qt_min, p.qt_max = self.es_min, self.es_max, self.qt_min, self.qt_max
+        p.ldtfix, p.apply = int(self.ldtfix), int(apply)
+        return p
+
+
+@dataclass
 class Domain:
     maxx: int
     maxy: int

@@ -17,6 +17,7 @@
 #include <new>
 #include <vector>
 
+#include <climits>
 #include <cmath>
 
 #include "mg_common.cuh"
@@ -47,6 +48,8 @@ struct mg_ctx {
     size_t bytes = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int gsteps[2] = {0, 0};
+    long long gen = 0;                   // bumped whenever recorded step graphs go stale
+    void *chk = nullptr;                 // scratch of the per-step checks
     // SGS diffusion (mg_set_sgs): per-level factors + qt0 on the device, the
     // deformation tensor and eddy viscosity of level n, the stored tendencies
     mg_sgs_params sgsp{};
@@ -240,7 +243,7 @@ static void free_ctx(mg_ctx *c)
     for (int i = 0; i < 3; i++) { cudaFree(c->mA[i]); cudaFree(c->mB[i]); cudaFree(c->tm[i]); }
     for (int f = 0; f < MG_MAXF; f++) { cudaFree(c->sA[f]); cudaFree(c->sB[f]); cudaFree(c->ts[f]); }
     for (int i = 0; i < 16; i++) cudaFree(c->unit[i]);
-    cudaFree(c->sgs_prof); cudaFree(c->fkv); cudaFree(c->sfe); cudaFree(c->snut);
+    cudaFree(c->sgs_prof); cudaFree(c->fkv); cudaFree(c->sfe); cudaFree(c->snut); cudaFree(c->chk);
     for (int q = 0; q < 6; q++) cudaFree(c->dij[q]);
     for (int q = 0; q < 3; q++) { cudaFree(c->sgm[q]); cudaFree(c->sfc[q]); }
     for (int f = 0; f < MG_MAXF; f++) cudaFree(c->sgsc[f]);
@@ -477,6 +480,15 @@ static cudaError_t project(mg_ctx *c, double *mu, double *mv, double *mw, const 
 }
 
 // ---------------- one step ----------------
+// step graphs recorded before a change of the step (time step, SGS switches) no longer
+// describe it: drop the context's own, and make ensembles that hold it re-record
+static void drop_graphs(mg_ctx *c)
+{
+    for (int i = 0; i < 2; i++)
+        if (c->gexec[i]) { cudaGraphExecDestroy(c->gexec[i]); c->gexec[i] = nullptr; }
+    c->gen++;
+}
+
 // ---------------- SGS diffusion ----------------
 static SgsDev sgs_dev(const mg_ctx *c)
 {
@@ -714,6 +726,7 @@ struct mg_ens {
     cudaEvent_t fork = nullptr;
     std::vector<cudaEvent_t> join;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    long long gen = -1;                  // sum of the members' generations the graphs were recorded at
     int launches = 0;
 };
 
@@ -777,6 +790,13 @@ extern "C" int mg_ensemble_step(mg_ens *e, int nsteps, int ntime0)
         if (c->prof_on) return MG_ERR_STATE;   // per-kernel events cannot be recorded into the graph
     }
     CKR(cudaSetDevice(e->device));
+    long long gsum = 0;
+    for (mg_ctx *c : e->m) gsum += c->gen;
+    if (gsum != e->gen) {   // a member's step changed since the graphs were recorded
+        for (int i = 0; i < 2; i++)
+            if (e->gexec[i]) { cudaGraphExecDestroy(e->gexec[i]); e->gexec[i] = nullptr; }
+        e->gen = gsum;
+    }
     int s = 0;
     while (nsteps - s >= 2) {
         const int par = (ntime0 + s) & 1;
@@ -914,9 +934,7 @@ extern "C" int mg_set_sgs(mg_ctx *c, const mg_sgs_params *s)
                 CKR(cudaMemset(c->sgsc[f], 0, c->fbytes));
             }
     c->sgs_on = s->with_dif != 0;
-    // step graphs recorded before this call no longer describe the step
-    for (int i = 0; i < 2; i++)
-        if (c->gexec[i]) { cudaGraphExecDestroy(c->gexec[i]); c->gexec[i] = nullptr; }
+    drop_graphs(c);
     return MG_OK;
 }
 
@@ -933,6 +951,94 @@ extern "C" int mg_set_surface_fluxes(mg_ctx *c, const double *esflux, const doub
         else CKR(cudaMemsetAsync(c->sfc[q], 0, b, c->stream));
     }
     return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+// ---- per-step checks and time-step control (src/IO/check.f90) ----
+extern "C" int mg_set_dt(mg_ctx *c, double dt0)
+{
+    if (!c || !std::isfinite(dt0) || !(dt0 > 0.)) return MG_ERR_PARAM;
+    if (dt0 == c->G.dt0) return MG_OK;
+    CKR(cudaSetDevice(c->device));
+    CKR(cudaStreamSynchronize(c->stream));
+    c->prm.dt0 = dt0;
+    c->G.dt0 = dt0;
+    drop_graphs(c);
+    return MG_OK;
+}
+
+extern "C" int mg_cfl_dt(const mg_check_params *p, double maxcfl, double dt0, double *dt0_new, int *stop)
+{
+    if (!p || !dt0_new || !stop) return MG_ERR_PARAM;
+    *dt0_new = dt0;
+    *stop = MG_STOP_NONE;
+    if (maxcfl > 2. || maxcfl < 1.e-7) {   // check.f90:191-202
+        *stop = MG_STOP_CFL;
+        return MG_OK;
+    }
+    const double dtref = dt0;
+    if (maxcfl >= p->cfl_max && p->ldtfix == 0) {   // :208-226
+        const double xx = maxcfl / dtref;
+        const double fac = 0.95 * p->cfl_max / xx;
+        *dt0_new = fac;
+        const double lim = p->limit_ts > 1. ? p->limit_ts : 1.;
+        if (p->limit_ts > 1. && *dt0_new <= p->dt0_i / lim) *stop = MG_STOP_DT;
+    }
+    if (maxcfl <= p->cfl_min && maxcfl > 0. && p->ldtfix == 0) {   // :253-264
+        const double xx = maxcfl / dtref;
+        const double fac = 1.15 * p->cfl_min / xx;
+        const double cap = 2. * p->dt0_i;
+        *dt0_new = fac < cap ? fac : cap;
+    }
+    return MG_OK;
+}
+
+extern "C" int mg_checkall(mg_ctx *c, const mg_check_params *p, mg_check_result *r)
+{
+    if (!c || !p || !r) return MG_ERR_PARAM;
+    if (!c->have_state) return MG_ERR_STATE;
+    CKR(cudaSetDevice(c->device));
+    if (!c->chk) {
+        CKR(cudaMalloc(&c->chk, check_scratch_bytes()));
+        c->bytes += check_scratch_bytes();
+    }
+    const DevGrid &G = c->G;
+    const int iqt = c->prm.iqt >= 0 ? 1 + c->prm.iqt : -1;
+    CKR(launch_check(G, c->mA[0], c->mA[1], c->mA[2], c->sA[1], iqt >= 0 ? c->sA[iqt] : nullptr, c->chk, c->stream));
+    struct { double v; long long L; } h[5];
+    const size_t off = check_scratch_bytes() - sizeof(h);
+    CKR(cudaMemcpyAsync(h, (char *)c->chk + off, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CKR(cudaStreamSynchronize(c->stream));
+    auto ijk = [&](long long L, int *o) {
+        if (L == LLONG_MAX) { o[0] = o[1] = o[2] = 0; return; }
+        o[0] = 4 + (int)(L % G.maxx);
+        const long long rr = L / G.maxx;
+        o[1] = 4 + (int)(rr % G.maxy);
+        o[2] = 1 + (int)(rr / G.maxy);
+    };
+    memset(r, 0, sizeof(*r));
+    r->maxcfl = h[0].L == LLONG_MAX ? 0. : h[0].v;
+    ijk(h[0].L, r->cfl_ijk);
+    r->es_max = h[1].v; ijk(h[1].L, r->es_max_ijk);
+    r->es_min = h[2].v; ijk(h[2].L, r->es_min_ijk);
+    if (iqt >= 0) {
+        r->qt_max = h[3].v; ijk(h[3].L, r->qt_max_ijk);
+        r->qt_min = h[4].v; ijk(h[4].L, r->qt_min_ijk);
+    }
+    r->dt0_old = r->dt0_new = G.dt0;
+    // checkall order: checkx(es), checkx(qt), checkwind; the first failing check stops
+    if (r->es_max > p->es_max || r->es_min < p->es_min) {
+        r->stop = MG_STOP_ES;
+    } else if (iqt >= 0 && (r->qt_max > p->qt_max || r->qt_min < p->qt_min)) {
+        r->stop = MG_STOP_QT;
+    } else {
+        int rc = mg_cfl_dt(p, r->maxcfl, G.dt0, &r->dt0_new, &r->stop);
+        if (rc) return rc;
+        if (p->apply && r->stop == MG_STOP_NONE && r->dt0_new != r->dt0_old) {
+            rc = mg_set_dt(c, r->dt0_new);
+            if (rc) return rc;
+        }
+    }
+    return MG_OK;
 }
 
 extern "C" int mg_calc_subgrid(mg_ctx *c, const double *u, const double *v, const double *w, const double *es,

@@ -143,6 +143,11 @@ cudaError_t launch_sgs_scal(const DevGrid &g, const SgsDev &s, const double *nut
 void sgs_host_profiles(int nz, double dx, double dy, double dz, const double *fdz0, const double *pt0,
                        const double *qv0, int anis_k, double zdec, double zrough, double *prof);
 
+// ---- per-step checks (k_check.cu) ----
+size_t check_scratch_bytes();
+cudaError_t launch_check(const DevGrid &g, const double *u, const double *v, const double *w, const double *es,
+                         const double *qt, void *scratch, cudaStream_t s);
+
 // tangent linear / adjoint of the scalar advection operator (k_adjoint.cu)
 cudaError_t launch_advection_tl(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
                                 const double *dx, const double *dmu, const double *dmv, const double *dmw, double *dA,

@@ -55,6 +55,25 @@ class Mimica:
     def launches_per_call(self) -> int:
         return int(self._L.mg_last_launch_count(self._h))
 
+    # ---- per-step checks and time-step control (check.f90) ----
+    def checkall(self, checks=None, apply: bool = True) -> dict:
+        """checkall on the resident state: max CFL (with location), es/qt bounds, and the
+        reference's advective time-step rule; with apply, a new dt0 is used from the next
+        step on."""
+        from .config import Checks
+        ch = checks if checks is not None else Checks()
+        p = ch.params(self.domain.dt0, apply)
+        r = _lib.MgCheckResult()
+        _lib.check(self._L.mg_checkall(self._h, C.byref(p), C.byref(r)), "mg_checkall")
+        out = {f: getattr(r, f) for f, _ in r._fields_}
+        for f, _ in r._fields_:
+            if f.endswith("_ijk"):
+                out[f] = tuple(out[f])
+        return out
+
+    def set_dt(self, dt0: float) -> None:
+        _lib.check(self._L.mg_set_dt(self._h, float(dt0)), "mg_set_dt")
+
     # ---- SGS turbulence diffusion (subgrid.f90) ----
     def set_sgs(self, sgs, with_dif: bool = True) -> None:
         """Switch SGS diffusion on (or off) for the following steps; uploads the surface

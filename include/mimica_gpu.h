@@ -180,6 +180,38 @@ int mg_fft_solve(mg_ctx *ctx, const double *tend, double *out);
 int mg_anelastic_pressure(mg_ctx *ctx, double *mu, double *mv, double *mw, double *p,
                           const double *wold, double *maxdiv, double *p1);
 
+/* ---- per-step checks and time-step control: checkall (src/IO/check.f90:59-95) ----
+ * checkx (:341-417) of es (theta) and qt, then checkwind (:102-337, ANELASTIC: the
+ * advective CFL only) on the resident level-n state, as the time loop calls it after
+ * each step (modelctl.f90:369).  Locations are absolute 1-based (i, j, k) of the first
+ * occurrence in the reference's loop order; the CFL location is (0, 0, 0) when every
+ * CFL number is 0.  stop reports what makes the reference call stop_mimica(1): the
+ * library itself never stops. */
+enum { MG_STOP_NONE = 0, MG_STOP_ES = 1, MG_STOP_QT = 2, MG_STOP_CFL = 3, MG_STOP_DT = 4 };
+typedef struct mg_check_params {
+    double cfl_max, cfl_min;   /* cfl_max, cfl_min (namelist defaults 0.5, 0.4) */
+    double dt0_i;              /* dt0_i: the run's initial time step */
+    double limit_ts;           /* limit_ts (default 20): stop when dt0 <= dt0_i/limit_ts */
+    double es_min, es_max;     /* checkx bounds of es (200, 4000 K) */
+    double qt_min, qt_max;     /* checkx bounds of qt (1e-15, 1); unused without qt */
+    int ldtfix;                /* ldtfix: 1 keeps dt0 */
+    int apply;                 /* 1: a new dt0 becomes the context's time step (mg_set_dt) */
+} mg_check_params;
+typedef struct mg_check_result {
+    double maxcfl;             /* maxcfl */
+    int cfl_ijk[3];            /* local_value of checkwind */
+    int stop;                  /* MG_STOP_*: the first check that stops the reference's run */
+    double dt0_old, dt0_new;   /* dt0 before and after the CFL rule */
+    double es_min, es_max, qt_min, qt_max;
+    int es_min_ijk[3], es_max_ijk[3], qt_min_ijk[3], qt_max_ijk[3];
+} mg_check_result;
+int mg_checkall(mg_ctx *ctx, const mg_check_params *p, mg_check_result *r);
+/* the advective time-step rule of checkwind (:193-264; no microphysics time scale):
+ * host only, no context */
+int mg_cfl_dt(const mg_check_params *p, double maxcfl, double dt0, double *dt0_new, int *stop);
+/* change the time step dt0 of a context (recorded step graphs are re-recorded) */
+int mg_set_dt(mg_ctx *ctx, double dt0);
+
 /* ---- SGS turbulence diffusion (src/PHYS/subgrid.f90) ----
  * The Smagorinsky-Lilly closure of the build without TKE: calc_subgrid (cal_dij,
  * stability, calc_smago with the 'Lilly' stability correction, :87-145, :793-866,

@@ -2017,6 +2017,48 @@ void mo_eff(const mo_grid *g, int kind, const double *dens, const double *fkv, c
 }
 
 /* ======================================================================
+ * Per-step checks: src/IO/check.f90 checkwind :102-159 (max CFL and the location of
+ * its first occurrence, ANELASTIC) and checkx :341-380 (maxval/minval and
+ * maxloc/minloc, first occurrence in array element order).  Locations are absolute
+ * 1-based (i, j, k); (0, 0, 0) when no cell has CFL > 0.
+ * ==================================================================== */
+void mo_checkwind(const mo_grid *g, const double *u, const double *v, const double *w, double *maxcfl, int *loc)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    const double dx1 = 1. / g->dx, dy1 = 1. / g->dy, dt0 = g->dt0;
+    double cflmax = 0.;
+    loc[0] = loc[1] = loc[2] = 0;
+    for (int k = 1; k <= nz; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) {
+                size_t c = IX(g, i, j, k);
+                double cflx = dt0 * fabs(u[c]) * dx1;
+                double cfly = dt0 * fabs(v[c]) * dy1;
+                double cflz = dt0 * fabs(w[c]) * P1(g->dz1w, k);
+                double cfl = dmax2(dmax2(cflx, cfly), cflz);
+                if (cfl > cflmax) {
+                    cflmax = cfl;
+                    loc[0] = i; loc[1] = j; loc[2] = k;
+                }
+            }
+    *maxcfl = cflmax;
+}
+
+void mo_checkx(const mo_grid *g, const double *x, double *mn, double *mx, int *locmin, int *locmax)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    int first = 1;
+    for (int k = 1; k <= nz; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) {
+                double a = x[IX(g, i, j, k)];
+                if (first || a > *mx) { *mx = a; locmax[0] = i; locmax[1] = j; locmax[2] = k; }
+                if (first || a < *mn) { *mn = a; locmin[0] = i; locmin[1] = j; locmin[2] = k; }
+                first = 0;
+            }
+}
+
+/* ======================================================================
  * One integrator step: src/INTEG/time_step.f90 stepping :76-334 (dynamics subset:
  * with_rad, with_mic, sponge, nudging off; w0 = 0; with_dif from g->sgs), integrate_all
  * :337-444, integ_mom/integ_scal src/INTEG/integpack.f90:54-284 with

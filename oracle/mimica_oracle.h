@@ -125,6 +125,10 @@ void mo_efud(const mo_grid *g, const double *u, const double *v, const double *w
  * ec := SGS tendency on the interior levels 1..nz-1 (conservative form) */
 void mo_eff(const mo_grid *g, int kind, const double *dens, const double *fkv, const double *x, double *ec);
 
+/* ---- per-step checks (src/IO/check.f90 checkwind, checkx) ---- */
+void mo_checkwind(const mo_grid *g, const double *u, const double *v, const double *w, double *maxcfl, int *loc);
+void mo_checkx(const mo_grid *g, const double *x, double *mn, double *mx, int *locmin, int *locmax);
+
 /* ---- one full integrator step (time_step.f90 stepping, dynamics subset) ----
  * State at time level n, natural variables, all arrays nx*ny*nz with valid halos:
  *   u, v, w (velocities), p, dens, scal[0..nsc)  (es = theta first, then qt if

@@ -81,6 +81,8 @@ def load(omp: bool = False) -> C.CDLL:
         L.mo_grid_metrics.argtypes = [C.c_int, C.c_double, _dp, _dp, _dp, _dp]
         L.mo_base_state.argtypes = [C.c_int, C.c_double, C.c_double, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         L.mo_get_wv.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _dp]
+        L.mo_checkwind.argtypes = [g, _dp, _dp, _dp, _dp, C.POINTER(C.c_int)]
+        L.mo_checkx.argtypes = [g, _dp, _dp, _dp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.mo_sgs_profiles.argtypes = [g, _dp]
         L.mo_cal_dij.argtypes = [g, _dp, _dp, _dp, C.POINTER(_dp)]
         L.mo_calc_subgrid.argtypes = [g, _dp, _dp, _dp, _dp, _dp, _dp]
@@ -137,6 +139,19 @@ class Oracle:
         xs = np.array(xs, dtype=np.float64, copy=True)
         self.L.mo_advection_ac(self.gp, P(np.ascontiguousarray(x)), P(ua), P(va), P(wa), P(xs), 0)
         return xs
+
+    # ---- per-step checks (check.f90) ----
+    def checkwind(self, u, v, w):
+        mx = C.c_double(0.0)
+        loc = (C.c_int * 3)()
+        self.L.mo_checkwind(self.gp, *[P(np.ascontiguousarray(a)) for a in (u, v, w)], C.byref(mx), loc)
+        return mx.value, tuple(loc)
+
+    def checkx(self, x):
+        mn, mx = C.c_double(0.0), C.c_double(0.0)
+        lmin, lmax = (C.c_int * 3)(), (C.c_int * 3)()
+        self.L.mo_checkx(self.gp, P(np.ascontiguousarray(x)), C.byref(mn), C.byref(mx), lmin, lmax)
+        return mn.value, mx.value, tuple(lmin), tuple(lmax)
 
     # ---- SGS turbulence (subgrid.f90) ----
     def sgs_profiles(self) -> np.ndarray:
