@@ -45,7 +45,7 @@ class MgSgsParams(C.Structure):
     ]
 
 
-SGS_NPROF = 10
+SGS_NPROF = 11
 
 MG_STOP_NONE, MG_STOP_ES, MG_STOP_QT, MG_STOP_CFL, MG_STOP_DT = 0, 1, 2, 3, 4
 
@@ -122,6 +122,7 @@ def lib() -> C.CDLL:
         L.mg_checkall.argtypes = [vp, C.POINTER(MgCheckParams), C.POINTER(MgCheckResult)]
         L.mg_cfl_dt.argtypes = [C.POINTER(MgCheckParams), C.c_double, C.c_double, _dp, C.POINTER(C.c_int)]
         L.mg_set_dt.argtypes = [vp, C.c_double]
+        L.mg_download_ksgs.argtypes = [vp, _dp]
         L.mg_set_sgs.argtypes = [vp, C.POINTER(MgSgsParams)]
         L.mg_set_surface_fluxes.argtypes = [vp, _dp, _dp, _dp]
         L.mg_sgs_profiles.argtypes = [C.POINTER(MgParams), C.POINTER(MgSgsParams), _dp]
@@ -160,5 +161,5 @@ EXPORTED = [
     "mg_fft_solve", "mg_anelastic_pressure", "mg_time_steps", "mg_profile_enable", "mg_profile_report",
     "mg_advection_tl", "mg_advection_ad", "mg_anelastic_pressure_ad", "mg_time_adjoint", "mg_ensemble_create", "mg_ensemble_destroy", "mg_ensemble_step", "mg_ensemble_time_steps", "mg_ensemble_launch_count",
     "mg_set_sgs", "mg_set_surface_fluxes", "mg_sgs_profiles", "mg_calc_subgrid", "mg_efud", "mg_eff",
-    "mg_checkall", "mg_cfl_dt", "mg_set_dt",
+    "mg_checkall", "mg_cfl_dt", "mg_set_dt", "mg_download_ksgs",
 ]

@@ -58,6 +58,7 @@ struct mg_ctx {
     double *sgs_prof = nullptr;          // SGS_NPROF*nz factors, then qt0 (nz)
     double *dij[6] = {}, *fkv = nullptr, *sfe = nullptr, *snut = nullptr, *sgm[3] = {}, *sgsc[MG_MAXF] = {};
     double *sfc[3] = {};                 // esflux, qvflux, mflux (nx*ny), zero until set
+    int have_fkv = 0;                    // fkv holds the viscosity of the last step's level n
     // per-kernel profiling (CUDA events on the context stream)
     int prof_on = 0;
     struct Ev { const char *name; cudaEvent_t a, b; };
@@ -539,11 +540,12 @@ static cudaError_t sgs_tendencies(mg_ctx *c, int *launches)
     const SgsDev S = sgs_dev(c);
     SgsDij D{};
     for (int q = 0; q < 6; q++) D.d[q] = c->dij[q];
-    const SgsVisc O{nullptr, c->sfe, c->snut};
+    const SgsVisc O{c->fkv, c->sfe, c->snut};
     PROF(c, "sgs_viscosity", launch_sgs_visc(G, S, c->mA[0], c->mA[1], c->mA[2], c->sA[ies], iqt >= 0 ? c->sA[iqt] : nullptr,
                                              c->sA[0], D, O, c->stream));
-    double *hf[8] = {c->dij[0], c->dij[1], c->dij[2], c->dij[3], c->dij[4], c->dij[5], c->sfe, c->snut};
-    PROF(c, "sgs_halo", launch_halo_fill(G, hf, 8, c->stream));
+    double *hf[9] = {c->dij[0], c->dij[1], c->dij[2], c->dij[3], c->dij[4], c->dij[5], c->sfe, c->snut, c->fkv};
+    PROF(c, "sgs_halo", launch_halo_fill(G, hf, 9, c->stream));
+    c->have_fkv = 1;
     PROF(c, "sgs_momentum", launch_sgs_mom(G, S, c->mA[0], c->mA[1], c->sfe, D, c->sfc[2], nullptr, nullptr, nullptr,
                                            c->sgm[0], c->sgm[1], c->sgm[2], c->stream));
     SgsScal A{};
@@ -934,6 +936,7 @@ extern "C" int mg_set_sgs(mg_ctx *c, const mg_sgs_params *s)
                 CKR(cudaMemset(c->sgsc[f], 0, c->fbytes));
             }
     c->sgs_on = s->with_dif != 0;
+    c->have_fkv = 0;
     drop_graphs(c);
     return MG_OK;
 }
@@ -1041,6 +1044,30 @@ extern "C" int mg_checkall(mg_ctx *c, const mg_check_params *p, mg_check_result 
     return MG_OK;
 }
 
+extern "C" int mg_download_ksgs(mg_ctx *c, double *ksgs)
+{
+    if (!c || !ksgs) return MG_ERR_PARAM;
+    if (!c->sgs_on || !c->have_fkv) return MG_ERR_STATE;
+    CKR(cudaSetDevice(c->device));
+    CKR(d2h(c, ksgs, c->fkv, cudaMemcpyDeviceToHost));
+    CKR(cudaStreamSynchronize(c->stream));
+    const DevGrid &G = c->G;
+    std::vector<double> prof((size_t)SGS_NPROF * G.nz);
+    const mg_params &P = c->prm;
+    sgs_host_profiles(G.nz, P.dx, P.dy, P.dz, P.fdz0, P.pt0, P.qv0, c->sgsp.anis_k, c->sgsp.zdec, c->sgsp.zrough,
+                      prof.data());
+    const double C_k = 0.12;   // shared_turbu.f90:48
+    const size_t pl = (size_t)G.nx * G.ny;
+    for (int k = 1; k <= G.nz; k++) {
+        const double cd = C_k * prof[(size_t)10 * G.nz + k - 1];
+        for (size_t q = (size_t)(k - 1) * pl; q < (size_t)k * pl; q++) {
+            const double t = ksgs[q] / cd;
+            ksgs[q] = t * t;
+        }
+    }
+    return MG_OK;
+}
+
 extern "C" int mg_calc_subgrid(mg_ctx *c, const double *u, const double *v, const double *w, const double *es,
                                const double *qt, double *fkv)
 {
@@ -1061,6 +1088,7 @@ extern "C" int mg_calc_subgrid(mg_ctx *c, const double *u, const double *v, cons
     double *hf[1] = {c->fkv};
     CKR(launch_halo_fill(c->G, hf, 1, c->stream));
     CKR(d2h(c, fkv, c->fkv, cudaMemcpyDeviceToHost));
+    c->have_fkv = 0;   // the buffer no longer holds the step's viscosity
     return cuerr(cudaStreamSynchronize(c->stream));
 }
 

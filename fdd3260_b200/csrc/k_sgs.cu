@@ -350,13 +350,14 @@ cudaError_t launch_sgs_scal(const DevGrid &g, const SgsDev &s, const double *nut
 // Per-level factors (host): z0 (define_grid.f90:132-135), length_scale
 // (subgrid.f90:1183-1232, l_d = 1e8 without TKE), the pran < 0 damping (:234-239),
 // f_an (:244-249), the N2 coefficients (:929-963) and the d/dz denominators of
-// grad_wind_3d (gradients.f90:884-905).  Layout prof[q*nz + k-1], q = 0..9.
+// grad_wind_3d (gradients.f90:884-905), and delta.  Layout prof[q*nz + k-1], q = 0..10.
 void sgs_host_profiles(int nz, double dx, double dy, double dz, const double *f, const double *pt0, const double *qv0,
                        int anis, double zdec, double zrough, double *prof)
 {
     double *z0 = prof, *cs2d = prof + nz, *func = prof + 2 * nz, *fan = prof + 3 * nz;
     double *n2c = prof + 4 * nz, *n2d = prof + 5 * nz;
     double *du = prof + 6 * nz, *dv = prof + 7 * nz, *dw = prof + 8 * nz, *dwt = prof + 9 * nz;
+    double *dl = prof + 10 * nz;
     for (int q = 0; q < SGS_NPROF * nz; q++) prof[q] = 0.;
     z0[0] = 0.5 * dz * f[0];
     for (int k = 2; k <= nz; k++) z0[k - 1] = z0[k - 2] + 0.5 * dz * (f[k - 2] + f[k - 1]);
@@ -367,6 +368,7 @@ void sgs_host_profiles(int nz, double dx, double dy, double dz, const double *f,
         const double delta = 1. / std::sqrt(1. / (deltas * deltas) + 1. / (l_d * l_d) + 1. / (l_z * l_z));
         const double cd = SGS_CS * delta;
         cs2d[k - 1] = cd * cd;
+        dl[k - 1] = delta;
         const double fv = 1. - std::exp(6. * (z0[k - 1] - zdec) / zdec);
         func[k - 1] = fv > 0. ? fv : 0.;
         if (anis) {

@@ -108,7 +108,7 @@ cudaError_t launch_k2_mixed(const DevGrid &g, const K2Args &a, const K2Maps &map
 cudaError_t launch_halo_fill(const DevGrid &g, double *const *fields, int nf, cudaStream_t s);
 
 // ---- SGS turbulence diffusion (k_sgs.cu) ----
-#define SGS_NPROF 10   // per-level factors: z0, (C_s delta)^2, func, f_an, N2 coef., N2 den., d/dz den. u, v, w, w(nz-1)
+#define SGS_NPROF 11   // per-level factors: z0, (C_s delta)^2, func, f_an, N2 coef., N2 den., d/dz den. u, v, w, w(nz-1), delta
 struct SgsDev {
     int anis_k, momsf, diff_on;
     double diff, pran, min_w;

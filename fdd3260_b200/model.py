@@ -26,6 +26,8 @@ class Mimica:
         _lib.check(L.mg_create(C.byref(params), device, C.byref(h)), "mg_create")
         self._h = h
         self._L = L
+        self.dt0 = domain.dt0          # current time step (checkall / set_dt may change it)
+        self._sgs_on = False
         if domain.sgs is not None:
             self.set_sgs(domain.sgs)
 
@@ -65,6 +67,8 @@ class Mimica:
         p = ch.params(self.domain.dt0, apply)
         r = _lib.MgCheckResult()
         _lib.check(self._L.mg_checkall(self._h, C.byref(p), C.byref(r)), "mg_checkall")
+        if apply and r.stop == _lib.MG_STOP_NONE:
+            self.dt0 = r.dt0_new
         out = {f: getattr(r, f) for f, _ in r._fields_}
         for f, _ in r._fields_:
             if f.endswith("_ijk"):
@@ -73,6 +77,54 @@ class Mimica:
 
     def set_dt(self, dt0: float) -> None:
         _lib.check(self._L.mg_set_dt(self._h, float(dt0)), "mg_set_dt")
+        self.dt0 = float(dt0)
+
+    # ---- restart files (restarting.f90 savedata / readdata) ----
+    def ksgs(self) -> np.ndarray:
+        """turbu%ksgs of the last step's level n (SGS diffusion on)."""
+        out = np.zeros(self.domain.shape)
+        _lib.check(self._L.mg_download_ksgs(self._h, _lib.ptr(out)), "mg_download_ksgs")
+        return out
+
+    def save_restart(self, path: str, time: float = 0.0, ntime: int = 0, ntau: int = 1, profiles: dict | None = None,
+                     xn_ccn0: float = 0.0, xn_in0: float = 0.0) -> None:
+        """Write the resident state as the reference's savedata does ('V04').  Profiles
+        not given are taken from the domain (p0, den0, avden0, stab0, pt0, qv0) or zero."""
+        from . import restart
+        d = self.domain
+        st = self.download()
+        qt = st.scal[st.iqt] if st.iqt >= 0 else np.zeros(d.shape)
+        passive = [a for q, a in enumerate(st.scal) if q != 0 and q != st.iqt]
+        prof = {"p0": d.p0, "den0": d.den0, "avden0": d.avden0, "stab0": d.stab0, "pt0": d.pt0, "qv0": d.qv0}
+        prof.update(profiles or {})
+        hdr = {"time": float(time), "ntime": int(ntime), "dt": float(self.dt0), "ntau": int(ntau), "nx": d.nx,
+               "ny": d.ny, "nz": d.nz, "dx": d.dx, "dy": d.dy, "dz": d.dz, "nscal": len(passive), "nparc": 0,
+               "xn_ccn0": float(xn_ccn0), "xn_in0": float(xn_in0)}
+        r = restart.Restart(hdr, prof, {"u": st.u, "v": st.v, "w": st.w, "p": st.p, "es": st.scal[0], "qt": qt,
+                                        "dens": st.dens}, passive, ksgs=self.ksgs() if self._sgs_on else None)
+        restart.write(path, r)
+
+    def load_restart(self, path: str) -> dict:
+        """Read a restart file of this domain, upload its state and take its time step;
+        returns the header (time, ntime, ...)."""
+        from . import restart
+        from .config import State
+        d = self.domain
+        r = restart.read(path, with_dif=self._sgs_on)
+        h = r.header
+        if (h["nx"], h["ny"], h["nz"]) != (d.nx, d.ny, d.nz):
+            raise ValueError("restart file of another grid (the reference interpolates; not supported here)")
+        npass = self.nscal - 1 - (1 if self.iqt >= 0 else 0)
+        if h["nscal"] != npass:
+            raise ValueError(f"restart file holds {h['nscal']} passive scalars, the context {npass}")
+        scal = [r.fields["es"]]
+        it = iter(r.scal)
+        for q in range(1, self.nscal):
+            scal.append(r.fields["qt"] if q == self.iqt else next(it))
+        self.upload(State(r.fields["u"], r.fields["v"], r.fields["w"], r.fields["p"], r.fields["dens"], scal, self.iqt))
+        if h["dt"] != self.dt0:
+            self.set_dt(h["dt"])
+        return h
 
     # ---- SGS turbulence diffusion (subgrid.f90) ----
     def set_sgs(self, sgs, with_dif: bool = True) -> None:
@@ -80,6 +132,7 @@ class Mimica:
         fluxes of ``sgs`` (``None`` = zero)."""
         p, keep = sgs.params(self.domain.nz, with_dif)
         _lib.check(self._L.mg_set_sgs(self._h, C.byref(p)), "mg_set_sgs")
+        self._sgs_on = bool(with_dif)
         self.set_surface_fluxes(sgs.esflux, sgs.qvflux, sgs.mflux)
 
     def set_surface_fluxes(self, esflux=None, qvflux=None, mflux=None) -> None:

@@ -240,9 +240,10 @@ int mg_set_sgs(mg_ctx *ctx, const mg_sgs_params *sgs);
  * nx*ny, i fastest, the reference's 2-D layout; NULL = 0).  The SGS step reads them on
  * the device; call again whenever the caller's surface layer updates them. */
 int mg_set_surface_fluxes(mg_ctx *ctx, const double *esflux, const double *qvflux, const double *mflux);
-/* per-level factors (host, prof[q*nz + k-1]): q = 0 z0, 1 (C_s delta)**2, 2 pran < 0
- * damping, 3 f_an, 4 N2 coefficient, 5 N2 denominator, 6..9 the d/dz denominators of
- * grad_wind_3d (gradients.f90:884-905) for u, v, w and w at nz-1. */
+/* per-level factors (host, prof[q*nz + k-1], 11*nz values): q = 0 z0, 1 (C_s delta)**2,
+ * 2 pran < 0 damping, 3 f_an, 4 N2 coefficient, 5 N2 denominator, 6..9 the d/dz
+ * denominators of grad_wind_3d (gradients.f90:884-905) for u, v, w and w at nz-1,
+ * 10 the length scale delta (length_scale, subgrid.f90:1183-1232). */
 int mg_sgs_profiles(const mg_params *p, const mg_sgs_params *sgs, double *prof);
 /* unit entries, host arrays in the reference layout with periodic ghosts:
  *   mg_calc_subgrid: fkv := turbu%fkv from natural u, v, w, es (theta), qt (NULL = dry)
@@ -256,6 +257,10 @@ int mg_efud(mg_ctx *ctx, const double *u, const double *v, const double *w, cons
             const double *fkv, double *su, double *sv, double *sw);
 int mg_eff(mg_ctx *ctx, int kind, const double *dens, const double *fkv, const double *x,
            const double *flux_s, double *ec);
+/* turbu%ksgs = (turbu%fkv/(C_k delta))**2 (calc_smago, subgrid.f90:860) of the viscosity of
+ * the last step's level n, as savedata writes it when with_dif (restarting.f90:876-880);
+ * host array nx*ny*nz.  MG_ERR_STATE before the first step with SGS diffusion on. */
+int mg_download_ksgs(mg_ctx *ctx, double *ksgs);
 
 /* ---- tangent linear and adjoint of the scalar advection operator (WENO; no counterpart
  * in the reference, whose adjoint does not exist) ----

@@ -1691,6 +1691,7 @@ void mo_sgs_profiles(const mo_grid *g, double *prof)
     double *z0 = prof, *cs2d = prof + nz, *func = prof + 2 * nz, *fan = prof + 3 * nz;
     double *n2c = prof + 4 * nz, *n2d = prof + 5 * nz;
     double *du = prof + 6 * nz, *dv = prof + 7 * nz, *dw = prof + 8 * nz, *dwt = prof + 9 * nz;
+    double *dl = prof + 10 * nz;
     const int anis = s ? s->anis_k : 0;
     const double zdec = s ? s->zdec : 2000., zrough = s ? s->zrough : 0.01;
     for (int q = 0; q < MO_SGS_NPROF * nz; q++) prof[q] = 0.;
@@ -1703,6 +1704,7 @@ void mo_sgs_profiles(const mo_grid *g, double *prof)
         double delta = 1. / sqrt(1. / (deltas * deltas) + 1. / (l_d * l_d) + 1. / (l_z * l_z));
         double cd = SGS_CS * delta;
         P1(cs2d, k) = cd * cd;
+        P1(dl, k) = delta;
         P1(func, k) = dmax2(1. - exp(6. * (P1(z0, k) - zdec) / zdec), 0.);
         if (anis) {
             double t = pow(dx * dy, 1. / 2.) / (dz * P1(f, k));

@@ -110,8 +110,9 @@ int  mo_anelastic_pressure(const mo_grid *g, double *mu, double *mv, double *mw,
 /* ---- SGS turbulence (src/PHYS/subgrid.f90, src/TOOLS/gradients.f90) ----
  * Per-level profiles, prof[q*nz + k-1] for q = 0..MO_SGS_NPROF-1:
  * 0 z0, 1 (C_s*delta)**2, 2 damping func, 3 anisotropy f_an, 4 N2 coefficient,
- * 5 N2 denominator, 6..8 denominators of the 4th-order d/dz of u, v, w. */
-#define MO_SGS_NPROF 10
+ * 5 N2 denominator, 6..9 denominators of the 4th-order d/dz of u, v, w and w at
+ * nz-1, 10 the length scale delta. */
+#define MO_SGS_NPROF 11
 void mo_sgs_profiles(const mo_grid *g, double *prof);
 /* cal_dij: d[0..5] = d11, d22, d33, d12, d13, d23 (cell centred, full arrays) */
 void mo_cal_dij(const mo_grid *g, const double *u, const double *v, const double *w, double *const *d);

@@ -31,7 +31,7 @@ class MoSgs(C.Structure):
     ]
 
 
-SGS_NPROF = 10
+SGS_NPROF = 11
 
 
 class MoGrid(C.Structure):
