@@ -123,6 +123,8 @@ def lib() -> C.CDLL:
         L.mg_cfl_dt.argtypes = [C.POINTER(MgCheckParams), C.c_double, C.c_double, _dp, C.POINTER(C.c_int)]
         L.mg_set_dt.argtypes = [vp, C.c_double]
         L.mg_download_ksgs.argtypes = [vp, _dp]
+        L.mg_qnadv_tl.argtypes = [vp, C.c_int] + [_dp] * 12
+        L.mg_qnadv_ad.argtypes = [vp, C.c_int] + [_dp] * 9
         L.mg_set_sgs.argtypes = [vp, C.POINTER(MgSgsParams)]
         L.mg_set_surface_fluxes.argtypes = [vp, _dp, _dp, _dp]
         L.mg_sgs_profiles.argtypes = [C.POINTER(MgParams), C.POINTER(MgSgsParams), _dp]
@@ -161,5 +163,5 @@ EXPORTED = [
     "mg_fft_solve", "mg_anelastic_pressure", "mg_time_steps", "mg_profile_enable", "mg_profile_report",
     "mg_advection_tl", "mg_advection_ad", "mg_anelastic_pressure_ad", "mg_time_adjoint", "mg_ensemble_create", "mg_ensemble_destroy", "mg_ensemble_step", "mg_ensemble_time_steps", "mg_ensemble_launch_count",
     "mg_set_sgs", "mg_set_surface_fluxes", "mg_sgs_profiles", "mg_calc_subgrid", "mg_efud", "mg_eff",
-    "mg_checkall", "mg_cfl_dt", "mg_set_dt", "mg_download_ksgs",
+    "mg_checkall", "mg_cfl_dt", "mg_set_dt", "mg_download_ksgs", "mg_qnadv_tl", "mg_qnadv_ad",
 ]

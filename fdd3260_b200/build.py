@@ -41,6 +41,7 @@ SOURCES = [
     ("k_adjoint.cu", ["-fmad=false"]),
     ("k_sgs.cu", ["-fmad=false", "-Xcompiler", "-ffp-contract=off"]),
     ("k_check.cu", ["-fmad=false"]),
+    ("k_momadj.cu", ["-fmad=false"]),
 ]
 
 

@@ -50,6 +50,7 @@ struct mg_ctx {
     int gsteps[2] = {0, 0};
     long long gen = 0;                   // bumped whenever recorded step graphs go stale
     void *chk = nullptr;                 // scratch of the per-step checks
+    void *momplan = nullptr;             // input offsets of the momentum-advection adjoint
     // SGS diffusion (mg_set_sgs): per-level factors + qt0 on the device, the
     // deformation tensor and eddy viscosity of level n, the stored tendencies
     mg_sgs_params sgsp{};
@@ -245,6 +246,7 @@ static void free_ctx(mg_ctx *c)
     for (int f = 0; f < MG_MAXF; f++) { cudaFree(c->sA[f]); cudaFree(c->sB[f]); cudaFree(c->ts[f]); }
     for (int i = 0; i < 16; i++) cudaFree(c->unit[i]);
     cudaFree(c->sgs_prof); cudaFree(c->fkv); cudaFree(c->sfe); cudaFree(c->snut); cudaFree(c->chk);
+    mom_adj_plan_destroy(c->momplan);
     for (int q = 0; q < 6; q++) cudaFree(c->dij[q]);
     for (int q = 0; q < 3; q++) { cudaFree(c->sgm[q]); cudaFree(c->sfc[q]); }
     for (int f = 0; f < MG_MAXF; f++) cudaFree(c->sgsc[f]);
@@ -1144,6 +1146,56 @@ extern "C" int mg_eff(mg_ctx *c, int kind, const double *dens, const double *fkv
     CKR(launch_sgs_prep(c->G, S, c->unit[0], c->unit[1], c->sfe, c->snut, c->stream));
     CKR(launch_sgs_scal(c->G, S, c->snut, A, c->stream));
     CKR(d2h(c, ec, c->unit[3], cudaMemcpyDeviceToHost));
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+// ---- tangent linear and adjoint of the momentum advection operator ----
+extern "C" int mg_qnadv_tl(mg_ctx *c, int ntime, const double *mu, const double *mv, const double *mw,
+                           const double *dmu, const double *dmv, const double *dmw, double *au, double *av, double *aw,
+                           double *dau, double *dav, double *daw)
+{
+    if (!c || !mu || !mv || !mw || !dmu || !dmv || !dmw || !dau || !dav || !daw) return MG_ERR_PARAM;
+    if (c->G.nz < 5) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    int rc = ensure_unit(c, 12);
+    if (rc) return rc;
+    const double *in[6] = {mu, mv, mw, dmu, dmv, dmw};
+    for (int q = 0; q < 6; q++) CKR(h2d(c, c->unit[q], in[q], cudaMemcpyHostToDevice));
+    for (int q = 6; q < 12; q++) CKR(cudaMemsetAsync(c->unit[q], 0, c->fbytes, c->stream));
+    CKR(launch_qnadv_tl(c->G, ntime, c->unit[0], c->unit[1], c->unit[2], c->unit[3], c->unit[4], c->unit[5],
+                        au ? c->unit[6] : nullptr, av ? c->unit[7] : nullptr, aw ? c->unit[8] : nullptr, c->unit[9],
+                        c->unit[10], c->unit[11], c->stream));
+    double *outs[6] = {au, av, aw, dau, dav, daw};
+    for (int q = 0; q < 6; q++)
+        if (outs[q]) CKR(d2h(c, outs[q], c->unit[6 + q], cudaMemcpyDeviceToHost));
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+static int ensure_momplan(mg_ctx *c, const double *mu, const double *mv, const double *mw)
+{
+    if (c->momplan) return MG_OK;
+    return cuerr(mom_adj_plan(c->G, 1, mu, mv, mw, &c->momplan, c->stream));
+}
+
+extern "C" int mg_qnadv_ad(mg_ctx *c, int ntime, const double *mu, const double *mv, const double *mw,
+                           const double *aubar, const double *avbar, const double *awbar, double *mubar, double *mvbar,
+                           double *mwbar)
+{
+    if (!c || !mu || !mv || !mw || !aubar || !avbar || !awbar || !mubar || !mvbar || !mwbar) return MG_ERR_PARAM;
+    if (c->G.nz < 5) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    int rc = ensure_unit(c, 9);
+    if (rc) return rc;
+    const double *in[6] = {mu, mv, mw, aubar, avbar, awbar};
+    for (int q = 0; q < 6; q++) CKR(h2d(c, c->unit[q], in[q], cudaMemcpyHostToDevice));
+    for (int q = 6; q < 9; q++) CKR(cudaMemsetAsync(c->unit[q], 0, c->fbytes, c->stream));
+    rc = ensure_momplan(c, c->unit[0], c->unit[1], c->unit[2]);
+    if (rc) return rc;
+    CKR(launch_qnadv_ad(c->G, c->momplan, ntime, c->unit[0], c->unit[1], c->unit[2], c->unit[3], c->unit[4], c->unit[5],
+                        c->unit[6], c->unit[7], c->unit[8], c->stream));
+    CKR(d2h(c, mubar, c->unit[6], cudaMemcpyDeviceToHost));
+    CKR(d2h(c, mvbar, c->unit[7], cudaMemcpyDeviceToHost));
+    CKR(d2h(c, mwbar, c->unit[8], cudaMemcpyDeviceToHost));
     return cuerr(cudaStreamSynchronize(c->stream));
 }
 

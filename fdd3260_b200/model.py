@@ -226,6 +226,25 @@ class Mimica:
                    "mg_advection_ad")
         return tuple(outs)
 
+    def qnadv_tl(self, mu, mv, mw, dmu, dmv, dmw, ntime: int = 1, values: bool = False):
+        """Tangent linear of qnadv_uvw at (mu, mv, mw) along (dmu, dmv, dmw); with values,
+        also the operator itself (the per-cell form the adjoint differentiates)."""
+        d = self.domain
+        c = [np.ascontiguousarray(a, dtype=np.float64) for a in (mu, mv, mw, dmu, dmv, dmw)]
+        outs = [np.zeros(d.shape) for _ in range(6)]
+        vals = outs[:3] if values else [None] * 3
+        _lib.check(self._L.mg_qnadv_tl(self._h, ntime, *[_lib.ptr(a) for a in c], *[_lib.ptr(a) for a in vals],
+                                       *[_lib.ptr(a) for a in outs[3:]]), "mg_qnadv_tl")
+        return (tuple(outs[:3]), tuple(outs[3:])) if values else tuple(outs[3:])
+
+    def qnadv_ad(self, mu, mv, mw, aub, avb, awb, ntime: int = 1):
+        d = self.domain
+        c = [np.ascontiguousarray(a, dtype=np.float64) for a in (mu, mv, mw, aub, avb, awb)]
+        outs = [np.zeros(d.shape) for _ in range(3)]
+        _lib.check(self._L.mg_qnadv_ad(self._h, ntime, *[_lib.ptr(a) for a in c], *[_lib.ptr(a) for a in outs]),
+                   "mg_qnadv_ad")
+        return tuple(outs)
+
     def anelastic_pressure_ad(self, mub, mvb, mwb, pb):
         """Adjoint of anelastic_pressure (the momentum/pressure map): returns (mub, mvb, mwb, pb)."""
         io = [np.array(a, dtype=np.float64, copy=True) for a in (mub, mvb, mwb, pb)]

@@ -278,6 +278,21 @@ int mg_advection_tl(mg_ctx *ctx, const double *x, const double *mu, const double
 int mg_advection_ad(mg_ctx *ctx, const double *x, const double *mu, const double *mv, const double *mw,
                     const double *Abar, double *xbar, double *mubar, double *mvbar, double *mwbar);
 
+/* ---- tangent linear and adjoint of qnadv_uvw (windadv.f90:46-1127; no counterpart in the
+ * reference) ----  The momentum advection tendency (au, av, aw) = qnadv(m) of
+ * mg_qnadv_uvw as a function of the momentum, its advective velocities m/rho0 - shift
+ * included; the artificial viscosity's |u| is differentiated along its sign.
+ *   mg_qnadv_tl: (dau, dav, daw) = dqnadv/dm . dm (interior); au, av, aw (may be NULL)
+ *                receive the operator itself from the same per-cell form.
+ *   mg_qnadv_ad: mbar = (dqnadv/dm)^T abar (overwritten; ghost adjoints folded onto the
+ *                interior cells they copy, so ghost entries are 0). */
+int mg_qnadv_tl(mg_ctx *ctx, int ntime, const double *mu, const double *mv, const double *mw,
+                const double *dmu, const double *dmv, const double *dmw, double *au, double *av, double *aw,
+                double *dau, double *dav, double *daw);
+int mg_qnadv_ad(mg_ctx *ctx, int ntime, const double *mu, const double *mv, const double *mw,
+                const double *aubar, const double *avbar, const double *awbar, double *mubar, double *mvbar,
+                double *mwbar);
+
 /* Adjoint of anelastic_pressure (pressure_solver.f90:73-140: nsubp passes of solve +
  * correction, then the level-mean removal of w) as a map of the momentum and pressure;
  * the map is affine (linear in m), so its tangent linear is mg_anelastic_pressure itself.
