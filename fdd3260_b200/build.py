@@ -42,6 +42,7 @@ SOURCES = [
     ("k_sgs.cu", ["-fmad=false", "-Xcompiler", "-ffp-contract=off"]),
     ("k_check.cu", ["-fmad=false"]),
     ("k_momadj.cu", ["-fmad=false"]),
+    ("k_traj.cu", ["-fmad=false"]),
 ]
 
 

@@ -14,6 +14,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <new>
 #include <vector>
 
@@ -1196,6 +1197,537 @@ extern "C" int mg_qnadv_ad(mg_ctx *c, int ntime, const double *mu, const double 
     CKR(d2h(c, mubar, c->unit[6], cudaMemcpyDeviceToHost));
     CKR(d2h(c, mvbar, c->unit[7], cudaMemcpyDeviceToHost));
     CKR(d2h(c, mwbar, c->unit[8], cudaMemcpyDeviceToHost));
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+// ---------------- trajectory tangent linear and adjoint ----------------
+// The FP64 step as a composition the linearisation follows: unit-mode K1 (advection
+// tendencies of all scalar fields), unit-mode K2 (qnadv), the stage glue of k_traj.cu
+// and the projection; natural <-> stage variables at the ends of the step.  The
+// adjoint recomputes each step's two stages from stored step-start states: states are
+// checkpointed every ckpt steps, and a segment is recomputed forward before it is
+// swept backward.  Scope: FP64 contexts, WENO scalars, SGS diffusion off.
+namespace {
+
+struct TrajBufs {
+    mg_ctx *c = nullptr;
+    std::vector<double *> own;
+    cudaError_t err = cudaSuccess;
+    double *get()
+    {
+        double *p = nullptr;
+        if (err == cudaSuccess) err = cudaMalloc(&p, c->fbytes);
+        if (err == cudaSuccess) err = cudaMemsetAsync(p, 0, c->fbytes, c->stream);
+        if (err == cudaSuccess) own.push_back(p);
+        return p;
+    }
+    ~TrajBufs()
+    {
+        if (c) cudaStreamSynchronize(c->stream);
+        for (double *p : own) cudaFree(p);
+    }
+};
+
+// natural state: m[0..2] = u, v, w; p; s[0] = density, s[1..nf-1] = scalars
+struct NatState {
+    double *m[3] = {};
+    double *p = nullptr;
+    double *s[MG_MAXF] = {};
+};
+
+// what a stage's tangent linear and adjoint need besides the level-n state
+struct StageRec {
+    double *xs[MG_MAXF] = {};   // scalar inputs (field 0: density)
+    double *xm[3] = {};         // momentum inputs
+    double *A[MG_MAXF] = {};    // advection tendencies of the inputs
+};
+
+NatState nat_alloc(TrajBufs &B, int nf)
+{
+    NatState n;
+    for (int q = 0; q < 3; q++) n.m[q] = B.get();
+    n.p = B.get();
+    for (int f = 0; f < nf; f++) n.s[f] = B.get();
+    return n;
+}
+
+cudaError_t nat_copy(mg_ctx *c, const NatState &dst, const NatState &src, int nf)
+{
+    cudaError_t e = cudaSuccess;
+    for (int q = 0; q < 3 && e == cudaSuccess; q++)
+        e = cudaMemcpyAsync(dst.m[q], src.m[q], c->fbytes, cudaMemcpyDeviceToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dst.p, src.p, c->fbytes, cudaMemcpyDeviceToDevice, c->stream);
+    for (int f = 0; f < nf && e == cudaSuccess; f++)
+        e = cudaMemcpyAsync(dst.s[f], src.s[f], c->fbytes, cudaMemcpyDeviceToDevice, c->stream);
+    return e;
+}
+
+cudaError_t nat_zero(mg_ctx *c, const NatState &n, int nf)
+{
+    cudaError_t e = cudaSuccess;
+    for (int q = 0; q < 3 && e == cudaSuccess; q++) e = cudaMemsetAsync(n.m[q], 0, c->fbytes, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(n.p, 0, c->fbytes, c->stream);
+    for (int f = 0; f < nf && e == cudaSuccess; f++) e = cudaMemsetAsync(n.s[f], 0, c->fbytes, c->stream);
+    return e;
+}
+
+}  // namespace
+
+// projection of (mu, mv, mw) with the pressure p, FP64, no diagnostics
+static cudaError_t traj_project(mg_ctx *c, double *mu, double *mv, double *mw, double *p)
+{
+    double *psave = c->p;
+    c->p = p;
+    int launches = 0;
+    cudaError_t e = project(c, mu, mv, mw, mw, -1, 0, 0, 0, &launches);
+    c->p = psave;
+    return e;
+}
+
+// one stage forward from R (xs, xm filled): R.A, tm/ts (in: previous stage's, out: this
+// stage's), p (in/out: projected), outputs xs_out, xm_out
+static cudaError_t traj_stage_fwd(mg_ctx *c, int ntime, int stage, const NatState &N, StageRec &R, double *const *ts,
+                                  double *const *tm, double *p, double *const *xs_out, double *const *xm_out,
+                                  double *const *au)
+{
+    const DevGrid &G = c->G;
+    const int nf = c->nf;
+    const int iqt = c->prm.iqt >= 0 ? 1 + c->prm.iqt : -1;
+    const double a_dt = (stage == 1 ? 1. : 0.5) * G.dt0, b = stage == 1 ? 0. : 1.;
+    cudaError_t e = cudaSuccess;
+    for (int f = 0; f < nf && e == cudaSuccess; f++) e = cudaMemsetAsync(R.A[f], 0, c->fbytes, c->stream);
+    for (int q = 0; q < 3 && e == cudaSuccess; q++) e = cudaMemsetAsync(au[q], 0, c->fbytes, c->stream);
+    if (e != cudaSuccess) return e;
+    // advection tendencies of every scalar field (K1 unit mode)
+    K1Args a1{};
+    a1.nf = nf; a1.dens_first = 0; a1.stage = 0; a1.mode = 1; a1.err = c->derr;
+    for (int f = 0; f < nf; f++) { a1.xin[f] = R.xs[f]; a1.xold[f] = R.xs[f]; a1.xout[f] = R.A[f]; }
+    a1.mw = R.xm[2];
+    K1Maps maps;
+    const double *xv[MG_MAXF];
+    for (int f = 0; f < nf; f++) xv[f] = R.xs[f];
+    if (build_maps(c, xv, nf, R.xm[0], R.xm[1], &maps)) return cudaErrorInvalidValue;
+    if ((e = launch_k1(G, a1, maps, c->stream)) != cudaSuccess) return e;
+    // momentum advection (K2 unit mode)
+    K2Args a2{};
+    a2.ntime = ntime; a2.mode = 1; a2.in_is_leveln = 0; a2.rep = REP_NAT;
+    a2.mu = R.xm[0]; a2.mv = R.xm[1]; a2.mw = R.xm[2];
+    a2.ou = au[0]; a2.ov = au[1]; a2.ow = au[2];
+    a2.err = c->derr;
+    K2Maps mm;
+    const double *m3[3] = {R.xm[0], R.xm[1], R.xm[2]};
+    if (build_mom_maps(c, m3, &mm)) return cudaErrorInvalidValue;
+    if ((e = launch_k2(G, a2, mm, c->stream)) != cudaSuccess) return e;
+    // momentum assembly and update
+    TrajMomArgs A{};
+    A.v[TM_P] = p; A.v[TM_MW] = R.xm[2]; A.v[TM_RHO] = R.xs[0]; A.v[TM_ES] = R.xs[1]; A.v[TM_AES] = R.A[1];
+    A.v[TM_QT] = iqt >= 0 ? R.xs[iqt] : nullptr; A.v[TM_AQT] = iqt >= 0 ? R.A[iqt] : nullptr;
+    A.v[TM_AU] = au[0]; A.v[TM_AV] = au[1]; A.v[TM_AW] = au[2];
+    A.v[TM_TU] = tm[0]; A.v[TM_TV] = tm[1]; A.v[TM_TW] = tm[2];
+    A.v[TM_UN] = N.m[0]; A.v[TM_VN] = N.m[1]; A.v[TM_WN] = N.m[2];
+    A.out[0] = tm[0]; A.out[1] = tm[1]; A.out[2] = tm[2];
+    A.out[3] = xm_out[0]; A.out[4] = xm_out[1]; A.out[5] = xm_out[2];
+    A.a_dt = a_dt; A.b = b;
+    if ((e = launch_stage_mom(G, A, 0, c->stream)) != cudaSuccess) return e;
+    // scalar update
+    TrajScalArgs S{};
+    S.nf = nf; S.rhon = N.s[0]; S.a_dt = a_dt; S.b = b;
+    for (int f = 0; f < nf; f++) {
+        S.adv[f] = R.A[f]; S.tprev[f] = ts[f]; S.sn[f] = N.s[f]; S.tout[f] = ts[f]; S.out[f] = xs_out[f];
+    }
+    if ((e = launch_stage_scal(G, S, 0, c->stream)) != cudaSuccess) return e;
+    double *hm[3] = {xm_out[0], xm_out[1], xm_out[2]};
+    if ((e = launch_halo_fill(G, hm, 3, c->stream)) != cudaSuccess) return e;
+    if ((e = launch_halo_fill(G, xs_out, nf, c->stream)) != cudaSuccess) return e;
+    return traj_project(c, xm_out[0], xm_out[1], xm_out[2], p);
+}
+
+// natural state -> stage-1 inputs (m = u rho0, psi = s rho; the density itself)
+static cudaError_t traj_to_stage(mg_ctx *c, const NatState &N, StageRec &R)
+{
+    TrajConv V{};
+    V.dir = 0; V.ns = c->nf - 1; V.rho = N.s[0];
+    for (int q = 0; q < 3; q++) { V.in[q] = N.m[q]; V.out[q] = R.xm[q]; }
+    for (int f = 1; f < c->nf; f++) { V.in[2 + f] = N.s[f]; V.out[2 + f] = R.xs[f]; }
+    cudaError_t e = launch_convert(c->G, V, 0, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(R.xs[0], N.s[0], c->fbytes, cudaMemcpyDeviceToDevice, c->stream);
+    return e;
+}
+
+// one step forward: N -> Nout (may alias nothing); R1, R2 receive the stages' records
+static cudaError_t traj_step_fwd(mg_ctx *c, int ntime, const NatState &N, const NatState &Nout, StageRec &R1,
+                                 StageRec &R2, double *const *ts, double *const *tm, double *const *au)
+{
+    const int nf = c->nf;
+    cudaError_t e = traj_to_stage(c, N, R1);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(Nout.p, N.p, c->fbytes, cudaMemcpyDeviceToDevice, c->stream);
+    if (e != cudaSuccess) return e;
+    if ((e = traj_stage_fwd(c, ntime, 1, N, R1, ts, tm, Nout.p, R2.xs, R2.xm, au)) != cudaSuccess) return e;
+    // stage 2 writes its outputs into Nout's buffers (stage variables), converted below
+    if ((e = traj_stage_fwd(c, ntime, 2, N, R2, ts, tm, Nout.p, Nout.s, Nout.m, au)) != cudaSuccess) return e;
+    TrajConv V{};
+    V.dir = 1; V.ns = nf - 1; V.rho = Nout.s[0];
+    for (int q = 0; q < 3; q++) { V.in[q] = Nout.m[q]; V.out[q] = Nout.m[q]; }
+    for (int f = 1; f < nf; f++) { V.in[2 + f] = Nout.s[f]; V.out[2 + f] = Nout.s[f]; }
+    if ((e = launch_convert(c->G, V, 0, c->stream)) != cudaSuccess) return e;
+    double *hm[3] = {Nout.m[0], Nout.m[1], Nout.m[2]};
+    if ((e = launch_halo_fill(c->G, hm, 3, c->stream)) != cudaSuccess) return e;
+    return launch_halo_fill(c->G, Nout.s, nf, c->stream);
+}
+
+// tangent of one stage (values of the stage, R and N, computed by traj_stage_fwd first)
+static cudaError_t traj_stage_tl(mg_ctx *c, int ntime, int stage, const NatState &N, const NatState &dN,
+                                 const StageRec &R, const StageRec &dR, double *const *ts, double *const *dts,
+                                 double *const *tm, double *const *dtm, double *p, double *dp,
+                                 double *const *dxs_out, double *const *dxm_out, double *const *dau)
+{
+    const DevGrid &G = c->G;
+    const int nf = c->nf;
+    const int iqt = c->prm.iqt >= 0 ? 1 + c->prm.iqt : -1;
+    const double a_dt = (stage == 1 ? 1. : 0.5) * G.dt0, b = stage == 1 ? 0. : 1.;
+    cudaError_t e = cudaSuccess;
+    for (int f = 0; f < nf && e == cudaSuccess; f++) {
+        e = cudaMemsetAsync(dR.A[f], 0, c->fbytes, c->stream);
+        if (e == cudaSuccess)
+            e = launch_advection_tl(G, R.xs[f], R.xm[0], R.xm[1], R.xm[2], dR.xs[f], dR.xm[0], dR.xm[1], dR.xm[2], dR.A[f],
+                                    c->stream);
+    }
+    for (int q = 0; q < 3 && e == cudaSuccess; q++) e = cudaMemsetAsync(dau[q], 0, c->fbytes, c->stream);
+    if (e == cudaSuccess)
+        e = launch_qnadv_tl(G, ntime, R.xm[0], R.xm[1], R.xm[2], dR.xm[0], dR.xm[1], dR.xm[2], nullptr, nullptr, nullptr,
+                            dau[0], dau[1], dau[2], c->stream);
+    if (e != cudaSuccess) return e;
+    TrajMomArgs A{};
+    A.v[TM_P] = p; A.v[TM_MW] = R.xm[2]; A.v[TM_RHO] = R.xs[0]; A.v[TM_ES] = R.xs[1]; A.v[TM_AES] = R.A[1];
+    A.v[TM_QT] = iqt >= 0 ? R.xs[iqt] : nullptr; A.v[TM_AQT] = iqt >= 0 ? R.A[iqt] : nullptr;
+    A.v[TM_AU] = dau[0]; A.v[TM_AV] = dau[1]; A.v[TM_AW] = dau[2];   // values unused (linear term)
+    A.v[TM_TU] = tm[0]; A.v[TM_TV] = tm[1]; A.v[TM_TW] = tm[2];
+    A.v[TM_UN] = N.m[0]; A.v[TM_VN] = N.m[1]; A.v[TM_WN] = N.m[2];
+    A.d[TM_P] = dp; A.d[TM_MW] = dR.xm[2]; A.d[TM_RHO] = dR.xs[0]; A.d[TM_ES] = dR.xs[1]; A.d[TM_AES] = dR.A[1];
+    A.d[TM_QT] = iqt >= 0 ? dR.xs[iqt] : nullptr; A.d[TM_AQT] = iqt >= 0 ? dR.A[iqt] : nullptr;
+    A.d[TM_AU] = dau[0]; A.d[TM_AV] = dau[1]; A.d[TM_AW] = dau[2];
+    A.d[TM_TU] = dtm[0]; A.d[TM_TV] = dtm[1]; A.d[TM_TW] = dtm[2];
+    A.d[TM_UN] = dN.m[0]; A.d[TM_VN] = dN.m[1]; A.d[TM_WN] = dN.m[2];
+    for (int q = 0; q < 3; q++) { A.dout[q] = dtm[q]; A.dout[3 + q] = dxm_out[q]; }
+    A.a_dt = a_dt; A.b = b;
+    if ((e = launch_stage_mom(G, A, 1, c->stream)) != cudaSuccess) return e;
+    TrajScalArgs S{};
+    S.nf = nf; S.rhon = N.s[0]; S.drhon = dN.s[0]; S.a_dt = a_dt; S.b = b;
+    for (int f = 0; f < nf; f++) {
+        S.adv[f] = R.A[f]; S.dadv[f] = dR.A[f]; S.tprev[f] = ts[f]; S.dtprev[f] = dts[f];
+        S.sn[f] = N.s[f]; S.dsn[f] = dN.s[f]; S.dtout[f] = dts[f]; S.dout[f] = dxs_out[f];
+    }
+    if ((e = launch_stage_scal(G, S, 1, c->stream)) != cudaSuccess) return e;
+    double *hm[3] = {dxm_out[0], dxm_out[1], dxm_out[2]};
+    if ((e = launch_halo_fill(G, hm, 3, c->stream)) != cudaSuccess) return e;
+    if ((e = launch_halo_fill(G, dxs_out, nf, c->stream)) != cudaSuccess) return e;
+    return traj_project(c, dxm_out[0], dxm_out[1], dxm_out[2], dp);
+}
+
+// tangent of one step: (N, dN) -> (Nout, dNout)
+static cudaError_t traj_step_tl(mg_ctx *c, int ntime, const NatState &N, const NatState &dN, const NatState &Nout,
+                                const NatState &dNout, StageRec &R1, StageRec &R2, StageRec &dR1, StageRec &dR2,
+                                double *const *ts, double *const *tm, double *const *dts, double *const *dtm,
+                                double *const *au)
+{
+    const int nf = c->nf;
+    cudaError_t e = traj_to_stage(c, N, R1);
+    if (e != cudaSuccess) return e;
+    {
+        TrajConv V{};
+        V.dir = 0; V.ns = nf - 1; V.rho = N.s[0]; V.drho = dN.s[0];
+        for (int q = 0; q < 3; q++) { V.in[q] = N.m[q]; V.din[q] = dN.m[q]; V.dout[q] = dR1.xm[q]; }
+        for (int f = 1; f < nf; f++) { V.in[2 + f] = N.s[f]; V.din[2 + f] = dN.s[f]; V.dout[2 + f] = dR1.xs[f]; }
+        if ((e = launch_convert(c->G, V, 1, c->stream)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(dR1.xs[0], dN.s[0], c->fbytes, cudaMemcpyDeviceToDevice, c->stream)) != cudaSuccess) return e;
+    }
+    if ((e = cudaMemcpyAsync(Nout.p, N.p, c->fbytes, cudaMemcpyDeviceToDevice, c->stream)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(dNout.p, dN.p, c->fbytes, cudaMemcpyDeviceToDevice, c->stream)) != cudaSuccess) return e;
+    if ((e = traj_stage_fwd(c, ntime, 1, N, R1, ts, tm, Nout.p, R2.xs, R2.xm, au)) != cudaSuccess) return e;
+    if ((e = traj_stage_tl(c, ntime, 1, N, dN, R1, dR1, ts, dts, tm, dtm, Nout.p, dNout.p, dR2.xs, dR2.xm, au)) != cudaSuccess)
+        return e;
+    if ((e = traj_stage_fwd(c, ntime, 2, N, R2, ts, tm, Nout.p, Nout.s, Nout.m, au)) != cudaSuccess) return e;
+    if ((e = traj_stage_tl(c, ntime, 2, N, dN, R2, dR2, ts, dts, tm, dtm, Nout.p, dNout.p, dNout.s, dNout.m, au)) != cudaSuccess)
+        return e;
+    // natural variables: tangent first (it needs the stage values), then the values
+    TrajConv V{};
+    V.dir = 1; V.ns = nf - 1; V.rho = Nout.s[0]; V.drho = dNout.s[0];
+    for (int q = 0; q < 3; q++) { V.in[q] = Nout.m[q]; V.din[q] = dNout.m[q]; V.dout[q] = dNout.m[q]; }
+    for (int f = 1; f < nf; f++) { V.in[2 + f] = Nout.s[f]; V.din[2 + f] = dNout.s[f]; V.dout[2 + f] = dNout.s[f]; }
+    if ((e = launch_convert(c->G, V, 1, c->stream)) != cudaSuccess) return e;
+    for (int q = 0; q < 3; q++) { V.out[q] = Nout.m[q]; V.dout[q] = nullptr; }
+    for (int f = 1; f < nf; f++) { V.out[2 + f] = Nout.s[f]; V.dout[2 + f] = nullptr; }
+    TrajConv W{};
+    W.dir = 1; W.ns = nf - 1; W.rho = Nout.s[0];
+    for (int q = 0; q < 3; q++) { W.in[q] = Nout.m[q]; W.out[q] = Nout.m[q]; }
+    for (int f = 1; f < nf; f++) { W.in[2 + f] = Nout.s[f]; W.out[2 + f] = Nout.s[f]; }
+    if ((e = launch_convert(c->G, W, 0, c->stream)) != cudaSuccess) return e;
+    double *hm[3] = {dNout.m[0], dNout.m[1], dNout.m[2]};
+    if ((e = launch_halo_fill(c->G, hm, 3, c->stream)) != cudaSuccess) return e;
+    double *hv[3] = {Nout.m[0], Nout.m[1], Nout.m[2]};
+    if ((e = launch_halo_fill(c->G, hv, 3, c->stream)) != cudaSuccess) return e;
+    if ((e = launch_halo_fill(c->G, dNout.s, nf, c->stream)) != cudaSuccess) return e;
+    return launch_halo_fill(c->G, Nout.s, nf, c->stream);
+}
+
+// adjoint of one stage; bars of the stage outputs (xm_bar after the projection, xs_bar) and
+// p_bar in; bars of the stage inputs (xs_in_bar, xm_in_bar, zeroed here) out, p_bar in place,
+// level-n bars Nbar accumulated, carries tcarry_in (from the later stage) / tcarry_out
+struct StageAdWork {
+    double *abar[3];
+    double *Abar[MG_MAXF];
+    double *tmp[4];
+    double *scratch[5];
+};
+
+static cudaError_t traj_stage_ad(mg_ctx *c, int ntime, int stage, const NatState &N, const NatState &Nbar,
+                                 const StageRec &R, double *const *xm_bar, double *const *xs_bar, double *p_bar,
+                                 double *const *xm_in_bar, double *const *xs_in_bar, double *const *tm_in,
+                                 double *const *ts_in, double *const *tm_out, double *const *ts_out, StageAdWork &W)
+{
+    const DevGrid &G = c->G;
+    const int nf = c->nf;
+    const int iqt = c->prm.iqt >= 0 ? 1 + c->prm.iqt : -1;
+    const double a_dt = (stage == 1 ? 1. : 0.5) * G.dt0, b = stage == 1 ? 0. : 1.;
+    cudaError_t e = pressure_adjoint(G, c->pp, c->prm.nsubp, xm_bar[0], xm_bar[1], xm_bar[2], p_bar, c->stream);
+    for (int q = 0; q < 3 && e == cudaSuccess; q++) {
+        e = cudaMemsetAsync(W.abar[q], 0, c->fbytes, c->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(xm_in_bar[q], 0, c->fbytes, c->stream);
+    }
+    for (int f = 0; f < nf && e == cudaSuccess; f++) {
+        e = cudaMemsetAsync(W.Abar[f], 0, c->fbytes, c->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(xs_in_bar[f], 0, c->fbytes, c->stream);
+    }
+    if (e != cudaSuccess) return e;
+    TrajMomAd M{};
+    for (int q = 0; q < 3; q++) {
+        M.mbar[q] = xm_bar[q]; M.tcarry[q] = tm_in ? tm_in[q] : nullptr; M.tprev_bar[q] = tm_out ? tm_out[q] : nullptr;
+        M.abar[q] = W.abar[q]; M.mnbar[q] = Nbar.m[q];
+    }
+    M.pbar = p_bar; M.mwin_bar = xm_in_bar[2];
+    M.rho = R.xs[0]; M.es = R.xs[1]; M.aes = R.A[1];
+    M.qt = iqt >= 0 ? R.xs[iqt] : nullptr; M.aqt = iqt >= 0 ? R.A[iqt] : nullptr;
+    M.rho_bar = xs_in_bar[0]; M.es_bar = xs_in_bar[1]; M.aes_bar = W.Abar[1];
+    M.qt_bar = iqt >= 0 ? xs_in_bar[iqt] : nullptr; M.aqt_bar = iqt >= 0 ? W.Abar[iqt] : nullptr;
+    M.a_dt = a_dt; M.b = b;
+    if ((e = launch_stage_mom_ad(G, M, c->stream)) != cudaSuccess) return e;
+    if ((e = launch_qnadv_ad(G, c->momplan, ntime, R.xm[0], R.xm[1], R.xm[2], W.abar[0], W.abar[1], W.abar[2],
+                             xm_in_bar[0], xm_in_bar[1], xm_in_bar[2], c->stream)) != cudaSuccess)
+        return e;
+    TrajScalAd S{};
+    S.nf = nf; S.rhon = N.s[0]; S.a_dt = a_dt; S.b = b;
+    for (int f = 0; f < nf; f++) {
+        S.psibar[f] = xs_bar[f]; S.tcarry[f] = ts_in ? ts_in[f] : nullptr; S.sn[f] = N.s[f];
+        S.advbar[f] = W.Abar[f]; S.tprev_bar[f] = ts_out ? ts_out[f] : nullptr; S.snbar[f] = Nbar.s[f];
+    }
+    if ((e = launch_stage_scal_ad(G, S, c->stream)) != cudaSuccess) return e;
+    for (int f = 0; f < nf; f++) {
+        if ((e = launch_advection_ad(G, R.xs[f], R.xm[0], R.xm[1], R.xm[2], W.Abar[f], W.tmp[0], W.tmp[1], W.tmp[2],
+                                     W.tmp[3], W.scratch, c->stream)) != cudaSuccess)
+            return e;
+        if ((e = launch_axpy(G, xs_in_bar[f], W.tmp[0], 1., c->stream)) != cudaSuccess) return e;
+        for (int q = 0; q < 3; q++)
+            if ((e = launch_axpy(G, xm_in_bar[q], W.tmp[1 + q], 1., c->stream)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+struct StepAdWork {
+    StageAdWork W;
+    double *xm2b[3], *xs2b[MG_MAXF], *xm1b[3], *xs1b[MG_MAXF], *xm0b[3], *xs0b[MG_MAXF], *pb;
+    double *tmc[3], *tsc[MG_MAXF];
+};
+
+// adjoint of one step: bar holds N_out-bar on entry and N-bar on exit; Nout = the step's
+// forward result from N (natural), R1/R2 its stage records
+static cudaError_t traj_step_ad(mg_ctx *c, int ntime, const NatState &N, const NatState &Nout, const StageRec &R1,
+                                const StageRec &R2, const NatState &bar, StepAdWork &S)
+{
+    const DevGrid &G = c->G;
+    const int nf = c->nf;
+    cudaError_t e = cudaSuccess;
+    // natural outputs -> stage-2 output bars
+    for (int q = 0; q < 3 && e == cudaSuccess; q++) e = cudaMemsetAsync(S.xm2b[q], 0, c->fbytes, c->stream);
+    for (int f = 1; f < nf && e == cudaSuccess; f++) e = cudaMemsetAsync(S.xs2b[f], 0, c->fbytes, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(S.xs2b[0], bar.s[0], c->fbytes, cudaMemcpyDeviceToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(S.pb, bar.p, c->fbytes, cudaMemcpyDeviceToDevice, c->stream);
+    if (e != cudaSuccess) return e;
+    {
+        TrajConvAd V{};
+        V.dir = 1; V.ns = nf - 1; V.rho = Nout.s[0]; V.rhobar = S.xs2b[0];
+        for (int q = 0; q < 3; q++) { V.outbar[q] = bar.m[q]; V.inbar[q] = S.xm2b[q]; }
+        for (int f = 1; f < nf; f++) { V.outbar[2 + f] = bar.s[f]; V.in[2 + f] = Nout.s[f]; V.inbar[2 + f] = S.xs2b[f]; }
+        if ((e = launch_convert_ad(G, V, c->stream)) != cudaSuccess) return e;
+    }
+    if ((e = nat_zero(c, bar, nf)) != cudaSuccess) return e;
+    if ((e = traj_stage_ad(c, ntime, 2, N, bar, R2, S.xm2b, S.xs2b, S.pb, S.xm1b, S.xs1b, nullptr, nullptr, S.tmc, S.tsc,
+                           S.W)) != cudaSuccess)
+        return e;
+    if ((e = traj_stage_ad(c, ntime, 1, N, bar, R1, S.xm1b, S.xs1b, S.pb, S.xm0b, S.xs0b, S.tmc, S.tsc, nullptr, nullptr,
+                           S.W)) != cudaSuccess)
+        return e;
+    // stage-1 inputs from the natural state
+    if ((e = launch_axpy(G, bar.s[0], S.xs0b[0], 1., c->stream)) != cudaSuccess) return e;
+    {
+        TrajConvAd V{};
+        V.dir = 0; V.ns = nf - 1; V.rho = N.s[0]; V.rhobar = bar.s[0];
+        for (int q = 0; q < 3; q++) { V.outbar[q] = S.xm0b[q]; V.inbar[q] = bar.m[q]; }
+        for (int f = 1; f < nf; f++) { V.outbar[2 + f] = S.xs0b[f]; V.in[2 + f] = N.s[f]; V.inbar[2 + f] = bar.s[f]; }
+        if ((e = launch_convert_ad(G, V, c->stream)) != cudaSuccess) return e;
+    }
+    return launch_axpy(G, bar.p, S.pb, 1., c->stream);
+}
+
+static int traj_check(mg_ctx *c)
+{
+    if (!c) return MG_ERR_PARAM;
+    if (!c->have_state) return MG_ERR_STATE;
+    if (c->prm.precision != MG_PREC_FP64 || c->prm.scal_adv != MG_WENO || c->sgs_on || c->G.nz < 5) return MG_ERR_PARAM;
+    return MG_OK;
+}
+
+static NatState traj_resident(mg_ctx *c)
+{
+    NatState n;
+    for (int q = 0; q < 3; q++) n.m[q] = c->mA[q];
+    n.p = c->p;
+    for (int f = 0; f < c->nf; f++) n.s[f] = c->sA[f];
+    return n;
+}
+
+static cudaError_t nat_h2d(mg_ctx *c, const NatState &n, const double *const *h)
+{
+    cudaError_t e = cudaSuccess;
+    for (int q = 0; q < 3 && e == cudaSuccess; q++) e = h2d(c, n.m[q], h[q], cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = h2d(c, n.p, h[3], cudaMemcpyHostToDevice);
+    for (int f = 0; f < c->nf && e == cudaSuccess; f++) e = h2d(c, n.s[f], h[4 + f], cudaMemcpyHostToDevice);
+    return e;
+}
+
+static cudaError_t nat_d2h(mg_ctx *c, double *const *h, const NatState &n)
+{
+    cudaError_t e = cudaSuccess;
+    for (int q = 0; q < 3 && e == cudaSuccess; q++) e = d2h(c, h[q], n.m[q], cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = d2h(c, h[3], n.p, cudaMemcpyDeviceToHost);
+    for (int f = 0; f < c->nf && e == cudaSuccess; f++) e = d2h(c, h[4 + f], n.s[f], cudaMemcpyDeviceToHost);
+    return e;
+}
+
+struct TrajCtx {
+    TrajBufs B;
+    StageRec R1, R2, dR1, dR2;
+    double *ts[MG_MAXF], *tm[3], *dts[MG_MAXF], *dtm[3], *au[3];
+    void init(mg_ctx *c, bool tangent)
+    {
+        B.c = c;
+        const int nf = c->nf;
+        for (StageRec *R : {&R1, &R2}) {
+            for (int f = 0; f < nf; f++) { R->xs[f] = B.get(); R->A[f] = B.get(); }
+            for (int q = 0; q < 3; q++) R->xm[q] = B.get();
+        }
+        for (int f = 0; f < nf; f++) ts[f] = B.get();
+        for (int q = 0; q < 3; q++) { tm[q] = B.get(); au[q] = B.get(); }
+        if (tangent) {
+            for (StageRec *R : {&dR1, &dR2}) {
+                for (int f = 0; f < nf; f++) { R->xs[f] = B.get(); R->A[f] = B.get(); }
+                for (int q = 0; q < 3; q++) R->xm[q] = B.get();
+            }
+            for (int f = 0; f < nf; f++) dts[f] = B.get();
+            for (int q = 0; q < 3; q++) dtm[q] = B.get();
+        }
+    }
+};
+
+extern "C" int mg_traj_forward(mg_ctx *c, int nsteps, int ntime0)
+{
+    int rc = traj_check(c);
+    if (rc) return rc;
+    if (nsteps < 0) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    TrajCtx T;
+    T.init(c, false);
+    const NatState res = traj_resident(c);
+    NatState a = nat_alloc(T.B, c->nf), b = nat_alloc(T.B, c->nf);
+    CKR(T.B.err);
+    CKR(nat_copy(c, a, res, c->nf));
+    for (int s = 0; s < nsteps; s++) {
+        CKR(traj_step_fwd(c, ntime0 + s, a, b, T.R1, T.R2, T.ts, T.tm, T.au));
+        std::swap(a, b);
+    }
+    CKR(nat_copy(c, res, a, c->nf));
+    c->rep = REP_NAT;
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+extern "C" int mg_traj_tl(mg_ctx *c, int nsteps, int ntime0, const double *const *dx0, double *const *dxT)
+{
+    int rc = traj_check(c);
+    if (rc) return rc;
+    if (nsteps < 0 || !dx0 || !dxT) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    TrajCtx T;
+    T.init(c, true);
+    NatState a = nat_alloc(T.B, c->nf), b = nat_alloc(T.B, c->nf), da = nat_alloc(T.B, c->nf), db = nat_alloc(T.B, c->nf);
+    CKR(T.B.err);
+    CKR(nat_copy(c, a, traj_resident(c), c->nf));
+    CKR(nat_h2d(c, da, dx0));
+    for (int s = 0; s < nsteps; s++) {
+        CKR(traj_step_tl(c, ntime0 + s, a, da, b, db, T.R1, T.R2, T.dR1, T.dR2, T.ts, T.tm, T.dts, T.dtm, T.au));
+        std::swap(a, b);
+        std::swap(da, db);
+    }
+    CKR(nat_d2h(c, dxT, da));
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+extern "C" int mg_traj_adjoint(mg_ctx *c, int nsteps, int ntime0, int ckpt, const double *const *lamT, double *const *g0)
+{
+    int rc = traj_check(c);
+    if (rc) return rc;
+    if (nsteps < 0 || ckpt < 1 || !lamT || !g0) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    rc = ensure_momplan(c, c->mA[0], c->mA[1], c->mA[2]);
+    if (rc) return rc;
+    const int nf = c->nf;
+    TrajCtx T;
+    T.init(c, false);
+    StepAdWork S{};
+    for (int q = 0; q < 3; q++) {
+        S.W.abar[q] = T.B.get(); S.xm2b[q] = T.B.get(); S.xm1b[q] = T.B.get(); S.xm0b[q] = T.B.get(); S.tmc[q] = T.B.get();
+    }
+    for (int f = 0; f < nf; f++) {
+        S.W.Abar[f] = T.B.get(); S.xs2b[f] = T.B.get(); S.xs1b[f] = T.B.get(); S.xs0b[f] = T.B.get(); S.tsc[f] = T.B.get();
+    }
+    for (int q = 0; q < 4; q++) S.W.tmp[q] = T.B.get();
+    for (int q = 0; q < 5; q++) S.W.scratch[q] = T.B.get();
+    S.pb = T.B.get();
+    // checkpoints (natural states every ckpt steps) and the states of one segment
+    const int nck = nsteps / ckpt + 1;
+    std::vector<NatState> ck(nck), seg(ckpt + 1);
+    for (int q = 0; q < nck; q++) ck[q] = nat_alloc(T.B, nf);
+    for (int q = 0; q <= ckpt; q++) seg[q] = nat_alloc(T.B, nf);
+    NatState bar = nat_alloc(T.B, nf), tmp = nat_alloc(T.B, nf);
+    CKR(T.B.err);
+    CKR(nat_copy(c, ck[0], traj_resident(c), nf));
+    for (int s = 0; s < nsteps; s++) {   // forward sweep: keep every ckpt-th state
+        const NatState &from = (s % ckpt == 0) ? ck[s / ckpt] : tmp;
+        NatState to = ((s + 1) % ckpt == 0) ? ck[(s + 1) / ckpt] : seg[0];
+        CKR(traj_step_fwd(c, ntime0 + s, from, to, T.R1, T.R2, T.ts, T.tm, T.au));
+        if ((s + 1) % ckpt != 0) CKR(nat_copy(c, tmp, to, nf));
+    }
+    CKR(nat_h2d(c, bar, lamT));
+    for (int s0 = ((nsteps - 1) / ckpt) * ckpt; nsteps > 0 && s0 >= 0; s0 -= ckpt) {
+        const int s1 = std::min(s0 + ckpt, nsteps);
+        CKR(nat_copy(c, seg[0], ck[s0 / ckpt], nf));
+        for (int s = s0; s < s1 - 1; s++)   // states at the starts of the segment's steps
+            CKR(traj_step_fwd(c, ntime0 + s, seg[s - s0], seg[s - s0 + 1], T.R1, T.R2, T.ts, T.tm, T.au));
+        for (int s = s1 - 1; s >= s0; s--) {
+            // this step's stage records and output, then its adjoint
+            CKR(traj_step_fwd(c, ntime0 + s, seg[s - s0], tmp, T.R1, T.R2, T.ts, T.tm, T.au));
+            CKR(traj_step_ad(c, ntime0 + s, seg[s - s0], tmp, T.R1, T.R2, bar, S));
+        }
+    }
+    CKR(nat_d2h(c, g0, bar));
     return cuerr(cudaStreamSynchronize(c->stream));
 }
 

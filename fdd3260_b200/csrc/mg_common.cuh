@@ -148,6 +148,57 @@ size_t check_scratch_bytes();
 cudaError_t launch_check(const DevGrid &g, const double *u, const double *v, const double *w, const double *es,
                          const double *qt, void *scratch, cudaStream_t s);
 
+// ---- one integrator stage for the trajectory tangent linear / adjoint (k_traj.cu) ----
+enum { TM_P, TM_MW, TM_RHO, TM_ES, TM_AES, TM_QT, TM_AQT, TM_AU, TM_AV, TM_AW, TM_TU, TM_TV, TM_TW, TM_UN, TM_VN,
+       TM_WN, TM_N };
+struct TrajMomArgs {
+    const double *v[TM_N], *d[TM_N];   // values and (tangent mode) tangents of the inputs
+    double *out[6], *dout[6];          // tu, tv, tw, mu, mv, mw (values may be null in tangent mode)
+    double a_dt, b;
+};
+struct TrajScalArgs {
+    int nf;                             // field 0: the density
+    const double *adv[MG_MAXF], *dadv[MG_MAXF], *tprev[MG_MAXF], *dtprev[MG_MAXF], *sn[MG_MAXF], *dsn[MG_MAXF];
+    const double *rhon, *drhon;
+    double *tout[MG_MAXF], *dtout[MG_MAXF], *out[MG_MAXF], *dout[MG_MAXF];
+    double a_dt, b;
+};
+struct TrajConv {
+    int dir, ns;                        // 0: natural -> stage variables; 1: back; ns scalars besides density
+    const double *in[3 + MG_MAXF], *din[3 + MG_MAXF];
+    double *out[3 + MG_MAXF], *dout[3 + MG_MAXF];
+    const double *rho, *drho;
+};
+struct TrajMomAd {
+    const double *mbar[3], *tcarry[3];
+    double *tprev_bar[3], *abar[3], *mnbar[3];
+    double *pbar, *mwin_bar;
+    const double *rho, *es, *aes, *qt, *aqt;
+    double *rho_bar, *es_bar, *aes_bar, *qt_bar, *aqt_bar;
+    double a_dt, b;
+};
+struct TrajScalAd {
+    int nf;
+    const double *psibar[MG_MAXF], *tcarry[MG_MAXF], *sn[MG_MAXF];
+    double *advbar[MG_MAXF], *tprev_bar[MG_MAXF], *snbar[MG_MAXF];
+    const double *rhon;
+    double a_dt, b;
+};
+struct TrajConvAd {
+    int dir, ns;
+    const double *outbar[3 + MG_MAXF], *in[3 + MG_MAXF];
+    double *inbar[3 + MG_MAXF];
+    const double *rho;
+    double *rhobar;
+};
+cudaError_t launch_stage_mom(const DevGrid &g, const TrajMomArgs &a, int tangent, cudaStream_t s);
+cudaError_t launch_stage_scal(const DevGrid &g, const TrajScalArgs &a, int tangent, cudaStream_t s);
+cudaError_t launch_convert(const DevGrid &g, const TrajConv &a, int tangent, cudaStream_t s);
+cudaError_t launch_stage_mom_ad(const DevGrid &g, const TrajMomAd &a, cudaStream_t s);
+cudaError_t launch_stage_scal_ad(const DevGrid &g, const TrajScalAd &a, cudaStream_t s);
+cudaError_t launch_convert_ad(const DevGrid &g, const TrajConvAd &a, cudaStream_t s);
+cudaError_t launch_axpy(const DevGrid &g, double *y, const double *x, double alpha, cudaStream_t s);
+
 // tangent linear / adjoint of the momentum advection operator (k_momadj.cu)
 cudaError_t mom_adj_plan(const DevGrid &g, int ntime, const double *mu, const double *mv, const double *mw, void **plan,
                          cudaStream_t s);

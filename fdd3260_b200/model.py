@@ -245,6 +245,38 @@ class Mimica:
                    "mg_qnadv_ad")
         return tuple(outs)
 
+    # ---- trajectory tangent linear and adjoint (FP64, WENO, SGS off) ----
+    def _fields(self, st) -> list:
+        return [np.ascontiguousarray(a, dtype=np.float64) for a in (st.u, st.v, st.w, st.p, st.dens, *st.scal)]
+
+    def _parr(self, arrs):
+        return (_lib._dp * len(arrs))(*[_lib.ptr(a) for a in arrs])
+
+    def _state_of(self, arrs):
+        from .config import State
+        return State(arrs[0], arrs[1], arrs[2], arrs[3], arrs[4], list(arrs[5:]), self.iqt)
+
+    def traj_forward(self, nsteps: int, ntime0: int = 1) -> None:
+        """Advance the resident state through the composition the trajectory adjoint
+        linearises (unit-mode K1/K2, stage kernels, projection)."""
+        _lib.check(self._L.mg_traj_forward(self._h, nsteps, ntime0), "mg_traj_forward")
+
+    def traj_tl(self, dx0, nsteps: int, ntime0: int = 1):
+        """Tangent linear of nsteps steps from the resident state along dx0 (a State)."""
+        din = self._fields(dx0)
+        out = [np.zeros(self.domain.shape) for _ in din]
+        _lib.check(self._L.mg_traj_tl(self._h, nsteps, ntime0, self._parr(din), self._parr(out)), "mg_traj_tl")
+        return self._state_of(out)
+
+    def traj_adjoint(self, lam, nsteps: int, ntime0: int = 1, ckpt: int = 4):
+        """Adjoint of nsteps steps from the resident state: the gradient, with respect to
+        the initial state, of J = sum over the interior of lam . x(final)."""
+        lin = self._fields(lam)
+        out = [np.zeros(self.domain.shape) for _ in lin]
+        _lib.check(self._L.mg_traj_adjoint(self._h, nsteps, ntime0, ckpt, self._parr(lin), self._parr(out)),
+                   "mg_traj_adjoint")
+        return self._state_of(out)
+
     def anelastic_pressure_ad(self, mub, mvb, mwb, pb):
         """Adjoint of anelastic_pressure (the momentum/pressure map): returns (mub, mvb, mwb, pb)."""
         io = [np.array(a, dtype=np.float64, copy=True) for a in (mub, mvb, mwb, pb)]

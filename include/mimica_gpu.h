@@ -293,6 +293,25 @@ int mg_qnadv_ad(mg_ctx *ctx, int ntime, const double *mu, const double *mv, cons
                 const double *aubar, const double *avbar, const double *awbar, double *mubar, double *mvbar,
                 double *mwbar);
 
+/* ---- trajectory tangent linear and adjoint (no counterpart in the reference) ----
+ * The integrator step of mg_step written as the composition its linearisation follows:
+ * the advection tendencies of all scalar fields (K1 unit mode), qnadv (K2 unit mode),
+ * the stage assembly (pressure gradient, implicit buoyancy, Heun update) and the
+ * projection, with the natural <-> stage variables at the ends of the step.  FP64
+ * contexts, WENO scalars, SGS diffusion off.  State arrays: 5 + nscal host pointers in
+ * the order u, v, w, p, dens, scal[0..nscal-1], reference layout.
+ *   mg_traj_forward: the resident state advanced nsteps by that composition.
+ *   mg_traj_tl:      dxT = (dx(T)/dx(0)) dx0 from the resident state x(0) (unchanged);
+ *                    dx0 with periodic ghost cells.
+ *   mg_traj_adjoint: g0 = (dx(T)/dx(0))^T lamT, the gradient of J = <lamT, x(T)> (interior
+ *                    inner product) with respect to x(0); the forward sweep keeps a state
+ *                    every ckpt steps and each segment is recomputed before its backward
+ *                    sweep, so memory is (nsteps/ckpt + ckpt + ~30) fields.  Ghost entries
+ *                    of g0 are 0. */
+int mg_traj_forward(mg_ctx *ctx, int nsteps, int ntime0);
+int mg_traj_tl(mg_ctx *ctx, int nsteps, int ntime0, const double *const *dx0, double *const *dxT);
+int mg_traj_adjoint(mg_ctx *ctx, int nsteps, int ntime0, int ckpt, const double *const *lamT, double *const *g0);
+
 /* Adjoint of anelastic_pressure (pressure_solver.f90:73-140: nsubp passes of solve +
  * correction, then the level-mean removal of w) as a map of the momentum and pressure;
  * the map is affine (linear in m), so its tangent linear is mg_anelastic_pressure itself.
