@@ -256,6 +256,8 @@ def main():
                     help="smagorinsky: SGS turbulence diffusion on (Smagorinsky-Lilly, pran=-0.4, zdec=2400 m, "
                          "surface heat, moisture and momentum fluxes), as the BOMEX template runs it")
     ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--traj-steps", type=int, default=200, help="steps of the trajectory adjoint leg (0: off)")
+    ap.add_argument("--traj-ckpt", type=int, default=25)
     ap.add_argument("--err-steps", type=int, default=10,
                     help="steps of the accuracy leg (mixed vs FP64 fields from the same initial state)")
     args = ap.parse_args()
@@ -336,6 +338,8 @@ def main():
         r.update(time_form(args, m, d, st, use_graph, ws, local))
         if form == "fp64" and args.scheme == "weno":
             r["adjoint"] = adjoint_leg(m)
+            if args.traj_steps > 0:
+                r["adjoint"]["trajectory"] = trajectory_leg(args, dev)
         if form == forms[0]:
             r.update(e2e_leg(args, m, d, st, ws))
         r["device_bytes"] = m.device_bytes
@@ -492,6 +496,35 @@ def adjoint_leg(m, reps: int = 3) -> dict:
             "advection_ad_over_fwd": f[2] / f[0], "projection_fwd_ms": f[3], "projection_ad_ms": f[4],
             "projection_ad_over_fwd": f[4] / f[3],
             "note": "operator level: one density-weighted field (WENO) and one anelastic_pressure call"}
+
+
+def trajectory_leg(args, dev) -> dict:
+    """Checkpointed trajectory adjoint against the forward model on the adjoint workload:
+    128 x 128 x 96 cells at 40 m, a dry warm bubble (u, v, w, theta; density carried),
+    traj_steps steps with a checkpoint every traj_ckpt steps.  Device times with CUDA
+    events: the production step (graph), the composition the linearisation follows, its
+    tangent linear, and the adjoint including its forward sweep and recomputation."""
+    from fdd3260_b200 import Mimica, config
+    d = config.warm_bubble_domain(128, 128, 96, dx=40.0, dy=40.0, dz=40.0, dt0=0.5)
+    st = config.warm_bubble_state(d, seed=1002, centre=(2560.0, 2560.0, 800.0), radius=600.0, nscal_passive=0)
+    n, ck = args.traj_steps, args.traj_ckpt
+    with Mimica(d, nscal=len(st.scal), device=dev) as m:
+        m.upload(st)
+        m.time_traj(2, 1)   # warm-up: plans, buffers, first launches
+        t = m.time_traj(n, ck)
+        m.upload(st)
+        ms = C.c_double(0.0)
+        m.stepping(3, ntime0=1, graph=True)
+        rc = m._L.mg_time_steps(m._h, n, 4, 1, C.byref(ms))
+        if rc:
+            raise RuntimeError(f"mg_time_steps failed: {rc}")
+    fwd = ms.value
+    return {"workload": "warm bubble 128x128x96 at 40 m, dry (u, v, w, theta, density), WENO3 switch, FD4",
+            "steps": n, "ckpt": ck, "step_ms": fwd, "composition_ms": t["forward_ms"], "tl_ms": t["tl_ms"],
+            "adjoint_ms": t["adjoint_ms"], "adjoint_over_fwd": t["adjoint_ms"] / fwd,
+            "adjoint_over_composition": t["adjoint_ms"] / t["forward_ms"], "tl_over_fwd": t["tl_ms"] / fwd,
+            "adjoint_device_gb": t["adjoint_device_bytes"] / 1e9,
+            "note": "adjoint_ms includes the forward sweep that stores checkpoints and the segment recomputation"}
 
 
 def field_errors(out, ref, st0, nsteps: int) -> dict:

@@ -126,6 +126,7 @@ def lib() -> C.CDLL:
         L.mg_traj_forward.argtypes = [vp, C.c_int, C.c_int]
         L.mg_traj_tl.argtypes = [vp, C.c_int, C.c_int, C.POINTER(_dp), C.POINTER(_dp)]
         L.mg_traj_adjoint.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(_dp), C.POINTER(_dp)]
+        L.mg_time_traj.argtypes = [vp, C.c_int, C.c_int, C.c_int, _dp]
         L.mg_qnadv_tl.argtypes = [vp, C.c_int] + [_dp] * 12
         L.mg_qnadv_ad.argtypes = [vp, C.c_int] + [_dp] * 9
         L.mg_set_sgs.argtypes = [vp, C.POINTER(MgSgsParams)]
@@ -167,5 +168,5 @@ EXPORTED = [
     "mg_advection_tl", "mg_advection_ad", "mg_anelastic_pressure_ad", "mg_time_adjoint", "mg_ensemble_create", "mg_ensemble_destroy", "mg_ensemble_step", "mg_ensemble_time_steps", "mg_ensemble_launch_count",
     "mg_set_sgs", "mg_set_surface_fluxes", "mg_sgs_profiles", "mg_calc_subgrid", "mg_efud", "mg_eff",
     "mg_checkall", "mg_cfl_dt", "mg_set_dt", "mg_download_ksgs", "mg_qnadv_tl", "mg_qnadv_ad",
-    "mg_traj_forward", "mg_traj_tl", "mg_traj_adjoint",
+    "mg_traj_forward", "mg_traj_tl", "mg_traj_adjoint", "mg_time_traj",
 ]

@@ -1638,55 +1638,85 @@ struct TrajCtx {
     }
 };
 
-extern "C" int mg_traj_forward(mg_ctx *c, int nsteps, int ntime0)
+// CUDA-event timer around a device-resident section (ms stays untouched when null)
+struct TrajTimer {
+    cudaStream_t s;
+    float *ms;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t start()
+    {
+        if (!ms) return cudaSuccess;
+        cudaError_t e = cudaEventCreate(&e0);
+        if (e == cudaSuccess) e = cudaEventCreate(&e1);
+        if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+        return e;
+    }
+    cudaError_t stop()
+    {
+        if (!ms) return cudaSuccess;
+        cudaError_t e = cudaEventRecord(e1, s);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+        return e;
+    }
+    ~TrajTimer()
+    {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
+};
+
+// nsteps of the composition from the resident state; written back when writeback
+static int traj_forward_run(mg_ctx *c, int nsteps, int ntime0, bool writeback, float *ms)
 {
-    int rc = traj_check(c);
-    if (rc) return rc;
-    if (nsteps < 0) return MG_ERR_PARAM;
-    CKR(cudaSetDevice(c->device));
     TrajCtx T;
     T.init(c, false);
     const NatState res = traj_resident(c);
     NatState a = nat_alloc(T.B, c->nf), b = nat_alloc(T.B, c->nf);
     CKR(T.B.err);
     CKR(nat_copy(c, a, res, c->nf));
+    TrajTimer tm{c->stream, ms};
+    CKR(tm.start());
     for (int s = 0; s < nsteps; s++) {
         CKR(traj_step_fwd(c, ntime0 + s, a, b, T.R1, T.R2, T.ts, T.tm, T.au));
         std::swap(a, b);
     }
-    CKR(nat_copy(c, res, a, c->nf));
-    c->rep = REP_NAT;
+    CKR(tm.stop());
+    if (writeback) {
+        CKR(nat_copy(c, res, a, c->nf));
+        c->rep = REP_NAT;
+    }
     return cuerr(cudaStreamSynchronize(c->stream));
 }
 
-extern "C" int mg_traj_tl(mg_ctx *c, int nsteps, int ntime0, const double *const *dx0, double *const *dxT)
+// tangent linear of nsteps; dx0 == nullptr starts from a copy of the resident state (timing)
+static int traj_tl_run(mg_ctx *c, int nsteps, int ntime0, const double *const *dx0, double *const *dxT, float *ms)
 {
-    int rc = traj_check(c);
-    if (rc) return rc;
-    if (nsteps < 0 || !dx0 || !dxT) return MG_ERR_PARAM;
-    CKR(cudaSetDevice(c->device));
     TrajCtx T;
     T.init(c, true);
     NatState a = nat_alloc(T.B, c->nf), b = nat_alloc(T.B, c->nf), da = nat_alloc(T.B, c->nf), db = nat_alloc(T.B, c->nf);
     CKR(T.B.err);
     CKR(nat_copy(c, a, traj_resident(c), c->nf));
-    CKR(nat_h2d(c, da, dx0));
+    if (dx0) CKR(nat_h2d(c, da, dx0));
+    else CKR(nat_copy(c, da, traj_resident(c), c->nf));
+    TrajTimer tm{c->stream, ms};
+    CKR(tm.start());
     for (int s = 0; s < nsteps; s++) {
         CKR(traj_step_tl(c, ntime0 + s, a, da, b, db, T.R1, T.R2, T.dR1, T.dR2, T.ts, T.tm, T.dts, T.dtm, T.au));
         std::swap(a, b);
         std::swap(da, db);
     }
-    CKR(nat_d2h(c, dxT, da));
+    CKR(tm.stop());
+    if (dxT) CKR(nat_d2h(c, dxT, da));
     return cuerr(cudaStreamSynchronize(c->stream));
 }
 
-extern "C" int mg_traj_adjoint(mg_ctx *c, int nsteps, int ntime0, int ckpt, const double *const *lamT, double *const *g0)
+// adjoint of nsteps with checkpoints every ckpt steps; lamT == nullptr seeds the adjoint
+// with a copy of the resident state (timing).  bytes: device memory the run held.
+static int traj_adjoint_run(mg_ctx *c, int nsteps, int ntime0, int ckpt, const double *const *lamT,
+                            double *const *g0, float *ms, double *bytes)
 {
-    int rc = traj_check(c);
-    if (rc) return rc;
-    if (nsteps < 0 || ckpt < 1 || !lamT || !g0) return MG_ERR_PARAM;
-    CKR(cudaSetDevice(c->device));
-    rc = ensure_momplan(c, c->mA[0], c->mA[1], c->mA[2]);
+    int rc = ensure_momplan(c, c->mA[0], c->mA[1], c->mA[2]);
     if (rc) return rc;
     const int nf = c->nf;
     TrajCtx T;
@@ -1708,14 +1738,18 @@ extern "C" int mg_traj_adjoint(mg_ctx *c, int nsteps, int ntime0, int ckpt, cons
     for (int q = 0; q <= ckpt; q++) seg[q] = nat_alloc(T.B, nf);
     NatState bar = nat_alloc(T.B, nf), tmp = nat_alloc(T.B, nf);
     CKR(T.B.err);
+    if (bytes) *bytes = (double)T.B.own.size() * (double)c->fbytes;
     CKR(nat_copy(c, ck[0], traj_resident(c), nf));
+    if (lamT) CKR(nat_h2d(c, bar, lamT));
+    else CKR(nat_copy(c, bar, traj_resident(c), nf));
+    TrajTimer tm{c->stream, ms};
+    CKR(tm.start());
     for (int s = 0; s < nsteps; s++) {   // forward sweep: keep every ckpt-th state
         const NatState &from = (s % ckpt == 0) ? ck[s / ckpt] : tmp;
         NatState to = ((s + 1) % ckpt == 0) ? ck[(s + 1) / ckpt] : seg[0];
         CKR(traj_step_fwd(c, ntime0 + s, from, to, T.R1, T.R2, T.ts, T.tm, T.au));
         if ((s + 1) % ckpt != 0) CKR(nat_copy(c, tmp, to, nf));
     }
-    CKR(nat_h2d(c, bar, lamT));
     for (int s0 = ((nsteps - 1) / ckpt) * ckpt; nsteps > 0 && s0 >= 0; s0 -= ckpt) {
         const int s1 = std::min(s0 + ckpt, nsteps);
         CKR(nat_copy(c, seg[0], ck[s0 / ckpt], nf));
@@ -1727,8 +1761,53 @@ extern "C" int mg_traj_adjoint(mg_ctx *c, int nsteps, int ntime0, int ckpt, cons
             CKR(traj_step_ad(c, ntime0 + s, seg[s - s0], tmp, T.R1, T.R2, bar, S));
         }
     }
-    CKR(nat_d2h(c, g0, bar));
+    CKR(tm.stop());
+    if (g0) CKR(nat_d2h(c, g0, bar));
     return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+extern "C" int mg_traj_forward(mg_ctx *c, int nsteps, int ntime0)
+{
+    int rc = traj_check(c);
+    if (rc) return rc;
+    if (nsteps < 0) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    return traj_forward_run(c, nsteps, ntime0, true, nullptr);
+}
+
+extern "C" int mg_traj_tl(mg_ctx *c, int nsteps, int ntime0, const double *const *dx0, double *const *dxT)
+{
+    int rc = traj_check(c);
+    if (rc) return rc;
+    if (nsteps < 0 || !dx0 || !dxT) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    return traj_tl_run(c, nsteps, ntime0, dx0, dxT, nullptr);
+}
+
+extern "C" int mg_traj_adjoint(mg_ctx *c, int nsteps, int ntime0, int ckpt, const double *const *lamT, double *const *g0)
+{
+    int rc = traj_check(c);
+    if (rc) return rc;
+    if (nsteps < 0 || ckpt < 1 || !lamT || !g0) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    return traj_adjoint_run(c, nsteps, ntime0, ckpt, lamT, g0, nullptr, nullptr);
+}
+
+// device times (ms) of nsteps of the trajectory forward composition, its tangent linear and
+// its checkpointed adjoint (forward sweep, segment recomputation and backward sweep), from
+// the resident state, which is left unchanged; out[3] = device bytes the adjoint held
+extern "C" int mg_time_traj(mg_ctx *c, int nsteps, int ntime0, int ckpt, double *out)
+{
+    int rc = traj_check(c);
+    if (rc) return rc;
+    if (nsteps < 1 || ckpt < 1 || !out) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    float t[3] = {0.f, 0.f, 0.f};
+    if ((rc = traj_forward_run(c, nsteps, ntime0, false, &t[0]))) return rc;
+    if ((rc = traj_tl_run(c, nsteps, ntime0, nullptr, nullptr, &t[1]))) return rc;
+    if ((rc = traj_adjoint_run(c, nsteps, ntime0, ckpt, nullptr, nullptr, &t[2], &out[3]))) return rc;
+    for (int q = 0; q < 3; q++) out[q] = t[q];
+    return check_err(c);
 }
 
 // ---- tangent linear and adjoint of the scalar advection operator (WENO) ----

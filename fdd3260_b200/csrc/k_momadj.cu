@@ -320,6 +320,9 @@ __global__ void __launch_bounds__(128) mom_ad_kernel(DevGrid G, int ntime, int c
     for (int t = 0; t < NCH && s0 + t < nslot; t++) {
         const int code = offs[s0 + t];
         const int dk = code % 5 - 2, dj = (code / 5) % 5 - 2, di = (code / 25) % 5 - 2, f = code / 125;
+        // the offsets are the union over all levels; near the surface and the lid some of
+        // them point outside 1..nz, where the stencils read nothing (the partial is 0)
+        if (k + dk < 1 || k + dk > G.nz) continue;
         const long long tq = gidx(G, wrap_x(G, i + di), wrap_y(G, j + dj), k + dk);
         atomicAdd(const_cast<double *>(bar.m[f]) + tq, a.d[t] * ab);
     }

@@ -277,6 +277,13 @@ class Mimica:
                    "mg_traj_adjoint")
         return self._state_of(out)
 
+    def time_traj(self, nsteps: int, ckpt: int, ntime0: int = 1) -> dict:
+        """Device times of nsteps of the trajectory composition, its tangent linear and its
+        checkpointed adjoint from the resident state (left unchanged)."""
+        out = np.zeros(4)
+        _lib.check(self._L.mg_time_traj(self._h, nsteps, ntime0, ckpt, _lib.ptr(out)), "mg_time_traj")
+        return {"forward_ms": out[0], "tl_ms": out[1], "adjoint_ms": out[2], "adjoint_device_bytes": int(out[3])}
+
     def anelastic_pressure_ad(self, mub, mvb, mwb, pb):
         """Adjoint of anelastic_pressure (the momentum/pressure map): returns (mub, mvb, mwb, pb)."""
         io = [np.array(a, dtype=np.float64, copy=True) for a in (mub, mvb, mwb, pb)]

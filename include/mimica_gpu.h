@@ -311,6 +311,11 @@ int mg_qnadv_ad(mg_ctx *ctx, int ntime, const double *mu, const double *mv, cons
 int mg_traj_forward(mg_ctx *ctx, int nsteps, int ntime0);
 int mg_traj_tl(mg_ctx *ctx, int nsteps, int ntime0, const double *const *dx0, double *const *dxT);
 int mg_traj_adjoint(mg_ctx *ctx, int nsteps, int ntime0, int ckpt, const double *const *lamT, double *const *g0);
+/* Device times (ms) of nsteps of mg_traj_forward's composition (out4[0]), of the tangent
+ * linear (out4[1]) and of the checkpointed adjoint, forward sweep and recomputation
+ * included (out4[2]), from the resident state, which is left unchanged; out4[3] = device
+ * bytes the adjoint held. */
+int mg_time_traj(mg_ctx *ctx, int nsteps, int ntime0, int ckpt, double *out4);
 
 /* Adjoint of anelastic_pressure (pressure_solver.f90:73-140: nsubp passes of solve +
  * correction, then the level-mean removal of w) as a map of the momentum and pressure;

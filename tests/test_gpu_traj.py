@@ -90,6 +90,23 @@ def test_dot_product(nsteps, ckpt):
     assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), abs(rhs)), (lhs, rhs)
 
 
+def test_dot_product_single_scalar_larger_grid():
+    """theta only (density + one scalar) on 96 x 96 x 48: the adjoint of the momentum
+    advection skips the stencil offsets that leave 1..nz at the surface and the lid."""
+    d = config.warm_bubble_domain(96, 96, 48, dx=40.0, dy=40.0, dz=40.0)
+    st = config.warm_bubble_state(d, seed=9, centre=(1900.0, 1900.0, 700.0), radius=500.0, nscal_passive=0)
+    rng = np.random.default_rng(12)
+    sc = [0.1, 0.1, 0.05, 1.0, 1e-3, 0.05]
+    dx0 = _rand_like(st, rng, sc)
+    lam = _rand_like(st, rng, [1.0] * 6)
+    with Mimica(d, nscal=1) as m:
+        m.upload(st)
+        tl = m.traj_tl(dx0, 2)
+        ad = m.traj_adjoint(lam, 2, ckpt=1)
+    lhs, rhs = _dot(tl, lam), _dot(dx0, ad)
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), abs(rhs)), (lhs, rhs)
+
+
 def test_checkpoint_interval_does_not_change_gradient():
     d = config.warm_bubble_domain(24, 24, 12)
     st = config.warm_bubble_state(d, seed=4, centre=(600.0, 600.0, 250.0), radius=300.0)
@@ -177,3 +194,17 @@ def test_central_difference_with_buoyancy_and_scalar_advection(target):
     eps = 1e-6
     cd = (J(eps, delta) - J(-eps, delta)) / (2 * eps)
     assert abs(cd - gd) <= 5e-6 * abs(gd), (cd, gd)
+
+
+def test_time_traj_leaves_state_and_reports():
+    d = config.warm_bubble_domain(24, 24, 12)
+    st = config.warm_bubble_state(d, seed=6, centre=(600.0, 600.0, 250.0), radius=300.0)
+    with Mimica(d, nscal=2) as m:
+        m.upload(st)
+        t = m.time_traj(4, 2)
+        out = m.download()
+    for x, y in zip(_fields(out), _fields(st)):
+        assert np.array_equal(_interior(x), _interior(y))
+    assert t["forward_ms"] > 0 and t["tl_ms"] > 0 and t["adjoint_ms"] > t["forward_ms"]
+    # checkpoints: 4/2 + 1 states, a segment of 3, adjoint, scratch and the stage records
+    assert t["adjoint_device_bytes"] >= (3 + 3 + 2) * 7 * 8 * np.prod(d.shape)
