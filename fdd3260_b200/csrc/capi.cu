@@ -51,7 +51,6 @@ struct mg_ctx {
     int gsteps[2] = {0, 0};
     long long gen = 0;                   // bumped whenever recorded step graphs go stale
     void *chk = nullptr;                 // scratch of the per-step checks
-    void *momplan = nullptr;             // input offsets of the momentum-advection adjoint
     // SGS diffusion (mg_set_sgs): per-level factors + qt0 on the device, the
     // deformation tensor and eddy viscosity of level n, the stored tendencies
     mg_sgs_params sgsp{};
@@ -247,7 +246,6 @@ static void free_ctx(mg_ctx *c)
     for (int f = 0; f < MG_MAXF; f++) { cudaFree(c->sA[f]); cudaFree(c->sB[f]); cudaFree(c->ts[f]); }
     for (int i = 0; i < 16; i++) cudaFree(c->unit[i]);
     cudaFree(c->sgs_prof); cudaFree(c->fkv); cudaFree(c->sfe); cudaFree(c->snut); cudaFree(c->chk);
-    mom_adj_plan_destroy(c->momplan);
     for (int q = 0; q < 6; q++) cudaFree(c->dij[q]);
     for (int q = 0; q < 3; q++) { cudaFree(c->sgm[q]); cudaFree(c->sfc[q]); }
     for (int f = 0; f < MG_MAXF; f++) cudaFree(c->sgsc[f]);
@@ -1172,12 +1170,6 @@ extern "C" int mg_qnadv_tl(mg_ctx *c, int ntime, const double *mu, const double 
     return cuerr(cudaStreamSynchronize(c->stream));
 }
 
-static int ensure_momplan(mg_ctx *c, const double *mu, const double *mv, const double *mw)
-{
-    if (c->momplan) return MG_OK;
-    return cuerr(mom_adj_plan(c->G, 1, mu, mv, mw, &c->momplan, c->stream));
-}
-
 extern "C" int mg_qnadv_ad(mg_ctx *c, int ntime, const double *mu, const double *mv, const double *mw,
                            const double *aubar, const double *avbar, const double *awbar, double *mubar, double *mvbar,
                            double *mwbar)
@@ -1190,10 +1182,9 @@ extern "C" int mg_qnadv_ad(mg_ctx *c, int ntime, const double *mu, const double 
     const double *in[6] = {mu, mv, mw, aubar, avbar, awbar};
     for (int q = 0; q < 6; q++) CKR(h2d(c, c->unit[q], in[q], cudaMemcpyHostToDevice));
     for (int q = 6; q < 9; q++) CKR(cudaMemsetAsync(c->unit[q], 0, c->fbytes, c->stream));
-    rc = ensure_momplan(c, c->unit[0], c->unit[1], c->unit[2]);
-    if (rc) return rc;
-    CKR(launch_qnadv_ad(c->G, c->momplan, ntime, c->unit[0], c->unit[1], c->unit[2], c->unit[3], c->unit[4], c->unit[5],
-                        c->unit[6], c->unit[7], c->unit[8], c->stream));
+    (void)ntime;   // the adjoint of the sum of the direction terms does not depend on their order
+    CKR(launch_qnadv_ad(c->G, c->unit[0], c->unit[1], c->unit[2], c->unit[3], c->unit[4], c->unit[5], c->unit[6],
+                        c->unit[7], c->unit[8], c->stream));
     CKR(d2h(c, mubar, c->unit[6], cudaMemcpyDeviceToHost));
     CKR(d2h(c, mvbar, c->unit[7], cudaMemcpyDeviceToHost));
     CKR(d2h(c, mwbar, c->unit[8], cudaMemcpyDeviceToHost));
@@ -1511,8 +1502,8 @@ static cudaError_t traj_stage_ad(mg_ctx *c, int ntime, int stage, const NatState
     M.qt_bar = iqt >= 0 ? xs_in_bar[iqt] : nullptr; M.aqt_bar = iqt >= 0 ? W.Abar[iqt] : nullptr;
     M.a_dt = a_dt; M.b = b;
     if ((e = launch_stage_mom_ad(G, M, c->stream)) != cudaSuccess) return e;
-    if ((e = launch_qnadv_ad(G, c->momplan, ntime, R.xm[0], R.xm[1], R.xm[2], W.abar[0], W.abar[1], W.abar[2],
-                             xm_in_bar[0], xm_in_bar[1], xm_in_bar[2], c->stream)) != cudaSuccess)
+    if ((e = launch_qnadv_ad(G, R.xm[0], R.xm[1], R.xm[2], W.abar[0], W.abar[1], W.abar[2], xm_in_bar[0], xm_in_bar[1],
+                             xm_in_bar[2], c->stream)) != cudaSuccess)
         return e;
     TrajScalAd S{};
     S.nf = nf; S.rhon = N.s[0]; S.a_dt = a_dt; S.b = b;
@@ -1716,8 +1707,6 @@ static int traj_tl_run(mg_ctx *c, int nsteps, int ntime0, const double *const *d
 static int traj_adjoint_run(mg_ctx *c, int nsteps, int ntime0, int ckpt, const double *const *lamT,
                             double *const *g0, float *ms, double *bytes)
 {
-    int rc = ensure_momplan(c, c->mA[0], c->mA[1], c->mA[2]);
-    if (rc) return rc;
     const int nf = c->nf;
     TrajCtx T;
     T.init(c, false);

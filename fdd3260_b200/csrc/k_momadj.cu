@@ -8,13 +8,10 @@
 // expressions and the direction order of ntime's parity, so its FP64 instance equals
 // the K2 momentum advection bit for bit (a test checks it).
 //   TL: the per-cell form on dual numbers with one partial (tangent = dm).
-//   AD: the per-cell form on dual numbers with 8 partials, seeded with 8 of the cell's
-//       stencil inputs at a time (the input offsets of each component are found once by
-//       a probe pass); the local Jacobian row times the output adjoint is scattered
-//       onto the inputs with atomics.  Inputs in periodic ghost cells are scattered onto
-//       the interior cells they are images of, so the ghosts of the result stay 0.
-#include <vector>
-
+//   AD: the transposed stencils, hand-written in gather form (one thread per input cell
+//       sums what every face flux and viscosity term that reads the cell passes back);
+//       no atomics.  What the forward reads through periodic ghost images lands on the
+//       interior cells they copy, so the ghosts of the result stay 0.
 #include "dual.cuh"
 #include "mg_common.cuh"
 #include "mimica_gpu.h"
@@ -22,12 +19,9 @@
 namespace {
 
 constexpr double AVISC = 1. / 16.;   // windadv.f90:39
-constexpr int NCH = 8;                // partials per AD pass
-constexpr int NOFF = 3 * 5 * 5 * 5;   // (field, di, dj, dk) offsets, |d| <= 2
 
 __device__ __forceinline__ int wrap_x(const DevGrid &G, int i) { return i < 4 ? i + G.maxx : (i > G.nx - 2 ? i - G.maxx : i); }
 __device__ __forceinline__ int wrap_y(const DevGrid &G, int j) { return j < 4 ? j + G.maxy : (j > G.ny - 2 ? j - G.maxy : j); }
-__device__ __forceinline__ int off_code(int f, int di, int dj, int dk) { return ((f * 5 + di + 2) * 5 + dj + 2) * 5 + dk + 2; }
 
 // advective velocity of momentum component f at level k (funcpack.f90:65-94)
 template <typename T>
@@ -249,36 +243,6 @@ struct LoadTL {
     __device__ D<1> t(int f, int i, int j, int k) const { return adv_vel(G, f, k, m(f, i, j, k)); }
 };
 
-// records the offsets an output reads (probe pass, plain values)
-struct LoadProbe {
-    const DevGrid &G;
-    Mom3 v;
-    int i0, j0, k0;
-    int *mask;
-    __device__ double m(int f, int i, int j, int k) const
-    {
-        mask[off_code(f, i - i0, j - j0, k - k0)] = 1;
-        return __ldg(v.m[f] + gidx(G, i, j, k));
-    }
-    __device__ double t(int f, int i, int j, int k) const { return adv_vel(G, f, k, m(f, i, j, k)); }
-};
-
-// 8 partials, seeded on the inputs whose compact slot lies in [s0, s0 + 8)
-struct LoadAD {
-    const DevGrid &G;
-    Mom3 v;
-    int i0, j0, k0, s0;
-    const short *slot;   // offset code -> compact slot of this component, or -1
-    __device__ D<NCH> m(int f, int i, int j, int k) const
-    {
-        D<NCH> r(__ldg(v.m[f] + gidx(G, i, j, k)));
-        const int s = slot[off_code(f, i - i0, j - j0, k - k0)] - s0;
-        if (s >= 0 && s < NCH) r.d[s] = 1.;
-        return r;
-    }
-    __device__ D<NCH> t(int f, int i, int j, int k) const { return adv_vel(G, f, k, m(f, i, j, k)); }
-};
-
 // ---------------- kernels ----------------
 __global__ void __launch_bounds__(128) mom_tl_kernel(DevGrid G, int ntime, Mom3 v, Mom3 d, Mom3 val, Mom3 tan)
 {
@@ -295,95 +259,350 @@ __global__ void __launch_bounds__(128) mom_tl_kernel(DevGrid G, int ntime, Mom3 
     }
 }
 
-__global__ void mom_probe_kernel(DevGrid G, int ntime, Mom3 v, int i0, int j0, int *masks)
-{
-    const int c = blockIdx.x;
-    for (int k = 1; k <= G.nz; k++) {
-        const LoadProbe ld{G, v, i0, j0, k, masks + c * NOFF};
-        (void)adv_comp<double>(G, ld, c, ntime, i0, j0, k);
-    }
-}
+// ---------------- adjoint: the transposed stencils in gather form ----------------
+// Each direction term is a sum of face fluxes Phi = a * b with constant coefficients
+// (a: an average of advective velocities, b: an average of the advected momentum; the
+// coefficients of the vertical terms depend on the level, as the forward's branches at
+// the surface and the lid), plus the artificial viscosity mu |velocity| D4(momentum).
+// The adjoint at an input cell sums, over every face that reads the cell, Phi-bar (the
+// coefficient-weighted adjoints of the outputs that difference the face) times the
+// partial of Phi, and likewise over the viscosity terms.  Positions wrap periodically in
+// x and y, so what the forward reads through a ghost image is gathered by the interior
+// cell it copies; outputs outside 1..nz (and w at the surface) do not exist.
 
-__global__ void __launch_bounds__(128) mom_ad_kernel(DevGrid G, int ntime, int c, int s0, int nslot, Mom3 v,
-                                                     const double *abar, const short *slot, const int *offs,
-                                                     Mom3 bar)
+__device__ __forceinline__ double sgnd(double x) { return x < 0. ? -1. : 1.; }   // d|x|/dx as dabs takes it
+__device__ __forceinline__ double w4(int d) { return d == 0 ? -6. : ((d == 1 || d == -1) ? 4. : -1.); }
+
+struct Gath {
+    const DevGrid &G;
+    Mom3 m, ab;
+    double c1s, c2s, c1c, c2c;
+    __device__ Gath(const DevGrid &g, Mom3 m_, Mom3 ab_) : G(g), m(m_), ab(ab_)
+    {
+        const bool fd4 = g.mom_ord == 4;
+        c1s = fd4 ? 4. / 3. : 1.; c2s = fd4 ? 1. / 3. : 0.;
+        c1c = fd4 ? 9. / 8. : 1.; c2c = fd4 ? 1. / 8. : 0.;
+    }
+    // (along, transverse) -> (i, j): direction 0 is x, 1 is y
+    __device__ static int ci(int dir, int a, int t) { return dir == 0 ? a : t; }
+    __device__ static int cj(int dir, int a, int t) { return dir == 0 ? t : a; }
+    __device__ int wrap_a(int dir, int a) const { return dir == 0 ? wrap_x(G, a) : wrap_y(G, a); }
+    __device__ double M(int f, int i, int j, int k) const { return __ldg(m.m[f] + gidx(G, i, j, k)); }
+    __device__ double T(int f, int i, int j, int k) const { return adv_vel<double>(G, f, k, M(f, i, j, k)); }
+    __device__ double A(int c, int i, int j, int k) const
+    {
+        if (k < 1 || k > G.nz || (c == 2 && k == 1)) return 0.;
+        return __ldg(ab.m[c] + gidx(G, wrap_x(G, i), wrap_y(G, j), k));
+    }
+    __device__ double Ma(int f, int dir, int a, int t, int k) const { return M(f, ci(dir, a, t), cj(dir, a, t), k); }
+    __device__ double Ta(int f, int dir, int a, int t, int k) const { return T(f, ci(dir, a, t), cj(dir, a, t), k); }
+    __device__ double Aa(int c, int dir, int a, int t, int k) const { return A(c, ci(dir, a, t), cj(dir, a, t), k); }
+    __device__ double rden(int f, int k) const { return 1. / __ldg((f == 2 ? G.avden0 : G.den0) + k - 1); }
+    __device__ double dzw(int q) const { return __ldg(G.dzw + q - 1); }
+    __device__ double dz1w(int q) const { return __ldg(G.dz1w + q - 1); }
+    __device__ double dz1(int q) const { return __ldg(G.dz1 + q - 1); }
+    __device__ double d1(int dir) const { return dir == 0 ? 1. / G.dx : 1. / G.dy; }
+
+    // ---- u_x (f 0, dir x) and v_y (f 1, dir y): the advected field is its own velocity ----
+    __device__ double self_h(int f, int i, int j, int k) const
+    {
+        const int dir = f, a0 = dir == 0 ? i : j, t = dir == 0 ? j : i;
+        const double h1 = d1(dir), h2 = dir == 0 ? 1. / (2. * G.dx) : 1. / (2. * G.dy), rd = rden(f, k);
+        double r = 0.;
+        for (int p = a0 - 1; p <= a0; p++) {   // F(p) = avg T(p, p+1) * avg m(p, p+1)
+            const double fb = c1s * h1 * (Aa(f, dir, p, t, k) - Aa(f, dir, p + 1, t, k));
+            r += fb * 0.5 * (0.5 * (Ma(f, dir, p + 1, t, k) + Ma(f, dir, p, t, k)) * rd +
+                             0.5 * (Ta(f, dir, p + 1, t, k) + Ta(f, dir, p, t, k)));
+        }
+        for (int p = a0 - 2; p <= a0; p += 2) {   // A(p) = avg T(p, p+2) * avg m(p, p+2)
+            const double gb = c2s * h2 * (Aa(f, dir, p + 2, t, k) - Aa(f, dir, p, t, k));
+            r += gb * 0.5 * (0.5 * (Ma(f, dir, p + 2, t, k) + Ma(f, dir, p, t, k)) * rd +
+                             0.5 * (Ta(f, dir, p + 2, t, k) + Ta(f, dir, p, t, k)));
+        }
+        if (G.lavisc) {
+            for (int o = a0 - 2; o <= a0 + 2; o++) r -= AVISC * h1 * Aa(f, dir, o, t, k) * fabs(Ta(f, dir, o, t, k)) * w4(a0 - o);
+            const double d4 = -Ma(f, dir, a0 + 2, t, k) + 4. * Ma(f, dir, a0 + 1, t, k) - 6. * Ma(f, dir, a0, t, k) +
+                              4. * Ma(f, dir, a0 - 1, t, k) - Ma(f, dir, a0 - 2, t, k);
+            r -= AVISC * h1 * Aa(f, dir, a0, t, k) * sgnd(Ta(f, dir, a0, t, k)) * rd * d4;
+        }
+        return r;
+    }
+
+    // ---- u_y (c 0: dir y, velocity v) and v_x (c 1: dir x, velocity u) ----
+    // face bar at along-position q of line t
+    __device__ double cross_fbar(int c, int dir, int q, int t, int k) const
+    {
+        const double h1 = d1(dir), h3 = dir == 0 ? 1. / (3. * G.dx) : 1. / (3. * G.dy);
+        return c1c * h1 * (Aa(c, dir, q, t, k) - Aa(c, dir, q + 1, t, k)) - c2c * h3 * Aa(c, dir, q - 1, t, k) +
+               c2c * h3 * Aa(c, dir, q + 2, t, k);
+    }
+    // partial wrt the advected momentum c at its own cell
+    __device__ double cross_adv(int c, int i, int j, int k) const
+    {
+        const int dir = 1 - c, g = 1 - c;
+        const int a0 = dir == 0 ? i : j, t = dir == 0 ? j : i;
+        double r = 0.;
+        for (int q = a0 - 1; q <= a0; q++) {
+            const double vel = c1c * (Ta(g, dir, q + 1, t - 1, k) + Ta(g, dir, q + 1, t, k)) * 0.5 -
+                               c2c * (Ta(g, dir, q + 1, t - 2, k) + Ta(g, dir, q + 1, t + 1, k)) * 0.5;
+            r += cross_fbar(c, dir, q, t, k) * 0.5 * vel;
+        }
+        if (G.lavisc)
+            for (int o = a0 - 2; o <= a0 + 2; o++) {
+                const int ob = wrap_a(dir, o);
+                const double mu = 0.25 * fabs(Ta(g, dir, ob, t - 1, k) + Ta(g, dir, ob, t, k) + Ta(g, dir, ob + 1, t - 1, k) +
+                                              Ta(g, dir, ob + 1, t, k)) * d1(dir);
+                r -= AVISC * Aa(c, dir, ob, t, k) * mu * w4(a0 - o);
+            }
+        return r;
+    }
+    // partial wrt the advecting momentum g = 1 - c at its own cell
+    __device__ double cross_vel(int c, int i, int j, int k) const
+    {
+        const int dir = 1 - c, g = 1 - c;
+        const int a0 = dir == 0 ? i : j, t0 = dir == 0 ? j : i;
+        const double rd = rden(g, k);
+        double r = 0.;
+        const int ds[4] = {-1, 0, -2, 1};
+        for (int n = 0; n < 4; n++) {   // the velocity at transverse offset d of line t = t0 - d, face q = a0 - 1
+            const int t = t0 - ds[n];
+            const double gam = n < 2 ? 0.5 * c1c : -0.5 * c2c;
+            const double fr = 0.5 * (Ma(c, dir, a0, t, k) + Ma(c, dir, a0 - 1, t, k));
+            r += cross_fbar(c, dir, a0 - 1, t, k) * fr * gam * rd;
+        }
+        if (G.lavisc)
+            for (int t = t0; t <= t0 + 1; t++)
+                for (int o = a0 - 1; o <= a0; o++) {
+                    const double s = Ta(g, dir, o, t - 1, k) + Ta(g, dir, o, t, k) + Ta(g, dir, o + 1, t - 1, k) +
+                                     Ta(g, dir, o + 1, t, k);
+                    const double d4 = -Ma(c, dir, o + 2, t, k) + 4. * Ma(c, dir, o + 1, t, k) - 6. * Ma(c, dir, o, t, k) +
+                                      4. * Ma(c, dir, o - 1, t, k) - Ma(c, dir, o - 2, t, k);
+                    r -= AVISC * Aa(c, dir, o, t, k) * d4 * 0.25 * d1(dir) * sgnd(s) * rd;
+                }
+        return r;
+    }
+
+    // ---- h_z (f 0: u with w at x offsets; f 1: v with w at y offsets) ----
+    // coefficient of face flux F(q) in the output at level ko (advhz's branches)
+    __device__ double hz_coef(int f, int ko, int q) const
+    {
+        const int nz = G.nz;
+        if (ko >= 3 && ko <= nz - 1) {
+            const double s3 = dzw(ko - 1) + dzw(ko) + dzw(ko + 1);
+            if (q == ko) return c1c * dz1w(ko);
+            if (q == ko - 1) return -c1c * dz1w(ko);
+            if (q == ko + 1) return -c2c / s3;
+            if (q == ko - 2) return c2c / s3;
+            return 0.;
+        }
+        if (ko == 1) return q == 1 ? dz1w(1) : 0.;
+        if (ko == 2) {
+            const double mz = dz1w(f == 1 ? 2 : 1);
+            if (q == 2) return c1c * mz;
+            if (q == 1) return -c1c * mz;
+            if (q == 3) return -c2c / (dzw(1) + dzw(2) + dzw(3));
+            return 0.;
+        }
+        return q == nz - 1 ? -dz1w(nz) : 0.;   // ko == nz
+    }
+    __device__ double hz_fbar(int f, int i, int j, int q) const
+    {
+        double r = 0.;
+        for (int ko = q - 1; ko <= q + 2; ko++)
+            if (ko >= 1 && ko <= G.nz) r += A(f, i, j, ko) * hz_coef(f, ko, q);
+        return r;
+    }
+    __device__ double WTo(int f, int i, int j, int d, int q) const { return f == 0 ? T(2, i + d, j, q) : T(2, i, j + d, q); }
+    __device__ double hz_adv(int f, int i, int j, int k) const
+    {
+        const int nz = G.nz;
+        double r = 0.;
+        for (int q = k - 1; q <= k; q++) {
+            if (q < 1 || q > nz - 1) continue;
+            const double ww = c1c * (WTo(f, i, j, -1, q + 1) + WTo(f, i, j, 0, q + 1)) * 0.5 -
+                              c2c * (WTo(f, i, j, -2, q + 1) + WTo(f, i, j, 1, q + 1)) * 0.5;
+            const double wgt = (q == k ? dzw(q) : dzw(q + 1)) / (dzw(q + 1) + dzw(q));
+            r += hz_fbar(f, i, j, q) * ww * wgt;
+        }
+        if (G.lavisc)
+            for (int ko = k - 2; ko <= k + 2; ko++) {
+                if (ko < 3 || ko > nz - 2) continue;
+                const double mu = 0.25 * fabs(WTo(f, i, j, -1, ko) + WTo(f, i, j, 0, ko) + WTo(f, i, j, -1, ko + 1) +
+                                              WTo(f, i, j, 0, ko + 1)) * dz1w(ko);
+                r -= AVISC * A(f, i, j, ko) * mu * w4(k - ko);
+            }
+        return r;
+    }
+    __device__ double hz_w(int f, int i, int j, int k) const   // partial wrt w at (i, j, k)
+    {
+        const int nz = G.nz;
+        const double ra = rden(2, k);
+        double r = 0.;
+        const int q = k - 1;
+        if (q >= 1 && q <= nz - 1) {
+            const int ds[4] = {-1, 0, -2, 1};
+            for (int n = 0; n < 4; n++) {
+                const int ii = f == 0 ? i - ds[n] : i, jj = f == 0 ? j : j - ds[n];
+                const double gam = n < 2 ? 0.5 * c1c : -0.5 * c2c;
+                const double fr = (dzw(q + 1) * M(f, ii, jj, q + 1) + dzw(q) * M(f, ii, jj, q)) / (dzw(q + 1) + dzw(q));
+                r += hz_fbar(f, ii, jj, q) * fr * gam * ra;
+            }
+        }
+        if (G.lavisc)
+            for (int s = 0; s <= 1; s++) {   // outputs at the column itself and one further along
+                const int ii = f == 0 ? i + s : i, jj = f == 0 ? j : j + s;
+                for (int ko = k - 1; ko <= k; ko++) {
+                    if (ko < 3 || ko > nz - 2) continue;
+                    const double sw = WTo(f, ii, jj, -1, ko) + WTo(f, ii, jj, 0, ko) + WTo(f, ii, jj, -1, ko + 1) +
+                                      WTo(f, ii, jj, 0, ko + 1);
+                    const double d4 = -M(f, ii, jj, ko + 2) + 4. * M(f, ii, jj, ko + 1) - 6. * M(f, ii, jj, ko) +
+                                      4. * M(f, ii, jj, ko - 1) - M(f, ii, jj, ko - 2);
+                    r -= AVISC * A(f, ii, jj, ko) * d4 * 0.25 * dz1w(ko) * sgnd(sw) * ra;
+                }
+            }
+        return r;
+    }
+
+    // ---- w_h (dir 0: velocity u along x; dir 1: v along y), outputs w at levels 2..nz ----
+    // weight of the velocity at level q in uu of the output at level kw
+    __device__ double wh_lam(int kw, int q) const
+    {
+        const int nz = G.nz;
+        if (kw == 2) return (q == 2 || q == 1) ? 0.5 : 0.;
+        if (kw == nz) return (q == nz || q == nz - 1) ? 0.5 : 0.;
+        if (q == kw || q == kw - 1) return 0.5 * c1c;
+        if (q == kw + 1 || q == kw - 2) return -0.5 * c2c;
+        return 0.;
+    }
+    __device__ double wh_fbar(int dir, int p, int t, int kw) const { return cross_fbar(2, dir, p, t, kw); }
+    __device__ double wh_w(int dir, int i, int j, int k) const   // partial wrt w (advected) at (i, j, k)
+    {
+        if (k < 2) return 0.;
+        const int a0 = dir == 0 ? i : j, t = dir == 0 ? j : i;
+        double r = 0.;
+        for (int p = a0 - 1; p <= a0; p++) {
+            double uu = 0.;
+            for (int q = k - 2; q <= k + 1; q++) {
+                const double l = wh_lam(k, q);
+                if (l != 0.) uu += l * Ta(dir, dir, p + 1, t, q);
+            }
+            r += wh_fbar(dir, p, t, k) * 0.5 * uu;
+        }
+        if (G.lavisc)
+            for (int o = a0 - 2; o <= a0 + 2; o++) {
+                const int ob = wrap_a(dir, o);
+                const double mu = 0.25 * fabs(Ta(dir, dir, ob, t, k) + Ta(dir, dir, ob, t, k - 1) + Ta(dir, dir, ob + 1, t, k) +
+                                              Ta(dir, dir, ob + 1, t, k - 1)) * d1(dir);
+                r -= AVISC * Aa(2, dir, ob, t, k) * mu * w4(a0 - o);
+            }
+        return r;
+    }
+    __device__ double wh_vel(int dir, int i, int j, int k) const   // partial wrt the velocity momentum (u or v)
+    {
+        const int nz = G.nz;
+        const int a0 = dir == 0 ? i : j, t = dir == 0 ? j : i;
+        const double rd = rden(dir, k);
+        double r = 0.;
+        for (int kw = k - 1; kw <= k + 2; kw++) {
+            if (kw < 2 || kw > nz) continue;
+            const double l = wh_lam(kw, k);
+            if (l == 0.) continue;
+            const double fr = 0.5 * (Ma(2, dir, a0, t, kw) + Ma(2, dir, a0 - 1, t, kw));
+            r += wh_fbar(dir, a0 - 1, t, kw) * fr * l * rd;
+        }
+        if (G.lavisc)
+            for (int kw = k; kw <= k + 1; kw++) {
+                if (kw < 2 || kw > nz) continue;
+                for (int o = a0 - 1; o <= a0; o++) {
+                    const double s = Ta(dir, dir, o, t, kw) + Ta(dir, dir, o, t, kw - 1) + Ta(dir, dir, o + 1, t, kw) +
+                                     Ta(dir, dir, o + 1, t, kw - 1);
+                    const double d4 = -Ma(2, dir, o + 2, t, kw) + 4. * Ma(2, dir, o + 1, t, kw) - 6. * Ma(2, dir, o, t, kw) +
+                                      4. * Ma(2, dir, o - 1, t, kw) - Ma(2, dir, o - 2, t, kw);
+                    r -= AVISC * Aa(2, dir, o, t, kw) * d4 * 0.25 * d1(dir) * sgnd(s) * rd;
+                }
+            }
+        return r;
+    }
+
+    // ---- w_z, outputs w at levels 2..nz ----
+    __device__ double wz_fcoef(int ko, int q) const
+    {
+        const int nz = G.nz;
+        if (ko >= 3 && ko <= nz - 1) return q == ko ? c1s * dz1(ko - 1) : (q == ko - 1 ? -c1s * dz1(ko - 1) : 0.);
+        if (ko == 2) return q == 2 ? c1s * dz1(1) : (q == 1 ? -c1s * dz1(1) : 0.);
+        if (ko == nz) return q == nz - 1 ? -dz1(nz - 1) : 0.;
+        return 0.;
+    }
+    __device__ double wz_acoef(int ko, int q) const
+    {
+        const int nz = G.nz;
+        if (ko >= 3 && ko <= nz - 1) {
+            const double s = dzw(ko) + dzw(ko - 1);
+            return q == ko ? -c2s / s : (q == ko - 2 ? c2s / s : 0.);
+        }
+        if (ko == 2) return q == 2 ? -c2s / (dzw(2) + dzw(1)) : 0.;
+        return 0.;
+    }
+    __device__ double wz_w(int i, int j, int k) const
+    {
+        const int nz = G.nz;
+        const double ra = rden(2, k);
+        auto W = [&](int q) { return M(2, i, j, q); };
+        auto WT = [&](int q) { return T(2, i, j, q); };
+        double r = 0.;
+        for (int q = k - 1; q <= k; q++) {   // F(q) = avg WT(q, q+1) * avg W(q, q+1)
+            if (q < 1 || q > nz - 1) continue;
+            const double fb = A(2, i, j, q) * wz_fcoef(q, q) + A(2, i, j, q + 1) * wz_fcoef(q + 1, q);
+            r += fb * 0.25 * ((W(q + 1) + W(q)) * ra + (WT(q + 1) + WT(q)));
+        }
+        for (int q = k - 2; q <= k; q += 2) {   // A(q): W(q) and W(q+2), or W(nz-1) alone at q = nz-1
+            if (q < 1 || q > nz - 1) continue;
+            const double gb = A(2, i, j, q) * wz_acoef(q, q) + A(2, i, j, q + 2) * wz_acoef(q + 2, q);
+            if (gb == 0.) continue;
+            if (q == nz - 1) {
+                if (k != q) continue;
+                const double dl = dzw(nz - 1), sg = dzw(nz) + dzw(nz - 1);
+                r += gb * dl * dl / (sg * sg) * (W(q) * ra + WT(q));
+            } else {
+                const double al = dzw(q + 1), be = dzw(q), sg = al + be;
+                const double ww2 = (al * WT(q + 2) + be * WT(q)) / sg, fr2 = (al * W(q + 2) + be * W(q)) / sg;
+                r += gb * (k == q + 2 ? al : be) / sg * (fr2 * ra + ww2);
+            }
+        }
+        if (G.lavisc) {
+            for (int ko = k - 2; ko <= k + 2; ko++) {
+                if (ko < 3 || ko > nz - 2) continue;
+                r -= AVISC * A(2, i, j, ko) * fabs(WT(ko)) * dz1(ko - 1) * w4(k - ko);
+            }
+            if (k >= 3 && k <= nz - 2) {
+                const double d4 = -W(k + 2) + 4. * W(k + 1) - 6. * W(k) + 4. * W(k - 1) - W(k - 2);
+                r -= AVISC * A(2, i, j, k) * dz1(k - 1) * sgnd(WT(k)) * ra * d4;
+            }
+        }
+        return r;
+    }
+};
+
+__global__ void __launch_bounds__(128) mom_ad_gather_kernel(DevGrid G, Mom3 v, Mom3 ab, Mom3 bar)
 {
     const int i = 4 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 4 + blockIdx.y;
     const int k = 1 + blockIdx.z;
     if (i > G.nx - 2) return;
+    const Gath g(G, v, ab);
     const long long q = gidx(G, i, j, k);
-    const double ab = abar[q];
-    if (ab == 0.) return;
-    const LoadAD ld{G, v, i, j, k, s0, slot};
-    const D<NCH> a = adv_comp<D<NCH>>(G, ld, c, ntime, i, j, k);
-    for (int t = 0; t < NCH && s0 + t < nslot; t++) {
-        const int code = offs[s0 + t];
-        const int dk = code % 5 - 2, dj = (code / 5) % 5 - 2, di = (code / 25) % 5 - 2, f = code / 125;
-        // the offsets are the union over all levels; near the surface and the lid some of
-        // them point outside 1..nz, where the stencils read nothing (the partial is 0)
-        if (k + dk < 1 || k + dk > G.nz) continue;
-        const long long tq = gidx(G, wrap_x(G, i + di), wrap_y(G, j + dj), k + dk);
-        atomicAdd(const_cast<double *>(bar.m[f]) + tq, a.d[t] * ab);
-    }
+    double *ub = const_cast<double *>(bar.m[0]), *vb = const_cast<double *>(bar.m[1]), *wb = const_cast<double *>(bar.m[2]);
+    // u: u_x, u_y (advected), h_z (f 0, advected), v_x (velocity), w_h x (velocity)
+    ub[q] += g.self_h(0, i, j, k) + g.cross_adv(0, i, j, k) + g.hz_adv(0, i, j, k) + g.cross_vel(1, i, j, k) +
+             g.wh_vel(0, i, j, k);
+    // v: v_y, v_x (advected), h_z (f 1, advected), u_y (velocity), w_h y (velocity)
+    vb[q] += g.self_h(1, i, j, k) + g.cross_adv(1, i, j, k) + g.hz_adv(1, i, j, k) + g.cross_vel(0, i, j, k) +
+             g.wh_vel(1, i, j, k);
+    // w: w_z, w_h x and y (advected), h_z f 0 and f 1 (velocity)
+    wb[q] += g.wz_w(i, j, k) + g.wh_w(0, i, j, k) + g.wh_w(1, i, j, k) + g.hz_w(0, i, j, k) + g.hz_w(1, i, j, k);
 }
 
 }  // namespace
-
-// host: offsets (per component) that qnadv_uvw reads, from a probe of one column
-struct MomAdjPlan {
-    short *slot = nullptr;   // [3][NOFF]
-    int *offs = nullptr;     // [3][NOFF] compact slot -> offset code
-    int nslot[3] = {0, 0, 0};
-};
-
-cudaError_t mom_adj_plan(const DevGrid &g, int ntime, const double *mu, const double *mv, const double *mw, void **plan,
-                         cudaStream_t s)
-{
-    MomAdjPlan *p = new MomAdjPlan();
-    int *mask = nullptr;
-    cudaError_t e = cudaMalloc(&mask, 3 * NOFF * sizeof(int));
-    if (e == cudaSuccess) e = cudaMemsetAsync(mask, 0, 3 * NOFF * sizeof(int), s);
-    if (e == cudaSuccess) {
-        // the deep interior column reads no periodic image twice
-        mom_probe_kernel<<<3, 1, 0, s>>>(g, ntime, Mom3{{mu, mv, mw}}, 4 + g.maxx / 2, 4 + g.maxy / 2, mask);
-        e = cudaGetLastError();
-    }
-    std::vector<int> hm(3 * NOFF, 0);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hm.data(), mask, hm.size() * sizeof(int), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    std::vector<short> hs(3 * NOFF, -1);
-    std::vector<int> ho(3 * NOFF, 0);
-    for (int c = 0; c < 3 && e == cudaSuccess; c++)
-        for (int o = 0; o < NOFF; o++)
-            if (hm[c * NOFF + o]) {
-                hs[c * NOFF + o] = (short)p->nslot[c];
-                ho[c * NOFF + p->nslot[c]] = o;
-                p->nslot[c]++;
-            }
-    if (e == cudaSuccess) e = cudaMalloc(&p->slot, hs.size() * sizeof(short));
-    if (e == cudaSuccess) e = cudaMalloc(&p->offs, ho.size() * sizeof(int));
-    if (e == cudaSuccess) e = cudaMemcpyAsync(p->slot, hs.data(), hs.size() * sizeof(short), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(p->offs, ho.data(), ho.size() * sizeof(int), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(mask);
-    if (e != cudaSuccess) {
-        cudaFree(p->slot); cudaFree(p->offs);
-        delete p;
-        return e;
-    }
-    *plan = p;
-    return cudaSuccess;
-}
-
-void mom_adj_plan_destroy(void *plan)
-{
-    MomAdjPlan *p = (MomAdjPlan *)plan;
-    if (!p) return;
-    cudaFree(p->slot);
-    cudaFree(p->offs);
-    delete p;
-}
 
 // val (optional) := qnadv_uvw(m) (positive convention), tan := its derivative along dm
 cudaError_t launch_qnadv_tl(const DevGrid &g, int ntime, const double *mu, const double *mv, const double *mw,
@@ -396,21 +615,14 @@ cudaError_t launch_qnadv_tl(const DevGrid &g, int ntime, const double *mu, const
     return cudaGetLastError();
 }
 
-// bar += (d qnadv / d m)^T abar (bar arrays must be zeroed by the caller for a plain adjoint)
-cudaError_t launch_qnadv_ad(const DevGrid &g, void *plan, int ntime, const double *mu, const double *mv, const double *mw,
-                            const double *aubar, const double *avbar, const double *awbar, double *mubar, double *mvbar,
-                            double *mwbar, cudaStream_t s)
+// bar += (d qnadv / d m)^T abar (bar arrays must be zeroed by the caller for a plain adjoint);
+// abar is read on the interior, the ghost entries of bar are left as they are
+cudaError_t launch_qnadv_ad(const DevGrid &g, const double *mu, const double *mv, const double *mw, const double *aubar,
+                            const double *avbar, const double *awbar, double *mubar, double *mvbar, double *mwbar,
+                            cudaStream_t s)
 {
-    MomAdjPlan *p = (MomAdjPlan *)plan;
-    if (!p) return cudaErrorInvalidValue;
     const dim3 grid((g.maxx + 127) / 128, g.maxy, g.nz);
-    const double *ab[3] = {aubar, avbar, awbar};
-    for (int c = 0; c < 3; c++)
-        for (int s0 = 0; s0 < p->nslot[c]; s0 += NCH) {
-            mom_ad_kernel<<<grid, 128, 0, s>>>(g, ntime, c, s0, p->nslot[c], Mom3{{mu, mv, mw}}, ab[c], p->slot + c * NOFF,
-                                               p->offs + c * NOFF, Mom3{{mubar, mvbar, mwbar}});
-            cudaError_t e = cudaGetLastError();
-            if (e != cudaSuccess) return e;
-        }
-    return cudaSuccess;
+    mom_ad_gather_kernel<<<grid, 128, 0, s>>>(g, Mom3{{mu, mv, mw}}, Mom3{{aubar, avbar, awbar}},
+                                              Mom3{{mubar, mvbar, mwbar}});
+    return cudaGetLastError();
 }

@@ -200,15 +200,12 @@ cudaError_t launch_convert_ad(const DevGrid &g, const TrajConvAd &a, cudaStream_
 cudaError_t launch_axpy(const DevGrid &g, double *y, const double *x, double alpha, cudaStream_t s);
 
 // tangent linear / adjoint of the momentum advection operator (k_momadj.cu)
-cudaError_t mom_adj_plan(const DevGrid &g, int ntime, const double *mu, const double *mv, const double *mw, void **plan,
-                         cudaStream_t s);
-void mom_adj_plan_destroy(void *plan);
 cudaError_t launch_qnadv_tl(const DevGrid &g, int ntime, const double *mu, const double *mv, const double *mw,
                             const double *dmu, const double *dmv, const double *dmw, double *au, double *av, double *aw,
                             double *dau, double *dav, double *daw, cudaStream_t s);
-cudaError_t launch_qnadv_ad(const DevGrid &g, void *plan, int ntime, const double *mu, const double *mv, const double *mw,
-                            const double *aubar, const double *avbar, const double *awbar, double *mubar, double *mvbar,
-                            double *mwbar, cudaStream_t s);
+cudaError_t launch_qnadv_ad(const DevGrid &g, const double *mu, const double *mv, const double *mw, const double *aubar,
+                            const double *avbar, const double *awbar, double *mubar, double *mvbar, double *mwbar,
+                            cudaStream_t s);
 
 // tangent linear / adjoint of the scalar advection operator (k_adjoint.cu)
 cudaError_t launch_advection_tl(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
