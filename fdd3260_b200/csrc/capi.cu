@@ -1726,6 +1726,19 @@ static int traj_adjoint_run(mg_ctx *c, int nsteps, int ntime0, int ckpt, const d
     for (int q = 0; q < nck; q++) ck[q] = nat_alloc(T.B, nf);
     for (int q = 0; q <= ckpt; q++) seg[q] = nat_alloc(T.B, nf);
     NatState bar = nat_alloc(T.B, nf), tmp = nat_alloc(T.B, nf);
+    // the stage records of every step of a segment, when they fit in half the free memory:
+    // the segment's forward recomputation then leaves them for its backward sweep;
+    // otherwise each backward step recomputes its own stages
+    size_t mfree = 0, mtot = 0;
+    CKR(T.B.err);
+    CKR(cudaMemGetInfo(&mfree, &mtot));
+    const bool keep = (double)ckpt * 2 * (2 * nf + 3) * (double)c->fbytes < 0.5 * (double)mfree;
+    std::vector<StageRec> rec1(keep ? ckpt : 0), rec2(keep ? ckpt : 0);
+    for (int q = 0; keep && q < ckpt; q++)
+        for (StageRec *R : {&rec1[q], &rec2[q]}) {
+            for (int f = 0; f < nf; f++) { R->xs[f] = T.B.get(); R->A[f] = T.B.get(); }
+            for (int m = 0; m < 3; m++) R->xm[m] = T.B.get();
+        }
     CKR(T.B.err);
     if (bytes) *bytes = (double)T.B.own.size() * (double)c->fbytes;
     CKR(nat_copy(c, ck[0], traj_resident(c), nf));
@@ -1742,6 +1755,14 @@ static int traj_adjoint_run(mg_ctx *c, int nsteps, int ntime0, int ckpt, const d
     for (int s0 = ((nsteps - 1) / ckpt) * ckpt; nsteps > 0 && s0 >= 0; s0 -= ckpt) {
         const int s1 = std::min(s0 + ckpt, nsteps);
         CKR(nat_copy(c, seg[0], ck[s0 / ckpt], nf));
+        if (keep) {
+            for (int s = s0; s < s1; s++)   // the segment's states and stage records
+                CKR(traj_step_fwd(c, ntime0 + s, seg[s - s0], seg[s - s0 + 1], rec1[s - s0], rec2[s - s0], T.ts, T.tm,
+                                  T.au));
+            for (int s = s1 - 1; s >= s0; s--)
+                CKR(traj_step_ad(c, ntime0 + s, seg[s - s0], seg[s - s0 + 1], rec1[s - s0], rec2[s - s0], bar, S));
+            continue;
+        }
         for (int s = s0; s < s1 - 1; s++)   // states at the starts of the segment's steps
             CKR(traj_step_fwd(c, ntime0 + s, seg[s - s0], seg[s - s0 + 1], T.R1, T.R2, T.ts, T.tm, T.au));
         for (int s = s1 - 1; s >= s0; s--) {

@@ -306,8 +306,11 @@ int mg_qnadv_ad(mg_ctx *ctx, int ntime, const double *mu, const double *mv, cons
  *   mg_traj_adjoint: g0 = (dx(T)/dx(0))^T lamT, the gradient of J = <lamT, x(T)> (interior
  *                    inner product) with respect to x(0); the forward sweep keeps a state
  *                    every ckpt steps and each segment is recomputed before its backward
- *                    sweep, so memory is (nsteps/ckpt + ckpt + ~30) fields.  Ghost entries
- *                    of g0 are 0. */
+ *                    sweep: (nsteps/ckpt + ckpt + 4) states of 4 + nf fields (nf = nscal
+ *                    + 1) and ~8 nf + 30 work fields, plus the segment's stage records,
+ *                    2 (2 nf + 3) fields per step, when they fit in half the free device
+ *                    memory (else each backward step recomputes its stages).  Ghost
+ *                    entries of g0 are 0. */
 int mg_traj_forward(mg_ctx *ctx, int nsteps, int ntime0);
 int mg_traj_tl(mg_ctx *ctx, int nsteps, int ntime0, const double *const *dx0, double *const *dxT);
 int mg_traj_adjoint(mg_ctx *ctx, int nsteps, int ntime0, int ckpt, const double *const *lamT, double *const *g0);
