@@ -30,7 +30,7 @@ struct mg_ctx {
     cudaStream_t stream = nullptr;
     DevGrid G{};
     int nf = 0;                          // 1 (density) + nscal
-    double *prof = nullptr;              // 9 profiles x nz
+    double *prof = nullptr;              // 11 profiles x nz
     std::vector<double> wv;
     size_t fbytes = 0;                   // bytes per field
     double *mA[3] = {}, *mB[3] = {}, *tm[3] = {};
@@ -290,17 +290,19 @@ extern "C" int mg_create(const mg_params *params, int device, mg_ctx **out)
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(cuerr(e));
     // profiles
-    e = cudaMalloc(&c->prof, 9 * nz * sizeof(double));
+    e = cudaMalloc(&c->prof, 11 * nz * sizeof(double));
     if (e != cudaSuccess) return fail(cuerr(e));
-    const double *src[9] = {params->fdz0, params->dzw, params->dz1w, params->dz1, params->den0,
-                            params->avden0, params->stab0, params->pt0, params->qv0};
-    for (int q = 0; q < 9; q++) {
+    std::vector<double> rden(2 * (size_t)nz);
+    for (int k = 0; k < nz; k++) { rden[k] = 1. / params->den0[k]; rden[nz + k] = 1. / params->avden0[k]; }
+    const double *src[11] = {params->fdz0, params->dzw, params->dz1w, params->dz1, params->den0, params->avden0,
+                             params->stab0, params->pt0, params->qv0, rden.data(), rden.data() + nz};
+    for (int q = 0; q < 11; q++) {
         e = cudaMemcpy(c->prof + q * nz, src[q], nz * sizeof(double), cudaMemcpyHostToDevice);
         if (e != cudaSuccess) return fail(cuerr(e));
     }
     G.fdz0 = c->prof; G.dzw = c->prof + nz; G.dz1w = c->prof + 2 * nz; G.dz1 = c->prof + 3 * nz;
     G.den0 = c->prof + 4 * nz; G.avden0 = c->prof + 5 * nz; G.stab0 = c->prof + 6 * nz;
-    G.pt0 = c->prof + 7 * nz; G.qv0 = c->prof + 8 * nz;
+    G.pt0 = c->prof + 7 * nz; G.qv0 = c->prof + 8 * nz; G.rden0 = c->prof + 9 * nz; G.ravden0 = c->prof + 10 * nz;
     // fields
     auto alloc = [&](double **p) -> int {
         cudaError_t ee = cudaMalloc(p, c->fbytes);

@@ -286,18 +286,25 @@ struct Gath {
     // (along, transverse) -> (i, j): direction 0 is x, 1 is y
     __device__ static int ci(int dir, int a, int t) { return dir == 0 ? a : t; }
     __device__ static int cj(int dir, int a, int t) { return dir == 0 ? t : a; }
-    __device__ int wrap_a(int dir, int a) const { return dir == 0 ? wrap_x(G, a) : wrap_y(G, a); }
+    __device__ int wx(int i) const { return wrap_x(G, i); }
+    __device__ int wy(int j) const { return wrap_y(G, j); }
+    __device__ int wrap_a(int dir, int a) const { return dir == 0 ? wx(a) : wy(a); }
     __device__ double M(int f, int i, int j, int k) const { return __ldg(m.m[f] + gidx(G, i, j, k)); }
-    __device__ double T(int f, int i, int j, int k) const { return adv_vel<double>(G, f, k, M(f, i, j, k)); }
+    // advective velocity with the reciprocal profiles (its partial is the same factor)
+    __device__ double T(int f, int i, int j, int k) const
+    {
+        const double x = M(f, i, j, k) * rden(f, k);
+        return f == 0 ? x - G.u0shift : (f == 1 ? x - G.v0shift : x);
+    }
     __device__ double A(int c, int i, int j, int k) const
     {
         if (k < 1 || k > G.nz || (c == 2 && k == 1)) return 0.;
-        return __ldg(ab.m[c] + gidx(G, wrap_x(G, i), wrap_y(G, j), k));
+        return __ldg(ab.m[c] + gidx(G, wx(i), wy(j), k));
     }
     __device__ double Ma(int f, int dir, int a, int t, int k) const { return M(f, ci(dir, a, t), cj(dir, a, t), k); }
     __device__ double Ta(int f, int dir, int a, int t, int k) const { return T(f, ci(dir, a, t), cj(dir, a, t), k); }
     __device__ double Aa(int c, int dir, int a, int t, int k) const { return A(c, ci(dir, a, t), cj(dir, a, t), k); }
-    __device__ double rden(int f, int k) const { return 1. / __ldg((f == 2 ? G.avden0 : G.den0) + k - 1); }
+    __device__ double rden(int f, int k) const { return __ldg((f == 2 ? G.ravden0 : G.rden0) + k - 1); }
     __device__ double dzw(int q) const { return __ldg(G.dzw + q - 1); }
     __device__ double dz1w(int q) const { return __ldg(G.dz1w + q - 1); }
     __device__ double dz1(int q) const { return __ldg(G.dz1 + q - 1); }

@@ -26,6 +26,7 @@ struct DevGrid {
     double dx, dy, dz, dt0, lim_tol, u0shift, v0shift;
     int scal_adv, muscl_lim, mom_ord, lavisc, with_buoy;
     const double *fdz0, *dzw, *dz1w, *dz1, *den0, *avden0, *stab0, *pt0, *qv0;  // device, nz each
+    const double *rden0, *ravden0;   // 1/den0, 1/avden0 (the linearised operators multiply by them)
 };
 
 __host__ __device__ inline long long gidx(const DevGrid &g, int i, int j, int k) {
