@@ -375,16 +375,25 @@ static int upload_impl(mg_ctx *c, const double *u, const double *v, const double
                        const double *dens, const double *const *scal, cudaMemcpyKind kind)
 {
     if (!c || !u || !v || !w || !p || !dens || !scal) return MG_ERR_PARAM;
-    CKR(cudaSetDevice(c->device));
-    CKR(h2d(c, c->mA[0], u, kind));
-    CKR(h2d(c, c->mA[1], v, kind));
-    CKR(h2d(c, c->mA[2], w, kind));
-    CKR(h2d(c, c->p, p, kind));
-    CKR(h2d(c, c->sA[0], dens, kind));
-    for (int s = 0; s < c->prm.nscal; s++) {
+    for (int s = 0; s < c->prm.nscal; s++)
         if (!scal[s]) return MG_ERR_PARAM;
-        CKR(h2d(c, c->sA[1 + s], scal[s], kind));
-    }
+    CKR(cudaSetDevice(c->device));
+    // host sources: one linear copy per field into a staging buffer (a stage buffer, free
+    // between steps), then unpacked into the padded layout; device sources are unpacked
+    // directly
+    const size_t packed = (size_t)c->G.nx * c->G.ny * c->G.nz * sizeof(double);
+    double *stage = c->sB[0];
+    auto put = [&](double *dst, const double *src) -> cudaError_t {
+        if (kind == cudaMemcpyDeviceToDevice) return launch_unpack(c->G, src, dst, c->stream);
+        cudaError_t e = cudaMemcpyAsync(stage, src, packed, kind, c->stream);
+        return e == cudaSuccess ? launch_unpack(c->G, stage, dst, c->stream) : e;
+    };
+    CKR(put(c->mA[0], u));
+    CKR(put(c->mA[1], v));
+    CKR(put(c->mA[2], w));
+    CKR(put(c->p, p));
+    CKR(put(c->sA[0], dens));
+    for (int s = 0; s < c->prm.nscal; s++) CKR(put(c->sA[1 + s], scal[s]));
     // ghost cells from the interior (the reference's state after update_prognostic)
     std::vector<double *> f = {c->mA[0], c->mA[1], c->mA[2], c->p};
     for (int q = 0; q < c->nf; q++) f.push_back(c->sA[q]);
@@ -423,9 +432,16 @@ static int download_impl(mg_ctx *c, double *u, double *v, double *w, double *p, 
     if (scal)
         for (int s = 0; s < c->prm.nscal; s++)
             if (scal[s]) items.push_back({scal[s], c->sA[1 + s], c->sA[0], 3});
+    // natural values written packed (nx*ny*nz), then one linear copy per field; device
+    // destinations receive them directly
+    const size_t packed = (size_t)G.nx * G.ny * G.nz * sizeof(double);
     for (auto &it : items) {
-        CKR(launch_to_natural(G, it.src, it.w, it.kind, c->rep, tmp, c->stream));
-        CKR(d2h(c, it.dst, tmp, kind));
+        if (kind == cudaMemcpyDeviceToDevice) {
+            CKR(launch_to_natural_packed(G, it.src, it.w, it.kind, c->rep, it.dst, c->stream));
+            continue;
+        }
+        CKR(launch_to_natural_packed(G, it.src, it.w, it.kind, c->rep, tmp, c->stream));
+        CKR(cudaMemcpyAsync(it.dst, tmp, packed, kind, c->stream));
     }
     return cuerr(cudaStreamSynchronize(c->stream));
 }

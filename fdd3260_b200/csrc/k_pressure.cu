@@ -741,18 +741,35 @@ __global__ void halo_fill_kernel(DevGrid G, HaloArgs H)
     }
 }
 
-__global__ void to_natural_kernel(DevGrid G, const double *src, const double *w, int kind, int rep, double *dst)
+// download conversion (get_velocities / get_scalars, funcpack.f90:65-178,429-485): the
+// natural value of a resident field (REP_CONS: divided by its weight) written into a
+// packed nx*ny*nz array (the reference layout without the row padding of the device
+// layout), so that the host copy is one linear transfer
+__global__ void to_natural_packed_kernel(DevGrid G, const double *src, const double *w, int kind, int rep, double *dst)
 {
-    const long long n = G.ps * G.nz;
+    const long long n = (long long)G.nx * G.ny * G.nz, plane = (long long)G.nx * G.ny;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        int k = (int)(t / G.ps) + 1;
-        double x = src[t];
+        const int k = (int)(t / plane) + 1;
+        const long long r = t - (k - 1) * plane;
+        const int j = (int)(r / G.nx) + 1, i = (int)(r - (long long)(j - 1) * G.nx) + 1;
+        const long long q = gidx(G, i, j, k);
+        double x = src[q];
         if (rep == REP_CONS) {
             if (kind == 1) x = x / __ldg(G.den0 + k - 1);
             else if (kind == 2) x = x / __ldg(G.avden0 + k - 1);
-            else if (kind == 3) x = x / w[t];
+            else if (kind == 3) x = x / w[q];
         }
         dst[t] = x;
+    }
+}
+
+// packed nx*ny*nz -> device layout (the padding columns are left as they are)
+__global__ void unpack_kernel(DevGrid G, const double *src, double *dst)
+{
+    const long long n = (long long)G.nx * G.ny * G.nz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long row = t / G.nx;
+        dst[row * G.px + (t - row * G.nx)] = src[t];
     }
 }
 
@@ -1110,10 +1127,15 @@ cudaError_t launch_halo_fill(const DevGrid &g, double *const *fields, int nf, cu
     return cudaSuccess;
 }
 
-cudaError_t launch_to_natural(const DevGrid &g, const double *src, const double *w, int weight_kind, int rep,
-                              double *dst, cudaStream_t s)
+cudaError_t launch_to_natural_packed(const DevGrid &g, const double *src, const double *w, int weight_kind, int rep,
+                                     double *dst, cudaStream_t s)
 {
-    to_natural_kernel<<<1184, 256, 0, s>>>(g, src, w, weight_kind, rep, dst);
+    to_natural_packed_kernel<<<1184, 256, 0, s>>>(g, src, w, weight_kind, rep, dst);
+    return cudaGetLastError();
+}
+cudaError_t launch_unpack(const DevGrid &g, const double *src, double *dst, cudaStream_t s)
+{
+    unpack_kernel<<<1184, 256, 0, s>>>(g, src, dst);
     return cudaGetLastError();
 }
 

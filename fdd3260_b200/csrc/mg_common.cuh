@@ -273,8 +273,10 @@ const double *pressure_maxdiv_dev(const PressurePlan *pp);
 cudaError_t pressure_adjoint(const DevGrid &g, PressurePlan *pp, int nsubp, double *mub, double *mvb, double *mwb,
                              double *pb, cudaStream_t s);
 
-// natural <-> resident conversions for download
-cudaError_t launch_to_natural(const DevGrid &g, const double *src, const double *w, int weight_kind,
-                              int rep, double *dst, cudaStream_t s);
+// host-layout transfers: the natural value of a resident field into a packed nx*ny*nz
+// array (download); packed nx*ny*nz -> device layout (upload)
+cudaError_t launch_to_natural_packed(const DevGrid &g, const double *src, const double *w, int weight_kind, int rep,
+                                     double *dst, cudaStream_t s);
+cudaError_t launch_unpack(const DevGrid &g, const double *src, double *dst, cudaStream_t s);
 // copy with pitch change: halo'd host layout (nx) <-> device layout (px)
 

@@ -170,13 +170,25 @@ class Mimica:
         _lib.check(self._L.mg_upload_state(self._h, _lib.ptr(st.u), _lib.ptr(st.v), _lib.ptr(st.w), _lib.ptr(st.p),
                                            _lib.ptr(st.dens), sp), "mg_upload_state")
 
-    def download(self) -> State:
+    def download(self, out: State | None = None) -> State:
+        """The resident state in natural variables.  out: arrays to fill (C-contiguous
+        float64 of the domain's shape, e.g. page-locked buffers reused across steps)."""
         d = self.domain
-        u, v, w, p, dens = (np.zeros(d.shape) for _ in range(5))
-        scal = [np.zeros(d.shape) for _ in range(self.nscal)]
+        if out is None:
+            u, v, w, p, dens = (np.zeros(d.shape) for _ in range(5))
+            scal = [np.zeros(d.shape) for _ in range(self.nscal)]
+        else:
+            u, v, w, p, dens, scal = out.u, out.v, out.w, out.p, out.dens, list(out.scal)
+            if len(scal) != self.nscal:
+                raise ValueError(f"out has {len(scal)} scalars, the context {self.nscal}")
+            for a in (u, v, w, p, dens, *scal):
+                if a.shape != d.shape or a.dtype != np.float64 or not a.flags.c_contiguous or not a.flags.writeable:
+                    raise ValueError("out arrays must be writeable C-contiguous float64 of the domain's shape")
         sp = (_lib._dp * len(scal))(*[_lib.ptr(a) for a in scal])
         _lib.check(self._L.mg_download_state(self._h, _lib.ptr(u), _lib.ptr(v), _lib.ptr(w), _lib.ptr(p),
                                              _lib.ptr(dens), sp), "mg_download_state")
+        if out is not None:
+            return out
         return State(u, v, w, p, dens, scal, self.iqt)
 
     def upload_device(self, ptrs: dict) -> None:
