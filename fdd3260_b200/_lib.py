@@ -68,6 +68,14 @@ class MgCheckResult(C.Structure):
     ]
 
 
+class MgTune(C.Structure):
+    _fields_ = [
+        ("x_nstage", C.c_int), ("x_radix", C.c_int * 16), ("y_nstage", C.c_int), ("y_radix", C.c_int * 16),
+        ("x_threads", C.c_int), ("y_threads", C.c_int), ("tri_block", C.c_int), ("candidates", C.c_int),
+        ("ms_default", C.c_double), ("ms_tuned", C.c_double),
+    ]
+
+
 class MimicaError(RuntimeError):
     def __init__(self, code: int, where: str):
         self.code = code
@@ -127,6 +135,10 @@ def lib() -> C.CDLL:
         L.mg_traj_tl.argtypes = [vp, C.c_int, C.c_int, C.POINTER(_dp), C.POINTER(_dp)]
         L.mg_traj_adjoint.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(_dp), C.POINTER(_dp)]
         L.mg_time_traj.argtypes = [vp, C.c_int, C.c_int, C.c_int, _dp]
+        L.mg_autotune.argtypes = [vp, C.c_int, C.POINTER(MgTune)]
+        L.mg_tune_get.argtypes = [vp, C.POINTER(MgTune)]
+        L.mg_tune_set.argtypes = [vp, C.POINTER(MgTune)]
+        L.mg_radix_candidates.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]
         L.mg_qnadv_tl.argtypes = [vp, C.c_int] + [_dp] * 12
         L.mg_qnadv_ad.argtypes = [vp, C.c_int] + [_dp] * 9
         L.mg_set_sgs.argtypes = [vp, C.POINTER(MgSgsParams)]
@@ -169,4 +181,5 @@ EXPORTED = [
     "mg_set_sgs", "mg_set_surface_fluxes", "mg_sgs_profiles", "mg_calc_subgrid", "mg_efud", "mg_eff",
     "mg_checkall", "mg_cfl_dt", "mg_set_dt", "mg_download_ksgs", "mg_qnadv_tl", "mg_qnadv_ad",
     "mg_traj_forward", "mg_traj_tl", "mg_traj_adjoint", "mg_time_traj",
+    "mg_autotune", "mg_tune_get", "mg_tune_set", "mg_radix_candidates",
 ]

@@ -2063,3 +2063,159 @@ extern "C" int mg_profile_report(mg_ctx *c, char *buf, size_t len)
     }
     return MG_OK;
 }
+
+// ---------------- autotuner: the projection's plan ----------------
+static void knobs_to_tune(const PressureKnobs &k, mg_tune *t)
+{
+    t->x_nstage = k.xst;
+    t->y_nstage = k.yst;
+    for (int q = 0; q < 16; q++) {
+        t->x_radix[q] = q < k.xst ? (int)((k.xr >> (4 * q)) & 15ull) : 0;
+        t->y_radix[q] = q < k.yst ? (int)((k.yr >> (4 * q)) & 15ull) : 0;
+    }
+    t->x_threads = k.xt;
+    t->y_threads = k.yt;
+    t->tri_block = k.tb;
+}
+
+static bool tune_to_knobs(const mg_tune *t, PressureKnobs *k)
+{
+    if (t->x_nstage < 1 || t->x_nstage > 16 || t->y_nstage < 1 || t->y_nstage > 16) return false;
+    k->xr = k->yr = 0ull;
+    for (int q = 0; q < t->x_nstage; q++) {
+        if (t->x_radix[q] < 2 || t->x_radix[q] > 8) return false;
+        k->xr |= (unsigned long long)t->x_radix[q] << (4 * q);
+    }
+    for (int q = 0; q < t->y_nstage; q++) {
+        if (t->y_radix[q] < 2 || t->y_radix[q] > 8) return false;
+        k->yr |= (unsigned long long)t->y_radix[q] << (4 * q);
+    }
+    k->xst = t->x_nstage;
+    k->yst = t->y_nstage;
+    k->xt = t->x_threads;
+    k->yt = t->y_threads;
+    k->tb = t->tri_block;
+    return true;
+}
+
+extern "C" int mg_tune_get(mg_ctx *c, mg_tune *t)
+{
+    if (!c || !t) return MG_ERR_PARAM;
+    memset(t, 0, sizeof(*t));
+    PressureKnobs k;
+    pressure_get_knobs(c->pp, &k);
+    knobs_to_tune(k, t);
+    return MG_OK;
+}
+
+extern "C" int mg_tune_set(mg_ctx *c, const mg_tune *t)
+{
+    if (!c || !t) return MG_ERR_PARAM;
+    PressureKnobs k;
+    if (!tune_to_knobs(t, &k) || !pressure_set_knobs(c->pp, c->G, k)) return MG_ERR_PARAM;
+    drop_graphs(c);
+    return MG_OK;
+}
+
+extern "C" int mg_radix_candidates(int n, int *radix, int *nstage, int maxc)
+{
+    if (n < 1 || !radix || !nstage || maxc < 1) return MG_ERR_PARAM;
+    std::vector<unsigned long long> pk(maxc);
+    std::vector<int> ns(maxc);
+    const int nc = pressure_radix_candidates(n, pk.data(), ns.data(), maxc);
+    for (int q = 0; q < nc; q++) {
+        nstage[q] = ns[q];
+        for (int s = 0; s < 16; s++) radix[16 * q + s] = s < ns[q] ? (int)((pk[q] >> (4 * s)) & 15ull) : 0;
+    }
+    return nc;
+}
+
+// mean device time (ms) of one projection of copies of the resident momentum and
+// pressure (the copies are refreshed before every projection, outside the timed part)
+static int time_projection(mg_ctx *c, int reps, double *ms)
+{
+    int rc = ensure_unit(c, 4);
+    if (rc) return rc;
+    double *u = c->unit[0], *v = c->unit[1], *w = c->unit[2], *p = c->unit[3];
+    cudaEvent_t e0, e1;
+    CKR(cudaEventCreate(&e0));
+    cudaError_t er = cudaEventCreate(&e1);
+    if (er != cudaSuccess) { cudaEventDestroy(e0); return cuerr(er); }
+    double tot = 0.;
+    for (int r = 0; r <= reps && er == cudaSuccess; r++) {   // r = 0: untimed warm-up
+        double *src[4] = {c->mA[0], c->mA[1], c->mA[2], c->p}, *dst[4] = {u, v, w, p};
+        for (int q = 0; q < 4 && er == cudaSuccess; q++)
+            er = cudaMemcpyAsync(dst[q], src[q], c->fbytes, cudaMemcpyDeviceToDevice, c->stream);
+        if (er == cudaSuccess) er = cudaEventRecord(e0, c->stream);
+        if (er == cudaSuccess) {
+            double *psave = c->p;
+            c->p = p;
+            int launches = 0;
+            er = project(c, u, v, w, w, -1, 0, 0, 0, &launches);
+            c->p = psave;
+        }
+        if (er == cudaSuccess) er = cudaEventRecord(e1, c->stream);
+        if (er == cudaSuccess) er = cudaEventSynchronize(e1);
+        float f = 0.f;
+        if (er == cudaSuccess) er = cudaEventElapsedTime(&f, e0, e1);
+        if (r > 0) tot += f;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (er != cudaSuccess) return cuerr(er);
+    *ms = tot / reps;
+    return check_err(c);
+}
+
+extern "C" int mg_autotune(mg_ctx *c, int reps, mg_tune *result)
+{
+    if (!c || reps < 1 || reps > 1000) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    PressureKnobs cur, k;
+    pressure_get_knobs(c->pp, &cur);
+    double best = 0., t = 0.;
+    int rc = time_projection(c, reps, &best);
+    if (rc) return rc;
+    const double ms_default = best;
+    int ncand = 1;
+    // one coordinate at a time; a change is kept when it gains more than 1 %
+    auto trial = [&](const PressureKnobs &cand) -> int {
+        if (!pressure_knobs_valid(c->G, cand)) return MG_OK;
+        pressure_set_knobs(c->pp, c->G, cand);
+        int r = time_projection(c, reps, &t);
+        if (r) { pressure_set_knobs(c->pp, c->G, cur); return r; }
+        ncand++;
+        if (t < 0.99 * best) { best = t; cur = cand; }
+        pressure_set_knobs(c->pp, c->G, cur);
+        return MG_OK;
+    };
+    unsigned long long pk[16];
+    int ns[16];
+    for (int axis = 0; axis < 2; axis++) {
+        const int nc = pressure_radix_candidates(axis == 0 ? c->G.maxx : c->G.maxy, pk, ns, 16);
+        for (int q = 0; q < nc; q++) {
+            k = cur;
+            if (axis == 0) { k.xr = pk[q]; k.xst = ns[q]; } else { k.yr = pk[q]; k.yst = ns[q]; }
+            if (axis == 0 ? (k.xr == cur.xr && k.xst == cur.xst) : (k.yr == cur.yr && k.yst == cur.yst)) continue;
+            if ((rc = trial(k))) return rc;
+        }
+    }
+    for (int xt = 8; xt <= 64; xt *= 2)
+        if (xt != cur.xt) { k = cur; k.xt = xt; if ((rc = trial(k))) return rc; }
+    for (int yt = 16; yt <= 128; yt *= 2)
+        if (yt != cur.yt) { k = cur; k.yt = yt; if ((rc = trial(k))) return rc; }
+    for (int tb = 64; tb <= 256; tb *= 2)
+        if (tb != cur.tb) { k = cur; k.tb = tb; if ((rc = trial(k))) return rc; }
+    pressure_set_knobs(c->pp, c->G, cur);
+    drop_graphs(c);
+    double tuned = 0.;
+    if ((rc = time_projection(c, reps, &tuned))) return rc;
+    if (result) {
+        memset(result, 0, sizeof(*result));
+        knobs_to_tune(cur, result);
+        result->candidates = ncand;
+        result->ms_default = ms_default;
+        result->ms_tuned = tuned;
+    }
+    return MG_OK;
+}

@@ -810,6 +810,7 @@ struct PressurePlan {
     double *gamT = nullptr, *akT = nullptr, *ckT = nullptr;   // transposed system (adjoint), built on first use
     int npartial = 0;
     size_t bytes = 0;
+    int xt = 32, yt = 32, tb = 128;   // launch shapes (threads per x row pair, per y row, per tridiagonal block)
 };
 
 static cudaError_t make_twiddles(int n, double2 **out)
@@ -854,6 +855,10 @@ cudaError_t pressure_plan_create(const DevGrid &g, const double *wv_host, int mi
         return cudaErrorInvalidValue;
     }
     pp->mixed = mixed ? 1 : 0;
+    pp->xt = g.maxx / 8 < 32 ? 32 : (g.maxx / 8 > XT_THREADS / (ROWS / 2) ? XT_THREADS / (ROWS / 2) : g.maxx / 8);
+    // fft_y<double2> holds 74 registers per thread: at most 512 threads per block (YROWS rows)
+    pp->yt = g.maxy / 8 < 32 ? 32 : (g.maxy / 8 > 128 ? 128 : g.maxy / 8);
+    pp->tb = 128;
     CK(make_twiddles(g.maxx, &pp->twx));
     CK(make_twiddles(g.maxy, &pp->twy));
     CK(make_twiddles_f(g.maxx, &pp->twxf));
@@ -943,6 +948,83 @@ void pressure_plan_destroy(PressurePlan *pp)
 }
 
 size_t pressure_plan_bytes(const PressurePlan *pp) { return pp ? pp->bytes : 0; }
+
+// ---- the autotuner's search space: radix sequences and launch shapes ----
+static bool radices_ok(int n, unsigned long long pk, int nst)
+{
+    if (nst < 1 || nst > MAXSTAGES) return false;
+    long long prod = 1;
+    for (int q = 0; q < nst; q++) {
+        const int r = (int)((pk >> (4 * q)) & 15ull);
+        if (r != 2 && r != 3 && r != 4 && r != 5 && r != 8) return false;
+        prod *= r;
+    }
+    return prod == n && (pk >> (4 * nst)) == 0ull;
+}
+
+void pressure_get_knobs(const PressurePlan *pp, PressureKnobs *k)
+{
+    k->xr = pp->px.rpack; k->xst = pp->px.nst;
+    k->yr = pp->py.rpack; k->yst = pp->py.nst;
+    k->xt = pp->xt; k->yt = pp->yt; k->tb = pp->tb;
+}
+
+bool pressure_knobs_valid(const DevGrid &g, const PressureKnobs &k)
+{
+    auto pow2_in = [](int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; };
+    return radices_ok(g.maxx, k.xr, k.xst) && radices_ok(g.maxy, k.yr, k.yst) && pow2_in(k.xt, 8, XT_THREADS / (ROWS / 2)) &&
+           pow2_in(k.yt, 16, 128) && pow2_in(k.tb, 64, 256);
+}
+
+bool pressure_set_knobs(PressurePlan *pp, const DevGrid &g, const PressureKnobs &k)
+{
+    if (!pressure_knobs_valid(g, k)) return false;
+    pp->px.rpack = k.xr; pp->px.nst = k.xst;
+    pp->py.rpack = k.yr; pp->py.nst = k.yst;
+    pp->xt = k.xt; pp->yt = k.yt; pp->tb = k.tb;
+    return true;
+}
+
+// distinct radix sequences for n = 2^a 3^b 5^c: the power-of-two part as radix 8 (then 4
+// or 2) or as radix 4 (then 2), the odd radices after or before it, each also reversed
+int pressure_radix_candidates(int n, unsigned long long *pk, int *nst, int maxc)
+{
+    int a = 0, b = 0, c = 0, m = n;
+    while (m % 2 == 0) { m /= 2; a++; }
+    while (m % 3 == 0) { m /= 3; b++; }
+    while (m % 5 == 0) { m /= 5; c++; }
+    if (m != 1) return 0;
+    std::vector<std::vector<int>> two(2), cand;
+    for (int q = 0; q < a / 3; q++) two[0].push_back(8);
+    if (a % 3 == 2) two[0].push_back(4);
+    if (a % 3 == 1) two[0].push_back(2);
+    for (int q = 0; q < a / 2; q++) two[1].push_back(4);
+    if (a % 2) two[1].push_back(2);
+    std::vector<int> odd;
+    for (int q = 0; q < b; q++) odd.push_back(3);
+    for (int q = 0; q < c; q++) odd.push_back(5);
+    for (auto &t : two)
+        for (int oddfirst = 0; oddfirst < 2; oddfirst++) {
+            std::vector<int> v = oddfirst ? odd : t;
+            const std::vector<int> &w = oddfirst ? t : odd;
+            v.insert(v.end(), w.begin(), w.end());
+            cand.push_back(v);
+            cand.push_back(std::vector<int>(v.rbegin(), v.rend()));
+        }
+    int nc = 0;
+    for (auto &v : cand) {
+        if (v.empty() || (int)v.size() > MAXSTAGES) continue;
+        unsigned long long p = 0;
+        for (size_t q = 0; q < v.size(); q++) p |= (unsigned long long)v[q] << (4 * q);
+        bool dup = false;
+        for (int q = 0; q < nc; q++) dup = dup || (pk[q] == p && nst[q] == (int)v.size());
+        if (dup || nc >= maxc) continue;
+        pk[nc] = p;
+        nst[nc] = (int)v.size();
+        nc++;
+    }
+    return nc;
+}
 const double *pressure_p1_dev(const PressurePlan *pp) { return pp->p1; }
 const double *pressure_maxdiv_dev(const PressurePlan *pp) { return pp->maxdiv; }
 const unsigned long long *pressure_resid_dev(const PressurePlan *pp) { return pp->resid; }
@@ -961,7 +1043,7 @@ template <typename C>
 static cudaError_t launch_x_fwd_t(const DevGrid &g, PressurePlan *pp, const XArgs &a, cudaStream_t s)
 {
     int groups = (g.maxy + ROWS - 1) / ROWS;
-    int nt_pair = g.maxx / 8 < 32 ? 32 : (g.maxx / 8 > XT_THREADS / (ROWS / 2) ? XT_THREADS / (ROWS / 2) : g.maxx / 8);
+    const int nt_pair = pp->xt;
     size_t sm = (size_t)(ROWS / 2) * 2 * g.maxx * sizeof(C);
     cudaError_t e = cudaFuncSetAttribute(fft_x_fwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
@@ -1022,7 +1104,7 @@ static cudaError_t pressure_solve_t(const DevGrid &g, PressurePlan *pp, int keep
     cudaError_t e;
     const int nh = g.maxx / 2 + 1;
     const int nrows = g.nz * nh;
-    int nt_row = g.maxy / 8 < 32 ? 32 : (g.maxy / 8 > 256 ? 256 : g.maxy / 8);
+    const int nt_row = pp->yt;
     size_t smy = (size_t)YROWS * 2 * g.maxy * sizeof(C);
     e = cudaFuncSetAttribute(fft_y<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy);
     if (e != cudaSuccess) return e;
@@ -1035,12 +1117,12 @@ static cudaError_t pressure_solve_t(const DevGrid &g, PressurePlan *pp, int keep
     T.sk = sk;
     T.scratch = pp->tri;
     long long ncol = (long long)nh * g.maxy;
-    tridiag_kernel<C><<<(unsigned)((ncol + 127) / 128), 128, 0, s>>>(g, T);
+    tridiag_kernel<C><<<(unsigned)((ncol + pp->tb - 1) / pp->tb), pp->tb, 0, s>>>(g, T);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     fft_y<C><<<(nrows + YROWS - 1) / YROWS, nt_row * YROWS, smy, s>>>(g, pp->py, pp->spec, nrows, 1, sk);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     int groups = (g.maxy + ROWS - 1) / ROWS;
-    int nt_pair = g.maxx / 8 < 32 ? 32 : (g.maxx / 8 > XT_THREADS / (ROWS / 2) ? XT_THREADS / (ROWS / 2) : g.maxx / 8);
+    const int nt_pair = pp->xt;
     size_t smx = (size_t)(ROWS / 2) * 2 * g.maxx * sizeof(C);
     e = cudaFuncSetAttribute(fft_x_inv<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
     if (e != cudaSuccess) return e;

@@ -222,6 +222,19 @@ cudaError_t pressure_plan_create(const DevGrid &g, const double *wv_host, int mi
                                  int *pivot_error);
 void pressure_plan_destroy(PressurePlan *pp);
 size_t pressure_plan_bytes(const PressurePlan *pp);
+// the projection's tunable plan: radix sequences of the x and y transforms (radix of
+// stage s in bits [4s, 4s+4)) and launch shapes
+struct PressureKnobs {
+    unsigned long long xr, yr;
+    int xst, yst;   // stages
+    int xt;         // threads per packed row pair of the x transforms: 8 .. 64, power of 2
+    int yt;         // threads per row of the y transforms: 16 .. 128, power of 2
+    int tb;         // threads per block of the tridiagonal solve: 64, 128, 256
+};
+void pressure_get_knobs(const PressurePlan *pp, PressureKnobs *k);
+bool pressure_knobs_valid(const DevGrid &g, const PressureKnobs &k);
+bool pressure_set_knobs(PressurePlan *pp, const DevGrid &g, const PressureKnobs &k);
+int pressure_radix_candidates(int n, unsigned long long *pk, int *nst, int maxc);
 // Refinement control of one projection pass.  The mixed form solves the Poisson system
 // A dp = b of the reference (b = div(m)/(dt0*rho0); A: periodic 5-point horizontal
 // Laplacian plus the vertical tridiagonal rows) with FP32 transforms, then refines:

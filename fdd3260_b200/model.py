@@ -75,6 +75,36 @@ class Mimica:
                 out[f] = tuple(out[f])
         return out
 
+    # ---- the projection's plan and its autotuner ----
+    def tune_get(self) -> dict:
+        from . import tune
+        t = _lib.MgTune()
+        _lib.check(self._L.mg_tune_get(self._h, C.byref(t)), "mg_tune_get")
+        return tune.to_dict(t)
+
+    def tune_set(self, plan: dict) -> None:
+        from . import tune
+        t = tune.from_dict(plan)
+        _lib.check(self._L.mg_tune_set(self._h, C.byref(t)), "mg_tune_set")
+
+    def autotune(self, reps: int = 5, wisdom: str | None = None) -> dict:
+        """Pick the projection's plan for this grid: from the wisdom file when it holds one
+        for this grid and precision, else by timing candidates (mg_autotune), which is
+        then stored there.  Returns the plan, with the timings when it was measured."""
+        from . import tune
+        d = self.domain
+        k = tune.key(d.maxx, d.maxy, d.nz, d.precision)
+        known = tune.load(wisdom).get(k) if wisdom else None
+        if known is not None:
+            self.tune_set(known)
+            return dict(known, source="wisdom")
+        t = _lib.MgTune()
+        _lib.check(self._L.mg_autotune(self._h, int(reps), C.byref(t)), "mg_autotune")
+        plan = tune.to_dict(t)
+        if wisdom:
+            tune.store(wisdom, k, plan)
+        return dict(plan, source="measured", candidates=t.candidates, ms_default=t.ms_default, ms_tuned=t.ms_tuned)
+
     def set_dt(self, dt0: float) -> None:
         _lib.check(self._L.mg_set_dt(self._h, float(dt0)), "mg_set_dt")
         self.dt0 = float(dt0)

@@ -159,6 +159,36 @@ int mg_profile_enable(mg_ctx *ctx, int on);
 /* text report, one line per kernel group: "<name> <launches> <total ms>" */
 int mg_profile_report(mg_ctx *ctx, char *buf, size_t len);
 
+/* ---- autotuner (no counterpart in the reference, whose transforms take FFTW's plans) ----
+ * The projection's plan: the radix sequence of the x and of the y transforms
+ * (shared-memory Stockham stages of radix 2, 3, 4, 5 or 8 whose product is maxx resp.
+ * maxy) and the launch shapes of the x transforms, the y transforms and the vertical
+ * tridiagonal solve.  Plans differ in rounding only (FP64 projection: ~1e-15).
+ *   mg_autotune:  times candidate plans on the context's own grid (the projection of
+ *                 copies of the resident momentum, or of zeros before an upload; the
+ *                 state is left unchanged), one coordinate at a time, and keeps the
+ *                 fastest (a change must gain more than 1 %); reps projections per
+ *                 candidate.  Step graphs recorded earlier are dropped.
+ *   mg_tune_get / mg_tune_set: the plan in force; mg_tune_set rejects a plan that does
+ *                 not fit the grid with MG_ERR_PARAM (and drops recorded step graphs).
+ *   mg_radix_candidates: the radix sequences mg_autotune tries for a transform of length
+ *                 n (host only, no device needed); returns their number (<= maxc),
+ *                 sequence q in radix[16 q ..], its length in nstage[q]. */
+typedef struct mg_tune {
+    int x_nstage, x_radix[16];
+    int y_nstage, y_radix[16];
+    int x_threads;      /* threads per packed pair of rows, x transforms: 8, 16, 32, 64 */
+    int y_threads;      /* threads per row, y transforms: 16, 32, 64, 128 */
+    int tri_block;      /* threads per block, tridiagonal solve: 64, 128, 256 */
+    int candidates;     /* plans timed by mg_autotune */
+    double ms_default;  /* one projection with the plan in force before mg_autotune */
+    double ms_tuned;    /* one projection with the plan it chose */
+} mg_tune;
+int mg_autotune(mg_ctx *ctx, int reps, mg_tune *result);
+int mg_tune_get(mg_ctx *ctx, mg_tune *t);
+int mg_tune_set(mg_ctx *ctx, const mg_tune *t);
+int mg_radix_candidates(int n, int *radix, int *nstage, int maxc);
+
 /* ---- unit-level entry points (host buffers, reference layout) ---- */
 /* advection_ac (src/TOOLS/advection.f90:801-915) of one density-weighted field x with
  * the advective velocity derived from momentum (mu,mv,mw) as get_advective does

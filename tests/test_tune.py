@@ -1,0 +1,47 @@
+"""CPU checks of the projection's plan space: the radix sequences the autotuner tries
+(host code of the library, no device needed) and the wisdom file."""
+import math
+
+import pytest
+
+from fdd3260_b200 import _lib, tune
+
+
+@pytest.mark.parametrize("n", [8, 24, 30, 64, 96, 128, 160, 192, 250, 256, 512, 1024, 4096])
+def test_radix_candidates_factor_n(n):
+    cands = tune.radix_candidates(n)
+    assert cands, n
+    seen = set()
+    for c in cands:
+        assert math.prod(c) == n
+        assert set(c) <= {2, 3, 4, 5, 8}
+        assert 1 <= len(c) <= 16
+        seen.add(tuple(c))
+    assert len(seen) == len(cands), "distinct sequences"
+
+
+def test_radix_candidates_start_with_the_default_plan():
+    # the plan at context creation: radix 8 first, then 4 or 2, then 3 and 5
+    assert tune.radix_candidates(512)[0] == [8, 8, 8]
+    assert tune.radix_candidates(96)[0] == [8, 4, 3]
+    assert tune.radix_candidates(160)[0] == [8, 4, 5]
+
+
+def test_radix_candidates_reject_other_primes():
+    assert tune.radix_candidates(14) == []
+    assert tune.radix_candidates(2 * 7 * 3) == []
+
+
+def test_wisdom_round_trip(tmp_path):
+    plan = {"x_radix": [4, 4, 4, 4, 2], "y_radix": [3, 8, 4], "x_threads": 16, "y_threads": 64, "tri_block": 256}
+    t = tune.from_dict(plan)
+    assert tune.to_dict(t) == plan
+    path = str(tmp_path / "wisdom.json")
+    k = tune.key(512, 96, 64, _lib.MG_PREC_FP64)
+    tune.store(path, k, dict(plan, ms_tuned=1.0))
+    tune.store(path, tune.key(64, 64, 32, _lib.MG_PREC_MIXED), plan)
+    w = tune.load(path)
+    assert w[k] == plan and len(w) == 2
+    assert tune.load(str(tmp_path / "absent.json")) == {}
+    with pytest.raises(ValueError):
+        tune.from_dict(dict(plan, x_radix=[]))
