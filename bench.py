@@ -363,7 +363,8 @@ def main():
                 "data": "synthetic (seeded PCG64)", "config": cfg,
                 "clocks": head["clocks"], "gpu_launches": head["gpu_launches"],
                 "e2e": head["e2e"], "roofline": head["roofline"], "kernel_share": head["kernel_share"],
-                "cpu_baseline": cpu, "graph": use_graph, "device_bytes": head["device_bytes"]}
+                "cpu_baseline": cpu, "graph": use_graph, "device_bytes": head["device_bytes"],
+                "projection_plan": head["projection_plan"]}
         if "mixed" in res and forms[0] != "mixed":
             mx = res["mixed"]
             line["mixed"] = {"form": "FP32 stencils, fluxes and spectra; FP64 state, tendencies, tridiagonal, "
@@ -371,7 +372,7 @@ def main():
                              "value": mx["value"], "unit": "Mcell-updates/s", "ms_per_step": mx["ms_per_step"],
                              "speedup_vs_fp64": mx["value"] / head["value"], "roofline": mx["roofline"],
                              "kernel_share": mx["kernel_share"], "clocks": mx["clocks"],
-                             "gpu_launches": mx["gpu_launches"]}
+                             "gpu_launches": mx["gpu_launches"], "projection_plan": mx["projection_plan"]}
             if "error_vs_fp64" in mx:
                 line["mixed"]["error_vs_fp64"] = mx["error_vs_fp64"]
                 line["mixed"]["fp64_twin_1e-9_error"] = head.get("twin_error")
@@ -406,6 +407,7 @@ def run_ensemble(args, ws, rank, local):
         members.append(m)
         states.append(st)
     ens = E.Ensemble(members)
+    plans = ens.autotune(reps=3)
     ens.step(args.warmup, ntime0=1)
     dist_barrier(ws)
     with ClockSampler(local) as clk:
@@ -433,16 +435,25 @@ def run_ensemble(args, ws, rank, local):
             "measured_on": f"largest member of rank 0 ({mb.domain.maxx}x{mb.domain.maxy}x{mb.domain.nz}), eager",
             "step_frac": ab["step"] * total_cells * args.steps / (t_ms / 1e3) / 1e9 / pk["hbm_gbs"] / ws}
     # end to end: every member's state uploaded, one ensemble step, every state downloaded
+    # into the same page-locked buffers
+    from fdd3260_b200 import config
+    hosts = []
+    for m, st in zip(members, states):
+        h = config.State(*[pinned_like(m.domain.shape) for _ in range(5)], [pinned_like(m.domain.shape) for _ in st.scal],
+                         st.iqt)
+        for a, b in zip([h.u, h.v, h.w, h.p, h.dens, *h.scal], [st.u, st.v, st.w, st.p, st.dens, *st.scal]):
+            a[...] = b
+        hosts.append(h)
     dist_barrier(ws)
     t0 = time.perf_counter()
     nbytes = 0
     for s_ in range(args.e2e_steps):
-        for m, st in zip(members, states):
-            m.upload(st)
+        for m, h in zip(members, hosts):
+            m.upload(h)
         ens.step(1, ntime0=1)
-        outs = [m.download() for m in members]
+        for m, h in zip(members, hosts):
+            m.download(out=h)
         nbytes = sum((5 + len(st.scal)) * m.domain.nx * m.domain.ny * m.domain.nz * 8 for m, st in zip(members, states))
-        del outs
     e2e_s = dist_max(time.perf_counter() - t0, ws)
     nbytes_all = dist_sum(nbytes, ws)
     launches = ens.launches_per_step
@@ -476,8 +487,11 @@ def run_ensemble(args, ws, rank, local):
                 "clocks": clk.summary(), "gpu_launches": launches * args.steps,
                 "e2e": {"value": total_cells * args.e2e_steps / e2e_s / 1e6, "unit": "Mcell-updates/s",
                         "h2d_bytes_per_step": nbytes_all, "d2h_bytes_per_step": nbytes_all,
-                        "timing": "host wall clock, synchronised"},
-                "roofline": roof, "cpu_baseline": cpu, "graph": True}
+                        "timing": "host wall clock, synchronised, page-locked buffers"},
+                "roofline": roof, "cpu_baseline": cpu, "graph": True,
+                "projection_plans": {k: {f: v[f] for f in ("x_radix", "y_radix", "x_threads", "y_threads", "tri_block",
+                                                           "ms_default", "ms_tuned") if f in v}
+                                     for k, v in plans.items()}}
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
@@ -544,6 +558,7 @@ def field_errors(out, ref, st0, nsteps: int) -> dict:
 
 def time_form(args, m, d, st, use_graph, ws, local) -> dict:
     L = m._L
+    plan = m.autotune(reps=3)
     m.stepping(args.warmup, ntime0=1, graph=use_graph)
     m.synchronize()
     # timed region (device time, CUDA events on the library stream), clocks sampled meanwhile
@@ -579,7 +594,8 @@ def time_form(args, m, d, st, use_graph, ws, local) -> dict:
             "step_frac": ab["step"] * d.cells * args.steps / (t_ms / 1e3) / 1e9 / pk["hbm_gbs"]}
     kshare = {k: round(v["total_ms"] / sum(x["total_ms"] for x in kern.values()), 4) for k, v in kern.items()}
     return {"value": value, "ms_per_step": t_ms / args.steps, "clocks": clk.summary(),
-            "gpu_launches": launches_per_step * args.steps, "roofline": roof, "kernel_share": kshare}
+            "gpu_launches": launches_per_step * args.steps, "roofline": roof, "kernel_share": kshare,
+            "projection_plan": plan}
 
 
 def e2e_leg(args, m, d, st, ws) -> dict:

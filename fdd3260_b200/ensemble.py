@@ -98,6 +98,21 @@ class Ensemble:
         _lib.check(self._L.mg_ensemble_time_steps(self._h, nsteps, ntime0, C.byref(ms)), "mg_ensemble_time_steps")
         return ms.value
 
+    def autotune(self, reps: int = 3, wisdom: str | None = None) -> dict:
+        """The projection's plan of every member (``Mimica.autotune``): each distinct grid
+        is timed once and its plan applied to the members of the same size.  Returns the
+        plans by grid key."""
+        from . import tune
+        plans = {}
+        for m in self.members:
+            d = m.domain
+            k = tune.key(d.maxx, d.maxy, d.nz, d.precision)
+            if k in plans:
+                m.tune_set({f: plans[k][f] for f in tune.FIELDS})
+            else:
+                plans[k] = m.autotune(reps=reps, wisdom=wisdom)
+        return plans
+
     @property
     def launches_per_step(self) -> int:
         return self._L.mg_ensemble_launch_count(self._h)
