@@ -208,3 +208,41 @@ def test_time_traj_leaves_state_and_reports():
     assert t["forward_ms"] > 0 and t["tl_ms"] > 0 and t["adjoint_ms"] > t["forward_ms"]
     # checkpoints: 4/2 + 1 states, a segment of 3, adjoint, scratch and the stage records
     assert t["adjoint_device_bytes"] >= (3 + 3 + 2) * 7 * 8 * np.prod(d.shape)
+
+
+@pytest.mark.parametrize("with_buoy,target,eps,rtol", [(0, "winds", 1e-4, 1e-7), (1, "theta", 1e-6, 1e-5)])
+def test_gradient_against_oracle_central_differences(with_buoy, target, eps, rtol):
+    """The GPU adjoint's gradient along smooth and single-cell directions of the initial
+    winds and theta against central differences of the CPU restatement of the
+    reference's step (the oracle), an implementation independent of the GPU code."""
+    from oracle import oracle as O
+    d = config.warm_bubble_domain(24, 24, 12, dt0=1.0, with_buoy=with_buoy)
+    st = _smooth_state(d, seed=2)
+    nsteps = 2
+    scales = [1.0, 1.0, 1.0, 0, 0, 0, 0] if target == "winds" else [0.3, 0.3, 0.3, 0, 0, 1.0, 0]
+    lam = _rand_like(st, np.random.default_rng(21), scales)
+    g = _gradient(d, st, lam, nsteps)
+    orc = O.Oracle(d)
+
+    def J(e, delta):
+        moved = config.State(*[a + e * b for a, b in zip(_fields(st)[:5], _fields(delta)[:5])],
+                             [a + e * b for a, b in zip(st.scal, delta.scal)], -1)
+        out, _, _ = orc.stepping(moved, nsteps=nsteps, ntime0=1)
+        return _dot(out, lam)
+
+    zero = lambda: np.zeros(d.shape)
+    directions = [_bump_direction(d)]
+    for f, (k, j, i) in [(0, (5, 9, 7)), (2, (6, 12, 15)), (5, (4, 8, 10))]:
+        arrs = [zero() for _ in range(7)]
+        arrs[f][k, j, i] = 1.0
+        config.periodic_fill(arrs[f])
+        directions.append(config.State(*arrs[:5], arrs[5:], -1))
+    # round-off of the central difference: a few ulps of the largest weighted field per
+    # cell, summed with the weights lam, over 2 eps (theta ~ 300 K: ~1e-6 at eps = 1e-6)
+    big = max(np.abs(_interior(x)).max() for x, w in zip(_fields(st), scales) if w)
+    lam2 = np.sqrt(sum(float(np.sum(_interior(x) ** 2)) for x in _fields(lam)))
+    noise = 4 * np.spacing(big) * lam2 / (2 * eps)
+    for delta in directions:
+        gd = _dot(g, delta)
+        cd = (J(eps, delta) - J(-eps, delta)) / (2 * eps)
+        assert abs(cd - gd) <= rtol * abs(gd) + noise, (cd, gd, noise)
