@@ -20,8 +20,6 @@ namespace {
 
 constexpr double AVISC = 1. / 16.;   // windadv.f90:39
 
-__device__ __forceinline__ int wrap_x(const DevGrid &G, int i) { return i < 4 ? i + G.maxx : (i > G.nx - 2 ? i - G.maxx : i); }
-__device__ __forceinline__ int wrap_y(const DevGrid &G, int j) { return j < 4 ? j + G.maxy : (j > G.ny - 2 ? j - G.maxy : j); }
 
 // advective velocity of momentum component f at level k (funcpack.f90:65-94)
 template <typename T>
@@ -277,29 +275,41 @@ struct Gath {
     const DevGrid &G;
     Mom3 m, ab;
     double c1s, c2s, c1c, c2c;
-    __device__ Gath(const DevGrid &g, Mom3 m_, Mom3 ab_) : G(g), m(m_), ab(ab_)
+    int i0, j0, k0;   // the thread's cell: every position is addressed from its index
+    long long q0;
+    __device__ Gath(const DevGrid &g, Mom3 m_, Mom3 ab_, int i, int j, int k) : G(g), m(m_), ab(ab_), i0(i), j0(j), k0(k)
     {
         const bool fd4 = g.mom_ord == 4;
         c1s = fd4 ? 4. / 3. : 1.; c2s = fd4 ? 1. / 3. : 0.;
         c1c = fd4 ? 9. / 8. : 1.; c2c = fd4 ? 1. / 8. : 0.;
+        q0 = gidx(g, i, j, k);
     }
     // (along, transverse) -> (i, j): direction 0 is x, 1 is y
     __device__ static int ci(int dir, int a, int t) { return dir == 0 ? a : t; }
     __device__ static int cj(int dir, int a, int t) { return dir == 0 ? t : a; }
-    __device__ int wx(int i) const { return wrap_x(G, i); }
-    __device__ int wy(int j) const { return wrap_y(G, j); }
-    __device__ int wrap_a(int dir, int a) const { return dir == 0 ? wx(a) : wy(a); }
-    __device__ double M(int f, int i, int j, int k) const { return __ldg(m.m[f] + gidx(G, i, j, k)); }
+    // the positions visited lie within 2 cells of the thread's (outputs) or 3 (momenta);
+    // only a viscosity term three cells along reads past the last ghost, and is moved to
+    // its periodic image
+    __device__ int img_a(int dir, int a) const
+    {
+        return dir == 0 ? (a + 1 > G.nx ? a - G.maxx : a) : (a + 1 > G.ny ? a - G.maxy : a);
+    }
+    __device__ long long idx(int i, int j, int k) const
+    {
+        return q0 + (i - i0) + (long long)(j - j0) * G.px + (long long)(k - k0) * G.ps;
+    }
+    __device__ double M(int f, int i, int j, int k) const { return __ldg(m.m[f] + idx(i, j, k)); }
     // advective velocity with the reciprocal profiles (its partial is the same factor)
     __device__ double T(int f, int i, int j, int k) const
     {
         const double x = M(f, i, j, k) * rden(f, k);
         return f == 0 ? x - G.u0shift : (f == 1 ? x - G.v0shift : x);
     }
+    // output adjoints, halo-filled: the ghost cells hold the periodic images
     __device__ double A(int c, int i, int j, int k) const
     {
         if (k < 1 || k > G.nz || (c == 2 && k == 1)) return 0.;
-        return __ldg(ab.m[c] + gidx(G, wx(i), wy(j), k));
+        return __ldg(ab.m[c] + idx(i, j, k));
     }
     __device__ double Ma(int f, int dir, int a, int t, int k) const { return M(f, ci(dir, a, t), cj(dir, a, t), k); }
     __device__ double Ta(int f, int dir, int a, int t, int k) const { return T(f, ci(dir, a, t), cj(dir, a, t), k); }
@@ -356,7 +366,7 @@ struct Gath {
         }
         if (G.lavisc)
             for (int o = a0 - 2; o <= a0 + 2; o++) {
-                const int ob = wrap_a(dir, o);
+                const int ob = img_a(dir, o);
                 const double mu = 0.25 * fabs(Ta(g, dir, ob, t - 1, k) + Ta(g, dir, ob, t, k) + Ta(g, dir, ob + 1, t - 1, k) +
                                               Ta(g, dir, ob + 1, t, k)) * d1(dir);
                 r -= AVISC * Aa(c, dir, ob, t, k) * mu * w4(a0 - o);
@@ -497,7 +507,7 @@ struct Gath {
         }
         if (G.lavisc)
             for (int o = a0 - 2; o <= a0 + 2; o++) {
-                const int ob = wrap_a(dir, o);
+                const int ob = img_a(dir, o);
                 const double mu = 0.25 * fabs(Ta(dir, dir, ob, t, k) + Ta(dir, dir, ob, t, k - 1) + Ta(dir, dir, ob + 1, t, k) +
                                               Ta(dir, dir, ob + 1, t, k - 1)) * d1(dir);
                 r -= AVISC * Aa(2, dir, ob, t, k) * mu * w4(a0 - o);
@@ -596,8 +606,8 @@ __global__ void __launch_bounds__(128) mom_ad_gather_kernel(DevGrid G, Mom3 v, M
     const int j = 4 + blockIdx.y;
     const int k = 1 + blockIdx.z;
     if (i > G.nx - 2) return;
-    const Gath g(G, v, ab);
-    const long long q = gidx(G, i, j, k);
+    const Gath g(G, v, ab, i, j, k);
+    const long long q = g.q0;
     double *ub = const_cast<double *>(bar.m[0]), *vb = const_cast<double *>(bar.m[1]), *wb = const_cast<double *>(bar.m[2]);
     // u: u_x, u_y (advected), h_z (f 0, advected), v_x (velocity), w_h x (velocity)
     ub[q] += g.self_h(0, i, j, k) + g.cross_adv(0, i, j, k) + g.hz_adv(0, i, j, k) + g.cross_vel(1, i, j, k) +
@@ -623,11 +633,14 @@ cudaError_t launch_qnadv_tl(const DevGrid &g, int ntime, const double *mu, const
 }
 
 // bar += (d qnadv / d m)^T abar (bar arrays must be zeroed by the caller for a plain adjoint);
-// abar is read on the interior, the ghost entries of bar are left as they are
-cudaError_t launch_qnadv_ad(const DevGrid &g, const double *mu, const double *mv, const double *mw, const double *aubar,
-                            const double *avbar, const double *awbar, double *mubar, double *mvbar, double *mwbar,
-                            cudaStream_t s)
+// abar is read on the interior (its ghost cells are overwritten with periodic images),
+// the ghost entries of bar are left as they are
+cudaError_t launch_qnadv_ad(const DevGrid &g, const double *mu, const double *mv, const double *mw, double *aubar,
+                            double *avbar, double *awbar, double *mubar, double *mvbar, double *mwbar, cudaStream_t s)
 {
+    double *ab[3] = {aubar, avbar, awbar};
+    cudaError_t e = launch_halo_fill(g, ab, 3, s);
+    if (e != cudaSuccess) return e;
     const dim3 grid((g.maxx + 127) / 128, g.maxy, g.nz);
     mom_ad_gather_kernel<<<grid, 128, 0, s>>>(g, Mom3{{mu, mv, mw}}, Mom3{{aubar, avbar, awbar}},
                                               Mom3{{mubar, mvbar, mwbar}});

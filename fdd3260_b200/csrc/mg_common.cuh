@@ -204,9 +204,8 @@ cudaError_t launch_axpy(const DevGrid &g, double *y, const double *x, double alp
 cudaError_t launch_qnadv_tl(const DevGrid &g, int ntime, const double *mu, const double *mv, const double *mw,
                             const double *dmu, const double *dmv, const double *dmw, double *au, double *av, double *aw,
                             double *dau, double *dav, double *daw, cudaStream_t s);
-cudaError_t launch_qnadv_ad(const DevGrid &g, const double *mu, const double *mv, const double *mw, const double *aubar,
-                            const double *avbar, const double *awbar, double *mubar, double *mvbar, double *mwbar,
-                            cudaStream_t s);
+cudaError_t launch_qnadv_ad(const DevGrid &g, const double *mu, const double *mv, const double *mw, double *aubar,
+                            double *avbar, double *awbar, double *mubar, double *mvbar, double *mwbar, cudaStream_t s);
 
 // tangent linear / adjoint of the scalar advection operator (k_adjoint.cu)
 cudaError_t launch_advection_tl(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
