@@ -108,7 +108,7 @@ __global__ void adv_tl_kernel(DevGrid G, AdvIn in, AdvIn d, double *dA)
 }
 
 // ---- adjoint, face pass of one direction: g[m][face] = Fbar * J[m], gv[face] = Fbar * Jv ----
-__global__ void adv_ad_face_kernel(DevGrid G, int dir, AdvIn in, const double *Abar, double *g0, double *g1,
+__global__ void __launch_bounds__(256, 3) adv_ad_face_kernel(DevGrid G, int dir, AdvIn in, const double *Abar, double *g0, double *g1,
                                    double *g2, double *g3, double *gv)
 {
     // faces indexed by their lower cell: x: i in [3, nx-2] (j, k interior); y: j in
