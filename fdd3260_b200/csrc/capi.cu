@@ -1388,7 +1388,7 @@ static cudaError_t traj_step_fwd(mg_ctx *c, int ntime, const NatState &N, const 
 static cudaError_t traj_stage_tl(mg_ctx *c, int ntime, int stage, const NatState &N, const NatState &dN,
                                  const StageRec &R, const StageRec &dR, double *const *ts, double *const *dts,
                                  double *const *tm, double *const *dtm, double *p, double *dp,
-                                 double *const *dxs_out, double *const *dxm_out, double *const *dau)
+                                 double *const *dxs_out, double *const *dxm_out, double *const *dau, double *tls)
 {
     const DevGrid &G = c->G;
     const int nf = c->nf;
@@ -1398,7 +1398,7 @@ static cudaError_t traj_stage_tl(mg_ctx *c, int ntime, int stage, const NatState
     for (int f = 0; f < nf && e == cudaSuccess; f++) {
         e = cudaMemsetAsync(dR.A[f], 0, c->fbytes, c->stream);
         if (e == cudaSuccess)
-            e = launch_advection_tl(G, R.xs[f], R.xm[0], R.xm[1], R.xm[2], dR.xs[f], dR.xm[0], dR.xm[1], dR.xm[2], dR.A[f],
+            e = launch_advection_tl(G, R.xs[f], R.xm[0], R.xm[1], R.xm[2], dR.xs[f], dR.xm[0], dR.xm[1], dR.xm[2], dR.A[f], tls,
                                     c->stream);
     }
     for (int q = 0; q < 3 && e == cudaSuccess; q++) e = cudaMemsetAsync(dau[q], 0, c->fbytes, c->stream);
@@ -1437,7 +1437,7 @@ static cudaError_t traj_stage_tl(mg_ctx *c, int ntime, int stage, const NatState
 static cudaError_t traj_step_tl(mg_ctx *c, int ntime, const NatState &N, const NatState &dN, const NatState &Nout,
                                 const NatState &dNout, StageRec &R1, StageRec &R2, StageRec &dR1, StageRec &dR2,
                                 double *const *ts, double *const *tm, double *const *dts, double *const *dtm,
-                                double *const *au)
+                                double *const *au, double *tls)
 {
     const int nf = c->nf;
     cudaError_t e = traj_to_stage(c, N, R1);
@@ -1453,10 +1453,12 @@ static cudaError_t traj_step_tl(mg_ctx *c, int ntime, const NatState &N, const N
     if ((e = cudaMemcpyAsync(Nout.p, N.p, c->fbytes, cudaMemcpyDeviceToDevice, c->stream)) != cudaSuccess) return e;
     if ((e = cudaMemcpyAsync(dNout.p, dN.p, c->fbytes, cudaMemcpyDeviceToDevice, c->stream)) != cudaSuccess) return e;
     if ((e = traj_stage_fwd(c, ntime, 1, N, R1, ts, tm, Nout.p, R2.xs, R2.xm, au)) != cudaSuccess) return e;
-    if ((e = traj_stage_tl(c, ntime, 1, N, dN, R1, dR1, ts, dts, tm, dtm, Nout.p, dNout.p, dR2.xs, dR2.xm, au)) != cudaSuccess)
+    if ((e = traj_stage_tl(c, ntime, 1, N, dN, R1, dR1, ts, dts, tm, dtm, Nout.p, dNout.p, dR2.xs, dR2.xm, au, tls)) !=
+        cudaSuccess)
         return e;
     if ((e = traj_stage_fwd(c, ntime, 2, N, R2, ts, tm, Nout.p, Nout.s, Nout.m, au)) != cudaSuccess) return e;
-    if ((e = traj_stage_tl(c, ntime, 2, N, dN, R2, dR2, ts, dts, tm, dtm, Nout.p, dNout.p, dNout.s, dNout.m, au)) != cudaSuccess)
+    if ((e = traj_stage_tl(c, ntime, 2, N, dN, R2, dR2, ts, dts, tm, dtm, Nout.p, dNout.p, dNout.s, dNout.m, au, tls)) !=
+        cudaSuccess)
         return e;
     // natural variables: tangent first (it needs the stage values), then the values
     TrajConv V{};
@@ -1625,7 +1627,7 @@ static cudaError_t nat_d2h(mg_ctx *c, double *const *h, const NatState &n)
 struct TrajCtx {
     TrajBufs B;
     StageRec R1, R2, dR1, dR2;
-    double *ts[MG_MAXF], *tm[3], *dts[MG_MAXF], *dtm[3], *au[3];
+    double *ts[MG_MAXF], *tm[3], *dts[MG_MAXF], *dtm[3], *au[3], *tls = nullptr;
     void init(mg_ctx *c, bool tangent)
     {
         B.c = c;
@@ -1643,6 +1645,7 @@ struct TrajCtx {
             }
             for (int f = 0; f < nf; f++) dts[f] = B.get();
             for (int q = 0; q < 3; q++) dtm[q] = B.get();
+            tls = B.get();   // face tangents of the advection TL
         }
     }
 };
@@ -1711,7 +1714,7 @@ static int traj_tl_run(mg_ctx *c, int nsteps, int ntime0, const double *const *d
     TrajTimer tm{c->stream, ms};
     CKR(tm.start());
     for (int s = 0; s < nsteps; s++) {
-        CKR(traj_step_tl(c, ntime0 + s, a, da, b, db, T.R1, T.R2, T.dR1, T.dR2, T.ts, T.tm, T.dts, T.dtm, T.au));
+        CKR(traj_step_tl(c, ntime0 + s, a, da, b, db, T.R1, T.R2, T.dR1, T.dR2, T.ts, T.tm, T.dts, T.dtm, T.au, T.tls));
         std::swap(a, b);
         std::swap(da, db);
     }
@@ -1845,13 +1848,13 @@ extern "C" int mg_advection_tl(mg_ctx *c, const double *x, const double *mu, con
     if (!c || !x || !mu || !mv || !mw || !dx || !dmu || !dmv || !dmw || !dA) return MG_ERR_PARAM;
     if (c->prm.scal_adv != MG_WENO) return MG_ERR_PARAM;
     CKR(cudaSetDevice(c->device));
-    int rc = ensure_unit(c, 9);
+    int rc = ensure_unit(c, 10);
     if (rc) return rc;
     const double *in[8] = {x, mu, mv, mw, dx, dmu, dmv, dmw};
     for (int q = 0; q < 8; q++) CKR(h2d(c, c->unit[q], in[q], cudaMemcpyHostToDevice));
     CKR(cudaMemsetAsync(c->unit[8], 0, c->fbytes, c->stream));
     CKR(launch_advection_tl(c->G, c->unit[0], c->unit[1], c->unit[2], c->unit[3], c->unit[4], c->unit[5], c->unit[6],
-                            c->unit[7], c->unit[8], c->stream));
+                            c->unit[7], c->unit[8], c->unit[9], c->stream));
     CKR(d2h(c, dA, c->unit[8], cudaMemcpyDeviceToHost));
     return cuerr(cudaStreamSynchronize(c->stream));
 }
@@ -1920,7 +1923,7 @@ extern "C" int mg_time_adjoint(mg_ctx *c, int reps, double *out)
         int launches = 0;
         switch (which) {
         case 0: return launch_k1(c->G, a, maps, c->stream);
-        case 1: return launch_advection_tl(c->G, u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7], u[8], c->stream);
+        case 1: return launch_advection_tl(c->G, u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7], u[8], u[9], c->stream);
         case 2: return launch_advection_ad(c->G, u[0], u[1], u[2], u[3], u[8], u[4], u[5], u[6], u[7], scratch, c->stream);
         case 3: return project(c, u[4], u[5], u[6], u[7], -1, 0, 0, 0, &launches);
         default: return pressure_adjoint(c->G, c->pp, c->prm.nsubp, u[4], u[5], u[6], u[7], c->stream);

@@ -10,7 +10,8 @@
 // velocity is obtained by evaluating the forward scheme templates on dual numbers
 // (dual.cuh): the switch to nonlinear weights and the positivity limiter follow the
 // branch the FP64 form takes, and the smoothness weights are differentiated.
-//   TL: dA = J (dx, dm), one thread per cell, both faces of each direction.
+//   TL: dA = J (dx, dm), per direction a face pass (each face's tangent flux once) and a
+//       difference pass over the cells.
 //   AD: (xbar, mbar) = J^T Abar, deterministic two-pass form per direction: a face pass
 //       stores Fbar * J per face, a gather pass sums the four faces that read each
 //       cell; the adjoints of the periodic ghost cells are then folded onto the cells
@@ -79,32 +80,40 @@ __device__ __forceinline__ double face_metric(const DevGrid &G, int dir, int k)
     return dir == 0 ? 1. / G.dx : (dir == 1 ? 1. / G.dy : __ldg(G.dz1w + k - 1));
 }
 
-// ---- tangent linear: dA over the interior ----
-__global__ void adv_tl_kernel(DevGrid G, AdvIn in, AdvIn d, double *dA)
+// ---- tangent linear, face pass of one direction: dF[face] = J (dx stencil, dm) ----
+// faces indexed by their lower cell, as the adjoint's face pass
+__global__ void __launch_bounds__(256, 3) adv_tl_face_kernel(DevGrid G, int dir, AdvIn in, AdvIn d, double *dF)
 {
-    const int maxx = G.maxx, maxy = G.maxy;
+    const int maxx = G.maxx, maxy = G.maxy, nz = G.nz;
+    const int ni = dir == 0 ? maxx + 1 : maxx, nj = dir == 1 ? maxy + 1 : maxy, nk = dir == 2 ? nz - 1 : nz;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)maxx * maxy * G.nz) return;
+    if (t >= (long long)ni * nj * nk) return;
+    const int i = (int)(t % ni) + (dir == 0 ? 3 : 4), j = (int)((t / ni) % nj) + (dir == 1 ? 3 : 4);
+    const int k = (int)(t / ((long long)ni * nj)) + 1;
+    const long long c = gidx(G, i, j, k);
+    const long long st = dir == 0 ? 1 : (dir == 1 ? G.px : G.ps);
+    const double *dm = dir == 0 ? d.mu : (dir == 1 ? d.mv : d.mw);
+    double J[4], Jv;
+    face_jac(G, dir, in, i, j, k, J, Jv);   // every face of the range exists
+    double v = 0.;
+    for (int m = 0; m < 4; m++)
+        if (J[m] != 0.) v += J[m] * __ldg(d.x + c + (m - 1) * st);
+    dF[c] = v + Jv * __ldg(dm + c + st);
+}
+
+// ---- tangent linear, difference pass: dA (-)= (dF(c+1/2) - dF(c-1/2)) * metric ----
+__global__ void adv_tl_diff_kernel(DevGrid G, int dir, const double *dF, double *dA, int first)
+{
+    const int maxx = G.maxx, maxy = G.maxy, nz = G.nz;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)maxx * maxy * nz) return;
     const int i = (int)(t % maxx) + 4, j = (int)((t / maxx) % maxy) + 4, k = (int)(t / ((long long)maxx * maxy)) + 1;
-    double acc = 0.;
-    for (int dir = 0; dir < 3; dir++) {
-        const long long st = dir == 0 ? 1 : (dir == 1 ? G.px : G.ps);
-        const double *dm = dir == 0 ? d.mu : (dir == 1 ? d.mv : d.mw);
-        double dF[2] = {0., 0.};
-        for (int s = 0; s < 2; s++) {   // faces c-1/2 (lower cell c-1) and c+1/2 (lower cell c)
-            const int li = dir == 0 ? i - 1 + s : i, lj = dir == 1 ? j - 1 + s : j, lk = dir == 2 ? k - 1 + s : k;
-            double J[4], Jv;
-            if (!face_jac(G, dir, in, li, lj, lk, J, Jv)) continue;
-            const long long lc = gidx(G, li, lj, lk);
-            double v = 0.;
-            for (int m = 0; m < 4; m++)
-                if (J[m] != 0.) v += J[m] * __ldg(d.x + lc + (m - 1) * st);
-            v += Jv * __ldg(dm + lc + st);
-            dF[s] = v;
-        }
-        acc += (dF[1] - dF[0]) * face_metric(G, dir, k);
-    }
-    dA[gidx(G, i, j, k)] = -acc;
+    const long long c = gidx(G, i, j, k);
+    const long long st = dir == 0 ? 1 : (dir == 1 ? G.px : G.ps);
+    const double up = (dir == 2 && k == nz) ? 0. : __ldg(dF + c);
+    const double lo = (dir == 2 && k == 1) ? 0. : __ldg(dF + c - st);
+    const double v = (up - lo) * face_metric(G, dir, k);
+    dA[c] = first ? -v : dA[c] - v;
 }
 
 // ---- adjoint, face pass of one direction: g[m][face] = Fbar * J[m], gv[face] = Fbar * Jv ----
@@ -197,13 +206,23 @@ inline unsigned nblk(long long n) { return (unsigned)((n + 255) / 256); }
 
 }  // namespace
 
+// dA = J (dx, dm) over the interior; scratch: one field (the face tangents of a direction)
 cudaError_t launch_advection_tl(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
                                 const double *dx, const double *dmu, const double *dmv, const double *dmw, double *dA,
-                                cudaStream_t s)
+                                double *scratch, cudaStream_t s)
 {
-    const long long n = (long long)g.maxx * g.maxy * g.nz;
-    adv_tl_kernel<<<nblk(n), 256, 0, s>>>(g, AdvIn{x, mu, mv, mw}, AdvIn{dx, dmu, dmv, dmw}, dA);
-    return cudaGetLastError();
+    const AdvIn in{x, mu, mv, mw}, d{dx, dmu, dmv, dmw};
+    const long long ncell = (long long)g.maxx * g.maxy * g.nz;
+    for (int dir = 0; dir < 3; dir++) {
+        const long long nf = (long long)(dir == 0 ? g.maxx + 1 : g.maxx) * (dir == 1 ? g.maxy + 1 : g.maxy) *
+                             (dir == 2 ? g.nz - 1 : g.nz);
+        adv_tl_face_kernel<<<nblk(nf), 256, 0, s>>>(g, dir, in, d, scratch);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        adv_tl_diff_kernel<<<nblk(ncell), 256, 0, s>>>(g, dir, scratch, dA, dir == 0);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 // xbar, mubar, mvbar, mwbar are overwritten; scratch: 5 fields

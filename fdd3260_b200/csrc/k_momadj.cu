@@ -32,7 +32,7 @@ __device__ __forceinline__ T adv_vel(const DevGrid &G, int f, int k, const T &m)
 
 // ---------------- the nine direction terms (oracle and K2 order of operations) ----------------
 template <typename T, class L>
-__device__ T u_x(const DevGrid &G, const L &ld, int i, int j, int k, T ua)
+__device__ __forceinline__ T u_x(const DevGrid &G, const L &ld, int i, int j, int k, T ua)
 {
     const bool fd4 = G.mom_ord == 4;
     const double dx1 = 1. / G.dx, dx2 = 1. / (2. * G.dx);
@@ -50,7 +50,7 @@ __device__ T u_x(const DevGrid &G, const L &ld, int i, int j, int k, T ua)
 }
 
 template <typename T, class L>
-__device__ T u_y(const DevGrid &G, const L &ld, int i, int j, int k, T ua)
+__device__ __forceinline__ T u_y(const DevGrid &G, const L &ld, int i, int j, int k, T ua)
 {
     const bool fd4 = G.mom_ord == 4;
     const double dy1 = 1. / G.dy, dy3 = 1. / (3. * G.dy);
@@ -72,7 +72,7 @@ __device__ T u_y(const DevGrid &G, const L &ld, int i, int j, int k, T ua)
 
 // advuz_fd / advvz_fd (advhz): f = 0 (u, w at i-1, i, i-2, i+1) or 1 (v, w at j-1, j, j-2, j+1)
 template <typename T, class L>
-__device__ T h_z(const DevGrid &G, const L &ld, int f, int i, int j, int k, T ua)
+__device__ __forceinline__ T h_z(const DevGrid &G, const L &ld, int f, int i, int j, int k, T ua)
 {
     const int nz = G.nz;
     const bool fd4 = G.mom_ord == 4;
@@ -103,7 +103,7 @@ __device__ T h_z(const DevGrid &G, const L &ld, int f, int i, int j, int k, T ua
 }
 
 template <typename T, class L>
-__device__ T v_x(const DevGrid &G, const L &ld, int i, int j, int k, T va)
+__device__ __forceinline__ T v_x(const DevGrid &G, const L &ld, int i, int j, int k, T va)
 {
     const bool fd4 = G.mom_ord == 4;
     const double dx1 = 1. / G.dx, dx3 = 1. / (3. * G.dx);
@@ -124,7 +124,7 @@ __device__ T v_x(const DevGrid &G, const L &ld, int i, int j, int k, T va)
 }
 
 template <typename T, class L>
-__device__ T v_y(const DevGrid &G, const L &ld, int i, int j, int k, T va)
+__device__ __forceinline__ T v_y(const DevGrid &G, const L &ld, int i, int j, int k, T va)
 {
     const bool fd4 = G.mom_ord == 4;
     const double dy1 = 1. / G.dy, dy2 = 1. / (2. * G.dy);
@@ -143,7 +143,7 @@ __device__ T v_y(const DevGrid &G, const L &ld, int i, int j, int k, T va)
 
 // advwx_fd / advwy_fd (advwh): dir 0 (x, velocity ua) or 1 (y, velocity va); levels 2..nz
 template <typename T, class L>
-__device__ T w_h(const DevGrid &G, const L &ld, int dir, int i, int j, int k, T wa)
+__device__ __forceinline__ T w_h(const DevGrid &G, const L &ld, int dir, int i, int j, int k, T wa)
 {
     const int nz = G.nz;
     const bool fd4 = G.mom_ord == 4;
@@ -170,7 +170,7 @@ __device__ T w_h(const DevGrid &G, const L &ld, int dir, int i, int j, int k, T 
 }
 
 template <typename T, class L>
-__device__ T w_z(const DevGrid &G, const L &ld, int i, int j, int k, T wa)
+__device__ __forceinline__ T w_z(const DevGrid &G, const L &ld, int i, int j, int k, T wa)
 {
     const int nz = G.nz;
     const bool fd4 = G.mom_ord == 4;
@@ -208,7 +208,7 @@ __device__ T w_z(const DevGrid &G, const L &ld, int i, int j, int k, T wa)
 // component c (0 u, 1 v, 2 w) of qnadv_uvw at interior cell (i,j,k): even ntime x, y, z;
 // odd ntime z, y, x (windadv.f90:58-76)
 template <typename T, class L>
-__device__ T adv_comp(const DevGrid &G, const L &ld, int c, int ntime, int i, int j, int k)
+__device__ __forceinline__ T adv_comp(const DevGrid &G, const L &ld, int c, int ntime, int i, int j, int k)
 {
     T a = T(0.);
     if (c == 2 && k == 1) return a;   // w(1): the surface, no advective tendency
@@ -250,6 +250,7 @@ __global__ void __launch_bounds__(128) mom_tl_kernel(DevGrid G, int ntime, Mom3 
     if (i > G.nx - 2) return;
     const LoadTL ld{G, v, d};
     const long long q = gidx(G, i, j, k);
+#pragma unroll
     for (int c = 0; c < 3; c++) {
         const D<1> a = adv_comp<D<1>>(G, ld, c, ntime, i, j, k);
         if (val.m[c]) const_cast<double *>(val.m[c])[q] = a.v;

@@ -210,7 +210,7 @@ cudaError_t launch_qnadv_ad(const DevGrid &g, const double *mu, const double *mv
 // tangent linear / adjoint of the scalar advection operator (k_adjoint.cu)
 cudaError_t launch_advection_tl(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
                                 const double *dx, const double *dmu, const double *dmv, const double *dmw, double *dA,
-                                cudaStream_t s);
+                                double *scratch, cudaStream_t s);
 cudaError_t launch_advection_ad(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
                                 const double *Abar, double *xbar, double *mubar, double *mvbar, double *mwbar,
                                 double *const *scratch, cudaStream_t s);
