@@ -526,6 +526,7 @@ def trajectory_leg(args, dev) -> dict:
         m.upload(st)
         m.time_traj(2, 1)   # warm-up: plans, buffers, first launches
         t = m.time_traj(n, ck)
+        t1 = m.time_traj(n, n)   # one segment: no recomputation (memory permitting)
         m.upload(st)
         ms = C.c_double(0.0)
         m.stepping(3, ntime0=1, graph=True)
@@ -538,6 +539,8 @@ def trajectory_leg(args, dev) -> dict:
             "adjoint_ms": t["adjoint_ms"], "adjoint_over_fwd": t["adjoint_ms"] / fwd,
             "adjoint_over_composition": t["adjoint_ms"] / t["forward_ms"], "tl_over_fwd": t["tl_ms"] / fwd,
             "adjoint_device_gb": t["adjoint_device_bytes"] / 1e9,
+            "one_segment": {"ckpt": n, "adjoint_ms": t1["adjoint_ms"], "adjoint_over_fwd": t1["adjoint_ms"] / fwd,
+                            "adjoint_device_gb": t1["adjoint_device_bytes"] / 1e9},
             "note": "adjoint_ms includes the forward sweep that stores checkpoints and the segment recomputation"}
 
 

@@ -135,6 +135,7 @@ def lib() -> C.CDLL:
         L.mg_traj_tl.argtypes = [vp, C.c_int, C.c_int, C.POINTER(_dp), C.POINTER(_dp)]
         L.mg_traj_adjoint.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(_dp), C.POINTER(_dp)]
         L.mg_time_traj.argtypes = [vp, C.c_int, C.c_int, C.c_int, _dp]
+        L.mg_traj_record_limit.argtypes = [vp, C.c_double]
         L.mg_autotune.argtypes = [vp, C.c_int, C.POINTER(MgTune)]
         L.mg_tune_get.argtypes = [vp, C.POINTER(MgTune)]
         L.mg_tune_set.argtypes = [vp, C.POINTER(MgTune)]
@@ -180,6 +181,6 @@ EXPORTED = [
     "mg_advection_tl", "mg_advection_ad", "mg_anelastic_pressure_ad", "mg_time_adjoint", "mg_ensemble_create", "mg_ensemble_destroy", "mg_ensemble_step", "mg_ensemble_time_steps", "mg_ensemble_launch_count",
     "mg_set_sgs", "mg_set_surface_fluxes", "mg_sgs_profiles", "mg_calc_subgrid", "mg_efud", "mg_eff",
     "mg_checkall", "mg_cfl_dt", "mg_set_dt", "mg_download_ksgs", "mg_qnadv_tl", "mg_qnadv_ad",
-    "mg_traj_forward", "mg_traj_tl", "mg_traj_adjoint", "mg_time_traj",
+    "mg_traj_forward", "mg_traj_tl", "mg_traj_adjoint", "mg_time_traj", "mg_traj_record_limit",
     "mg_autotune", "mg_tune_get", "mg_tune_set", "mg_radix_candidates",
 ]

@@ -44,6 +44,7 @@ struct mg_ctx {
     K2Maps mmaps1, mmaps2;               // TMA descriptors of the K2 stencil momentum, per stage
     int *derr = nullptr;                 // device error flag of bounded waits
     int rep = REP_NAT;
+    double traj_rec_limit = -1.;         // bytes the trajectory adjoint's stage records may take (< 0: half the free memory)
     int have_state = 0;
     int launches = 0;
     size_t bytes = 0;
@@ -1753,7 +1754,8 @@ static int traj_adjoint_run(mg_ctx *c, int nsteps, int ntime0, int ckpt, const d
     size_t mfree = 0, mtot = 0;
     CKR(T.B.err);
     CKR(cudaMemGetInfo(&mfree, &mtot));
-    const bool keep = (double)ckpt * 2 * (2 * nf + 3) * (double)c->fbytes < 0.5 * (double)mfree;
+    const double rec_bytes = (double)ckpt * 2 * (2 * nf + 3) * (double)c->fbytes;
+    const bool keep = rec_bytes < 0.5 * (double)mfree && (c->traj_rec_limit < 0. || rec_bytes <= c->traj_rec_limit);
     std::vector<StageRec> rec1(keep ? ckpt : 0), rec2(keep ? ckpt : 0);
     for (int q = 0; keep && q < ckpt; q++)
         for (StageRec *R : {&rec1[q], &rec2[q]}) {
@@ -1767,23 +1769,35 @@ static int traj_adjoint_run(mg_ctx *c, int nsteps, int ntime0, int ckpt, const d
     else CKR(nat_copy(c, bar, traj_resident(c), nf));
     TrajTimer tm{c->stream, ms};
     CKR(tm.start());
-    for (int s = 0; s < nsteps; s++) {   // forward sweep: keep every ckpt-th state
+    // forward sweep: keep every ckpt-th state; with the records kept, the last segment (the
+    // first swept backward) keeps its states and records here and is not recomputed
+    const int s0_last = nsteps > 0 ? ((nsteps - 1) / ckpt) * ckpt : 0;
+    for (int s = 0; s < nsteps; s++) {
+        if (keep && s >= s0_last) {
+            if (s == s0_last) CKR(nat_copy(c, seg[0], ck[s0_last / ckpt], nf));
+            CKR(traj_step_fwd(c, ntime0 + s, seg[s - s0_last], seg[s - s0_last + 1], rec1[s - s0_last],
+                              rec2[s - s0_last], T.ts, T.tm, T.au));
+            continue;
+        }
         const NatState &from = (s % ckpt == 0) ? ck[s / ckpt] : tmp;
         NatState to = ((s + 1) % ckpt == 0) ? ck[(s + 1) / ckpt] : seg[0];
         CKR(traj_step_fwd(c, ntime0 + s, from, to, T.R1, T.R2, T.ts, T.tm, T.au));
         if ((s + 1) % ckpt != 0) CKR(nat_copy(c, tmp, to, nf));
     }
-    for (int s0 = ((nsteps - 1) / ckpt) * ckpt; nsteps > 0 && s0 >= 0; s0 -= ckpt) {
+    for (int s0 = s0_last; nsteps > 0 && s0 >= 0; s0 -= ckpt) {
         const int s1 = std::min(s0 + ckpt, nsteps);
-        CKR(nat_copy(c, seg[0], ck[s0 / ckpt], nf));
         if (keep) {
-            for (int s = s0; s < s1; s++)   // the segment's states and stage records
-                CKR(traj_step_fwd(c, ntime0 + s, seg[s - s0], seg[s - s0 + 1], rec1[s - s0], rec2[s - s0], T.ts, T.tm,
-                                  T.au));
+            if (s0 != s0_last) {   // the segment's states and stage records
+                CKR(nat_copy(c, seg[0], ck[s0 / ckpt], nf));
+                for (int s = s0; s < s1; s++)
+                    CKR(traj_step_fwd(c, ntime0 + s, seg[s - s0], seg[s - s0 + 1], rec1[s - s0], rec2[s - s0], T.ts,
+                                      T.tm, T.au));
+            }
             for (int s = s1 - 1; s >= s0; s--)
                 CKR(traj_step_ad(c, ntime0 + s, seg[s - s0], seg[s - s0 + 1], rec1[s - s0], rec2[s - s0], bar, S));
             continue;
         }
+        CKR(nat_copy(c, seg[0], ck[s0 / ckpt], nf));
         for (int s = s0; s < s1 - 1; s++)   // states at the starts of the segment's steps
             CKR(traj_step_fwd(c, ntime0 + s, seg[s - s0], seg[s - s0 + 1], T.R1, T.R2, T.ts, T.tm, T.au));
         for (int s = s1 - 1; s >= s0; s--) {
@@ -1822,6 +1836,13 @@ extern "C" int mg_traj_adjoint(mg_ctx *c, int nsteps, int ntime0, int ckpt, cons
     if (nsteps < 0 || ckpt < 1 || !lamT || !g0) return MG_ERR_PARAM;
     CKR(cudaSetDevice(c->device));
     return traj_adjoint_run(c, nsteps, ntime0, ckpt, lamT, g0, nullptr, nullptr);
+}
+
+extern "C" int mg_traj_record_limit(mg_ctx *c, double bytes)
+{
+    if (!c || bytes != bytes) return MG_ERR_PARAM;
+    c->traj_rec_limit = bytes;
+    return MG_OK;
 }
 
 // device times (ms) of nsteps of the trajectory forward composition, its tangent linear and

@@ -319,6 +319,11 @@ class Mimica:
                    "mg_traj_adjoint")
         return self._state_of(out)
 
+    def traj_record_limit(self, nbytes: float) -> None:
+        """Cap the device bytes the trajectory adjoint may keep as stage records (< 0: half
+        the free memory; 0: recompute every backward step's stages)."""
+        _lib.check(self._L.mg_traj_record_limit(self._h, float(nbytes)), "mg_traj_record_limit")
+
     def time_traj(self, nsteps: int, ckpt: int, ntime0: int = 1) -> dict:
         """Device times of nsteps of the trajectory composition, its tangent linear and its
         checkpointed adjoint from the resident state (left unchanged)."""

@@ -339,11 +339,17 @@ int mg_qnadv_ad(mg_ctx *ctx, int ntime, const double *mu, const double *mv, cons
  *                    sweep: (nsteps/ckpt + ckpt + 4) states of 4 + nf fields (nf = nscal
  *                    + 1) and ~8 nf + 30 work fields, plus the segment's stage records,
  *                    2 (2 nf + 3) fields per step, when they fit in half the free device
- *                    memory (else each backward step recomputes its stages).  Ghost
- *                    entries of g0 are 0. */
+ *                    memory and in mg_traj_record_limit (else each backward step
+ *                    recomputes its stages); with the records, the last segment keeps
+ *                    those of the forward sweep and is not recomputed (ckpt >= nsteps:
+ *                    one forward pass in all).  Ghost entries of g0 are 0. */
 int mg_traj_forward(mg_ctx *ctx, int nsteps, int ntime0);
 int mg_traj_tl(mg_ctx *ctx, int nsteps, int ntime0, const double *const *dx0, double *const *dxT);
 int mg_traj_adjoint(mg_ctx *ctx, int nsteps, int ntime0, int ckpt, const double *const *lamT, double *const *g0);
+/* Cap on the device bytes mg_traj_adjoint may hold for a segment's stage records
+ * (bytes < 0: half the free device memory, the default; 0: never keep them, so that
+ * every backward step recomputes its stages). */
+int mg_traj_record_limit(mg_ctx *ctx, double bytes);
 /* Device times (ms) of nsteps of mg_traj_forward's composition (out4[0]), of the tangent
  * linear (out4[1]) and of the checkpointed adjoint, forward sweep and recomputation
  * included (out4[2]), from the resident state, which is left unchanged; out4[3] = device
