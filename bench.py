@@ -93,6 +93,16 @@ def alg_bytes(nf_scalar: int, nsubp: int, sgs: bool = False) -> dict:
     return out
 
 
+# DRAM bytes per interior cell of one launch (mean of the two stages), from ncu captures
+# of the WENO cumulus workload with density + 5 scalars, SGS off, plain FP64, at
+# 384x384x64 (the mixed form moved the same bytes at 256x256x64).  Per-launch traffic
+# grows in proportion to the cells processed: K1 207.4 B/cell at 256x256x64 and 211.3 at
+# 384x384x64, K2 140.0 and 143.9.
+MEASURED_TRAFFIC_PER_CELL = {"k1_scalar_advection": 211.3, "k2_momentum": 143.9}
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one stage-1 and one stage-2 launch at "
+                  "384x384x64 (profiles/k1_k2_traffic_cumulus.md), per interior cell, times this launch's cells")
+
+
 class ClockSampler:
     """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
 
@@ -429,9 +439,12 @@ def run_ensemble(args, ws, rank, local):
     dom = max((k for k in kern if k in ab), key=lambda k: kern[k][1])
     avg_ms = kern[dom][1] / kern[dom][0]
     achieved = ab[dom] * mb.domain.cells / (avg_ms / 1e3) / 1e9
+    measured = args.scheme == "weno" and len(st.scal) == 5 and d.sgs is None and dom in MEASURED_TRAFFIC_PER_CELL
+    traffic = MEASURED_TRAFFIC_PER_CELL[dom] * d.cells if measured else None
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_source": pk_src,
-            "algorithmic_bytes_per_cell": ab[dom], "avg_launch_ms": avg_ms,
+            "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "traffic_unit": "bytes per launch",
+            "traffic_source": TRAFFIC_SOURCE if measured else "no capture of this configuration",
+            "peak_source": pk_src, "algorithmic_bytes_per_cell": ab[dom], "avg_launch_ms": avg_ms,
             "measured_on": f"largest member of rank 0 ({mb.domain.maxx}x{mb.domain.maxy}x{mb.domain.nz}), eager",
             "step_frac": ab["step"] * total_cells * args.steps / (t_ms / 1e3) / 1e9 / pk["hbm_gbs"] / ws}
     # end to end: every member's state uploaded, one ensemble step, every state downloaded
@@ -590,9 +603,12 @@ def time_form(args, m, d, st, use_graph, ws, local) -> dict:
     dom = max((k for k in kern if k in ab), key=lambda k: kern[k]["total_ms"])
     avg_ms = kern[dom]["total_ms"] / kern[dom]["launches"]
     achieved = ab[dom] * d.cells / (avg_ms / 1e3) / 1e9
+    measured = args.scheme == "weno" and len(st.scal) == 5 and d.sgs is None and dom in MEASURED_TRAFFIC_PER_CELL
+    traffic = MEASURED_TRAFFIC_PER_CELL[dom] * d.cells if measured else None
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_source": pk_src,
-            "algorithmic_bytes_per_cell": ab[dom], "avg_launch_ms": avg_ms,
+            "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "traffic_unit": "bytes per launch",
+            "traffic_source": TRAFFIC_SOURCE if measured else "no capture of this configuration",
+            "peak_source": pk_src, "algorithmic_bytes_per_cell": ab[dom], "avg_launch_ms": avg_ms,
             "step_alg_bytes_per_cell": ab["step"],
             "step_frac": ab["step"] * d.cells * args.steps / (t_ms / 1e3) / 1e9 / pk["hbm_gbs"]}
     kshare = {k: round(v["total_ms"] / sum(x["total_ms"] for x in kern.values()), 4) for k, v in kern.items()}
