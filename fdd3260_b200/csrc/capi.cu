@@ -44,6 +44,7 @@ struct mg_ctx {
     K2Maps mmaps1, mmaps2;               // TMA descriptors of the K2 stencil momentum, per stage
     int *derr = nullptr;                 // device error flag of bounded waits
     int rep = REP_NAT;
+    int k1_nseg = 0;                     // K1 k segments per tile (0: chosen per launch for this grid alone)
     double traj_rec_limit = -1.;         // bytes the trajectory adjoint's stage records may take (< 0: half the free memory)
     int have_state = 0;
     int launches = 0;
@@ -599,6 +600,7 @@ static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int wa
         // ---- K1: density + scalars (level-n buffers hold natural variables) ----
         K1Args a1{};
         a1.nf = nf; a1.dens_first = 1; a1.stage = stage; a1.a_dt = a_dt; a1.b = b; a1.mode = 0;
+        a1.nseg = c->k1_nseg;
         a1.err = c->derr;
         for (int f = 0; f < nf; f++) {
             a1.xin[f] = stage == 1 ? c->sA[f] : c->sB[f];
@@ -797,7 +799,11 @@ static cudaError_t ens_issue(mg_ens *e, int ntime, int nst, int *launches)
     for (size_t i = 0; i < e->m.size() && er == cudaSuccess; i++) {
         mg_ctx *c = e->m[i];
         er = cudaStreamWaitEvent(c->stream, e->fork, 0);
+        // the members run side by side and fill the device together: whole columns per CTA
+        const int nseg_own = c->k1_nseg;
+        c->k1_nseg = 1;
         for (int s = 0; s < nst && er == cudaSuccess; s++) er = step_once(c, ntime + s, 0, 0, 0, launches);
+        c->k1_nseg = nseg_own;
         if (er == cudaSuccess) er = cudaEventRecord(e->join[i], c->stream);
         if (er == cudaSuccess) er = cudaStreamWaitEvent(e->stream, e->join[i], 0);
     }

@@ -4,12 +4,17 @@
 // differences, FP64 fluxes and state).
 //
 // One CTA (288 threads: 8 cell warps + 1 helper warp) owns a 32 x 8 column tile and
-// marches up k.  Per level, the fields are processed in groups of PF (2 for WENO and
+// marches up a segment [kb, ke] of its levels (A.nseg segments per tile, so that small
+// grids fill the GPU and the last wave of CTAs is short).  A segment above the surface
+// first runs level kb-1 as a prologue that computes only its vertical face kb-1/2, the
+// flux the first level of the segment differences (the same arithmetic on the same
+// values as the segment below, so the result does not depend on the split).  Per level, the fields are processed in groups of PF (2 for WENO and
 // MUSCL, 1 for PPM, whose per-field reconstruction arrays are large): the haloed planes
 // of a group arrive by TMA (NPS group slots in flight), their x/y faces are computed as
 // independent chains, one barrier publishes them, then each cell thread finishes the
 // vertical face and the stage update of every field of the group.
 #pragma once
+#include <algorithm>
 #include "mg_common.cuh"
 #include "schemes.cuh"
 #include "tma.cuh"
@@ -70,6 +75,27 @@ __host__ __device__ inline Layout make_layout(int scheme, int nf)
     return L;
 }
 
+// k segments per column tile: the count that minimises (waves of CTAs) x (levels per
+// segment + 3, the prologue and the pipeline fill), with segments of at least 8 levels.
+// PPM keeps one: its vertical reconstruction chain carries more than one face.
+inline int k1_segments(const DevGrid &g, int scheme, size_t smem)
+{
+    if (scheme == MG_PPM) return 1;
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        nsm = 148;
+    const long long per_sm = std::max<long long>(1, std::min<long long>(2, (228LL * 1024) / ((long long)smem + 1024)));
+    const long long slots = (long long)nsm * per_sm;
+    const long long tiles = (long long)((g.maxx + TX - 1) / TX) * ((g.maxy + TY - 1) / TY);
+    int best = 1;
+    double bt = 1e300;
+    for (int sgm = 1; sgm <= std::max(1, g.nz / 8); sgm++) {
+        const double t = (double)((tiles * sgm + slots - 1) / slots) * ((double)g.nz / sgm + 3.);
+        if (t < 0.999 * bt) { bt = t; best = sgm; }
+    }
+    return best;
+}
+
 __device__ __forceinline__ double ldg(const double *p, long long i) { return __ldg(p + i); }
 
 // plane element of halo index h in [0, NHALO): rows 0..2 and 11..13, then the halo
@@ -110,8 +136,9 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
     double *chain = (double *)(sm + Ly.chain);   // PPM: [0][f] Fr of the cell below, [1][f] its xplus
     double *crx = (double *)(sm + Ly.crx), *cry = (double *)(sm + Ly.cry);
 
-    const int ntx = (G.maxx + TX - 1) / TX;
-    const int ti = blockIdx.x % ntx, tj = blockIdx.x / ntx;
+    const int ntx = (G.maxx + TX - 1) / TX, nty = (G.maxy + TY - 1) / TY;
+    const int tile = blockIdx.x % (ntx * nty), seg = blockIdx.x / (ntx * nty);
+    const int ti = tile % ntx, tj = tile / ntx;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const int i0 = 4 + ti * TX, j0 = 4 + tj * TY;
     const int nx = G.nx, ny = G.ny, nz = G.nz;
@@ -124,7 +151,12 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
     const double dx1 = 1. / G.dx, dy1 = 1. / G.dy, dt0 = G.dt0;
     const bool conv1 = CONV1;
     const int NG = (F + PF - 1) / PF;      // field groups per level
-    const int total_groups = nz * NG;
+    // this CTA's levels [kb, ke], the prologue level kp (= kb - 1 above the surface), and
+    // its plane groups [qb, qe); slots and barrier phases count from qb
+    const int kb = 1 + (int)(((long long)seg * nz) / A.nseg), ke = (int)(((long long)(seg + 1) * nz) / A.nseg);
+    const int kp = kb > 1 ? kb - 1 : 1;
+    const int qb = (kb - 1) * NG, qe = ke * NG;
+    const int zmax = min(nz, ke + L);      // last level the z-window needs
     const int MB_VEL = NPS;
 
     if (tid == 0) {
@@ -135,7 +167,7 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
 
     auto issue_group = [&](int qg) {   // group qg = (k-1)*NG + g: planes of fields g*PF ..
         const int k = qg / NG + 1, g = qg - (k - 1) * NG;
-        const int slot = qg % NPS;
+        const int slot = (qg - qb) % NPS;
         const int nfg = min(PF, F - g * PF);
         fence_proxy_async_shared();
         mbar_arrive_expect_tx(&mb[slot], nfg * PLANE_BYTES);
@@ -150,7 +182,7 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
         tma_load_3d(vbv, &M.mv, i0 - 2, j0 - 1, k - 1, &mb[MB_VEL]);
     };
     auto issue_z = [&](int l) {   // own-column values of every field and w at level l
-        if (cellt && l <= nz) {
+        if (cellt && l <= zmax) {
             const long long idx = gidx(G, ic, jc, l);
             const int s = l % ZS;
             for (int f = 0; f < F; f++) cp_async_8(&zring[(f * ZS + s) * NCELL + cid], A.xin[f] + idx);
@@ -160,13 +192,13 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
     };
 
     if (tid == 0) {
-        for (int q0 = 0; q0 < NPS - 1 && q0 < total_groups; q0++) issue_group(q0);
-        issue_vel(1);
+        for (int q0 = qb; q0 < qb + NPS - 1 && q0 < qe; q0++) issue_group(q0);
+        issue_vel(kb);
     }
-    for (int l = 1; l <= L + 1; l++) issue_z(l);
+    for (int l = max(1, kp - 1); l <= kp + L; l++) issue_z(l);
 
     double dn_old = 0., dn_new = 0., rdn_new = 0.;   // density of the own cell: level n and new (stage 2)
-    int k_cur = 1;
+    int k_cur = kp;
     // per-field vertical state
     if (cellt)
         for (int f = 0; f < F; f++) zf[f * NCELL + cid] = 0.;
@@ -186,6 +218,7 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
     double wz2 = 0., wz3 = 0.;   // w_adv of the own column at levels k+1 and k+2
     // stage 2: level-n value and tendency of the group's fields, loaded one group ahead
     const long long idx0 = gidx(G, ic, jc, 1);
+    const long long idxb = idx0 + (long long)(kb - 1) * G.ps;
     double nx_xold[PF], nx_tend[PF];
     double nx_sgs[PF];   // SGS tendencies (both stages), loaded one group ahead as well
 #pragma unroll
@@ -194,19 +227,21 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
         nx_tend[u] = 0.;
         nx_sgs[u] = 0.;
         if (STAGE == 2 && act && u < F) {
-            nx_xold[u] = ldg(A.xold[u], idx0);
-            nx_tend[u] = ldg(A.tend[u], idx0);
+            nx_xold[u] = ldg(A.xold[u], idxb);
+            nx_tend[u] = ldg(A.tend[u], idxb);
         }
-        if (SGS && act && u < F && A.sgs[u]) nx_sgs[u] = ldg(A.sgs[u], idx0);
+        if (SGS && act && u < F && A.sgs[u]) nx_sgs[u] = ldg(A.sgs[u], idxb);
     }
-    for (int k = 1; k <= nz; k++) {
+    for (int k = kp; k <= ke; k++) {
+        const bool pro = k < kb;   // prologue level: its vertical face only
         k_cur = k;
 #pragma unroll
         for (int m = 0; m < L + 2; m++) zsl[m] = (k - 1 + m) % ZS;
         const double d0 = ldg(G.den0, k - 1);
         // momentum boxes of level k -> face velocities.  Previous readers of su/sv (the
         // faces of iteration k-1) passed that iteration's last face barrier.
-        mbar_wait_bounded(&mb[MB_VEL], (uint32_t)((k - 1) & 1), A.err);
+        if (!pro) {
+        mbar_wait_bounded(&mb[MB_VEL], (uint32_t)((k - kb) & 1), A.err);
         for (int q = tid; q < TY * (TX + 1) + (TY + 1) * TX; q += NT) {
             if (q < TY * (TX + 1)) {
                 int r = q / (TX + 1), c = q - r * (TX + 1);
@@ -222,9 +257,10 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
             }
         }
         __syncthreads();   // su/sv complete; the momentum boxes are free again
-        if (tid == 0 && k + 1 <= nz) issue_vel(k + 1);
+        if (tid == 0 && k + 1 <= ke) issue_vel(k + 1);
+        }
         for (int g = 0; g < NG; g++) {
-            const int qg = (k - 1) * NG + g, gb = g * PF;
+            const int qg = (k - 1) * NG + g, qr = qg - qb, gb = g * PF;
             // this group's stage-2 operands, then the next group's loads (they complete
             // while this group's faces are computed)
             double cur_xold[PF], cur_tend[PF], cur_sgs[PF];
@@ -234,7 +270,11 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
                 cur_tend[u] = nx_tend[u];
                 cur_sgs[u] = nx_sgs[u];
             }
-            if ((STAGE == 2 || SGS) && act && qg + 1 < total_groups) {
+            double *fxb = fx + (NFB == 2 ? (qr & 1) : 0) * PF * FXN;
+            double *fyb = fy + (NFB == 2 ? (qr & 1) : 0) * PF * FYN;
+            double plane_xo[PF];
+            if (!pro) {
+            if ((STAGE == 2 || SGS) && act && qg + 1 < qe) {
                 const int gn = g + 1 < NG ? g + 1 : 0, kn = g + 1 < NG ? k : k + 1;
                 const long long idn = idx0 + (long long)(kn - 1) * G.ps;
 #pragma unroll
@@ -249,12 +289,11 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
             }
             // slot (qg+NPS-1)%NPS last held group qg-1, whose faces all threads finished
             // before the face barrier of group qg-1
-            if (tid == 0 && qg + NPS - 1 < total_groups) issue_group(qg + NPS - 1);
-            mbar_wait_bounded(&mb[qg % NPS], (uint32_t)((qg / NPS) & 1), A.err);
-            double *plq = planes + (size_t)(qg % NPS) * PF * (PLANE_SLOT / 8);
+            if (tid == 0 && qg + NPS - 1 < qe) issue_group(qg + NPS - 1);
+            mbar_wait_bounded(&mb[qr % NPS], (uint32_t)((qr / NPS) & 1), A.err);
+            double *plq = planes + (size_t)(qr % NPS) * PF * (PLANE_SLOT / 8);
             // level-n values of the own cell (stage 1: they are the planes' own elements,
             // read before the density products below)
-            double plane_xo[PF];
 #pragma unroll
             for (int u = 0; u < PF; u++) plane_xo[u] = (cellt && gb + u < F) ? plq[u * (PLANE_SLOT / 8) + own_e] : 0.;
             if constexpr (CONV1) {
@@ -279,10 +318,8 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
                 }
             }
             if ((CONV1 && (PF == 2 || g > 0)) || NFB == 1) __syncthreads();
-            double *fxb = fx + (NFB == 2 ? (qg & 1) : 0) * PF * FXN;
-            double *fyb = fy + (NFB == 2 ? (qg & 1) : 0) * PF * FYN;
-            double *crxq = crx + (NFB == 2 ? (qg & 1) : 0) * 4 * TY * (TX + 2);
-            double *cryq = cry + (NFB == 2 ? (qg & 1) : 0) * 4 * (TY + 2) * TX;
+            double *crxq = crx + (NFB == 2 ? (qr & 1) : 0) * 4 * TY * (TX + 2);
+            double *cryq = cry + (NFB == 2 ? (qr & 1) : 0) * 4 * (TY + 2) * TX;
             if constexpr (SCHEME == MG_PPM) {
                 const double *pl = plq;
                 auto V = [&](int e) -> double { return pl[e]; };
@@ -406,14 +443,16 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
                     }
             }
             __syncthreads();   // faces of group qg complete
+            }
             if (!cellt) continue;
 
             // ---- vertical faces k+1/2 of the own column ----
             if (g == 0) {
                 cp_async_wait_all();
                 if (conv1) {
-                    // newly arrived levels: 1..L+1 at k = 1, else k+L
-                    const int m_lo = k == 1 ? 1 : L + 1;
+                    // newly arrived levels: the whole window at the first level (without level
+                    // 0 at the surface), else k+L
+                    const int m_lo = k == kp ? (k == 1 ? 1 : 0) : L + 1;
                     for (int m = m_lo; m <= L + 1; m++) {
                         if (k - 1 + m > nz) break;
                         const int sl = (k - 1 + m) % ZS;
@@ -429,8 +468,8 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
                 const int f = gb + u;
                 if (PF > 1 && f >= F) continue;
                 const double *fxq = fxb + u * FXN, *fyq = fyb + u * FYN;
-                const double Tx = (fxq[ty * (TX + 1) + tx + 1] - fxq[ty * (TX + 1) + tx]) * dx1;
-                const double Ty = (fyq[(ty + 1) * TX + tx] - fyq[ty * TX + tx]) * dy1;
+                const double Tx = pro ? 0. : (fxq[ty * (TX + 1) + tx + 1] - fxq[ty * (TX + 1) + tx]) * dx1;
+                const double Ty = pro ? 0. : (fyq[(ty + 1) * TX + tx] - fyq[ty * TX + tx]) * dy1;
                     const double dzw1 = ldg(G.dz1w, k - 1);
                     double Fzn = 0.;
                     double *zfo = &zf[f * NCELL + cid];
@@ -577,7 +616,7 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
                     *zfo = Fzn;
 
                 // ---- epilogue ----
-                if (act) {
+                if (act && !pro) {
                     const long long idx = idx0 + (long long)(k - 1) * G.ps;
                     if constexpr (STAGE == 0) {
                         double *xs = A.xout[f];

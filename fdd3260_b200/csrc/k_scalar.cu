@@ -10,12 +10,15 @@ template <int SCHEME, int STAGE>
 cudaError_t launch_one(const DevGrid &g, const K1Args &a, const K1Maps &maps, size_t sm, cudaStream_t s)
 {
     const int ntx = (g.maxx + TX - 1) / TX, nty = (g.maxy + TY - 1) / TY;
+    K1Args as = a;
+    if (as.nseg < 1 || as.nseg > g.nz) as.nseg = k1_segments(g, SCHEME, sm);
+    if (SCHEME == MG_PPM) as.nseg = 1;
     bool sgs = false;
     for (int f = 0; f < a.nf; f++) sgs = sgs || a.sgs[f] != nullptr;
     if (STAGE != 0 && sgs)
-        k1_kernel<SCHEME, false, STAGE, true><<<dim3(ntx * nty), dim3(TX, TY + 1), sm, s>>>(g, a, maps);
+        k1_kernel<SCHEME, false, STAGE, true><<<dim3(ntx * nty * as.nseg), dim3(TX, TY + 1), sm, s>>>(g, as, maps);
     else
-        k1_kernel<SCHEME, false, STAGE, false><<<dim3(ntx * nty), dim3(TX, TY + 1), sm, s>>>(g, a, maps);
+        k1_kernel<SCHEME, false, STAGE, false><<<dim3(ntx * nty * as.nseg), dim3(TX, TY + 1), sm, s>>>(g, as, maps);
     return cudaGetLastError();
 }
 template <int SCHEME>

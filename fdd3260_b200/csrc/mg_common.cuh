@@ -65,6 +65,7 @@ struct K1Args {
     // initial tendency that advection_ac then updates (tracers: tracers.f90:81-106).
     const double *sgs[MG_MAXF];
     unsigned sgs_post;
+    int nseg;                      // k segments per column tile (0: launch_k1 chooses for the grid alone)
 };
 // TMA descriptors of the K1 inputs: haloed planes (38 x 14) of every field, momentum boxes (34 x 9)
 struct alignas(64) K1Maps {
