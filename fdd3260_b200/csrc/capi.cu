@@ -584,6 +584,30 @@ static cudaError_t sgs_tendencies(mg_ctx *c, int *launches)
     return cudaSuccess;
 }
 
+// K1's arguments for one stage of the step (stage 1 writes only the stage buffers)
+static void k1_stage_args(mg_ctx *c, int stage, K1Args &a1)
+{
+    const DevGrid &G = c->G;
+    const int nf = c->nf;
+    const int ies = 1, iqt = c->prm.iqt >= 0 ? 1 + c->prm.iqt : -1;
+    a1.nf = nf; a1.dens_first = 1; a1.stage = stage; a1.mode = 0;
+    a1.a_dt = (stage == 1 ? 1. : 0.5) * G.dt0;
+    a1.b = stage == 1 ? 0. : 1.;
+    a1.nseg = c->k1_nseg;
+    a1.err = c->derr;
+    for (int f = 0; f < nf; f++) {
+        a1.xin[f] = stage == 1 ? c->sA[f] : c->sB[f];
+        a1.xold[f] = c->sA[f];
+        a1.xold_is_xin = stage == 1;
+        a1.xout[f] = stage == 1 ? c->sB[f] : c->sA[f];
+        a1.tend[f] = c->ts[f];
+        a1.fst[f] = (f == ies && G.with_buoy) ? c->fes : ((f == iqt && G.with_buoy) ? c->fqt : nullptr);
+        a1.sgs[f] = (c->sgs_on && f >= 1) ? c->sgsc[f] : nullptr;
+    }
+    a1.sgs_post = c->sgs_on ? ((1u << ies) | (iqt >= 0 ? 1u << iqt : 0u)) : 0u;
+    a1.mw = (stage == 1 ? c->mA : c->mB)[2];
+}
+
 static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int want_maxdiv, int *launches)
 {
     const DevGrid &G = c->G;
@@ -599,21 +623,8 @@ static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int wa
         const double b = stage == 1 ? 0. : 1.;
         // ---- K1: density + scalars (level-n buffers hold natural variables) ----
         K1Args a1{};
-        a1.nf = nf; a1.dens_first = 1; a1.stage = stage; a1.a_dt = a_dt; a1.b = b; a1.mode = 0;
-        a1.nseg = c->k1_nseg;
-        a1.err = c->derr;
-        for (int f = 0; f < nf; f++) {
-            a1.xin[f] = stage == 1 ? c->sA[f] : c->sB[f];
-            a1.xold[f] = c->sA[f];
-            a1.xold_is_xin = stage == 1;
-            a1.xout[f] = stage == 1 ? c->sB[f] : c->sA[f];
-            a1.tend[f] = c->ts[f];
-            a1.fst[f] = (f == ies && G.with_buoy) ? c->fes : ((f == iqt && G.with_buoy) ? c->fqt : nullptr);
-            a1.sgs[f] = (c->sgs_on && f >= 1) ? c->sgsc[f] : nullptr;
-        }
-        a1.sgs_post = c->sgs_on ? ((1u << ies) | (iqt >= 0 ? 1u << iqt : 0u)) : 0u;
+        k1_stage_args(c, stage, a1);
         const double *const *mom = stage == 1 ? c->mA : c->mB;
-        a1.mw = mom[2];
         if (P.precision == MG_PREC_MIXED)
             PROF(c, "k1_scalar_advection", launch_k1_mixed(G, a1, stage == 1 ? c->maps1 : c->maps2, c->stream));
         else
@@ -2108,6 +2119,34 @@ static void knobs_to_tune(const PressureKnobs &k, mg_tune *t)
     t->tri_block = k.tb;
 }
 
+// mean device time (ms) of one stage-1 K1 launch, which reads the resident state and
+// writes only the stage buffers
+static int time_k1(mg_ctx *c, int reps, double *ms)
+{
+    K1Args a{};
+    k1_stage_args(c, 1, a);
+    cudaEvent_t e0, e1;
+    CKR(cudaEventCreate(&e0));
+    cudaError_t er = cudaEventCreate(&e1);
+    if (er != cudaSuccess) { cudaEventDestroy(e0); return cuerr(er); }
+    auto launch = [&]() {
+        return c->prm.precision == MG_PREC_MIXED ? launch_k1_mixed(c->G, a, c->maps1, c->stream)
+                                                  : launch_k1(c->G, a, c->maps1, c->stream);
+    };
+    er = launch();   // warm-up
+    if (er == cudaSuccess) er = cudaEventRecord(e0, c->stream);
+    for (int r = 0; r < reps && er == cudaSuccess; r++) er = launch();
+    if (er == cudaSuccess) er = cudaEventRecord(e1, c->stream);
+    if (er == cudaSuccess) er = cudaEventSynchronize(e1);
+    float f = 0.f;
+    if (er == cudaSuccess) er = cudaEventElapsedTime(&f, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (er != cudaSuccess) return cuerr(er);
+    *ms = f / reps;
+    return check_err(c);
+}
+
 static bool tune_to_knobs(const mg_tune *t, PressureKnobs *k)
 {
     if (t->x_nstage < 1 || t->x_nstage > 16 || t->y_nstage < 1 || t->y_nstage > 16) return false;
@@ -2135,6 +2174,7 @@ extern "C" int mg_tune_get(mg_ctx *c, mg_tune *t)
     PressureKnobs k;
     pressure_get_knobs(c->pp, &k);
     knobs_to_tune(k, t);
+    t->k1_segments = c->k1_nseg;
     return MG_OK;
 }
 
@@ -2142,7 +2182,9 @@ extern "C" int mg_tune_set(mg_ctx *c, const mg_tune *t)
 {
     if (!c || !t) return MG_ERR_PARAM;
     PressureKnobs k;
+    if (t->k1_segments < 0 || t->k1_segments > c->G.nz) return MG_ERR_PARAM;
     if (!tune_to_knobs(t, &k) || !pressure_set_knobs(c->pp, c->G, k)) return MG_ERR_PARAM;
+    c->k1_nseg = t->k1_segments;
     drop_graphs(c);
     return MG_OK;
 }
@@ -2237,15 +2279,37 @@ extern "C" int mg_autotune(mg_ctx *c, int reps, mg_tune *result)
     for (int tb = 64; tb <= 256; tb *= 2)
         if (tb != cur.tb) { k = cur; k.tb = tb; if ((rc = trial(k))) return rc; }
     pressure_set_knobs(c->pp, c->G, cur);
-    drop_graphs(c);
     double tuned = 0.;
     if ((rc = time_projection(c, reps, &tuned))) return rc;
+    // K1's k segments per column tile (0: the wave model's choice); PPM keeps whole columns
+    double k1_def = 0., k1_best = 0., t1 = 0.;
+    const int nseg_in = c->k1_nseg;
+    int nseg_best = nseg_in;
+    if (c->prm.scal_adv != MG_PPM) {
+        if ((rc = time_k1(c, reps, &k1_def))) return rc;
+        k1_best = k1_def;
+        const int cands[9] = {0, 1, 2, 3, 4, 6, 8, 12, 16};
+        for (int n : cands) {
+            if (n == nseg_in || n * 8 > c->G.nz) continue;
+            c->k1_nseg = n;
+            rc = time_k1(c, reps, &t1);
+            c->k1_nseg = nseg_in;
+            if (rc) return rc;
+            ncand++;
+            if (t1 < 0.99 * k1_best) { k1_best = t1; nseg_best = n; }
+        }
+        c->k1_nseg = nseg_best;
+    }
+    drop_graphs(c);
     if (result) {
         memset(result, 0, sizeof(*result));
         knobs_to_tune(cur, result);
+        result->k1_segments = nseg_best;
         result->candidates = ncand;
         result->ms_default = ms_default;
         result->ms_tuned = tuned;
+        result->k1_ms_default = k1_def;
+        result->k1_ms_tuned = k1_best;
     }
     return MG_OK;
 }

@@ -106,7 +106,7 @@ class Ensemble:
         plans = {}
         for m in self.members:
             d = m.domain
-            k = tune.key(d.maxx, d.maxy, d.nz, d.precision)
+            k = tune.key(d.maxx, d.maxy, d.nz, d.precision, m.nscal)
             if k in plans:
                 m.tune_set({f: plans[k][f] for f in tune.FIELDS})
             else:

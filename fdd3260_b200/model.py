@@ -93,7 +93,7 @@ class Mimica:
         then stored there.  Returns the plan, with the timings when it was measured."""
         from . import tune
         d = self.domain
-        k = tune.key(d.maxx, d.maxy, d.nz, d.precision)
+        k = tune.key(d.maxx, d.maxy, d.nz, d.precision, self.nscal)
         known = tune.load(wisdom).get(k) if wisdom else None
         if known is not None:
             self.tune_set(known)
@@ -103,7 +103,8 @@ class Mimica:
         plan = tune.to_dict(t)
         if wisdom:
             tune.store(wisdom, k, plan)
-        return dict(plan, source="measured", candidates=t.candidates, ms_default=t.ms_default, ms_tuned=t.ms_tuned)
+        return dict(plan, source="measured", candidates=t.candidates, ms_default=t.ms_default, ms_tuned=t.ms_tuned,
+                    k1_ms_default=t.k1_ms_default, k1_ms_tuned=t.k1_ms_tuned)
 
     def set_dt(self, dt0: float) -> None:
         _lib.check(self._L.mg_set_dt(self._h, float(dt0)), "mg_set_dt")

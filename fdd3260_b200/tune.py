@@ -1,8 +1,9 @@
-"""The projection's plan (radix sequences of the horizontal transforms, launch shapes of
-the transforms and of the vertical tridiagonal solve) as a dictionary, and a wisdom
-file that keeps the plans ``mg_autotune`` chose, keyed by grid and precision, so that a
-later run on the same grid applies them without timing again (as FFTW's wisdom does for
-the reference's transforms).  The file is JSON: {key: plan}."""
+"""The tuned plan as a dictionary -- radix sequences of the horizontal transforms, launch
+shapes of the transforms and of the vertical tridiagonal solve, and the scalar
+advection's k segments per column tile (0: chosen per launch) -- and a wisdom file that
+keeps the plans ``mg_autotune`` chose, keyed by grid, precision and scalar count, so that
+a later run on the same problem applies them without timing again (as FFTW's wisdom does
+for the reference's transforms).  The file is JSON: {key: plan}."""
 from __future__ import annotations
 
 import ctypes as C
@@ -11,12 +12,12 @@ import os
 
 from . import _lib
 
-FIELDS = ("x_radix", "y_radix", "x_threads", "y_threads", "tri_block")
+FIELDS = ("x_radix", "y_radix", "x_threads", "y_threads", "tri_block", "k1_segments")
 
 
 def to_dict(t: _lib.MgTune) -> dict:
     return {"x_radix": list(t.x_radix)[:t.x_nstage], "y_radix": list(t.y_radix)[:t.y_nstage],
-            "x_threads": t.x_threads, "y_threads": t.y_threads, "tri_block": t.tri_block}
+            "x_threads": t.x_threads, "y_threads": t.y_threads, "tri_block": t.tri_block, "k1_segments": t.k1_segments}
 
 
 def from_dict(d: dict) -> _lib.MgTune:
@@ -30,11 +31,14 @@ def from_dict(d: dict) -> _lib.MgTune:
     for q, r in enumerate(yr):
         t.y_radix[q] = int(r)
     t.x_threads, t.y_threads, t.tri_block = int(d["x_threads"]), int(d["y_threads"]), int(d["tri_block"])
+    t.k1_segments = int(d.get("k1_segments", 0))
     return t
 
 
-def key(maxx: int, maxy: int, nz: int, precision: int) -> str:
-    return f"{maxx}x{maxy}x{nz}/{'mixed' if precision == _lib.MG_PREC_MIXED else 'fp64'}"
+def key(maxx: int, maxy: int, nz: int, precision: int, nscal: int) -> str:
+    """grid, precision and scalar count (the scalar advection's shared memory, and so its
+    CTAs per SM, depends on the number of fields)"""
+    return f"{maxx}x{maxy}x{nz}/{'mixed' if precision == _lib.MG_PREC_MIXED else 'fp64'}/{nscal}"
 
 
 def load(path: str) -> dict:

@@ -163,7 +163,9 @@ int mg_profile_report(mg_ctx *ctx, char *buf, size_t len);
  * The projection's plan: the radix sequence of the x and of the y transforms
  * (shared-memory Stockham stages of radix 2, 3, 4, 5 or 8 whose product is maxx resp.
  * maxy) and the launch shapes of the x transforms, the y transforms and the vertical
- * tridiagonal solve.  Plans differ in rounding only (FP64 projection: ~1e-15).
+ * tridiagonal solve; and the work split of the scalar advection (k segments per column
+ * tile).  Plans differ in rounding only (FP64 projection: ~1e-15; the segments not at
+ * all).
  *   mg_autotune:  times candidate plans on the context's own grid (the projection of
  *                 copies of the resident momentum, or of zeros before an upload; the
  *                 state is left unchanged), one coordinate at a time, and keeps the
@@ -180,9 +182,12 @@ typedef struct mg_tune {
     int x_threads;      /* threads per packed pair of rows, x transforms: 8, 16, 32, 64 */
     int y_threads;      /* threads per row, y transforms: 16, 32, 64, 128 */
     int tri_block;      /* threads per block, tridiagonal solve: 64, 128, 256 */
+    int k1_segments;    /* scalar advection: k segments per 32 x 8 column tile (0: chosen per
+                           launch from the grid by a wave model; PPM keeps whole columns) */
     int candidates;     /* plans timed by mg_autotune */
     double ms_default;  /* one projection with the plan in force before mg_autotune */
     double ms_tuned;    /* one projection with the plan it chose */
+    double k1_ms_default, k1_ms_tuned;   /* one stage-1 scalar-advection launch, likewise */
 } mg_tune;
 int mg_autotune(mg_ctx *ctx, int reps, mg_tune *result);
 int mg_tune_get(mg_ctx *ctx, mg_tune *t);

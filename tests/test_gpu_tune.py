@@ -62,8 +62,10 @@ def test_autotune_keeps_state_and_step_parity():
         back = m.download()
         for x, y in zip(_fields(back), _fields(st)):
             assert np.array_equal(x[:, 3:-2, 3:-2], y[:, 3:-2, 3:-2])
-        # a non-default plan, then a few steps against the oracle
-        m.tune_set(dict(plan, x_radix=[2, 8, 3], y_radix=[5, 8], x_threads=16, y_threads=16, tri_block=64))
+        # a non-default plan (the scalar advection in its two k segments of 10 levels), then
+        # a few steps against the oracle
+        m.tune_set(dict(plan, x_radix=[2, 8, 3], y_radix=[5, 8], x_threads=16, y_threads=16, tri_block=64,
+                        k1_segments=2))
         m.stepping(3, ntime0=1, graph=True)
         g = m.download()
     r, _, _ = O.Oracle(d).stepping(st, nsteps=3, ntime0=1)
@@ -77,7 +79,8 @@ def test_invalid_plans_rejected():
     with Mimica(d, nscal=1) as m:
         base = m.tune_get()
         for bad in (dict(base, x_radix=[8, 8]), dict(base, y_radix=[7, 3]), dict(base, x_threads=128),
-                    dict(base, y_threads=256), dict(base, tri_block=96), dict(base, x_radix=[6, 4])):
+                    dict(base, y_threads=256), dict(base, tri_block=96), dict(base, x_radix=[6, 4]),
+                    dict(base, k1_segments=-1), dict(base, k1_segments=13)):
             with pytest.raises(_lib.MimicaError):
                 m.tune_set(bad)
         assert m.tune_get() == base
@@ -89,7 +92,7 @@ def test_wisdom_replays_a_plan(tmp_path):
     with Mimica(d, nscal=1) as m:
         first = m.autotune(reps=2, wisdom=path)
     assert first["source"] == "measured"
-    stored = tune.load(path)[tune.key(64, 48, 16, _lib.MG_PREC_FP64)]
+    stored = tune.load(path)[tune.key(64, 48, 16, _lib.MG_PREC_FP64, 1)]
     with Mimica(d, nscal=1) as m:
         second = m.autotune(wisdom=path)
         assert second["source"] == "wisdom"

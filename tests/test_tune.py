@@ -33,15 +33,17 @@ def test_radix_candidates_reject_other_primes():
 
 
 def test_wisdom_round_trip(tmp_path):
-    plan = {"x_radix": [4, 4, 4, 4, 2], "y_radix": [3, 8, 4], "x_threads": 16, "y_threads": 64, "tri_block": 256}
+    plan = {"x_radix": [4, 4, 4, 4, 2], "y_radix": [3, 8, 4], "x_threads": 16, "y_threads": 64, "tri_block": 256,
+            "k1_segments": 2}
     t = tune.from_dict(plan)
     assert tune.to_dict(t) == plan
     path = str(tmp_path / "wisdom.json")
-    k = tune.key(512, 96, 64, _lib.MG_PREC_FP64)
+    k = tune.key(512, 96, 64, _lib.MG_PREC_FP64, 5)
     tune.store(path, k, dict(plan, ms_tuned=1.0))
-    tune.store(path, tune.key(64, 64, 32, _lib.MG_PREC_MIXED), plan)
+    tune.store(path, tune.key(64, 64, 32, _lib.MG_PREC_MIXED, 2), plan)
     w = tune.load(path)
     assert w[k] == plan and len(w) == 2
     assert tune.load(str(tmp_path / "absent.json")) == {}
+    assert tune.key(512, 96, 64, _lib.MG_PREC_FP64, 5) != tune.key(512, 96, 64, _lib.MG_PREC_FP64, 2)
     with pytest.raises(ValueError):
         tune.from_dict(dict(plan, x_radix=[]))
