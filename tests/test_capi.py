@@ -61,6 +61,18 @@ def test_null_pointers_rejected():
     assert L.mg_destroy(None) == _lib.MG_ERR_PARAM
     assert L.mg_step(None, 1, 1, None, None) == _lib.MG_ERR_PARAM
     assert L.mg_grid_metrics(1, 1.0, None, None, None, None) == _lib.MG_ERR_PARAM
+    # trajectory, autotuner and timing entries: a null context is rejected before any
+    # device work
+    assert L.mg_traj_forward(None, 1, 1) == _lib.MG_ERR_PARAM
+    assert L.mg_traj_tl(None, 1, 1, None, None) == _lib.MG_ERR_PARAM
+    assert L.mg_traj_adjoint(None, 1, 1, 1, None, None) == _lib.MG_ERR_PARAM
+    assert L.mg_traj_record_limit(None, 0.0) == _lib.MG_ERR_PARAM
+    assert L.mg_time_traj(None, 1, 1, 1, None) == _lib.MG_ERR_PARAM
+    assert L.mg_autotune(None, 3, None) == _lib.MG_ERR_PARAM
+    assert L.mg_tune_get(None, None) == _lib.MG_ERR_PARAM
+    assert L.mg_tune_set(None, None) == _lib.MG_ERR_PARAM
+    assert L.mg_radix_candidates(0, None, None, 4) == _lib.MG_ERR_PARAM
+    assert L.mg_qnadv_ad(None, 1, *([None] * 9)) == _lib.MG_ERR_PARAM
 
 
 def test_host_precompute_matches_formulas():
