@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(256) sgs_prep_kernel(DevGrid G, SgsDev S, cons
 
 // efud (subgrid.f90:187-456): out := (in + eh) + ev for u, v (levels 1..nz-1) and
 // w (levels 2..nz-1), in = 0 when null.  fkv and the dij fields carry periodic ghosts.
-__global__ void __launch_bounds__(256) sgs_mom_kernel(DevGrid G, SgsDev S, const double *__restrict__ u,
+__global__ void __launch_bounds__(256, 4) sgs_mom_kernel(DevGrid G, SgsDev S, const double *__restrict__ u,
                                                       const double *__restrict__ v, const double *__restrict__ fev,
                                                       SgsDij D, const double *mflux,
                                                       const double *in_u, const double *in_v, const double *in_w,
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(256) sgs_mom_kernel(DevGrid G, SgsDev S, const
 // eff (subgrid.f90:604-789) with grad_quick (gradients.f90:62-187), CONSERVATIVE:
 // out := SGS tendency of each density-weighted scalar on levels 1..nz-1.  One thread
 // per cell serves every field: the diffusivities of the seven points are loaded once.
-__global__ void __launch_bounds__(256) sgs_scal_kernel(DevGrid G, SgsDev S, const double *__restrict__ nutv, SgsScal A)
+__global__ void __launch_bounds__(256, 5) sgs_scal_kernel(DevGrid G, SgsDev S, const double *__restrict__ nutv, SgsScal A)
 {
     const int i = 4 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 4 + blockIdx.y * blockDim.y + threadIdx.y;
