@@ -45,6 +45,7 @@ struct mg_ctx {
     int *derr = nullptr;                 // device error flag of bounded waits
     int rep = REP_NAT;
     int k1_nseg = 0;                     // K1 k segments per tile (0: chosen per launch for this grid alone)
+    int k2_nseg = 0;                     // K2 likewise
     double traj_rec_limit = -1.;         // bytes the trajectory adjoint's stage records may take (< 0: half the free memory)
     int have_state = 0;
     int launches = 0;
@@ -637,6 +638,7 @@ static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int wa
         // ---- K2: momentum ----
         K2Args a2{};
         a2.stage = stage; a2.rep = REP_NAT; a2.ntime = ntime; a2.a_dt = a_dt; a2.b = b;
+        a2.nseg = c->k2_nseg;
         a2.mu = mom[0]; a2.mv = mom[1]; a2.mw = mom[2];
         a2.in_is_leveln = stage == 1;
         a2.mu_n = c->mA[0]; a2.mv_n = c->mA[1]; a2.mw_n = c->mA[2];
@@ -811,10 +813,12 @@ static cudaError_t ens_issue(mg_ens *e, int ntime, int nst, int *launches)
         mg_ctx *c = e->m[i];
         er = cudaStreamWaitEvent(c->stream, e->fork, 0);
         // the members run side by side and fill the device together: whole columns per CTA
-        const int nseg_own = c->k1_nseg;
+        const int nseg1 = c->k1_nseg, nseg2 = c->k2_nseg;
         c->k1_nseg = 1;
+        c->k2_nseg = 1;
         for (int s = 0; s < nst && er == cudaSuccess; s++) er = step_once(c, ntime + s, 0, 0, 0, launches);
-        c->k1_nseg = nseg_own;
+        c->k1_nseg = nseg1;
+        c->k2_nseg = nseg2;
         if (er == cudaSuccess) er = cudaEventRecord(e->join[i], c->stream);
         if (er == cudaSuccess) er = cudaStreamWaitEvent(e->stream, e->join[i], 0);
     }

@@ -23,6 +23,28 @@ template <typename R> __host__ __device__ constexpr size_t k2_ring_bytes() { ret
 template <typename R> __host__ __device__ constexpr size_t k2_smem_bytes() { return k2_ring_bytes<R>() + 3 * STG_SLOT + 128 + 128; }
 constexpr double AVISC = 1. / 16.;   // windadv.f90:39
 
+// k segments per column tile, as K1's (k1_body.cuh): the count that minimises (waves of
+// CTAs) x (levels per segment + 2, the prologue's flux levels and the ring fill), with
+// segments of at least 8 levels; CTAs per SM from the shared memory (at most 2 by the
+// registers of 256 threads)
+inline int k2_segments(const DevGrid &g, size_t smem)
+{
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        nsm = 148;
+    long long per_sm = (228LL * 1024) / ((long long)smem + 1024);
+    per_sm = per_sm < 1 ? 1 : (per_sm > 2 ? 2 : per_sm);
+    const long long slots = (long long)nsm * per_sm;
+    const long long tiles = (long long)((g.maxx + TX - 1) / TX) * ((g.maxy + TY - 1) / TY);
+    int best = 1;
+    double bt = 1e300;
+    for (int sgm = 1; sgm <= (g.nz / 8 > 1 ? g.nz / 8 : 1); sgm++) {
+        const double t = (double)((tiles * sgm + slots - 1) / slots) * ((double)g.nz / sgm + 2.);
+        if (t < 0.999 * bt) { bt = t; best = sgm; }
+    }
+    return best;
+}
+
 __device__ __forceinline__ double ldg(const double *p, long long i) { return __ldg(p + i); }
 __device__ __forceinline__ double abs_r(double x) { return fabs(x); }
 __device__ __forceinline__ float abs_r(float x) { return fabsf(x); }
@@ -40,8 +62,9 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
     double *stg = reinterpret_cast<double *>(smb + k2_ring_bytes<R>());   // [3][SBH][SBW] raw level
     uint64_t *mbar = reinterpret_cast<uint64_t *>(smb + k2_ring_bytes<R>() + 3 * STG_SLOT);
 
-    const int ntx = (G.maxx + TX - 1) / TX;
-    const int ti = blockIdx.x % ntx, tj = blockIdx.x / ntx;
+    const int ntx = (G.maxx + TX - 1) / TX, nty = (G.maxy + TY - 1) / TY;
+    const int tile = blockIdx.x % (ntx * nty), seg = blockIdx.x / (ntx * nty);
+    const int ti = tile % ntx, tj = tile / ntx;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const int i0 = 4 + ti * TX, j0 = 4 + tj * TY;
     const int i = i0 + tx, j = j0 + ty;
@@ -63,6 +86,11 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
     }
     __syncthreads();
     // raw level l -> staging (single slot; the l-th copy completes phase (l-1)&1)
+    // this CTA's levels [kb, ke]; a segment above the surface starts at kp = kb - 3 with
+    // prologue levels that only advance the carried vertical fluxes
+    const int kb = 1 + (int)(((long long)seg * nz) / A.nseg), ke = (int)(((long long)(seg + 1) * nz) / A.nseg);
+    const int kp = kb > 3 ? kb - 3 : 1;
+    const int lmax = min(nz, ke + 2);   // last level the ring needs
     auto issue_raw = [&](int l) {
         fence_proxy_async_shared();
         mbar_arrive_expect_tx(mbar, 3 * STG_BYTES);
@@ -72,7 +100,7 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
     // staging -> ring slot of level l: stencil momentum and advective velocity (zero
     // outside the domain, as the reference's arrays are read there)
     auto convert_level = [&](int l) {
-        mbar_wait_bounded(mbar, (uint32_t)((l - 1) & 1), A.err);
+        mbar_wait_bounded(mbar, (uint32_t)((l - kp) & 1), A.err);
         const int slot = l % NSLOT;
         const double d0 = ldg(G.den0, l - 1), a0 = ldg(G.avden0, l - 1);
         for (int q = tid; q < 3 * PL; q += TX * TY) {
@@ -107,15 +135,15 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
 #define ACC1(acc, a) do { acc = acc + (a); } while (0)
 #define SUB1(acc, a) do { acc = acc - (a); } while (0)
 
-    if (tid == 0) issue_raw(1);
-    convert_level(1);
+    if (tid == 0) issue_raw(kp);
+    convert_level(kp);
     __syncthreads();
-    if (nz >= 2) {
-        if (tid == 0) issue_raw(2);
-        convert_level(2);
+    if (kp + 1 <= lmax) {
+        if (tid == 0) issue_raw(kp + 1);
+        convert_level(kp + 1);
         __syncthreads();
     }
-    if (tid == 0 && nz >= 3) issue_raw(3);
+    if (tid == 0 && kp + 2 <= lmax) issue_raw(kp + 2);
 
     double bb_prev = 0.;   // buoyancy at level k-1 (cell centre)
     // vertical fluxes carried up the column (each computed once):
@@ -128,17 +156,42 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
     const double grav = 9.81, epsm = 0.60243, cdiag = 0.5;
     const int own = (ty + RH) * PW + (tx + RH);
 
-    for (int k = 1; k <= nz; k++) {
+    // buoyancy bb of a cell (imp_buoy: state + cdiag*dt0*states)
+    auto buoy_bb = [&](int k, double dn, double esv, double qtv, double fesv, double fqtv) {
+        if (A.dens_is_leveln) {
+            esv = rep_value(A.rep, esv, dn);
+            if (A.qt) qtv = rep_value(A.rep, qtv, dn);
+        }
+        double est = esv + cdiag * dt0 * fesv;
+        double qtt = A.qt ? qtv + cdiag * dt0 * fqtv : 0.;
+        double den1 = 1. / dn;
+        double pt = den1 * est;
+        double sumh = 0.;
+        double ref = ldg(G.pt0, k - 1) * (1. + epsm * ldg(G.qv0, k - 1));
+        return dn * grav * (pt * (1. + epsm * den1 * (qtt - sumh) - den1 * sumh) / ref - 1.);
+    };
+    // a segment above the surface: p/rho0 and the buoyancy of level kb-1, as the
+    // segment below computes them
+    if (kb > 1 && act && A.mode != 1) {
+        const long long idm = gidx(G, i, j, kb - 1);
+        pp_below = ldg(A.p, idm) / ldg(G.den0, kb - 2);
+        if (G.with_buoy)
+            bb_prev = buoy_bb(kb - 1, ldg(A.dens, idm), ldg(A.es, idm), A.qt ? ldg(A.qt, idm) : 0., ldg(A.fes, idm),
+                              A.qt ? ldg(A.fqt, idm) : 0.);
+    }
+
+    for (int k = kp; k <= ke; k++) {
+        const bool pro = k < kb;   // prologue level: the carried vertical fluxes only
         __syncthreads();   // ring slot (k+2)%5 (level k-3) no longer read
-        if (k + 2 <= nz) convert_level(k + 2);
+        if (k + 2 <= lmax) convert_level(k + 2);
         __syncthreads();   // ring complete for level k; the staging slot is free
-        if (tid == 0 && k + 3 <= nz) issue_raw(k + 3);
+        if (tid == 0 && k + 3 <= lmax) issue_raw(k + 3);
         if (!act) continue;   // no further barriers in this iteration
         // epilogue operands of this level, issued before the stencil arithmetic
         const long long idx = gidx(G, i, j, k);
         double e_p = 0., e_pw = 0., e_ps = 0., e_dn = 0., e_es = 0., e_qt = 0., e_fes = 0., e_fqt = 0.;
         double e_tu = 0., e_tv = 0., e_tw = 0., e_un = 0., e_vn = 0., e_wn = 0.;
-        if (A.mode != 1) {
+        if (A.mode != 1 && !pro) {
             e_p = ldg(A.p, idx);
             e_pw = ldg(A.p, idx - 1);
             e_ps = ldg(A.p, idx - G.px);
@@ -198,6 +251,7 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
             fzw0 = fzw1; fzw1 = fw;
             azw0 = azw1; azw1 = azw2; azw2 = aw_;
         }
+        if (pro) continue;
 
         // ---------------- u component ----------------
         double au = 0.;
@@ -346,19 +400,7 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
         // ---------------- buoyancy (imp_buoy: state + cdiag*dt0*states) ----------------
         double buoy = 0.;
         if (G.with_buoy) {
-            double dn = e_dn;
-            double esv = e_es, qtv = A.qt ? e_qt : 0.;
-            if (A.dens_is_leveln) {
-                esv = rep_value(A.rep, esv, dn);
-                if (A.qt) qtv = rep_value(A.rep, qtv, dn);
-            }
-            double est = esv + cdiag * dt0 * e_fes;
-            double qtt = A.qt ? qtv + cdiag * dt0 * e_fqt : 0.;
-            double den1 = 1. / dn;
-            double pt = den1 * est;
-            double sumh = 0.;
-            double ref = ldg(G.pt0, k - 1) * (1. + epsm * ldg(G.qv0, k - 1));
-            double bb = dn * grav * (pt * (1. + epsm * den1 * (qtt - sumh) - den1 * sumh) / ref - 1.);
+            const double bb = buoy_bb(k, e_dn, e_es, A.qt ? e_qt : 0., e_fes, e_fqt);
             buoy = k >= 2 ? 0.5 * (bb_prev + bb) : bb;
             bb_prev = bb;
         }

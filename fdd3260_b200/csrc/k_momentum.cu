@@ -8,6 +8,8 @@ cudaError_t launch_k2(const DevGrid &g, const K2Args &a, const K2Maps &maps, cud
     const size_t sm = k2_smem_bytes<double>();
     cudaError_t e = cudaFuncSetAttribute(k2_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    k2_kernel<false><<<ntx * nty, dim3(TX, TY), sm, s>>>(g, a, maps);
+    K2Args as = a;
+    if (as.nseg < 1 || as.nseg > g.nz) as.nseg = k2_segments(g, sm);
+    k2_kernel<false><<<ntx * nty * as.nseg, dim3(TX, TY), sm, s>>>(g, as, maps);
     return cudaGetLastError();
 }

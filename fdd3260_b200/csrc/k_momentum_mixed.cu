@@ -9,6 +9,8 @@ cudaError_t launch_k2_mixed(const DevGrid &g, const K2Args &a, const K2Maps &map
     const size_t sm = k2_smem_bytes<float>();
     cudaError_t e = cudaFuncSetAttribute(k2_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    k2_kernel<true><<<ntx * nty, dim3(TX, TY), sm, s>>>(g, a, maps);
+    K2Args as = a;
+    if (as.nseg < 1 || as.nseg > g.nz) as.nseg = k2_segments(g, sm);
+    k2_kernel<true><<<ntx * nty * as.nseg, dim3(TX, TY), sm, s>>>(g, as, maps);
     return cudaGetLastError();
 }

@@ -91,6 +91,7 @@ struct K2Args {
     int mode;                      // 0: full stage; 1: unit mode: ou/ov/ow := advection tendency only
     int *err;                      // device error flag (bounded waits)
     const double *su, *sv, *sw;    // SGS momentum tendencies (efud), or null: winds starts at S
+    int nseg;                      // k segments per column tile (0: launch_k2 chooses for the grid alone)
 };
 // TMA descriptors of the K2 stencil momentum (boxes of 38 x 12 doubles)
 struct alignas(64) K2Maps {
