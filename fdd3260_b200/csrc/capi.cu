@@ -1765,9 +1765,10 @@ static int traj_adjoint_run(mg_ctx *c, int nsteps, int ntime0, int ckpt, const d
     S.pb = T.B.get();
     // checkpoints (natural states every ckpt steps) and the states of one segment
     const int nck = nsteps / ckpt + 1;
-    std::vector<NatState> ck(nck), seg(ckpt + 1);
+    const int nseg = std::max(1, std::min(ckpt, nsteps));   // steps of the longest segment
+    std::vector<NatState> ck(nck), seg(nseg + 1);
     for (int q = 0; q < nck; q++) ck[q] = nat_alloc(T.B, nf);
-    for (int q = 0; q <= ckpt; q++) seg[q] = nat_alloc(T.B, nf);
+    for (int q = 0; q <= nseg; q++) seg[q] = nat_alloc(T.B, nf);
     NatState bar = nat_alloc(T.B, nf), tmp = nat_alloc(T.B, nf);
     // the stage records of every step of a segment, when they fit in half the free memory:
     // the segment's forward recomputation then leaves them for its backward sweep;
@@ -1775,10 +1776,10 @@ static int traj_adjoint_run(mg_ctx *c, int nsteps, int ntime0, int ckpt, const d
     size_t mfree = 0, mtot = 0;
     CKR(T.B.err);
     CKR(cudaMemGetInfo(&mfree, &mtot));
-    const double rec_bytes = (double)ckpt * 2 * (2 * nf + 3) * (double)c->fbytes;
+    const double rec_bytes = (double)nseg * 2 * (2 * nf + 3) * (double)c->fbytes;
     const bool keep = rec_bytes < 0.5 * (double)mfree && (c->traj_rec_limit < 0. || rec_bytes <= c->traj_rec_limit);
-    std::vector<StageRec> rec1(keep ? ckpt : 0), rec2(keep ? ckpt : 0);
-    for (int q = 0; keep && q < ckpt; q++)
+    std::vector<StageRec> rec1(keep ? nseg : 0), rec2(keep ? nseg : 0);
+    for (int q = 0; keep && q < nseg; q++)
         for (StageRec *R : {&rec1[q], &rec2[q]}) {
             for (int f = 0; f < nf; f++) { R->xs[f] = T.B.get(); R->A[f] = T.B.get(); }
             for (int m = 0; m < 3; m++) R->xm[m] = T.B.get();
