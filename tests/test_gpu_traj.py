@@ -114,7 +114,7 @@ def test_checkpoint_interval_does_not_change_gradient():
     res = []
     with Mimica(d, nscal=2) as m:
         m.upload(st)
-        for ck in (1, 2, 5):
+        for ck in (1, 2, 5, 10):   # 10: one segment longer than the trajectory
             res.append(m.traj_adjoint(lam, 5, ckpt=ck))
         # no stage records kept: every backward step recomputes its stages
         m.traj_record_limit(0)
