@@ -276,7 +276,13 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
 
-    ws, rank, local = dist_init()
+    if args.impl == "reference":
+        # the CPU arm needs no process group: rank 0 runs it, the other ranks exit at once
+        ws, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+        if rank != 0:
+            return
+    else:
+        ws, rank, local = dist_init()
     if args.workload == "ensemble":
         return run_ensemble(args, ws, rank, local)
     from fdd3260_b200 import Mimica, config
