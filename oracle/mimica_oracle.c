@@ -116,6 +116,7 @@ void mo_get_wv(int nxp, int nyp, double dx, double dy, double *wv)
 void mo_statebc(const mo_grid *g, double *x)
 {
     const int nx = g->nx, ny = g->ny, nz = g->nz;
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= nz; k++)
         for (int j = 1; j <= ny; j++) {
             x[IX(g, 1, j, k)] = x[IX(g, nx - 4, j, k)];
@@ -124,6 +125,7 @@ void mo_statebc(const mo_grid *g, double *x)
             x[IX(g, nx, j, k)] = x[IX(g, 5, j, k)];
             x[IX(g, nx - 1, j, k)] = x[IX(g, 4, j, k)];
         }
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= nz; k++)
         for (int i = 1; i <= nx; i++) {
             x[IX(g, i, 1, k)] = x[IX(g, i, ny - 4, k)];
@@ -980,6 +982,7 @@ void mo_advection_ac(const mo_grid *g, const double *x, const double *ua, const 
 void mo_get_advective(const mo_grid *g, const double *mu, const double *mv, const double *mw,
                       double *ua, double *va, double *wa)
 {
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= g->nz; k++) {
         double d0 = P1(g->den0, k), ad0 = P1(g->avden0, k);
         for (int j = 1; j <= g->ny; j++)
@@ -1327,18 +1330,21 @@ void mo_caldiv(const mo_grid *g, double *mu, double *mv, double *mw, double *div
     double dx1 = 1. / g->dx, dy1 = 1. / g->dy;
     memset(div, 0, ncell(g) * sizeof(double));
     windbc(g, mu, mv, mw);
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= nz; k++)
         for (int j = 4; j <= ny - 2; j++)
             for (int i = 4; i <= nx - 2; i++) {
                 size_t c = IX(g, i, j, k);
                 div[c] = div[c] + (mu[IX(g, i + 1, j, k)] - mu[c]) * dx1;
             }
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= nz; k++)
         for (int j = 4; j <= ny - 2; j++)
             for (int i = 4; i <= nx - 2; i++) {
                 size_t c = IX(g, i, j, k);
                 div[c] = div[c] + (mv[IX(g, i, j + 1, k)] - mv[c]) * dy1;
             }
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= nz - 1; k++)
         for (int j = 4; j <= ny - 2; j++)
             for (int i = 4; i <= nx - 2; i++) {
@@ -1362,6 +1368,7 @@ void mo_gradp(const mo_grid *g, double *p, const double *w, double *gpx, double 
     memset(gpx, 0, nc * sizeof(double));
     memset(gpy, 0, nc * sizeof(double));
     memset(gpz, 0, nc * sizeof(double));
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= nz; k++)
         for (int j = 4; j <= ny - 2; j++)
             for (int i = 4; i <= nx - 2; i++) {
@@ -1369,6 +1376,7 @@ void mo_gradp(const mo_grid *g, double *p, const double *w, double *gpx, double 
                 gpx[c] = (p[c] - p[IX(g, i - 1, j, k)]) * dx1;
                 gpy[c] = (p[c] - p[IX(g, i, j - 1, k)]) * dy1;
             }
+#pragma omp parallel for schedule(static)
     for (int k = 2; k <= nz; k++)
         for (int j = 4; j <= ny - 2; j++)
             for (int i = 4; i <= nx - 2; i++) {
@@ -1390,6 +1398,7 @@ void mo_buoyancy(const mo_grid *g, const double *dens, const double *es, const d
     const int nx = g->nx, ny = g->ny, nz = g->nz;
     size_t plane = (size_t)nx * ny;
     double *bb = dalloc(ncell(g));
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= nz; k++) {
         double ref = P1(g->pt0, k) * (1. + epsm * P1(g->qv0, k));
         for (size_t c = (size_t)(k - 1) * plane; c < (size_t)k * plane; c++) {
@@ -1400,6 +1409,7 @@ void mo_buoyancy(const mo_grid *g, const double *dens, const double *es, const d
             bb[c] = dens[c] * grav * (pt * (1. + epsm * den1 * (q - sumh) - den1 * sumh) / ref - 1.);
         }
     }
+#pragma omp parallel for schedule(static)
     for (int k = 2; k <= nz; k++)
         for (size_t c = 0; c < plane; c++)
             buoy[(size_t)(k - 1) * plane + c] = 0.5 * (bb[(size_t)(k - 2) * plane + c] + bb[(size_t)(k - 1) * plane + c]);
@@ -1466,12 +1476,97 @@ static void fft1d(int n, double *re, double *im, size_t stride, int sign)
     free(ir); free(ii); free(or_); free(oi); free(scr);
 }
 
+#ifdef MO_FAST_FFT
+/* The timed CPU build (OpenMP): the same mixed-radix decimation in time, with the
+ * twiddles exp(sign 2 pi i t / n) tabulated once per call (long double trigonometry
+ * rounded to double) and double arithmetic, as an FFT library does.  It agrees with the
+ * restatement above to ~1e-15 relative; the parity build keeps the restatement. */
+typedef struct { int n; double *c, *s; } mo_tw;
+
+static void fft1d_rec_fast(int n, int stride, const double *ire, const double *iim, double *ore, double *oim,
+                           int sign, double *scratch, const mo_tw *W)
+{
+    if (n == 1) { ore[0] = ire[0]; oim[0] = iim[0]; return; }
+    int p = 0;
+    for (int r = 2; r * r <= n; r++) if (n % r == 0) { p = r; break; }
+    if (!p) p = n;
+    const int m = n / p, step = W->n / n;   /* twiddle t/n of this level = table entry t*step */
+    if (p == n) {
+        for (int kk = 0; kk < n; kk++) {
+            double sr = 0., si = 0.;
+            int r = 0;   /* kk*t mod n, advanced by kk per term */
+            for (int t = 0; t < n; t++) {
+                const int e = r * step;
+                const double c = W->c[e], sn = sign * W->s[e];
+                sr += ire[(size_t)t * stride] * c - iim[(size_t)t * stride] * sn;
+                si += ire[(size_t)t * stride] * sn + iim[(size_t)t * stride] * c;
+                r += kk;
+                if (r >= n) r -= n;
+            }
+            ore[kk] = sr; oim[kk] = si;
+        }
+        return;
+    }
+    for (int q = 0; q < p; q++)
+        fft1d_rec_fast(m, stride * p, ire + (size_t)q * stride, iim + (size_t)q * stride, ore + (size_t)q * m,
+                       oim + (size_t)q * m, sign, scratch + 2 * n, W);
+    double *tr = scratch, *ti = scratch + n;
+    for (int kk = 0, k1 = 0; kk < n; kk++, k1 = (k1 + 1 == m) ? 0 : k1 + 1) {
+        double sr = 0., si = 0.;
+        int r = 0;   /* q*kk mod n, advanced by kk per term */
+        for (int q = 0; q < p; q++) {
+            const int e = r * step;
+            const double c = W->c[e], sn = sign * W->s[e];
+            const double xr = ore[(size_t)q * m + k1], xi = oim[(size_t)q * m + k1];
+            sr += xr * c - xi * sn;
+            si += xr * sn + xi * c;
+            r += kk;
+            if (r >= n) r -= n;
+        }
+        tr[kk] = sr; ti[kk] = si;
+    }
+    memcpy(ore, tr, n * sizeof(double));
+    memcpy(oim, ti, n * sizeof(double));
+}
+
+static mo_tw tw_make(int n)
+{
+    mo_tw W = {n, dalloc(n), dalloc(n)};
+    for (int t = 0; t < n; t++) {
+        const long double ang = 2.0L * 3.141592653589793238462643383279502884L * (long double)t / n;
+        W.c[t] = (double)cosl(ang);
+        W.s[t] = (double)sinl(ang);
+    }
+    return W;
+}
+
+void mo_fft2d(int nxp, int nyp, double *re, double *im, int inverse)
+{
+    const int sign = inverse ? +1 : -1, nmax = nxp > nyp ? nxp : nyp;
+    mo_tw Wx = tw_make(nxp), Wy = tw_make(nyp);
+    double *ir = dalloc(nmax), *ii = dalloc(nmax), *or_ = dalloc(nmax), *oi = dalloc(nmax), *scr = dalloc((size_t)8 * nmax + 64);
+    for (int m = 0; m < nyp; m++) {
+        double *r = re + (size_t)m * nxp, *i = im + (size_t)m * nxp;
+        fft1d_rec_fast(nxp, 1, r, i, or_, oi, sign, scr, &Wx);
+        memcpy(r, or_, nxp * sizeof(double));
+        memcpy(i, oi, nxp * sizeof(double));
+    }
+    for (int l = 0; l < nxp; l++) {
+        for (int t = 0; t < nyp; t++) { ir[t] = re[l + (size_t)t * nxp]; ii[t] = im[l + (size_t)t * nxp]; }
+        fft1d_rec_fast(nyp, 1, ir, ii, or_, oi, sign, scr, &Wy);
+        for (int t = 0; t < nyp; t++) { re[l + (size_t)t * nxp] = or_[t]; im[l + (size_t)t * nxp] = oi[t]; }
+    }
+    free(ir); free(ii); free(or_); free(oi); free(scr);
+    free(Wx.c); free(Wx.s); free(Wy.c); free(Wy.s);
+}
+#else
 void mo_fft2d(int nxp, int nyp, double *re, double *im, int inverse)
 {
     int sign = inverse ? +1 : -1;
     for (int m = 0; m < nyp; m++) fft1d(nxp, re + (size_t)m * nxp, im + (size_t)m * nxp, 1, sign);
     for (int l = 0; l < nxp; l++) fft1d(nyp, re + l, im + l, (size_t)nxp, sign);
 }
+#endif
 
 /* src/PRESSURE/fft_tools.f90:202-237 */
 static int tridag2(const double *A, const double *B, const double *C, const double *R, double *U, int N)
@@ -1547,6 +1642,7 @@ int mo_fft_solve(const mo_grid *g, const double *tend, double *out)
     const int nxp = g->nx - 5, nyp = g->ny - 5, nzp = g->nz;
     size_t pl = (size_t)nxp * nyp;
     double *re = dalloc(pl * nzp), *im = dalloc(pl * nzp);
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= nzp; k++)
         for (int m = 1; m <= nyp; m++)
             for (int l = 1; l <= nxp; l++)
@@ -1565,6 +1661,7 @@ int mo_fft_solve(const mo_grid *g, const double *tend, double *out)
     }
 #pragma omp parallel for schedule(static)
     for (int k = 0; k < nzp; k++) mo_fft2d(nxp, nyp, re + (size_t)k * pl, im + (size_t)k * pl, 1);
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= nzp; k++)
         for (int m = 1; m <= nyp; m++)
             for (int l = 1; l <= nxp; l++)
@@ -1577,6 +1674,7 @@ int mo_fft_solve(const mo_grid *g, const double *tend, double *out)
 void mo_horav(const mo_grid *g, const double *x, double *xav)
 {
     const int nx = g->nx, ny = g->ny, nz = g->nz;
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= nz; k++) {
         double s = 0., ii = 0.;
         for (int j = 4; j <= ny - 2; j++)
@@ -1594,9 +1692,11 @@ void mo_rescale_pressure(const mo_grid *g, double *pp)
 {
     size_t nc = ncell(g), pl = (size_t)g->nx * g->ny;
     double nh = (double)((g->nx - 5) * (g->ny - 5));
+#pragma omp parallel for schedule(static)
     for (size_t c = 0; c < nc; c++) pp[c] = pp[c] / nh;
     double *pav = dalloc(g->nz);
     mo_horav(g, pp, pav);
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= g->nz; k++)
         for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) pp[c] = pp[c] - P1(pav, k);
     free(pav);
@@ -1616,6 +1716,7 @@ int mo_anelastic_pressure(const mo_grid *g, double *mu, double *mv, double *mw, 
     for (int ip = 1; ip <= g->nsubp; ip++) {
         /* solve_pressure */
         mo_caldiv(g, mu, mv, mw, tend);
+#pragma omp parallel for schedule(static)
         for (int k = 1; k <= nz; k++)
             for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) tend[c] = dt1 * tend[c] / P1(g->den0, k);
         memset(deltap, 0, nc * sizeof(double));
@@ -1623,9 +1724,11 @@ int mo_anelastic_pressure(const mo_grid *g, double *mu, double *mv, double *mw, 
         if (e && !err) err = e;
         mo_rescale_pressure(g, deltap);
         /* correction */
+#pragma omp parallel for schedule(static)
         for (int k = 1; k <= nz; k++)
             for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) p[c] = p[c] + P1(g->den0, k) * deltap[c];
         mo_gradp(g, deltap, mw, gpx, gpy, gpz);
+#pragma omp parallel for schedule(static)
         for (int k = 1; k <= nz; k++)
             for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) {
                 mu[c] = mu[c] - g->dt0 * P1(g->den0, k) * gpx[c];
@@ -1637,6 +1740,7 @@ int mo_anelastic_pressure(const mo_grid *g, double *mu, double *mv, double *mw, 
     /* cal_p1 */
     {
         double *wav = dalloc(nz);
+#pragma omp parallel for schedule(static)
         for (size_t c = 0; c < nc; c++) tend[c] = (mw[c] - wold[c]) / g->dt0;
         mo_horav(g, tend, wav);
         if (p1) {
@@ -1645,6 +1749,7 @@ int mo_anelastic_pressure(const mo_grid *g, double *mu, double *mv, double *mw, 
                 P1(p1, k) = P1(p1, k + 1) + P1(wav, k + 1) * 0.5 * g->dz * (P1(g->fdz0, k) + P1(g->fdz0, k + 1));
         }
         mo_horav(g, mw, wav);
+#pragma omp parallel for schedule(static)
         for (int k = 1; k <= nz; k++)
             for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) mw[c] = mw[c] - P1(wav, k);
         free(wav);
@@ -2082,14 +2187,17 @@ int mo_step(const mo_grid *g, int ntime, double *u, double *v, double *w, double
     for (int s = 0; s < nsc; s++) { s2[s] = dalloc(nc); memcpy(s2[s], scal[s], nc * 8); }
     /* working state: momentum and conserved scalars */
     double *mu = dalloc(nc), *mv = dalloc(nc), *mw = dalloc(nc);
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= nz; k++)
         for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) {
             mu[c] = u[c] * P1(g->den0, k);
             mv[c] = v[c] * P1(g->den0, k);
             mw[c] = w[c] * P1(g->avden0, k);
         }
-    for (int s = 0; s < nsc; s++)
+    for (int s = 0; s < nsc; s++) {
+#pragma omp parallel for schedule(static)
         for (size_t c = 0; c < nc; c++) scal[s][c] = scal[s][c] * dens[c];
+    }
     /* tendency accumulators (tend, reset at step start) */
     double *tu = dalloc(nc), *tv = dalloc(nc), *tw = dalloc(nc), *td = dalloc(nc);
     double **ts = (double **)calloc(nsc ? nsc : 1, sizeof(double *));
@@ -2140,9 +2248,11 @@ int mo_step(const mo_grid *g, int ntime, double *u, double *v, double *w, double
                 if (s == 0 || s == iqt)
                     for (size_t c = 0; c < nc; c++) wss[s][c] = wss[s][c] + sgsc[s][c];
         /* momentum */
+#pragma omp parallel for schedule(static)
         for (int k = 1; k <= nz; k++)
             for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) pp[c] = p[c] / P1(g->den0, k);
         mo_gradp(g, pp, mw, gpx, gpy, gpz);
+#pragma omp parallel for schedule(static)
         for (int k = 1; k <= nz; k++)
             for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) {
                 wsu[c] = wsu[c] - P1(g->den0, k) * gpx[c];
@@ -2159,6 +2269,7 @@ int mo_step(const mo_grid *g, int ntime, double *u, double *v, double *w, double
             for (size_t c = 0; c < nc; c++) buoy[c] = 0. * 0. + (1. - 0.) * buoy[c];
         }
         mo_qnadv_uvw(g, ntime, mu, mv, mw, ua, va, wa, au, av, aw);
+#pragma omp parallel for schedule(static)
         for (int k = 1; k <= nz; k++)
             for (int j = 4; j <= ny - 2; j++)
                 for (int i = 4; i <= nx - 2; i++) {
@@ -2168,6 +2279,7 @@ int mo_step(const mo_grid *g, int ntime, double *u, double *v, double *w, double
                     wsw[c] = -aw[c] + wsw[c] + buoy[c];
                 }
         /* integrate_all(im): level-n values re-weighted */
+#pragma omp parallel for schedule(static)
         for (int k = 1; k <= nz; k++)
             for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) {
                 tu[c] = wsu[c] + b_lm * tu[c];
@@ -2177,6 +2289,7 @@ int mo_step(const mo_grid *g, int ntime, double *u, double *v, double *w, double
                 mv[c] = v2[c] * P1(g->den0, k) + a_lm * dt0 * tv[c];
                 mw[c] = 1. * (w2[c] * P1(g->avden0, k) + a_lm * dt0 * tw[c]);
             }
+#pragma omp parallel for schedule(static)
         for (size_t c = 0; c < nc; c++) {
             td[c] = wsd[c] + b_lm * td[c];
             for (int s = 0; s < nsc; s++) ts[s][c] = wss[s][c] + b_lm * ts[s][c];
@@ -2193,14 +2306,17 @@ int mo_step(const mo_grid *g, int ntime, double *u, double *v, double *w, double
         }
     }
     /* get_velocities, get_scalars, update_prognostic BCs */
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= nz; k++)
         for (size_t c = (size_t)(k - 1) * pl; c < (size_t)k * pl; c++) {
             u[c] = mu[c] / P1(g->den0, k);
             v[c] = mv[c] / P1(g->den0, k);
             w[c] = mw[c] / P1(g->avden0, k);
         }
-    for (int s = 0; s < nsc; s++)
+    for (int s = 0; s < nsc; s++) {
+#pragma omp parallel for schedule(static)
         for (size_t c = 0; c < nc; c++) scal[s][c] = scal[s][c] / dens[c];
+    }
     windbc(g, u, v, w);
     mo_statebc(g, p);
     mo_statebc(g, dens);
