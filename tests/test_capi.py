@@ -29,6 +29,13 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_integration_guide_binds_every_declared_symbol():
+    """Every entry point of include/*.h has its binding or usage written in INTEGRATION.md."""
+    guide = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    missing = [n for n in _declared() if not re.search(rf"\b{n}\b", guide)]
+    assert not missing, missing
+
+
 def test_error_strings():
     L = _lib.lib()
     for code in range(8):
