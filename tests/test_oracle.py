@@ -191,9 +191,11 @@ def _tridiag_apply(d, y):
     return out
 
 
-def test_fft_solve_manufactured_solution():
-    """fft_solve inverts the reference's spectral operator: build rhs from a known solution."""
-    d = config.cumulus_domain(16, 12, 20)
+@pytest.mark.parametrize("maxx,maxy,nz", [(16, 12, 20), (20, 30, 12), (10, 18, 9), (8, 50, 15)])
+def test_fft_solve_manufactured_solution(maxx, maxy, nz):
+    """fft_solve inverts the reference's spectral operator: build rhs from a known solution.
+    Grids with radix 2, 3 and 5 factors (the sizes the product accepts), non-square, odd nz."""
+    d = config.cumulus_domain(maxx, maxy, nz)
     orc = O.Oracle(d)
     rng = np.random.default_rng(5)
     sol = rng.normal(size=(d.nz, d.maxy, d.maxx))
