@@ -29,6 +29,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -223,9 +224,22 @@ def sgs_label(args):
     return {"none": "off", "smagorinsky": "Smagorinsky-Lilly, pran=-0.4, zdec=2400 m, surface fluxes"}[args.sgs]
 
 
-def cpu_reference(args, d_full, scheme, nsamp_steps=1, omp=True):
+def timed_cpu_sample(orc, st, seconds):
+    """One timed warm-up step (page faults, OpenMP pool), then as many steps as fill about
+    `seconds` of wall time (1 to 20), timed as one call: returns (steps, elapsed s)."""
+    t0 = time.perf_counter()
+    orc.stepping(st, nsteps=1, ntime0=1)
+    warm = time.perf_counter() - t0
+    n = int(min(20, max(1, math.ceil(seconds / max(warm, 1e-3)))))
+    t0 = time.perf_counter()
+    orc.stepping(st, nsteps=n, ntime0=1)
+    return n, time.perf_counter() - t0
+
+
+def cpu_reference(args, d_full, scheme, omp=True):
     """The reference's algorithm timed on the host cores: the CPU restatement, bounded
-    sample = a horizontally reduced domain with the same dz profile, spacing and fields."""
+    sample = a horizontally reduced domain with the same dz profile, spacing and fields.
+    The sample runs as many steps as fill about args.cpu_seconds of wall time."""
     from fdd3260_b200 import config
     from oracle import oracle as O
     mx = args.cpu_sample_xy
@@ -233,13 +247,11 @@ def cpu_reference(args, d_full, scheme, nsamp_steps=1, omp=True):
     d.sgs = bench_sgs(args, d)
     st = config.cumulus_state(d, seed=1000, n_extra=3)
     orc = O.Oracle(d, omp=omp)
-    orc.stepping(st, nsteps=1, ntime0=1)   # warm-up (page faults, OpenMP pool)
-    t0 = time.perf_counter()
-    orc.stepping(st, nsteps=nsamp_steps, ntime0=1)
-    dt = time.perf_counter() - t0
+    nsamp_steps, dt = timed_cpu_sample(orc, st, args.cpu_seconds)
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)) if omp else 1
     val = d.cells * nsamp_steps / dt / 1e6
-    return val, cores, f"{mx}x{mx}x{d.nz} interior cells, {nsamp_steps} step(s), same dz/dt/fields as the workload"
+    return val, cores, (f"{mx}x{mx}x{d.nz} interior cells, {nsamp_steps} step(s) in {dt:.1f} s, same dz/dt/fields "
+                        f"as the workload")
 
 
 def main():
@@ -252,6 +264,8 @@ def main():
     ap.add_argument("--maxx", type=int, default=512)
     ap.add_argument("--nz", type=int, default=256)
     ap.add_argument("--cpu-sample-xy", type=int, default=64)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0,
+                    help="wall time the CPU sample is sized to (steps of the 64x64xnz sample, 1 to 20)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
@@ -303,10 +317,10 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        val, cores, sample = cpu_reference(args, d, args.scheme, nsamp_steps=1)
+        val, cores, sample = cpu_reference(args, d, args.scheme)
         vals = [val]
         for _ in range(max(0, min(args.steps, 2) - 1)):
-            vals.append(cpu_reference(args, d, args.scheme, nsamp_steps=1)[0])
+            vals.append(cpu_reference(args, d, args.scheme)[0])
         v = statistics.median(vals)
         line = {"impl": "reference", "metric": metric, "value": v, "unit": "Mcell-updates/s", "n_gpus": ws,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": d.cells / v / 1e3,
@@ -368,7 +382,7 @@ def main():
     cpu = None
     if rank == 0 and not args.skip_cpu:
         try:
-            v, cores, sample = cpu_reference(args, d, args.scheme, nsamp_steps=1)
+            v, cores, sample = cpu_reference(args, d, args.scheme)
             cpu = {"value": v, "unit": "Mcell-updates/s", "cores": cores, "kind": "port", "sample": sample}
         except Exception as e:  # pragma: no cover
             cpu = {"value": None, "unit": "Mcell-updates/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
@@ -486,13 +500,10 @@ def run_ensemble(args, ws, rank, local):
         sp = min(specs, key=lambda q: q.cells)
         d, st = E.member_problem(sp)
         orc = O.Oracle(d, omp=True)
-        orc.stepping(st, nsteps=1, ntime0=1)
-        t0 = time.perf_counter()
-        orc.stepping(st, nsteps=1, ntime0=1)
-        dt = time.perf_counter() - t0
+        n, dt = timed_cpu_sample(orc, st, args.cpu_seconds)
         cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-        cpu = {"value": d.cells / dt / 1e6, "unit": "Mcell-updates/s", "cores": cores, "kind": "port",
-               "sample": f"smallest member {d.maxx}x{d.maxy}x{d.nz}, 1 step"}
+        cpu = {"value": d.cells * n / dt / 1e6, "unit": "Mcell-updates/s", "cores": cores, "kind": "port",
+               "sample": f"smallest member {d.maxx}x{d.maxy}x{d.nz}, {n} step(s) in {dt:.1f} s"}
     for m in members:
         m.close()
     if rank == 0:
