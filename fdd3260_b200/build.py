@@ -105,7 +105,7 @@ def build_oracle(verbose: bool = False) -> str:
         _run(["gcc", "-O2", "-fno-fast-math", "-ffp-contract=off", "-fPIC", "-shared", "-o", out, src, "-lm"], verbose)
     out_omp = os.path.join(ORACLE_DIR, "libmimica_oracle_omp.so")
     if _stale(out_omp, [src, hdr]):
-        # the timed CPU baseline: OpenMP, and the table-driven FFT (MO_FAST_FFT); built here and run on
+        # the timed CPU baseline: OpenMP, the table-driven FFT and a heap that keeps freed fields (MO_FAST_FFT); built here and run on
         # another host, so the instruction set is a portable x86-64-v3 (AVX2), not this host's
         _run(["gcc", "-O3", "-march=x86-64-v3", "-fno-fast-math", "-ffp-contract=off", "-fopenmp", "-DMO_FAST_FFT", "-fPIC",
               "-shared", "-o", out_omp, src, "-lm"], verbose)
