@@ -390,7 +390,7 @@ def main():
     if rank == 0:
         head = res[forms[0]]
         line = {"metric": metric, "value": head["value"], "unit": "Mcell-updates/s", "n_gpus": ws, "steps": args.steps,
-                "warmup": args.warmup + 2, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64" if forms[0] == "fp64" else "f32 fluxes/spectra, f64 state",
                 "data": "synthetic (seeded PCG64)", "config": cfg,
                 "clocks": head["clocks"], "gpu_launches": head["gpu_launches"],
@@ -440,11 +440,12 @@ def run_ensemble(args, ws, rank, local):
         states.append(st)
     ens = E.Ensemble(members)
     plans = ens.autotune(reps=3) if args.autotune == "on" else {}
-    ens.step(args.warmup, ntime0=1)
-    ens.step(2, ntime0=1 + args.warmup)   # both pair graphs recorded before timing
+    # W warm-up steps, the last pair at the timed steps' parity (its graph is the one timed)
+    ens.step(args.warmup - 2, ntime0=1)
+    ens.step(2, ntime0=args.warmup - 1)
     dist_barrier(ws)
     with ClockSampler(local) as clk:
-        t_ms = ens.time_steps(args.steps, ntime0=3 + args.warmup)
+        t_ms = ens.time_steps(args.steps, ntime0=1 + args.warmup)
     t_ms = dist_max(t_ms, ws)
     value = total_cells * args.steps / (t_ms / 1e3) / 1e6
     # roofline of the dominant kernel, from an eager profiled pass of this rank's largest member
@@ -452,7 +453,7 @@ def run_ensemble(args, ws, rank, local):
     mb = members[big]
     L = mb._L
     L.mg_profile_enable(mb._h, 1)
-    mb.stepping(2, ntime0=3 + args.warmup + args.steps)
+    mb.stepping(2, ntime0=1 + args.warmup + args.steps)
     buf = C.create_string_buffer(8192)
     L.mg_profile_report(mb._h, buf, 8192)
     L.mg_profile_enable(mb._h, 0)
@@ -508,7 +509,7 @@ def run_ensemble(args, ws, rank, local):
         m.close()
     if rank == 0:
         line = {"metric": "Mcell-updates/s per integrator step (2-stage Heun + projection), batched ensemble",
-                "value": value, "unit": "Mcell-updates/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup + 2,
+                "value": value, "unit": "Mcell-updates/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "strong",
                 "vs_baseline": None, "dtype": "f64" if form == "fp64" else "f32 fluxes/spectra, f64 state",
                 "data": "synthetic (seeded PCG64)",
@@ -595,16 +596,17 @@ def field_errors(out, ref, st0, nsteps: int) -> dict:
 def time_form(args, m, d, st, use_graph, ws, local) -> dict:
     L = m._L
     plan = m.autotune(reps=3) if args.autotune == "on" else dict(m.tune_get(), source="default")
-    m.stepping(args.warmup, ntime0=1, graph=use_graph)
-    # one more pair at the timed region's step parity: both pair graphs (the momentum
-    # direction order alternates with the step's parity) are recorded before timing
-    m.stepping(2, ntime0=1 + args.warmup, graph=use_graph)
+    # W warm-up steps; the last two form a pair at the timed region's step parity, so the
+    # pair graph the timed steps replay (the momentum direction order alternates with the
+    # step's parity) is recorded inside the warm-up
+    m.stepping(args.warmup - 2, ntime0=1, graph=use_graph)
+    m.stepping(2, ntime0=args.warmup - 1, graph=use_graph)
     m.synchronize()
     # timed region (device time, CUDA events on the library stream), clocks sampled meanwhile
     dist_barrier(ws)
     ms = C.c_double(0.0)
     with ClockSampler(local) as clk:
-        rc = L.mg_time_steps(m._h, args.steps, 3 + args.warmup, 1 if use_graph else 0, C.byref(ms))
+        rc = L.mg_time_steps(m._h, args.steps, 1 + args.warmup, 1 if use_graph else 0, C.byref(ms))
     if rc:
         raise RuntimeError(f"mg_time_steps failed: {rc}")
     t_ms = dist_max(ms.value, ws)
@@ -613,7 +615,7 @@ def time_form(args, m, d, st, use_graph, ws, local) -> dict:
 
     # per-kernel device times (separate eager pass, events around each launch group)
     L.mg_profile_enable(m._h, 1)
-    m.stepping(2, ntime0=3 + args.warmup + args.steps)
+    m.stepping(2, ntime0=1 + args.warmup + args.steps)
     buf = C.create_string_buffer(8192)
     L.mg_profile_report(m._h, buf, 8192)
     L.mg_profile_enable(m._h, 0)
