@@ -8,6 +8,15 @@
  * without FMA contraction, reproduce them bit for bit.  Build with
  * -O2 -fno-fast-math -ffp-contract=off.
  *
+ * Parity status: "parity unpinned" against the Fortran routines, which cannot be
+ * compiled here and have no golden vectors for this path; the FFT is pinned against
+ * the reference's own KISS FFT (src/fftmpi/src/kissfft.h) and its committed vectors.
+ *
+ * The timed CPU baseline is a second build of this file with -fopenmp and
+ * -DMO_FAST_FFT: thread-parallel loops (each cell's arithmetic unchanged), a
+ * tabulated-twiddle FFT (agreeing with the parity build's to ~5e-16 relative) and a
+ * heap that keeps freed fields.  The parity build ignores both.
+ *
  * Documented deviations from the reference (each one a choice the reference
  * leaves undefined):
  *  - advsz_weno interior-face loop starts at k=2: the reference loop

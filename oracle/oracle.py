@@ -7,7 +7,11 @@ Parity status: the Fortran reference cannot be compiled here and ships no golden
 vectors for this path, so the restatement is "parity unpinned" against a
 reference binary; its FFT is pinned against the reference's own KISS FFT
 (oracle/_ref/libkissref.so, built from src/fftmpi/src/kissfft.h when the
-reference tree is present) and numpy.fft.
+reference tree is present; its outputs are committed in tests/golden/kiss_fft.npz)
+and numpy.fft.
+
+Oracle(d) loads the parity build (libmimica_oracle.so); Oracle(d, omp=True) loads the
+timed OpenMP build (libmimica_oracle_omp.so) that bench.py's CPU legs time.
 """
 from __future__ import annotations
 
