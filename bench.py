@@ -463,8 +463,11 @@ def run_ensemble(args, ws, rank, local):
     dom = max((k for k in kern if k in ab), key=lambda k: kern[k][1])
     avg_ms = kern[dom][1] / kern[dom][0]
     achieved = ab[dom] * mb.domain.cells / (avg_ms / 1e3) / 1e9
-    measured = args.scheme == "weno" and len(st.scal) == 5 and d.sgs is None and dom in MEASURED_TRAFFIC_PER_CELL
-    traffic = MEASURED_TRAFFIC_PER_CELL[dom] * d.cells if measured else None
+    # the traffic captures are of the 5-scalar cumulus workload; the profiled member's own
+    # field count and SGS setting decide whether they apply
+    measured = (args.scheme == "weno" and len(states[big].scal) == 5 and getattr(mb.domain, "sgs", None) is None
+                and dom in MEASURED_TRAFFIC_PER_CELL)
+    traffic = MEASURED_TRAFFIC_PER_CELL[dom] * mb.domain.cells if measured else None
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "traffic_unit": "bytes per launch",
             "traffic_source": TRAFFIC_SOURCE if measured else "no capture of this configuration",
