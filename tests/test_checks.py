@@ -2,7 +2,6 @@
 (mg_cfl_dt, host code) against a transcription of checkwind's advective branch, and the
 oracle's CFL / bounds reductions against known answers."""
 import ctypes as C
-import math
 
 import numpy as np
 import pytest

@@ -3,7 +3,6 @@ two-rank (gloo, CPU) path that shards members with no data-path collective."""
 import os
 import socket
 
-import numpy as np
 import pytest
 
 from fdd3260_b200 import ensemble as E

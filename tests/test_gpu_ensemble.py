@@ -3,7 +3,7 @@ members' streams) gives, bit for bit, what stepping every member alone gives."""
 import numpy as np
 import pytest
 
-from fdd3260_b200 import Mimica, _lib, config
+from fdd3260_b200 import Mimica, _lib
 from fdd3260_b200 import ensemble as E
 
 pytestmark = pytest.mark.gpu

@@ -13,7 +13,7 @@ import os
 import numpy as np
 import pytest
 
-from fdd3260_b200 import _lib, config
+from fdd3260_b200 import config
 from oracle import oracle as O
 
 
