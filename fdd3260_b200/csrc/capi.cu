@@ -738,13 +738,11 @@ extern "C" int mg_step_graph(mg_ctx *c, int nsteps, int ntime0, double *maxdiv, 
         if (rc) return rc;
     } else if (maxdiv || p1) {
         // diagnostics of the final state
-        int launches = 0;
         const DevGrid &G = c->G;
         if (maxdiv) {
             CKR(launch_maxdiv(G, c->pp, c->mA[0], c->mA[1], c->mA[2], c->stream));
             CKR(cudaMemcpyAsync(maxdiv, pressure_maxdiv_dev(c->pp), 8, cudaMemcpyDeviceToHost, c->stream));
         }
-        (void)launches;
         if (p1) memset(p1, 0, sizeof(double) * G.nz);
         CKR(cudaStreamSynchronize(c->stream));
     }
