@@ -42,16 +42,24 @@ def key(maxx: int, maxy: int, nz: int, precision: int, nscal: int) -> str:
 
 
 def load(path: str) -> dict:
+    """The wisdom file's plans; a missing or unreadable file is an empty cache."""
     if not path or not os.path.exists(path):
         return {}
-    with open(path) as f:
-        return json.load(f)
+    try:
+        with open(path) as f:
+            w = json.load(f)
+    except (OSError, ValueError):
+        return {}
+    return w if isinstance(w, dict) else {}
 
 
 def store(path: str, k: str, plan: dict) -> None:
+    """Add one plan. The file is replaced atomically through a temporary file of this
+    process, so concurrent writers (ranks tuning their own grids) never leave a partial
+    file; one writer's entry can be lost to another's, and is then tuned again."""
     w = load(path)
     w[k] = {f: plan[f] for f in FIELDS}
-    tmp = path + ".tmp"
+    tmp = f"{path}.{os.getpid()}.tmp"
     with open(tmp, "w") as f:
         json.dump(w, f, indent=1, sort_keys=True)
     os.replace(tmp, path)

@@ -1,6 +1,8 @@
 """CPU checks of the projection's plan space: the radix sequences the autotuner tries
 (host code of the library, no device needed) and the wisdom file."""
+import json
 import math
+import os
 
 import pytest
 
@@ -47,3 +49,37 @@ def test_wisdom_round_trip(tmp_path):
     assert tune.key(512, 96, 64, _lib.MG_PREC_FP64, 5) != tune.key(512, 96, 64, _lib.MG_PREC_FP64, 2)
     with pytest.raises(ValueError):
         tune.from_dict(dict(plan, x_radix=[]))
+
+
+def _store_many(path, wid, n):
+    from fdd3260_b200 import tune as T
+    plan = {"x_radix": [4, 4, 2], "y_radix": [8, 4], "x_threads": 16, "y_threads": 64, "tri_block": 128,
+            "k1_segments": wid}
+    for i in range(n):
+        T.store(path, f"writer{wid}-{i}", plan)
+
+
+def test_wisdom_concurrent_writers_leave_a_valid_file(tmp_path):
+    """Ranks that tune at the same time write the same wisdom file: every replacement is
+    a complete file (entries may be lost to another writer, never half-written)."""
+    import multiprocessing as mp
+    path = str(tmp_path / "wisdom.json")
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_store_many, args=(path, w, 25)) for w in range(4)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    with open(path) as f:
+        w = json.load(f)
+    assert w and all(k.startswith("writer") for k in w)
+    assert not [f for f in os.listdir(tmp_path) if f.endswith(".tmp")]
+
+
+def test_wisdom_unreadable_file_is_an_empty_cache(tmp_path):
+    path = tmp_path / "wisdom.json"
+    path.write_text('{"truncated": ')
+    assert tune.load(str(path)) == {}
+    path.write_text("[1, 2]")
+    assert tune.load(str(path)) == {}
