@@ -157,12 +157,21 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+PAGEABLE_FALLBACKS = []   # shapes for which page-locked allocation failed (reported in e2e)
+
+
+def host_buffers() -> str:
+    return "page-locked" if not PAGEABLE_FALLBACKS else f"{len(PAGEABLE_FALLBACKS)} pageable (cudaMallocHost failed)"
+
+
 def pinned_like(shape):
-    """numpy array in page-locked host memory (cudaMallocHost)."""
+    """numpy array in page-locked host memory (cudaMallocHost); pageable if that fails,
+    which the e2e object reports."""
     rt = C.CDLL("libcudart.so")
     n = int(np.prod(shape)) * 8
     p = C.c_void_p()
     if rt.cudaMallocHost(C.byref(p), C.c_size_t(n)) != 0:
+        PAGEABLE_FALLBACKS.append(tuple(shape))
         return np.zeros(shape)
     buf = (C.c_double * int(np.prod(shape))).from_address(p.value)
     return np.frombuffer(buf, dtype=np.float64).reshape(shape)
@@ -524,7 +533,8 @@ def run_ensemble(args, ws, rank, local):
                 "clocks": clk.summary(), "gpu_launches": launches * args.steps,
                 "e2e": {"value": total_cells * args.e2e_steps / e2e_s / 1e6, "unit": "Mcell-updates/s",
                         "h2d_bytes_per_step": nbytes_all, "d2h_bytes_per_step": nbytes_all,
-                        "timing": "host wall clock, synchronised, page-locked buffers"},
+                        "timing": "host wall clock, synchronised, page-locked buffers",
+                        "host_buffers": host_buffers()},
                 "roofline": roof, "cpu_baseline": cpu, "graph": True,
                 "projection_plans": {k: {f: v[f] for f in ("x_radix", "y_radix", "x_threads", "y_threads", "tri_block",
                                                            "ms_default", "ms_tuned") if f in v}
@@ -670,7 +680,8 @@ def e2e_leg(args, m, d, st, ws) -> dict:
     nbytes = (5 + len(st.scal)) * d.nx * d.ny * d.nz * 8
     return {"e2e": {"value": d.cells * args.e2e_steps * ws / e2e_s / 1e6, "unit": "Mcell-updates/s",
                     "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-                    "timing": "host wall clock, synchronised, one set of page-locked buffers for upload and download"}}
+                    "timing": "host wall clock, synchronised, one set of page-locked buffers for upload and download",
+                    "host_buffers": host_buffers()}}
 
 
 if __name__ == "__main__":
