@@ -245,6 +245,17 @@ def timed_cpu_sample(orc, st, seconds):
     return n, time.perf_counter() - t0
 
 
+def cpu_domain(args, mx, nz, scheme):
+    """The workload's domain at a reduced horizontal size, built entirely on the CPU: the grid
+    metrics and base state come from the oracle's restatement of the reference's init
+    routines, so this path never loads the CUDA library."""
+    from fdd3260_b200 import config
+    from oracle import oracle as O
+    d = config.cumulus_domain(mx, mx, nz, scheme=scheme, init=O.Init(omp=True), muscl_limiter=args.limiter)
+    d.sgs = bench_sgs(args, d)
+    return d
+
+
 def cpu_reference(args, d_full, scheme, omp=True):
     """The reference's algorithm timed on the host cores: the CPU restatement, bounded
     sample = a horizontally reduced domain with the same dz profile, spacing and fields.
@@ -252,8 +263,7 @@ def cpu_reference(args, d_full, scheme, omp=True):
     from fdd3260_b200 import config
     from oracle import oracle as O
     mx = args.cpu_sample_xy
-    d = config.cumulus_domain(mx, mx, d_full.nz, scheme=scheme)
-    d.sgs = bench_sgs(args, d)
+    d = cpu_domain(args, mx, d_full.nz, scheme)
     st = config.cumulus_state(d, seed=1000, n_extra=3)
     orc = O.Oracle(d, omp=omp)
     nsamp_steps, dt = timed_cpu_sample(orc, st, args.cpu_seconds)
@@ -261,6 +271,47 @@ def cpu_reference(args, d_full, scheme, omp=True):
     val = d.cells * nsamp_steps / dt / 1e6
     return val, cores, (f"{mx}x{mx}x{d.nz} interior cells, {nsamp_steps} step(s) in {dt:.1f} s, same dz/dt/fields "
                         f"as the workload")
+
+
+def reference_arm(args, cfg, metric, ws):
+    """--impl reference: the reference's algorithm (the oracle's timed OpenMP build; the
+    Fortran reference cannot be built on these hosts) on all host cores, exactly W warm-up
+    and K timed integrator steps.  Each step is one step of a bounded sample of the workload:
+    the same dz profile, spacing, fields and scheme on a horizontally reduced domain, whose
+    size is halved from --ref-sample-xy until W + K steps fit in about --ref-seconds.
+    ms_per_step is the sample's own time per step.  Nothing here loads the CUDA library."""
+    from fdd3260_b200 import config
+    from oracle import oracle as O
+    mx = args.ref_sample_xy
+    while True:
+        d = cpu_domain(args, mx, args.nz, args.scheme)
+        st = config.cumulus_state(d, seed=1000, n_extra=3)
+        orc = O.Oracle(d, omp=True)
+        t0 = time.perf_counter()
+        st, _, _ = orc.stepping(st, nsteps=1, ntime0=1)      # warm-up step 1 (page faults, thread pool)
+        one = time.perf_counter() - t0
+        if one * (args.warmup + args.steps) <= args.ref_seconds or mx <= 32:
+            break
+        mx //= 2
+    if args.warmup > 1:
+        st, _, _ = orc.stepping(st, nsteps=args.warmup - 1, ntime0=2)
+    t0 = time.perf_counter()
+    orc.stepping(st, nsteps=args.steps, ntime0=1 + args.warmup)
+    dt = time.perf_counter() - t0
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    v = d.cells * args.steps / dt / 1e6
+    sample = (f"bounded sample of the workload: {mx}x{mx}x{d.nz} interior cells ({d.cells} cells, "
+              f"{d.cells / cfg['interior_cells']:.4f} of the workload) with the same dz profile, spacing, fields and "
+              f"scheme; {args.warmup} warm-up + {args.steps} timed steps, {dt:.1f} s timed; ms_per_step is per step of "
+              f"the sample")
+    line = {"impl": "reference", "metric": metric, "value": v, "unit": "Mcell-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded PCG64)", "config": cfg,
+            "sample": {"maxx": mx, "maxy": mx, "nz": d.nz, "cells": d.cells, "reduced_size": mx != args.maxx},
+            "cpu_baseline": {"value": v, "unit": "Mcell-updates/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -272,7 +323,12 @@ def main():
     ap.add_argument("--scheme", default="weno", choices=["weno", "ppm", "muscl", "lw", "quick"])
     ap.add_argument("--maxx", type=int, default=512)
     ap.add_argument("--nz", type=int, default=256)
+    ap.add_argument("--limiter", default="minmod", choices=["minmod", "VL", "MC", "default"],
+                    help="MUSCL limiter (the reference's muscllimiter; module default minmod)")
     ap.add_argument("--cpu-sample-xy", type=int, default=64)
+    ap.add_argument("--ref-sample-xy", type=int, default=256,
+                    help="--impl reference: horizontal size of the sample (halved until W+K steps fit --ref-seconds)")
+    ap.add_argument("--ref-seconds", type=float, default=150.0)
     ap.add_argument("--cpu-seconds", type=float, default=10.0,
                     help="wall time the CPU sample is sized to (steps of the 64x64xnz sample, 1 to 20)")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -293,7 +349,7 @@ def main():
                     help="pick the projection plan and K1's segments by timing before the timed steps")
     ap.add_argument("--traj-steps", type=int, default=200, help="steps of the trajectory adjoint leg (0: off)")
     ap.add_argument("--traj-ckpt", type=int, default=25)
-    ap.add_argument("--err-steps", type=int, default=10,
+    ap.add_argument("--err-steps", type=int, default=50,
                     help="steps of the accuracy leg (mixed vs FP64 fields from the same initial state)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -308,37 +364,26 @@ def main():
         ws, rank, local = dist_init()
     if args.workload == "ensemble":
         return run_ensemble(args, ws, rank, local)
-    from fdd3260_b200 import Mimica, config
-    d = config.cumulus_domain(args.maxx, args.maxx, args.nz, scheme=args.scheme)
-    d.sgs = bench_sgs(args, d)
-    from fdd3260_b200 import _lib
     metric = "Mcell-updates/s per integrator step (2-stage Heun + projection)"
+    lim = f" ({args.limiter} limiter)" if args.scheme == "muscl" else ""
     cfg = {"workload": f"shallow-cumulus domain {args.maxx}x{args.maxx}x{args.nz}, dx=dy=25 m, stretched dz 10->100 m, "
-                       f"3 momentum + density + 5 scalars, {args.scheme.upper()} (reference scheme), FD4 momentum, "
+                       f"3 momentum + density + 5 scalars, {args.scheme.upper()}{lim} (reference scheme), FD4 momentum, "
                        f"dt=1 s, nsubp=1",
            "fields": "theta_l 298->310 K, qt 17->4 g/kg, qr/nr/aerosol smooth decreasing profiles; "
                      "seeded Gaussian perturbations below 500 m; u=-8+N(0,0.5), v=N(0,0.5) m/s",
            "form": {"both": "plain FP64 (headline) + mixed", "fp64": "plain FP64",
                     "mixed": "mixed (FP32 stencils, fluxes and spectra; FP64 state)"}[args.form],
-           "scheme": args.scheme, "sgs": sgs_label(args), "interior_cells": d.cells,
+           "scheme": args.scheme, "sgs": sgs_label(args), "interior_cells": args.maxx * args.maxx * args.nz,
            "l2": "inputs larger than L2 (~16 GB working set)", "parallelism": f"replicas x{ws}"}
+    if args.scheme == "muscl":
+        cfg["limiter"] = args.limiter
 
     if args.impl == "reference":
-        if rank != 0:
-            return
-        val, cores, sample = cpu_reference(args, d, args.scheme)
-        vals = [val]
-        for _ in range(max(0, min(args.steps, 2) - 1)):
-            vals.append(cpu_reference(args, d, args.scheme)[0])
-        v = statistics.median(vals)
-        line = {"impl": "reference", "metric": metric, "value": v, "unit": "Mcell-updates/s", "n_gpus": ws,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": d.cells / v / 1e3,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded)", "config": cfg,
-                "cpu_baseline": {"value": v, "unit": "Mcell-updates/s", "cores": cores, "kind": "port", "sample": sample},
-                "e2e": {"value": v, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return
+        return reference_arm(args, cfg, metric, ws)
+
+    from fdd3260_b200 import Mimica, _lib, config
+    d = config.cumulus_domain(args.maxx, args.maxx, args.nz, scheme=args.scheme, muscl_limiter=args.limiter)
+    d.sgs = bench_sgs(args, d)
 
     st = config.cumulus_state(d, seed=1000 + rank, n_extra=3)
     use_graph = not args.no_graph
@@ -533,7 +578,7 @@ def run_ensemble(args, ws, rank, local):
                 "clocks": clk.summary(), "gpu_launches": launches * args.steps,
                 "e2e": {"value": total_cells * args.e2e_steps / e2e_s / 1e6, "unit": "Mcell-updates/s",
                         "h2d_bytes_per_step": nbytes_all, "d2h_bytes_per_step": nbytes_all,
-                        "timing": "host wall clock, synchronised, page-locked buffers",
+                        "timing": f"host wall clock, synchronised, host buffers: {host_buffers()}",
                         "host_buffers": host_buffers()},
                 "roofline": roof, "cpu_baseline": cpu, "graph": True,
                 "projection_plans": {k: {f: v[f] for f in ("x_radix", "y_radix", "x_threads", "y_threads", "tri_block",
@@ -680,7 +725,8 @@ def e2e_leg(args, m, d, st, ws) -> dict:
     nbytes = (5 + len(st.scal)) * d.nx * d.ny * d.nz * 8
     return {"e2e": {"value": d.cells * args.e2e_steps * ws / e2e_s / 1e6, "unit": "Mcell-updates/s",
                     "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-                    "timing": "host wall clock, synchronised, one set of page-locked buffers for upload and download",
+                    "timing": "host wall clock, synchronised, one set of host buffers for upload and download "
+                              f"({host_buffers()})",
                     "host_buffers": host_buffers()}}
 
 

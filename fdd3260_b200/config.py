@@ -122,16 +122,28 @@ class Domain:
     def cells(self) -> int:
         return self.maxx * self.maxy * self.nz
 
-    def finish(self) -> "Domain":
-        L = _lib.lib()
+    def finish(self, init=None) -> "Domain":
+        """Fill the grid metrics and the base state.
+
+        ``init`` is None for the library's own init routines (mg_grid_metrics,
+        mg_base_state), or an object with ``grid_metrics(nz, dz, fdz0, dzw, dz1w, dz1)``
+        and ``base_state(nz, dz, psurf, fdz0, dz1, pt0, qv0, p0, den0, avden0, stab0)``
+        methods taking numpy arrays, for a caller that must not load the CUDA library
+        (a CPU-only timing of another implementation)."""
         nz = self.nz
         self.fdz0 = np.ascontiguousarray(self.fdz0, dtype=np.float64)
         self.pt0 = np.ascontiguousarray(self.pt0, dtype=np.float64)
         self.qv0 = np.ascontiguousarray(self.qv0, dtype=np.float64)
         self.dzw, self.dz1w, self.dz1 = (np.zeros(nz) for _ in range(3))
+        self.p0, self.den0, self.avden0, self.stab0 = (np.zeros(nz) for _ in range(4))
+        if init is not None:
+            init.grid_metrics(nz, self.dz, self.fdz0, self.dzw, self.dz1w, self.dz1)
+            init.base_state(nz, self.dz, self.psurf, self.fdz0, self.dz1, self.pt0, self.qv0, self.p0, self.den0,
+                            self.avden0, self.stab0)
+            return self
+        L = _lib.lib()
         _lib.check(L.mg_grid_metrics(nz, self.dz, _lib.ptr(self.fdz0), _lib.ptr(self.dzw), _lib.ptr(self.dz1w),
                                      _lib.ptr(self.dz1)), "mg_grid_metrics")
-        self.p0, self.den0, self.avden0, self.stab0 = (np.zeros(nz) for _ in range(4))
         _lib.check(L.mg_base_state(nz, self.dz, self.psurf, _lib.ptr(self.fdz0), _lib.ptr(self.dz1),
                                    _lib.ptr(self.pt0), _lib.ptr(self.qv0), _lib.ptr(self.p0), _lib.ptr(self.den0),
                                    _lib.ptr(self.avden0), _lib.ptr(self.stab0)), "mg_base_state")
@@ -252,10 +264,10 @@ def tanh_levels(nz: int, dz_bottom: float, dz_top: float, width: float = 0.18) -
     return dz_bottom + (dz_top - dz_bottom) * 0.5 * (1.0 + np.tanh((s - 0.5) / width))
 
 
-def cumulus_domain(maxx=512, maxy=512, nz=256, dx=25.0, dy=25.0, dt0=1.0, scheme="weno", **kw) -> Domain:
+def cumulus_domain(maxx=512, maxy=512, nz=256, dx=25.0, dy=25.0, dt0=1.0, scheme="weno", init=None, **kw) -> Domain:
     """Shallow-cumulus-like domain: stretched grid, 10 m at the surface to 100 m at the top.
     Thicknesses enter through fdz = thickness/dz as the grid-file path
-    (src/TOOLS/define_grid.f90:143-172) would produce them."""
+    (src/TOOLS/define_grid.f90:143-172) would produce them.  ``init``: see Domain.finish."""
     dz = 10.0
     thick = tanh_levels(nz, 10.0, 100.0)
     fdz = thick / dz
@@ -265,7 +277,7 @@ def cumulus_domain(maxx=512, maxy=512, nz=256, dx=25.0, dy=25.0, dt0=1.0, scheme
     qt = np.interp(zc, [0.0, 500.0, 1500.0, zt], [17e-3, 16e-3, 8e-3, 4e-3])
     d = Domain(maxx=maxx, maxy=maxy, nz=nz, dx=dx, dy=dy, dz=dz, dt0=dt0, fdz0=fdz, pt0=pt0, qv0=qt,
                scal_adv=scheme, **kw)
-    return d.finish()
+    return d.finish(init)
 
 
 def cumulus_state(d: Domain, seed: int = 1000, n_extra: int = 3, lognormal_extras: bool = False) -> State:

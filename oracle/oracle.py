@@ -103,6 +103,22 @@ def P(a):
     return a.ctypes.data_as(_dp)
 
 
+class Init:
+    """The oracle's restatement of the reference's init routines, in the form
+    config.Domain.finish(init=...) takes: grid metrics (define_grid.f90:179-187) and the
+    anelastic base state (initial.f90:473-558).  Used where a domain must be built without
+    loading the CUDA library (bench.py's CPU reference arm)."""
+
+    def __init__(self, omp: bool = False):
+        self.L = load(omp)
+
+    def grid_metrics(self, nz, dz, fdz0, dzw, dz1w, dz1):
+        self.L.mo_grid_metrics(nz, dz, P(fdz0), P(dzw), P(dz1w), P(dz1))
+
+    def base_state(self, nz, dz, psurf, fdz0, dz1, pt0, qv0, p0, den0, avden0, stab0):
+        self.L.mo_base_state(nz, dz, psurf, P(fdz0), P(dz1), P(pt0), P(qv0), P(p0), P(den0), P(avden0), P(stab0))
+
+
 class Oracle:
     """Oracle bound to one domain (config.Domain)."""
 
