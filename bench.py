@@ -349,6 +349,8 @@ def main():
                     help="pick the projection plan and K1's segments by timing before the timed steps")
     ap.add_argument("--traj-steps", type=int, default=200, help="steps of the trajectory adjoint leg (0: off)")
     ap.add_argument("--traj-ckpt", type=int, default=25)
+    ap.add_argument("--exact-nsubp", type=int, default=3,
+                    help="passes of the exact projection legs (fp64_exact, mixed_exact); 0 or 1: not run")
     ap.add_argument("--err-steps", type=int, default=50,
                     help="steps of the accuracy leg (mixed vs FP64 fields from the same initial state)")
     args = ap.parse_args()
@@ -389,22 +391,32 @@ def main():
     use_graph = not args.no_graph
     dev = local if ws > 1 else 0
     forms = ["fp64", "mixed"] if args.form == "both" else [args.form]
+    # the exact projection: the reference's own nsubp loop (pressure_solver.f90:100-111),
+    # each pass solving for the physical divergence of the corrected momentum (caldiv,
+    # gradients.f90:986-1052), run to exact_nsubp passes; in the mixed form every pass is an
+    # FP32 solve against an FP64 divergence, with no refinement against the Poisson operator.
+    # fp64_exact is only run for its fields (the reference for mixed_exact's error).
+    if args.form == "both" and args.exact_nsubp > 1 and args.err_steps > 0:
+        forms += ["fp64_exact", "mixed_exact"]
+    spec = {"fp64": (_lib.MG_PREC_FP64, 1, d.refine_iters), "mixed": (_lib.MG_PREC_MIXED, 1, d.refine_iters),
+            "fp64_exact": (_lib.MG_PREC_FP64, args.exact_nsubp, 0),
+            "mixed_exact": (_lib.MG_PREC_MIXED, args.exact_nsubp, 0)}
     res = {}
-    ref_fields = None
+    ref = {}
     for form in forms:
-        d.precision = _lib.MG_PREC_MIXED if form == "mixed" else _lib.MG_PREC_FP64
+        d.precision, d.nsubp, d.refine_iters = spec[form]
         m = Mimica(d, nscal=len(st.scal), iqt=st.iqt, device=dev)
         r = {}
         # accuracy leg: err_steps steps from the initial state, fields downloaded; the mixed
         # form is compared with the plain FP64 form (bit-exact with the CPU restatement of
-        # the reference routines)
-        if args.err_steps > 0 and len(forms) == 2:
+        # the reference routines), the mixed exact form with the FP64 exact form
+        if args.err_steps > 0 and len(forms) >= 2:
             m.upload(st)
             md, _ = m.stepping(args.err_steps, ntime0=1, diagnostics=True, graph=use_graph)
             out = m.download()
             r["maxdiv"] = md
             if form == "fp64":
-                ref_fields = out
+                ref["fp64"] = out
                 # FP64 twin: the same run from u perturbed by 1e-9 relative (seeded).  The
                 # reference's WENO3 switch is discontinuous, so any perturbation of about
                 # this size flips faces and the trajectories separate along the flow's own
@@ -415,13 +427,20 @@ def main():
                 del tw
                 m.stepping(args.err_steps, ntime0=1, graph=use_graph)
                 twin = m.download()
-                r["twin_error"] = field_errors(twin, ref_fields, st, args.err_steps)
+                r["twin_error"] = field_errors(twin, ref["fp64"], st, args.err_steps)
                 del twin
+            elif form == "mixed":
+                r["error_vs_fp64"] = field_errors(out, ref["fp64"], st, args.err_steps)
+            elif form == "fp64_exact":
+                r["departure_from_one_pass"] = field_errors(out, ref["fp64"], st, args.err_steps)
+                ref["fp64_exact"] = out
             else:
-                r["error_vs_fp64"] = field_errors(out, ref_fields, st, args.err_steps)
+                r["error_vs_fp64_exact"] = field_errors(out, ref["fp64_exact"], st, args.err_steps)
+                r["departure_from_one_pass"] = field_errors(out, ref["fp64"], st, args.err_steps)
             del out
-        m.upload(st)
-        r.update(time_form(args, m, d, st, use_graph, ws, local))
+        if form != "fp64_exact":
+            m.upload(st)
+            r.update(time_form(args, m, d, st, use_graph, ws, local))
         if form == "fp64" and args.scheme == "weno":
             r["adjoint"] = adjoint_leg(m)
             if args.traj_steps > 0:
@@ -431,7 +450,8 @@ def main():
         r["device_bytes"] = m.device_bytes
         m.close()
         res[form] = r
-    ref_fields = None
+    ref = None
+    d.precision, d.nsubp, d.refine_iters = spec[forms[0]]
 
     cpu = None
     if rank == 0 and not args.skip_cpu:
@@ -464,6 +484,19 @@ def main():
                 line["mixed"]["fp64_twin_1e-9_error"] = head.get("twin_error")
                 line["mixed"]["maxdiv"] = mx["maxdiv"]
                 line["mixed"]["maxdiv_fp64"] = head.get("maxdiv")
+        if "mixed_exact" in res:
+            mx, fx = res["mixed_exact"], res["fp64_exact"]
+            line["mixed_exact"] = {
+                "form": f"exact projection: {args.exact_nsubp} passes of the reference's nsubp loop, each an FP32 "
+                        "solve for the FP64 physical divergence of the corrected momentum; FP32 stencils, fluxes "
+                        "and spectra, FP64 state",
+                "value": mx["value"], "unit": "Mcell-updates/s", "ms_per_step": mx["ms_per_step"],
+                "speedup_vs_fp64": mx["value"] / head["value"], "roofline": mx["roofline"],
+                "kernel_share": mx["kernel_share"], "clocks": mx["clocks"], "gpu_launches": mx["gpu_launches"],
+                "maxdiv": mx["maxdiv"], "maxdiv_fp64_exact": fx["maxdiv"],
+                "error_vs_fp64_exact": mx["error_vs_fp64_exact"],
+                "departure_from_one_pass": mx["departure_from_one_pass"],
+                "fp64_exact_departure_from_one_pass": fx["departure_from_one_pass"]}
         if "adjoint" in head:
             line["adjoint"] = head["adjoint"]
         print(json.dumps(line), flush=True)
