@@ -64,7 +64,7 @@ class MgCheckResult(C.Structure):
         ("dt0_old", C.c_double), ("dt0_new", C.c_double),
         ("es_min", C.c_double), ("es_max", C.c_double), ("qt_min", C.c_double), ("qt_max", C.c_double),
         ("es_min_ijk", C.c_int * 3), ("es_max_ijk", C.c_int * 3), ("qt_min_ijk", C.c_int * 3),
-        ("qt_max_ijk", C.c_int * 3),
+        ("qt_max_ijk", C.c_int * 3), ("nonfinite", C.c_int), ("nonfinite_ijk", C.c_int * 3),
     ]
 
 
@@ -131,6 +131,7 @@ def lib() -> C.CDLL:
         L.mg_checkall.argtypes = [vp, C.POINTER(MgCheckParams), C.POINTER(MgCheckResult)]
         L.mg_cfl_dt.argtypes = [C.POINTER(MgCheckParams), C.c_double, C.c_double, _dp, C.POINTER(C.c_int)]
         L.mg_set_dt.argtypes = [vp, C.c_double]
+        L.mg_selftest_wait.argtypes = [vp, C.c_longlong]
         L.mg_download_ksgs.argtypes = [vp, _dp]
         L.mg_traj_forward.argtypes = [vp, C.c_int, C.c_int]
         L.mg_traj_tl.argtypes = [vp, C.c_int, C.c_int, C.POINTER(_dp), C.POINTER(_dp)]

@@ -1046,7 +1046,7 @@ extern "C" int mg_checkall(mg_ctx *c, const mg_check_params *p, mg_check_result 
     const DevGrid &G = c->G;
     const int iqt = c->prm.iqt >= 0 ? 1 + c->prm.iqt : -1;
     CKR(launch_check(G, c->mA[0], c->mA[1], c->mA[2], c->sA[1], iqt >= 0 ? c->sA[iqt] : nullptr, c->chk, c->stream));
-    struct { double v; long long L; } h[5];
+    struct { double v; long long L; } h[6];
     const size_t off = check_scratch_bytes() - sizeof(h);
     CKR(cudaMemcpyAsync(h, (char *)c->chk + off, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
     CKR(cudaStreamSynchronize(c->stream));
@@ -1067,6 +1067,12 @@ extern "C" int mg_checkall(mg_ctx *c, const mg_check_params *p, mg_check_result 
         r->qt_min = h[4].v; ijk(h[4].L, r->qt_min_ijk);
     }
     r->dt0_old = r->dt0_new = G.dt0;
+    if (h[5].L != LLONG_MAX) {
+        // a non-finite value: reported with its first location, no time-step decision
+        r->nonfinite = 1;
+        ijk(h[5].L, r->nonfinite_ijk);
+        return MG_ERR_NAN;
+    }
     // checkall order: checkx(es), checkx(qt), checkwind; the first failing check stops
     if (r->es_max > p->es_max || r->es_min < p->es_min) {
         r->stop = MG_STOP_ES;
@@ -1081,6 +1087,14 @@ extern "C" int mg_checkall(mg_ctx *c, const mg_check_params *p, mg_check_result 
         }
     }
     return MG_OK;
+}
+
+extern "C" int mg_selftest_wait(mg_ctx *c, long long limit_cycles)
+{
+    if (!c || limit_cycles < 0 || limit_cycles > MG_WAIT_CYCLES) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    CKR(launch_selftest_wait(limit_cycles, c->derr, c->stream));
+    return check_err(c);
 }
 
 extern "C" int mg_download_ksgs(mg_ctx *c, double *ksgs)

@@ -1,6 +1,8 @@
 // k_check.cu -- the per-step checks of checkall (src/IO/check.f90:59-95): the maximum
 // advective CFL number of checkwind (:102-337) and the bounds of checkx (:341-417)
-// for es and qt, each with the location of its first occurrence.
+// for es and qt, each with the location of its first occurrence, and the first
+// non-finite value of u, v, w, es or qt (the library's MG_ERR_NAN; the reference has no
+// such check: a NaN passes checkx's comparisons and ends its run later, if at all).
 //
 // One pass over the interior of the resident level-n state: every thread keeps its
 // extremes with their linear indices L = ((k-1)*maxy + (j-4))*maxx + (i-4), which
@@ -10,12 +12,13 @@
 #include <climits>
 
 #include "mg_common.cuh"
+#include "tma.cuh"
 
 namespace {
 
 constexpr long long NONE = LLONG_MAX;
 constexpr int CHECK_BLOCKS = 592;   // 4 x 148 SMs
-constexpr int NX = 5;               // cfl max, es max, es min, qt max, qt min
+constexpr int NX = 6;               // cfl max, es max, es min, qt max, qt min, first non-finite
 
 struct Ext {
     double v;
@@ -38,6 +41,7 @@ __device__ __forceinline__ void combine(Ext *a, const Ext *b)
     take_min(a[2], b[2]);
     take_max(a[3], b[3]);
     take_min(a[4], b[4]);
+    if (b[5].L != NONE && (a[5].L == NONE || b[5].L < a[5].L)) a[5] = b[5];
 }
 
 __device__ void block_reduce(Ext *mine, Ext *out)
@@ -78,11 +82,14 @@ __global__ void __launch_bounds__(256) check_partial_kernel(DevGrid G, const dou
         const double e = __ldg(es + c);
         take_max(m[1], Ext{e, L});
         take_min(m[2], Ext{e, L});
+        bool finite = isfinite(cflx) && isfinite(cfly) && isfinite(cflz) && isfinite(e);
         if (qt) {
             const double q = __ldg(qt + c);
             take_max(m[3], Ext{q, L});
             take_min(m[4], Ext{q, L});
+            finite = finite && isfinite(q);
         }
+        if (!finite && m[5].L == NONE) m[5] = Ext{0., L};   // L grows along the loop: the first is the smallest
     }
     block_reduce(m, part + (size_t)blockIdx.x * NX);
 }
@@ -95,11 +102,34 @@ __global__ void __launch_bounds__(256) check_final_kernel(const Ext *part, int n
     block_reduce(m, out);
 }
 
+// The failure path of the bounded waits, exercised on purpose: one thread arms an
+// mbarrier for 16 transaction bytes, issues no copy (nothing is in flight), and waits
+// for it with the production wait and a cycle limit of the caller's choosing.  The wait
+// runs out and raises the context's error flag, which the host reads as MG_ERR_TIMEOUT;
+// the CTA then exits with nothing outstanding.
+__global__ void selftest_wait_kernel(long long limit, int *err)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+        mbar_arrive_expect_tx(&bar, 16);
+        mbar_wait_bounded_n(&bar, 0, err, limit);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_selftest_wait(long long limit, int *err, cudaStream_t s)
+{
+    selftest_wait_kernel<<<1, 32, 0, s>>>(limit, err);
+    return cudaGetLastError();
+}
 
 size_t check_scratch_bytes() { return (size_t)(CHECK_BLOCKS + 1) * NX * sizeof(Ext); }
 
-// out (device): 5 x {double value, long long L} (L = LLONG_MAX when no candidate)
+// out (device): 6 x {double value, long long L} (L = LLONG_MAX when no candidate); the
+// sixth is the first non-finite cell
 cudaError_t launch_check(const DevGrid &g, const double *u, const double *v, const double *w, const double *es,
                          const double *qt, void *scratch, cudaStream_t s)
 {

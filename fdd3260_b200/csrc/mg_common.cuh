@@ -150,6 +150,8 @@ void sgs_host_profiles(int nz, double dx, double dy, double dz, const double *fd
 size_t check_scratch_bytes();
 cudaError_t launch_check(const DevGrid &g, const double *u, const double *v, const double *w, const double *es,
                          const double *qt, void *scratch, cudaStream_t s);
+// a bounded mbarrier wait that runs out after `limit` cycles and raises *err
+cudaError_t launch_selftest_wait(long long limit, int *err, cudaStream_t s);
 
 // ---- one integrator stage for the trajectory tangent linear / adjoint (k_traj.cu) ----
 enum { TM_P, TM_MW, TM_RHO, TM_ES, TM_AES, TM_QT, TM_AQT, TM_AU, TM_AV, TM_AW, TM_TU, TM_TV, TM_TW, TM_UN, TM_VN,

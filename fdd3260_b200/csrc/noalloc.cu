@@ -16,7 +16,10 @@
 //  * nothing in the scratch has to start at zero: every launched block writes its own
 //    partial and the final reduction reads exactly those;
 //  * the first call on a device resolves the scratch address; make it before any
-//    stream capture that is to contain the call;
+//    stream capture that is to contain the call.  The address is kept for the life of
+//    the process: after cudaDeviceReset (or any teardown of the device's primary
+//    context) the module is loaded again and the array may move, so the entry must not
+//    be used across a device reset;
 //  * the scratch is one array per device: two calls in flight at the same time on one
 //    device (other streams or host threads) race on it, so callers serialise them.
 #include <mutex>

@@ -56,18 +56,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// bounded wait; returns false (and raises *err) on timeout
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err)
+// bounded wait of at most `limit` SM clock cycles; returns false (and raises *err) on timeout
+__device__ __forceinline__ bool mbar_wait_bounded_n(uint64_t *bar, uint32_t parity, int *err, long long limit)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > MG_WAIT_CYCLES) {
+        if (clock64() - t0 > limit) {
             if (err) atomicOr(err, 1);
             return false;
         }
     }
     return true;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err)
+{
+    return mbar_wait_bounded_n(bar, parity, err, MG_WAIT_CYCLES);
 }
 
 // 3-D tiled bulk copy global -> shared, completion signalled on bar

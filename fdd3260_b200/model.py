@@ -66,7 +66,12 @@ class Mimica:
         ch = checks if checks is not None else Checks()
         p = ch.params(self.domain.dt0, apply)
         r = _lib.MgCheckResult()
-        _lib.check(self._L.mg_checkall(self._h, C.byref(p), C.byref(r)), "mg_checkall")
+        rc = self._L.mg_checkall(self._h, C.byref(p), C.byref(r))
+        if rc == _lib.MG_ERR_NAN:
+            err = _lib.MimicaError(rc, f"mg_checkall: non-finite value at (i, j, k) = {tuple(r.nonfinite_ijk)}")
+            err.ijk = tuple(r.nonfinite_ijk)
+            raise err
+        _lib.check(rc, "mg_checkall")
         if apply and r.stop == _lib.MG_STOP_NONE:
             self.dt0 = r.dt0_new
         out = {f: getattr(r, f) for f, _ in r._fields_}

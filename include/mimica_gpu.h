@@ -221,7 +221,9 @@ int mg_anelastic_pressure(mg_ctx *ctx, double *mu, double *mv, double *mw, doubl
  * each step (modelctl.f90:369).  Locations are absolute 1-based (i, j, k) of the first
  * occurrence in the reference's loop order; the CFL location is (0, 0, 0) when every
  * CFL number is 0.  stop reports what makes the reference call stop_mimica(1): the
- * library itself never stops. */
+ * library itself never stops.  A NaN or Inf in u, v, w, es or qt returns MG_ERR_NAN
+ * with nonfinite = 1 and the first such cell in nonfinite_ijk (no dt decision is made;
+ * the reference has no such check). */
 enum { MG_STOP_NONE = 0, MG_STOP_ES = 1, MG_STOP_QT = 2, MG_STOP_CFL = 3, MG_STOP_DT = 4 };
 typedef struct mg_check_params {
     double cfl_max, cfl_min;   /* cfl_max, cfl_min (namelist defaults 0.5, 0.4) */
@@ -239,6 +241,8 @@ typedef struct mg_check_result {
     double dt0_old, dt0_new;   /* dt0 before and after the CFL rule */
     double es_min, es_max, qt_min, qt_max;
     int es_min_ijk[3], es_max_ijk[3], qt_min_ijk[3], qt_max_ijk[3];
+    int nonfinite;             /* 1: a NaN or Inf in u, v, w, es or qt (the call returns MG_ERR_NAN) */
+    int nonfinite_ijk[3];      /* its first location in the loop order above */
 } mg_check_result;
 int mg_checkall(mg_ctx *ctx, const mg_check_params *p, mg_check_result *r);
 /* the advective time-step rule of checkwind (:193-264; no microphysics time scale):
@@ -246,6 +250,13 @@ int mg_checkall(mg_ctx *ctx, const mg_check_params *p, mg_check_result *r);
 int mg_cfl_dt(const mg_check_params *p, double maxcfl, double dt0, double *dt0_new, int *stop);
 /* change the time step dt0 of a context (recorded step graphs are re-recorded) */
 int mg_set_dt(mg_ctx *ctx, double dt0);
+/* Failure-path check of the bounded device waits (no counterpart in the reference, which
+ * has no device code): one kernel arms an mbarrier for bytes that no copy delivers and
+ * waits for it with the same bounded wait the TMA pipelines use, limited to limit_cycles
+ * SM clock cycles (0 .. the library's own limit).  The wait runs out, the context's error
+ * flag is raised and read back, and the call returns MG_ERR_TIMEOUT with the flag
+ * cleared, so the next call on the context proceeds normally. */
+int mg_selftest_wait(mg_ctx *ctx, long long limit_cycles);
 
 /* ---- SGS turbulence diffusion (src/PHYS/subgrid.f90) ----
  * The Smagorinsky-Lilly closure of the build without TKE: calc_subgrid (cal_dij,
@@ -382,7 +393,9 @@ int mg_time_adjoint(mg_ctx *ctx, int reps, double *out5);
  * result; stream: a cudaStream_t (or NULL for the legacy default stream).
  * Limits: maxx, maxy <= 4096, 3 <= nz <= 4096 (MG_ERR_PARAM beyond).  The first call
  * on a device resolves the scratch address and must precede any stream capture that
- * is to contain the call; calls in flight together on one device race on the scratch. */
+ * is to contain the call; the address is kept for the process's life, so the entry must
+ * not be used across a cudaDeviceReset of that device; calls in flight together on one
+ * device race on the scratch. */
 int mg_maxdiv_noalloc(int maxx, int maxy, int nz, double dx, double dy, const double *dz1w,
                       const double *mu, const double *mv, const double *mw, double *maxdiv,
                       void *stream);
