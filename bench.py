@@ -512,28 +512,28 @@ def run_ensemble(args, ws, rank, local):
     from fdd3260_b200 import Mimica, _lib
     from fdd3260_b200 import ensemble as E
     specs = E.ensemble_specs(args.members, seed=3000)
-    parts = E.partition([s.cells for s in specs], ws)
-    mine = [specs[i] for i in parts[rank]]
     total_cells = sum(s.cells for s in specs)
     form = "mixed" if args.form == "mixed" else "fp64"
     prec = _lib.MG_PREC_MIXED if form == "mixed" else _lib.MG_PREC_FP64
     dev = local if ws > 1 else 0
-    members, states = [], []
-    for sp in mine:
-        d, st = E.member_problem(sp, precision=prec)
-        m = Mimica(d, nscal=len(st.scal), iqt=st.iqt, device=dev)
-        m.upload(st)
-        members.append(m)
-        states.append(st)
-    ens = E.Ensemble(members)
-    plans = ens.autotune(reps=3) if args.autotune == "on" else {}
-    # W warm-up steps, the last pair at the timed steps' parity (its graph is the one timed)
-    ens.step(args.warmup - 2, ntime0=1)
-    ens.step(2, ntime0=args.warmup - 1)
-    dist_barrier(ws)
-    with ClockSampler(local) as clk:
-        t_ms = ens.time_steps(args.steps, ntime0=1 + args.warmup)
-    t_ms = dist_max(t_ms, ws)
+    members, states, plans = [], [], {}
+
+    def build(mine):
+        for sp in mine:
+            d, st = E.member_problem(sp, precision=prec)
+            m = Mimica(d, nscal=len(st.scal), iqt=st.iqt, device=dev)
+            m.upload(st)
+            members.append(m)
+            states.append(st)
+        ens = E.Ensemble(members)
+        if args.autotune == "on":
+            plans.update(ens.autotune(reps=3))
+        return ens
+
+    clk = ClockSampler(local)
+    sh = E.shard_and_time(specs, rank, ws, build, args.warmup, args.steps, barrier=lambda: dist_barrier(ws),
+                          reduce_max=lambda x: dist_max(x, ws), reduce_sum=lambda x: dist_sum(x, ws), timed_region=clk)
+    ens, parts, t_ms = sh["stepper"], sh["parts"], sh["t_ms"]
     value = total_cells * args.steps / (t_ms / 1e3) / 1e6
     # roofline of the dominant kernel, from an eager profiled pass of this rank's largest member
     big = max(range(len(members)), key=lambda q: members[q].domain.cells)

@@ -222,11 +222,12 @@ def _new(d: Domain) -> np.ndarray:
     return np.zeros(d.shape)
 
 
-def warm_bubble_domain(maxx=64, maxy=64, nz=64, dx=50.0, dy=50.0, dz=50.0, dt0=0.5, scheme="weno", **kw) -> Domain:
-    """Dry warm bubble: doubly periodic box, rigid lid, theta0 = 300 K."""
+def warm_bubble_domain(maxx=64, maxy=64, nz=64, dx=50.0, dy=50.0, dz=50.0, dt0=0.5, scheme="weno", init=None,
+                       **kw) -> Domain:
+    """Dry warm bubble: doubly periodic box, rigid lid, theta0 = 300 K.  ``init``: see Domain.finish."""
     d = Domain(maxx=maxx, maxy=maxy, nz=nz, dx=dx, dy=dy, dz=dz, dt0=dt0, fdz0=np.ones(nz),
                pt0=np.full(nz, 300.0), qv0=np.zeros(nz), scal_adv=scheme, **kw)
-    return d.finish()
+    return d.finish(init)
 
 
 def warm_bubble_state(d: Domain, seed: int = 0, amp: float = 2.0, radius: float = 500.0,

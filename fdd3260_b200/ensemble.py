@@ -36,14 +36,16 @@ class MemberSpec:
         return self.nxy * self.nxy * self.nz
 
 
-def ensemble_specs(n: int = 64, seed: int = 3000, dx: float = 50.0, dz: float = 40.0) -> list[MemberSpec]:
-    """Seeded uneven sizes: nx = ny in {96,...,256}, nz in {64, 96, 128}; warm bubble of
-    amplitude U[1,3] K centred at a random point in the lower third of the domain."""
+def ensemble_specs(n: int = 64, seed: int = 3000, dx: float = 50.0, dz: float = 40.0,
+                   nx_choices=NX_CHOICES, nz_choices=NZ_CHOICES) -> list[MemberSpec]:
+    """Seeded uneven sizes: nx = ny in {96,...,256}, nz in {64, 96, 128} (or the given
+    sets); warm bubble of amplitude U[1,3] K centred at a random point in the lower third
+    of the domain."""
     rng = np.random.Generator(np.random.PCG64(seed))
     out = []
     for i in range(n):
-        nxy = int(rng.choice(NX_CHOICES))
-        nz = int(rng.choice(NZ_CHOICES))
+        nxy = int(rng.choice(nx_choices))
+        nz = int(rng.choice(nz_choices))
         amp = float(rng.uniform(1.0, 3.0))
         lx, lz = nxy * dx, nz * dz
         centre = (float(rng.uniform(0.2, 0.8) * lx), float(rng.uniform(0.2, 0.8) * lx),
@@ -66,10 +68,41 @@ def partition(cells: list[int], nranks: int) -> list[list[int]]:
     return [sorted(p) for p in parts]
 
 
+def shard_and_time(specs: list[MemberSpec], rank: int, world: int, build, warmup: int, steps: int,
+                   barrier=lambda: None, reduce_max=lambda x: x, reduce_sum=lambda x: x, timed_region=None) -> dict:
+    """The per-rank path of a sharded ensemble run.  The members are partitioned over the
+    ranks by cell count; ``build(my_specs)`` returns this rank's stepper (an object with
+    ``step(n, ntime0)`` and ``time_steps(n, ntime0) -> ms``, e.g. an ``Ensemble``).  It runs
+    exactly ``warmup`` untimed steps, the last two at the timed steps' parity (the momentum
+    direction order alternates with the step's parity, so that pair is what the timed steps
+    repeat), then ``steps`` timed steps after a barrier.  Only scalars cross ranks: the max
+    of the timed milliseconds and the sum of the cells stepped.  ``timed_region`` is an
+    optional context manager around the timed steps (clock sampling)."""
+    if warmup < 3:
+        raise ValueError("warmup >= 3")
+    parts = partition([s.cells for s in specs], world)
+    mine = [specs[i] for i in parts[rank]]
+    stepper = build(mine)
+    stepper.step(warmup - 2, ntime0=1)
+    stepper.step(2, ntime0=warmup - 1)
+    barrier()
+    if timed_region is None:
+        t_ms = stepper.time_steps(steps, ntime0=1 + warmup)
+    else:
+        with timed_region:
+            t_ms = stepper.time_steps(steps, ntime0=1 + warmup)
+    t_max = reduce_max(t_ms)
+    cells = reduce_sum(sum(s.cells for s in mine))
+    return {"t_ms": t_max, "rank_ms": t_ms, "cells": cells, "members": parts[rank], "parts": parts,
+            "stepper": stepper, "value": cells * steps / (t_max / 1e3) / 1e6}
+
+
 def member_problem(spec: MemberSpec, precision: int = _lib.MG_PREC_FP64, dx: float = 50.0, dz: float = 40.0,
-                   dt0: float = 0.5):
-    """(Domain, State) of a member: dry warm bubble, WENO, FD4 momentum."""
-    d = config.warm_bubble_domain(spec.nxy, spec.nxy, spec.nz, dx=dx, dy=dx, dz=dz, dt0=dt0, scheme="weno")
+                   dt0: float = 0.5, init=None):
+    """(Domain, State) of a member: dry warm bubble, WENO, FD4 momentum.  ``init``: see
+    config.Domain.finish."""
+    d = config.warm_bubble_domain(spec.nxy, spec.nxy, spec.nz, dx=dx, dy=dx, dz=dz, dt0=dt0, scheme="weno",
+                                  init=init)
     d.precision = precision
     st = config.warm_bubble_state(d, seed=spec.seed, amp=spec.amp, radius=min(500.0, 0.25 * spec.nz * dz),
                                   centre=spec.centre)

@@ -2,7 +2,9 @@
 two-rank (gloo, CPU) path that shards members with no data-path collective."""
 import os
 import socket
+import time
 
+import numpy as np
 import pytest
 
 from fdd3260_b200 import ensemble as E
@@ -66,3 +68,86 @@ def test_two_rank_sharding_over_gloo():
     (r0, m0, g0), (r1, m1, g1) = res
     assert g0 == g1 == [m0, m1]
     assert set(m0).isdisjoint(m1) and sorted(m0 + m1) == list(range(64))
+
+
+# ---- the sharded run with work: each of two gloo ranks steps its own members ----
+SMALL = dict(nx_choices=(16, 24, 32), nz_choices=(8, 12))
+
+
+class _OracleShard:
+    """CPU stand-in for a rank's Ensemble, with its interface (step, time_steps): every
+    member of the rank is stepped by the oracle (the CPU restatement of the reference)."""
+
+    def __init__(self, specs):
+        from oracle import oracle as O
+        self.items = []
+        for sp in specs:
+            d, st = E.member_problem(sp, init=O.Init())
+            self.items.append([sp.index, O.Oracle(d), st])
+
+    def step(self, n, ntime0=1):
+        for it in self.items:
+            if n > 0:
+                it[2], _, _ = it[1].stepping(it[2], nsteps=n, ntime0=ntime0)
+
+    def time_steps(self, n, ntime0=1):
+        t0 = time.perf_counter()
+        self.step(n, ntime0)
+        return (time.perf_counter() - t0) * 1e3
+
+
+def _work_rank(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+
+    def rmax(x):
+        t = torch.tensor([float(x)], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def rsum(x):
+        t = torch.tensor([float(x)], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    specs = E.ensemble_specs(6, seed=4000, **SMALL)
+    sh = E.shard_and_time(specs, rank, world, _OracleShard, warmup=3, steps=2, barrier=dist.barrier,
+                          reduce_max=rmax, reduce_sum=rsum)
+    finals = {it[0]: (it[2].u, it[2].w, it[2].scal[0]) for it in sh["stepper"].items}
+    dist.destroy_process_group()
+    q.put((rank, {k: sh[k] for k in ("t_ms", "rank_ms", "cells", "members", "value")}, finals))
+
+
+def test_two_ranks_step_their_members_and_gather_only_metrics():
+    """The path bench.py's ensemble workload takes (ensemble.shard_and_time), with the
+    oracle as each rank's stepper: the ranks' members are disjoint and cover the ensemble,
+    the gathered time is the max over ranks and the cells the sum, and every member ends
+    bit for bit where it ends when stepped alone: nothing couples the ranks' data."""
+    import torch.multiprocessing as mp
+    from oracle import oracle as O
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_work_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted([q.get(timeout=300) for _ in procs], key=lambda x: x[0])
+    for p in procs:
+        p.join(timeout=60)
+    assert all(p.exitcode == 0 for p in procs)
+    (_, m0, f0), (_, m1, f1) = res
+    specs = E.ensemble_specs(6, seed=4000, **SMALL)
+    assert set(m0["members"]).isdisjoint(m1["members"])
+    assert sorted(m0["members"] + m1["members"]) == list(range(6))
+    assert m0["t_ms"] == m1["t_ms"] == max(m0["rank_ms"], m1["rank_ms"])
+    assert m0["cells"] == m1["cells"] == sum(s.cells for s in specs)
+    assert m0["value"] == m0["cells"] * 2 / (m0["t_ms"] / 1e3) / 1e6
+    finals = {**f0, **f1}
+    for sp in specs:
+        d, st = E.member_problem(sp, init=O.Init())
+        alone, _, _ = O.Oracle(d).stepping(st, nsteps=5, ntime0=1)
+        u, w, th = finals[sp.index]
+        assert np.array_equal(u, alone.u) and np.array_equal(w, alone.w) and np.array_equal(th, alone.scal[0])
