@@ -7,8 +7,8 @@
 * ``oracle/libmimica_oracle.so`` -- the CPU restatement used as the checker by
   the tests (gcc, -O2 -fno-fast-math -ffp-contract=off), plus an OpenMP build
   ``oracle/libmimica_oracle_omp.so`` used as the timed CPU baseline.
-* ``oracle/_ref/libkissref.so`` -- only when the reference tree is present in
-  this container: the reference's own KISS FFT header compiled from where it
+* ``oracle/_ref/libkissref.so`` -- only when MIMICA_REFERENCE_TREE names a
+  reference tree: the reference's own KISS FFT header compiled from where it
   lies (see ``oracle/build_ref.sh``).
 
 Run ``python -m fdd3260_b200.build`` (or ``python fdd3260_b200/build.py``).
@@ -113,12 +113,14 @@ def build_oracle(verbose: bool = False) -> str:
 
 
 def build_reference_kiss(verbose: bool = False) -> str | None:
-    """Compile the reference's KISS FFT (checker only) when its sources are present."""
+    """Compile the reference's KISS FFT (checker only) when a reference tree is named by
+    the MIMICA_REFERENCE_TREE environment variable and holds its sources."""
     script = os.path.join(ORACLE_DIR, "build_ref.sh")
     target = os.path.join(ORACLE_DIR, "_ref", "libkissref.so")
-    if os.path.isdir("/root/reference/src/fftmpi/src") and os.path.exists(script):
+    tree = os.environ.get("MIMICA_REFERENCE_TREE", "")
+    if tree and os.path.isdir(os.path.join(tree, "src", "fftmpi", "src")) and os.path.exists(script):
         if _stale(target, [script, os.path.join(ORACLE_DIR, "ref_kiss_shim.cpp")]):
-            _run(["bash", script], verbose)
+            _run(["bash", script, tree], verbose)
     return target if os.path.exists(target) else None
 
 
