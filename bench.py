@@ -338,9 +338,10 @@ def main():
                     help="both (default): the plain FP64 form is the headline, the mixed form (FP32 "
                          "stencils/fluxes/spectra, FP64 state) is reported beside it with its error against "
                          "the FP64 form; fp64 / mixed: one form only")
-    ap.add_argument("--workload", default="cumulus", choices=["cumulus", "ensemble"],
+    ap.add_argument("--workload", default="cumulus", choices=["cumulus", "ensemble", "capacity"],
                     help="cumulus: the 512x512x256 shallow-cumulus domain (default); ensemble: 64 independent "
-                         "warm-bubble domains of seeded uneven sizes, batched per GPU, sharded over ranks")
+                         "warm-bubble domains of seeded uneven sizes, batched per GPU, sharded over ranks; "
+                         "capacity: one 1024x1024x256 domain with 3 momentum + density + 12 scalars (mixed form)")
     ap.add_argument("--sgs", default="none", choices=["none", "smagorinsky"],
                     help="smagorinsky: SGS turbulence diffusion on (Smagorinsky-Lilly, pran=-0.4, zdec=2400 m, "
                          "surface heat, moisture and momentum fluxes), as the BOMEX template runs it")
@@ -366,6 +367,8 @@ def main():
         ws, rank, local = dist_init()
     if args.workload == "ensemble":
         return run_ensemble(args, ws, rank, local)
+    if args.workload == "capacity":
+        return run_capacity(args, ws, rank, local)
     metric = "Mcell-updates/s per integrator step (2-stage Heun + projection)"
     lim = f" ({args.limiter} limiter)" if args.scheme == "muscl" else ""
     cfg = {"workload": f"shallow-cumulus domain {args.maxx}x{args.maxx}x{args.nz}, dx=dy=25 m, stretched dz 10->100 m, "
@@ -617,6 +620,52 @@ def run_ensemble(args, ws, rank, local):
                 "projection_plans": {k: {f: v[f] for f in ("x_radix", "y_radix", "x_threads", "y_threads", "tri_block",
                                                            "ms_default", "ms_tuned") if f in v}
                                      for k, v in plans.items()}}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_capacity(args, ws, rank, local):
+    """The capacity run: one 1024 x 1024 x 256 domain (dx = dy = 20 m, the cumulus tanh dz,
+    dt = 0.5 s) with 3 momentum fields, density and 12 scalars (theta_l, qt and 10 lognormal
+    tracers, sigma_log = 1), WENO, in the mixed form with the refined Poisson solve (or
+    --form fp64).  The state is generated and uploaded one field at a time, so the host
+    never holds more than one 2.2 GB field; the context holds the rest on the device."""
+    from types import SimpleNamespace
+
+    from fdd3260_b200 import Mimica, _lib, config
+    form = "fp64" if args.form == "fp64" else "mixed"
+    d = config.cumulus_domain(1024, 1024, 256, dx=20.0, dy=20.0, dt0=0.5, scheme=args.scheme,
+                              muscl_limiter=args.limiter)
+    d.precision = _lib.MG_PREC_MIXED if form == "mixed" else _lib.MG_PREC_FP64
+    nscal = 12
+    dev = local if ws > 1 else 0
+    m = Mimica(d, nscal=nscal, iqt=1, device=dev)
+    t0 = time.perf_counter()
+    for f in range(_lib.MG_FIELD_SCAL + nscal):
+        m.upload_field(f, config.cumulus_field(d, f, seed=4000 + rank))
+    t_up = time.perf_counter() - t0
+    st = SimpleNamespace(scal=[None] * nscal)
+    r = time_form(args, m, d, st, not args.no_graph, ws, local)
+    md, _ = m.stepping(1, ntime0=2 + args.warmup + args.steps, diagnostics=True, graph=False)
+    dev_bytes = m.device_bytes
+    m.close()
+    if rank == 0:
+        line = {"metric": "Mcell-updates/s per integrator step (2-stage Heun + projection), capacity run",
+                "value": r["value"], "unit": "Mcell-updates/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if form == "fp64" else "f32 fluxes/spectra, f64 state",
+                "data": "synthetic (seeded PCG64, one stream per field)",
+                "config": {"workload": "capacity domain 1024x1024x256, dx=dy=20 m, stretched dz 10->100 m, "
+                                       f"3 momentum + density + 12 scalars, {args.scheme.upper()}, FD4, dt=0.5 s",
+                           "form": form, "interior_cells": d.cells, "parallelism": f"replicas x{ws}",
+                           "l2": "inputs larger than L2"},
+                "clocks": r["clocks"], "gpu_launches": r["gpu_launches"], "roofline": r["roofline"],
+                "kernel_share": r["kernel_share"], "projection_plan": r["projection_plan"],
+                "device_bytes": dev_bytes, "maxdiv_after": md, "upload_s": t_up,
+                "e2e": None, "e2e_note": "not measured: 15 fields of 2.2 GB cross the bus each way per step",
+                "cpu_baseline": None}
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, "libmimica_gpu.so")
 
 # status codes (mimica_gpu.h)
 MG_OK, MG_ERR_PARAM, MG_ERR_CUDA, MG_ERR_NAN, MG_ERR_PIVOT, MG_ERR_TIMEOUT, MG_ERR_NOMEM, MG_ERR_STATE = range(8)
+MG_FIELD_U, MG_FIELD_V, MG_FIELD_W, MG_FIELD_P, MG_FIELD_DENS, MG_FIELD_SCAL = range(6)
 MG_WENO, MG_PPM, MG_MUSCL, MG_LW, MG_QUICK = 0, 1, 2, 3, 4
 MG_LIM_MINMOD, MG_LIM_VL, MG_LIM_MC, MG_LIM_DEFAULT = 0, 1, 2, 3
 MG_PREC_FP64, MG_PREC_MIXED = 0, 1
@@ -132,6 +133,8 @@ def lib() -> C.CDLL:
         L.mg_cfl_dt.argtypes = [C.POINTER(MgCheckParams), C.c_double, C.c_double, _dp, C.POINTER(C.c_int)]
         L.mg_set_dt.argtypes = [vp, C.c_double]
         L.mg_selftest_wait.argtypes = [vp, C.c_longlong]
+        L.mg_upload_field.argtypes = [vp, C.c_int, _dp]
+        L.mg_download_field.argtypes = [vp, C.c_int, _dp]
         L.mg_download_ksgs.argtypes = [vp, _dp]
         L.mg_traj_forward.argtypes = [vp, C.c_int, C.c_int]
         L.mg_traj_tl.argtypes = [vp, C.c_int, C.c_int, C.POINTER(_dp), C.POINTER(_dp)]

@@ -313,6 +313,44 @@ def cumulus_state(d: Domain, seed: int = 1000, n_extra: int = 3, lognormal_extra
     return State(u, v, w, _new(d), dens, scal, iqt=1)
 
 
+def cumulus_field(d: Domain, field: int, seed: int = 1000, lognormal_extras: bool = True) -> np.ndarray:
+    """One field of a cumulus-like state, for states too large to hold on the host at once
+    (fields are uploaded one at a time).  ``field`` is _lib.MG_FIELD_U .. _DENS or
+    MG_FIELD_SCAL + s: s = 0 theta_l, 1 qt, 2.. extra tracers.  Each field draws from its
+    own PCG64 stream (seed * 100 + field), with the distributions of cumulus_state: theta_l
+    and qt from the base profiles plus N(0, 0.1 K / 0.1 g/kg) below 500 m, u = -8 + N(0, 0.5),
+    v = N(0, 0.5), w = 0, p = 0, dens = rho0(z), extra tracers lognormal (sigma_log = 1)
+    with magnitudes 1e-4, 1e5, 1e8 in turn, or smooth profiles when not lognormal_extras."""
+    rng = np.random.Generator(np.random.PCG64(seed * 100 + field))
+    sh = (d.nz, d.maxy, d.maxx)
+    zc = d.zc()
+    low = (zc < 500.0)[:, None, None]
+
+    def field3(vals):
+        a = _new(d)
+        a[:, 3:3 + d.maxy, 3:3 + d.maxx] = vals
+        return periodic_fill(a)
+
+    if field == _lib.MG_FIELD_U:
+        return field3(-8.0 + rng.normal(0, 0.5, sh))
+    if field == _lib.MG_FIELD_V:
+        return field3(rng.normal(0, 0.5, sh))
+    if field in (_lib.MG_FIELD_W, _lib.MG_FIELD_P):
+        return _new(d)
+    if field == _lib.MG_FIELD_DENS:
+        return np.broadcast_to(d.den0[:, None, None], d.shape).copy()
+    s = field - _lib.MG_FIELD_SCAL
+    if s == 0:
+        return field3(d.pt0[:, None, None] + np.where(low, rng.normal(0, 0.1, sh), 0.0))
+    if s == 1:
+        return field3(np.maximum(d.qv0[:, None, None] + np.where(low, rng.normal(0, 1e-4, sh), 0.0), 1e-6))
+    scale = (1e-4, 1e5, 1e8)[(s - 2) % 3]
+    if lognormal_extras:
+        return field3(scale * np.exp(rng.normal(0.0, 1.0, sh)))
+    prof = np.exp(-zc / 1500.0)[:, None, None]
+    return field3(scale * prof * (1.0 + np.where(low, rng.normal(0, 0.01, sh), 0.0)))
+
+
 def random_state(d: Domain, seed: int = 7, nscal: int = 2) -> State:
     """Generic smooth-ish random state for unit tests (positive scalars)."""
     rng = np.random.Generator(np.random.PCG64(seed))

@@ -48,6 +48,7 @@ struct mg_ctx {
     int k2_nseg = 0;                     // K2 likewise
     double traj_rec_limit = -1.;         // bytes the trajectory adjoint's stage records may take (< 0: half the free memory)
     int have_state = 0;
+    unsigned up_mask = 0;                // fields uploaded one at a time (bit = MG_FIELD_*) before a full state
     int launches = 0;
     size_t bytes = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -417,6 +418,32 @@ extern "C" int mg_upload_state_device(mg_ctx *c, const double *u, const double *
     return upload_impl(c, u, v, w, p, dens, scal, cudaMemcpyDeviceToDevice);
 }
 
+// one field of the level-n state (natural values) from host memory: a linear copy into a
+// stage buffer (free between steps), unpacked into the padded layout, ghosts refreshed
+extern "C" int mg_upload_field(mg_ctx *c, int field, const double *src)
+{
+    if (!c || !src || field < MG_FIELD_U || field >= MG_FIELD_SCAL + c->prm.nscal) return MG_ERR_PARAM;
+    if (c->have_state && c->rep != REP_NAT) return MG_ERR_STATE;
+    CKR(cudaSetDevice(c->device));
+    double *dst = field == MG_FIELD_U ? c->mA[0] : field == MG_FIELD_V ? c->mA[1] : field == MG_FIELD_W ? c->mA[2]
+                : field == MG_FIELD_P ? c->p : c->sA[field - MG_FIELD_DENS];
+    const size_t packed = (size_t)c->G.nx * c->G.ny * c->G.nz * sizeof(double);
+    double *stage = c->sB[0];
+    CKR(cudaMemcpyAsync(stage, src, packed, cudaMemcpyHostToDevice, c->stream));
+    CKR(launch_unpack(c->G, stage, dst, c->stream));
+    CKR(launch_halo_fill(c->G, &dst, 1, c->stream));
+    CKR(cudaStreamSynchronize(c->stream));
+    if (!c->have_state) {
+        c->up_mask |= 1u << field;
+        const unsigned all = (1u << (MG_FIELD_SCAL + c->prm.nscal)) - 1u;   // nscal < MG_MAXF: fits 32 bits
+        if (c->up_mask == all) {
+            c->rep = REP_NAT;
+            c->have_state = 1;
+        }
+    }
+    return MG_OK;
+}
+
 static int download_impl(mg_ctx *c, double *u, double *v, double *w, double *p, double *dens, double *const *scal,
                          cudaMemcpyKind kind)
 {
@@ -452,6 +479,16 @@ static int download_impl(mg_ctx *c, double *u, double *v, double *w, double *p, 
 extern "C" int mg_download_state(mg_ctx *c, double *u, double *v, double *w, double *p, double *dens, double *const *scal)
 {
     return download_impl(c, u, v, w, p, dens, scal, cudaMemcpyDeviceToHost);
+}
+extern "C" int mg_download_field(mg_ctx *c, int field, double *dst)
+{
+    if (!c || !dst || field < MG_FIELD_U || field >= MG_FIELD_SCAL + c->prm.nscal) return MG_ERR_PARAM;
+    std::vector<double *> sc(c->prm.nscal > 0 ? c->prm.nscal : 1, nullptr);
+    if (field >= MG_FIELD_SCAL) sc[field - MG_FIELD_SCAL] = dst;
+    return download_impl(c, field == MG_FIELD_U ? dst : nullptr, field == MG_FIELD_V ? dst : nullptr,
+                         field == MG_FIELD_W ? dst : nullptr, field == MG_FIELD_P ? dst : nullptr,
+                         field == MG_FIELD_DENS ? dst : nullptr, field >= MG_FIELD_SCAL ? sc.data() : nullptr,
+                         cudaMemcpyDeviceToHost);
 }
 extern "C" int mg_download_state_device(mg_ctx *c, double *u, double *v, double *w, double *p, double *dens,
                                         double *const *scal)

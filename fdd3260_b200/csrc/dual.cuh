@@ -55,12 +55,15 @@ template <int N> __device__ __forceinline__ D<N> operator*(const D<N> &a, const 
     for (int q = 0; q < N; q++) r.d[q] = a.d[q] * b.v + a.v * b.d[q];
     return r;
 }
+// the value is the correctly rounded quotient (the forward's); the partials use one
+// reciprocal of the divisor
 template <int N> __device__ __forceinline__ D<N> operator/(const D<N> &a, const D<N> &b)
 {
     const double qv = a.v / b.v;
+    const double rb = 1. / b.v;
     D<N> r(qv);
 #pragma unroll
-    for (int q = 0; q < N; q++) r.d[q] = (a.d[q] - qv * b.d[q]) / b.v;
+    for (int q = 0; q < N; q++) r.d[q] = (a.d[q] - qv * b.d[q]) * rb;
     return r;
 }
 template <int N> __device__ __forceinline__ bool operator<(const D<N> &a, const D<N> &b) { return a.v < b.v; }

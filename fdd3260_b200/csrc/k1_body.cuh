@@ -381,11 +381,11 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
                         double Fx, Fy;
                         if (SCHEME == MG_WENO) {
                             if constexpr (MIXED) {
-                                Fx = weno_face_mixed(V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu, true);
-                                Fy = weno_face_mixed(V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv, true);
+                                Fx = weno_face_up_mixed(V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu, true);
+                                Fy = weno_face_up_mixed(V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv, true);
                             } else {
-                                Fx = weno_face(V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu, true);
-                                Fy = weno_face(V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv, true);
+                                Fx = weno_face_up(V(bx - 1), V(bx), V(bx + 1), V(bx + 2), uu, true);
+                                Fy = weno_face_up(V(by - SW), V(by), V(by + SW), V(by + 2 * SW), vv, true);
                             }
                         } else if (SCHEME == MG_MUSCL) {
                             if constexpr (MIXED) {
@@ -479,11 +479,11 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
                             if constexpr (MIXED) {
                                 if (k == 1) Fzn = weno_face_bottom_mixed(ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww);
                                 else if (k == nz - 1) Fzn = weno_face_top_mixed(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ww);
-                                else Fzn = weno_face_mixed(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww, (k >= 3 && k <= nz - 3));
+                                else Fzn = weno_face_up_mixed(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww, (k >= 3 && k <= nz - 3));
                             } else {
                                 if (k == 1) Fzn = weno_face_bottom(ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww);
                                 else if (k == nz - 1) Fzn = weno_face_top(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ww);
-                                else Fzn = weno_face(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww, (k >= 3 && k <= nz - 3));
+                                else Fzn = weno_face_up(ZVAL(f, 0), ZVAL(f, 1), ZVAL(f, 2), ZVAL(f, 3), ww, (k >= 3 && k <= nz - 3));
                             }
                         } else if (SCHEME == MG_MUSCL) {
                             const int kind = k == 1 ? 1 : (k == nz - 1 ? 2 : 0);

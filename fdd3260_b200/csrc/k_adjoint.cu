@@ -9,7 +9,10 @@
 // The Jacobian of every face flux with respect to its four stencil values and its
 // velocity is obtained by evaluating the forward scheme templates on dual numbers
 // (dual.cuh): the switch to nonlinear weights and the positivity limiter follow the
-// branch the FP64 form takes, and the smoothness weights are differentiated.
+// branch the FP64 form takes, and the smoothness weights are differentiated.  The
+// face template is the upwind-only one the forward kernel runs (weno_face_up): the
+// downwind side's term is zero with a zero derivative, so only the upwind side's
+// weights are carried on dual numbers.
 //   TL: dA = J (dx, dm), per direction a face pass (each face's tangent flux once) and a
 //       difference pass over the cells.
 //   AD: (xbar, mbar) = J^T Abar, deterministic two-pass form per direction: a face pass
@@ -47,7 +50,7 @@ __device__ bool face_jac(const DevGrid &G, int dir, const AdvIn &in, int i, int 
         const D5 v = D5::var(mom / d0 - shift, 4);
         const D5 a = D5::var(__ldg(in.x + c - st), 0), b = D5::var(__ldg(in.x + c), 1);
         const D5 cc = D5::var(__ldg(in.x + c + st), 2), e = D5::var(__ldg(in.x + c + 2 * st), 3);
-        const D5 F = weno_face<D5>(a, b, cc, e, v, true);
+        const D5 F = weno_face_up<D5>(a, b, cc, e, v, true);
         for (int m = 0; m < 4; m++) J[m] = F.d[m];
         Jv = F.d[4] / d0;
         return true;
@@ -68,7 +71,7 @@ __device__ bool face_jac(const DevGrid &G, int dir, const AdvIn &in, int i, int 
     } else {
         const D5 a = D5::var(__ldg(in.x + c - st), 0), b = D5::var(__ldg(in.x + c), 1);
         const D5 cc = D5::var(__ldg(in.x + c + st), 2), e = D5::var(__ldg(in.x + c + 2 * st), 3);
-        F = weno_face<D5>(a, b, cc, e, w, k >= 3 && k <= nz - 3);
+        F = weno_face_up<D5>(a, b, cc, e, w, k >= 3 && k <= nz - 3);
     }
     for (int m = 0; m < 4; m++) J[m] = F.d[m];
     Jv = F.d[4] / a1;

@@ -42,49 +42,49 @@ template <> __device__ __forceinline__ float min_abs_ratio_1<float>(float num, f
 }
 
 // ---------------- WENO3-switch: src/TOOLS/advq_weno.f90 ----------------
-// weights of one face, :304-353 (loop body); linear weights unless the smoothness
-// ratio exceeds 20.  (eps+eta)**2 is the correctly rounded product.
+// Face flux at i+1/2 (:92-110; weights :304-353, limiter :462-491).  The reference
+// evaluates both sides, Flux = 0.5*Fl*(u+|u|) + 0.5*Fr*(u-|u|), with Fl = w0*ffim1 +
+// w1*ffip1p and Fr = w2*ffip1m + w3*ffip2 from the limited candidates, and weights that
+// are linear (1/3, 2/3) unless the smoothness ratio max/min(eta) exceeds 20, then
+// g/(eps+eta)^2 normalised; (eps+eta)**2 is the correctly rounded product.
+// weno_face_up evaluates only the upwind side's weights and reconstruction.  For u > 0
+// the reference's downwind term is 0.5*Fr*(u-|u|) = 0.5*Fr*0, a zero, and adding a zero
+// to the upwind term leaves its value unchanged (u < 0 alike), so the result equals the
+// reference's up to the sign of a zero flux.  The downwind side's
+// weights (and their divisions) are not computed.  The right side is the left side's
+// formula on the mirrored stencil (xp2, xp1, x0): eta1 <-> eta3, the candidates
+// 1.5*xp1 - 0.5*xp2 and 0.5*xp1 + 0.5*x0, and the weight sum g1/y3^2 + g2/y2^2; every
+// swapped operand pair is an IEEE addition or product, which commutes bit for bit.  The
+// positivity limiter scales all four candidates about x0 with phi from their minimum,
+// as :462-491 do, before one side is chosen.  u = 0 takes the left side: its value is a
+// zero either way, and on dual numbers (whose |u| has slope +1 at 0) the left side's
+// term 0.5*Fl*(u+|u|) is the one whose derivative, Fl*du, the two-sided form has.
 template <typename T>
-__device__ __forceinline__ void weno_weights(T xm1, T x0, T xp1, T xp2, T &w0, T &w1, T &w2, T &w3)
+__device__ __forceinline__ T weno_face_up(T xm1, T x0, T xp1, T xp2, T uu, bool full_weights)
 {
-    const T g1 = T(1.) / T(3.), g2 = T(2.) / T(3.), eps = T(1.e-15), thres = T(20.);
-    T d1 = x0 - xm1, d2 = xp1 - x0, d3 = xp2 - xp1;
-    T eta1 = d1 * d1, eta2 = d2 * d2, eta3 = d3 * d3;
-    w0 = g1; w1 = g2; w2 = g2; w3 = g1;
-    if (ratio_gt(tmax(eta1, eta2), tmin(eta1, eta2) + eps, thres)) {
-        T y1 = eps + eta1, y2 = eps + eta2;
-        T a = g1 / (y1 * y1), b = g2 / (y2 * y2);
-        T s = a + b;
-        w0 = a / s; w1 = b / s;
-    }
-    if (ratio_gt(tmax(eta2, eta3), tmin(eta2, eta3) + eps, thres)) {
-        T y2 = eps + eta2, y3 = eps + eta3;
-        T a = g2 / (y2 * y2), b = g1 / (y3 * y3);
-        T s = a + b;
-        w2 = a / s; w3 = b / s;
-    }
-}
-
-// face flux at i+1/2 (advq_weno.f90:92-110, limiter :462-491)
-template <typename T>
-__device__ __forceinline__ T weno_face(T xm1, T x0, T xp1, T xp2, T uu, bool full_weights)
-{
-    const T eps = T(1.e-15);
-    T w0 = T(1.) / T(3.), w1 = T(2.) / T(3.), w2 = T(2.) / T(3.), w3 = T(1.) / T(3.);
-    if (full_weights) weno_weights(xm1, x0, xp1, xp2, w0, w1, w2, w3);
+    const T eps = T(1.e-15), g1 = T(1.) / T(3.), g2 = T(2.) / T(3.), thres = T(20.);
     T ffim1 = (-(T(0.5) * xm1) + T(1.5) * x0);
-    T ffip1p = (T(0.5) * x0 + T(0.5) * xp1);
-    T ffip1m = ffip1p;
+    T ffip1 = (T(0.5) * x0 + T(0.5) * xp1);
     T ffip2 = (T(1.5) * xp1 - T(0.5) * xp2);
-    T minp = tmin(tmin(tmin(ffim1, ffip1m), ffip1p), ffip2);
+    T minp = tmin(tmin(tmin(ffim1, ffip1), ffip1), ffip2);
     T phi = min_abs_ratio_1(T(0.) - x0, (minp - x0) + eps);
-    ffim1 = phi * (ffim1 - x0) + x0;
-    ffip1m = phi * (ffip1m - x0) + x0;
-    ffip1p = phi * (ffip1p - x0) + x0;
-    ffip2 = phi * (ffip2 - x0) + x0;
-    T Fl = w0 * ffim1 + w1 * ffip1p;
-    T Fr = w2 * ffip1m + w3 * ffip2;
-    return T(0.5) * Fl * (uu + dabs(uu)) + T(0.5) * Fr * (uu - dabs(uu));
+    const bool pos = !(uu < T(0.));
+    const T far = phi * ((pos ? ffim1 : ffip2) - x0) + x0;
+    const T cen = phi * (ffip1 - x0) + x0;
+    T wf = g1, wc = g2;
+    if (full_weights) {
+        const T dout = pos ? (x0 - xm1) : (xp2 - xp1);
+        const T dmid = xp1 - x0;
+        const T eo = dout * dout, em = dmid * dmid;
+        if (ratio_gt(tmax(eo, em), tmin(eo, em) + eps, thres)) {
+            const T yo = eps + eo, ym = eps + em;
+            const T a = g1 / (yo * yo), b = g2 / (ym * ym);
+            const T s = a + b;
+            wf = a / s; wc = b / s;
+        }
+    }
+    const T F = wf * far + wc * cen;
+    return T(0.5) * F * (pos ? (uu + dabs(uu)) : (uu - dabs(uu)));
 }
 // vertical bottom face (k=1), :232-241
 template <typename T>
@@ -112,26 +112,25 @@ __device__ __forceinline__ T weno_face_top(T xm1, T x0, T xp1, T ww)
 }
 
 // ---------------- MUSCL: src/TOOLS/advq_muscl.f90 ----------------
+// limiter_muscl (:335-383) for one side: phil is muscl_phi(.., ffip1, ffim1), phir is
+// muscl_phi(.., ffip1, ffip2); the reference's two sides are the same expressions on
+// their own slope.
 template <typename T>
-__device__ __forceinline__ void muscl_limiter(int lim, T lim_tol, T xx, T ffip1, T ffip2, T ffim1, T &phir, T &phil)
+__device__ __forceinline__ T muscl_phi(int lim, T lim_tol, T xx, T ffip1, T ffo)
 {
-    T rp1 = T(1.), rp2 = T(1.);
-    if (dabs(ffim1) > lim_tol * dabs(xx) && dabs(ffip1) < dabs(ffim1) / lim_tol) rp1 = ffip1 / ffim1;
-    if (dabs(ffip2) > lim_tol * dabs(xx) && dabs(ffip1) < dabs(ffip2) / lim_tol) rp2 = ffip1 / ffip2;
-    if (lim == 1) {        // VL
-        phil = (rp1 + dabs(rp1)) / (T(1.) + dabs(rp1));
-        phir = (rp2 + dabs(rp2)) / (T(1.) + dabs(rp2));
-    } else if (lim == 2) { // MC
-        phil = tmax(T(0.), tmin(tmin(T(2.) * rp1, T(0.5) * (rp1 + T(1.))), T(2.)));
-        phir = tmax(T(0.), tmin(tmin(T(2.) * rp2, T(0.5) * (rp2 + T(1.))), T(2.)));
-    } else if (lim == 0) { // minmod
-        phil = tmax(T(0.), tmin(T(1.), rp1));
-        phir = tmax(T(0.), tmin(T(1.), rp2));
-    } else {
-        phil = T(0.5) * (rp1 + T(1.));
-        phir = T(0.5) * (rp2 + T(1.));
-    }
+    T r = T(1.);
+    if (dabs(ffo) > lim_tol * dabs(xx) && dabs(ffip1) < dabs(ffo) / lim_tol) r = ffip1 / ffo;
+    if (lim == 1) return (r + dabs(r)) / (T(1.) + dabs(r));                               // VL
+    if (lim == 2) return tmax(T(0.), tmin(tmin(T(2.) * r, T(0.5) * (r + T(1.))), T(2.)));   // MC
+    if (lim == 0) return tmax(T(0.), tmin(T(1.), r));                                      // minmod
+    return T(0.5) * (r + T(1.));
 }
+
+// The face fluxes below evaluate only the upwind side.  The reference's flux is
+// 0.5*u*(Fl*(1+sign(1,u)) + Fr*(1-sign(1,u))) (:99): for sign(1,u) = 1 the second product
+// is Fr*0, a zero, and Fl*2 + 0 = Fl*2, so the value is 0.5*u*(Fl*2) (sign(1,u) = -1
+// alike with Fr); it differs from the two-sided expression at most in the sign of a zero.
+// sign(1,u) has copysign semantics, so u = -0 takes the Fr side as the reference does.
 
 // horizontal face between i and i+1 (advq_muscl.f90:81-100); d = dx, d1 = 1/dx
 template <typename T>
@@ -141,17 +140,15 @@ __device__ __forceinline__ T muscl_face_h(int lim, T lim_tol, T d, T d1, T xm1, 
     T slope_p = (xp1 - x0) * d1;
     T slope_p2 = (xp2 - xp1) * d1;
     T slope_m = (x0 - xm1) * d1;
-    T Fr, Fl;
+    const bool pos = sign1(uu) > T(0.);
+    T F;
     if (d * dabs(slope_m) > lim_tol * dabs(x0) + eps || d * dabs(slope_p2) > lim_tol * dabs(x0) + eps) {
-        T phir, phil;
-        muscl_limiter(lim, lim_tol, x0, slope_p, slope_p2, slope_m, phir, phil);
-        Fr = xp1 - T(0.5) * phir * slope_p2 * d;
-        Fl = x0 + T(0.5) * phil * slope_m * d;
+        const T phi = muscl_phi(lim, lim_tol, x0, slope_p, pos ? slope_m : slope_p2);
+        F = pos ? x0 + T(0.5) * phi * slope_m * d : xp1 - T(0.5) * phi * slope_p2 * d;
     } else {
-        Fr = xp1 - T(0.5) * slope_p * d;
-        Fl = x0 + T(0.5) * slope_p * d;
+        F = pos ? x0 + T(0.5) * slope_p * d : xp1 - T(0.5) * slope_p * d;
     }
-    return T(0.5) * uu * (Fl * (T(1.) + sign1(uu)) + Fr * (T(1.) - sign1(uu)));
+    return T(0.5) * uu * (F * T(2.));
 }
 
 // vertical face k+1/2 (advq_muscl.f90:245-302).  kind: 0 core, 1 bottom (k=1), 2 top (k=nz-1).
@@ -162,21 +159,13 @@ __device__ __forceinline__ T muscl_face_z(int kind, int lim, T lim_tol, T dz, T 
                                           T d1m, T d10, T d1p, T fm, T fp, T dzw1, T ww)
 {
     const T eps = T(1.e-18);
-    T slope_p, slope_p2, slope_m, Fl, Fr, phir, phil;
+    T slope_p, slope_p2, slope_m;
     bool lim_on;
     if (kind == 1) {
         slope_p = (xp1 - x0) * d10;
         slope_p2 = (xp2 - xp1) * d1p;
         slope_m = slope_p;
         lim_on = fp * dz * dabs(slope_p2) > lim_tol * dabs(x0) + eps;
-        if (lim_on) {
-            muscl_limiter(lim, lim_tol, x0, slope_p, slope_p2, slope_m, phir, phil);
-            Fl = x0 + T(0.5) * phil * slope_m / dzw1;
-            Fr = xp1 - T(0.5) * phir * slope_p2 / dzw1;
-        } else {
-            Fl = x0 + T(0.5) * slope_p / dzw1;
-            Fr = xp1 - T(0.5) * slope_p / dzw1;
-        }
     } else {
         slope_p = (xp1 - x0) * d10;
         slope_m = (x0 - xm1) * d1m;
@@ -188,16 +177,16 @@ __device__ __forceinline__ T muscl_face_z(int kind, int lim, T lim_tol, T dz, T 
             lim_on = fm * dz * dabs(slope_m) > lim_tol * dabs(x0) + eps ||
                      fp * dz * dabs(slope_p2) > lim_tol * dabs(x0) + eps;
         }
-        if (lim_on) {
-            muscl_limiter(lim, lim_tol, x0, slope_p, slope_p2, slope_m, phir, phil);
-            Fr = xp1 - T(0.5) * phir * slope_p2 / dzw1;
-            Fl = x0 + T(0.5) * phil * slope_m / dzw1;
-        } else {
-            Fr = xp1 - T(0.5) * slope_p / dzw1;
-            Fl = x0 + T(0.5) * slope_p / dzw1;
-        }
     }
-    return T(0.5) * ww * (Fl * (T(1.) + sign1(ww)) + Fr * (T(1.) - sign1(ww)));
+    const bool pos = sign1(ww) > T(0.);
+    T F;
+    if (lim_on) {
+        const T phi = muscl_phi(lim, lim_tol, x0, slope_p, pos ? slope_m : slope_p2);
+        F = pos ? x0 + T(0.5) * phi * slope_m / dzw1 : xp1 - T(0.5) * phi * slope_p2 / dzw1;
+    } else {
+        F = pos ? x0 + T(0.5) * slope_p / dzw1 : xp1 - T(0.5) * slope_p / dzw1;
+    }
+    return T(0.5) * ww * (F * T(2.));
 }
 
 // ---------------- lw: src/TOOLS/advq_lw.f90 (limiter 'MC', the module constant) ----------------
@@ -447,42 +436,33 @@ __device__ __forceinline__ T ppm_xplus_z(T x0, T ffip1, T ffip2, T ffim1, T delt
 // cancellation in the flux differences costs no digits of the FP64 state.
 // =====================================================================================
 
-// WENO3-switch face i+1/2: returns the flux in FP64
-__device__ __forceinline__ double weno_face_mixed(double xm1, double x0, double xp1, double xp2, double uu,
-                                                  bool full_weights)
+// WENO3-switch face i+1/2, returning the flux in FP64: the scheme logic runs in FP32 on
+// the differences from x0; only the upwind side's weights are evaluated (the mirrored
+// stencil for u < 0, as weno_face_up explains); the limiter sees all four candidates.
+__device__ __forceinline__ double weno_face_up_mixed(double xm1, double x0, double xp1, double xp2, double uu,
+                                                     bool full_weights)
 {
     const float eps = 1.e-15f, thres = 20.f, g1 = 1.f / 3.f, g2 = 2.f / 3.f;
     const float a = (float)(xm1 - x0), b = (float)(xp1 - x0), c = (float)(xp2 - x0);
-    float w0 = g1, w1 = g2, w2 = g2, w3 = g1;
+    const bool pos = uu > 0.;
+    float wf = g1, wc = g2;
     if (full_weights) {
-        const float d3 = c - b;
-        const float eta1 = a * a, eta2 = b * b, eta3 = d3 * d3;
-        // The switch is decided on the FP32 smoothness indicators.  Being discontinuous,
-        // it can differ from the plain form's decision where the ratio lies within the
-        // FP32 rounding band (~1e-6 relative) of the threshold; the plain form itself
-        // flips such faces under perturbations of ~1e-9 of its state.
-        const bool nl1 = fmaxf(eta1, eta2) > thres * (fminf(eta1, eta2) + eps);
-        const bool nl2 = fmaxf(eta2, eta3) > thres * (fminf(eta2, eta3) + eps);
-        if (nl1) {
-            const float y1 = eps + eta1, y2 = eps + eta2;
-            // w0 = g1/y1^2 / (g1/y1^2 + g2/y2^2) = g1 y2^2 / (g1 y2^2 + g2 y1^2)
-            const float p = g1 * (y2 * y2), q = g2 * (y1 * y1), r = __frcp_rn(p + q);
-            w0 = p * r; w1 = q * r;
-        }
-        if (nl2) {
-            const float y2 = eps + eta2, y3 = eps + eta3;
-            const float p = g2 * (y3 * y3), q = g1 * (y2 * y2), r = __frcp_rn(p + q);
-            w2 = p * r; w3 = q * r;
+        const float dout = pos ? a : c - b;
+        const float eo = dout * dout, em = b * b;
+        if (fmaxf(eo, em) > thres * (fminf(eo, em) + eps)) {
+            const float yo = eps + eo, ym = eps + em;
+            // wf = g1/yo^2 / (g1/yo^2 + g2/ym^2) = g1 ym^2 / (g1 ym^2 + g2 yo^2)
+            const float p = g1 * (ym * ym), q = g2 * (yo * yo), r = __frcp_rn(p + q);
+            wf = p * r; wc = q * r;
         }
     }
-    float d1 = -0.5f * a, d2 = 0.5f * b, dd3 = 1.5f * b - 0.5f * c;   // reconstructions minus x0
-    const float mind = fminf(fminf(d1, d2), dd3);
+    const float d1 = -0.5f * a, d2 = 0.5f * b, d3 = 1.5f * b - 0.5f * c;   // reconstructions minus x0
+    const float mind = fminf(fminf(d1, d2), d3);
     const float x0f = (float)x0;
     const float den = mind + eps;
     const float phi = fabsf(x0f) >= fabsf(den) ? 1.f : fabsf(x0f / den);
-    d1 *= phi; d2 *= phi; dd3 *= phi;
-    const float dl = w0 * d1 + w1 * d2, dr = w2 * d2 + w3 * dd3;
-    return uu > 0. ? uu * (x0 + (double)dl) : (uu < 0. ? uu * (x0 + (double)dr) : 0.);
+    const float dsel = phi * (wf * (pos ? d1 : d3) + wc * d2);
+    return uu == 0. ? 0. : uu * (x0 + (double)dsel);
 }
 __device__ __forceinline__ double weno_face_bottom_mixed(double x1, double x2, double x3, double ww)
 {
@@ -505,19 +485,16 @@ __device__ __forceinline__ double muscl_face_h_mixed(int lim, float lim_tol, flo
     const float eps = 1.e-18f;
     const float sp = (float)(xp1 - x0) * d1, sp2 = (float)(xp2 - xp1) * d1, sm = (float)(x0 - xm1) * d1;
     const float ax = fabsf((float)x0);
-    float dr, dl;
+    const bool pos = uu >= 0.;
+    float dd;   // upwind face value minus its cell value
     if (d * fabsf(sm) > lim_tol * ax + eps || d * fabsf(sp2) > lim_tol * ax + eps) {
-        float phir, phil;
-        muscl_limiter(lim, lim_tol, (float)x0, sp, sp2, sm, phir, phil);
-        dr = -0.5f * phir * sp2 * d;   // Flux_r - x(i+1)
-        dl = 0.5f * phil * sm * d;     // Flux_l - x(i)
+        const float phi = muscl_phi(lim, lim_tol, (float)x0, sp, pos ? sm : sp2);
+        dd = pos ? 0.5f * phi * sm * d : -0.5f * phi * sp2 * d;
     } else {
-        dr = -0.5f * sp * d;
-        dl = 0.5f * sp * d;
+        dd = pos ? 0.5f * sp * d : -0.5f * sp * d;
     }
-    return uu >= 0. ? uu * (x0 + (double)dl) : uu * (xp1 + (double)dr);
+    return uu * ((pos ? x0 : xp1) + (double)dd);
 }
-// MUSCL vertical face (kind: 0 core, 1 bottom, 2 top), same argument meaning as muscl_face_z
 __device__ __forceinline__ double muscl_face_z_mixed(int kind, int lim, float lim_tol, float dz, double xm1, double x0,
                                                      double xp1, double xp2, float d1m, float d10, float d1p, float fm,
                                                      float fp, float dzw1, double ww)
@@ -542,17 +519,15 @@ __device__ __forceinline__ double muscl_face_z_mixed(int kind, int lim, float li
         }
     }
     const float h = 0.5f / dzw1;
-    float dr, dl;
+    const bool pos = ww >= 0.;
+    float dd;   // upwind face value minus its cell value
     if (lim_on) {
-        float phir, phil;
-        muscl_limiter(lim, lim_tol, (float)x0, sp, sp2, sm, phir, phil);
-        dl = phil * sm * h;
-        dr = -(phir * sp2 * h);
+        const float phi = muscl_phi(lim, lim_tol, (float)x0, sp, pos ? sm : sp2);
+        dd = pos ? phi * sm * h : -(phi * sp2 * h);
     } else {
-        dl = sp * h;
-        dr = -(sp * h);
+        dd = pos ? sp * h : -(sp * h);
     }
-    return ww >= 0. ? ww * (x0 + (double)dl) : ww * (xp1 + (double)dr);
+    return ww * ((pos ? x0 : xp1) + (double)dd);
 }
 
 // lw faces in the mixed form: FP32 slopes of differences relative to the upwind cell,

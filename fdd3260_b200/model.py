@@ -227,6 +227,22 @@ class Mimica:
             return out
         return State(u, v, w, p, dens, scal, self.iqt)
 
+    def upload_field(self, field: int, a: np.ndarray) -> None:
+        """One field of the level-n state (``_lib.MG_FIELD_*``; ``MG_FIELD_SCAL + s`` for
+        scalar s), natural values of the domain's shape."""
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if a.shape != self.domain.shape:
+            raise ValueError("field shape differs from the domain's")
+        _lib.check(self._L.mg_upload_field(self._h, int(field), _lib.ptr(a)), "mg_upload_field")
+
+    def download_field(self, field: int, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.zeros(self.domain.shape)
+        elif out.shape != self.domain.shape or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("out must be C-contiguous float64 of the domain's shape")
+        _lib.check(self._L.mg_download_field(self._h, int(field), _lib.ptr(out)), "mg_download_field")
+        return out
+
     def upload_device(self, ptrs: dict) -> None:
         """Upload from device pointers (ints), same layout as the host path."""
         sp = (C.c_void_p * self.nscal)(*ptrs["scal"])

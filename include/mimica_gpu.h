@@ -112,6 +112,15 @@ int mg_upload_state(mg_ctx *ctx, const double *u, const double *v, const double 
                     const double *p, const double *dens, const double *const *scal);
 int mg_download_state(mg_ctx *ctx, double *u, double *v, double *w, double *p,
                       double *dens, double *const *scal);
+/* One field at a time, for callers that cannot hold every field on the host at once
+ * (the 1024 x 1024 x 256 capacity case has 2.2 GB per field).  field: MG_FIELD_U, _V,
+ * _W, _P, _DENS, or MG_FIELD_SCAL + s for scal[s].  Host pointers, reference layout,
+ * natural values, as mg_upload_state / mg_download_state take them.  A fresh context
+ * holds a state once every field has been uploaded; afterwards an upload replaces its
+ * field between steps (as the host physics' hand-over of one field would). */
+enum { MG_FIELD_U = 0, MG_FIELD_V = 1, MG_FIELD_W = 2, MG_FIELD_P = 3, MG_FIELD_DENS = 4, MG_FIELD_SCAL = 5 };
+int mg_upload_field(mg_ctx *ctx, int field, const double *src);
+int mg_download_field(mg_ctx *ctx, int field, double *dst);
 /* Device-pointer variants (pointers into device memory, same layout) */
 int mg_upload_state_device(mg_ctx *ctx, const double *u, const double *v, const double *w,
                            const double *p, const double *dens, const double *const *scal);

@@ -74,6 +74,8 @@ def test_null_pointers_rejected():
     assert L.mg_radix_candidates(0, None, None, 4) == _lib.MG_ERR_PARAM
     assert L.mg_qnadv_ad(None, 1, *([None] * 9)) == _lib.MG_ERR_PARAM
     assert L.mg_selftest_wait(None, 1000) == _lib.MG_ERR_PARAM
+    assert L.mg_upload_field(None, 0, None) == _lib.MG_ERR_PARAM
+    assert L.mg_download_field(None, 0, None) == _lib.MG_ERR_PARAM
 
 
 def test_host_precompute_matches_formulas():
