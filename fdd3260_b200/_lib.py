@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(HERE, "libmimica_gpu.so")
 # status codes (mimica_gpu.h)
 MG_OK, MG_ERR_PARAM, MG_ERR_CUDA, MG_ERR_NAN, MG_ERR_PIVOT, MG_ERR_TIMEOUT, MG_ERR_NOMEM, MG_ERR_STATE = range(8)
 MG_FIELD_U, MG_FIELD_V, MG_FIELD_W, MG_FIELD_P, MG_FIELD_DENS, MG_FIELD_SCAL = range(6)
+MG_CKPT_AUTO, MG_CKPT_DEVICE, MG_CKPT_HOST = -1, 0, 1
 MG_WENO, MG_PPM, MG_MUSCL, MG_LW, MG_QUICK = 0, 1, 2, 3, 4
 MG_LIM_MINMOD, MG_LIM_VL, MG_LIM_MC, MG_LIM_DEFAULT = 0, 1, 2, 3
 MG_PREC_FP64, MG_PREC_MIXED = 0, 1
@@ -141,6 +142,7 @@ def lib() -> C.CDLL:
         L.mg_traj_adjoint.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(_dp), C.POINTER(_dp)]
         L.mg_time_traj.argtypes = [vp, C.c_int, C.c_int, C.c_int, _dp]
         L.mg_traj_record_limit.argtypes = [vp, C.c_double]
+        L.mg_traj_checkpoints.argtypes = [vp, C.c_int]
         L.mg_autotune.argtypes = [vp, C.c_int, C.POINTER(MgTune)]
         L.mg_tune_get.argtypes = [vp, C.POINTER(MgTune)]
         L.mg_tune_set.argtypes = [vp, C.POINTER(MgTune)]
@@ -186,6 +188,6 @@ EXPORTED = [
     "mg_advection_tl", "mg_advection_ad", "mg_anelastic_pressure_ad", "mg_time_adjoint", "mg_ensemble_create", "mg_ensemble_destroy", "mg_ensemble_step", "mg_ensemble_time_steps", "mg_ensemble_launch_count",
     "mg_set_sgs", "mg_set_surface_fluxes", "mg_sgs_profiles", "mg_calc_subgrid", "mg_efud", "mg_eff",
     "mg_checkall", "mg_cfl_dt", "mg_set_dt", "mg_download_ksgs", "mg_qnadv_tl", "mg_qnadv_ad",
-    "mg_traj_forward", "mg_traj_tl", "mg_traj_adjoint", "mg_time_traj", "mg_traj_record_limit",
+    "mg_traj_forward", "mg_traj_tl", "mg_traj_adjoint", "mg_time_traj", "mg_traj_record_limit", "mg_traj_checkpoints",
     "mg_autotune", "mg_tune_get", "mg_tune_set", "mg_radix_candidates",
 ]

@@ -47,6 +47,7 @@ struct mg_ctx {
     int k1_nseg = 0;                     // K1 k segments per tile (0: chosen per launch for this grid alone)
     int k2_nseg = 0;                     // K2 likewise
     double traj_rec_limit = -1.;         // bytes the trajectory adjoint's stage records may take (< 0: half the free memory)
+    int traj_ck_where = MG_CKPT_AUTO;    // where the trajectory adjoint keeps its checkpoints (MG_CKPT_*)
     int have_state = 0;
     unsigned up_mask = 0;                // fields uploaded one at a time (bit = MG_FIELD_*) before a full state
     int launches = 0;
@@ -1331,14 +1332,43 @@ NatState nat_alloc(TrajBufs &B, int nf)
     return n;
 }
 
+// page-locked host buffers of field size (checkpoints kept off the device)
+struct HostBufs {
+    size_t bytes = 0;
+    std::vector<double *> own;
+    cudaError_t err = cudaSuccess;
+    double *get()
+    {
+        double *p = nullptr;
+        if (err == cudaSuccess) err = cudaMallocHost(&p, bytes);
+        if (err == cudaSuccess) own.push_back(p);
+        return p;
+    }
+    ~HostBufs()
+    {
+        for (double *p : own) cudaFreeHost(p);
+    }
+};
+
+NatState nat_alloc_host(HostBufs &H, int nf)
+{
+    NatState n;
+    for (int q = 0; q < 3; q++) n.m[q] = H.get();
+    n.p = H.get();
+    for (int f = 0; f < nf; f++) n.s[f] = H.get();
+    return n;
+}
+
+// field-by-field copy on the context stream; either side may be page-locked host memory
+// (the direction follows from the unified address space)
 cudaError_t nat_copy(mg_ctx *c, const NatState &dst, const NatState &src, int nf)
 {
     cudaError_t e = cudaSuccess;
     for (int q = 0; q < 3 && e == cudaSuccess; q++)
-        e = cudaMemcpyAsync(dst.m[q], src.m[q], c->fbytes, cudaMemcpyDeviceToDevice, c->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dst.p, src.p, c->fbytes, cudaMemcpyDeviceToDevice, c->stream);
+        e = cudaMemcpyAsync(dst.m[q], src.m[q], c->fbytes, cudaMemcpyDefault, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dst.p, src.p, c->fbytes, cudaMemcpyDefault, c->stream);
     for (int f = 0; f < nf && e == cudaSuccess; f++)
-        e = cudaMemcpyAsync(dst.s[f], src.s[f], c->fbytes, cudaMemcpyDeviceToDevice, c->stream);
+        e = cudaMemcpyAsync(dst.s[f], src.s[f], c->fbytes, cudaMemcpyDefault, c->stream);
     return e;
 }
 
@@ -1812,17 +1842,28 @@ static int traj_adjoint_run(mg_ctx *c, int nsteps, int ntime0, int ckpt, const d
     for (int q = 0; q < 4; q++) S.W.tmp[q] = T.B.get();
     for (int q = 0; q < 5; q++) S.W.scratch[q] = T.B.get();
     S.pb = T.B.get();
-    // checkpoints (natural states every ckpt steps) and the states of one segment
+    // checkpoints (natural states every ckpt steps) and the states of one segment; the
+    // checkpoints go to page-locked host memory when asked, or (auto) when on the device
+    // they would take more than a quarter of the free memory.  Kernels never read them in
+    // place: they are copied to and from device work states, so both places give the same
+    // gradient bit for bit.
     const int nck = nsteps / ckpt + 1;
     const int nseg = std::max(1, std::min(ckpt, nsteps));   // steps of the longest segment
+    size_t mfree = 0, mtot = 0;
+    CKR(T.B.err);
+    CKR(cudaMemGetInfo(&mfree, &mtot));
+    const double ck_bytes = (double)nck * (4 + nf) * (double)c->fbytes;
+    const bool ck_host = c->traj_ck_where == MG_CKPT_HOST || (c->traj_ck_where == MG_CKPT_AUTO && ck_bytes > 0.25 * (double)mfree);
+    HostBufs H;
+    H.bytes = c->fbytes;
     std::vector<NatState> ck(nck), seg(nseg + 1);
-    for (int q = 0; q < nck; q++) ck[q] = nat_alloc(T.B, nf);
+    for (int q = 0; q < nck; q++) ck[q] = ck_host ? nat_alloc_host(H, nf) : nat_alloc(T.B, nf);
+    if (H.err != cudaSuccess) return cuerr(H.err);
     for (int q = 0; q <= nseg; q++) seg[q] = nat_alloc(T.B, nf);
     NatState bar = nat_alloc(T.B, nf), tmp = nat_alloc(T.B, nf);
     // the stage records of every step of a segment, when they fit in half the free memory:
     // the segment's forward recomputation then leaves them for its backward sweep;
     // otherwise each backward step recomputes its own stages
-    size_t mfree = 0, mtot = 0;
     CKR(T.B.err);
     CKR(cudaMemGetInfo(&mfree, &mtot));
     const double rec_bytes = (double)nseg * 2 * (2 * nf + 3) * (double)c->fbytes;
@@ -1841,19 +1882,22 @@ static int traj_adjoint_run(mg_ctx *c, int nsteps, int ntime0, int ckpt, const d
     TrajTimer tm{c->stream, ms};
     CKR(tm.start());
     // forward sweep: keep every ckpt-th state; with the records kept, the last segment (the
-    // first swept backward) keeps its states and records here and is not recomputed
+    // first swept backward) keeps its states and records here and is not recomputed.  The
+    // steps run between two device work states (tmp, seg[1]), from which each checkpoint
+    // is copied out.
     const int s0_last = nsteps > 0 ? ((nsteps - 1) / ckpt) * ckpt : 0;
+    NatState cur = tmp, nxt = seg[std::min(1, nseg)];
+    CKR(nat_copy(c, cur, ck[0], nf));
     for (int s = 0; s < nsteps; s++) {
         if (keep && s >= s0_last) {
-            if (s == s0_last) CKR(nat_copy(c, seg[0], ck[s0_last / ckpt], nf));
+            if (s == s0_last) CKR(nat_copy(c, seg[0], cur, nf));
             CKR(traj_step_fwd(c, ntime0 + s, seg[s - s0_last], seg[s - s0_last + 1], rec1[s - s0_last],
                               rec2[s - s0_last], T.ts, T.tm, T.au));
             continue;
         }
-        const NatState &from = (s % ckpt == 0) ? ck[s / ckpt] : tmp;
-        NatState to = ((s + 1) % ckpt == 0) ? ck[(s + 1) / ckpt] : seg[0];
-        CKR(traj_step_fwd(c, ntime0 + s, from, to, T.R1, T.R2, T.ts, T.tm, T.au));
-        if ((s + 1) % ckpt != 0) CKR(nat_copy(c, tmp, to, nf));
+        CKR(traj_step_fwd(c, ntime0 + s, cur, nxt, T.R1, T.R2, T.ts, T.tm, T.au));
+        std::swap(cur, nxt);
+        if ((s + 1) % ckpt == 0) CKR(nat_copy(c, ck[(s + 1) / ckpt], cur, nf));
     }
     for (int s0 = s0_last; nsteps > 0 && s0 >= 0; s0 -= ckpt) {
         const int s1 = std::min(s0 + ckpt, nsteps);
@@ -1907,6 +1951,13 @@ extern "C" int mg_traj_adjoint(mg_ctx *c, int nsteps, int ntime0, int ckpt, cons
     if (nsteps < 0 || ckpt < 1 || !lamT || !g0) return MG_ERR_PARAM;
     CKR(cudaSetDevice(c->device));
     return traj_adjoint_run(c, nsteps, ntime0, ckpt, lamT, g0, nullptr, nullptr);
+}
+
+extern "C" int mg_traj_checkpoints(mg_ctx *c, int where)
+{
+    if (!c || where < MG_CKPT_AUTO || where > MG_CKPT_HOST) return MG_ERR_PARAM;
+    c->traj_ck_where = where;
+    return MG_OK;
 }
 
 extern "C" int mg_traj_record_limit(mg_ctx *c, double bytes)

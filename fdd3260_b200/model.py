@@ -346,6 +346,11 @@ class Mimica:
         the free memory; 0: recompute every backward step's stages)."""
         _lib.check(self._L.mg_traj_record_limit(self._h, float(nbytes)), "mg_traj_record_limit")
 
+    def traj_checkpoints(self, where: int) -> None:
+        """Where the trajectory adjoint keeps its checkpoints: _lib.MG_CKPT_DEVICE,
+        MG_CKPT_HOST (page-locked host memory) or MG_CKPT_AUTO (the default)."""
+        _lib.check(self._L.mg_traj_checkpoints(self._h, int(where)), "mg_traj_checkpoints")
+
     def time_traj(self, nsteps: int, ckpt: int, ntime0: int = 1) -> dict:
         """Device times of nsteps of the trajectory composition, its tangent linear and its
         checkpointed adjoint from the resident state (left unchanged)."""

@@ -361,7 +361,8 @@ int mg_qnadv_ad(mg_ctx *ctx, int ntime, const double *mu, const double *mv, cons
  *   mg_traj_adjoint: g0 = (dx(T)/dx(0))^T lamT, the gradient of J = <lamT, x(T)> (interior
  *                    inner product) with respect to x(0); the forward sweep keeps a state
  *                    every ckpt steps and each segment is recomputed before its backward
- *                    sweep: (nsteps/ckpt + ckpt + 4) states of 4 + nf fields (nf = nscal
+ *                    sweep: (nsteps/ckpt + 1) checkpoints (on the device or on the host,
+ *                    mg_traj_checkpoints) and ckpt + 3 states of 4 + nf fields (nf = nscal
  *                    + 1) and ~8 nf + 30 work fields, plus the segment's stage records,
  *                    2 (2 nf + 3) fields per step, when they fit in half the free device
  *                    memory and in mg_traj_record_limit (else each backward step
@@ -375,6 +376,13 @@ int mg_traj_adjoint(mg_ctx *ctx, int nsteps, int ntime0, int ckpt, const double 
  * (bytes < 0: half the free device memory, the default; 0: never keep them, so that
  * every backward step recomputes its stages). */
 int mg_traj_record_limit(mg_ctx *ctx, double bytes);
+/* Where mg_traj_adjoint keeps its checkpoints (the nsteps/ckpt + 1 states of 4 + nf
+ * fields): MG_CKPT_DEVICE, MG_CKPT_HOST (page-locked host memory, copied in and out on
+ * the context stream), or MG_CKPT_AUTO (the default: on the host when on the device they
+ * would take more than a quarter of the free memory).  The gradient does not depend on
+ * the choice. */
+enum { MG_CKPT_AUTO = -1, MG_CKPT_DEVICE = 0, MG_CKPT_HOST = 1 };
+int mg_traj_checkpoints(mg_ctx *ctx, int where);
 /* Device times (ms) of nsteps of mg_traj_forward's composition (out4[0]), of the tangent
  * linear (out4[1]) and of the checkpointed adjoint, forward sweep and recomputation
  * included (out4[2]), from the resident state, which is left unchanged; out4[3] = device

@@ -67,6 +67,7 @@ def test_null_pointers_rejected():
     assert L.mg_traj_tl(None, 1, 1, None, None) == _lib.MG_ERR_PARAM
     assert L.mg_traj_adjoint(None, 1, 1, 1, None, None) == _lib.MG_ERR_PARAM
     assert L.mg_traj_record_limit(None, 0.0) == _lib.MG_ERR_PARAM
+    assert L.mg_traj_checkpoints(None, 1) == _lib.MG_ERR_PARAM
     assert L.mg_time_traj(None, 1, 1, 1, None) == _lib.MG_ERR_PARAM
     assert L.mg_autotune(None, 3, None) == _lib.MG_ERR_PARAM
     assert L.mg_tune_get(None, None) == _lib.MG_ERR_PARAM

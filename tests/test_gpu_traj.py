@@ -126,6 +126,32 @@ def test_checkpoint_interval_does_not_change_gradient():
             assert np.abs(x - y).max() <= 1e-12 * max(np.abs(x).max(), 1e-300)
 
 
+@pytest.mark.parametrize("records", [True, False])
+def test_host_checkpoints_give_the_same_gradient(records):
+    """Checkpoints kept in page-locked host memory (forced) give the gradient the device
+    checkpoints give, bit for bit, with and without the segment's stage records; the
+    dot-product test passes with the host checkpoints."""
+    from fdd3260_b200 import _lib
+    d = config.warm_bubble_domain(24, 24, 12)
+    st = config.warm_bubble_state(d, seed=6, centre=(600.0, 600.0, 250.0), radius=300.0)
+    rng = np.random.default_rng(10)
+    dx0 = _rand_like(st, rng, [0.1, 0.1, 0.05, 1.0, 1e-3, 0.05, 0.01])
+    lam = _rand_like(st, rng, [1.0] * 7)
+    with Mimica(d, nscal=2) as m:
+        m.upload(st)
+        if not records:
+            m.traj_record_limit(0)
+        m.traj_checkpoints(_lib.MG_CKPT_DEVICE)
+        dev = m.traj_adjoint(lam, 6, ckpt=2)
+        m.traj_checkpoints(_lib.MG_CKPT_HOST)
+        host = m.traj_adjoint(lam, 6, ckpt=2)
+        tl = m.traj_tl(dx0, 6)
+    for x, y in zip(_fields(dev), _fields(host)):
+        assert np.array_equal(x, y)
+    lhs, rhs = _dot(tl, lam), _dot(dx0, host)
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), abs(rhs)), (lhs, rhs)
+
+
 def _bump_direction(d):
     """A smooth perturbation of u, v, w and theta (w stays 0 on the ground)."""
     nz, ny, nx = d.shape
