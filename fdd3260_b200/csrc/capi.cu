@@ -1589,7 +1589,6 @@ struct StageAdWork {
     double *abar[3];
     double *Abar[MG_MAXF];
     double *tmp[4];
-    double *scratch[5];
 };
 
 static cudaError_t traj_stage_ad(mg_ctx *c, int ntime, int stage, const NatState &N, const NatState &Nbar,
@@ -1635,7 +1634,7 @@ static cudaError_t traj_stage_ad(mg_ctx *c, int ntime, int stage, const NatState
     if ((e = launch_stage_scal_ad(G, S, c->stream)) != cudaSuccess) return e;
     for (int f = 0; f < nf; f++) {
         if ((e = launch_advection_ad(G, R.xs[f], R.xm[0], R.xm[1], R.xm[2], W.Abar[f], W.tmp[0], W.tmp[1], W.tmp[2],
-                                     W.tmp[3], W.scratch, c->stream)) != cudaSuccess)
+                                     W.tmp[3], c->stream)) != cudaSuccess)
             return e;
         if ((e = launch_axpy(G, xs_in_bar[f], W.tmp[0], 1., c->stream)) != cudaSuccess) return e;
         for (int q = 0; q < 3; q++)
@@ -1840,7 +1839,6 @@ static int traj_adjoint_run(mg_ctx *c, int nsteps, int ntime0, int ckpt, const d
         S.W.Abar[f] = T.B.get(); S.xs2b[f] = T.B.get(); S.xs1b[f] = T.B.get(); S.xs0b[f] = T.B.get(); S.tsc[f] = T.B.get();
     }
     for (int q = 0; q < 4; q++) S.W.tmp[q] = T.B.get();
-    for (int q = 0; q < 5; q++) S.W.scratch[q] = T.B.get();
     S.pb = T.B.get();
     // checkpoints (natural states every ckpt steps) and the states of one segment; the
     // checkpoints go to page-locked host memory when asked, or (auto) when on the device
@@ -2008,13 +2006,12 @@ extern "C" int mg_advection_ad(mg_ctx *c, const double *x, const double *mu, con
     if (!c || !x || !mu || !mv || !mw || !Abar || !xbar || !mubar || !mvbar || !mwbar) return MG_ERR_PARAM;
     if (c->prm.scal_adv != MG_WENO) return MG_ERR_PARAM;
     CKR(cudaSetDevice(c->device));
-    int rc = ensure_unit(c, 14);
+    int rc = ensure_unit(c, 9);
     if (rc) return rc;
     const double *in[5] = {x, mu, mv, mw, Abar};
     for (int q = 0; q < 5; q++) CKR(h2d(c, c->unit[q], in[q], cudaMemcpyHostToDevice));
-    double *scratch[5] = {c->unit[9], c->unit[10], c->unit[11], c->unit[12], c->unit[13]};
     CKR(launch_advection_ad(c->G, c->unit[0], c->unit[1], c->unit[2], c->unit[3], c->unit[4], c->unit[5], c->unit[6],
-                            c->unit[7], c->unit[8], scratch, c->stream));
+                            c->unit[7], c->unit[8], c->stream));
     double *outs[4] = {xbar, mubar, mvbar, mwbar};
     for (int q = 0; q < 4; q++) CKR(d2h(c, outs[q], c->unit[5 + q], cudaMemcpyDeviceToHost));
     return cuerr(cudaStreamSynchronize(c->stream));
@@ -2046,7 +2043,7 @@ extern "C" int mg_time_adjoint(mg_ctx *c, int reps, double *out)
     if (!c->have_state) return MG_ERR_STATE;
     if (c->prm.precision != MG_PREC_FP64 || c->prm.scal_adv != MG_WENO) return MG_ERR_PARAM;
     CKR(cudaSetDevice(c->device));
-    int rc = ensure_unit(c, 14);
+    int rc = ensure_unit(c, 10);
     if (rc) return rc;
     const size_t fb = c->fbytes;
     double **u = c->unit;
@@ -2061,13 +2058,12 @@ extern "C" int mg_time_adjoint(mg_ctx *c, int reps, double *out)
     const double *xv[1] = {u[0]};
     rc = build_maps(c, xv, 1, u[1], u[2], &maps);
     if (rc) return rc;
-    double *scratch[5] = {u[9], u[10], u[11], u[12], u[13]};
     auto run = [&](int which) -> cudaError_t {
         int launches = 0;
         switch (which) {
         case 0: return launch_k1(c->G, a, maps, c->stream);
         case 1: return launch_advection_tl(c->G, u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7], u[8], u[9], c->stream);
-        case 2: return launch_advection_ad(c->G, u[0], u[1], u[2], u[3], u[8], u[4], u[5], u[6], u[7], scratch, c->stream);
+        case 2: return launch_advection_ad(c->G, u[0], u[1], u[2], u[3], u[8], u[4], u[5], u[6], u[7], c->stream);
         case 3: return project(c, u[4], u[5], u[6], u[7], -1, 0, 0, 0, &launches);
         default: return pressure_adjoint(c->G, c->pp, c->prm.nsubp, u[4], u[5], u[6], u[7], c->stream);
         }

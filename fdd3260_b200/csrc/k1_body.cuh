@@ -32,6 +32,7 @@ constexpr int VBOX_SLOT = 2560;
 constexpr int NCELL = TX * TY;
 constexpr int FXN = TY * (TX + 1), FYN = (TY + 1) * TX;   // x faces, y faces of one field
 constexpr int NHALO = SW * SH - TX * TY;          // 276 plane elements outside the cells
+constexpr int K1_FC = 6;                          // field count with kernels of its own (density + 5 scalars)
 
 // fields per group, group slots of planes in flight, face buffers (parity-double-buffered
 // when a group is one field, single otherwise: an extra barrier then guards reuse)
@@ -114,14 +115,16 @@ __device__ __forceinline__ int halo_elem(int h)
 // density); STAGE 0: unit mode (advection_ac of one field, xout := ((xout-Tx)-Ty)-Tz)
 // SGS: the stage adds stored SGS tendencies (A.sgs), loaded one group ahead; a variant of
 // its own so that the kernels without SGS keep their register budget
-template <int SCHEME, bool MIXED, int STAGE, bool SGS>
+// FC: the field count when it is known at compile time (0: A.nf at run time); with it the
+// group loop unrolls and every shared-memory offset of the z-window is a constant
+template <int SCHEME, bool MIXED, int STAGE, bool SGS, int FC = 0>
 __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __grid_constant__ K1Maps M)
 {
     constexpr int PF = k1_pf(SCHEME), NPS = k1_nps(SCHEME), NFB = k1_nfb(SCHEME);
     constexpr bool CONV1 = STAGE == 1;   // stage-1 inputs are natural: psi = s * rho
     extern __shared__ unsigned char smraw[];
     unsigned char *sm = (unsigned char *)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
-    const int F = A.nf;
+    const int F = FC > 0 ? FC : A.nf;
     const Layout Ly = make_layout(SCHEME, F);
     constexpr int ZS = SCHEME == MG_PPM ? 5 : 4;   // z-ring slots
     constexpr int L = SCHEME == MG_PPM ? 3 : 2;    // window x(k-1 .. k+L)
@@ -238,6 +241,7 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
 #pragma unroll
         for (int m = 0; m < L + 2; m++) zsl[m] = (k - 1 + m) % ZS;
         const double d0 = ldg(G.den0, k - 1);
+        const double rd0 = MIXED ? 1. / d0 : 0.;   // the mixed form multiplies by 1/rho0
         // momentum boxes of level k -> face velocities.  Previous readers of su/sv (the
         // faces of iteration k-1) passed that iteration's last face barrier.
         if (!pro) {
@@ -247,18 +251,19 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
                 int r = q / (TX + 1), c = q - r * (TX + 1);
                 double m = vbu[r * VW + c + 1];
                 if (conv1) m = m * d0;
-                su[q] = m / d0 - G.u0shift;
+                su[q] = (MIXED ? m * rd0 : m / d0) - G.u0shift;
             } else {
                 int qq = q - TY * (TX + 1);
                 int r = qq / TX, c = qq - r * TX;
                 double m = vbv[r * VW + c + 1];
                 if (conv1) m = m * d0;
-                sv[qq] = m / d0 - G.v0shift;
+                sv[qq] = (MIXED ? m * rd0 : m / d0) - G.v0shift;
             }
         }
         __syncthreads();   // su/sv complete; the momentum boxes are free again
         if (tid == 0 && k + 1 <= ke) issue_vel(k + 1);
         }
+#pragma unroll 1
         for (int g = 0; g < NG; g++) {
             const int qg = (k - 1) * NG + g, qr = qg - qb, gb = g * PF;
             // this group's stage-2 operands, then the next group's loads (they complete

@@ -103,6 +103,8 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
         mbar_wait_bounded(mbar, (uint32_t)((l - kp) & 1), A.err);
         const int slot = l % NSLOT;
         const double d0 = ldg(G.den0, l - 1), a0 = ldg(G.avden0, l - 1);
+        // the mixed form multiplies by the level's reciprocal densities instead of dividing
+        const double rd0 = MIXED ? 1. / d0 : 0., ra0 = MIXED ? 1. / a0 : 0.;
         for (int q = tid; q < 3 * PL; q += TX * TY) {
             int arr = q / PL, o = q - arr * PL;
             int r = o / PW, c = o - r * PW;
@@ -112,7 +114,7 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
                 double w = arr == 2 ? a0 : d0;
                 double x = stg[arr * (STG_SLOT / 8) + r * SBW + c + 1];
                 mv = A.in_is_leveln ? rep_value(A.rep, x, w) : x;
-                av = mv / w;
+                av = MIXED ? mv * (arr == 2 ? ra0 : rd0) : mv / w;
                 if (arr == 0) av = av - G.u0shift;
                 else if (arr == 1) av = av - G.v0shift;
             }

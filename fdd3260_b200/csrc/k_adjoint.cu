@@ -15,13 +15,14 @@
 // weights are carried on dual numbers.
 //   TL: dA = J (dx, dm), per direction a face pass (each face's tangent flux once) and a
 //       difference pass over the cells.
-//   AD: (xbar, mbar) = J^T Abar, deterministic two-pass form per direction: a face pass
-//       stores Fbar * J per face, a gather pass sums the four faces that read each
-//       cell; the adjoints of the periodic ghost cells are then folded onto the cells
-//       they are images of.
+//   AD: (xbar, mbar) = J^T Abar, deterministic per direction: one kernel computes Fbar * J
+//       of the faces around a tile into shared memory and sums, for each cell of the
+//       tile, the four faces that read it; the adjoints of the periodic ghost cells are
+//       then folded onto the cells they are images of.
 #include "dual.cuh"
 #include "mg_common.cuh"
 #include "mimica_gpu.h"
+#include "weno_partials.cuh"
 
 namespace {
 
@@ -47,12 +48,10 @@ __device__ bool face_jac(const DevGrid &G, int dir, const AdvIn &in, int i, int 
         const double d0 = __ldg(G.den0 + k - 1);
         const double mom = dir == 0 ? __ldg(in.mu + c + 1) : __ldg(in.mv + c + G.px);
         const double shift = dir == 0 ? G.u0shift : G.v0shift;
-        const D5 v = D5::var(mom / d0 - shift, 4);
-        const D5 a = D5::var(__ldg(in.x + c - st), 0), b = D5::var(__ldg(in.x + c), 1);
-        const D5 cc = D5::var(__ldg(in.x + c + st), 2), e = D5::var(__ldg(in.x + c + 2 * st), 3);
-        const D5 F = weno_face_up<D5>(a, b, cc, e, v, true);
-        for (int m = 0; m < 4; m++) J[m] = F.d[m];
-        Jv = F.d[4] / d0;
+        double Ju;
+        weno_face_partials(__ldg(in.x + c - st), __ldg(in.x + c), __ldg(in.x + c + st), __ldg(in.x + c + 2 * st),
+                           mom / d0 - shift, true, J, Ju);
+        Jv = Ju / d0;
         return true;
     }
     const long long c = gidx(G, i, j, k);
@@ -69,9 +68,11 @@ __device__ bool face_jac(const DevGrid &G, int dir, const AdvIn &in, int i, int 
         const D5 cc = D5::var(__ldg(in.x + c + st), 2);
         F = weno_face_top<D5>(a, b, cc, w);
     } else {
-        const D5 a = D5::var(__ldg(in.x + c - st), 0), b = D5::var(__ldg(in.x + c), 1);
-        const D5 cc = D5::var(__ldg(in.x + c + st), 2), e = D5::var(__ldg(in.x + c + 2 * st), 3);
-        F = weno_face_up<D5>(a, b, cc, e, w, k >= 3 && k <= nz - 3);
+        double Ju;
+        weno_face_partials(__ldg(in.x + c - st), __ldg(in.x + c), __ldg(in.x + c + st), __ldg(in.x + c + 2 * st), w.v,
+                           k >= 3 && k <= nz - 3, J, Ju);
+        Jv = Ju / a1;
+        return true;
     }
     for (int m = 0; m < 4; m++) J[m] = F.d[m];
     Jv = F.d[4] / a1;
@@ -119,63 +120,80 @@ __global__ void adv_tl_diff_kernel(DevGrid G, int dir, const double *dF, double 
     dA[c] = first ? -v : dA[c] - v;
 }
 
-// ---- adjoint, face pass of one direction: g[m][face] = Fbar * J[m], gv[face] = Fbar * Jv ----
-__global__ void __launch_bounds__(256, 3) adv_ad_face_kernel(DevGrid G, int dir, AdvIn in, const double *Abar, double *g0, double *g1,
-                                   double *g2, double *g3, double *gv)
-{
-    // faces indexed by their lower cell: x: i in [3, nx-2] (j, k interior); y: j in
-    // [3, ny-2]; z: k in [1, nz-1]
-    const int maxx = G.maxx, maxy = G.maxy, nz = G.nz;
-    const int ni = dir == 0 ? maxx + 1 : maxx, nj = dir == 1 ? maxy + 1 : maxy, nk = dir == 2 ? nz - 1 : nz;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)ni * nj * nk) return;
-    const int i = (int)(t % ni) + (dir == 0 ? 3 : 4), j = (int)((t / ni) % nj) + (dir == 1 ? 3 : 4);
-    const int k = (int)(t / ((long long)ni * nj)) + 1;
-    const long long c = gidx(G, i, j, k);
-    const long long st = dir == 0 ? 1 : (dir == 1 ? G.px : G.ps);
-    auto interior = [&](int ii, int jj, int kk) { return ii >= 4 && ii <= G.nx - 2 && jj >= 4 && jj <= G.ny - 2 && kk >= 1 && kk <= nz; };
-    // A(lower) has -F*metric(lower), A(upper) has +F*metric(upper)
-    const int ui = dir == 0 ? i + 1 : i, uj = dir == 1 ? j + 1 : j, uk = dir == 2 ? k + 1 : k;
-    double Fbar = 0.;
-    if (interior(i, j, k)) Fbar -= Abar[c] * face_metric(G, dir, k);
-    if (interior(ui, uj, uk)) Fbar += Abar[c + st] * face_metric(G, dir, uk);
-    double J[4], Jv;
-    if (!face_jac(G, dir, in, i, j, k, J, Jv)) {
-        J[0] = J[1] = J[2] = J[3] = Jv = 0.;
-    }
-    g0[c] = Fbar * J[0];
-    g1[c] = Fbar * J[1];
-    g2[c] = Fbar * J[2];
-    g3[c] = Fbar * J[3];
-    gv[c] = Fbar * Jv;
-}
+// ---- adjoint of one direction in one pass: face partials and gather per tile ----
+// A tile is LA cells along the direction times LB across it (x: 32 x 8 rows at one level;
+// y: 16 rows x 32 columns at one level; z: 16 levels x 32 columns at one row), over every
+// cell, ghosts included.  Its CTA computes Fbar * J of the LA + 3 faces along each line
+// whose stencil or velocity touches the tile (lower cells a0-2 .. a0+LA; faces that do not
+// exist are zeros) into shared memory, then each cell sums the four faces that read it and
+// the face its velocity carries, as adv_ad_face_kernel + adv_ad_gather_kernel do with the
+// face values in global memory.
+template <int DIR>
+struct AdTile {
+    static constexpr int LA = DIR == 0 ? 32 : 16, LB = DIR == 0 ? 8 : 32, NF = (LA + 3) * LB;
+};
 
-// ---- adjoint, gather pass of one direction over every cell (ghosts included) ----
-__global__ void adv_ad_gather_kernel(DevGrid G, int dir, const double *g0, const double *g1, const double *g2,
-                                     const double *g3, const double *gv, double *xbar, double *mbar)
+template <int DIR>
+__global__ void __launch_bounds__(256) adv_ad_fused_kernel(DevGrid G, AdvIn in, const double *Abar, double *xbar,
+                                                          double *mbar)
 {
+    using T = AdTile<DIR>;
+    __shared__ double gs[5][T::NF];
     const int nx = G.nx, ny = G.ny, nz = G.nz;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)nx * ny * nz) return;
-    const int i = (int)(t % nx) + 1, j = (int)((t / nx) % ny) + 1, k = (int)(t / ((long long)nx * ny)) + 1;
-    const long long c = gidx(G, i, j, k);
-    const long long st = dir == 0 ? 1 : (dir == 1 ? G.px : G.ps);
-    // face with lower cell l exists for: x: l in [3, nx-2], j, k interior; y likewise; z: l in [1, nz-1]
-    auto face_ok = [&](int l) {
-        if (dir == 0) return l >= 3 && l <= nx - 2 && j >= 4 && j <= ny - 2;
-        if (dir == 1) return l >= 3 && l <= ny - 2 && i >= 4 && i <= nx - 2;
-        return l >= 1 && l <= nz - 1 && i >= 4 && i <= nx - 2 && j >= 4 && j <= ny - 2;
+    const int na = DIR == 0 ? nx : (DIR == 1 ? ny : nz), nb = DIR == 0 ? ny : nx;
+    const int ta = (na + T::LA - 1) / T::LA, tb = (nb + T::LB - 1) / T::LB;
+    const int t = blockIdx.x % (ta * tb), fixed = blockIdx.x / (ta * tb) + 1;   // k (x, y) or j (z)
+    const int a0 = 1 + (t % ta) * T::LA, b0 = 1 + (t / ta) * T::LB;
+    const long long sa = DIR == 0 ? 1 : (DIR == 1 ? G.px : G.ps);
+    auto cell = [&](int a, int b, int &i, int &j, int &k) {
+        if (DIR == 0) { i = a; j = b; k = fixed; }
+        else if (DIR == 1) { i = b; j = a; k = fixed; }
+        else { i = b; j = fixed; k = a; }
     };
-    const int p = dir == 0 ? i : (dir == 1 ? j : k);
-    double s = 0.;
-    // cell p is stencil position m of the face with lower cell p + 1 - m
-    if (face_ok(p + 1)) s += g0[c + st];
-    if (face_ok(p)) s += g1[c];
-    if (face_ok(p - 1)) s += g2[c - st];
-    if (face_ok(p - 2)) s += g3[c - 2 * st];
-    xbar[c] += s;
-    // the face with lower cell p-1 is carried by the velocity at index p
-    if (face_ok(p - 1)) mbar[c] += gv[c - st];
+    auto interior = [&](int ii, int jj, int kk) { return ii >= 4 && ii <= nx - 2 && jj >= 4 && jj <= ny - 2 && kk >= 1 && kk <= nz; };
+    for (int q = threadIdx.x; q < T::NF; q += blockDim.x) {
+        // x: consecutive q run along a (x) for coalescing; y/z: along b (x)
+        const int fa = DIR == 0 ? q % (T::LA + 3) : q / T::LB, fb = DIR == 0 ? q / (T::LA + 3) : q % T::LB;
+        const int l = a0 - 2 + fa, bb = b0 + fb;
+        int i, j, k;
+        cell(l, bb, i, j, k);
+        bool ok;
+        if (DIR == 0) ok = l >= 3 && l <= nx - 2 && j >= 4 && j <= ny - 2 && k >= 1 && k <= nz;
+        else if (DIR == 1) ok = l >= 3 && l <= ny - 2 && i >= 4 && i <= nx - 2 && k >= 1 && k <= nz;
+        else ok = l >= 1 && l <= nz - 1 && i >= 4 && i <= nx - 2 && j >= 4 && j <= ny - 2;
+        double g[5] = {0., 0., 0., 0., 0.};
+        if (ok) {
+            const long long c = gidx(G, i, j, k);
+            const int ui = DIR == 0 ? i + 1 : i, uj = DIR == 1 ? j + 1 : j, uk = DIR == 2 ? k + 1 : k;
+            double Fbar = 0.;
+            if (interior(i, j, k)) Fbar -= Abar[c] * face_metric(G, DIR, k);
+            if (interior(ui, uj, uk)) Fbar += Abar[c + sa] * face_metric(G, DIR, uk);
+            double J[4], Jv;
+            if (face_jac(G, DIR, in, i, j, k, J, Jv)) {
+                for (int m = 0; m < 4; m++) g[m] = Fbar * J[m];
+                g[4] = Fbar * Jv;
+            }
+        }
+        for (int m = 0; m < 5; m++) gs[m][q] = g[m];
+    }
+    __syncthreads();
+    // face (lower cell l, cross index fb) sits at smem index face_at(l - (a0 - 2), fb)
+    auto face_at = [&](int fa, int fb) { return DIR == 0 ? fb * (T::LA + 3) + fa : fa * T::LB + fb; };
+    for (int q = threadIdx.x; q < T::LA * T::LB; q += blockDim.x) {
+        const int ca = DIR == 0 ? q % T::LA : q / T::LB, cb = DIR == 0 ? q / T::LA : q % T::LB;
+        const int p = a0 + ca, bb = b0 + cb;
+        if (p > na || bb > nb) continue;
+        int i, j, k;
+        cell(p, bb, i, j, k);
+        const long long c = gidx(G, i, j, k);
+        // cell p is stencil position m of the face with lower cell p + 1 - m
+        const int f0 = p + 1 - (a0 - 2);
+        const double s = ((gs[0][face_at(f0, cb)] + gs[1][face_at(f0 - 1, cb)]) + gs[2][face_at(f0 - 2, cb)]) +
+                         gs[3][face_at(f0 - 3, cb)];
+        xbar[c] += s;
+        // the face with lower cell p-1 is carried by the velocity at index p
+        mbar[c] += gs[4][face_at(f0 - 2, cb)];
+    }
 }
 
 // adjoint of the periodic ghost images: ghost columns then ghost rows are added onto
@@ -228,10 +246,10 @@ cudaError_t launch_advection_tl(const DevGrid &g, const double *x, const double 
     return cudaSuccess;
 }
 
-// xbar, mubar, mvbar, mwbar are overwritten; scratch: 5 fields
+// xbar, mubar, mvbar, mwbar are overwritten
 cudaError_t launch_advection_ad(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
                                 const double *Abar, double *xbar, double *mubar, double *mvbar, double *mwbar,
-                                double *const *scratch, cudaStream_t s)
+                                cudaStream_t s)
 {
     const size_t fbytes = (size_t)g.ps * g.nz * 8;
     cudaError_t e;
@@ -239,19 +257,15 @@ cudaError_t launch_advection_ad(const DevGrid &g, const double *x, const double 
     for (int q = 0; q < 4; q++)
         if ((e = cudaMemsetAsync(outs[q], 0, fbytes, s)) != cudaSuccess) return e;
     const AdvIn in{x, mu, mv, mw};
-    const long long ncell = (long long)g.nx * g.ny * g.nz;
-    for (int dir = 0; dir < 3; dir++) {
-        // every face entry the gather reads is written by the face pass: no clearing
-        const long long nf = (long long)(dir == 0 ? g.maxx + 1 : g.maxx) * (dir == 1 ? g.maxy + 1 : g.maxy) *
-                             (dir == 2 ? g.nz - 1 : g.nz);
-        adv_ad_face_kernel<<<nblk(nf), 256, 0, s>>>(g, dir, in, Abar, scratch[0], scratch[1], scratch[2], scratch[3],
-                                                    scratch[4]);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        double *mb = dir == 0 ? mubar : (dir == 1 ? mvbar : mwbar);
-        adv_ad_gather_kernel<<<nblk(ncell), 256, 0, s>>>(g, dir, scratch[0], scratch[1], scratch[2], scratch[3],
-                                                         scratch[4], xbar, mb);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    }
+    auto tiles = [&](int na, int la, int nb, int lb, int nfix) {
+        return (unsigned)(((na + la - 1) / la) * ((nb + lb - 1) / lb) * nfix);
+    };
+    adv_ad_fused_kernel<0><<<tiles(g.nx, AdTile<0>::LA, g.ny, AdTile<0>::LB, g.nz), 256, 0, s>>>(g, in, Abar, xbar, mubar);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    adv_ad_fused_kernel<1><<<tiles(g.ny, AdTile<1>::LA, g.nx, AdTile<1>::LB, g.nz), 256, 0, s>>>(g, in, Abar, xbar, mvbar);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    adv_ad_fused_kernel<2><<<tiles(g.nz, AdTile<2>::LA, g.nx, AdTile<2>::LB, g.ny), 256, 0, s>>>(g, in, Abar, xbar, mwbar);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     for (int q = 0; q < 4; q++) {
         fold_x_kernel<<<nblk(5LL * g.ny * g.nz), 256, 0, s>>>(g, outs[q]);
         fold_y_kernel<<<nblk(5LL * g.nx * g.nz), 256, 0, s>>>(g, outs[q]);

@@ -17,6 +17,8 @@ cudaError_t launch_one(const DevGrid &g, const K1Args &a, const K1Maps &maps, si
     for (int f = 0; f < a.nf; f++) sgs = sgs || a.sgs[f] != nullptr;
     if (STAGE != 0 && sgs)
         k1_kernel<SCHEME, false, STAGE, true><<<dim3(ntx * nty * as.nseg), dim3(TX, TY + 1), sm, s>>>(g, as, maps);
+    else if (STAGE != 0 && a.nf == K1_FC)   // density + 5 scalars: the field count compiled in
+        k1_kernel<SCHEME, false, STAGE, false, K1_FC><<<dim3(ntx * nty * as.nseg), dim3(TX, TY + 1), sm, s>>>(g, as, maps);
     else
         k1_kernel<SCHEME, false, STAGE, false><<<dim3(ntx * nty * as.nseg), dim3(TX, TY + 1), sm, s>>>(g, as, maps);
     return cudaGetLastError();
@@ -37,6 +39,8 @@ cudaError_t init_scheme()
     if ((e = cudaFuncSetAttribute(k1_kernel<SCHEME, false, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k1_kernel<SCHEME, false, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k1_kernel<SCHEME, false, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k1_kernel<SCHEME, false, 1, false, K1_FC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k1_kernel<SCHEME, false, 2, false, K1_FC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)) != cudaSuccess) return e;
     return cudaFuncSetAttribute(k1_kernel<SCHEME, false, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
 }
 }  // namespace

@@ -217,7 +217,7 @@ cudaError_t launch_advection_tl(const DevGrid &g, const double *x, const double 
                                 double *scratch, cudaStream_t s);
 cudaError_t launch_advection_ad(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
                                 const double *Abar, double *xbar, double *mubar, double *mvbar, double *mwbar,
-                                double *const *scratch, cudaStream_t s);
+                                cudaStream_t s);
 
 // projection
 struct PressurePlan;

@@ -6,35 +6,35 @@
 #pragma once
 #include <cuda_runtime.h>
 
-template <typename T> __device__ __forceinline__ T tmin(T a, T b) { return a < b ? a : b; }
-template <typename T> __device__ __forceinline__ T tmax(T a, T b) { return a > b ? a : b; }
-__device__ __forceinline__ double dabs(double a) { return fabs(a); }
-__device__ __forceinline__ float dabs(float a) { return fabsf(a); }
-__device__ __forceinline__ double sign1(double b) { return copysign(1.0, b); }
-__device__ __forceinline__ float sign1(float b) { return copysignf(1.0f, b); }
+template <typename T> __host__ __device__ __forceinline__ T tmin(T a, T b) { return a < b ? a : b; }
+template <typename T> __host__ __device__ __forceinline__ T tmax(T a, T b) { return a > b ? a : b; }
+__host__ __device__ __forceinline__ double dabs(double a) { return fabs(a); }
+__host__ __device__ __forceinline__ float dabs(float a) { return fabsf(a); }
+__host__ __device__ __forceinline__ double sign1(double b) { return copysign(1.0, b); }
+__host__ __device__ __forceinline__ float sign1(float b) { return copysignf(1.0f, b); }
 
 // RN(a/b) > thr for b > 0, decided without the division when a lies clearly on one
 // side of thr*b (a relative band of 1e-7 around thr); bit-identical to the division.
-template <typename T> __device__ __forceinline__ bool ratio_gt(T a, T b, T thr);
-template <> __device__ __forceinline__ bool ratio_gt<double>(double a, double b, double thr)
+template <typename T> __host__ __device__ __forceinline__ bool ratio_gt(T a, T b, T thr);
+template <> __host__ __device__ __forceinline__ bool ratio_gt<double>(double a, double b, double thr)
 {
     if (a > b * (thr * 1.0000001)) return true;
     if (a < b * (thr * 0.9999999)) return false;
     return a / b > thr;
 }
-template <> __device__ __forceinline__ bool ratio_gt<float>(float a, float b, float thr) { return a > thr * b; }
+template <> __host__ __device__ __forceinline__ bool ratio_gt<float>(float a, float b, float thr) { return a > thr * b; }
 
 // min(|num/den|, 1) of the positivity limiters: 1 exactly whenever |num| >= |den|
 // (then |num/den| >= 1 and its rounding too, or the quotient is inf/NaN and min()
 // returns 1), so the division is only evaluated when it can matter.
-template <typename T> __device__ __forceinline__ T min_abs_ratio_1(T num, T den);
-template <> __device__ __forceinline__ double min_abs_ratio_1<double>(double num, double den)
+template <typename T> __host__ __device__ __forceinline__ T min_abs_ratio_1(T num, T den);
+template <> __host__ __device__ __forceinline__ double min_abs_ratio_1<double>(double num, double den)
 {
     if (fabs(num) >= fabs(den)) return 1.;
     const double q = fabs(num / den);
     return q < 1. ? q : 1.;
 }
-template <> __device__ __forceinline__ float min_abs_ratio_1<float>(float num, float den)
+template <> __host__ __device__ __forceinline__ float min_abs_ratio_1<float>(float num, float den)
 {
     if (fabsf(num) >= fabsf(den)) return 1.f;
     const float q = fabsf(num / den);
@@ -60,7 +60,7 @@ template <> __device__ __forceinline__ float min_abs_ratio_1<float>(float num, f
 // zero either way, and on dual numbers (whose |u| has slope +1 at 0) the left side's
 // term 0.5*Fl*(u+|u|) is the one whose derivative, Fl*du, the two-sided form has.
 template <typename T>
-__device__ __forceinline__ T weno_face_up(T xm1, T x0, T xp1, T xp2, T uu, bool full_weights)
+__host__ __device__ __forceinline__ T weno_face_up(T xm1, T x0, T xp1, T xp2, T uu, bool full_weights)
 {
     const T eps = T(1.e-15), g1 = T(1.) / T(3.), g2 = T(2.) / T(3.), thres = T(20.);
     T ffim1 = (-(T(0.5) * xm1) + T(1.5) * x0);
@@ -88,7 +88,7 @@ __device__ __forceinline__ T weno_face_up(T xm1, T x0, T xp1, T xp2, T uu, bool 
 }
 // vertical bottom face (k=1), :232-241
 template <typename T>
-__device__ __forceinline__ T weno_face_bottom(T x1, T x2, T x3, T ww)
+__host__ __device__ __forceinline__ T weno_face_bottom(T x1, T x2, T x3, T ww)
 {
     const T g1 = T(1.) / T(3.), g2 = T(2.) / T(3.);
     T ffip1p = (T(0.5) * x1 + T(0.5) * x2);
@@ -100,7 +100,7 @@ __device__ __forceinline__ T weno_face_bottom(T x1, T x2, T x3, T ww)
 }
 // vertical top face (k=nz-1), :262-271
 template <typename T>
-__device__ __forceinline__ T weno_face_top(T xm1, T x0, T xp1, T ww)
+__host__ __device__ __forceinline__ T weno_face_top(T xm1, T x0, T xp1, T ww)
 {
     const T g1 = T(1.) / T(3.), g2 = T(2.) / T(3.);
     T ffim1 = (-(T(0.5) * xm1) + T(1.5) * x0);
@@ -116,7 +116,7 @@ __device__ __forceinline__ T weno_face_top(T xm1, T x0, T xp1, T ww)
 // muscl_phi(.., ffip1, ffip2); the reference's two sides are the same expressions on
 // their own slope.
 template <typename T>
-__device__ __forceinline__ T muscl_phi(int lim, T lim_tol, T xx, T ffip1, T ffo)
+__host__ __device__ __forceinline__ T muscl_phi(int lim, T lim_tol, T xx, T ffip1, T ffo)
 {
     T r = T(1.);
     if (dabs(ffo) > lim_tol * dabs(xx) && dabs(ffip1) < dabs(ffo) / lim_tol) r = ffip1 / ffo;
@@ -134,7 +134,7 @@ __device__ __forceinline__ T muscl_phi(int lim, T lim_tol, T xx, T ffip1, T ffo)
 
 // horizontal face between i and i+1 (advq_muscl.f90:81-100); d = dx, d1 = 1/dx
 template <typename T>
-__device__ __forceinline__ T muscl_face_h(int lim, T lim_tol, T d, T d1, T xm1, T x0, T xp1, T xp2, T uu)
+__host__ __device__ __forceinline__ T muscl_face_h(int lim, T lim_tol, T d, T d1, T xm1, T x0, T xp1, T xp2, T uu)
 {
     const T eps = T(1.e-18);
     T slope_p = (xp1 - x0) * d1;
@@ -155,7 +155,7 @@ __device__ __forceinline__ T muscl_face_h(int lim, T lim_tol, T d, T d1, T xm1, 
 // xm1..xp2 = x(k-1..k+2); d1m = dz1(k-1), d10 = dz1(k), d1p = dz1(k+1); fm = fdz0(k-1),
 // fp = fdz0(k+1); dzw1 = dz1w(k).
 template <typename T>
-__device__ __forceinline__ T muscl_face_z(int kind, int lim, T lim_tol, T dz, T xm1, T x0, T xp1, T xp2,
+__host__ __device__ __forceinline__ T muscl_face_z(int kind, int lim, T lim_tol, T dz, T xm1, T x0, T xp1, T xp2,
                                           T d1m, T d10, T d1p, T fm, T fp, T dzw1, T ww)
 {
     const T eps = T(1.e-18);
@@ -191,7 +191,7 @@ __device__ __forceinline__ T muscl_face_z(int kind, int lim, T lim_tol, T dz, T 
 
 // ---------------- lw: src/TOOLS/advq_lw.f90 (limiter 'MC', the module constant) ----------------
 template <typename T>
-__device__ __forceinline__ void lw_limiter(T lim_tol, T xx, T ffip1, T ffip2, T ffim1, T &phir, T &phil)
+__host__ __device__ __forceinline__ void lw_limiter(T lim_tol, T xx, T ffip1, T ffip2, T ffim1, T &phir, T &phil)
 {
     const T eps = T(1.e-18);
     T rp1 = T(1.), rp2 = T(1.);
@@ -203,7 +203,7 @@ __device__ __forceinline__ void lw_limiter(T lim_tol, T xx, T ffip1, T ffip2, T 
 
 // horizontal face between i and i+1 (advq_lw.f90:82-101); d1 = 1/dx
 template <typename T>
-__device__ __forceinline__ T lw_face_h(T lim_tol, T dt0, T d1, T xm1, T x0, T xp1, T xp2, T uu)
+__host__ __device__ __forceinline__ T lw_face_h(T lim_tol, T dt0, T d1, T xm1, T x0, T xp1, T xp2, T uu)
 {
     const T eps = T(1.e-18);
     const T ffip1 = xp1 - x0, ffim1 = x0 - xm1, ffip2 = xp2 - xp1;
@@ -224,7 +224,7 @@ __device__ __forceinline__ T lw_face_h(T lim_tol, T dt0, T d1, T xm1, T x0, T xp
 // vertical face k+1/2 (advq_lw.f90:246-311).  kind: 0 core, 1 bottom (k=1, ffim1 = ffip1),
 // 2 top (k=nz-1, ffip2 = ffip1).  d1m, d10, d1p = dz1(k-1), dz1(k), dz1(k+1); dzw1 = dz1w(k).
 template <typename T>
-__device__ __forceinline__ T lw_face_z(int kind, T lim_tol, T dz, T dt0, T xm1, T x0, T xp1, T xp2,
+__host__ __device__ __forceinline__ T lw_face_z(int kind, T lim_tol, T dz, T dt0, T xm1, T x0, T xp1, T xp2,
                                        T d1m, T d10, T d1p, T dzw1, T ww)
 {
     const T eps = T(1.e-18);
@@ -247,7 +247,7 @@ __device__ __forceinline__ T lw_face_z(int kind, T lim_tol, T dz, T dt0, T xm1, 
 
 // ---------------- QUICK: src/TOOLS/advq_quick.f90 ----------------
 template <typename T>
-__device__ __forceinline__ void quick_limiter(T lim_tol, T phic, T ffip1, T ffip2, T ffim1, T &phil, T &phir)
+__host__ __device__ __forceinline__ void quick_limiter(T lim_tol, T phic, T ffip1, T ffip2, T ffim1, T &phil, T &phir)
 {
     const T eps = T(1.e-18);
     const T c1 = T(1.) / T(3.);
@@ -269,7 +269,7 @@ __device__ __forceinline__ void quick_limiter(T lim_tol, T phic, T ffip1, T ffip
 
 // horizontal face between i and i+1 (advq_quick.f90:79-93)
 template <typename T>
-__device__ __forceinline__ T quick_face_h(T lim_tol, T xm1, T x0, T xp1, T xp2, T uu)
+__host__ __device__ __forceinline__ T quick_face_h(T lim_tol, T xm1, T x0, T xp1, T xp2, T uu)
 {
     const T ffip1 = xp1 - x0, ffip2 = xp2 - xp1, ffim1 = x0 - xm1;
     T phil, phir;
@@ -281,7 +281,7 @@ __device__ __forceinline__ T quick_face_h(T lim_tol, T xm1, T x0, T xp1, T xp2, 
 
 // vertical face k+1/2 (advq_quick.f90:235-279), kinds and arguments as lw_face_z
 template <typename T>
-__device__ __forceinline__ T quick_face_z(int kind, T lim_tol, T dz, T xm1, T x0, T xp1, T xp2, T d1m, T d10,
+__host__ __device__ __forceinline__ T quick_face_z(int kind, T lim_tol, T dz, T xm1, T x0, T xp1, T xp2, T d1m, T d10,
                                           T d1p, T dzw1, T ww)
 {
     const T ffip1 = (xp1 - x0) * d10;
@@ -315,7 +315,7 @@ __device__ __forceinline__ float tsqrt(float x) { return sqrtf(x); }
 
 // limiter_ppm :449-530 with ppmlimiter='PPM'
 template <typename T>
-__device__ __forceinline__ void ppm_limiter(T xx, T xp, T xm, T xplus, T xmin, T ffip1, T ffip2, T ffim1,
+__host__ __device__ __forceinline__ void ppm_limiter(T xx, T xp, T xm, T xplus, T xmin, T ffip1, T ffip2, T ffim1,
                                             T ffim2, T &phir, T &phil, T &phi1, T &phi2)
 {
     const T eps = T(1.e-15), thres = T(10.);
@@ -362,7 +362,7 @@ __device__ __forceinline__ void ppm_limiter(T xx, T xp, T xm, T xplus, T xmin, T
 
 // uniform-grid face value xplus of cell i (advq_ppm.f90:108-110)
 template <typename T>
-__device__ __forceinline__ T ppm_xplus_core(T xm1, T x0, T xp1, T xp2)
+__host__ __device__ __forceinline__ T ppm_xplus_core(T xm1, T x0, T xp1, T xp2)
 {
     T ffip1 = (xp1 - x0), ffip2 = (xp2 - xp1), ffim1 = (x0 - xm1);
     T sl = T(0.5) * (ffip1 + ffim1);
@@ -371,9 +371,9 @@ __device__ __forceinline__ T ppm_xplus_core(T xm1, T x0, T xp1, T xp2)
 }
 
 // Courant-number fluxes (advq_ppm.f90:93-94)
-template <typename T> __device__ __forceinline__ T ppm_fr(T phir, T mup, T phi1, T phi2)
+template <typename T> __host__ __device__ __forceinline__ T ppm_fr(T phir, T mup, T phi1, T phi2)
 { return phir - T(0.5) * mup * (phi1 + (T(1.) - T(2.) / T(3.) * mup) * phi2); }
-template <typename T> __device__ __forceinline__ T ppm_fl(T phil, T muc, T phi1, T phi2)
+template <typename T> __host__ __device__ __forceinline__ T ppm_fl(T phil, T muc, T phi1, T phi2)
 { return phil + T(0.5) * muc * (phi1 - (T(1.) - T(2.) / T(3.) * muc) * phi2); }
 
 // Horizontal cell reconstruction of cell c, pencil of length n (1-based).
@@ -383,7 +383,7 @@ template <typename T> __device__ __forceinline__ T ppm_fl(T phil, T muc, T phi1,
 // xmin of a cell is the unlimited xplus of the cell before it (:98,117).
 // Returns phir, phil, phi1, phi2 (the velocity-independent part).
 template <typename T>
-__device__ __forceinline__ void ppm_cell_h(int kind, const T *xv, T &phir, T &phil, T &phi1, T &phi2)
+__host__ __device__ __forceinline__ void ppm_cell_h(int kind, const T *xv, T &phir, T &phil, T &phi1, T &phi2)
 {
     T xm2 = xv[0], xm1 = xv[1], x0 = xv[2], xp1 = xv[3], xp2 = xv[4];
     T ffip1, ffip2, ffim1, ffim2, xplus, xmin;
@@ -415,7 +415,7 @@ __device__ __forceinline__ void ppm_cell_h(int kind, const T *xv, T &phir, T &ph
 
 // Stretched-grid face value of cell k (advq_ppm.f90:374-383); dm1..dp2 = dz1w(k-1..k+2)
 template <typename T>
-__device__ __forceinline__ T ppm_xplus_z(T x0, T ffip1, T ffip2, T ffim1, T deltam1, T delta, T deltap1, T deltap2)
+__host__ __device__ __forceinline__ T ppm_xplus_z(T x0, T ffip1, T ffip2, T ffim1, T deltam1, T delta, T deltap1, T deltap2)
 {
     T sl = delta / (deltam1 + delta + deltap1) *
            ((T(2.) * deltam1 + delta) / (deltap1 + delta) * ffip1 + (delta + T(2.) * deltap1) / (deltam1 + delta) * ffim1);

@@ -118,6 +118,21 @@ def test_step_parity_moist_stretched():
     _compare_states(g, r)
 
 
+@pytest.mark.parametrize("scheme", ["weno", "ppm", "muscl", "lw", "quick"])
+def test_step_parity_six_fields(scheme):
+    """Density + 5 scalars, the bench's field count, whose scalar-advection kernels are
+    compiled with the field count built in."""
+    d = config.cumulus_domain(32, 32, 24, scheme=scheme)
+    st = config.cumulus_state(d, seed=1001, n_extra=3)
+    assert 1 + len(st.scal) == 6
+    with Mimica(d, nscal=len(st.scal), iqt=1) as m:
+        m.upload(st)
+        m.stepping(2, ntime0=1)
+        g = m.download()
+    r, _, _ = O.Oracle(d).stepping(st, nsteps=2, ntime0=1)
+    _compare_states(g, r)
+
+
 def test_warm_bubble_64cubed_10_steps():
     """The CPU-runnable configuration: 64^3 warm bubble, WENO, 10 steps, dt = 0.5 s."""
     d = config.warm_bubble_domain(64, 64, 64, scheme="weno")
