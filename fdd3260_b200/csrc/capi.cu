@@ -775,10 +775,11 @@ extern "C" int mg_step_graph(mg_ctx *c, int nsteps, int ntime0, double *maxdiv, 
         rc = mg_step(c, nsteps - s, ntime0 + s, maxdiv, p1);
         if (rc) return rc;
     } else if (maxdiv || p1) {
-        // diagnostics of the final state
+        // diagnostics of the final state: the level-n buffers hold velocities, whose
+        // momentum the residual is the divergence of
         const DevGrid &G = c->G;
         if (maxdiv) {
-            CKR(launch_maxdiv(G, c->pp, c->mA[0], c->mA[1], c->mA[2], c->stream));
+            CKR(launch_maxdiv(G, c->pp, c->mA[0], c->mA[1], c->mA[2], c->stream, 1));
             CKR(cudaMemcpyAsync(maxdiv, pressure_maxdiv_dev(c->pp), 8, cudaMemcpyDeviceToHost, c->stream));
         }
         if (p1) memset(p1, 0, sizeof(double) * G.nz);

@@ -49,7 +49,9 @@ __device__ __forceinline__ double ldg(const double *p, long long i) { return __l
 __device__ __forceinline__ double abs_r(double x) { return fabs(x); }
 __device__ __forceinline__ float abs_r(float x) { return fabsf(x); }
 
-template <bool MIXED>
+// EVEN: the parity of ntime (the direction order of windadv.f90:103,158), so that each
+// instantiation evaluates the three directions as straight-line code
+template <bool MIXED, bool EVEN>
 __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const __grid_constant__ K2Maps M)
 {
     // R: type of the stencil arithmetic (FP64 plain form, FP32 mixed form)
@@ -154,7 +156,6 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
     R fzu0 = 0, fzu1 = 0, fzu2 = 0, fzu3 = 0, fzv0 = 0, fzv1 = 0, fzv2 = 0, fzv3 = 0;
     R fzw0 = 0, fzw1 = 0, azw0 = 0, azw1 = 0, azw2 = 0;
     double pp_below = 0.;
-    const bool even = (A.ntime % 2) == 0;
     const double grav = 9.81, epsm = 0.60243, cdiag = 0.5;
     const int own = (ty + RH) * PW + (tx + RH);
 
@@ -257,9 +258,8 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
 
         // ---------------- u component ----------------
         double au = 0.;
-        for (int pass = 0; pass < 3; pass++) {
-            int dir = even ? pass : 2 - pass;
-            if (dir == 0) {   // advux_fd
+        {
+            auto dx_ = [&]() {   // advux_fd
 #define FX(p) (((AA(0, 0, (p) + 1, 0) + AA(0, 0, (p), 0)) * HALF) * ((MM(0, 0, (p) + 1, 0) + MM(0, 0, (p), 0)) * HALF))
 #define AX(p) (((AA(0, 0, (p) + 2, 0) + AA(0, 0, (p), 0)) * HALF) * ((MM(0, 0, (p) + 2, 0) + MM(0, 0, (p), 0)) * HALF))
                 ACC2(au, c1a * (FX(0) - FX(-1)) * dx1, c2a * (AX(0) - AX(-2)) * dx2);
@@ -269,7 +269,8 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
                     const R mu = abs_r(AA(0, 0, 0, 0)) * dx1;
                     SUB1(au, AVR * mu * (-MM(0, 0, 2, 0) + FOUR * MM(0, 0, 1, 0) - SIX * MM(0, 0, 0, 0) + FOUR * MM(0, 0, -1, 0) - MM(0, 0, -2, 0)));
                 }
-            } else if (dir == 1) {   // advuy_fd: vt1=vt(i-1), vt2=vt(i), vt3=vt(i-2), vt4=vt(i+1)
+            };
+            auto dy_ = [&]() {   // advuy_fd: vt1=vt(i-1), vt2=vt(i), vt3=vt(i-2), vt4=vt(i+1)
 #define FY(p) ((c1b * (AA(1, 0, -1, (p) + 1) + AA(1, 0, 0, (p) + 1)) * HALF - c2b * (AA(1, 0, -2, (p) + 1) + AA(1, 0, 1, (p) + 1)) * HALF) * \
                ((MM(0, 0, 0, (p) + 1) + MM(0, 0, 0, (p))) * HALF))
                 ACC2(au, c1b * (FY(0) - FY(-1)) * dy1, c2b * (FY(1) - FY(-2)) * dy3);
@@ -278,7 +279,8 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
                     const R mu = QUART * abs_r(AA(1, 0, -1, 0) + AA(1, 0, 0, 0) + AA(1, 0, -1, 1) + AA(1, 0, 0, 1)) * dy1;
                     SUB1(au, AVR * mu * (-MM(0, 0, 0, 2) + FOUR * MM(0, 0, 0, 1) - SIX * MM(0, 0, 0, 0) + FOUR * MM(0, 0, 0, -1) - MM(0, 0, 0, -2)));
                 }
-            } else {   // advuz_fd, Flux(k-2..k+1) = fzu0..fzu3
+            };
+            auto dz_ = [&]() {   // advuz_fd, Flux(k-2..k+1) = fzu0..fzu3
                 if (k >= 3 && k <= nz - 1)
                     ACC2(au, c1b * (fzu2 - fzu1) * ZW1(k), c2b * (fzu3 - fzu0) / (ZW(k - 1) + ZW(k) + ZW(k + 1)));
                 else if (k == 1)
@@ -291,14 +293,14 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
                     const R mu = QUART * abs_r(AA(2, 0, -1, 0) + AA(2, 0, 0, 0) + AA(2, 1, -1, 0) + AA(2, 1, 0, 0)) * ZW1(k);
                     SUB1(au, AVR * mu * (-MM(0, 2, 0, 0) + FOUR * MM(0, 1, 0, 0) - SIX * MM(0, 0, 0, 0) + FOUR * MM(0, -1, 0, 0) - MM(0, -2, 0, 0)));
                 }
-            }
+            };
+            // the reference's direction order, which alternates with ntime's parity
+            if constexpr (EVEN) { dx_(); dy_(); dz_(); } else { dz_(); dy_(); dx_(); }
         }
-
         // ---------------- v component ----------------
         double av = 0.;
-        for (int pass = 0; pass < 3; pass++) {
-            int dir = even ? pass : 2 - pass;
-            if (dir == 0) {   // advvx_fd: ut1=ut(j-1), ut2=ut(j), ut3=ut(j-2), ut4=ut(j+1)
+        {
+            auto dx_ = [&]() {   // advvx_fd: ut1=ut(j-1), ut2=ut(j), ut3=ut(j-2), ut4=ut(j+1)
 #define FX(p) ((c1b * (AA(0, 0, (p) + 1, -1) + AA(0, 0, (p) + 1, 0)) * HALF - c2b * (AA(0, 0, (p) + 1, -2) + AA(0, 0, (p) + 1, 1)) * HALF) * \
                ((MM(1, 0, (p) + 1, 0) + MM(1, 0, (p), 0)) * HALF))
                 ACC2(av, c1b * (FX(0) - FX(-1)) * dx1, c2b * (FX(1) - FX(-2)) * dx3);
@@ -307,7 +309,8 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
                     const R mu = QUART * abs_r(AA(0, 0, 0, -1) + AA(0, 0, 0, 0) + AA(0, 0, 1, -1) + AA(0, 0, 1, 0)) * dx1;
                     SUB1(av, AVR * mu * (-MM(1, 0, 2, 0) + FOUR * MM(1, 0, 1, 0) - SIX * MM(1, 0, 0, 0) + FOUR * MM(1, 0, -1, 0) - MM(1, 0, -2, 0)));
                 }
-            } else if (dir == 1) {   // advvy_fd
+            };
+            auto dy_ = [&]() {   // advvy_fd
 #define FY(p) (((AA(1, 0, 0, (p) + 1) + AA(1, 0, 0, (p))) * HALF) * ((MM(1, 0, 0, (p) + 1) + MM(1, 0, 0, (p))) * HALF))
 #define AY(p) (((AA(1, 0, 0, (p) + 2) + AA(1, 0, 0, (p))) * HALF) * ((MM(1, 0, 0, (p) + 2) + MM(1, 0, 0, (p))) * HALF))
                 ACC2(av, c1a * (FY(0) - FY(-1)) * dy1, c2a * (AY(0) - AY(-2)) * dy2);
@@ -317,7 +320,8 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
                     const R mu = abs_r(AA(1, 0, 0, 0)) * dy1;
                     SUB1(av, AVR * mu * (-MM(1, 0, 0, 2) + FOUR * MM(1, 0, 0, 1) - SIX * MM(1, 0, 0, 0) + FOUR * MM(1, 0, 0, -1) - MM(1, 0, 0, -2)));
                 }
-            } else {   // advvz_fd, Flux(k-2..k+1) = fzv0..fzv3
+            };
+            auto dz_ = [&]() {   // advvz_fd, Flux(k-2..k+1) = fzv0..fzv3
                 if (k >= 3 && k <= nz - 1)
                     ACC2(av, c1b * (fzv2 - fzv1) * ZW1(k), c2b * (fzv3 - fzv0) / (ZW(k - 1) + ZW(k) + ZW(k + 1)));
                 else if (k == 1)
@@ -330,15 +334,15 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
                     const R mu = QUART * abs_r(AA(2, 0, 0, -1) + AA(2, 0, 0, 0) + AA(2, 1, 0, -1) + AA(2, 1, 0, 0)) * ZW1(k);
                     SUB1(av, AVR * mu * (-MM(1, 2, 0, 0) + FOUR * MM(1, 1, 0, 0) - SIX * MM(1, 0, 0, 0) + FOUR * MM(1, -1, 0, 0) - MM(1, -2, 0, 0)));
                 }
-            }
+            };
+            // the reference's direction order, which alternates with ntime's parity
+            if constexpr (EVEN) { dx_(); dy_(); dz_(); } else { dz_(); dy_(); dx_(); }
         }
-
         // ---------------- w component (k >= 2) ----------------
         double aw = 0.;
         if (k >= 2) {
-            for (int pass = 0; pass < 3; pass++) {
-                int dir = even ? pass : 2 - pass;
-                if (dir == 0) {   // advwx_fd
+            {
+                auto dx_ = [&]() {   // advwx_fd
 #define HV(p, d) AA(0, d, p, 0)
 #define WV(p) MM(2, 0, p, 0)
 #define FH(p) ((k == 2 ? (HV((p) + 1, 0) + HV((p) + 1, -1)) * HALF                                            \
@@ -353,7 +357,8 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
                     }
 #undef HV
 #undef WV
-                } else if (dir == 1) {   // advwy_fd
+                };
+                auto dy_ = [&]() {   // advwy_fd
 #define HV(p, d) AA(1, d, 0, p)
 #define WV(p) MM(2, 0, 0, p)
                     ACC2(aw, c1b * (FH(0) - FH(-1)) * dy1, c2b * (FH(1) - FH(-2)) * dy3);
@@ -364,7 +369,8 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
 #undef HV
 #undef WV
 #undef FH
-                } else {   // advwz_fd, Flux(k-1..k) = fzw0..1, Adv(k-2..k) = azw0..2
+                };
+                auto dz_ = [&]() {   // advwz_fd, Flux(k-1..k) = fzw0..1, Adv(k-2..k) = azw0..2
                     if (k >= 3 && k <= nz - 1)
                         ACC2(aw, c1a * (fzw1 - fzw0) * Z1(k - 1), c2a * (azw2 - azw0) / (ZW(k) + ZW(k - 1)));
                     else if (k == 2)
@@ -375,7 +381,9 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
                         const R mu = abs_r(AA(2, 0, 0, 0)) * Z1(k - 1);
                         SUB1(aw, AVR * mu * (-MM(2, 2, 0, 0) + FOUR * MM(2, 1, 0, 0) - SIX * MM(2, 0, 0, 0) + FOUR * MM(2, -1, 0, 0) - MM(2, -2, 0, 0)));
                     }
-                }
+                };
+                // the reference's direction order, which alternates with ntime's parity
+                if constexpr (EVEN) { dx_(); dy_(); dz_(); } else { dz_(); dy_(); dx_(); }
             }
         }
 

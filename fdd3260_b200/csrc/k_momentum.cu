@@ -6,10 +6,15 @@ cudaError_t launch_k2(const DevGrid &g, const K2Args &a, const K2Maps &maps, cud
 {
     int ntx = (g.maxx + TX - 1) / TX, nty = (g.maxy + TY - 1) / TY;
     const size_t sm = k2_smem_bytes<double>();
-    cudaError_t e = cudaFuncSetAttribute(k2_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const bool even = (a.ntime % 2) == 0;   // direction order of the step (windadv.f90:103,158)
+    cudaError_t e = even ? cudaFuncSetAttribute(k2_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)
+                         : cudaFuncSetAttribute(k2_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     K2Args as = a;
     if (as.nseg < 1 || as.nseg > g.nz) as.nseg = k2_segments(g, sm);
-    k2_kernel<false><<<ntx * nty * as.nseg, dim3(TX, TY), sm, s>>>(g, as, maps);
+    if (even)
+        k2_kernel<false, true><<<ntx * nty * as.nseg, dim3(TX, TY), sm, s>>>(g, as, maps);
+    else
+        k2_kernel<false, false><<<ntx * nty * as.nseg, dim3(TX, TY), sm, s>>>(g, as, maps);
     return cudaGetLastError();
 }

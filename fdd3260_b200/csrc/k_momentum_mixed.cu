@@ -7,10 +7,15 @@ cudaError_t launch_k2_mixed(const DevGrid &g, const K2Args &a, const K2Maps &map
 {
     int ntx = (g.maxx + TX - 1) / TX, nty = (g.maxy + TY - 1) / TY;
     const size_t sm = k2_smem_bytes<float>();
-    cudaError_t e = cudaFuncSetAttribute(k2_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const bool even = (a.ntime % 2) == 0;   // direction order of the step (windadv.f90:103,158)
+    cudaError_t e = even ? cudaFuncSetAttribute(k2_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)
+                         : cudaFuncSetAttribute(k2_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     K2Args as = a;
     if (as.nseg < 1 || as.nseg > g.nz) as.nseg = k2_segments(g, sm);
-    k2_kernel<true><<<ntx * nty * as.nseg, dim3(TX, TY), sm, s>>>(g, as, maps);
+    if (even)
+        k2_kernel<true, true><<<ntx * nty * as.nseg, dim3(TX, TY), sm, s>>>(g, as, maps);
+    else
+        k2_kernel<true, false><<<ntx * nty * as.nseg, dim3(TX, TY), sm, s>>>(g, as, maps);
     return cudaGetLastError();
 }

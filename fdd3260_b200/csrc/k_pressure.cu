@@ -657,8 +657,11 @@ __global__ void p1_kernel(DevGrid G, const double *wavd, double *p1)
         p1[k - 1] = p1[k] + wavd[k] * 0.5 * G.dz * (G.fdz0[k - 1] + G.fdz0[k]);
 }
 
-// caldiv over the interior, k = 2..nz-1, signed max (pressure_solver.f90:121-130)
-__global__ void maxdiv_kernel(DevGrid G, const double *mu, const double *mv, const double *mw, double *partial)
+// caldiv over the interior, k = 2..nz-1, signed max (pressure_solver.f90:121-130), of the
+// momentum; natural = 1: the inputs are velocities, and the momentum is formed on the fly as
+// get_momentum does (rho0(k) u, rho0(k) v, avden0(k) w)
+__global__ void maxdiv_kernel(DevGrid G, const double *mu, const double *mv, const double *mw, int natural,
+                              double *partial)
 {
     __shared__ double sm[256];
     const int maxx = G.maxx, maxy = G.maxy;
@@ -669,9 +672,16 @@ __global__ void maxdiv_kernel(DevGrid G, const double *mu, const double *mv, con
         int ix = (int)(t % maxx), jy = (int)((t / maxx) % maxy), k = (int)(t / ((long long)maxx * maxy)) + 2;
         long long c = gidx(G, ix + 4, jy + 4, k);
         double d = 0.;
-        d = d + (mu[c + 1] - mu[c]) * dx1;
-        d = d + (mv[c + G.px] - mv[c]) * dy1;
-        d = d + (mw[c + G.ps] - mw[c]) * __ldg(G.dz1w + k - 1);
+        if (natural) {
+            const double r = __ldg(G.den0 + k - 1), a0 = __ldg(G.avden0 + k - 1), a1 = __ldg(G.avden0 + k);
+            d = d + (r * mu[c + 1] - r * mu[c]) * dx1;
+            d = d + (r * mv[c + G.px] - r * mv[c]) * dy1;
+            d = d + (a1 * mw[c + G.ps] - a0 * mw[c]) * __ldg(G.dz1w + k - 1);
+        } else {
+            d = d + (mu[c + 1] - mu[c]) * dx1;
+            d = d + (mv[c + G.px] - mv[c]) * dy1;
+            d = d + (mw[c + G.ps] - mw[c]) * __ldg(G.dz1w + k - 1);
+        }
         m = fmax(m, d);
     }
     sm[threadIdx.x] = m;
@@ -1183,10 +1193,10 @@ cudaError_t launch_to_velocity(const DevGrid &g, double *mu, double *mv, double 
 }
 
 cudaError_t launch_maxdiv(const DevGrid &g, PressurePlan *pp, const double *mu, const double *mv, const double *mw,
-                          cudaStream_t s)
+                          cudaStream_t s, int natural)
 {
     int nb = pp->npartial;
-    maxdiv_kernel<<<nb, 256, 0, s>>>(g, mu, mv, mw, pp->partial);
+    maxdiv_kernel<<<nb, 256, 0, s>>>(g, mu, mv, mw, natural, pp->partial);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     max_final<<<1, 256, 0, s>>>(pp->partial, nb, pp->maxdiv);

@@ -280,7 +280,7 @@ cudaError_t launch_cal_p1(const DevGrid &g, PressurePlan *pp, double *mw, const 
 // momentum -> natural velocities over all cells (get_velocities, funcpack.f90:265-344)
 cudaError_t launch_to_velocity(const DevGrid &g, double *mu, double *mv, double *mw, cudaStream_t s);
 cudaError_t launch_maxdiv(const DevGrid &g, PressurePlan *pp, const double *mu, const double *mv,
-                          const double *mw, cudaStream_t s);
+                          const double *mw, cudaStream_t s, int natural = 0);
 // results of the last cal_p1 / maxdiv (device pointers inside the plan)
 const double *pressure_p1_dev(const PressurePlan *pp);
 const double *pressure_maxdiv_dev(const PressurePlan *pp);

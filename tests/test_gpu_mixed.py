@@ -8,7 +8,11 @@ that field over the run, in the L2 norm over the interior:
 (for the pressure, whose initial value is zero, that is the relative L2 error).
 Scalars and velocities carry large base values, so an error relative to the value
 itself would say nothing about the FP32 arithmetic; the change over the run is what
-the FP32 fluxes compute.  Tolerance: MIXED_TOL = 2e-4 per field.
+the FP32 fluxes compute.  Tolerances per field, about five times the measured errors:
+- warm bubble 32 x 32 x 24, 4 steps, every scheme: winds and density 2.5e-10 measured,
+  pressure 3.4e-8, scalars 4.7e-7;
+- moist cumulus 32 x 32 x 40, 4 steps: winds 5.8e-7, pressure 2.4e-6, density 6.8e-8,
+  scalars 1.2e-7 to 7.9e-6.
 """
 import numpy as np
 import pytest
@@ -18,7 +22,12 @@ from fdd3260_b200 import _lib
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
-MIXED_TOL = 2e-4
+BUBBLE_TOL = {"u": 2e-9, "v": 2e-9, "w": 2e-9, "p": 2e-7, "dens": 2e-9, "scalars": 3e-6}
+CUMULUS_TOL = {"u": 3e-6, "v": 3e-6, "w": 3e-6, "p": 1.5e-5, "dens": 4e-7, "scalars": 4e-5}
+
+
+def _over(err, tol):
+    return {k: v for k, v in err.items() if not v <= tol.get(k, tol["scalars"])}
 
 
 def _interior(a):
@@ -56,7 +65,7 @@ def test_mixed_warm_bubble(scheme):
     st = config.warm_bubble_state(d, seed=21, centre=(800.0, 800.0, 400.0), radius=400.0)
     err = _run_mixed(d, st, 4, nscal=2)
     print(scheme, err)
-    bad = {k: v for k, v in err.items() if not v <= MIXED_TOL}
+    bad = _over(err, BUBBLE_TOL)
     assert not bad, (bad, err)
 
 
@@ -65,7 +74,7 @@ def test_mixed_cumulus_moist():
     st = config.cumulus_state(d, seed=1000, n_extra=2)
     err = _run_mixed(d, st, 4, nscal=len(st.scal), iqt=1)
     print("cumulus", err)
-    bad = {k: v for k, v in err.items() if not v <= MIXED_TOL}
+    bad = _over(err, CUMULUS_TOL)
     assert not bad, (bad, err)
 
 

@@ -160,6 +160,25 @@ def test_graph_replay_equals_eager():
         assert np.array_equal(x, y)
 
 
+@pytest.mark.parametrize("nsubp", [1, 3])
+def test_graph_diagnostics_equal_eager(nsubp):
+    """maxdiv after an even number of graph-replayed steps (computed on the final state,
+    whose level-n buffers hold velocities) is the divergence of the momentum, as the eager
+    step computes it inside the projection: equal to rounding."""
+    d = config.cumulus_domain(32, 32, 24, nsubp=nsubp)
+    st = config.cumulus_state(d, seed=8, n_extra=1)
+    mds = []
+    for graph in (False, True):
+        with Mimica(d, nscal=len(st.scal), iqt=1) as m:
+            m.upload(st)
+            md, _ = m.stepping(4, ntime0=1, diagnostics=True, graph=graph)
+            mds.append(md)
+    a, b = mds
+    assert abs(a - b) <= 1e-6 * abs(a) + 1e-14, (a, b)
+    if nsubp == 3:
+        assert abs(b) <= 1e-10
+
+
 def test_deterministic_reruns():
     d = config.warm_bubble_domain(32, 32, 16)
     st = config.warm_bubble_state(d, seed=6, centre=(800.0, 800.0, 300.0), radius=300.0)
