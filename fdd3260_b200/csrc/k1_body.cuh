@@ -151,16 +151,6 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
     const int ic = min(i, nx - 2), jc = min(j, ny - 2);
     const int cid = ty * TX + tx;   // cell slot (valid for cell threads)
     const int own_e = (ty + H) * SW + tx + H;   // own cell in a plane (cell threads)
-    // the plane element outside the cells this thread scales in stage 1 (NHALO < NT: one each)
-    static_assert(NHALO <= NT, "one halo element per thread");
-    const int my_halo = tid < NHALO ? halo_elem(tid) : -1;
-    // this thread's faces of a plane: x face (i0 + cx - 1/2) of row rx for the first
-    // TY*(TX+1) threads, y face (j0 + ry - 1/2) of column cy for all; stencil starts bx, by
-    const bool hasx = tid < TY * (TX + 1);
-    const int rx = hasx ? tid / (TX + 1) : 0, cx = hasx ? tid - rx * (TX + 1) : 0;
-    const int ry = tid / TX, cy = tid - ry * TX;
-    const int bx = (rx + H) * SW + H + cx - 1;   // x(i0 + cx - 1) in row rx
-    const int by = (ry - 1 + H) * SW + H + cy;   // x(j0 + ry - 1) in column cy
     const double dx1 = 1. / G.dx, dy1 = 1. / G.dy, dt0 = G.dt0;
     const bool conv1 = CONV1;
     const int NG = (F + PF - 1) / PF;      // field groups per level
@@ -217,11 +207,10 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
         for (int f = 0; f < F; f++) zf[f * NCELL + cid] = 0.;
 
     int zsl[L + 2];   // z-ring slot of level k-1+m, refreshed per level
-    const double *zp[L + 2];   // the own column's entry of field 0 at level k-1+m; field f at + f*ZS*NCELL
     // stencil value of a field at level l = k-1+m of the own column (stage 1: the other
     // fields' entries are multiplied by the density entry of the same level once, when
     // the level arrives)
-#define ZVAL(f, m) (zp[(m)][(f) * (ZS * NCELL)])
+#define ZVAL(f, m) (zring[((f) * ZS + zsl[(m)]) * NCELL + cid])
     auto wval = [&](int m) -> double {   // w_adv at level k-1+m of the own column
         const double a0 = ldg(G.avden0, k_cur - 2 + m);
         double x = wring[((k_cur - 1 + m) % ZS) * NCELL + cid];
@@ -250,10 +239,7 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
         const bool pro = k < kb;   // prologue level: its vertical face only
         k_cur = k;
 #pragma unroll
-        for (int m = 0; m < L + 2; m++) {
-            zsl[m] = (k - 1 + m) % ZS;
-            zp[m] = zring + zsl[m] * NCELL + cid;
-        }
+        for (int m = 0; m < L + 2; m++) zsl[m] = (k - 1 + m) % ZS;
         const double d0 = ldg(G.den0, k - 1);
         const double rd0 = MIXED ? 1. / d0 : 0.;   // the mixed form multiplies by 1/rho0
         // momentum boxes of level k -> face velocities.  Previous readers of su/sv (the
@@ -329,8 +315,8 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
                     } else {
                         const double *dsrc = g == 0 ? plq : densp;   // group 0: the density plane itself
                         if (cellt) plw[own_e] = plane_xo[u] * dsrc[own_e];
-                        if (my_halo >= 0) {
-                            const int e = my_halo;
+                        for (int h = tid; h < NHALO; h += NT) {
+                            const int e = halo_elem(h);
                             plw[e] = plw[e] * dsrc[e];
                         }
                     }
@@ -391,7 +377,12 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
                     // TX*(TY+1) faces), written as two independent chains for instruction-level
                     // parallelism
                     {
+                        const bool hasx = tid < TY * (TX + 1);
+                        const int rx = hasx ? tid / (TX + 1) : 0, cx = hasx ? tid - rx * (TX + 1) : 0;
+                        const int ry = tid / TX, cy = tid - ry * TX;
                         const double uu = su[hasx ? tid : 0], vv = sv[tid];
+                        const int bx = (rx + H) * SW + H + cx - 1;   // x(i0 + cx - 1) in row rx
+                        const int by = (ry - 1 + H) * SW + H + cy;   // x(j0 + ry - 1) in column cy
                         double Fx, Fy;
                         if (SCHEME == MG_WENO) {
                             if constexpr (MIXED) {
