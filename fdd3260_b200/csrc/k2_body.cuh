@@ -101,27 +101,44 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
     };
     // staging -> ring slot of level l: stencil momentum and advective velocity (zero
     // outside the domain, as the reference's arrays are read there)
+    // This thread's ring elements of a level: o = tid and o = tid + 256 of each component's
+    // PW x PH plane (PL = 432 < 512), with their staging offsets and whether they lie in
+    // the domain; the same for every level, so they are found once.
+    static_assert(PL > TX * TY && PL <= 2 * TX * TY, "two ring elements per thread and component");
+    const int ro1 = tid + TX * TY;
+    const bool has1 = ro1 < PL;
+    auto stg_of = [&](int o, bool &in) {
+        const int r = o / PW, c = o - r * PW;
+        const int ii = i0 - RH + c, jj = j0 - RH + r;
+        in = ii >= 1 && ii <= nx && jj >= 1 && jj <= ny;
+        return r * SBW + c + 1;
+    };
+    bool in0, in1 = false;
+    const int so0 = stg_of(tid, in0);
+    const int so1 = has1 ? stg_of(ro1, in1) : 0;
     auto convert_level = [&](int l) {
         mbar_wait_bounded(mbar, (uint32_t)((l - kp) & 1), A.err);
         const int slot = l % NSLOT;
         const double d0 = ldg(G.den0, l - 1), a0 = ldg(G.avden0, l - 1);
         // the mixed form multiplies by the level's reciprocal densities instead of dividing
         const double rd0 = MIXED ? 1. / d0 : 0., ra0 = MIXED ? 1. / a0 : 0.;
-        for (int q = tid; q < 3 * PL; q += TX * TY) {
-            int arr = q / PL, o = q - arr * PL;
-            int r = o / PW, c = o - r * PW;
-            int ii = i0 - RH + c, jj = j0 - RH + r;
-            double mv = 0., av = 0.;
-            if (ii >= 1 && ii <= nx && jj >= 1 && jj <= ny) {
-                double w = arr == 2 ? a0 : d0;
-                double x = stg[arr * (STG_SLOT / 8) + r * SBW + c + 1];
-                mv = A.in_is_leveln ? rep_value(A.rep, x, w) : x;
-                av = MIXED ? mv * (arr == 2 ? ra0 : rd0) : mv / w;
-                if (arr == 0) av = av - G.u0shift;
-                else if (arr == 1) av = av - G.v0shift;
-            }
-            ring_m[(slot * 3 + arr) * PL + o] = (R)mv;
-            ring_a[(slot * 3 + arr) * PL + o] = (R)av;
+#pragma unroll
+        for (int arr = 0; arr < 3; arr++) {
+            const double w = arr == 2 ? a0 : d0;
+            const double shift = arr == 0 ? G.u0shift : (arr == 1 ? G.v0shift : 0.);
+            auto one = [&](int o, int so, bool in) {
+                double mv = 0., av = 0.;
+                if (in) {
+                    const double x = stg[arr * (STG_SLOT / 8) + so];
+                    mv = A.in_is_leveln ? rep_value(A.rep, x, w) : x;
+                    av = MIXED ? mv * (arr == 2 ? ra0 : rd0) : mv / w;
+                    if (arr < 2) av = av - shift;
+                }
+                ring_m[(slot * 3 + arr) * PL + o] = (R)mv;
+                ring_a[(slot * 3 + arr) * PL + o] = (R)av;
+            };
+            one(tid, so0, in0);
+            if (has1) one(ro1, so1, in1);
         }
     };
     // Per level k: lb[d+2] = this thread's element of ring slot (k+d) mod 5, d = -2..2.

@@ -597,8 +597,10 @@ __global__ void level_sums(DevGrid G, const double *x, const double *xold, int o
     const int maxx = G.maxx, maxy = G.maxy;
     const double a0 = __ldg(G.avden0 + k - 1);
     double acc = 0., accd = 0.;
-    for (long long q = threadIdx.x; q < (long long)maxx * maxy; q += blockDim.x) {
-        int ix = (int)(q % maxx), jy = (int)(q / maxx);
+    // q = jy * maxx + ix runs from threadIdx.x in steps of blockDim.x; (ix, jy) advance
+    // incrementally instead of by a division per element
+    int ix = (int)threadIdx.x % maxx, jy = (int)threadIdx.x / maxx;
+    for (; jy < maxy;) {
         long long c = gidx(G, ix + 4, jy + 4, k);
         double v = x[c];
         acc += v;
@@ -607,6 +609,8 @@ __global__ void level_sums(DevGrid G, const double *x, const double *xold, int o
             if (old_rep >= 0) wo = rep_value(old_rep, wo, a0);
             accd += (v - wo) / dt0;
         }
+        ix += blockDim.x;
+        while (ix >= maxx) { ix -= maxx; ++jy; }
     }
     s1[threadIdx.x] = acc;
     s2[threadIdx.x] = accd;
