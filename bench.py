@@ -346,6 +346,8 @@ def main():
                     help="smagorinsky: SGS turbulence diffusion on (Smagorinsky-Lilly, pran=-0.4, zdec=2400 m, "
                          "surface heat, moisture and momentum fluxes), as the BOMEX template runs it")
     ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--ens-mode", choices=["grouped", "streams"], default="grouped",
+                    help="ensemble graphs: one launch per kernel of a stage over all members, or per-member streams")
     ap.add_argument("--autotune", default="on", choices=["on", "off"],
                     help="pick the projection plan and K1's segments by timing before the timed steps")
     ap.add_argument("--traj-steps", type=int, default=200, help="steps of the trajectory adjoint leg (0: off)")
@@ -528,7 +530,7 @@ def run_ensemble(args, ws, rank, local):
             m.upload(st)
             members.append(m)
             states.append(st)
-        ens = E.Ensemble(members)
+        ens = E.Ensemble(members, mode=args.ens_mode)
         if args.autotune == "on":
             plans.update(ens.autotune(reps=3))
         return ens
@@ -538,6 +540,22 @@ def run_ensemble(args, ws, rank, local):
                           reduce_max=lambda x: dist_max(x, ws), reduce_sum=lambda x: dist_sum(x, ws), timed_region=clk)
     ens, parts, t_ms = sh["stepper"], sh["parts"], sh["t_ms"]
     value = total_cells * args.steps / (t_ms / 1e3) / 1e6
+    launches = ens.launches_per_step
+    # the other recording mode on the same members, same step count, for comparison
+    other = "streams" if args.ens_mode == "grouped" else "grouped"
+    cmp_ = None
+    try:
+        ens.mode = other
+    except Exception as ex:   # members that cannot share grouped launches
+        cmp_ = {"mode": other, "unavailable": str(ex)}
+    if cmp_ is None:
+        t1 = 1 + args.warmup + args.steps
+        ens.step(2, ntime0=t1)   # records the pair graph at the timed parity
+        dist_barrier(ws)
+        ms_o = dist_max(ens.time_steps(args.steps, ntime0=t1 + 2), ws)
+        cmp_ = {"mode": other, "value": total_cells * args.steps / (ms_o / 1e3) / 1e6,
+                "ms_per_step": ms_o / args.steps, "gpu_launches_per_step": ens.launches_per_step}
+        ens.mode = args.ens_mode
     # roofline of the dominant kernel, from an eager profiled pass of this rank's largest member
     big = max(range(len(members)), key=lambda q: members[q].domain.cells)
     mb = members[big]
@@ -586,7 +604,6 @@ def run_ensemble(args, ws, rank, local):
         nbytes = sum((5 + len(st.scal)) * m.domain.nx * m.domain.ny * m.domain.nz * 8 for m, st in zip(members, states))
     e2e_s = dist_max(time.perf_counter() - t0, ws)
     nbytes_all = dist_sum(nbytes, ws)
-    launches = ens.launches_per_step
     ens.close()
     cpu = None
     if rank == 0 and not args.skip_cpu:
@@ -610,7 +627,8 @@ def run_ensemble(args, ws, rank, local):
                                        f"nz in {E.NZ_CHOICES} (seeded), dx=dy=50 m, dz=40 m, WENO, FD4, dt=0.5 s",
                            "total_cells": total_cells, "members_per_rank": [len(p) for p in parts],
                            "form": form, "parallelism": f"members sharded over {ws} rank(s), no collective",
-                           "l2": "inputs larger than L2"},
+                           "l2": "inputs larger than L2", "ensemble_mode": args.ens_mode},
+                "other_mode": cmp_,
                 "clocks": clk.summary(), "gpu_launches": launches * args.steps,
                 "e2e": {"value": total_cells * args.e2e_steps / e2e_s / 1e6, "unit": "Mcell-updates/s",
                         "h2d_bytes_per_step": nbytes_all, "d2h_bytes_per_step": nbytes_all,

@@ -20,6 +20,7 @@ MG_CKPT_AUTO, MG_CKPT_DEVICE, MG_CKPT_HOST = -1, 0, 1
 MG_WENO, MG_PPM, MG_MUSCL, MG_LW, MG_QUICK = 0, 1, 2, 3, 4
 MG_LIM_MINMOD, MG_LIM_VL, MG_LIM_MC, MG_LIM_DEFAULT = 0, 1, 2, 3
 MG_PREC_FP64, MG_PREC_MIXED = 0, 1
+MG_ENS_GROUPED, MG_ENS_STREAMS = 1, 2
 
 SCHEMES = {"weno": MG_WENO, "ppm": MG_PPM, "muscl": MG_MUSCL, "lw": MG_LW, "quick": MG_QUICK}
 LIMITERS = {"minmod": MG_LIM_MINMOD, "VL": MG_LIM_VL, "MC": MG_LIM_MC, "default": MG_LIM_DEFAULT}
@@ -130,6 +131,8 @@ def lib() -> C.CDLL:
         L.mg_ensemble_step.argtypes = [vp, C.c_int, C.c_int]
         L.mg_ensemble_time_steps.argtypes = [vp, C.c_int, C.c_int, _dp]
         L.mg_ensemble_launch_count.argtypes = [vp]
+        L.mg_ensemble_set_mode.argtypes = [vp, C.c_int]
+        L.mg_ensemble_get_mode.argtypes = [vp]
         L.mg_checkall.argtypes = [vp, C.POINTER(MgCheckParams), C.POINTER(MgCheckResult)]
         L.mg_cfl_dt.argtypes = [C.POINTER(MgCheckParams), C.c_double, C.c_double, _dp, C.POINTER(C.c_int)]
         L.mg_set_dt.argtypes = [vp, C.c_double]
@@ -186,6 +189,7 @@ EXPORTED = [
     "mg_step", "mg_step_graph", "mg_synchronize", "mg_last_launch_count", "mg_advection_ac", "mg_qnadv_uvw",
     "mg_fft_solve", "mg_anelastic_pressure", "mg_time_steps", "mg_profile_enable", "mg_profile_report",
     "mg_advection_tl", "mg_advection_ad", "mg_anelastic_pressure_ad", "mg_time_adjoint", "mg_ensemble_create", "mg_ensemble_destroy", "mg_ensemble_step", "mg_ensemble_time_steps", "mg_ensemble_launch_count",
+    "mg_ensemble_set_mode", "mg_ensemble_get_mode",
     "mg_set_sgs", "mg_set_surface_fluxes", "mg_sgs_profiles", "mg_calc_subgrid", "mg_efud", "mg_eff",
     "mg_checkall", "mg_cfl_dt", "mg_set_dt", "mg_download_ksgs", "mg_qnadv_tl", "mg_qnadv_ad",
     "mg_traj_forward", "mg_traj_tl", "mg_traj_adjoint", "mg_time_traj", "mg_traj_record_limit", "mg_traj_checkpoints",

@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <new>
+#include <memory>
 #include <vector>
 
 #include <climits>
@@ -647,23 +648,47 @@ static void k1_stage_args(mg_ctx *c, int stage, K1Args &a1)
     a1.mw = (stage == 1 ? c->mA : c->mB)[2];
 }
 
+static void k2_stage_args(mg_ctx *c, int stage, int ntime, K2Args &a2)
+{
+    const DevGrid &G = c->G;
+    const int ies = 1, iqt = c->prm.iqt >= 0 ? 1 + c->prm.iqt : -1;
+    const double *const *mom = stage == 1 ? c->mA : c->mB;
+    a2.stage = stage; a2.rep = REP_NAT; a2.ntime = ntime;
+    a2.a_dt = (stage == 1 ? 1. : 0.5) * G.dt0;
+    a2.b = stage == 1 ? 0. : 1.;
+    a2.nseg = c->k2_nseg;
+    a2.mu = mom[0]; a2.mv = mom[1]; a2.mw = mom[2];
+    a2.in_is_leveln = stage == 1;
+    a2.mu_n = c->mA[0]; a2.mv_n = c->mA[1]; a2.mw_n = c->mA[2];
+    a2.p = c->p;
+    // buoyancy reads the stage's input density and scalars: level n in stage 1 (natural,
+    // unchanged by K1 stage 1), the working values in stage 2
+    a2.dens = stage == 1 ? c->sA[0] : c->sB[0];
+    a2.es = stage == 1 ? c->sA[ies] : c->sB[ies];
+    a2.qt = iqt >= 0 ? (stage == 1 ? c->sA[iqt] : c->sB[iqt]) : nullptr;
+    a2.dens_is_leveln = stage == 1;
+    a2.fes = c->fes; a2.fqt = iqt >= 0 ? c->fqt : nullptr;
+    double **mo = stage == 1 ? c->mB : c->mA;
+    a2.ou = mo[0]; a2.ov = mo[1]; a2.ow = mo[2];
+    a2.tu = c->tm[0]; a2.tv = c->tm[1]; a2.tw = c->tm[2];
+    a2.mode = 0;
+    a2.err = c->derr;
+    if (c->sgs_on) { a2.su = c->sgm[0]; a2.sv = c->sgm[1]; a2.sw = c->sgm[2]; }
+}
+
 static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int want_maxdiv, int *launches)
 {
     const DevGrid &G = c->G;
     const mg_params &P = c->prm;
     const int nf = c->nf;
-    const int ies = 1, iqt = P.iqt >= 0 ? 1 + P.iqt : -1;
     if (c->sgs_on) {
         cudaError_t e = sgs_tendencies(c, launches);
         if (e != cudaSuccess) return e;
     }
     for (int stage = 1; stage <= 2; stage++) {
-        const double a_dt = (stage == 1 ? 1. : 0.5) * G.dt0;
-        const double b = stage == 1 ? 0. : 1.;
         // ---- K1: density + scalars (level-n buffers hold natural variables) ----
         K1Args a1{};
         k1_stage_args(c, stage, a1);
-        const double *const *mom = stage == 1 ? c->mA : c->mB;
         if (P.precision == MG_PREC_MIXED)
             PROF(c, "k1_scalar_advection", launch_k1_mixed(G, a1, stage == 1 ? c->maps1 : c->maps2, c->stream));
         else
@@ -675,25 +700,8 @@ static cudaError_t step_once(mg_ctx *c, int ntime, int last, int want_p1, int wa
         }
         // ---- K2: momentum ----
         K2Args a2{};
-        a2.stage = stage; a2.rep = REP_NAT; a2.ntime = ntime; a2.a_dt = a_dt; a2.b = b;
-        a2.nseg = c->k2_nseg;
-        a2.mu = mom[0]; a2.mv = mom[1]; a2.mw = mom[2];
-        a2.in_is_leveln = stage == 1;
-        a2.mu_n = c->mA[0]; a2.mv_n = c->mA[1]; a2.mw_n = c->mA[2];
-        a2.p = c->p;
-        // buoyancy reads the stage's input density and scalars: level n in stage 1 (natural,
-        // unchanged by K1 stage 1), the working values in stage 2
-        a2.dens = stage == 1 ? c->sA[0] : c->sB[0];
-        a2.es = stage == 1 ? c->sA[ies] : c->sB[ies];
-        a2.qt = iqt >= 0 ? (stage == 1 ? c->sA[iqt] : c->sB[iqt]) : nullptr;
-        a2.dens_is_leveln = stage == 1;
-        a2.fes = c->fes; a2.fqt = iqt >= 0 ? c->fqt : nullptr;
+        k2_stage_args(c, stage, ntime, a2);
         double **mo = stage == 1 ? c->mB : c->mA;
-        a2.ou = mo[0]; a2.ov = mo[1]; a2.ow = mo[2];
-        a2.tu = c->tm[0]; a2.tv = c->tm[1]; a2.tw = c->tm[2];
-        a2.mode = 0;
-        a2.err = c->derr;
-        if (c->sgs_on) { a2.su = c->sgm[0]; a2.sv = c->sgm[1]; a2.sw = c->sgm[2]; }
         const K2Maps &mm = stage == 1 ? c->mmaps1 : c->mmaps2;
         if (P.precision == MG_PREC_MIXED)
             PROF(c, "k2_momentum", launch_k2_mixed(G, a2, mm, c->stream));
@@ -790,19 +798,137 @@ extern "C" int mg_step_graph(mg_ctx *c, int nsteps, int ntime0, double *maxdiv, 
 
 // ---------------- ensembles of independent domains ----------------
 // The members are contexts of their own (sizes, parameters, streams).  A pair of steps
-// of all members is recorded once per parity into one CUDA graph that forks from the
-// ensemble's stream to every member's stream and joins back, so that the launches of
-// small members run concurrently and one graph launch advances the whole ensemble.
+// of all members is recorded once per parity into one CUDA graph, in one of two modes:
+//  * MG_ENS_GROUPED: every kernel of a stage is ONE launch over the blocks of all
+//    members (a work table of (member, block) items, largest blocks first, with each
+//    member's arguments and tensor maps in device memory), so a stage is the same dozen
+//    or so launches whatever the member count;
+//  * MG_ENS_STREAMS: the graph forks from the ensemble's stream to every member's stream
+//    and joins back; each member's launches are its single-domain ones.
+// Both run the same kernel bodies on the same data: the results are identical.
 struct mg_ens {
     std::vector<mg_ctx *> m;
     int device = 0;
+    int mode = MG_ENS_STREAMS;
     cudaStream_t stream = nullptr;
     cudaEvent_t fork = nullptr;
     std::vector<cudaEvent_t> join;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    unsigned char *gdev[2] = {nullptr, nullptr};   // grouped mode: device tables of each parity's graph
     long long gen = -1;                  // sum of the members' generations the graphs were recorded at
     int launches = 0;
 };
+
+// members that can share grouped launches: one arithmetic form, scheme and field count,
+// no SGS, the same projection passes
+static bool ens_groupable(const mg_ens *e)
+{
+    const mg_ctx *a = e->m[0];
+    for (const mg_ctx *c : e->m) {
+        if (c->sgs_on || c->prm.precision != a->prm.precision || c->G.scal_adv != a->G.scal_adv || c->nf != a->nf ||
+            c->prm.nsubp != a->prm.nsubp)
+            return false;
+        if (a->prm.precision == MG_PREC_MIXED &&
+            (c->prm.refine_iters != a->prm.refine_iters || c->prm.refine_tol != a->prm.refine_tol))
+            return false;
+    }
+    return true;
+}
+
+static void ens_drop_graphs(mg_ens *e)
+{
+    for (int i = 0; i < 2; i++) {
+        if (e->gexec[i]) { cudaGraphExecDestroy(e->gexec[i]); e->gexec[i] = nullptr; }
+        if (e->gdev[i]) { cudaFree(e->gdev[i]); e->gdev[i] = nullptr; }
+    }
+}
+
+// steps ntime0, ntime0+1 of the members `mem` as grouped launches (the launch sequence
+// of step_once without SGS, last = 0)
+static void ens_group_record(const std::vector<mg_ctx *> &mem, int ntime0, GroupProgram &P)
+{
+    const int n = (int)mem.size();
+    const mg_ctx *c0 = mem[0];
+    const bool mixed = c0->prm.precision == MG_PREC_MIXED;
+    const int scheme = c0->G.scal_adv, nf = c0->nf;
+    const int nsub = c0->prm.nsubp, nref = mixed ? c0->prm.refine_iters : 0;
+    const double tol = c0->prm.refine_tol;
+    for (int st = 0; st < 2; st++) {
+        const int ntime = ntime0 + st;
+        for (int stage = 1; stage <= 2; stage++) {
+            std::vector<int> nb(n);
+            std::vector<double> cost(n);
+            for (int q = 0; q < n; q++) {
+                const DevGrid &G = mem[q]->G;
+                nb[q] = ((G.maxx + 31) / 32) * ((G.maxy + 7) / 8);   // whole-column tiles of K1 and K2 (32 x 8)
+                cost[q] = (double)G.nz;
+            }
+            const std::vector<GItem> it = group_items(nb, cost);
+            const size_t io = P.put(it);
+            const int ni = (int)it.size();
+            // ---- K1 and the scalars' ghost cells ----
+            std::vector<K1Member> k1(n);
+            std::vector<GroupHaloIn> hs(n);
+            for (int q = 0; q < n; q++) {
+                mg_ctx *c = mem[q];
+                k1[q].M = stage == 1 ? c->maps1 : c->maps2;
+                k1[q].G = c->G;
+                k1[q].A = K1Args{};
+                k1_stage_args(c, stage, k1[q].A);
+                k1[q].A.nseg = 1;
+                hs[q].G = &c->G;
+                hs[q].nf = nf;
+                for (int f = 0; f < nf; f++) hs[q].f[f] = k1[q].A.xout[f];
+            }
+            const size_t m1 = P.put(k1);
+            P.ops.push_back([=](const unsigned char *d, cudaStream_t s) {
+                return mixed ? launch_k1_group_mixed(scheme, stage, nf, (const K1Member *)(d + m1), (const GItem *)(d + io), ni, s)
+                             : launch_k1_group(scheme, stage, nf, (const K1Member *)(d + m1), (const GItem *)(d + io), ni, s);
+            });
+            P.launches++;
+            group_halo(P, hs);
+            // ---- K2 (one launch per K2G_MAX members) and the momentum's ghost cells ----
+            std::vector<GroupHaloIn> hm(n);
+            std::vector<GroupProjIn> pj(n);
+            const int even = (ntime % 2) == 0;
+            for (int c0 = 0; c0 < n; c0 += K2G_MAX) {
+                const int cn = std::min(K2G_MAX, n - c0);
+                auto prm = std::make_shared<K2GroupParams>();
+                std::vector<K2Maps> maps(cn);
+                for (int q = 0; q < cn; q++) {
+                    mg_ctx *c = mem[c0 + q];
+                    maps[q] = stage == 1 ? c->mmaps1 : c->mmaps2;
+                    prm->a[q].G = c->G;
+                    prm->a[q].A = K2Args{};
+                    k2_stage_args(c, stage, ntime, prm->a[q].A);
+                    prm->a[q].A.nseg = 1;
+                }
+                const std::vector<GItem> itc =
+                    group_items(std::vector<int>(nb.begin() + c0, nb.begin() + c0 + cn),
+                                std::vector<double>(cost.begin() + c0, cost.begin() + c0 + cn));
+                const size_t mm = P.put(maps), ic = P.put(itc);
+                const int nic = (int)itc.size();
+                P.ops.push_back([=](const unsigned char *d, cudaStream_t s) {
+                    return mixed ? launch_k2_group_mixed(even, *prm, (const K2Maps *)(d + mm), (const GItem *)(d + ic), nic, s)
+                                 : launch_k2_group(even, *prm, (const K2Maps *)(d + mm), (const GItem *)(d + ic), nic, s);
+                });
+                P.launches++;
+            }
+            for (int q = 0; q < n; q++) {
+                mg_ctx *c = mem[q];
+                double **mo = stage == 1 ? c->mB : c->mA;
+                hm[q].G = &c->G;
+                hm[q].nf = 3;
+                for (int f = 0; f < 3; f++) hm[q].f[f] = mo[f];
+                pj[q] = GroupProjIn{&c->G, c->pp, mo[0], mo[1], mo[2], c->p, stage == 1 ? c->mA[2] : c->mB[2],
+                                    stage == 1 ? REP_NAT : -1};
+            }
+            group_halo(P, hm);
+            // ---- projection ----
+            group_projection(P, pj, stage == 2, nsub, nref, tol);
+        }
+    }
+}
 
 extern "C" int mg_ensemble_create(mg_ctx *const *members, int n, mg_ens **out)
 {
@@ -817,6 +943,7 @@ extern "C" int mg_ensemble_create(mg_ctx *const *members, int n, mg_ens **out)
     mg_ens *e = new mg_ens();
     e->device = members[0]->device;
     e->m.assign(members, members + n);
+    e->mode = ens_groupable(e) ? MG_ENS_GROUPED : MG_ENS_STREAMS;
     cudaError_t er = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
     if (er == cudaSuccess) er = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
     e->join.resize(n, nullptr);
@@ -834,7 +961,7 @@ extern "C" int mg_ensemble_destroy(mg_ens *e)
     if (!e) return MG_ERR_PARAM;
     cudaSetDevice(e->device);
     if (e->stream) cudaStreamSynchronize(e->stream);
-    for (int i = 0; i < 2; i++) if (e->gexec[i]) cudaGraphExecDestroy(e->gexec[i]);
+    ens_drop_graphs(e);
     for (cudaEvent_t ev : e->join) if (ev) cudaEventDestroy(ev);
     if (e->fork) cudaEventDestroy(e->fork);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -873,19 +1000,33 @@ extern "C" int mg_ensemble_step(mg_ens *e, int nsteps, int ntime0)
     long long gsum = 0;
     for (mg_ctx *c : e->m) gsum += c->gen;
     if (gsum != e->gen) {   // a member's step changed since the graphs were recorded
-        for (int i = 0; i < 2; i++)
-            if (e->gexec[i]) { cudaGraphExecDestroy(e->gexec[i]); e->gexec[i] = nullptr; }
+        ens_drop_graphs(e);
         e->gen = gsum;
     }
+    if (e->mode == MG_ENS_GROUPED && !ens_groupable(e)) return MG_ERR_PARAM;
     int s = 0;
     while (nsteps - s >= 2) {
         const int par = (ntime0 + s) & 1;
         if (!e->gexec[par]) {
+            GroupProgram prog;
+            if (e->mode == MG_ENS_GROUPED) {   // tables first: nothing is allocated or copied during the capture
+                ens_group_record(e->m, ntime0 + s, prog);
+                if (e->gdev[par]) { cudaFree(e->gdev[par]); e->gdev[par] = nullptr; }
+                CKR(cudaMalloc(&e->gdev[par], prog.host.size()));
+                CKR(cudaMemcpy(e->gdev[par], prog.host.data(), prog.host.size(), cudaMemcpyHostToDevice));
+            }
             cudaGraph_t graph;
             CKR(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
             int launches = 0;
-            cudaError_t er = ens_issue(e, ntime0 + s, 2, &launches);
+            cudaError_t er = cudaSuccess;
+            if (e->mode == MG_ENS_GROUPED) {
+                for (size_t q = 0; q < prog.ops.size() && er == cudaSuccess; q++) er = prog.ops[q](e->gdev[par], e->stream);
+                launches = prog.launches;
+            } else {
+                er = ens_issue(e, ntime0 + s, 2, &launches);
+            }
             cudaError_t er2 = cudaStreamEndCapture(e->stream, &graph);
+            if (er2 == cudaSuccess && er != cudaSuccess) cudaGraphDestroy(graph);
             if (er != cudaSuccess) return cuerr(er);
             if (er2 != cudaSuccess) return cuerr(er2);
             er = cudaGraphInstantiate(&e->gexec[par], graph, 0);
@@ -932,6 +1073,21 @@ extern "C" int mg_ensemble_time_steps(mg_ens *e, int nsteps, int ntime0, double 
 }
 
 extern "C" int mg_ensemble_launch_count(const mg_ens *e) { return e ? e->launches : -1; }
+
+extern "C" int mg_ensemble_set_mode(mg_ens *e, int mode)
+{
+    if (!e || (mode != MG_ENS_GROUPED && mode != MG_ENS_STREAMS)) return MG_ERR_PARAM;
+    if (mode == MG_ENS_GROUPED && !ens_groupable(e)) return MG_ERR_PARAM;
+    if (mode != e->mode) {
+        CKR(cudaSetDevice(e->device));
+        CKR(cudaStreamSynchronize(e->stream));
+        ens_drop_graphs(e);
+        e->mode = mode;
+    }
+    return MG_OK;
+}
+
+extern "C" int mg_ensemble_get_mode(const mg_ens *e) { return e ? e->mode : MG_ERR_PARAM; }
 
 extern "C" int mg_synchronize(mg_ctx *c)
 {

@@ -117,8 +117,9 @@ __device__ __forceinline__ int halo_elem(int h)
 // its own so that the kernels without SGS keep their register budget
 // FC: the field count when it is known at compile time (0: A.nf at run time); with it the
 // group loop unrolls and every shared-memory offset of the z-window is a constant
-template <int SCHEME, bool MIXED, int STAGE, bool SGS, int FC = 0>
-__global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __grid_constant__ K1Maps M)
+// bid: the block's index in the domain's own grid of tiles x segments
+template <int SCHEME, bool MIXED, int STAGE, bool SGS, int FC>
+__device__ __forceinline__ void k1_run(const DevGrid &G, const K1Args &A, const K1Maps &M, const int bid)
 {
     constexpr int PF = k1_pf(SCHEME), NPS = k1_nps(SCHEME), NFB = k1_nfb(SCHEME);
     constexpr bool CONV1 = STAGE == 1;   // stage-1 inputs are natural: psi = s * rho
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
     double *crx = (double *)(sm + Ly.crx), *cry = (double *)(sm + Ly.cry);
 
     const int ntx = (G.maxx + TX - 1) / TX, nty = (G.maxy + TY - 1) / TY;
-    const int tile = blockIdx.x % (ntx * nty), seg = blockIdx.x / (ntx * nty);
+    const int tile = bid % (ntx * nty), seg = bid / (ntx * nty);
     const int ti = tile % ntx, tj = tile / ntx;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const int i0 = 4 + ti * TX, j0 = 4 + tj * TY;
@@ -667,6 +668,31 @@ __global__ void __launch_bounds__(NT, 2) k1_kernel(DevGrid G, K1Args A, const __
     }
     cp_async_wait_all();
 #undef ZVAL
+}
+
+template <int SCHEME, bool MIXED, int STAGE, bool SGS, int FC = 0>
+__global__ void __launch_bounds__(NT, 2)
+    k1_kernel(const __grid_constant__ DevGrid G, const __grid_constant__ K1Args A, const __grid_constant__ K1Maps M)
+{
+    k1_run<SCHEME, MIXED, STAGE, SGS, FC>(G, A, M, blockIdx.x);
+}
+
+// One launch over the blocks of several domains (an ensemble stage): block b of the
+// launch runs block items[b].b of domain items[b].m, whose grid, arguments and tensor
+// maps (in global memory, written before the launch and never changed while it runs)
+// are mem[items[b].m].
+template <int SCHEME, bool MIXED, int STAGE, int FC = 0>
+__global__ void __launch_bounds__(NT, 2) k1_group_kernel(const K1Member *__restrict__ mem, const GItem *__restrict__ items)
+{
+    const GItem it = items[blockIdx.x];
+    const K1Member &m = mem[it.m];
+    if (threadIdx.x == 0 && threadIdx.y == 0) {   // the thread that issues the bulk copies
+        const int F = FC > 0 ? FC : m.A.nf;
+        for (int f = 0; f < F; f++) tensormap_acquire(&m.M.x[f]);
+        tensormap_acquire(&m.M.mu);
+        tensormap_acquire(&m.M.mv);
+    }
+    k1_run<SCHEME, MIXED, STAGE, false, FC>(m.G, m.A, m.M, it.b);
 }
 
 }  // namespace

@@ -51,8 +51,9 @@ __device__ __forceinline__ float abs_r(float x) { return fabsf(x); }
 
 // EVEN: the parity of ntime (the direction order of windadv.f90:103,158), so that each
 // instantiation evaluates the three directions as straight-line code
+// bid: the block's index in the domain's own grid of tiles x segments
 template <bool MIXED, bool EVEN>
-__global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const __grid_constant__ K2Maps M)
+__device__ __forceinline__ void k2_run(const DevGrid &G, const K2Args &A, const K2Maps &M, const int bid)
 {
     // R: type of the stencil arithmetic (FP64 plain form, FP32 mixed form)
     using R = typename std::conditional<MIXED, float, double>::type;
@@ -65,7 +66,7 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
     uint64_t *mbar = reinterpret_cast<uint64_t *>(smb + k2_ring_bytes<R>() + 3 * STG_SLOT);
 
     const int ntx = (G.maxx + TX - 1) / TX, nty = (G.maxy + TY - 1) / TY;
-    const int tile = blockIdx.x % (ntx * nty), seg = blockIdx.x / (ntx * nty);
+    const int tile = bid % (ntx * nty), seg = bid / (ntx * nty);
     const int ti = tile % ntx, tj = tile / ntx;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const int i0 = 4 + ti * TX, j0 = 4 + tj * TY;
@@ -455,6 +456,46 @@ __global__ void __launch_bounds__(TX *TY) k2_kernel(DevGrid G, K2Args A, const _
 #undef ZW
 #undef ZW1
 #undef Z1
+}
+
+template <bool MIXED, bool EVEN>
+__global__ void __launch_bounds__(TX *TY)
+    k2_kernel(const __grid_constant__ DevGrid G, const __grid_constant__ K2Args A, const __grid_constant__ K2Maps M)
+{
+    k2_run<MIXED, EVEN>(G, A, M, blockIdx.x);
+}
+
+// One launch over the blocks of up to K2G_MAX domains: block b runs block items[b].b of
+// domain items[b].m.  The domains' grids and arguments are a kernel parameter (constant
+// bank: read-only, so the compiler reloads them where the single-domain kernel does
+// instead of holding them in registers); their tensor maps are in global memory, written
+// before the launch and unchanged while it runs.
+template <bool MIXED, bool EVEN>
+__global__ void __launch_bounds__(TX * TY, 2)
+    k2_group_kernel(const __grid_constant__ K2GroupParams P, const K2Maps *__restrict__ maps, const GItem *__restrict__ items)
+{
+    const GItem it = items[blockIdx.x];
+    const K2Maps &M = maps[it.m];
+    if (threadIdx.x == 0 && threadIdx.y == 0)   // the thread that issues the bulk copies
+        for (int c = 0; c < 3; c++) tensormap_acquire(&M.m[c]);
+    k2_run<MIXED, EVEN>(P.a[it.m].G, P.a[it.m].A, M, it.b);
+}
+
+// K2 over the blocks of several members, all at one ntime parity
+template <bool MIXED>
+cudaError_t launch_k2_group_t(int even, const K2GroupParams &P, const K2Maps *maps, const GItem *items, int nitems,
+                              cudaStream_t s)
+{
+    const size_t sm = k2_smem_bytes<typename std::conditional<MIXED, float, double>::type>();
+    cudaError_t e = even ? cudaFuncSetAttribute(k2_group_kernel<MIXED, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)
+                         : cudaFuncSetAttribute(k2_group_kernel<MIXED, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    if (nitems < 1) return cudaErrorInvalidValue;
+    if (even)
+        k2_group_kernel<MIXED, true><<<nitems, dim3(TX, TY), sm, s>>>(P, maps, items);
+    else
+        k2_group_kernel<MIXED, false><<<nitems, dim3(TX, TY), sm, s>>>(P, maps, items);
+    return cudaGetLastError();
 }
 
 }  // namespace

@@ -18,3 +18,9 @@ cudaError_t launch_k2(const DevGrid &g, const K2Args &a, const K2Maps &maps, cud
         k2_kernel<false, false><<<ntx * nty * as.nseg, dim3(TX, TY), sm, s>>>(g, as, maps);
     return cudaGetLastError();
 }
+
+cudaError_t launch_k2_group(int even, const K2GroupParams &P, const K2Maps *maps, const GItem *items, int nitems,
+                            cudaStream_t s)
+{
+    return launch_k2_group_t<false>(even, P, maps, items, nitems, s);
+}

@@ -19,3 +19,9 @@ cudaError_t launch_k2_mixed(const DevGrid &g, const K2Args &a, const K2Maps &map
         k2_kernel<true, false><<<ntx * nty * as.nseg, dim3(TX, TY), sm, s>>>(g, as, maps);
     return cudaGetLastError();
 }
+
+cudaError_t launch_k2_group_mixed(int even, const K2GroupParams &P, const K2Maps *maps, const GItem *items, int nitems,
+                            cudaStream_t s)
+{
+    return launch_k2_group_t<true>(even, P, maps, items, nitems, s);
+}

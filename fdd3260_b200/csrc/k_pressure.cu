@@ -257,8 +257,9 @@ __device__ __forceinline__ double poisson_apply(const DevGrid &G, const XArgs &A
 // shared memory and S[k][kx][ky] through a [kx][8 rows] staging tile in the free half,
 // 8 consecutive ky (one 64/128-byte segment) per kx instead of 2 scattered values.
 constexpr int XT_THREADS = 256;
+// bid: the block's index in the domain's own grid (nz x row groups)
 template <typename C>
-__global__ void __launch_bounds__(XT_THREADS, 3) fft_x_fwd(DevGrid G, FftPlan1 P, XArgs A)
+__device__ __forceinline__ void fft_x_fwd_run(const DevGrid &G, const FftPlan1 &P, const XArgs &A, const int bid)
 {
     using R = typename CT<C>::R;
     extern __shared__ double2 smraw_x[];
@@ -266,7 +267,7 @@ __global__ void __launch_bounds__(XT_THREADS, 3) fft_x_fwd(DevGrid G, FftPlan1 P
     C *spec = reinterpret_cast<C *>(A.spec);
     const int n = P.n, nh = n / 2 + 1, maxy = G.maxy;
     const int groups = (maxy + ROWS - 1) / ROWS;
-    const int k = blockIdx.x / groups + 1, jg = blockIdx.x % groups;
+    const int k = bid / groups + 1, jg = bid % groups;
     const int jb = jg * ROWS;                       // first interior row (0-based)
     const int nt_pair = blockDim.x / (ROWS / 2);
     const int pair = threadIdx.x / nt_pair, lt = threadIdx.x % nt_pair;
@@ -275,7 +276,7 @@ __global__ void __launch_bounds__(XT_THREADS, 3) fft_x_fwd(DevGrid G, FftPlan1 P
     __shared__ unsigned long long bmax;
     __shared__ double wsum[32];
     if (converged(A.prev)) {   // uniform over the grid: nothing left to refine
-        if (blockIdx.x == 0 && threadIdx.x == 0 && A.resid) *A.resid = *A.prev.flag;
+        if (bid == 0 && threadIdx.x == 0 && A.resid) *A.resid = *A.prev.flag;
         return;
     }
     if (threadIdx.x == 0) bmax = 0ull;
@@ -352,11 +353,18 @@ __global__ void __launch_bounds__(XT_THREADS, 3) fft_x_fwd(DevGrid G, FftPlan1 P
     }
 }
 
+template <typename C>
+__global__ void __launch_bounds__(XT_THREADS, 3)
+    fft_x_fwd(const __grid_constant__ DevGrid G, const __grid_constant__ FftPlan1 P, const __grid_constant__ XArgs A)
+{
+    fft_x_fwd_run<C>(G, P, A, blockIdx.x);
+}
+
 // -------------------- steps 2/4: y transform --------------------
 constexpr int YROWS = 4;   // (k,kx) rows per block
 
 template <typename C>
-__global__ void fft_y(DevGrid G, FftPlan1 P, void *spec_v, int nrows, int inv, Skip sk)
+__device__ __forceinline__ void fft_y_run(const FftPlan1 &P, void *spec_v, int nrows, int inv, const Skip &sk, const int bid)
 {
     if (converged(sk)) return;
     extern __shared__ double2 smraw_y[];
@@ -365,7 +373,7 @@ __global__ void fft_y(DevGrid G, FftPlan1 P, void *spec_v, int nrows, int inv, S
     const int n = P.n;
     const int nt_row = blockDim.x / YROWS;
     const int rr = threadIdx.x / nt_row, lt = threadIdx.x % nt_row;
-    const long long row = (long long)blockIdx.x * YROWS + rr;
+    const long long row = (long long)bid * YROWS + rr;
     C *a = smc + rr * 2 * n, *b = a + n;
     const bool ok = row < nrows;
     if (ok)
@@ -374,6 +382,12 @@ __global__ void fft_y(DevGrid G, FftPlan1 P, void *spec_v, int nrows, int inv, S
     C *res = stockham<C>(P, a, b, lt, nt_row, inv);
     if (ok)
         for (int t = lt; t < n; t += nt_row) spec[row * n + t] = res[t];
+}
+template <typename C>
+__global__ void fft_y(DevGrid G, const __grid_constant__ FftPlan1 P, void *spec_v, int nrows, int inv, Skip sk)
+{
+    (void)G;
+    fft_y_run<C>(P, spec_v, nrows, inv, sk, blockIdx.x);
 }
 
 // -------------------- step 3: vertical tridiagonal --------------------
@@ -405,11 +419,11 @@ __device__ __forceinline__ void st_spec(double2 *s, double2 v) { *s = v; }
 __device__ __forceinline__ void st_spec(float2 *s, double2 v) { *s = make_float2((float)v.x, (float)v.y); }
 
 template <typename C>
-__global__ void tridiag_kernel(DevGrid G, TriArgs T)
+__device__ __forceinline__ void tridiag_run(const DevGrid &G, const TriArgs &T, const int bid)
 {
     if (converged(T.sk)) return;
     const int nh = G.maxx / 2 + 1, maxy = G.maxy, nz = G.nz;
-    const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long col = (long long)bid * blockDim.x + threadIdx.x;
     if (col >= (long long)nh * maxy) return;
     const int kx = (int)(col / maxy), ky = (int)(col % maxy);
     const long long lstride = (long long)nh * maxy;
@@ -475,6 +489,12 @@ __global__ void tridiag_kernel(DevGrid G, TriArgs T)
     }
 }
 
+template <typename C>
+__global__ void tridiag_kernel(const __grid_constant__ DevGrid G, const __grid_constant__ TriArgs T)
+{
+    tridiag_run<C>(G, T, blockIdx.x);
+}
+
 // GAM(k) = C(k-1)/BET(k-1), BET(k) = B(k) - A(k)*GAM(k); zero pivots flagged
 __global__ void gam_kernel(DevGrid G, TriArgs T, double *gam, int *err)
 {
@@ -506,7 +526,7 @@ struct XInvArgs {
 };
 
 template <typename C>
-__global__ void __launch_bounds__(XT_THREADS, 3) fft_x_inv(DevGrid G, FftPlan1 P, XInvArgs A)
+__device__ __forceinline__ void fft_x_inv_run(const DevGrid &G, const FftPlan1 &P, const XInvArgs &A, const int bid)
 {
     if (converged(A.sk)) return;
     using R = typename CT<C>::R;
@@ -515,7 +535,7 @@ __global__ void __launch_bounds__(XT_THREADS, 3) fft_x_inv(DevGrid G, FftPlan1 P
     const C *spec = reinterpret_cast<const C *>(A.spec);
     const int n = P.n, nh = n / 2 + 1, maxy = G.maxy;
     const int groups = (maxy + ROWS - 1) / ROWS;
-    const int k = blockIdx.x / groups + 1, jg = blockIdx.x % groups;
+    const int k = bid / groups + 1, jg = bid % groups;
     const int jb = jg * ROWS;
     const int nt_pair = blockDim.x / (ROWS / 2);
     const int pair = threadIdx.x / nt_pair, lt = threadIdx.x % nt_pair;
@@ -558,13 +578,19 @@ __global__ void __launch_bounds__(XT_THREADS, 3) fft_x_inv(DevGrid G, FftPlan1 P
     }
     (void)sizeof(R);
 }
+template <typename C>
+__global__ void __launch_bounds__(XT_THREADS, 3)
+    fft_x_inv(const __grid_constant__ DevGrid G, const __grid_constant__ FftPlan1 P, const __grid_constant__ XInvArgs A)
+{
+    fft_x_inv_run<C>(G, P, A, blockIdx.x);
+}
 
 // -------------------- step 6: correction --------------------
-__global__ void correction_kernel(DevGrid G, const double *dp, double *mu, double *mv, double *mw, double *p,
-                                  int natural_uv)
+__device__ __forceinline__ void correction_run(const DevGrid &G, const double *dp, double *mu, double *mv, double *mw,
+                                               double *p, int natural_uv, const int bid)
 {
     const int maxx = G.maxx, maxy = G.maxy;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long t = (long long)bid * blockDim.x + threadIdx.x;
     if (t >= (long long)maxx * maxy * G.nz) return;
     const int ix = (int)(t % maxx), jy = (int)((t / maxx) % maxy), k = (int)(t / ((long long)maxx * maxy)) + 1;
     const int i = ix + 4, j = jy + 4;
@@ -586,14 +612,19 @@ __global__ void correction_kernel(DevGrid G, const double *dp, double *mu, doubl
     mu[c] = natural_uv ? mun / d0 : mun;
     mv[c] = natural_uv ? mvn / d0 : mvn;
 }
+__global__ void correction_kernel(const __grid_constant__ DevGrid G, const double *dp, double *mu, double *mv, double *mw,
+                                  double *p, int natural_uv)
+{
+    correction_run(G, dp, mu, mv, mw, p, natural_uv, blockIdx.x);
+}
 
 // -------------------- reductions --------------------
 // per-level sums over the interior, fixed-order tree (deterministic)
-__global__ void level_sums(DevGrid G, const double *x, const double *xold, int old_rep, double dt0,
-                           double *out_mean, double *out_mean_d)
+__device__ __forceinline__ void level_sums_run(const DevGrid &G, const double *x, const double *xold, int old_rep,
+                                               double dt0, double *out_mean, double *out_mean_d, const int bid)
 {
     __shared__ double s1[256], s2[256];
-    const int k = blockIdx.x + 1;
+    const int k = bid + 1;
     const int maxx = G.maxx, maxy = G.maxy;
     const double a0 = __ldg(G.avden0 + k - 1);
     double acc = 0., accd = 0.;
@@ -628,16 +659,26 @@ __global__ void level_sums(DevGrid G, const double *x, const double *xold, int o
         if (out_mean_d) out_mean_d[k - 1] = s2[0] / nn;
     }
 }
+__global__ void level_sums(const __grid_constant__ DevGrid G, const double *x, const double *xold, int old_rep, double dt0,
+                           double *out_mean, double *out_mean_d)
+{
+    level_sums_run(G, x, xold, old_rep, dt0, out_mean, out_mean_d, blockIdx.x);
+}
 
 // w -= <w>_k over all cells (cal_p1 :786-790); natural_w: then w/avden0 (get_velocities)
-__global__ void subtract_level_mean(DevGrid G, double *x, const double *mean, int natural_w)
+__device__ __forceinline__ void subtract_level_mean_run(const DevGrid &G, double *x, const double *mean, int natural_w,
+                                                        const int bid, const int nblk)
 {
     const long long n = G.ps * G.nz;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    for (long long t = (long long)bid * blockDim.x + threadIdx.x; t < n; t += (long long)nblk * blockDim.x) {
         int k = (int)(t / G.ps) + 1;
         const double v = x[t] - __ldg(mean + k - 1);
         x[t] = natural_w ? v / __ldg(G.avden0 + k - 1) : v;
     }
+}
+__global__ void subtract_level_mean(const __grid_constant__ DevGrid G, double *x, const double *mean, int natural_w)
+{
+    subtract_level_mean_run(G, x, mean, natural_w, blockIdx.x, gridDim.x);
 }
 
 __global__ void to_velocity_kernel(DevGrid G, double *mu, double *mv, double *mw)
@@ -729,12 +770,12 @@ __global__ void interior_scatter(DevGrid G, const double *src, double *dst)
 
 // ghost cells := periodic images (statebc/windbc serial periodic branches)
 struct HaloArgs { double *f[MG_MAXF]; int nf; };
-__global__ void halo_fill_kernel(DevGrid G, HaloArgs H)
+__device__ __forceinline__ void halo_fill_run(const DevGrid &G, const HaloArgs &H, const int bid, const int nblk)
 {
     const int nx = G.nx, ny = G.ny, maxx = G.maxx, maxy = G.maxy;
     const long long per_plane = 5LL * nx + 5LL * maxy;
     const long long tot = per_plane * G.nz;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+    for (long long t = (long long)bid * blockDim.x + threadIdx.x; t < tot; t += (long long)nblk * blockDim.x) {
         int k = (int)(t / per_plane) + 1;
         long long g = t % per_plane;
         int i, j;
@@ -753,6 +794,10 @@ __global__ void halo_fill_kernel(DevGrid G, HaloArgs H)
         long long dsti = gidx(G, i, j, k), srci = gidx(G, si, sj, k);
         for (int f = 0; f < H.nf; f++) H.f[f][dsti] = H.f[f][srci];
     }
+}
+__global__ void halo_fill_kernel(const __grid_constant__ DevGrid G, const __grid_constant__ HaloArgs H)
+{
+    halo_fill_run(G, H, blockIdx.x, gridDim.x);
 }
 
 // download conversion (get_velocities / get_scalars, funcpack.f90:65-178,429-485): the
@@ -785,6 +830,73 @@ __global__ void unpack_kernel(DevGrid G, const double *src, double *dst)
         const long long row = t / G.nx;
         dst[row * G.px + (t - row * G.nx)] = src[t];
     }
+}
+
+// -------------------- grouped launches over several domains --------------------
+// Each grouped kernel runs, in block b of its launch, block items[b].b of member
+// items[b].m's own grid with that member's arguments (global memory, written before
+// the launch and unchanged while it runs).  The bodies are the single-domain ones.
+struct XFwdMember { DevGrid G; FftPlan1 P; XArgs A; };
+struct YMember { FftPlan1 P; void *spec; int nrows, inv; Skip sk; };
+struct TriMember { DevGrid G; TriArgs T; };
+struct XInvMember { DevGrid G; FftPlan1 P; XInvArgs A; };
+struct CorrMember { DevGrid G; const double *dp; double *mu, *mv, *mw, *p; int natural_uv; };
+struct LevelMember { DevGrid G; double *w; const double *wold; int wold_rep; double *mean; int natural_w, nb; };
+struct HaloMember { DevGrid G; HaloArgs H; int nb; };
+
+template <typename C>
+__global__ void __launch_bounds__(XT_THREADS, 3) fft_x_fwd_grp(const XFwdMember *__restrict__ mem, const GItem *__restrict__ it)
+{
+    const GItem g = it[blockIdx.x];
+    fft_x_fwd_run<C>(mem[g.m].G, mem[g.m].P, mem[g.m].A, g.b);
+}
+template <typename C>
+__global__ void fft_y_grp(const YMember *__restrict__ mem, const GItem *__restrict__ it)
+{
+    const GItem g = it[blockIdx.x];
+    const YMember &m = mem[g.m];
+    fft_y_run<C>(m.P, m.spec, m.nrows, m.inv, m.sk, g.b);
+}
+template <typename C>
+__global__ void tridiag_grp(const TriMember *__restrict__ mem, const GItem *__restrict__ it)
+{
+    const GItem g = it[blockIdx.x];
+    tridiag_run<C>(mem[g.m].G, mem[g.m].T, g.b);
+}
+template <typename C>
+__global__ void __launch_bounds__(XT_THREADS, 3) fft_x_inv_grp(const XInvMember *__restrict__ mem, const GItem *__restrict__ it)
+{
+    const GItem g = it[blockIdx.x];
+    fft_x_inv_run<C>(mem[g.m].G, mem[g.m].P, mem[g.m].A, g.b);
+}
+__global__ void correction_grp(const CorrMember *__restrict__ mem, const GItem *__restrict__ it)
+{
+    const GItem g = it[blockIdx.x];
+    const CorrMember &m = mem[g.m];
+    correction_run(m.G, m.dp, m.mu, m.mv, m.mw, m.p, m.natural_uv, g.b);
+}
+__global__ void level_sums_grp(const LevelMember *__restrict__ mem, const GItem *__restrict__ it)
+{
+    const GItem g = it[blockIdx.x];
+    const LevelMember &m = mem[g.m];
+    level_sums_run(m.G, m.w, m.wold, m.wold_rep, m.G.dt0, m.mean, nullptr, g.b);
+}
+__global__ void subtract_level_mean_grp(const LevelMember *__restrict__ mem, const GItem *__restrict__ it)
+{
+    const GItem g = it[blockIdx.x];
+    const LevelMember &m = mem[g.m];
+    subtract_level_mean_run(m.G, m.w, m.mean, m.natural_w, g.b, m.nb);
+}
+__global__ void halo_fill_grp(const HaloMember *__restrict__ mem, const GItem *__restrict__ it)
+{
+    const GItem g = it[blockIdx.x];
+    halo_fill_run(mem[g.m].G, mem[g.m].H, g.b, mem[g.m].nb);
+}
+// block m zeroes member m's residual slots
+__global__ void resid_reset_grp(unsigned long long *const *__restrict__ resid)
+{
+    unsigned long long *r = resid[blockIdx.x];
+    for (int q = threadIdx.x; q < MG_MAXPASS; q += blockDim.x) r[q] = 0ull;
 }
 
 // -------------------- host side: plan --------------------
@@ -1353,4 +1465,273 @@ cudaError_t pressure_adjoint(const DevGrid &g, PressurePlan *pp, int nsubp, doub
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+// ======================== grouped launches over several members ========================
+void group_halo(GroupProgram &P, const std::vector<GroupHaloIn> &in)
+{
+    const int n = (int)in.size();
+    std::vector<HaloMember> mem(n);
+    std::vector<int> nb(n);
+    std::vector<double> cost(n, 1.);
+    for (int q = 0; q < n; q++) {
+        const DevGrid &g = *in[q].G;
+        mem[q].G = g;
+        mem[q].H.nf = in[q].nf;
+        for (int f = 0; f < in[q].nf; f++) mem[q].H.f[f] = in[q].f[f];
+        const long long tot = (5LL * g.nx + 5LL * g.maxy) * g.nz;
+        nb[q] = (int)std::min<long long>(4096, (tot + 255) / 256);
+        mem[q].nb = nb[q];
+    }
+    const std::vector<GItem> it = group_items(nb, cost);
+    const size_t mo = P.put(mem), io = P.put(it);
+    const int ni = (int)it.size();
+    P.ops.push_back([=](const unsigned char *d, cudaStream_t s) {
+        halo_fill_grp<<<ni, 256, 0, s>>>((const HaloMember *)(d + mo), (const GItem *)(d + io));
+        return cudaGetLastError();
+    });
+    P.launches++;
+}
+
+namespace {
+// the members' indices grouped by the x transforms' threads per row pair
+std::vector<std::vector<int>> by_xt(const std::vector<GroupProjIn> &in)
+{
+    std::vector<std::vector<int>> out;
+    std::vector<int> keys;
+    for (int q = 0; q < (int)in.size(); q++) {
+        const int xt = in[q].pp->xt;
+        size_t c = std::find(keys.begin(), keys.end(), xt) - keys.begin();
+        if (c == keys.size()) { keys.push_back(xt); out.emplace_back(); }
+        out[c].push_back(q);
+    }
+    return out;
+}
+
+// one grouped x transform (forward with the given per-member arguments, or inverse)
+template <typename C>
+void group_x(GroupProgram &P, const std::vector<GroupProjIn> &in, const std::vector<XArgs> *fwd,
+             const std::vector<XInvArgs> *inv)
+{
+    for (const std::vector<int> &sub : by_xt(in)) {
+        const int n = (int)sub.size();
+        std::vector<int> nb(n);
+        std::vector<double> cost(n);
+        size_t sm = 0;
+        for (int q = 0; q < n; q++) {
+            const DevGrid &g = *in[sub[q]].G;
+            nb[q] = g.nz * ((g.maxy + ROWS - 1) / ROWS);
+            cost[q] = (double)g.maxx;
+            sm = std::max(sm, (size_t)(ROWS / 2) * 2 * g.maxx * sizeof(C));
+        }
+        const std::vector<GItem> it = group_items(nb, cost);
+        const int ni = (int)it.size(), threads = in[sub[0]].pp->xt * (ROWS / 2);
+        size_t mo;
+        if (fwd) {
+            std::vector<XFwdMember> mem(n);
+            for (int q = 0; q < n; q++) mem[q] = XFwdMember{*in[sub[q]].G, in[sub[q]].pp->px, (*fwd)[sub[q]]};
+            mo = P.put(mem);
+        } else {
+            std::vector<XInvMember> mem(n);
+            for (int q = 0; q < n; q++) mem[q] = XInvMember{*in[sub[q]].G, in[sub[q]].pp->px, (*inv)[sub[q]]};
+            mo = P.put(mem);
+        }
+        const size_t io = P.put(it);
+        const bool is_fwd = fwd != nullptr;
+        P.ops.push_back([=](const unsigned char *d, cudaStream_t s) {
+            cudaError_t e;
+            if (is_fwd) {
+                e = cudaFuncSetAttribute(fft_x_fwd_grp<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                if (e != cudaSuccess) return e;
+                fft_x_fwd_grp<C><<<ni, threads, sm, s>>>((const XFwdMember *)(d + mo), (const GItem *)(d + io));
+            } else {
+                e = cudaFuncSetAttribute(fft_x_inv_grp<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                if (e != cudaSuccess) return e;
+                fft_x_inv_grp<C><<<ni, threads, sm, s>>>((const XInvMember *)(d + mo), (const GItem *)(d + io));
+            }
+            return cudaGetLastError();
+        });
+        P.launches++;
+    }
+}
+
+// y transform, tridiagonal, y transform, inverse x transform of every member (pressure_solve_t)
+template <typename C>
+void group_solve(GroupProgram &P, const std::vector<GroupProjIn> &in, const PassCtl &pc)
+{
+    const int n = (int)in.size();
+    std::vector<Skip> sk(n);
+    for (int q = 0; q < n; q++) sk[q] = skip_self(in[q].pp, pc);
+    // y transforms: threads per row = the largest member's knob (the rows' arithmetic does
+    // not depend on it)
+    int yt = 16, tb = 64;
+    size_t smy = 0;
+    std::vector<int> nby(n), nbt(n);
+    std::vector<double> cy(n), ct(n);
+    for (int q = 0; q < n; q++) {
+        const DevGrid &g = *in[q].G;
+        const int nh = g.maxx / 2 + 1;
+        yt = std::max(yt, in[q].pp->yt);
+        tb = std::max(tb, in[q].pp->tb);
+        smy = std::max(smy, (size_t)YROWS * 2 * g.maxy * sizeof(C));
+        nby[q] = (g.nz * nh + YROWS - 1) / YROWS;
+        cy[q] = (double)g.maxy;
+        ct[q] = (double)g.nz;
+    }
+    for (int q = 0; q < n; q++) {
+        const DevGrid &g = *in[q].G;
+        nbt[q] = (int)(((long long)(g.maxx / 2 + 1) * g.maxy + tb - 1) / tb);
+    }
+    for (int dir = 0; dir < 2; dir++) {
+        std::vector<YMember> ym(n);
+        for (int q = 0; q < n; q++) {
+            const DevGrid &g = *in[q].G;
+            ym[q] = YMember{in[q].pp->py, in[q].pp->spec, g.nz * (g.maxx / 2 + 1), dir, sk[q]};
+        }
+        const std::vector<GItem> it = group_items(nby, cy);
+        const size_t mo = P.put(ym), io = P.put(it);
+        const int ni = (int)it.size();
+        auto push_y = [&, mo, io, ni]() {
+            P.ops.push_back([=](const unsigned char *d, cudaStream_t s) {
+                cudaError_t e = cudaFuncSetAttribute(fft_y_grp<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy);
+                if (e != cudaSuccess) return e;
+                fft_y_grp<C><<<ni, yt * YROWS, smy, s>>>((const YMember *)(d + mo), (const GItem *)(d + io));
+                return cudaGetLastError();
+            });
+            P.launches++;
+        };
+        if (dir == 1) {   // the tridiagonal solve sits between the two y transforms
+            std::vector<TriMember> tm(n);
+            for (int q = 0; q < n; q++) {
+                PressurePlan *pp = in[q].pp;
+                TriArgs T{};
+                T.spec = pp->spec; T.gam = pp->gam; T.wv = pp->wv; T.ak = pp->ak; T.ck = pp->ck; T.dka = pp->dka;
+                T.dkb = pp->dkb; T.keep00 = 0; T.sk = sk[q]; T.scratch = pp->tri;
+                tm[q] = TriMember{*in[q].G, T};
+            }
+            const std::vector<GItem> it2 = group_items(nbt, ct);
+            const size_t mo2 = P.put(tm), io2 = P.put(it2);
+            const int ni2 = (int)it2.size();
+            P.ops.push_back([=](const unsigned char *d, cudaStream_t s) {
+                tridiag_grp<C><<<ni2, tb, 0, s>>>((const TriMember *)(d + mo2), (const GItem *)(d + io2));
+                return cudaGetLastError();
+            });
+            P.launches++;
+        }
+        push_y();
+    }
+    std::vector<XInvArgs> xa(n);
+    for (int q = 0; q < n; q++) {
+        const DevGrid &g = *in[q].G;
+        xa[q] = XInvArgs{};
+        xa[q].spec = in[q].pp->spec; xa[q].dp = in[q].pp->dp;
+        xa[q].scale_div = (double)g.maxx * (double)g.maxy;
+        xa[q].sk = sk[q];
+        xa[q].accumulate = pc.refine;
+    }
+    group_x<C>(P, in, nullptr, &xa);
+}
+
+template <typename C>
+void group_projection_t(GroupProgram &P, const std::vector<GroupProjIn> &in, int finalize, int nsub, int nref,
+                        double tol)
+{
+    const int n = (int)in.size();
+    {   // residual slots of every member
+        std::vector<unsigned long long *> r(n);
+        for (int q = 0; q < n; q++) r[q] = in[q].pp->resid;
+        const size_t ro = P.put(r);
+        P.ops.push_back([=](const unsigned char *d, cudaStream_t s) {
+            resid_reset_grp<<<n, 64, 0, s>>>((unsigned long long *const *)(d + ro));
+            return cudaGetLastError();
+        });
+        P.launches++;
+    }
+    for (int ip = 0; ip < nsub; ip++) {
+        const int last = ip == nsub - 1;
+        const int slot0 = ip * (1 + nref);
+        const PassCtl p0 = {slot0, 0, 0, nref > 0, tol};
+        std::vector<XArgs> xf(n);
+        for (int q = 0; q < n; q++) {   // launch_div_rhs
+            PressurePlan *pp = in[q].pp;
+            XArgs a{};
+            a.mode = 0;
+            a.mu = in[q].mu; a.mv = in[q].mv; a.mw = in[q].mw; a.spec = pp->spec; a.dt1 = 1. / in[q].G->dt0;
+            if (p0.store_b) { a.store_b = 1; a.rbuf = pp->rbuf; a.bsum = pp->bsum; }
+            set_resid(pp, p0, a);
+            xf[q] = a;
+        }
+        group_x<C>(P, in, &xf, nullptr);
+        group_solve<C>(P, in, p0);
+        for (int r = 0; r < nref; r++) {
+            const PassCtl pr = {slot0 + 1 + r, 1, r > 0, 0, tol};
+            for (int q = 0; q < n; q++) {   // launch_resid_rhs
+                PressurePlan *pp = in[q].pp;
+                XArgs a{};
+                a.mode = 2;
+                a.rbuf = pp->rbuf; a.bsum = pp->bsum; a.dp = pp->dp;
+                a.ak = pp->ak; a.ck = pp->ck; a.dka = pp->dka; a.dkb = pp->dkb;
+                a.spec = pp->spec; a.dt1 = 1. / in[q].G->dt0;
+                set_resid(pp, pr, a);
+                xf[q] = a;
+            }
+            group_x<C>(P, in, &xf, nullptr);
+            group_solve<C>(P, in, pr);
+        }
+        {   // correction, then the ghost refresh of m and p
+            std::vector<CorrMember> cm(n);
+            std::vector<int> nb(n);
+            std::vector<double> cost(n, 1.);
+            std::vector<GroupHaloIn> h(n);
+            for (int q = 0; q < n; q++) {
+                const DevGrid &g = *in[q].G;
+                cm[q] = CorrMember{g, in[q].pp->dp, in[q].mu, in[q].mv, in[q].mw, in[q].p, finalize && last};
+                nb[q] = (int)(((long long)g.maxx * g.maxy * g.nz + 255) / 256);
+                h[q].G = in[q].G;
+                h[q].nf = 4;
+                h[q].f[0] = in[q].mu; h[q].f[1] = in[q].mv; h[q].f[2] = in[q].mw; h[q].f[3] = in[q].p;
+            }
+            const std::vector<GItem> it = group_items(nb, cost);
+            const size_t mo = P.put(cm), io = P.put(it);
+            const int ni = (int)it.size();
+            P.ops.push_back([=](const unsigned char *d, cudaStream_t s) {
+                correction_grp<<<ni, 256, 0, s>>>((const CorrMember *)(d + mo), (const GItem *)(d + io));
+                return cudaGetLastError();
+            });
+            P.launches++;
+            group_halo(P, h);
+        }
+    }
+    {   // cal_p1 without p1: level means of w, then w -= mean (natural w when finalizing)
+        std::vector<LevelMember> lm(n);
+        std::vector<int> nbs(n), nbm(n);
+        std::vector<double> cs(n), cm(n, 1.);
+        for (int q = 0; q < n; q++) {
+            const DevGrid &g = *in[q].G;
+            nbs[q] = g.nz;
+            cs[q] = (double)g.maxx * g.maxy;
+            nbm[q] = (int)std::min<long long>(1184, (g.ps * g.nz + 2047) / 2048);
+            lm[q] = LevelMember{g, in[q].mw, in[q].wold, in[q].wold_rep, in[q].pp->mean, finalize, nbm[q]};
+        }
+        const std::vector<GItem> its = group_items(nbs, cs), itm = group_items(nbm, cm);
+        const size_t mo = P.put(lm), io1 = P.put(its), io2 = P.put(itm);
+        const int n1 = (int)its.size(), n2 = (int)itm.size();
+        P.ops.push_back([=](const unsigned char *d, cudaStream_t s) {
+            level_sums_grp<<<n1, 256, 0, s>>>((const LevelMember *)(d + mo), (const GItem *)(d + io1));
+            return cudaGetLastError();
+        });
+        P.ops.push_back([=](const unsigned char *d, cudaStream_t s) {
+            subtract_level_mean_grp<<<n2, 256, 0, s>>>((const LevelMember *)(d + mo), (const GItem *)(d + io2));
+            return cudaGetLastError();
+        });
+        P.launches += 2;
+    }
+}
+}  // namespace
+
+void group_projection(GroupProgram &P, const std::vector<GroupProjIn> &in, int finalize, int nsub, int nref, double tol)
+{
+    if (in.empty()) return;
+    if (in[0].pp->mixed) group_projection_t<float2>(P, in, finalize, nsub, nref, tol);
+    else group_projection_t<double2>(P, in, finalize, nsub, nref, tol);
 }

@@ -43,6 +43,28 @@ cudaError_t init_scheme()
     if ((e = cudaFuncSetAttribute(k1_kernel<SCHEME, false, 2, false, K1_FC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)) != cudaSuccess) return e;
     return cudaFuncSetAttribute(k1_kernel<SCHEME, false, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
 }
+template <int SCHEME, int STAGE>
+cudaError_t group_one(int nf, const K1Member *mem, const GItem *items, int nitems, cudaStream_t s)
+{
+    const size_t sm = make_layout(SCHEME, nf).total;
+    if (nf == K1_FC) {
+        cudaError_t e = cudaFuncSetAttribute(k1_group_kernel<SCHEME, false, STAGE, K1_FC>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        k1_group_kernel<SCHEME, false, STAGE, K1_FC><<<nitems, dim3(TX, TY + 1), sm, s>>>(mem, items);
+    } else {
+        cudaError_t e = cudaFuncSetAttribute(k1_group_kernel<SCHEME, false, STAGE>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        k1_group_kernel<SCHEME, false, STAGE><<<nitems, dim3(TX, TY + 1), sm, s>>>(mem, items);
+    }
+    return cudaGetLastError();
+}
+template <int SCHEME>
+cudaError_t group_scheme(int stage, int nf, const K1Member *mem, const GItem *items, int nitems, cudaStream_t s)
+{
+    return stage == 1 ? group_one<SCHEME, 1>(nf, mem, items, nitems, s) : group_one<SCHEME, 2>(nf, mem, items, nitems, s);
+}
 }  // namespace
 
 cudaError_t launch_k1(const DevGrid &g, const K1Args &a, const K1Maps &maps, cudaStream_t s)
@@ -68,4 +90,18 @@ cudaError_t k1_init()
     if ((e = init_scheme<MG_LW>()) != cudaSuccess) return e;
     if ((e = init_scheme<MG_QUICK>()) != cudaSuccess) return e;
     return init_scheme<MG_MUSCL>();
+}
+
+// K1 over the blocks of several members (same scheme, stage and field count; no SGS)
+cudaError_t launch_k1_group(int scheme, int stage, int nf, const K1Member *mem, const GItem *items, int nitems, cudaStream_t s)
+{
+    if (nf <= 0 || nf > MG_MAXF || (stage != 1 && stage != 2) || nitems < 1) return cudaErrorInvalidValue;
+    if (make_layout(scheme, nf).total > 232448) return cudaErrorInvalidValue;
+    switch (scheme) {
+    case MG_WENO: return group_scheme<MG_WENO>(stage, nf, mem, items, nitems, s);
+    case MG_PPM: return group_scheme<MG_PPM>(stage, nf, mem, items, nitems, s);
+    case MG_LW: return group_scheme<MG_LW>(stage, nf, mem, items, nitems, s);
+    case MG_QUICK: return group_scheme<MG_QUICK>(stage, nf, mem, items, nitems, s);
+    default: return group_scheme<MG_MUSCL>(stage, nf, mem, items, nitems, s);
+    }
 }

@@ -16,6 +16,13 @@
 #include <stdint.h>
 
 #include "mimica_gpu.h"
+#ifndef __CUDACC_RTC__
+#include <string.h>
+#include <algorithm>
+#include <functional>
+#include <numeric>
+#include <vector>
+#endif
 
 #define MG_MAXF 16   // max fields handled by one scalar-advection launch
 
@@ -73,6 +80,46 @@ struct alignas(64) K1Maps {
     CUtensorMap mu, mv;
 };
 
+// ---- grouped launches: one launch over the blocks of several domains ----
+// Work item of a grouped launch: the domain (member) and the block of that domain's own
+// grid that one block of the launch runs.  The items are ordered heaviest first.
+struct GItem {
+    int m, b;
+};
+// A recorded sequence of grouped launches: the member and item tables of every launch
+// in one host image (uploaded once to `dev`), and per launch a closure that issues it
+// given the device image.  Recorded once, issued (captured into a graph) many times.
+struct GroupProgram {
+    std::vector<unsigned char> host;
+    std::vector<std::function<cudaError_t(const unsigned char *dev, cudaStream_t s)>> ops;
+    int launches = 0;
+    template <class T> size_t put(const std::vector<T> &v)
+    {
+        const size_t o = (host.size() + 127) / 128 * 128;
+        host.resize(o + v.size() * sizeof(T));
+        if (!v.empty()) memcpy(host.data() + o, v.data(), v.size() * sizeof(T));
+        return o;
+    }
+};
+// The work items of a grouped launch: every block of every member, the members with the
+// costliest blocks first (largest-first list scheduling over the GPU's CTA slots), each
+// member's blocks in order.
+inline std::vector<GItem> group_items(const std::vector<int> &nblk, const std::vector<double> &cost)
+{
+    std::vector<int> ord(nblk.size());
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<GItem> it;
+    for (int m : ord)
+        for (int b = 0; b < nblk[m]; b++) it.push_back(GItem{m, b});
+    return it;
+}
+// K1 arguments of one member, in global memory (the maps 64-byte aligned)
+struct alignas(64) K1Member {
+    K1Maps M;
+    DevGrid G;
+    K1Args A;
+};
 // ---- momentum advection + pgf + buoyancy + stage update (K2) ----
 struct K2Args {
     int stage;
@@ -98,16 +145,37 @@ struct alignas(64) K2Maps {
     CUtensorMap m[3];
 };
 
+// K2 arguments of the members of one grouped launch, passed as the kernel parameter
+// (64 x 440 bytes, inside the 32 KB parameter limit); more members take more launches
+constexpr int K2G_MAX = 64;
+struct K2GroupArgs {
+    DevGrid G;
+    K2Args A;
+};
+struct K2GroupParams {
+    K2GroupArgs a[K2G_MAX];
+};
 // launch wrappers (implemented in the .cu files)
 cudaError_t launch_k1(const DevGrid &g, const K1Args &a, const K1Maps &maps, cudaStream_t s);
 cudaError_t k1_init();
 cudaError_t launch_k1_mixed(const DevGrid &g, const K1Args &a, const K1Maps &maps, cudaStream_t s);
 cudaError_t k1_mixed_init();
 size_t k1_smem_bytes(int scheme, int nf);
+// K1 over the blocks of several members: same scheme, stage (1 or 2) and field count, no SGS
+cudaError_t launch_k1_group(int scheme, int stage, int nf, const K1Member *mem, const GItem *items, int nitems,
+                            cudaStream_t s);
+cudaError_t launch_k1_group_mixed(int scheme, int stage, int nf, const K1Member *mem, const GItem *items, int nitems,
+                                  cudaStream_t s);
 // TMA descriptor of one field buffer (box in doubles)
 int make_field_map(const DevGrid &g, const double *base, int boxx, int boxy, CUtensorMap *map);
 cudaError_t launch_k2(const DevGrid &g, const K2Args &a, const K2Maps &maps, cudaStream_t s);
 cudaError_t launch_k2_mixed(const DevGrid &g, const K2Args &a, const K2Maps &maps, cudaStream_t s);
+// K2 over the blocks of up to K2G_MAX members at one ntime parity (even: ntime % 2 == 0);
+// maps[m]: member m's tensor maps in device memory
+cudaError_t launch_k2_group(int even, const K2GroupParams &P, const K2Maps *maps, const GItem *items, int nitems,
+                            cudaStream_t s);
+cudaError_t launch_k2_group_mixed(int even, const K2GroupParams &P, const K2Maps *maps, const GItem *items, int nitems,
+                                  cudaStream_t s);
 cudaError_t launch_halo_fill(const DevGrid &g, double *const *fields, int nf, cudaStream_t s);
 
 // ---- SGS turbulence diffusion (k_sgs.cu) ----
@@ -255,6 +323,29 @@ struct PassCtl {
 };
 constexpr PassCtl kNoPassCtl = {-1, 0, 0, 0, 0.};
 constexpr int MG_MAXPASS = 64;
+// ---- grouped projection and halo refresh over several members (k_pressure.cu) ----
+struct GroupHaloIn {
+    const DevGrid *G;
+    int nf;
+    double *f[MG_MAXF];
+};
+// the ghost-cell refresh of every member's fields as one launch
+void group_halo(GroupProgram &P, const std::vector<GroupHaloIn> &m);
+struct GroupProjIn {
+    const DevGrid *G;
+    PressurePlan *pp;
+    double *mu, *mv, *mw, *p;   // momentum and pressure of the stage
+    const double *wold;         // w of the stage's input (cal_p1), with its representation
+    int wold_rep;
+};
+// One projection of every member as grouped launches, the same passes as the
+// single-domain path (nsub passes, nref refinement passes each in the mixed form, the
+// correction with its ghost refresh, cal_p1 without p1; finalize: the last correction and
+// cal_p1 leave natural velocities).  All members share the arithmetic form.  The x
+// transforms are launched once per distinct threads-per-row-pair plan knob (the block
+// sums of the refined form's right-hand side follow that thread layout); every other
+// launch covers all members.
+void group_projection(GroupProgram &P, const std::vector<GroupProjIn> &m, int finalize, int nsub, int nref, double tol);
 // zero the residual slots before a projection
 cudaError_t pressure_resid_reset(PressurePlan *pp, cudaStream_t s);
 const unsigned long long *pressure_resid_dev(const PressurePlan *pp);

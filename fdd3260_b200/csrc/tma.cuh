@@ -74,6 +74,14 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return mbar_wait_bounded_n(bar, parity, err, MG_WAIT_CYCLES);
 }
 
+// A tensor map that the host wrote to global memory (cudaMemcpy) before the launch:
+// acquire it for the tensor-map proxy before this thread's first bulk copy through it
+// (system scope: the write came from the host).
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap *map)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"((uint64_t)map) : "memory");
+}
+
 // 3-D tiled bulk copy global -> shared, completion signalled on bar
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar)
 {

@@ -109,10 +109,17 @@ def member_problem(spec: MemberSpec, precision: int = _lib.MG_PREC_FP64, dx: flo
     return d, st
 
 
-class Ensemble:
-    """Members on one device advanced together (``mg_ensemble_*``)."""
+MODES = {"grouped": _lib.MG_ENS_GROUPED, "streams": _lib.MG_ENS_STREAMS}
 
-    def __init__(self, members: list[Mimica]):
+
+class Ensemble:
+    """Members on one device advanced together (``mg_ensemble_*``).
+
+    ``mode`` "grouped" (the default when the members allow it) launches each kernel of a
+    stage once over the blocks of all members; "streams" forks every member's own
+    launches onto its stream.  Both give the same results."""
+
+    def __init__(self, members: list[Mimica], mode: str | None = None):
         if not members:
             raise ValueError("an ensemble needs at least one member")
         self.members = members
@@ -122,6 +129,19 @@ class Ensemble:
         _lib.check(L.mg_ensemble_create(arr, len(members), C.byref(h)), "mg_ensemble_create")
         self._h = h
         self._L = L
+        if mode is not None:
+            self.mode = mode
+
+    @property
+    def mode(self) -> str:
+        m = self._L.mg_ensemble_get_mode(self._h)
+        return {v: k for k, v in MODES.items()}[m]
+
+    @mode.setter
+    def mode(self, mode: str) -> None:
+        if mode not in MODES:
+            raise ValueError(f"unknown ensemble mode {mode!r}")
+        _lib.check(self._L.mg_ensemble_set_mode(self._h, MODES[mode]), "mg_ensemble_set_mode")
 
     def step(self, nsteps: int, ntime0: int = 1) -> None:
         _lib.check(self._L.mg_ensemble_step(self._h, nsteps, ntime0), "mg_ensemble_step")

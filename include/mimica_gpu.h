@@ -158,6 +158,16 @@ int mg_ensemble_step(mg_ens *ens, int nsteps, int ntime0);
 int mg_ensemble_time_steps(mg_ens *ens, int nsteps, int ntime0, double *ms);
 /* kernels launched per ensemble step (all members) */
 int mg_ensemble_launch_count(const mg_ens *ens);
+/* How a step pair of all members is recorded into its CUDA graph:
+ *   MG_ENS_GROUPED  each kernel of a stage is one launch over the blocks of every member
+ *                   (a (member, block) work table, largest blocks first); members must
+ *                   share the arithmetic form, scheme, field count and projection passes
+ *                   and run without SGS (MG_ERR_PARAM otherwise, here and at the step);
+ *   MG_ENS_STREAMS  each member's own launches, on its own stream, forked and joined.
+ * The default is MG_ENS_GROUPED when the members allow it.  The results are identical. */
+enum { MG_ENS_GROUPED = 1, MG_ENS_STREAMS = 2 };
+int mg_ensemble_set_mode(mg_ens *ens, int mode);
+int mg_ensemble_get_mode(const mg_ens *ens);
 
 /* ---- timing and profiling (no counterpart in the reference, whose only timer is the
  * per-step wall clock of src/MAIN/modelctl.f90:395-397) ---- */
