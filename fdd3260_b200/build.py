@@ -43,6 +43,7 @@ SOURCES = [
     ("k_check.cu", ["-fmad=false"]),
     ("k_momadj.cu", ["-fmad=false"]),
     ("k_traj.cu", ["-fmad=false"]),
+    ("k_acoustic.cu", ["-fmad=false"]),
 ]
 
 

@@ -2286,6 +2286,68 @@ extern "C" int mg_fft_solve(mg_ctx *c, const double *tend, double *out)
     return cuerr(cudaStreamSynchronize(c->stream));
 }
 
+// ---- the compressible model's acoustic sub-steps (src/INTEG/prognostic_pressure.f90) ----
+extern "C" int mg_prognostic_pressure(mg_ctx *c, const mg_acoustic *a)
+{
+    if (!c || !a) return MG_ERR_PARAM;
+    if (a->ntau < 1 || (a->im != 1 && a->im != 2) || a->nscal < 0 || a->nscal > MG_MAXF - 4 ||
+        (a->cst_cp != 0 && a->cst_cp != 1))
+        return MG_ERR_PARAM;
+    if (c->G.scal_adv == MG_QUICK) return MG_ERR_PARAM;
+    const double *in[9] = {a->su, a->sv, a->sw, a->sdens, a->ses, a->sqt, a->uadv, a->vadv, a->wadv};
+    double *io[14] = {a->dens, a->p, a->u, a->v, a->w, a->es, a->qt, a->tu, a->tv, a->tw, a->tdens, a->tes, a->tqt,
+                      a->cs2};
+    if (!a->p0) return MG_ERR_PARAM;
+    for (const double *x : in) if (!x) return MG_ERR_PARAM;
+    for (double *x : io) if (!x) return MG_ERR_PARAM;
+    const int ns = a->nscal;
+    if (ns > 0 && (!a->sscal || !a->scal || !a->tscal)) return MG_ERR_PARAM;
+    for (int h = 0; h < ns; h++)
+        if (!a->sscal[h] || !a->scal[h] || !a->tscal[h]) return MG_ERR_PARAM;
+    CKR(cudaSetDevice(c->device));
+    const DevGrid &G = c->G;
+    const size_t fe = c->fbytes / sizeof(double);
+    const int nfield = 9 + 14 + 3 + 3 * ns;   // inputs, in/out, dens2/es2/div, scalar triples
+    double *blk = nullptr;
+    CKR(cudaMalloc(&blk, (size_t)nfield * c->fbytes + 2 * (size_t)G.nz * sizeof(double)));
+    auto fld = [&](int q) { return blk + (size_t)q * fe; };
+    double *p0 = fld(nfield), *lvl = p0 + G.nz;
+    AcousticFields f{};
+    f.nscal = ns;
+    f.p0 = p0;
+    f.su = fld(0); f.sv = fld(1); f.sw = fld(2); f.sdens = fld(3); f.ses = fld(4); f.sqt = fld(5);
+    f.uadv = fld(6); f.vadv = fld(7); f.wadv = fld(8);
+    double **iod[14] = {&f.dens, &f.p, &f.u, &f.v, &f.w, &f.es, &f.qt, &f.tu, &f.tv, &f.tw, &f.tdens, &f.tes, &f.tqt,
+                        &f.cs2};
+    for (int q = 0; q < 14; q++) *iod[q] = fld(9 + q);
+    f.dens2 = fld(23); f.es2 = fld(24); f.div = fld(25);
+    for (int h = 0; h < ns; h++) {
+        f.sscal[h] = fld(26 + 3 * h);
+        f.scal[h] = fld(27 + 3 * h);
+        f.tscal[h] = fld(28 + 3 * h);
+    }
+    cudaError_t e = cudaMemsetAsync(blk, 0, (size_t)nfield * c->fbytes, c->stream);
+    for (int q = 0; q < 9 && e == cudaSuccess; q++) e = h2d(c, fld(q), in[q], cudaMemcpyHostToDevice);
+    for (int q = 0; q < 14 && e == cudaSuccess; q++) e = h2d(c, fld(9 + q), io[q], cudaMemcpyHostToDevice);
+    for (int h = 0; h < ns && e == cudaSuccess; h++) {
+        e = h2d(c, fld(26 + 3 * h), a->sscal[h], cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = h2d(c, fld(27 + 3 * h), a->scal[h], cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = h2d(c, fld(28 + 3 * h), a->tscal[h], cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(p0, a->p0, G.nz * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = launch_acoustic(G, f, a->im, a->ntau, a->cst_cp, lvl, c->stream);
+    for (int q = 0; q < 14 && e == cudaSuccess; q++) e = d2h(c, io[q], fld(9 + q), cudaMemcpyDeviceToHost);
+    for (int h = 0; h < ns && e == cudaSuccess; h++) {
+        e = d2h(c, a->scal[h], fld(27 + 3 * h), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = d2h(c, a->tscal[h], fld(28 + 3 * h), cudaMemcpyDeviceToHost);
+    }
+    const cudaError_t es = cudaStreamSynchronize(c->stream);
+    cudaFree(blk);
+    if (e == cudaErrorInvalidValue) return MG_ERR_PARAM;
+    if (e != cudaSuccess) return cuerr(e);
+    return cuerr(es);
+}
+
 extern "C" int mg_anelastic_pressure(mg_ctx *c, double *mu, double *mv, double *mw, double *p, const double *wold,
                                      double *maxdiv, double *p1)
 {

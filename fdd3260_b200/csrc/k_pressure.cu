@@ -1302,6 +1302,12 @@ cudaError_t launch_cal_p1(const DevGrid &g, PressurePlan *pp, double *mw, const 
     return cudaGetLastError();
 }
 
+cudaError_t launch_level_mean(const DevGrid &g, const double *x, double *mean, cudaStream_t s)
+{
+    level_sums<<<g.nz, 256, 0, s>>>(g, x, nullptr, -1, g.dt0, mean, nullptr);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_to_velocity(const DevGrid &g, double *mu, double *mv, double *mw, cudaStream_t s)
 {
     to_velocity_kernel<<<1184, 256, 0, s>>>(g, mu, mv, mw);

@@ -346,6 +346,26 @@ struct GroupProjIn {
 // sums of the refined form's right-hand side follow that thread layout); every other
 // launch covers all members.
 void group_projection(GroupProgram &P, const std::vector<GroupProjIn> &m, int finalize, int nsub, int nref, double tol);
+// ---- the compressible model's acoustic sub-steps (k_acoustic.cu) ----
+// device fields (halo'd layout) of prognostic_pressure; dens2 and es2 are work fields
+// of the same size, div a work field
+struct AcousticFields {
+    int nscal;
+    const double *p0;
+    const double *su, *sv, *sw, *sdens, *ses, *sqt;
+    const double *sscal[MG_MAXF];
+    const double *uadv, *vadv, *wadv;
+    double *dens, *dens2, *es, *es2, *p, *u, *v, *w, *qt;
+    double *scal[MG_MAXF];
+    double *tu, *tv, *tw, *tdens, *tes, *tqt;
+    double *tscal[MG_MAXF];
+    double *cs2, *div;
+};
+// ntau sub-steps of stage im (lvl: nz doubles of device scratch)
+cudaError_t launch_acoustic(const DevGrid &g, const AcousticFields &f, int im, int ntau, int cst_cp, double *lvl,
+                            cudaStream_t s);
+// the level means of a field over the interior (horav), into nz doubles
+cudaError_t launch_level_mean(const DevGrid &g, const double *x, double *mean, cudaStream_t s);
 // zero the residual slots before a projection
 cudaError_t pressure_resid_reset(PressurePlan *pp, cudaStream_t s);
 const unsigned long long *pressure_resid_dev(const PressurePlan *pp);

@@ -378,6 +378,31 @@ class Mimica:
         _lib.check(self._L.mg_fft_solve(self._h, _lib.ptr(np.ascontiguousarray(tend)), _lib.ptr(out)), "mg_fft_solve")
         return out
 
+    def prognostic_pressure(self, inp, st):
+        """src/INTEG/prognostic_pressure.f90:64 (the compressible model's acoustic
+        sub-steps) on copies of an acoustic.AcousticState with acoustic.AcousticInput;
+        returns the updated copy."""
+        st = st.copy()
+        c = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+        keep = [c(x) for x in (inp.p0, inp.su, inp.sv, inp.sw, inp.sdens, inp.ses, inp.sqt, inp.uadv, inp.vadv,
+                               inp.wadv)]
+        sscal = [c(x) for x in inp.sscal]
+        a = _lib.MgAcoustic()
+        a.im, a.ntau, a.cst_cp, a.nscal = inp.im, inp.ntau, inp.cst_cp, len(st.scal)
+        (a.p0, a.su, a.sv, a.sw, a.sdens, a.ses, a.sqt, a.uadv, a.vadv, a.wadv) = [_lib.ptr(x) for x in keep]
+        for f in st.FIELDS:
+            setattr(st, f, c(getattr(st, f)))
+            setattr(a, f, _lib.ptr(getattr(st, f)))
+        st.scal = [c(x) for x in st.scal]
+        st.tscal = [c(x) for x in st.tscal]
+        arr = lambda xs: (C.POINTER(C.c_double) * max(1, len(xs)))(*[_lib.ptr(x) for x in xs])  # noqa: E731
+        ps, pc, pt = arr(sscal), arr(st.scal), arr(st.tscal)
+        a.sscal = C.cast(ps, C.POINTER(C.POINTER(C.c_double)))
+        a.scal = C.cast(pc, C.POINTER(C.POINTER(C.c_double)))
+        a.tscal = C.cast(pt, C.POINTER(C.POINTER(C.c_double)))
+        _lib.check(self._L.mg_prognostic_pressure(self._h, C.byref(a)), "mg_prognostic_pressure")
+        return st
+
     def anelastic_pressure(self, mu, mv, mw, p, wold):
         """src/PRESSURE/pressure_solver.f90:73 anelastic_pressure; returns (mu, mv, mw, p, maxdiv, p1)."""
         mu, mv, mw, p = (np.array(a, dtype=np.float64, copy=True) for a in (mu, mv, mw, p))

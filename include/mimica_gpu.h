@@ -234,6 +234,42 @@ int mg_fft_solve(mg_ctx *ctx, const double *tend, double *out);
 int mg_anelastic_pressure(mg_ctx *ctx, double *mu, double *mv, double *mw, double *p,
                           const double *wold, double *maxdiv, double *p1);
 
+/* ---- the compressible model's acoustic sub-steps ----
+ * prognostic_pressure (src/INTEG/prognostic_pressure.f90:64-259), the step the
+ * compressible build (no ANELASTIC) runs in place of the projection: ntau sub-steps of
+ * dtau = dt0/ntau at integrator stage im, for the dry ISENTROPIC CONSERVATIVE build
+ * (es = density-weighted potential temperature, div_pressure compiled out, no
+ * hydrometeors, the two-stage scheme, sponge off).  Each sub-step advects density and
+ * es with the unlimited Lax-Wendroff faces (advq_lw_nolim.f90) on wind_adv, integrates
+ * every scalar with its slow tendency (integ_scal), evaluates the equation of state
+ * (thermodynamics.f90:74-294) and integrates the momentum with the pressure gradient,
+ * the density buoyancy and the divergence damping 0.2 dtau <cs2>_k grad(div m)
+ * (integ_mom).  The tendency accumulators tu..tqt, tscal (integpack's tend) are read
+ * and updated.  All arrays are nx*ny*nz host arrays of the reference layout with their
+ * ghost cells; the grid, dt0, den0 and the metrics are the context's.  The context's
+ * scheme selects the faces: every scheme but quick uses the Lax-Wendroff ones
+ * (advection.f90:582-592); quick (advq_quick_nolim.f90) is not built: MG_ERR_PARAM. */
+typedef struct mg_acoustic {
+    int im;                          /* integrator stage: 1 or 2 */
+    int ntau;                        /* sub-steps, >= 1 */
+    int cst_cp;                      /* 1: cp_a, cv_a; 0: moist-air cp, cv from qt */
+    int nscal;                       /* passive scalars, 0 .. 12 */
+    const double *p0;                /* base-state pressure, nz */
+    const double *su, *sv, *sw;      /* winds: the step's slow momentum tendencies */
+    const double *sdens, *ses, *sqt; /* pressures%dens, states%es, states%qt */
+    const double *const *sscal;      /* states%scal, nscal arrays */
+    const double *uadv, *vadv, *wadv;/* wind_adv */
+    double *dens, *p;                /* in/out: pressure%dens, pressure%p (p is overwritten) */
+    double *u, *v, *w;               /* in/out: momentum */
+    double *es, *qt;                 /* in/out: density-weighted es, qt */
+    double *const *scal;             /* in/out: density-weighted passive scalars */
+    double *tu, *tv, *tw;            /* in/out: tendency accumulators (interior cells written) */
+    double *tdens, *tes, *tqt;
+    double *const *tscal;
+    double *cs2;                     /* out: thermo_prop%cs2 */
+} mg_acoustic;
+int mg_prognostic_pressure(mg_ctx *ctx, const mg_acoustic *a);
+
 /* ---- per-step checks and time-step control: checkall (src/IO/check.f90:59-95) ----
  * checkx (:341-417) of es (theta) and qt, then checkwind (:102-337, ANELASTIC: the
  * advective CFL only) on the resident level-n state, as the time loop calls it after

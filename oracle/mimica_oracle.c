@@ -908,10 +908,68 @@ static void advs_quick_z(const mo_grid *g, const double *x, const double *w, dou
     free(F);
 }
 
+/* src/TOOLS/advq_lw_nolim.f90:54-111 (advsx_lw_nl; advsy_lw_nl :114-185 is the same
+ * along y without CHANNEL): the unlimited Lax-Wendroff faces of the acoustic sub-steps.
+ * The Courant number uses dt0, as the reference does, also inside the sub-steps. */
+static void advs_lwnl_h(const mo_grid *g, int n, int i1, int i2, double d, const double *x, const double *u,
+                        double *xa, int adv)
+{
+    const double dx1 = 1. / d;
+    double *F = dalloc((size_t)n);
+    for (int i = i1 - 1; i <= i2; i++) {
+        const double uu = P1(u, i + 1);
+        const double mu = fabs(uu) * g->dt0 * dx1;
+        const double xx = P1(x, i);
+        const double ffip1 = P1(x, i + 1) - xx;
+        const double fl = xx + 0.5 * ffip1 * (1. - mu);
+        const double fr = P1(x, i + 1) - 0.5 * ffip1 * (1. - mu);
+        P1(F, i) = 0.5 * fl * (uu + fabs(uu)) + 0.5 * fr * (uu - fabs(uu));
+    }
+    double fold = P1(F, i1 - 1);
+    for (int i = i1; i <= i2; i++) {
+        P1(xa, i) = P1(xa, i) + (P1(F, i) - fold) * dx1;
+        fold = P1(F, i);
+    }
+    if (adv) {
+        double uu = P1(u, i2 + 1);
+        for (int i = i2; i >= i1; i--) {
+            P1(xa, i) = P1(xa, i) - P1(x, i) * (uu - P1(u, i)) * dx1;
+            uu = P1(u, i);
+        }
+    }
+    free(F);
+}
+
+/* src/TOOLS/advq_lw_nolim.f90:188-265 (advsz_lw_nl), 'nnf' bottom and top, flux form */
+static void advs_lwnl_z(const mo_grid *g, const double *x, const double *w, double *xa)
+{
+    const int nz = g->nz;
+    const double *dz1 = g->dz1, *dz1w = g->dz1w;
+    double *F = dalloc((size_t)nz);
+    for (int k = 1; k <= nz - 1; k++) {
+        const double ww = P1(w, k + 1);
+        const double mu = fabs(ww) * g->dt0 * P1(dz1, k);
+        const double xx = P1(x, k);
+        const double ffip1 = (P1(x, k + 1) - xx) * P1(dz1, k);
+        const double fl = xx + 0.5 * ffip1 * (1. - mu) / P1(dz1w, k);
+        const double fr = P1(x, k + 1) - 0.5 * ffip1 * (1. - mu) / P1(dz1w, k);
+        P1(F, k) = 0.5 * fl * (ww + fabs(ww)) + 0.5 * fr * (ww - fabs(ww));
+    }
+    double fold = P1(F, 1);
+    for (int k = 2; k <= nz - 1; k++) {
+        P1(xa, k) = P1(xa, k) + (P1(F, k) - fold) * P1(dz1w, k);
+        fold = P1(F, k);
+    }
+    P1(xa, 1) = P1(xa, 1) + (P1(F, 1) - 0.) * P1(dz1w, 1);
+    P1(xa, nz) = P1(xa, nz) + (0. - P1(F, nz - 1)) * P1(dz1w, nz);
+    free(F);
+}
+
 void mo_advs_h(const mo_grid *g, int scheme, int n, int i1, int i2, double d, const double *x,
                const double *u, double *xa, int adv)
 {
     switch (scheme) {
+    case MO_LW_NL: advs_lwnl_h(g, n, i1, i2, d, x, u, xa, adv); break;
     case MO_WENO: advs_weno_h(n, i1, i2, d, x, u, xa, adv); break;
     case MO_PPM: advs_ppm_h(g, n, i1, i2, d, x, u, xa, adv); break;
     case MO_LW: advs_lw_h(g, n, i1, i2, d, x, u, xa, adv); break;
@@ -923,6 +981,7 @@ void mo_advs_h(const mo_grid *g, int scheme, int n, int i1, int i2, double d, co
 void mo_advs_z(const mo_grid *g, int scheme, const double *x, const double *w, double *xa, int adv)
 {
     switch (scheme) {
+    case MO_LW_NL: advs_lwnl_z(g, x, w, xa); break;
     case MO_WENO: advs_weno_z(g, x, w, xa, adv); break;
     case MO_PPM: advs_ppm_z(g, x, w, xa, adv); break;
     case MO_LW: advs_lw_z(g, x, w, xa, adv); break;
@@ -935,7 +994,14 @@ void mo_advs_z(const mo_grid *g, int scheme, const double *x, const double *w, d
  * 3-D scalar advection: src/TOOLS/advection.f90 advection_x/y/z :556-798
  * (pencil loops with copy-in temporaries) and advection_ac :801-915.
  * ==================================================================== */
+static void advection_dir_s(const mo_grid *g, int scheme, int dir, const double *xtmp, const double *uadv, double *xs,
+                            int adv);
 void mo_advection_dir(const mo_grid *g, int dir, const double *xtmp, const double *uadv, double *xs, int adv)
+{
+    advection_dir_s(g, g->scal_adv, dir, xtmp, uadv, xs, adv);
+}
+static void advection_dir_s(const mo_grid *g, int scheme, int dir, const double *xtmp, const double *uadv, double *xs,
+                            int adv)
 {
     const int nx = g->nx, ny = g->ny, nz = g->nz;
     const int its = 4, ite = nx - 2, jts = 4, jte = ny - 2;
@@ -954,7 +1020,7 @@ void mo_advection_dir(const mo_grid *g, int dir, const double *xtmp, const doubl
                         P1(pu, i) = uadv[IX(g, i, j, k)];
                         P1(pa, i) = xx[IX(g, i, j, k)];
                     }
-                    mo_advs_h(g, g->scal_adv, nx, its, ite, g->dx, px, pu, pa, adv);
+                    mo_advs_h(g, scheme, nx, its, ite, g->dx, px, pu, pa, adv);
                     for (int i = 1; i <= nx; i++) xx[IX(g, i, j, k)] = P1(pa, i);
                 }
         } else if (dir == 1) {
@@ -966,7 +1032,7 @@ void mo_advection_dir(const mo_grid *g, int dir, const double *xtmp, const doubl
                         P1(pu, j) = uadv[IX(g, i, j, k)];
                         P1(pa, j) = xx[IX(g, i, j, k)];
                     }
-                    mo_advs_h(g, g->scal_adv, ny, jts, jte, g->dy, px, pu, pa, adv);
+                    mo_advs_h(g, scheme, ny, jts, jte, g->dy, px, pu, pa, adv);
                     for (int j = 1; j <= ny; j++) xx[IX(g, i, j, k)] = P1(pa, j);
                 }
         } else {
@@ -978,7 +1044,7 @@ void mo_advection_dir(const mo_grid *g, int dir, const double *xtmp, const doubl
                         P1(pu, k) = uadv[IX(g, i, j, k)];
                         P1(pa, k) = xx[IX(g, i, j, k)];
                     }
-                    mo_advs_z(g, g->scal_adv, px, pu, pa, adv);
+                    mo_advs_z(g, scheme, px, pu, pa, adv);
                     for (int k = 1; k <= nz; k++) xx[IX(g, i, j, k)] = P1(pa, k);
                 }
         }
@@ -1705,6 +1771,150 @@ void mo_horav(const mo_grid *g, const double *x, double *xav)
             }
         P1(xav, k) = s / dmax2(ii, 1.);
     }
+}
+
+/* ======================================================================
+ * The compressible model's acoustic sub-steps: src/INTEG/prognostic_pressure.f90:64-259
+ * (prognostic_pressure) for the dry ISENTROPIC CONSERVATIVE build, with its callees:
+ * advect with limiter=.false., full=.false. (src/TOOLS/advection.f90:84-314, unsplit),
+ * integ_scal / integ_mom (src/INTEG/integpack.f90:54-260, sponge off),
+ * equation_of_state (src/TOOLS/thermodynamics.f90:74-294, pt_in, density_in,
+ * conservative), buoyancy (:472-493, non-ANELASTIC branch), caldiv and gradp
+ * (src/TOOLS/gradients.f90:986-1052,1205-1292, gpz(1) = 0 without ANELASTIC) and horav.
+ * ==================================================================== */
+static void gradp_compressible(const mo_grid *g, double *p, double *gpx, double *gpy, double *gpz)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    const double dx1 = 1. / g->dx, dy1 = 1. / g->dy;
+    const size_t nc = ncell(g);
+    mo_statebc(g, p);
+    memset(gpx, 0, nc * sizeof(double));
+    memset(gpy, 0, nc * sizeof(double));
+    memset(gpz, 0, nc * sizeof(double));
+    for (int k = 1; k <= nz; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) {
+                const size_t c = IX(g, i, j, k);
+                gpx[c] = (p[c] - p[IX(g, i - 1, j, k)]) * dx1;
+                gpy[c] = (p[c] - p[IX(g, i, j - 1, k)]) * dy1;
+            }
+    for (int k = 2; k <= nz; k++)
+        for (int j = 4; j <= ny - 2; j++)
+            for (int i = 4; i <= nx - 2; i++) {
+                const size_t c = IX(g, i, j, k);
+                gpz[c] = (p[c] - p[IX(g, i, j, k - 1)]) * P1(g->dz1, k - 1);
+            }
+}
+
+int mo_prognostic_pressure(const mo_grid *g, const mo_acoustic *a, const mo_acoustic_state *s)
+{
+    if (g->scal_adv == MO_QUICK) return 1;
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    const double grav = 9.81, pref = 100000., cp_a = 1004., cv_a = 716., cp_v = 1827., cv_v = 1388.5;
+    const double adiv = 0.2;                       /* prognostic_pressure.f90:53 */
+    const double a_lm = a->im == 1 ? 1. : 0.5, b_lm = a->im == 1 ? 0. : 1.;
+    const double tau1 = 1. / (double)a->ntau;
+    const double dtau = g->dt0 * tau1;
+    const size_t nc = ncell(g);
+    double *densa = dalloc(nc), *esa = dalloc(nc);
+    double *gpx = dalloc(nc), *gpy = dalloc(nc), *gpz = dalloc(nc), *div = dalloc(nc);
+    double *gdx = dalloc(nc), *gdy = dalloc(nc), *gdz = dalloc(nc), *buoy = dalloc(nc);
+    double *wu = dalloc(nc), *wv = dalloc(nc), *ww = dalloc(nc), *damp = dalloc((size_t)nz);
+    for (int it = 1; it <= a->ntau; it++) {
+        /* pressurea = pressures, statea = states, winda = 0, buoy = 0 */
+        memcpy(densa, a->sdens, nc * sizeof(double));
+        memcpy(esa, a->ses, nc * sizeof(double));
+        memset(wu, 0, nc * sizeof(double));
+        memset(wv, 0, nc * sizeof(double));
+        memset(ww, 0, nc * sizeof(double));
+        memset(buoy, 0, nc * sizeof(double));
+        /* advect: density (adv=.false.) then es (flux form, CONSERVATIVE), x, y, z */
+        advection_dir_s(g, MO_LW_NL, 0, s->dens, a->uadv, densa, 0);
+        advection_dir_s(g, MO_LW_NL, 0, s->es, a->uadv, esa, 0);
+        advection_dir_s(g, MO_LW_NL, 1, s->dens, a->vadv, densa, 0);
+        advection_dir_s(g, MO_LW_NL, 1, s->es, a->vadv, esa, 0);
+        advection_dir_s(g, MO_LW_NL, 2, s->dens, a->wadv, densa, 0);
+        advection_dir_s(g, MO_LW_NL, 2, s->es, a->wadv, esa, 0);
+        /* integ_scal (integpack.f90:171-217) */
+        for (size_t c = 0; c < nc; c++) {
+            s->tdens[c] = densa[c] + b_lm * s->tdens[c];
+            s->tes[c] = esa[c] + b_lm * s->tes[c];
+            s->tqt[c] = a->sqt[c] + b_lm * s->tqt[c];
+            for (int h = 0; h < a->nscal; h++) s->tscal[h][c] = a->sscal[h][c] + b_lm * s->tscal[h][c];
+            s->dens[c] = s->dens[c] + a_lm * dtau * s->tdens[c];
+            s->es[c] = s->es[c] + a_lm * dtau * s->tes[c];
+            s->qt[c] = s->qt[c] + a_lm * dtau * s->tqt[c];
+            for (int h = 0; h < a->nscal; h++) s->scal[h][c] = s->scal[h][c] + a_lm * dtau * s->tscal[h][c];
+        }
+        /* pressurebc, statebc */
+        mo_statebc(g, s->dens);
+        mo_statebc(g, s->p);
+        mo_statebc(g, s->es);
+        mo_statebc(g, s->qt);
+        for (int h = 0; h < a->nscal; h++) mo_statebc(g, s->scal[h]);
+        /* equation_of_state(state, density_in=dens, pressure_out=p, thermo_out, conservative) */
+        for (int k = 1; k <= nz; k++)
+            for (int j = 1; j <= ny; j++)
+                for (int i = 1; i <= nx; i++) {
+                    const size_t c = IX(g, i, j, k);
+                    const double d = s->dens[c];
+                    const double es = s->es[c] / d, qt = s->qt[c] / d;
+                    double cp = cp_a, cv = cv_a;
+                    if (!a->cst_cp) {
+                        const double qv = qt;
+                        cp = (1. - qt) * cp_a + cp_v * qv;
+                        cv = (1. - qt) * cv_a + cv_v * qv;
+                    }
+                    const double exn = pow(d * (cp - cv) * es / pref, (cp_a - cv_a) / cv_a);
+                    const double tt = es * exn;
+                    const double pp = d * (cp - cv) * tt;
+                    s->cs2[c] = cp_a / cv_a * pp / d;
+                    s->p[c] = pp - P1(a->p0, k);
+                    s->es[c] = es * d;
+                    s->qt[c] = qt * d;
+                }
+        /* gradp(pressure%p, wind%w) */
+        gradp_compressible(g, s->p, gpx, gpy, gpz);
+        /* buoyancy(pressure%dens) */
+        for (int k = 2; k <= nz; k++)
+            for (int j = 1; j <= ny; j++)
+                for (int i = 1; i <= nx; i++) {
+                    const size_t c = IX(g, i, j, k), cm = IX(g, i, j, k - 1);
+                    buoy[c] = -(0.5 * grav * (s->dens[c] + s->dens[cm] - P1(g->den0, k) - P1(g->den0, k - 1)));
+                }
+        for (int j = 1; j <= ny; j++)
+            for (int i = 1; i <= nx; i++) {
+                const size_t c = IX(g, i, j, 1);
+                buoy[c] = -(grav * (s->dens[c] - P1(g->den0, 1)));
+            }
+        /* divergence damping: caldiv(wind), gradp(div, zero), horav(cs2) */
+        mo_caldiv(g, s->u, s->v, s->w, div);
+        gradp_compressible(g, div, gdx, gdy, gdz);
+        mo_horav(g, s->cs2, damp);
+        for (int k = 1; k <= nz; k++)
+            for (int j = 4; j <= ny - 2; j++)
+                for (int i = 4; i <= nx - 2; i++) {
+                    const size_t c = IX(g, i, j, k);
+                    wu[c] = a->su[c] - gpx[c] + adiv * dtau * P1(damp, k) * gdx[c];
+                    wv[c] = a->sv[c] - gpy[c] + adiv * dtau * P1(damp, k) * gdy[c];
+                    ww[c] = a->sw[c] - gpz[c] + adiv * dtau * P1(damp, k) * gdz[c] + buoy[c];
+                }
+        for (int j = 1; j <= ny; j++)
+            for (int i = 1; i <= nx; i++) ww[IX(g, i, j, 1)] = 0.;
+        /* integ_mom (integpack.f90:100-119, tauw = 1) */
+        for (size_t c = 0; c < nc; c++) {
+            s->tu[c] = wu[c] + b_lm * s->tu[c];
+            s->tv[c] = wv[c] + b_lm * s->tv[c];
+            s->tw[c] = ww[c] + b_lm * s->tw[c];
+            s->u[c] = s->u[c] + a_lm * dtau * s->tu[c];
+            s->v[c] = s->v[c] + a_lm * dtau * s->tv[c];
+            s->w[c] = 1. * (s->w[c] + a_lm * dtau * s->tw[c]);
+        }
+        windbc(g, s->u, s->v, s->w);
+    }
+    free(densa); free(esa); free(gpx); free(gpy); free(gpz); free(div);
+    free(gdx); free(gdy); free(gdz); free(buoy); free(wu); free(wv); free(ww); free(damp);
+    return 0;
 }
 
 /* src/PRESSURE/pressure_solver.f90:415-459 */

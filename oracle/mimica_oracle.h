@@ -28,6 +28,8 @@ extern "C" {
 #endif
 
 enum { MO_WENO = 0, MO_PPM = 1, MO_MUSCL = 2, MO_LW = 3, MO_QUICK = 4 };
+/* the unlimited Lax-Wendroff faces of the acoustic sub-steps (advq_lw_nolim.f90) */
+enum { MO_LW_NL = 16 };
 enum { MO_LIM_MINMOD = 0, MO_LIM_VL = 1, MO_LIM_MC = 2, MO_LIM_DEFAULT = 3 };
 
 /* SGS turbulence switches (src/TYPES/shared_data.f90, INCLUDE/default.h), the
@@ -138,6 +140,34 @@ void mo_checkx(const mo_grid *g, const double *x, double *mn, double *mx, int *l
  */
 int mo_step(const mo_grid *g, int ntime, double *u, double *v, double *w, double *p,
             double *dens, int nsc, double **scal, int iqt, double *maxdiv, double *p1);
+
+/* ---- the compressible model's acoustic sub-steps (src/INTEG/prognostic_pressure.f90) ----
+ * Dry ISENTROPIC CONSERVATIVE build: es is density-weighted potential temperature,
+ * div_pressure is compiled out, nhydro = 0, sorder = 2 (Heun coefficients of stage im),
+ * sponge off.  All arrays nx*ny*nz. */
+typedef struct mo_acoustic {
+    int im;                        /* integrator stage: a_lm, b_lm (INCLUDE/integ.h) */
+    int ntau;                      /* acoustic sub-steps per dt0 */
+    int cst_cp;                    /* 1: cp_a, cv_a; 0: cp, cv of moist air from qt */
+    int nscal;                     /* passive scalars */
+    const double *p0;              /* base-state pressure (nz) */
+    const double *su, *sv, *sw;    /* winds: the step's slow momentum tendencies */
+    const double *sdens, *ses, *sqt;   /* pressures%dens, states%es, states%qt */
+    const double *const *sscal;    /* states%scal */
+    const double *uadv, *vadv, *wadv;  /* wind_adv */
+} mo_acoustic;
+typedef struct mo_acoustic_state {
+    double *dens, *p;              /* pressure%dens, pressure%p */
+    double *u, *v, *w;             /* wind (momentum) */
+    double *es, *qt;               /* state (density-weighted) */
+    double **scal;
+    double *tu, *tv, *tw;          /* the integrator's tendency accumulators (integpack tend) */
+    double *tdens, *tes, *tqt;
+    double **tscal;
+    double *cs2;                   /* out: thermo_prop%cs2 */
+} mo_acoustic_state;
+/* returns 0, or 1 for scal_adv = quick (advq_quick_nolim.f90, not restated) */
+int mo_prognostic_pressure(const mo_grid *g, const mo_acoustic *a, const mo_acoustic_state *s);
 
 #ifdef __cplusplus
 }

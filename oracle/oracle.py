@@ -50,6 +50,22 @@ class MoGrid(C.Structure):
     ]
 
 
+class MoAcoustic(C.Structure):
+    _fields_ = [
+        ("im", C.c_int), ("ntau", C.c_int), ("cst_cp", C.c_int), ("nscal", C.c_int), ("p0", _dp),
+        ("su", _dp), ("sv", _dp), ("sw", _dp), ("sdens", _dp), ("ses", _dp), ("sqt", _dp),
+        ("sscal", C.POINTER(_dp)), ("uadv", _dp), ("vadv", _dp), ("wadv", _dp),
+    ]
+
+
+class MoAcousticState(C.Structure):
+    _fields_ = [
+        ("dens", _dp), ("p", _dp), ("u", _dp), ("v", _dp), ("w", _dp), ("es", _dp), ("qt", _dp),
+        ("scal", C.POINTER(_dp)), ("tu", _dp), ("tv", _dp), ("tw", _dp), ("tdens", _dp), ("tes", _dp),
+        ("tqt", _dp), ("tscal", C.POINTER(_dp)), ("cs2", _dp),
+    ]
+
+
 _libs = {}
 
 
@@ -245,6 +261,33 @@ class Oracle:
                 raise RuntimeError(f"oracle tridiagonal pivot error {rc}")
         st.scal = scal
         return st, md.value, p1
+
+    def prognostic_pressure(self, inp, st):
+        """The acoustic sub-steps (prognostic_pressure.f90) on copies of an
+        acoustic.AcousticState; returns the updated copy."""
+        st = st.copy()
+        c = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+        keep = [c(a) for a in (inp.p0, inp.su, inp.sv, inp.sw, inp.sdens, inp.ses, inp.sqt, inp.uadv, inp.vadv,
+                               inp.wadv)]
+        sscal = [c(a) for a in inp.sscal]
+        a = MoAcoustic()
+        a.im, a.ntau, a.cst_cp, a.nscal = inp.im, inp.ntau, inp.cst_cp, len(st.scal)
+        (a.p0, a.su, a.sv, a.sw, a.sdens, a.ses, a.sqt, a.uadv, a.vadv, a.wadv) = [P(x) for x in keep]
+        sp = (_dp * max(1, len(sscal)))(*[P(x) for x in sscal])
+        a.sscal = C.cast(sp, C.POINTER(_dp))
+        s = MoAcousticState()
+        for f in ("dens", "p", "u", "v", "w", "es", "qt", "tu", "tv", "tw", "tdens", "tes", "tqt", "cs2"):
+            setattr(st, f, c(getattr(st, f)))
+            setattr(s, f, P(getattr(st, f)))
+        st.scal = [c(x) for x in st.scal]
+        st.tscal = [c(x) for x in st.tscal]
+        scp = (_dp * max(1, len(st.scal)))(*[P(x) for x in st.scal])
+        tsp = (_dp * max(1, len(st.tscal)))(*[P(x) for x in st.tscal])
+        s.scal, s.tscal = C.cast(scp, C.POINTER(_dp)), C.cast(tsp, C.POINTER(_dp))
+        rc = self.L.mo_prognostic_pressure(self.gp, C.byref(a), C.byref(s))
+        if rc:
+            raise RuntimeError("the oracle's acoustic sub-steps do not cover scal_adv = quick")
+        return st
 
     def buoyancy(self, dens, es, qt=None):
         out = np.zeros(self.d.shape)
