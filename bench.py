@@ -338,10 +338,12 @@ def main():
                     help="both (default): the plain FP64 form is the headline, the mixed form (FP32 "
                          "stencils/fluxes/spectra, FP64 state) is reported beside it with its error against "
                          "the FP64 form; fp64 / mixed: one form only")
-    ap.add_argument("--workload", default="cumulus", choices=["cumulus", "ensemble", "capacity"],
+    ap.add_argument("--workload", default="cumulus", choices=["cumulus", "ensemble", "capacity", "acoustic"],
                     help="cumulus: the 512x512x256 shallow-cumulus domain (default); ensemble: 64 independent "
                          "warm-bubble domains of seeded uneven sizes, batched per GPU, sharded over ranks; "
-                         "capacity: one 1024x1024x256 domain with 3 momentum + density + 12 scalars (mixed form)")
+                         "capacity: one 1024x1024x256 domain with 3 momentum + density + 12 scalars (mixed form); "
+                         "acoustic: the compressible model's acoustic sub-steps (prognostic_pressure) on "
+                         "--maxx x --maxx x --nz")
     ap.add_argument("--sgs", default="none", choices=["none", "smagorinsky"],
                     help="smagorinsky: SGS turbulence diffusion on (Smagorinsky-Lilly, pran=-0.4, zdec=2400 m, "
                          "surface heat, moisture and momentum fluxes), as the BOMEX template runs it")
@@ -371,6 +373,8 @@ def main():
         return run_ensemble(args, ws, rank, local)
     if args.workload == "capacity":
         return run_capacity(args, ws, rank, local)
+    if args.workload == "acoustic":
+        return run_acoustic(args, ws, rank, local)
     metric = "Mcell-updates/s per integrator step (2-stage Heun + projection)"
     lim = f" ({args.limiter} limiter)" if args.scheme == "muscl" else ""
     cfg = {"workload": f"shallow-cumulus domain {args.maxx}x{args.maxx}x{args.nz}, dx=dy=25 m, stretched dz 10->100 m, "
@@ -684,6 +688,82 @@ def run_capacity(args, ws, rank, local):
                 "device_bytes": dev_bytes, "maxdiv_after": md, "upload_s": t_up,
                 "e2e": None, "e2e_note": "not measured: 15 fields of 2.2 GB cross the bus each way per step",
                 "cpu_baseline": None}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# algorithmic HBM bytes per interior cell of one acoustic sub-step (FP64), with nscal
+# passive scalars: the scalar kernel reads dens, es, uadv, vadv, wadv, sdens, ses, sqt,
+# tdens, tes, tqt, qt and writes dens', es', tdens, tes, tqt, qt (18 fields); the
+# equation of state reads dens, es, qt and writes cs2, p, es, qt (7); the divergence
+# reads u, v, w and writes div (4); the momentum kernel reads p, div, dens, su, sv, sw,
+# tu, tv, tw, u, v, w and writes tu, tv, tw, u, v, w (18); each passive scalar reads
+# sscal, tscal, scal and writes tscal, scal (5)
+def acoustic_alg_bytes(nscal: int) -> int:
+    return 8 * (18 + 7 + 4 + 18 + 5 * nscal)
+
+
+def run_acoustic(args, ws, rank, local):
+    """The compressible model's acoustic sub-steps (prognostic_pressure.f90, dry ISENTROPIC
+    CONSERVATIVE build) on one domain per rank: ntau = 8 sub-steps of stage 1 per call,
+    W untimed and K timed calls on the resident fields (device time, CUDA events),
+    value = all ranks' cell sub-steps / max over ranks of the time."""
+    from fdd3260_b200 import Mimica, acoustic, config
+    dev = local if ws > 1 else 0
+    d = config.warm_bubble_domain(args.maxx, args.maxx, args.nz, dx=50.0, dy=50.0, dz=40.0, dt0=0.5)
+    nscal, ntau = 1, 8
+    inp, st = acoustic.acoustic_case(d, seed=31 + rank, im=1, ntau=ntau, nscal=nscal)
+    with Mimica(d, nscal=1, device=dev) as m:
+        dist_barrier(ws)
+        with ClockSampler(local) as clk:
+            _, ms = m.prognostic_pressure(inp, st, reps=args.steps, warmup=args.warmup)
+        # end to end: one call from host arrays (upload, ntau sub-steps, download)
+        t0 = time.perf_counter()
+        m.prognostic_pressure(inp, st)
+        e2e_s = time.perf_counter() - t0
+    ms = dist_max(ms, ws)
+    e2e_s = dist_max(e2e_s, ws)
+    cells = d.cells
+    value = ws * cells * ntau / (ms / 1e3) / 1e6
+    pk, pk_src = peaks()
+    ab = acoustic_alg_bytes(nscal)
+    achieved = ab * cells * ntau / (ms / 1e3) / 1e9
+    nio = 16 + 3 * nscal   # host arrays uploaded (inputs and state) and 14 + 2 nscal downloaded
+    cpu = None
+    if rank == 0 and not args.skip_cpu:
+        from oracle import oracle as O
+        ds = config.warm_bubble_domain(64, 64, args.nz, dx=50.0, dy=50.0, dz=40.0, dt0=0.5)
+        si, ss = acoustic.acoustic_case(ds, seed=31, im=1, ntau=ntau, nscal=nscal)
+        orc = O.Oracle(ds)
+        orc.prognostic_pressure(si, ss)
+        n, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < min(args.cpu_seconds, 20.0) and n < 20:
+            orc.prognostic_pressure(si, ss)
+            n += 1
+        dt = time.perf_counter() - t0
+        cpu = {"value": ds.cells * ntau * n / dt / 1e6, "unit": "Mcell-substeps/s", "cores": 1, "kind": "port",
+               "sample": f"64x64x{args.nz} interior cells, {n} call(s) of {ntau} sub-steps in {dt:.1f} s"}
+    if rank == 0:
+        line = {"metric": "Mcell-substeps/s of the compressible acoustic sub-steps (prognostic_pressure)",
+                "value": value, "unit": "Mcell-substeps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms, "step": f"one call: {ntau} acoustic sub-steps", "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)",
+                "config": {"workload": f"compressible acoustic sub-steps {args.maxx}x{args.maxx}x{args.nz}, "
+                                       f"dx=dy=50 m, dz=40 m, dt0=0.5 s, ntau={ntau}, stage 1, density + es + qt + "
+                                       f"{nscal} passive scalar, Lax-Wendroff faces without limiter",
+                           "interior_cells": cells, "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2"},
+                "clocks": clk.summary(), "gpu_launches": args.steps * (1 + ntau * 9),
+                "roofline": {"bound": "hbm", "kernel": "acoustic sub-step (4 kernels + ghost refreshes)",
+                             "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                             "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_source": pk_src,
+                             "algorithmic_bytes_per_cell": ab},
+                "e2e": {"value": ws * cells * ntau / e2e_s / 1e6, "unit": "Mcell-substeps/s",
+                        "h2d_bytes_per_step": nio * d.nx * d.ny * d.nz * 8,
+                        "d2h_bytes_per_step": (14 + 2 * nscal) * d.nx * d.ny * d.nz * 8,
+                        "timing": "host wall clock of one mg_prognostic_pressure call from pageable numpy arrays"},
+                "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist

@@ -144,6 +144,7 @@ def lib() -> C.CDLL:
         L.mg_ensemble_launch_count.argtypes = [vp]
         L.mg_ensemble_set_mode.argtypes = [vp, C.c_int]
         L.mg_prognostic_pressure.argtypes = [vp, C.POINTER(MgAcoustic)]
+        L.mg_time_prognostic_pressure.argtypes = [vp, C.POINTER(MgAcoustic), C.c_int, C.c_int, _dp]
         L.mg_ensemble_get_mode.argtypes = [vp]
         L.mg_checkall.argtypes = [vp, C.POINTER(MgCheckParams), C.POINTER(MgCheckResult)]
         L.mg_cfl_dt.argtypes = [C.POINTER(MgCheckParams), C.c_double, C.c_double, _dp, C.POINTER(C.c_int)]
@@ -202,6 +203,7 @@ EXPORTED = [
     "mg_fft_solve", "mg_anelastic_pressure", "mg_time_steps", "mg_profile_enable", "mg_profile_report",
     "mg_advection_tl", "mg_advection_ad", "mg_anelastic_pressure_ad", "mg_time_adjoint", "mg_ensemble_create", "mg_ensemble_destroy", "mg_ensemble_step", "mg_ensemble_time_steps", "mg_ensemble_launch_count",
     "mg_ensemble_set_mode", "mg_ensemble_get_mode", "mg_prognostic_pressure",
+    "mg_time_prognostic_pressure",
     "mg_set_sgs", "mg_set_surface_fluxes", "mg_sgs_profiles", "mg_calc_subgrid", "mg_efud", "mg_eff",
     "mg_checkall", "mg_cfl_dt", "mg_set_dt", "mg_download_ksgs", "mg_qnadv_tl", "mg_qnadv_ad",
     "mg_traj_forward", "mg_traj_tl", "mg_traj_adjoint", "mg_time_traj", "mg_traj_record_limit", "mg_traj_checkpoints",

@@ -2287,7 +2287,9 @@ extern "C" int mg_fft_solve(mg_ctx *c, const double *tend, double *out)
 }
 
 // ---- the compressible model's acoustic sub-steps (src/INTEG/prognostic_pressure.f90) ----
-extern "C" int mg_prognostic_pressure(mg_ctx *c, const mg_acoustic *a)
+// reps > 0: after the first call, `warmup` untimed calls and `reps` calls timed with
+// events run on the resident fields (ms: device time of one call of ntau sub-steps)
+static int acoustic_impl(mg_ctx *c, const mg_acoustic *a, int warmup, int reps, double *ms)
 {
     if (!c || !a) return MG_ERR_PARAM;
     if (a->ntau < 1 || (a->im != 1 && a->im != 2) || a->nscal < 0 || a->nscal > MG_MAXF - 4 ||
@@ -2336,6 +2338,22 @@ extern "C" int mg_prognostic_pressure(mg_ctx *c, const mg_acoustic *a)
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(p0, a->p0, G.nz * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = launch_acoustic(G, f, a->im, a->ntau, a->cst_cp, lvl, c->stream);
+    if (reps > 0 && e == cudaSuccess) {
+        for (int r = 0; r < warmup && e == cudaSuccess; r++) e = launch_acoustic(G, f, a->im, a->ntau, a->cst_cp, lvl, c->stream);
+        cudaEvent_t t0 = nullptr, t1 = nullptr;
+        if (e == cudaSuccess) e = cudaEventCreate(&t0);
+        if (e == cudaSuccess) e = cudaEventCreate(&t1);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(t0, c->stream);
+        for (int r = 0; r < reps && e == cudaSuccess; r++) e = launch_acoustic(G, f, a->im, a->ntau, a->cst_cp, lvl, c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(t1, c->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+        float tm = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&tm, t0, t1);
+        if (e == cudaSuccess && ms) *ms = tm / reps;
+        if (t0) cudaEventDestroy(t0);
+        if (t1) cudaEventDestroy(t1);
+    }
     for (int q = 0; q < 14 && e == cudaSuccess; q++) e = d2h(c, io[q], fld(9 + q), cudaMemcpyDeviceToHost);
     for (int h = 0; h < ns && e == cudaSuccess; h++) {
         e = d2h(c, a->scal[h], fld(27 + 3 * h), cudaMemcpyDeviceToHost);
@@ -2346,6 +2364,14 @@ extern "C" int mg_prognostic_pressure(mg_ctx *c, const mg_acoustic *a)
     if (e == cudaErrorInvalidValue) return MG_ERR_PARAM;
     if (e != cudaSuccess) return cuerr(e);
     return cuerr(es);
+}
+
+extern "C" int mg_prognostic_pressure(mg_ctx *c, const mg_acoustic *a) { return acoustic_impl(c, a, 0, 0, nullptr); }
+
+extern "C" int mg_time_prognostic_pressure(mg_ctx *c, const mg_acoustic *a, int warmup, int reps, double *ms)
+{
+    if (warmup < 0 || reps < 1 || !ms) return MG_ERR_PARAM;
+    return acoustic_impl(c, a, warmup, reps, ms);
 }
 
 extern "C" int mg_anelastic_pressure(mg_ctx *c, double *mu, double *mv, double *mw, double *p, const double *wold,

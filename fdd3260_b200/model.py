@@ -378,10 +378,12 @@ class Mimica:
         _lib.check(self._L.mg_fft_solve(self._h, _lib.ptr(np.ascontiguousarray(tend)), _lib.ptr(out)), "mg_fft_solve")
         return out
 
-    def prognostic_pressure(self, inp, st):
+    def prognostic_pressure(self, inp, st, reps: int = 0, warmup: int = 0):
         """src/INTEG/prognostic_pressure.f90:64 (the compressible model's acoustic
         sub-steps) on copies of an acoustic.AcousticState with acoustic.AcousticInput;
-        returns the updated copy."""
+        returns the updated copy.  reps >= 1: after the call, `warmup` untimed and `reps`
+        timed calls run on the uploaded fields (mg_time_prognostic_pressure), and
+        (state, device ms per call) is returned."""
         st = st.copy()
         c = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
         keep = [c(x) for x in (inp.p0, inp.su, inp.sv, inp.sw, inp.sdens, inp.ses, inp.sqt, inp.uadv, inp.vadv,
@@ -400,6 +402,11 @@ class Mimica:
         a.sscal = C.cast(ps, C.POINTER(C.POINTER(C.c_double)))
         a.scal = C.cast(pc, C.POINTER(C.POINTER(C.c_double)))
         a.tscal = C.cast(pt, C.POINTER(C.POINTER(C.c_double)))
+        if reps >= 1:
+            ms = C.c_double(0.0)
+            _lib.check(self._L.mg_time_prognostic_pressure(self._h, C.byref(a), warmup, reps, C.byref(ms)),
+                       "mg_time_prognostic_pressure")
+            return st, ms.value
         _lib.check(self._L.mg_prognostic_pressure(self._h, C.byref(a)), "mg_prognostic_pressure")
         return st
 

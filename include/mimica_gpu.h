@@ -269,6 +269,10 @@ typedef struct mg_acoustic {
     double *cs2;                     /* out: thermo_prop%cs2 */
 } mg_acoustic;
 int mg_prognostic_pressure(mg_ctx *ctx, const mg_acoustic *a);
+/* the same call, then `warmup` (>= 0) untimed and `reps` (>= 1) timed calls on the
+ * uploaded fields; ms = device time of one call of ntau sub-steps (CUDA events, the mean
+ * over the timed calls); the fields written back are those after all calls */
+int mg_time_prognostic_pressure(mg_ctx *ctx, const mg_acoustic *a, int warmup, int reps, double *ms);
 
 /* ---- per-step checks and time-step control: checkall (src/IO/check.f90:59-95) ----
  * checkx (:341-417) of es (theta) and qt, then checkwind (:102-337, ANELASTIC: the
