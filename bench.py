@@ -695,14 +695,13 @@ def run_capacity(args, ws, rank, local):
 
 
 # algorithmic HBM bytes per interior cell of one acoustic sub-step (FP64), with nscal
-# passive scalars: the scalar kernel reads dens, es, uadv, vadv, wadv, sdens, ses, sqt,
-# tdens, tes, tqt, qt and writes dens', es', tdens, tes, tqt, qt (18 fields); the
-# equation of state reads dens, es, qt and writes cs2, p, es, qt (7); the divergence
-# reads u, v, w and writes div (4); the momentum kernel reads p, div, dens, su, sv, sw,
-# tu, tv, tw, u, v, w and writes tu, tv, tw, u, v, w (18); each passive scalar reads
-# sscal, tscal, scal and writes tscal, scal (5)
+# passive scalars: the scalar kernel (advection, integ_scal, equation of state,
+# divergence) reads dens, es, uadv, vadv, wadv, sdens, ses, sqt, tdens, tes, tqt, qt, u,
+# v, w and writes dens', es', tdens, tes, tqt, qt, p, cs2, div (24 fields); the momentum
+# kernel reads p, div, dens, su, sv, sw, tu, tv, tw, u, v, w and writes tu, tv, tw, u, v,
+# w (18); each passive scalar reads sscal, tscal, scal and writes tscal, scal (5)
 def acoustic_alg_bytes(nscal: int) -> int:
-    return 8 * (18 + 7 + 4 + 18 + 5 * nscal)
+    return 8 * (24 + 18 + 5 * nscal)
 
 
 def run_acoustic(args, ws, rank, local):
@@ -754,8 +753,8 @@ def run_acoustic(args, ws, rank, local):
                                        f"dx=dy=50 m, dz=40 m, dt0=0.5 s, ntau={ntau}, stage 1, density + es + qt + "
                                        f"{nscal} passive scalar, Lax-Wendroff faces without limiter",
                            "interior_cells": cells, "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2"},
-                "clocks": clk.summary(), "gpu_launches": args.steps * (1 + ntau * 9),
-                "roofline": {"bound": "hbm", "kernel": "acoustic sub-step (4 kernels + ghost refreshes)",
+                "clocks": clk.summary(), "gpu_launches": args.steps * (1 + ntau * 5),
+                "roofline": {"bound": "hbm", "kernel": "acoustic sub-step (2 kernels + ghost refreshes and level sums)",
                              "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                              "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_source": pk_src,
                              "algorithmic_bytes_per_cell": ab},

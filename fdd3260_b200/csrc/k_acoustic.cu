@@ -10,17 +10,20 @@
 // the non-ANELASTIC branch), caldiv and gradp (src/TOOLS/gradients.f90:986-1052,
 // 1205-1292; gpz(1) = 0 without ANELASTIC) and horav.
 //
-// One sub-step is four kernels over the interior cells, each followed by the periodic
+// One sub-step is two kernels over the interior cells, each followed by the periodic
 // ghost refresh of what it wrote:
 //   ac_scal_kernel  advective tendencies of density and es (x, y, z faces of the cell,
 //                   as the reference subtracts them direction by direction), the
-//                   tendency accumulators and the integ_scal update of every scalar;
-//   ac_eos_kernel   the equation of state: pressure, sound speed, es and qt through the
-//                   reference's divide-and-multiply round trip;
+//                   tendency accumulators and the integ_scal update of every scalar,
+//                   then, on the cell's new values, the equation of state (pressure,
+//                   sound speed, es and qt through the reference's divide-and-multiply
+//                   round trip), and the divergence of the momentum (caldiv: the
+//                   momentum is not changed before it in the sub-step);
 //   (level means of the sound speed, horav)
-//   ac_div_kernel   the divergence of the momentum (caldiv);
 //   ac_mom_kernel   pressure gradient, divergence-damping gradient, buoyancy, the
 //                   tendency accumulators and the integ_mom update.
+// The reference's whole-array passes are pointwise where they are fused here, so the
+// fused order gives the same values.
 // Everything matches the CPU restatement bit for bit except the power of the equation
 // of state (CUDA's pow against the C library's) and the order of the level sums.
 #include <math.h>
@@ -108,6 +111,27 @@ __device__ __forceinline__ double lwnl_tendency(const DevGrid &G, const AcDev &A
     return s - zz;
 }
 
+// equation_of_state(state, density_in=dens, pressure_out=p, thermo_out, conservative=.true.)
+// for potential temperature (thermodynamics.f90:126-134, 193-203, 208-211, 254-258,
+// 266-288) on a cell's density d and density-weighted es, qt (updated in place)
+__device__ __forceinline__ void ac_eos(const AcDev &A, int k, long long c, double d, double &es_w, double &qt_w)
+{
+    const double es = es_w / d, qt = qt_w / d;
+    double cp = AC_CPA, cv = AC_CVA;
+    if (!A.cst_cp) {   // get_cp_cv_3d (:331-343), lmicro = 0: qv = qt
+        const double qv = qt;
+        cp = (1. - qt) * AC_CPA + AC_CPV * qv;
+        cv = (1. - qt) * AC_CVA + AC_CVV * qv;
+    }
+    const double exn = pow(d * (cp - cv) * es / AC_PREF, (AC_CPA - AC_CVA) / AC_CVA);
+    const double tt = es * exn;
+    const double pp = d * (cp - cv) * tt;
+    A.cs2[c] = AC_CPA / AC_CVA * pp / d;
+    A.p[c] = pp - __ldg(A.p0 + k - 1);
+    es_w = es * d;
+    qt_w = qt * d;
+}
+
 __global__ void ac_scal_kernel(const __grid_constant__ DevGrid G, const __grid_constant__ AcDev A)
 {
     int i, j, k;
@@ -122,53 +146,26 @@ __global__ void ac_scal_kernel(const __grid_constant__ DevGrid G, const __grid_c
     A.tdens[c] = td;
     A.tes[c] = te;
     A.tqt[c] = tq;
-    A.dens2[c] = __ldg(A.dens + c) + A.a_lm * A.dtau * td;
-    A.es2[c] = __ldg(A.es + c) + A.a_lm * A.dtau * te;
-    A.qt[c] = A.qt[c] + A.a_lm * A.dtau * tq;
+    const double dn = __ldg(A.dens + c) + A.a_lm * A.dtau * td;
+    double en = __ldg(A.es + c) + A.a_lm * A.dtau * te;
+    double qn = A.qt[c] + A.a_lm * A.dtau * tq;
     for (int h = 0; h < A.nscal; h++) {
         const double ts = __ldg(A.sscal[h] + c) + A.b_lm * A.tscal[h][c];
         A.tscal[h][c] = ts;
         A.scal[h][c] = A.scal[h][c] + A.a_lm * A.dtau * ts;
     }
-}
-
-// equation_of_state(state, density_in=dens, pressure_out=p, thermo_out, conservative=.true.)
-// for potential temperature (thermodynamics.f90:126-134, 193-203, 208-211, 254-258, 266-288)
-__global__ void ac_eos_kernel(const __grid_constant__ DevGrid G, const __grid_constant__ AcDev A)
-{
-    int i, j, k;
-    if (!ac_cell(G, (long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
-    const long long c = gidx(G, i, j, k);
-    const double d = A.dens[c];
-    const double es = A.es2[c] / d, qt = A.qt[c] / d;
-    double cp = AC_CPA, cv = AC_CVA;
-    if (!A.cst_cp) {   // get_cp_cv_3d (:331-343), lmicro = 0: qv = qt
-        const double qv = qt;
-        cp = (1. - qt) * AC_CPA + AC_CPV * qv;
-        cv = (1. - qt) * AC_CVA + AC_CVV * qv;
-    }
-    const double exn = pow(d * (cp - cv) * es / AC_PREF, (AC_CPA - AC_CVA) / AC_CVA);
-    const double tt = es * exn;
-    const double pp = d * (cp - cv) * tt;
-    A.cs2[c] = AC_CPA / AC_CVA * pp / d;
-    A.p[c] = pp - __ldg(A.p0 + k - 1);
-    A.es2[c] = es * d;
-    A.qt[c] = qt * d;
-}
-
-// caldiv (gradients.f90:1014-1039) of the momentum
-__global__ void ac_div_kernel(const __grid_constant__ DevGrid G, const __grid_constant__ AcDev A)
-{
-    int i, j, k;
-    if (!ac_cell(G, (long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
-    const long long c = gidx(G, i, j, k);
+    ac_eos(A, k, c, dn, en, qn);
+    A.dens2[c] = dn;
+    A.es2[c] = en;
+    A.qt[c] = qn;
+    // caldiv (gradients.f90:1014-1039) of the momentum
     const double dx1 = 1. / G.dx, dy1 = 1. / G.dy;
-    double d = 0.;
-    d = d + (A.u[c + 1] - A.u[c]) * dx1;
-    d = d + (A.v[c + G.px] - A.v[c]) * dy1;
-    if (k < G.nz) d = d + (A.w[c + G.ps] - A.w[c]) * __ldg(G.dz1w + k - 1);
-    else d = d + (0. - A.w[c]) * __ldg(G.dz1w + k - 1);
-    A.div[c] = d;
+    double dv = 0.;
+    dv = dv + (A.u[c + 1] - A.u[c]) * dx1;
+    dv = dv + (A.v[c + G.px] - A.v[c]) * dy1;
+    if (k < G.nz) dv = dv + (A.w[c + G.ps] - A.w[c]) * __ldg(G.dz1w + k - 1);
+    else dv = dv + (0. - A.w[c]) * __ldg(G.dz1w + k - 1);
+    A.div[c] = dv;
 }
 
 // gradp of the pressure and of the divergence (gpz(1) = 0), buoyancy of the density,
@@ -246,27 +243,15 @@ cudaError_t launch_acoustic(const DevGrid &g, const AcousticFields &f, int im, i
         ac_scal_kernel<<<nb, 256, 0, s>>>(g, A);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         {
-            double *hf[4 + MG_MAXF];
+            double *hf[7 + MG_MAXF];
             int nf = 0;
-            hf[nf++] = dens2; hf[nf++] = es2; hf[nf++] = f.qt;
+            hf[nf++] = dens2; hf[nf++] = es2; hf[nf++] = f.qt; hf[nf++] = f.p; hf[nf++] = f.cs2; hf[nf++] = f.div;
             for (int h = 0; h < f.nscal; h++) hf[nf++] = f.scal[h];
             if ((e = launch_halo_fill(g, hf, nf, s)) != cudaSuccess) return e;
         }
-        // the new density and es are this sub-step's state from here on
-        A.dens = dens2; A.es = es2;
-        ac_eos_kernel<<<nb, 256, 0, s>>>(g, A);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        {
-            double *hf[4] = {f.p, es2, f.qt, f.cs2};
-            if ((e = launch_halo_fill(g, hf, 4, s)) != cudaSuccess) return e;
-        }
         if ((e = launch_level_mean(g, f.cs2, lvl, s)) != cudaSuccess) return e;
-        ac_div_kernel<<<nb, 256, 0, s>>>(g, A);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        {
-            double *hf[1] = {f.div};
-            if ((e = launch_halo_fill(g, hf, 1, s)) != cudaSuccess) return e;
-        }
+        // the new density is this sub-step's state from here on
+        A.dens = dens2;
         ac_mom_kernel<<<nb, 256, 0, s>>>(g, A);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         {
