@@ -20,6 +20,7 @@ class Mimica:
         self.domain = domain
         self.nscal = nscal
         self.iqt = iqt
+        self.device = device
         L = _lib.lib()
         params, self._keep = domain.params(nscal, iqt)
         h = C.c_void_p()
