@@ -132,7 +132,9 @@ __device__ __forceinline__ void ac_eos(const AcDev &A, int k, long long c, doubl
     qt_w = qt * d;
 }
 
-__global__ void ac_scal_kernel(const __grid_constant__ DevGrid G, const __grid_constant__ AcDev A)
+// six CTAs per SM (40 registers, a few spilled): the kernel waits on its stencil loads,
+// and the extra warps hide them (+5 % against 54 registers and four CTAs)
+__global__ void __launch_bounds__(256, 6) ac_scal_kernel(const __grid_constant__ DevGrid G, const __grid_constant__ AcDev A)
 {
     int i, j, k;
     if (!ac_cell(G, (long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
