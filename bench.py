@@ -700,6 +700,11 @@ def run_capacity(args, ws, rank, local):
 # v, w and writes dens', es', tdens, tes, tqt, qt, p, cs2, div (24 fields); the momentum
 # kernel reads p, div, dens, su, sv, sw, tu, tv, tw, u, v, w and writes tu, tv, tw, u, v,
 # w (18); each passive scalar reads sscal, tscal, scal and writes tscal, scal (5)
+# measured DRAM bytes per interior cell of one sub-step with one passive scalar:
+# ac_scal_kernel 230 + ac_mom_kernel 138 (ncu, 256x256x64)
+ACOUSTIC_TRAFFIC_PER_CELL = 230.0 + 138.0
+
+
 def acoustic_alg_bytes(nscal: int) -> int:
     return 8 * (24 + 18 + 5 * nscal)
 
@@ -756,8 +761,14 @@ def run_acoustic(args, ws, rank, local):
                 "clocks": clk.summary(), "gpu_launches": args.steps * (1 + ntau * 5),
                 "roofline": {"bound": "hbm", "kernel": "acoustic sub-step (2 kernels + ghost refreshes and level sums)",
                              "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                             "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_source": pk_src,
-                             "algorithmic_bytes_per_cell": ab},
+                             "frac": achieved / pk["hbm_gbs"],
+                             "traffic": ACOUSTIC_TRAFFIC_PER_CELL * cells if nscal == 1 else None,
+                             "traffic_unit": "bytes per sub-step",
+                             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of ac_scal_kernel and "
+                                               "ac_mom_kernel at 256x256x64 with 1 passive scalar "
+                                               "(profiles/acoustic_substep_256x256x64.md), per interior cell, times "
+                                               "this domain's cells",
+                             "peak_source": pk_src, "algorithmic_bytes_per_cell": ab},
                 "e2e": {"value": ws * cells * ntau / e2e_s / 1e6, "unit": "Mcell-substeps/s",
                         "h2d_bytes_per_step": nio * d.nx * d.ny * d.nz * 8,
                         "d2h_bytes_per_step": (14 + 2 * nscal) * d.nx * d.ny * d.nz * 8,
