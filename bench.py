@@ -716,7 +716,8 @@ def run_acoustic(args, ws, rank, local):
     value = all ranks' cell sub-steps / max over ranks of the time."""
     from fdd3260_b200 import Mimica, acoustic, config
     dev = local if ws > 1 else 0
-    d = config.warm_bubble_domain(args.maxx, args.maxx, args.nz, dx=50.0, dy=50.0, dz=40.0, dt0=0.5)
+    d = config.warm_bubble_domain(args.maxx, args.maxx, args.nz, dx=50.0, dy=50.0, dz=40.0, dt0=0.5,
+                                  scheme=args.scheme)
     nscal, ntau = 1, 8
     inp, st = acoustic.acoustic_case(d, seed=31 + rank, im=1, ntau=ntau, nscal=nscal)
     with Mimica(d, nscal=1, device=dev) as m:
@@ -738,7 +739,7 @@ def run_acoustic(args, ws, rank, local):
     cpu = None
     if rank == 0 and not args.skip_cpu:
         from oracle import oracle as O
-        ds = config.warm_bubble_domain(64, 64, args.nz, dx=50.0, dy=50.0, dz=40.0, dt0=0.5)
+        ds = config.warm_bubble_domain(64, 64, args.nz, dx=50.0, dy=50.0, dz=40.0, dt0=0.5, scheme=args.scheme)
         si, ss = acoustic.acoustic_case(ds, seed=31, im=1, ntau=ntau, nscal=nscal)
         orc = O.Oracle(ds)
         orc.prognostic_pressure(si, ss)
@@ -756,7 +757,8 @@ def run_acoustic(args, ws, rank, local):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)",
                 "config": {"workload": f"compressible acoustic sub-steps {args.maxx}x{args.maxx}x{args.nz}, "
                                        f"dx=dy=50 m, dz=40 m, dt0=0.5 s, ntau={ntau}, stage 1, density + es + qt + "
-                                       f"{nscal} passive scalar, Lax-Wendroff faces without limiter",
+                                       f"{nscal} passive scalar, "
+                                       f"{'QUICK' if args.scheme == 'quick' else 'Lax-Wendroff'} faces without limiter",
                            "interior_cells": cells, "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2"},
                 "clocks": clk.summary(), "gpu_launches": args.steps * (1 + ntau * 5),
                 "roofline": {"bound": "hbm", "kernel": "acoustic sub-step (2 kernels + ghost refreshes and level sums)",

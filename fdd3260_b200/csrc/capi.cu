@@ -2295,7 +2295,7 @@ static int acoustic_impl(mg_ctx *c, const mg_acoustic *a, int warmup, int reps, 
     if (a->ntau < 1 || (a->im != 1 && a->im != 2) || a->nscal < 0 || a->nscal > MG_MAXF - 4 ||
         (a->cst_cp != 0 && a->cst_cp != 1))
         return MG_ERR_PARAM;
-    if (c->G.scal_adv == MG_QUICK) return MG_ERR_PARAM;
+    if (c->G.scal_adv == MG_QUICK && c->G.nz < 6) return MG_ERR_PARAM;
     const double *in[9] = {a->su, a->sv, a->sw, a->sdens, a->ses, a->sqt, a->uadv, a->vadv, a->wadv};
     double *io[14] = {a->dens, a->p, a->u, a->v, a->w, a->es, a->qt, a->tu, a->tv, a->tw, a->tdens, a->tes, a->tqt,
                       a->cs2};

@@ -4,7 +4,8 @@
 // Replaces src/INTEG/prognostic_pressure.f90:64-259 for the dry ISENTROPIC CONSERVATIVE
 // build (div_pressure compiled out, nhydro = 0, sorder = 2, sponge off), with its
 // callees: advect with limiter=.false., full=.false. (src/TOOLS/advection.f90:84-314,
-// unsplit; the faces of src/TOOLS/advq_lw_nolim.f90), integ_scal and integ_mom
+// unsplit; the faces of src/TOOLS/advq_lw_nolim.f90, or of advq_quick_nolim.f90 for the
+// quick scheme), integ_scal and integ_mom
 // (src/INTEG/integpack.f90:54-260), equation_of_state (src/TOOLS/thermodynamics.f90:
 // 74-294: potential temperature in, density in, conservative), buoyancy (:472-493,
 // the non-ANELASTIC branch), caldiv and gradp (src/TOOLS/gradients.f90:986-1052,
@@ -87,27 +88,86 @@ __device__ __forceinline__ double lwnl_face_z(const DevGrid &G, const double *x,
     return 0.5 * fl * (ww + fabs(ww)) + 0.5 * fr * (ww - fabs(ww));
 }
 
+// face flux of advsx_quick_nl / advsy_quick_nl (advq_quick_nolim.f90:80-94): between
+// x0 and xp1, with xm1 and xp2 beside them
+__device__ __forceinline__ double quicknl_face_h(double xm1, double x0, double xp1, double xp2, double uu)
+{
+    const double cc = 1. / 4.;
+    const double ffip1 = (xp1 - x0), ffip2 = (xp2 - xp1), ffim1 = (x0 - xm1);
+    const double phil = ffip1 - cc * (ffip1 - ffim1);
+    const double phir = ffip1 + cc * (ffip2 - ffip1);
+    const double fl = x0 + 0.5 * phil;
+    const double fr = xp1 - 0.5 * phir;
+    return 0.5 * fl * (uu + fabs(uu)) + 0.5 * fr * (uu - fabs(uu));
+}
+
+// face flux k+1/2 of advsz_quick_nl (advq_quick_nolim.f90:218-272), 1 <= k <= nz-1, 'nnf'
+// (bc51 = bc61 = 0: the one-sided slopes of the end faces are the reference's
+// 0*(...) + 1*ffip1); c is the cell (k) of the column whose base is c0 (level 1)
+__device__ __forceinline__ double quicknl_face_z(const DevGrid &G, const double *x, const double *w, long long c0, int k)
+{
+    const int nz = G.nz;
+    const double cc = 1. / 4., bc = 0.;
+    auto X = [&](int l) { return __ldg(x + c0 + (long long)(l - 1) * G.ps); };
+    auto D1 = [&](int l) { return __ldg(G.dz1 + l - 1); };
+    const double xx = X(k), ww = __ldg(w + c0 + (long long)k * G.ps);
+    const double ffip1 = (X(k + 1) - xx) * D1(k);
+    double ffip2, ffim1;
+    if (k == 1) {
+        ffip2 = (X(3) - X(2)) * D1(2);
+        ffim1 = bc * (X(nz - 4) - X(nz - 5)) * D1(nz - 5) + (1. - bc) * ffip1;
+    } else if (k == nz - 1) {
+        ffim1 = (xx - X(k - 1)) * D1(k - 1);
+        ffip2 = bc * (X(6) - X(5)) * D1(5) + (1. - bc) * ffip1;
+    } else {
+        ffip2 = (X(k + 2) - X(k + 1)) * D1(k + 1);
+        ffim1 = (xx - X(k - 1)) * D1(k - 1);
+    }
+    const double phil = ffip1 - cc * (ffip1 - ffim1);
+    const double phir = ffip1 + cc * (ffip2 - ffip1);
+    const double d1w = __ldg(G.dz1w + k - 1);
+    const double fl = xx + 0.5 * phil / d1w;
+    const double fr = X(k + 1) - 0.5 * phir / d1w;
+    return 0.5 * fl * (ww + fabs(ww)) + 0.5 * fr * (ww - fabs(ww));
+}
+
 // advection_x/y/z (advection.f90:556-798, non-split: xs = xs - xx per direction) of one
-// field at cell c, starting from the slow tendency s
-__device__ __forceinline__ double lwnl_tendency(const DevGrid &G, const AcDev &A, const double *x, double s, long long c,
-                                                int k)
+// field at cell c, starting from the slow tendency s; QUICK selects advq_quick_nolim's
+// faces, false advq_lw_nolim's
+template <bool QUICK>
+__device__ __forceinline__ double nl_tendency(const DevGrid &G, const AcDev &A, const double *x, double s, long long c,
+                                              int k)
 {
     const double dx1 = 1. / G.dx, dy1 = 1. / G.dy;
-    const double fxm = lwnl_face_h(__ldg(x + c - 1), __ldg(x + c), __ldg(A.uadv + c), G.dt0, dx1);
-    const double fxp = lwnl_face_h(__ldg(x + c), __ldg(x + c + 1), __ldg(A.uadv + c + 1), G.dt0, dx1);
+    auto L = [&](long long q) { return __ldg(x + q); };
+    double fxm, fxp, fym, fyp;
+    if constexpr (QUICK) {
+        fxm = quicknl_face_h(L(c - 2), L(c - 1), L(c), L(c + 1), __ldg(A.uadv + c));
+        fxp = quicknl_face_h(L(c - 1), L(c), L(c + 1), L(c + 2), __ldg(A.uadv + c + 1));
+        fym = quicknl_face_h(L(c - 2 * G.px), L(c - G.px), L(c), L(c + G.px), __ldg(A.vadv + c));
+        fyp = quicknl_face_h(L(c - G.px), L(c), L(c + G.px), L(c + 2 * G.px), __ldg(A.vadv + c + G.px));
+    } else {
+        fxm = lwnl_face_h(L(c - 1), L(c), __ldg(A.uadv + c), G.dt0, dx1);
+        fxp = lwnl_face_h(L(c), L(c + 1), __ldg(A.uadv + c + 1), G.dt0, dx1);
+        fym = lwnl_face_h(L(c - G.px), L(c), __ldg(A.vadv + c), G.dt0, dy1);
+        fyp = lwnl_face_h(L(c), L(c + G.px), __ldg(A.vadv + c + G.px), G.dt0, dy1);
+    }
     s = s - (0. + (fxp - fxm) * dx1);
-    const double fym = lwnl_face_h(__ldg(x + c - G.px), __ldg(x + c), __ldg(A.vadv + c), G.dt0, dy1);
-    const double fyp = lwnl_face_h(__ldg(x + c), __ldg(x + c + G.px), __ldg(A.vadv + c + G.px), G.dt0, dy1);
     s = s - (0. + (fyp - fym) * dy1);
     const int nz = G.nz;
     const double d1w = __ldg(G.dz1w + k - 1);
+    const long long c0 = c - (long long)(k - 1) * G.ps;
+    auto FZ = [&](int kf) {   // face kf+1/2
+        if constexpr (QUICK) return quicknl_face_z(G, x, A.wadv, c0, kf);
+        else return lwnl_face_z(G, x, A.wadv, c0 + (long long)(kf - 1) * G.ps, kf);
+    };
     double zz;
     if (k == 1)   // 'nnf' bottom: xa(1) = xa(1) + (Flux(1) - 0.)*dz1w(1)
-        zz = 0. + ((nz >= 2 ? lwnl_face_z(G, x, A.wadv, c, 1) : 0.) - 0.) * d1w;
+        zz = 0. + ((nz >= 2 ? FZ(1) : 0.) - 0.) * d1w;
     else if (k == nz)   // 'nnf' top: xa(nz) = xa(nz) + (0. - Flux(nz-1))*dz1w(nz)
-        zz = 0. + (0. - lwnl_face_z(G, x, A.wadv, c - G.ps, k - 1)) * d1w;
+        zz = 0. + (0. - FZ(k - 1)) * d1w;
     else
-        zz = 0. + (lwnl_face_z(G, x, A.wadv, c, k) - lwnl_face_z(G, x, A.wadv, c - G.ps, k - 1)) * d1w;
+        zz = 0. + (FZ(k) - FZ(k - 1)) * d1w;
     return s - zz;
 }
 
@@ -134,14 +194,15 @@ __device__ __forceinline__ void ac_eos(const AcDev &A, int k, long long c, doubl
 
 // six CTAs per SM (40 registers, a few spilled): the kernel waits on its stencil loads,
 // and the extra warps hide them (+5 % against 54 registers and four CTAs)
+template <bool QUICK>
 __global__ void __launch_bounds__(256, 6) ac_scal_kernel(const __grid_constant__ DevGrid G, const __grid_constant__ AcDev A)
 {
     int i, j, k;
     if (!ac_cell(G, (long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
     const long long c = gidx(G, i, j, k);
     // advect (density with adv=.false., es in flux form), then integ_scal (integpack.f90:171-217)
-    const double densa = lwnl_tendency(G, A, A.dens, __ldg(A.sdens + c), c, k);
-    const double esa = lwnl_tendency(G, A, A.es, __ldg(A.ses + c), c, k);
+    const double densa = nl_tendency<QUICK>(G, A, A.dens, __ldg(A.sdens + c), c, k);
+    const double esa = nl_tendency<QUICK>(G, A, A.es, __ldg(A.ses + c), c, k);
     const double td = densa + A.b_lm * A.tdens[c];
     const double te = esa + A.b_lm * A.tes[c];
     const double tq = __ldg(A.sqt + c) + A.b_lm * A.tqt[c];
@@ -214,6 +275,7 @@ cudaError_t launch_acoustic(const DevGrid &g, const AcousticFields &f, int im, i
                             cudaStream_t s)
 {
     if (ntau < 1 || (im != 1 && im != 2) || f.nscal < 0 || f.nscal > MG_MAXF - 4) return cudaErrorInvalidValue;
+    if (g.scal_adv == MG_QUICK && g.nz < 6) return cudaErrorInvalidValue;   // the bottom face reads x(nz-5)
     AcDev A{};
     A.nscal = f.nscal;
     A.cst_cp = cst_cp;
@@ -242,7 +304,10 @@ cudaError_t launch_acoustic(const DevGrid &g, const AcousticFields &f, int im, i
     }
     for (int it = 0; it < ntau; it++) {
         A.dens = dens; A.dens2 = dens2; A.es = es; A.es2 = es2;
-        ac_scal_kernel<<<nb, 256, 0, s>>>(g, A);
+        if (g.scal_adv == MG_QUICK)
+            ac_scal_kernel<true><<<nb, 256, 0, s>>>(g, A);
+        else
+            ac_scal_kernel<false><<<nb, 256, 0, s>>>(g, A);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         {
             double *hf[7 + MG_MAXF];

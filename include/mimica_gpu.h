@@ -247,8 +247,9 @@ int mg_anelastic_pressure(mg_ctx *ctx, double *mu, double *mv, double *mw, doubl
  * (integ_mom).  The tendency accumulators tu..tqt, tscal (integpack's tend) are read
  * and updated.  All arrays are nx*ny*nz host arrays of the reference layout with their
  * ghost cells; the grid, dt0, den0 and the metrics are the context's.  The context's
- * scheme selects the faces: every scheme but quick uses the Lax-Wendroff ones
- * (advection.f90:582-592); quick (advq_quick_nolim.f90) is not built: MG_ERR_PARAM. */
+ * scheme selects the faces (advection.f90:582-592): quick its own unlimited ones
+ * (advq_quick_nolim.f90, nz >= 6, else MG_ERR_PARAM), every other scheme the
+ * Lax-Wendroff ones (advq_lw_nolim.f90). */
 typedef struct mg_acoustic {
     int im;                          /* integrator stage: 1 or 2 */
     int ntau;                        /* sub-steps, >= 1 */

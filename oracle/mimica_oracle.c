@@ -965,10 +965,97 @@ static void advs_lwnl_z(const mo_grid *g, const double *x, const double *w, doub
     free(F);
 }
 
+/* src/TOOLS/advq_quick_nolim.f90:53-111 (advsx_quick_nl; advsy_quick_nl :120-185 is the
+ * same along y without CHANNEL): QUICK faces without the limiter */
+static void advs_quicknl_h(int n, int i1, int i2, double d, const double *x, const double *u, double *xa, int adv)
+{
+    const double cc = 1. / 4., dx1 = 1. / d;
+    double *F = dalloc((size_t)n);
+    for (int i = i1 - 1; i <= i2; i++) {
+        const double uu = P1(u, i + 1);
+        const double xx = P1(x, i);
+        const double ffip1 = (P1(x, i + 1) - xx);
+        const double ffip2 = (P1(x, i + 2) - P1(x, i + 1));
+        const double ffim1 = (xx - P1(x, i - 1));
+        const double phil = ffip1 - cc * (ffip1 - ffim1);
+        const double phir = ffip1 + cc * (ffip2 - ffip1);
+        const double fl = xx + 0.5 * phil;
+        const double fr = P1(x, i + 1) - 0.5 * phir;
+        P1(F, i) = 0.5 * fl * (uu + fabs(uu)) + 0.5 * fr * (uu - fabs(uu));
+    }
+    double fold = P1(F, i1 - 1);
+    for (int i = i1; i <= i2; i++) {
+        P1(xa, i) = P1(xa, i) + (P1(F, i) - fold) * dx1;
+        fold = P1(F, i);
+    }
+    if (adv) {
+        double uold = P1(u, i2 + 1);
+        for (int i = i2; i >= i1; i--) {
+            P1(xa, i) = P1(xa, i) - P1(x, i) * (uold - P1(u, i)) * dx1;
+            uold = P1(u, i);
+        }
+    }
+    free(F);
+}
+
+/* src/TOOLS/advq_quick_nolim.f90:188-318 (advsz_quick_nl), 'nnf' bottom and top
+ * (bc51 = bc61 = 0), flux form; nz >= 6 (the bottom face's periodic branch reads
+ * x(nz-5)) */
+static void advs_quicknl_z(const mo_grid *g, const double *x, const double *w, double *xa)
+{
+    const int nz = g->nz;
+    const double *dz1 = g->dz1, *dz1w = g->dz1w;
+    const double cc = 1. / 4., bc51 = 0., bc61 = 0.;
+    double *F = dalloc((size_t)nz);
+    {
+        const double xx = P1(x, 1), ww = P1(w, 2);
+        const double ffip1 = (P1(x, 2) - xx) * P1(dz1, 1);
+        const double ffip2 = (P1(x, 3) - P1(x, 2)) * P1(dz1, 2);
+        const double ffim1 = bc51 * (P1(x, nz - 4) - P1(x, nz - 5)) * P1(dz1, nz - 5) + (1. - bc51) * ffip1;
+        const double phil = ffip1 - cc * (ffip1 - ffim1);
+        const double phir = ffip1 + cc * (ffip2 - ffip1);
+        const double fl = xx + 0.5 * phil / P1(dz1w, 1);
+        const double fr = P1(x, 2) - 0.5 * phir / P1(dz1w, 1);
+        P1(F, 1) = 0.5 * fl * (ww + fabs(ww)) + 0.5 * fr * (ww - fabs(ww));
+    }
+    for (int k = 2; k <= nz - 2; k++) {
+        const double xx = P1(x, k), ww = P1(w, k + 1);
+        const double ffip1 = (P1(x, k + 1) - xx) * P1(dz1, k);
+        const double ffip2 = (P1(x, k + 2) - P1(x, k + 1)) * P1(dz1, k + 1);
+        const double ffim1 = (xx - P1(x, k - 1)) * P1(dz1, k - 1);
+        const double phil = ffip1 - cc * (ffip1 - ffim1);
+        const double phir = ffip1 + cc * (ffip2 - ffip1);
+        const double fl = xx + 0.5 * phil / P1(dz1w, k);
+        const double fr = P1(x, k + 1) - 0.5 * phir / P1(dz1w, k);
+        P1(F, k) = 0.5 * fl * (ww + fabs(ww)) + 0.5 * fr * (ww - fabs(ww));
+    }
+    {
+        const int k = nz - 1;
+        const double xx = P1(x, nz - 1), ww = P1(w, nz);
+        const double ffip1 = (P1(x, k + 1) - xx) * P1(dz1, k);
+        const double ffim1 = (xx - P1(x, k - 1)) * P1(dz1, k - 1);
+        const double ffip2 = bc61 * (P1(x, 6) - P1(x, 5)) * P1(dz1, 5) + (1. - bc61) * ffip1;
+        const double phil = ffip1 - cc * (ffip1 - ffim1);
+        const double phir = ffip1 + cc * (ffip2 - ffip1);
+        const double fl = xx + 0.5 * phil / P1(dz1w, k);
+        const double fr = P1(x, k + 1) - 0.5 * phir / P1(dz1w, k);
+        P1(F, k) = 0.5 * fl * (ww + fabs(ww)) + 0.5 * fr * (ww - fabs(ww));
+    }
+    double fold = P1(F, 1);
+    for (int k = 2; k <= nz - 1; k++) {
+        P1(xa, k) = P1(xa, k) + (P1(F, k) - fold) * P1(dz1w, k);
+        fold = P1(F, k);
+    }
+    P1(xa, 1) = P1(xa, 1) + (P1(F, 1) - 0.) * P1(dz1w, 1);
+    P1(xa, nz) = P1(xa, nz) + (0. - P1(F, nz - 1)) * P1(dz1w, nz);
+    free(F);
+}
+
 void mo_advs_h(const mo_grid *g, int scheme, int n, int i1, int i2, double d, const double *x,
                const double *u, double *xa, int adv)
 {
     switch (scheme) {
+    case MO_QUICK_NL: advs_quicknl_h(n, i1, i2, d, x, u, xa, adv); break;
     case MO_LW_NL: advs_lwnl_h(g, n, i1, i2, d, x, u, xa, adv); break;
     case MO_WENO: advs_weno_h(n, i1, i2, d, x, u, xa, adv); break;
     case MO_PPM: advs_ppm_h(g, n, i1, i2, d, x, u, xa, adv); break;
@@ -982,6 +1069,7 @@ void mo_advs_z(const mo_grid *g, int scheme, const double *x, const double *w, d
 {
     switch (scheme) {
     case MO_LW_NL: advs_lwnl_z(g, x, w, xa); break;
+    case MO_QUICK_NL: advs_quicknl_z(g, x, w, xa); break;
     case MO_WENO: advs_weno_z(g, x, w, xa, adv); break;
     case MO_PPM: advs_ppm_z(g, x, w, xa, adv); break;
     case MO_LW: advs_lw_z(g, x, w, xa, adv); break;
@@ -1808,7 +1896,10 @@ static void gradp_compressible(const mo_grid *g, double *p, double *gpx, double 
 
 int mo_prognostic_pressure(const mo_grid *g, const mo_acoustic *a, const mo_acoustic_state *s)
 {
-    if (g->scal_adv == MO_QUICK) return 1;
+    /* without the limiter, quick takes its own faces and every other scheme the
+     * Lax-Wendroff ones (advection.f90:582-592) */
+    const int nl = g->scal_adv == MO_QUICK ? MO_QUICK_NL : MO_LW_NL;
+    if (nl == MO_QUICK_NL && g->nz < 6) return 1;
     const int nx = g->nx, ny = g->ny, nz = g->nz;
     const double grav = 9.81, pref = 100000., cp_a = 1004., cv_a = 716., cp_v = 1827., cv_v = 1388.5;
     const double adiv = 0.2;                       /* prognostic_pressure.f90:53 */
@@ -1829,12 +1920,12 @@ int mo_prognostic_pressure(const mo_grid *g, const mo_acoustic *a, const mo_acou
         memset(ww, 0, nc * sizeof(double));
         memset(buoy, 0, nc * sizeof(double));
         /* advect: density (adv=.false.) then es (flux form, CONSERVATIVE), x, y, z */
-        advection_dir_s(g, MO_LW_NL, 0, s->dens, a->uadv, densa, 0);
-        advection_dir_s(g, MO_LW_NL, 0, s->es, a->uadv, esa, 0);
-        advection_dir_s(g, MO_LW_NL, 1, s->dens, a->vadv, densa, 0);
-        advection_dir_s(g, MO_LW_NL, 1, s->es, a->vadv, esa, 0);
-        advection_dir_s(g, MO_LW_NL, 2, s->dens, a->wadv, densa, 0);
-        advection_dir_s(g, MO_LW_NL, 2, s->es, a->wadv, esa, 0);
+        advection_dir_s(g, nl, 0, s->dens, a->uadv, densa, 0);
+        advection_dir_s(g, nl, 0, s->es, a->uadv, esa, 0);
+        advection_dir_s(g, nl, 1, s->dens, a->vadv, densa, 0);
+        advection_dir_s(g, nl, 1, s->es, a->vadv, esa, 0);
+        advection_dir_s(g, nl, 2, s->dens, a->wadv, densa, 0);
+        advection_dir_s(g, nl, 2, s->es, a->wadv, esa, 0);
         /* integ_scal (integpack.f90:171-217) */
         for (size_t c = 0; c < nc; c++) {
             s->tdens[c] = densa[c] + b_lm * s->tdens[c];

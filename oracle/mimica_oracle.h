@@ -28,8 +28,9 @@ extern "C" {
 #endif
 
 enum { MO_WENO = 0, MO_PPM = 1, MO_MUSCL = 2, MO_LW = 3, MO_QUICK = 4 };
-/* the unlimited Lax-Wendroff faces of the acoustic sub-steps (advq_lw_nolim.f90) */
-enum { MO_LW_NL = 16 };
+/* the unlimited faces of the acoustic sub-steps: Lax-Wendroff (advq_lw_nolim.f90) and
+ * QUICK (advq_quick_nolim.f90) */
+enum { MO_LW_NL = 16, MO_QUICK_NL = 17 };
 enum { MO_LIM_MINMOD = 0, MO_LIM_VL = 1, MO_LIM_MC = 2, MO_LIM_DEFAULT = 3 };
 
 /* SGS turbulence switches (src/TYPES/shared_data.f90, INCLUDE/default.h), the
@@ -166,7 +167,7 @@ typedef struct mo_acoustic_state {
     double **tscal;
     double *cs2;                   /* out: thermo_prop%cs2 */
 } mo_acoustic_state;
-/* returns 0, or 1 for scal_adv = quick (advq_quick_nolim.f90, not restated) */
+/* returns 0, or 1 for scal_adv = quick with nz < 6 (its bottom face reads x(nz-5)) */
 int mo_prognostic_pressure(const mo_grid *g, const mo_acoustic *a, const mo_acoustic_state *s);
 
 #ifdef __cplusplus

@@ -286,7 +286,7 @@ class Oracle:
         s.scal, s.tscal = C.cast(scp, C.POINTER(_dp)), C.cast(tsp, C.POINTER(_dp))
         rc = self.L.mo_prognostic_pressure(self.gp, C.byref(a), C.byref(s))
         if rc:
-            raise RuntimeError("the oracle's acoustic sub-steps do not cover scal_adv = quick")
+            raise RuntimeError("the oracle's acoustic sub-steps need nz >= 6 with scal_adv = quick")
         return st
 
     def buoyancy(self, dens, es, qt=None):

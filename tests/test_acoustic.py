@@ -1,6 +1,6 @@
 """The compressible model's acoustic sub-steps (prognostic_pressure.f90) in the oracle:
-the flux-form Lax-Wendroff faces conserve mass, so over ntau sub-steps of stage 1 the
-domain's mass changes by exactly the slow tendency's share; quick is refused."""
+the flux-form faces conserve mass, so over ntau sub-steps of stage 1 the domain's mass
+changes by exactly the slow tendency's share; quick takes its own faces."""
 import numpy as np
 import pytest
 
@@ -12,7 +12,7 @@ def _interior(d):
     return (slice(None), slice(3, 3 + d.maxy), slice(3, 3 + d.maxx))
 
 
-@pytest.mark.parametrize("scheme", ["weno", "muscl"])
+@pytest.mark.parametrize("scheme", ["weno", "muscl", "quick"])
 def test_stage1_mass_changes_by_the_slow_tendency_only(scheme):
     d = config.warm_bubble_domain(24, 20, 16, dz=40.0, dt0=0.5, scheme=scheme)
     inp, st = acoustic.acoustic_case(d, seed=11, im=1, ntau=8)
@@ -36,8 +36,21 @@ def test_stage1_mass_changes_by_the_slow_tendency_only(scheme):
     np.testing.assert_allclose(out.p[I] + d.p0[:, None, None], pfull, rtol=1e-12)
 
 
-def test_quick_is_not_restated():
-    d = config.warm_bubble_domain(16, 16, 8, scheme="quick")
+def test_quick_needs_six_levels():
+    """advsz_quick_nl's bottom face reads x(nz-5) (advq_quick_nolim.f90:233)."""
+    d = config.warm_bubble_domain(16, 16, 5, scheme="quick")
     inp, st = acoustic.acoustic_case(d, seed=1, ntau=2)
     with pytest.raises(RuntimeError):
         O.Oracle(d).prognostic_pressure(inp, st)
+
+
+def test_quick_and_lax_wendroff_faces_differ():
+    """Without the limiter, quick takes its own faces and every other scheme the
+    Lax-Wendroff ones (advection.f90:582-592)."""
+    out = {}
+    for scheme in ("quick", "weno", "ppm"):
+        d = config.warm_bubble_domain(24, 20, 16, dz=40.0, dt0=0.5, scheme=scheme)
+        inp, st = acoustic.acoustic_case(d, seed=2, ntau=2)
+        out[scheme] = O.Oracle(d).prognostic_pressure(inp, st)
+    assert np.array_equal(out["weno"].dens, out["ppm"].dens)
+    assert not np.array_equal(out["weno"].dens, out["quick"].dens)

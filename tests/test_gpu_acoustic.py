@@ -57,11 +57,22 @@ def test_every_limited_scheme_uses_the_lax_wendroff_faces():
         _check(d, _run(d, inp, st), ref)
 
 
-def test_quick_is_refused():
-    d = config.warm_bubble_domain(16, 16, 8, scheme="quick")
+@pytest.mark.parametrize("im", [1, 2])
+def test_quick_faces_match_the_oracle(im):
+    """quick takes advq_quick_nolim's faces (advection.f90:586-587)."""
+    d = config.warm_bubble_domain(40, 32, 24, dz=40.0, dt0=0.5, scheme="quick")
+    inp, st = acoustic.acoustic_case(d, seed=40 + im, im=im, ntau=5, nscal=1)
+    ref = O.Oracle(d).prognostic_pressure(inp, st)
+    _check(d, _run(d, inp, st), ref)
+
+
+def test_quick_needs_six_levels():
+    """A quick context of 5 levels is refused (by mg_create, which needs more levels for
+    the anelastic step, or by the acoustic entry, whose bottom face reads x(nz-5))."""
+    d = config.warm_bubble_domain(16, 16, 5, scheme="quick")
     inp, st = acoustic.acoustic_case(d, seed=1, ntau=2)
-    with Mimica(d, nscal=1) as m:
-        with pytest.raises(_lib.MimicaError) as ex:
+    with pytest.raises(_lib.MimicaError) as ex:
+        with Mimica(d, nscal=1) as m:
             m.prognostic_pressure(inp, st)
     assert ex.value.code == _lib.MG_ERR_PARAM
 
