@@ -75,8 +75,9 @@ class MgTune(C.Structure):
     _fields_ = [
         ("x_nstage", C.c_int), ("x_radix", C.c_int * 16), ("y_nstage", C.c_int), ("y_radix", C.c_int * 16),
         ("x_threads", C.c_int), ("y_threads", C.c_int), ("tri_block", C.c_int), ("k1_segments", C.c_int),
-        ("candidates", C.c_int), ("ms_default", C.c_double), ("ms_tuned", C.c_double),
-        ("k1_ms_default", C.c_double), ("k1_ms_tuned", C.c_double),
+        ("k2_segments", C.c_int), ("candidates", C.c_int), ("ms_default", C.c_double), ("ms_tuned", C.c_double),
+        ("k1_ms_default", C.c_double), ("k1_ms_tuned", C.c_double), ("k2_ms_default", C.c_double),
+        ("k2_ms_tuned", C.c_double),
     ]
 
 

@@ -2493,6 +2493,33 @@ static int time_k1(mg_ctx *c, int reps, double *ms)
     return check_err(c);
 }
 
+// one stage-1 momentum launch (K2 writes the stage buffers only), averaged over reps
+static int time_k2(mg_ctx *c, int reps, double *ms)
+{
+    K2Args a{};
+    k2_stage_args(c, 1, 1, a);
+    cudaEvent_t e0, e1;
+    CKR(cudaEventCreate(&e0));
+    cudaError_t er = cudaEventCreate(&e1);
+    if (er != cudaSuccess) { cudaEventDestroy(e0); return cuerr(er); }
+    auto launch = [&]() {
+        return c->prm.precision == MG_PREC_MIXED ? launch_k2_mixed(c->G, a, c->mmaps1, c->stream)
+                                                  : launch_k2(c->G, a, c->mmaps1, c->stream);
+    };
+    er = launch();   // warm-up
+    if (er == cudaSuccess) er = cudaEventRecord(e0, c->stream);
+    for (int r = 0; r < reps && er == cudaSuccess; r++) er = launch();
+    if (er == cudaSuccess) er = cudaEventRecord(e1, c->stream);
+    if (er == cudaSuccess) er = cudaEventSynchronize(e1);
+    float f = 0.f;
+    if (er == cudaSuccess) er = cudaEventElapsedTime(&f, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (er != cudaSuccess) return cuerr(er);
+    *ms = f / reps;
+    return check_err(c);
+}
+
 static bool tune_to_knobs(const mg_tune *t, PressureKnobs *k)
 {
     if (t->x_nstage < 1 || t->x_nstage > 16 || t->y_nstage < 1 || t->y_nstage > 16) return false;
@@ -2521,6 +2548,7 @@ extern "C" int mg_tune_get(mg_ctx *c, mg_tune *t)
     pressure_get_knobs(c->pp, &k);
     knobs_to_tune(k, t);
     t->k1_segments = c->k1_nseg;
+    t->k2_segments = c->k2_nseg;
     return MG_OK;
 }
 
@@ -2529,8 +2557,10 @@ extern "C" int mg_tune_set(mg_ctx *c, const mg_tune *t)
     if (!c || !t) return MG_ERR_PARAM;
     PressureKnobs k;
     if (t->k1_segments < 0 || t->k1_segments > c->G.nz) return MG_ERR_PARAM;
+    if (t->k2_segments < 0 || t->k2_segments > c->G.nz) return MG_ERR_PARAM;
     if (!tune_to_knobs(t, &k) || !pressure_set_knobs(c->pp, c->G, k)) return MG_ERR_PARAM;
     c->k1_nseg = t->k1_segments;
+    c->k2_nseg = t->k2_segments;
     drop_graphs(c);
     return MG_OK;
 }
@@ -2646,16 +2676,38 @@ extern "C" int mg_autotune(mg_ctx *c, int reps, mg_tune *result)
         }
         c->k1_nseg = nseg_best;
     }
+    // K2's k segments per column tile, the same candidates
+    double k2_def = 0., k2_best = 0., t2 = 0.;
+    const int nseg2_in = c->k2_nseg;
+    int nseg2_best = nseg2_in;
+    {
+        if ((rc = time_k2(c, reps, &k2_def))) return rc;
+        k2_best = k2_def;
+        const int cands[9] = {0, 1, 2, 3, 4, 6, 8, 12, 16};
+        for (int n : cands) {
+            if (n == nseg2_in || n * 8 > c->G.nz) continue;
+            c->k2_nseg = n;
+            rc = time_k2(c, reps, &t2);
+            c->k2_nseg = nseg2_in;
+            if (rc) return rc;
+            ncand++;
+            if (t2 < 0.99 * k2_best) { k2_best = t2; nseg2_best = n; }
+        }
+        c->k2_nseg = nseg2_best;
+    }
     drop_graphs(c);
     if (result) {
         memset(result, 0, sizeof(*result));
         knobs_to_tune(cur, result);
         result->k1_segments = nseg_best;
+        result->k2_segments = nseg2_best;
         result->candidates = ncand;
         result->ms_default = ms_default;
         result->ms_tuned = tuned;
         result->k1_ms_default = k1_def;
         result->k1_ms_tuned = k1_best;
+        result->k2_ms_default = k2_def;
+        result->k2_ms_tuned = k2_best;
     }
     return MG_OK;
 }

@@ -110,7 +110,8 @@ class Mimica:
         if wisdom:
             tune.store(wisdom, k, plan)
         return dict(plan, source="measured", candidates=t.candidates, ms_default=t.ms_default, ms_tuned=t.ms_tuned,
-                    k1_ms_default=t.k1_ms_default, k1_ms_tuned=t.k1_ms_tuned)
+                    k1_ms_default=t.k1_ms_default, k1_ms_tuned=t.k1_ms_tuned, k2_ms_default=t.k2_ms_default,
+                    k2_ms_tuned=t.k2_ms_tuned)
 
     def set_dt(self, dt0: float) -> None:
         _lib.check(self._L.mg_set_dt(self._h, float(dt0)), "mg_set_dt")

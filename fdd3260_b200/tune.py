@@ -12,12 +12,13 @@ import os
 
 from . import _lib
 
-FIELDS = ("x_radix", "y_radix", "x_threads", "y_threads", "tri_block", "k1_segments")
+FIELDS = ("x_radix", "y_radix", "x_threads", "y_threads", "tri_block", "k1_segments", "k2_segments")
 
 
 def to_dict(t: _lib.MgTune) -> dict:
     return {"x_radix": list(t.x_radix)[:t.x_nstage], "y_radix": list(t.y_radix)[:t.y_nstage],
-            "x_threads": t.x_threads, "y_threads": t.y_threads, "tri_block": t.tri_block, "k1_segments": t.k1_segments}
+            "x_threads": t.x_threads, "y_threads": t.y_threads, "tri_block": t.tri_block, "k1_segments": t.k1_segments,
+            "k2_segments": t.k2_segments}
 
 
 def from_dict(d: dict) -> _lib.MgTune:
@@ -32,6 +33,7 @@ def from_dict(d: dict) -> _lib.MgTune:
         t.y_radix[q] = int(r)
     t.x_threads, t.y_threads, t.tri_block = int(d["x_threads"]), int(d["y_threads"]), int(d["tri_block"])
     t.k1_segments = int(d.get("k1_segments", 0))
+    t.k2_segments = int(d.get("k2_segments", 0))
     return t
 
 
@@ -58,7 +60,8 @@ def store(path: str, k: str, plan: dict) -> None:
     process, so concurrent writers (ranks tuning their own grids) never leave a partial
     file; one writer's entry can be lost to another's, and is then tuned again."""
     w = load(path)
-    w[k] = {f: plan[f] for f in FIELDS}
+    # the segment counts default to the wave model's choice (0)
+    w[k] = {f: plan.get(f, 0) if f.endswith("_segments") else plan[f] for f in FIELDS}
     tmp = f"{path}.{os.getpid()}.tmp"
     with open(tmp, "w") as f:
         json.dump(w, f, indent=1, sort_keys=True)

@@ -203,10 +203,12 @@ typedef struct mg_tune {
     int tri_block;      /* threads per block, tridiagonal solve: 64, 128, 256 */
     int k1_segments;    /* scalar advection: k segments per 32 x 8 column tile (0: chosen per
                            launch from the grid by a wave model; PPM keeps whole columns) */
+    int k2_segments;    /* momentum: k segments per 32 x 8 column tile (0: the wave model) */
     int candidates;     /* plans timed by mg_autotune */
     double ms_default;  /* one projection with the plan in force before mg_autotune */
     double ms_tuned;    /* one projection with the plan it chose */
     double k1_ms_default, k1_ms_tuned;   /* one stage-1 scalar-advection launch, likewise */
+    double k2_ms_default, k2_ms_tuned;   /* one stage-1 momentum launch, likewise */
 } mg_tune;
 int mg_autotune(mg_ctx *ctx, int reps, mg_tune *result);
 int mg_tune_get(mg_ctx *ctx, mg_tune *t);

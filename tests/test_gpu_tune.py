@@ -62,10 +62,11 @@ def test_autotune_keeps_state_and_step_parity():
         back = m.download()
         for x, y in zip(_fields(back), _fields(st)):
             assert np.array_equal(x[:, 3:-2, 3:-2], y[:, 3:-2, 3:-2])
-        # a non-default plan (the scalar advection in its two k segments of 10 levels), then
+        # a non-default plan (the scalar advection and the momentum in two k segments of
+        # 10 levels each), then
         # a few steps against the oracle
         m.tune_set(dict(plan, x_radix=[2, 8, 3], y_radix=[5, 8], x_threads=16, y_threads=16, tri_block=64,
-                        k1_segments=2))
+                        k1_segments=2, k2_segments=2))
         m.stepping(3, ntime0=1, graph=True)
         g = m.download()
     r, _, _ = O.Oracle(d).stepping(st, nsteps=3, ntime0=1)
@@ -80,7 +81,8 @@ def test_invalid_plans_rejected():
         base = m.tune_get()
         for bad in (dict(base, x_radix=[8, 8]), dict(base, y_radix=[7, 3]), dict(base, x_threads=128),
                     dict(base, y_threads=256), dict(base, tri_block=96), dict(base, x_radix=[6, 4]),
-                    dict(base, k1_segments=-1), dict(base, k1_segments=13)):
+                    dict(base, k1_segments=-1), dict(base, k1_segments=13), dict(base, k2_segments=-1),
+                    dict(base, k2_segments=13)):
             with pytest.raises(_lib.MimicaError):
                 m.tune_set(bad)
         assert m.tune_get() == base

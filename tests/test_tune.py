@@ -36,9 +36,12 @@ def test_radix_candidates_reject_other_primes():
 
 def test_wisdom_round_trip(tmp_path):
     plan = {"x_radix": [4, 4, 4, 4, 2], "y_radix": [3, 8, 4], "x_threads": 16, "y_threads": 64, "tri_block": 256,
-            "k1_segments": 2}
+            "k1_segments": 2, "k2_segments": 3}
     t = tune.from_dict(plan)
     assert tune.to_dict(t) == plan
+    # a plan stored before K2's segments were a coordinate replays with the wave model's choice
+    old = {f: v for f, v in plan.items() if f != "k2_segments"}
+    assert tune.to_dict(tune.from_dict(old)) == dict(old, k2_segments=0)
     path = str(tmp_path / "wisdom.json")
     k = tune.key(512, 96, 64, _lib.MG_PREC_FP64, 5)
     tune.store(path, k, dict(plan, ms_tuned=1.0))
