@@ -1745,7 +1745,6 @@ static cudaError_t traj_step_tl(mg_ctx *c, int ntime, const NatState &N, const N
 struct StageAdWork {
     double *abar[3];
     double *Abar[MG_MAXF];
-    double *tmp[4];
 };
 
 static cudaError_t traj_stage_ad(mg_ctx *c, int ntime, int stage, const NatState &N, const NatState &Nbar,
@@ -1789,14 +1788,12 @@ static cudaError_t traj_stage_ad(mg_ctx *c, int ntime, int stage, const NatState
         S.advbar[f] = W.Abar[f]; S.tprev_bar[f] = ts_out ? ts_out[f] : nullptr; S.snbar[f] = Nbar.s[f];
     }
     if ((e = launch_stage_scal_ad(G, S, c->stream)) != cudaSuccess) return e;
-    for (int f = 0; f < nf; f++) {
-        if ((e = launch_advection_ad(G, R.xs[f], R.xm[0], R.xm[1], R.xm[2], W.Abar[f], W.tmp[0], W.tmp[1], W.tmp[2],
-                                     W.tmp[3], c->stream)) != cudaSuccess)
+    // each field's advection adjoint adds onto the stage-input bars directly (their ghost
+    // cells are zero: every other contribution above writes the interior only)
+    for (int f = 0; f < nf; f++)
+        if ((e = launch_advection_ad(G, R.xs[f], R.xm[0], R.xm[1], R.xm[2], W.Abar[f], xs_in_bar[f], xm_in_bar[0],
+                                     xm_in_bar[1], xm_in_bar[2], c->stream, 1)) != cudaSuccess)
             return e;
-        if ((e = launch_axpy(G, xs_in_bar[f], W.tmp[0], 1., c->stream)) != cudaSuccess) return e;
-        for (int q = 0; q < 3; q++)
-            if ((e = launch_axpy(G, xm_in_bar[q], W.tmp[1 + q], 1., c->stream)) != cudaSuccess) return e;
-    }
     return cudaSuccess;
 }
 
@@ -1995,7 +1992,6 @@ static int traj_adjoint_run(mg_ctx *c, int nsteps, int ntime0, int ckpt, const d
     for (int f = 0; f < nf; f++) {
         S.W.Abar[f] = T.B.get(); S.xs2b[f] = T.B.get(); S.xs1b[f] = T.B.get(); S.xs0b[f] = T.B.get(); S.tsc[f] = T.B.get();
     }
-    for (int q = 0; q < 4; q++) S.W.tmp[q] = T.B.get();
     S.pb = T.B.get();
     // checkpoints (natural states every ckpt steps) and the states of one segment; the
     // checkpoints go to page-locked host memory when asked, or (auto) when on the device

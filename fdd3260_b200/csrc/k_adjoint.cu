@@ -246,15 +246,17 @@ cudaError_t launch_advection_tl(const DevGrid &g, const double *x, const double 
     return cudaSuccess;
 }
 
-// xbar, mubar, mvbar, mwbar are overwritten
+// xbar, mubar, mvbar, mwbar are overwritten (accumulate = 0) or added to (1: their ghost
+// cells are zero on entry; the ghost folds below move the kernels' ghost contributions
+// onto the cells they image and leave the ghosts zero)
 cudaError_t launch_advection_ad(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
                                 const double *Abar, double *xbar, double *mubar, double *mvbar, double *mwbar,
-                                cudaStream_t s)
+                                cudaStream_t s, int accumulate)
 {
     const size_t fbytes = (size_t)g.ps * g.nz * 8;
     cudaError_t e;
     double *outs[4] = {xbar, mubar, mvbar, mwbar};
-    for (int q = 0; q < 4; q++)
+    for (int q = 0; q < 4 && !accumulate; q++)
         if ((e = cudaMemsetAsync(outs[q], 0, fbytes, s)) != cudaSuccess) return e;
     const AdvIn in{x, mu, mv, mw};
     auto tiles = [&](int na, int la, int nb, int lb, int nfix) {

@@ -283,9 +283,11 @@ cudaError_t launch_qnadv_ad(const DevGrid &g, const double *mu, const double *mv
 cudaError_t launch_advection_tl(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
                                 const double *dx, const double *dmu, const double *dmv, const double *dmw, double *dA,
                                 double *scratch, cudaStream_t s);
+// accumulate = 0: xbar, mubar, mvbar, mwbar are overwritten; 1: added to (their ghost
+// cells must be zero on entry, and are zero on exit)
 cudaError_t launch_advection_ad(const DevGrid &g, const double *x, const double *mu, const double *mv, const double *mw,
                                 const double *Abar, double *xbar, double *mubar, double *mvbar, double *mwbar,
-                                cudaStream_t s);
+                                cudaStream_t s, int accumulate = 0);
 
 // projection
 struct PressurePlan;

@@ -100,3 +100,29 @@ def test_grouped_mode_refuses_mixed_forms():
     finally:
         for m in members:
             m.close()
+
+
+@pytest.mark.parametrize("scheme", ["ppm", "muscl", "quick"])
+def test_grouped_other_schemes_equal_members_stepped_alone(scheme):
+    """The grouped K1 instantiates every scheme (PPM keeps whole columns, as here)."""
+    specs = [E.MemberSpec(0, 24, 16, 21, 2.0, (600.0, 600.0, 200.0)),
+             E.MemberSpec(1, 32, 12, 22, 1.5, (800.0, 700.0, 150.0))]
+    probs = []
+    for s in specs:
+        d, st = E.member_problem(s, precision=_lib.MG_PREC_FP64)
+        d.scal_adv = scheme
+        probs.append((d, st))
+    batched, _ = _batched(probs, 4, "grouped")
+    _same(_alone(probs, 4), batched)
+
+
+def test_grouped_more_members_than_one_momentum_launch_holds():
+    """K2's grouped arguments are a kernel parameter of at most 64 members: 70 members
+    take two K2 launches per stage, with the same results."""
+    rng = np.random.default_rng(7)
+    specs = [E.MemberSpec(q, int(rng.choice([16, 24])), 12, 100 + q, 1.0 + q % 3, (300.0, 300.0, 150.0))
+             for q in range(70)]
+    probs = [E.member_problem(s, precision=_lib.MG_PREC_FP64) for s in specs]
+    batched, launches = _batched(probs, 2, "grouped")
+    _same(_alone(probs, 2), batched)
+    assert launches == 2 * (14 + 1)   # one more K2 launch per stage
