@@ -190,3 +190,30 @@ def test_exact_projection_reaches_fp64_divergence():
     # the mixed exact form stays close to the FP64 exact form (measured in the print above)
     bad = {k: v for k, v in e.items() if not v <= 1e-5}
     assert not bad, (bad, e)
+
+
+@pytest.mark.parametrize("maxy", [64, 128, 256])
+def test_mixed_fft_solve_with_the_shuffle_y_transform(maxy):
+    """FP32 spectra whose y length is 64..512 take the warp-shuffle y transform: the
+    mixed fft_solve stays within FP32 rounding of the oracle's FP64 solve."""
+    d = config.warm_bubble_domain(48, maxy, 12)
+    d.precision = _lib.MG_PREC_MIXED
+    rng = np.random.default_rng(maxy)
+    tend = rng.standard_normal(d.shape)
+    with Mimica(d, nscal=1) as m:
+        got = m.fft_solve(tend)
+    d.precision = _lib.MG_PREC_FP64
+    ref = O.Oracle(d).fft_solve(tend)
+    a, b = _interior(got), _interior(ref)
+    rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+    print(f"maxy {maxy}: mixed fft_solve relative L2 {rel:.2e}")
+    assert rel <= 1e-4
+
+
+def test_mixed_step_with_the_shuffle_y_transform():
+    """Four mixed steps of a 64 x 64 bubble (the shuffle y transform in every projection
+    pass) within the warm bubble's tolerances of the FP64 oracle."""
+    d = config.warm_bubble_domain(64, 64, 24)
+    st = config.warm_bubble_state(d, seed=12, centre=(1600.0, 1600.0, 400.0), radius=500.0)
+    err = _run_mixed(d, st, 4, len(st.scal))
+    assert not _over(err, BUBBLE_TOL), err
