@@ -124,7 +124,9 @@ __device__ __forceinline__ void k1_run(const DevGrid &G, const K1Args &A, const 
     constexpr int PF = k1_pf(SCHEME), NPS = k1_nps(SCHEME), NFB = k1_nfb(SCHEME);
     constexpr bool CONV1 = STAGE == 1;   // stage-1 inputs are natural: psi = s * rho
     extern __shared__ unsigned char smraw[];
-    unsigned char *sm = (unsigned char *)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
+    // 128-byte alignment by an offset from the shared array itself, so that every pointer
+    // derived from it stays a shared-memory pointer
+    unsigned char *sm = smraw + ((128u - (smem_u32(smraw) & 127u)) & 127u);
     const int F = FC > 0 ? FC : A.nf;
     const Layout Ly = make_layout(SCHEME, F);
     constexpr int ZS = SCHEME == MG_PPM ? 5 : 4;   // z-ring slots

@@ -58,7 +58,9 @@ __device__ __forceinline__ void k2_run(const DevGrid &G, const K2Args &A, const 
     // R: type of the stencil arithmetic (FP64 plain form, FP32 mixed form)
     using R = typename std::conditional<MIXED, float, double>::type;
     extern __shared__ unsigned char sm_raw[];
-    unsigned char *smb = (unsigned char *)(((uintptr_t)sm_raw + 127) & ~(uintptr_t)127);
+    // 128-byte alignment by an offset from the shared array itself, so that every pointer
+    // derived from it stays a shared-memory pointer
+    unsigned char *smb = sm_raw + ((128u - (smem_u32(sm_raw) & 127u)) & 127u);
     R *sm = reinterpret_cast<R *>(smb);
     R *ring_m = sm;                            // [slot][3][PL] momentum (stencil values)
     R *ring_a = sm + NSLOT * 3 * PL;           // [slot][3][PL] advective velocity
