@@ -601,6 +601,8 @@ struct Gath {
     }
 };
 
+// one output component per launch (C: 0 u, 1 v, 2 w): a third of the code each
+template <int C>
 __global__ void __launch_bounds__(128) mom_ad_gather_kernel(DevGrid G, Mom3 v, Mom3 ab, Mom3 bar)
 {
     const int i = 4 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -609,15 +611,15 @@ __global__ void __launch_bounds__(128) mom_ad_gather_kernel(DevGrid G, Mom3 v, M
     if (i > G.nx - 2) return;
     const Gath g(G, v, ab, i, j, k);
     const long long q = g.q0;
-    double *ub = const_cast<double *>(bar.m[0]), *vb = const_cast<double *>(bar.m[1]), *wb = const_cast<double *>(bar.m[2]);
-    // u: u_x, u_y (advected), h_z (f 0, advected), v_x (velocity), w_h x (velocity)
-    ub[q] += g.self_h(0, i, j, k) + g.cross_adv(0, i, j, k) + g.hz_adv(0, i, j, k) + g.cross_vel(1, i, j, k) +
-             g.wh_vel(0, i, j, k);
-    // v: v_y, v_x (advected), h_z (f 1, advected), u_y (velocity), w_h y (velocity)
-    vb[q] += g.self_h(1, i, j, k) + g.cross_adv(1, i, j, k) + g.hz_adv(1, i, j, k) + g.cross_vel(0, i, j, k) +
-             g.wh_vel(1, i, j, k);
-    // w: w_z, w_h x and y (advected), h_z f 0 and f 1 (velocity)
-    wb[q] += g.wz_w(i, j, k) + g.wh_w(0, i, j, k) + g.wh_w(1, i, j, k) + g.hz_w(0, i, j, k) + g.hz_w(1, i, j, k);
+    double *b = const_cast<double *>(bar.m[C]);
+    if constexpr (C == 0)   // u: u_x, u_y (advected), h_z (f 0, advected), v_x (velocity), w_h x (velocity)
+        b[q] += g.self_h(0, i, j, k) + g.cross_adv(0, i, j, k) + g.hz_adv(0, i, j, k) + g.cross_vel(1, i, j, k) +
+                g.wh_vel(0, i, j, k);
+    else if constexpr (C == 1)   // v: v_y, v_x (advected), h_z (f 1, advected), u_y (velocity), w_h y (velocity)
+        b[q] += g.self_h(1, i, j, k) + g.cross_adv(1, i, j, k) + g.hz_adv(1, i, j, k) + g.cross_vel(0, i, j, k) +
+                g.wh_vel(1, i, j, k);
+    else   // w: w_z, w_h x and y (advected), h_z f 0 and f 1 (velocity)
+        b[q] += g.wz_w(i, j, k) + g.wh_w(0, i, j, k) + g.wh_w(1, i, j, k) + g.hz_w(0, i, j, k) + g.hz_w(1, i, j, k);
 }
 
 }  // namespace
@@ -643,7 +645,9 @@ cudaError_t launch_qnadv_ad(const DevGrid &g, const double *mu, const double *mv
     cudaError_t e = launch_halo_fill(g, ab, 3, s);
     if (e != cudaSuccess) return e;
     const dim3 grid((g.maxx + 127) / 128, g.maxy, g.nz);
-    mom_ad_gather_kernel<<<grid, 128, 0, s>>>(g, Mom3{{mu, mv, mw}}, Mom3{{aubar, avbar, awbar}},
-                                              Mom3{{mubar, mvbar, mwbar}});
+    const Mom3 v{{mu, mv, mw}}, ab3{{aubar, avbar, awbar}}, bar{{mubar, mvbar, mwbar}};
+    mom_ad_gather_kernel<0><<<grid, 128, 0, s>>>(g, v, ab3, bar);
+    mom_ad_gather_kernel<1><<<grid, 128, 0, s>>>(g, v, ab3, bar);
+    mom_ad_gather_kernel<2><<<grid, 128, 0, s>>>(g, v, ab3, bar);
     return cudaGetLastError();
 }
