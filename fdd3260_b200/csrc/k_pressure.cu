@@ -728,10 +728,13 @@ __global__ void correction_kernel(const __grid_constant__ DevGrid G, const doubl
 
 // -------------------- reductions --------------------
 // per-level sums over the interior, fixed-order tree (deterministic)
+// one block of LSUM_THREADS threads per level (a fixed-order tree: the sums do not depend
+// on the launch); 1024 threads so that a few hundred levels fill the GPU
+constexpr int LSUM_THREADS = 1024;
 __device__ __forceinline__ void level_sums_run(const DevGrid &G, const double *x, const double *xold, int old_rep,
                                                double dt0, double *out_mean, double *out_mean_d, const int bid)
 {
-    __shared__ double s1[256], s2[256];
+    __shared__ double s1[LSUM_THREADS], s2[LSUM_THREADS];
     const int k = bid + 1;
     const int maxx = G.maxx, maxy = G.maxy;
     const double a0 = __ldg(G.avden0 + k - 1);
@@ -767,7 +770,7 @@ __device__ __forceinline__ void level_sums_run(const DevGrid &G, const double *x
         if (out_mean_d) out_mean_d[k - 1] = s2[0] / nn;
     }
 }
-__global__ void level_sums(const __grid_constant__ DevGrid G, const double *x, const double *xold, int old_rep, double dt0,
+__global__ void __launch_bounds__(LSUM_THREADS) level_sums(const __grid_constant__ DevGrid G, const double *x, const double *xold, int old_rep, double dt0,
                            double *out_mean, double *out_mean_d)
 {
     level_sums_run(G, x, xold, old_rep, dt0, out_mean, out_mean_d, blockIdx.x);
@@ -991,7 +994,8 @@ __global__ void correction_grp(const CorrMember *__restrict__ mem, const GItem *
     const CorrMember &m = mem[g.m];
     correction_run(m.G, m.dp, m.mu, m.mv, m.mw, m.p, m.natural_uv, g.b);
 }
-__global__ void level_sums_grp(const LevelMember *__restrict__ mem, const GItem *__restrict__ it)
+__global__ void __launch_bounds__(LSUM_THREADS) level_sums_grp(const LevelMember *__restrict__ mem,
+                                                               const GItem *__restrict__ it)
 {
     const GItem g = it[blockIdx.x];
     const LevelMember &m = mem[g.m];
@@ -1419,7 +1423,7 @@ cudaError_t launch_correction(const DevGrid &g, PressurePlan *pp, double *mu, do
 cudaError_t launch_cal_p1(const DevGrid &g, PressurePlan *pp, double *mw, const double *wold, int wold_rep,
                           int want_p1, int natural_w, cudaStream_t s)
 {
-    level_sums<<<g.nz, 256, 0, s>>>(g, mw, wold, wold_rep, g.dt0, pp->mean, want_p1 ? pp->mean_d : nullptr);
+    level_sums<<<g.nz, LSUM_THREADS, 0, s>>>(g, mw, wold, wold_rep, g.dt0, pp->mean, want_p1 ? pp->mean_d : nullptr);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (want_p1) {
@@ -1432,7 +1436,7 @@ cudaError_t launch_cal_p1(const DevGrid &g, PressurePlan *pp, double *mw, const 
 
 cudaError_t launch_level_mean(const DevGrid &g, const double *x, double *mean, cudaStream_t s)
 {
-    level_sums<<<g.nz, 256, 0, s>>>(g, x, nullptr, -1, g.dt0, mean, nullptr);
+    level_sums<<<g.nz, LSUM_THREADS, 0, s>>>(g, x, nullptr, -1, g.dt0, mean, nullptr);
     return cudaGetLastError();
 }
 
@@ -1583,7 +1587,7 @@ cudaError_t pressure_adjoint(const DevGrid &g, PressurePlan *pp, int nsubp, doub
     const long long n = (long long)g.maxx * g.maxy * nz;
     const unsigned nb = (unsigned)((n + 255) / 256);
     // cal_p1^T: remove the level mean of wbar (interior)
-    level_sums<<<nz, 256, 0, s>>>(g, mwb, mwb, -1, g.dt0, pp->mean, nullptr);
+    level_sums<<<nz, LSUM_THREADS, 0, s>>>(g, mwb, mwb, -1, g.dt0, pp->mean, nullptr);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     adj_sub_level_mean_kernel<<<nb, 256, 0, s>>>(g, mwb, pp->mean);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1883,7 +1887,7 @@ void group_projection_t(GroupProgram &P, const std::vector<GroupProjIn> &in, int
         const size_t mo = P.put(lm), io1 = P.put(its), io2 = P.put(itm);
         const int n1 = (int)its.size(), n2 = (int)itm.size();
         P.ops.push_back([=](const unsigned char *d, cudaStream_t s) {
-            level_sums_grp<<<n1, 256, 0, s>>>((const LevelMember *)(d + mo), (const GItem *)(d + io1));
+            level_sums_grp<<<n1, LSUM_THREADS, 0, s>>>((const LevelMember *)(d + mo), (const GItem *)(d + io1));
             return cudaGetLastError();
         });
         P.ops.push_back([=](const unsigned char *d, cudaStream_t s) {
