@@ -969,10 +969,10 @@ def e2e_leg(args, m, d, st, ws) -> dict:
     return {"e2e": {"value": pipelined, "unit": "Mcell-updates/s",
                     "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                     "serial_value": serial,
-                    "timing": "host wall clock, synchronised; every step uploads its whole state from page-locked "
+                    "timing": "host wall clock, synchronised; every step uploads its whole state from the host "
                               "buffers and downloads its result; value: two contexts in two host threads, one upload "
-                              f"apart, {2 * args.e2e_steps} steps; serial_value: one context, {args.e2e_steps} steps "
-                              f"({host_buffers()})",
+                              f"apart, {2 * args.e2e_steps} steps; serial_value: one context, {args.e2e_steps} steps; "
+                              f"host buffers: {host_buffers()}",
                     "host_buffers": host_buffers()}}
 
 

@@ -34,27 +34,32 @@ constexpr int FXN = TY * (TX + 1), FYN = (TY + 1) * TX;   // x faces, y faces of
 constexpr int NHALO = SW * SH - TX * TY;          // 276 plane elements outside the cells
 constexpr int K1_FC = 6;                          // field count with kernels of its own (density + 5 scalars)
 
-// fields per group, group slots of planes in flight, face buffers (parity-double-buffered
-// when a group is one field, single otherwise: an extra barrier then guards reuse)
+// fields per group, group slots of planes in flight, face buffers: parity-double-buffered
+// (a group's faces are written while the cells still read the previous group's) when a
+// group is one field, and in stage 2 and unit mode, which have no density plane; single
+// in stage 1 of two-field groups, whose density products need a barrier before the faces
+// anyway (two face buffers and the density plane would leave one CTA per SM at 6 fields)
 __host__ __device__ constexpr int k1_pf(int scheme) { return scheme == MG_PPM ? 1 : 2; }
 __host__ __device__ constexpr int k1_nps(int scheme) { return scheme == MG_PPM ? 4 : 2; }
-__host__ __device__ constexpr int k1_nfb(int scheme) { return k1_pf(scheme) == 1 ? 2 : 1; }
+__host__ __device__ constexpr int k1_nfb(int scheme, int stage) { return (k1_pf(scheme) == 1 || stage != 1) ? 2 : 1; }
 
 struct Layout {
     int zs;             // z-ring slots
     size_t planes, vbu, vbv, densp, su, sv, fx, fy, mbar, zring, wring, zf, chain, crx, cry, total;
 };
 
-__host__ __device__ inline Layout make_layout(int scheme, int nf)
+// stage: 1, 2, or 0 (unit mode); only stage 1 keeps the density plane
+__host__ __device__ inline Layout make_layout(int scheme, int nf, int stage)
 {
     Layout L;
-    const int PF = k1_pf(scheme), NPS = k1_nps(scheme), NFB = k1_nfb(scheme);
+    const int PF = k1_pf(scheme), NPS = k1_nps(scheme), NFB = k1_nfb(scheme, stage);
     L.zs = scheme == MG_PPM ? 5 : 4;   // window x(k-1..k+L), L = 3 (PPM) or 2
     size_t o = 0;
     L.planes = o; o += (size_t)NPS * PF * PLANE_SLOT;
     L.vbu = o; o += VBOX_SLOT;
     L.vbv = o; o += VBOX_SLOT;
-    L.densp = o; o += PLANE_SLOT;
+    L.densp = o;
+    if (stage == 1) o += PLANE_SLOT;
     L.su = o; o += TY * (TX + 1) * 8;
     L.sv = o; o += (TY + 1) * TX * 8;
     L.fx = o; o += (size_t)NFB * PF * FXN * 8;
@@ -74,6 +79,12 @@ __host__ __device__ inline Layout make_layout(int scheme, int nf)
     }
     L.total = o + 128;   // slack for 128-byte alignment of the base
     return L;
+}
+
+// the largest layout over the stages and unit mode (the launch checks)
+inline size_t k1_smem_max(int scheme, int nf)
+{
+    return std::max(make_layout(scheme, nf, 0).total, std::max(make_layout(scheme, nf, 1).total, make_layout(scheme, nf, 2).total));
 }
 
 // k segments per column tile: the count that minimises (waves of CTAs) x (levels per
@@ -121,14 +132,14 @@ __device__ __forceinline__ int halo_elem(int h)
 template <int SCHEME, bool MIXED, int STAGE, bool SGS, int FC>
 __device__ __forceinline__ void k1_run(const DevGrid &G, const K1Args &A, const K1Maps &M, const int bid)
 {
-    constexpr int PF = k1_pf(SCHEME), NPS = k1_nps(SCHEME), NFB = k1_nfb(SCHEME);
+    constexpr int PF = k1_pf(SCHEME), NPS = k1_nps(SCHEME), NFB = k1_nfb(SCHEME, STAGE);
     constexpr bool CONV1 = STAGE == 1;   // stage-1 inputs are natural: psi = s * rho
     extern __shared__ unsigned char smraw[];
     // 128-byte alignment by an offset from the shared array itself, so that every pointer
     // derived from it stays a shared-memory pointer
     unsigned char *sm = smraw + ((128u - (smem_u32(smraw) & 127u)) & 127u);
     const int F = FC > 0 ? FC : A.nf;
-    const Layout Ly = make_layout(SCHEME, F);
+    const Layout Ly = make_layout(SCHEME, F, STAGE);
     constexpr int ZS = SCHEME == MG_PPM ? 5 : 4;   // z-ring slots
     constexpr int L = SCHEME == MG_PPM ? 3 : 2;    // window x(k-1 .. k+L)
     double *planes = (double *)(sm + Ly.planes);

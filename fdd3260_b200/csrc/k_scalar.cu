@@ -3,12 +3,13 @@
 // with -fmad=false: bit-identical to the CPU restatement.
 #include "k1_body.cuh"
 
-size_t k1_smem_bytes(int scheme, int nf) { return make_layout(scheme, nf).total; }
+size_t k1_smem_bytes(int scheme, int nf) { return k1_smem_max(scheme, nf); }
 
 namespace {
 template <int SCHEME, int STAGE>
-cudaError_t launch_one(const DevGrid &g, const K1Args &a, const K1Maps &maps, size_t sm, cudaStream_t s)
+cudaError_t launch_one(const DevGrid &g, const K1Args &a, const K1Maps &maps, cudaStream_t s)
 {
+    const size_t sm = make_layout(SCHEME, a.nf, STAGE).total;
     const int ntx = (g.maxx + TX - 1) / TX, nty = (g.maxy + TY - 1) / TY;
     K1Args as = a;
     if (as.nseg < 1 || as.nseg > g.nz) as.nseg = k1_segments(g, SCHEME, sm);
@@ -24,11 +25,11 @@ cudaError_t launch_one(const DevGrid &g, const K1Args &a, const K1Maps &maps, si
     return cudaGetLastError();
 }
 template <int SCHEME>
-cudaError_t launch_scheme(const DevGrid &g, const K1Args &a, const K1Maps &maps, size_t sm, cudaStream_t s)
+cudaError_t launch_scheme(const DevGrid &g, const K1Args &a, const K1Maps &maps, cudaStream_t s)
 {
-    if (a.mode == 1) return launch_one<SCHEME, 0>(g, a, maps, sm, s);
-    if (a.stage == 1) return launch_one<SCHEME, 1>(g, a, maps, sm, s);
-    return launch_one<SCHEME, 2>(g, a, maps, sm, s);
+    if (a.mode == 1) return launch_one<SCHEME, 0>(g, a, maps, s);
+    if (a.stage == 1) return launch_one<SCHEME, 1>(g, a, maps, s);
+    return launch_one<SCHEME, 2>(g, a, maps, s);
 }
 template <int SCHEME>
 cudaError_t init_scheme()
@@ -46,7 +47,7 @@ cudaError_t init_scheme()
 template <int SCHEME, int STAGE>
 cudaError_t group_one(int nf, const K1Member *mem, const GItem *items, int nitems, cudaStream_t s)
 {
-    const size_t sm = make_layout(SCHEME, nf).total;
+    const size_t sm = make_layout(SCHEME, nf, STAGE).total;
     if (nf == K1_FC) {
         cudaError_t e = cudaFuncSetAttribute(k1_group_kernel<SCHEME, false, STAGE, K1_FC>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -71,14 +72,13 @@ cudaError_t launch_k1(const DevGrid &g, const K1Args &a, const K1Maps &maps, cud
 {
     if (a.nf <= 0 || a.nf > MG_MAXF) return cudaErrorInvalidValue;
     if (a.mode != 1 && a.stage != 1 && a.stage != 2) return cudaErrorInvalidValue;
-    const size_t sm = make_layout(g.scal_adv, a.nf).total;
-    if (sm > 232448) return cudaErrorInvalidValue;
+    if (k1_smem_max(g.scal_adv, a.nf) > 232448) return cudaErrorInvalidValue;
     switch (g.scal_adv) {
-    case MG_WENO: return launch_scheme<MG_WENO>(g, a, maps, sm, s);
-    case MG_PPM: return launch_scheme<MG_PPM>(g, a, maps, sm, s);
-    case MG_LW: return launch_scheme<MG_LW>(g, a, maps, sm, s);
-    case MG_QUICK: return launch_scheme<MG_QUICK>(g, a, maps, sm, s);
-    default: return launch_scheme<MG_MUSCL>(g, a, maps, sm, s);
+    case MG_WENO: return launch_scheme<MG_WENO>(g, a, maps, s);
+    case MG_PPM: return launch_scheme<MG_PPM>(g, a, maps, s);
+    case MG_LW: return launch_scheme<MG_LW>(g, a, maps, s);
+    case MG_QUICK: return launch_scheme<MG_QUICK>(g, a, maps, s);
+    default: return launch_scheme<MG_MUSCL>(g, a, maps, s);
     }
 }
 
@@ -96,7 +96,7 @@ cudaError_t k1_init()
 cudaError_t launch_k1_group(int scheme, int stage, int nf, const K1Member *mem, const GItem *items, int nitems, cudaStream_t s)
 {
     if (nf <= 0 || nf > MG_MAXF || (stage != 1 && stage != 2) || nitems < 1) return cudaErrorInvalidValue;
-    if (make_layout(scheme, nf).total > 232448) return cudaErrorInvalidValue;
+    if (k1_smem_max(scheme, nf) > 232448) return cudaErrorInvalidValue;
     switch (scheme) {
     case MG_WENO: return group_scheme<MG_WENO>(stage, nf, mem, items, nitems, s);
     case MG_PPM: return group_scheme<MG_PPM>(stage, nf, mem, items, nitems, s);

@@ -81,14 +81,18 @@ __global__ void na_max_final(const double *partial, int n, double *out)
     if (threadIdx.x == 0) *out = sm[0];
 }
 
-// scratch address of the current device, resolved on first use
-int scratch_of_current_device(double **out)
+// scratch address of the current device.  Resolved again on every call outside a stream
+// capture (a device reset reloads the module, and the symbol can move); a capture uses
+// the address of the last call outside one, so that it issues no symbol lookup.
+int scratch_of_current_device(cudaStream_t s, double **out)
 {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return MG_ERR_CUDA;
     if (dev < 0 || dev >= NA_MAX_DEVICES) return MG_ERR_PARAM;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) return MG_ERR_CUDA;
     std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (!g_scratch[dev]) {
+    if (!g_scratch[dev] || cs == cudaStreamCaptureStatusNone) {
         double *p = nullptr;
         cudaError_t rc = cudaGetSymbolAddress((void **)&p, g_maxdiv_partials);
         if (rc != cudaSuccess || !p) return MG_ERR_CUDA;
@@ -106,13 +110,13 @@ extern "C" int mg_maxdiv_noalloc(int maxx, int maxy, int nz, double dx, double d
 {
     if (maxx < 1 || maxy < 1 || maxx > 4096 || maxy > 4096 || nz < 3 || nz > 4096) return MG_ERR_PARAM;
     if (!dz1w || !mu || !mv || !mw || !maxdiv || !(dx > 0.) || !(dy > 0.)) return MG_ERR_PARAM;
+    cudaStream_t s = (cudaStream_t)stream;
     double *partial = nullptr;
-    int st = scratch_of_current_device(&partial);
+    int st = scratch_of_current_device(s, &partial);
     if (st != MG_OK) return st;
     const long long tot = (long long)maxx * maxy * (nz - 2);
     long long nb = (tot + NA_THREADS - 1) / NA_THREADS;
     if (nb > NA_MAX_PARTIALS) nb = NA_MAX_PARTIALS;
-    cudaStream_t s = (cudaStream_t)stream;
     na_maxdiv_partial<<<(unsigned)nb, NA_THREADS, 0, s>>>(maxx, maxy, nz, dx, dy, dz1w, mu, mv, mw, partial);
     if (cudaGetLastError() != cudaSuccess) return MG_ERR_CUDA;
     na_max_final<<<1, NA_THREADS, 0, s>>>(partial, (int)nb, maxdiv);
