@@ -256,26 +256,24 @@ __device__ __forceinline__ void k1_run(const DevGrid &G, const K1Args &A, const 
         for (int m = 0; m < L + 2; m++) zsl[m] = (k - 1 + m) % ZS;
         const double d0 = ldg(G.den0, k - 1);
         const double rd0 = MIXED ? 1. / d0 : 0.;   // the mixed form multiplies by 1/rho0
-        // momentum boxes of level k -> face velocities.  Previous readers of su/sv (the
-        // faces of iteration k-1) passed that iteration's last face barrier.
+        // momentum boxes of level k -> face velocities.  Each thread converts the two
+        // velocities of its own faces (su[tid]: x face, sv[tid]: y face), so the faces need
+        // no barrier after this; the boxes are refilled for level k+1 after this level's
+        // first face barrier, which every thread passes after its conversion.
         if (!pro) {
-        mbar_wait_bounded(&mb[MB_VEL], (uint32_t)((k - kb) & 1), A.err);
-        for (int q = tid; q < TY * (TX + 1) + (TY + 1) * TX; q += NT) {
-            if (q < TY * (TX + 1)) {
-                int r = q / (TX + 1), c = q - r * (TX + 1);
+            mbar_wait_bounded(&mb[MB_VEL], (uint32_t)((k - kb) & 1), A.err);
+            if (tid < TY * (TX + 1)) {
+                const int r = tid / (TX + 1), c = tid - r * (TX + 1);
                 double m = vbu[r * VW + c + 1];
                 if (conv1) m = m * d0;
-                su[q] = (MIXED ? m * rd0 : m / d0) - G.u0shift;
-            } else {
-                int qq = q - TY * (TX + 1);
-                int r = qq / TX, c = qq - r * TX;
+                su[tid] = (MIXED ? m * rd0 : m / d0) - G.u0shift;
+            }
+            {
+                const int r = tid / TX, c = tid - r * TX;
                 double m = vbv[r * VW + c + 1];
                 if (conv1) m = m * d0;
-                sv[qq] = (MIXED ? m * rd0 : m / d0) - G.v0shift;
+                sv[tid] = (MIXED ? m * rd0 : m / d0) - G.v0shift;
             }
-        }
-        __syncthreads();   // su/sv complete; the momentum boxes are free again
-        if (tid == 0 && k + 1 <= ke) issue_vel(k + 1);
         }
 #pragma unroll 1
         for (int g = 0; g < NG; g++) {
@@ -394,7 +392,7 @@ __device__ __forceinline__ void k1_run(const DevGrid &G, const K1Args &A, const 
                         const bool hasx = tid < TY * (TX + 1);
                         const int rx = hasx ? tid / (TX + 1) : 0, cx = hasx ? tid - rx * (TX + 1) : 0;
                         const int ry = tid / TX, cy = tid - ry * TX;
-                        const double uu = su[hasx ? tid : 0], vv = sv[tid];
+                        const double uu = hasx ? su[tid] : 0., vv = sv[tid];   // the thread's own entries
                         const int bx = (rx + H) * SW + H + cx - 1;   // x(i0 + cx - 1) in row rx
                         const int by = (ry - 1 + H) * SW + H + cy;   // x(j0 + ry - 1) in column cy
                         double Fx, Fy;
@@ -462,6 +460,8 @@ __device__ __forceinline__ void k1_run(const DevGrid &G, const K1Args &A, const 
                     }
             }
             __syncthreads();   // faces of group qg complete
+            // every thread has read the momentum boxes of level k
+            if (g == 0 && tid == 0 && k + 1 <= ke) issue_vel(k + 1);
             }
             if (!cellt) continue;
 
