@@ -35,7 +35,6 @@ SOURCES = [
     ("k_momentum.cu", ["-fmad=false"]),
     ("k_momentum_mixed.cu", []),
     ("k_pressure.cu", ["-fmad=false"]),
-    ("k_pressure_mixed.cu", []),
     ("capi.cu", []),
     ("noalloc.cu", ["-fmad=false"]),
     ("k_adjoint.cu", ["-fmad=false"]),

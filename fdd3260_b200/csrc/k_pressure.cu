@@ -306,11 +306,71 @@ __device__ __forceinline__ void fft_x_fwd_run(const DevGrid &G, const FftPlan1 &
     };
     const int r0 = jb + 2 * pair, r1 = r0 + 1;
     double mx = 0., sm = 0.;
-    for (int t = lt; t < n; t += nt_pair) {
-        const double v0 = rhs(r0, t), v1 = rhs(r1, t);
-        mx = fmax(mx, fmax(fabs(v0), fabs(v1)));
-        sm += v0 + v1;
-        a[t] = mkc<C>((R)v0, (R)v1);
+    if (A.mode == 0) {
+        // rhs from the momentum, XU columns of both rows at a time: all their loads are
+        // issued before the arithmetic (the momentum and b's buffer do not overlap)
+        const double *__restrict__ mu = A.mu, *__restrict__ mv = A.mv, *__restrict__ mw = A.mw;
+        double *__restrict__ rb = A.rbuf;
+        const bool has0 = r0 < maxy, has1 = r1 < maxy, top = k >= G.nz;
+        const long long cr0 = gidx(G, 4, (has0 ? r0 : 0) + 4, k), cr1 = gidx(G, 4, (has1 ? r1 : 0) + 4, k);
+        const long long px = G.px, ps = G.ps;
+        const long long o0 = ((long long)(k - 1) * maxy + r0) * G.maxx, o1 = o0 + G.maxx;
+        constexpr int XU = 2;
+        for (int tb = lt; tb < n; tb += XU * nt_pair) {
+            double m0[XU][6], m1[XU][6];   // u(c), u(c+1), v(c), v(c+px), w(c), w(c+ps)
+#pragma unroll
+            for (int q = 0; q < XU; q++) {
+                const int t = tb + q * nt_pair;
+                if (t < n) {
+                    if (has0) {
+                        const long long c = cr0 + t;
+                        m0[q][0] = __ldg(mu + c); m0[q][1] = __ldg(mu + c + 1);
+                        m0[q][2] = __ldg(mv + c); m0[q][3] = __ldg(mv + c + px);
+                        m0[q][4] = __ldg(mw + c); m0[q][5] = top ? 0. : __ldg(mw + c + ps);
+                    }
+                    if (has1) {
+                        const long long c = cr1 + t;
+                        m1[q][0] = __ldg(mu + c); m1[q][1] = __ldg(mu + c + 1);
+                        m1[q][2] = __ldg(mv + c); m1[q][3] = __ldg(mv + c + px);
+                        m1[q][4] = __ldg(mw + c); m1[q][5] = top ? 0. : __ldg(mw + c + ps);
+                    }
+                }
+            }
+            // the divergence of caldiv in its order of terms; at the top w(nz+1) = 0
+            auto div = [&](const double *m) {
+                double d = 0.;
+                d = d + (m[1] - m[0]) * dx1;
+                d = d + (m[3] - m[2]) * dy1;
+                if (!top) d = d + (m[5] - m[4]) * dzw1;
+                else d = d + (0. - m[4]) * dzw1;
+                return d * rfac;
+            };
+#pragma unroll
+            for (int q = 0; q < XU; q++) {
+                const int t = tb + q * nt_pair;
+                if (t < n) {
+                    double v0 = 0., v1 = 0.;
+                    if (has0) {
+                        v0 = div(m0[q]);
+                        if (A.store_b) rb[o0 + t] = v0;
+                    }
+                    if (has1) {
+                        v1 = div(m1[q]);
+                        if (A.store_b) rb[o1 + t] = v1;
+                    }
+                    mx = fmax(mx, fmax(fabs(v0), fabs(v1)));
+                    sm += v0 + v1;
+                    a[t] = mkc<C>((R)v0, (R)v1);
+                }
+            }
+        }
+    } else {
+        for (int t = lt; t < n; t += nt_pair) {
+            const double v0 = rhs(r0, t), v1 = rhs(r1, t);
+            mx = fmax(mx, fmax(fabs(v0), fabs(v1)));
+            sm += v0 + v1;
+            a[t] = mkc<C>((R)v0, (R)v1);
+        }
     }
     if (A.store_b) {   // deterministic block sum of b: fixed shuffle tree, warps in order
         for (int o = 16; o > 0; o >>= 1) sm += __shfl_xor_sync(0xffffffffu, sm, o);
