@@ -364,6 +364,64 @@ __device__ __forceinline__ void fft_x_fwd_run(const DevGrid &G, const FftPlan1 &
                 }
             }
         }
+    } else if (A.mode == 2) {
+        // refinement residual r = (b - <b>_k) - A dp, both rows of a column at a time with
+        // their loads issued ahead of the arithmetic (poisson_apply's operands and order)
+        const double *__restrict__ dp = A.dp, *__restrict__ rb = A.rbuf;
+        const int maxx = G.maxx, nz = G.nz;
+        const long long lev = (long long)maxx * maxy;
+        const double idx2 = 1. / (G.dx * G.dx), idy2 = 1. / (G.dy * G.dy);
+        double dv;
+        if (k == 1) dv = -__ldg(A.dka) - __ldg(A.dkb);
+        else if (k == nz) dv = -__ldg(A.dka + nz - 1) + __ldg(A.dkb + nz - 1);
+        else dv = -__ldg(A.dka + k - 1);
+        const double akk = k > 1 ? __ldg(A.ak + k - 1) : 0., ckk = k < nz ? __ldg(A.ck + k - 1) : 0.;
+        const bool has[2] = {r0 < maxy, r1 < maxy};
+        constexpr int XU = 1;
+        for (int tb = lt; tb < n; tb += XU * nt_pair) {
+            double m[XU][2][8];   // b, x, xw, xe, xs, xn, x below, x above
+#pragma unroll
+            for (int q = 0; q < XU; q++) {
+                const int t = tb + q * nt_pair;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int jr = h == 0 ? r0 : r1;
+                    if (t < n && has[h]) {
+                        const double *pl = dp + (long long)(k - 1) * lev;
+                        const long long o = (long long)jr * maxx + t;
+                        m[q][h][0] = rb[(long long)(k - 1) * lev + o];
+                        m[q][h][1] = __ldg(pl + o);
+                        m[q][h][2] = __ldg(pl + (long long)jr * maxx + (t == 0 ? maxx - 1 : t - 1));
+                        m[q][h][3] = __ldg(pl + (long long)jr * maxx + (t == maxx - 1 ? 0 : t + 1));
+                        m[q][h][4] = __ldg(pl + (long long)(jr == 0 ? maxy - 1 : jr - 1) * maxx + t);
+                        m[q][h][5] = __ldg(pl + (long long)(jr == maxy - 1 ? 0 : jr + 1) * maxx + t);
+                        m[q][h][6] = k > 1 ? __ldg(pl + o - lev) : 0.;
+                        m[q][h][7] = k < nz ? __ldg(pl + o + lev) : 0.;
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < XU; q++) {
+                const int t = tb + q * nt_pair;
+                if (t < n) {
+                    double vv[2] = {0., 0.};
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        if (!has[h]) continue;
+                        const double *e = m[q][h];
+                        const double x = e[1];
+                        double v = (e[3] - 2. * x + e[2]) * idx2 + (e[5] - 2. * x + e[4]) * idy2;
+                        v += dv * x;
+                        if (k > 1) v += akk * e[6];
+                        if (k < nz) v += ckk * e[7];
+                        vv[h] = (e[0] - bmean) - v;
+                    }
+                    mx = fmax(mx, fmax(fabs(vv[0]), fabs(vv[1])));
+                    sm += vv[0] + vv[1];
+                    a[t] = mkc<C>((R)vv[0], (R)vv[1]);
+                }
+            }
+        }
     } else {
         for (int t = lt; t < n; t += nt_pair) {
             const double v0 = rhs(r0, t), v1 = rhs(r1, t);
