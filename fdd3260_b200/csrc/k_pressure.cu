@@ -147,6 +147,12 @@ template <> __device__ __forceinline__ void dft_small<double2, 5>(double2 *v, in
 template <> __device__ __forceinline__ void dft_small<float2, 5>(float2 *v, int inv) { dft5(v, inv); }
 
 // one Stockham stage of radix R: butterflies j = lt, lt+nt, ... < n/R; Ns = product of
+// Row buffers of the shared-memory transforms keep one padding element after every 8
+// (element i at i + i/8): the stride-R writes of a radix-8 stage (the first stage writes
+// every 8th element) then fall in distinct banks.
+__host__ __device__ constexpr int padded_len(int n) { return n + (n + 7) / 8; }
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 3); }
+
 // the earlier radices (ns_shift = log2 Ns when Ns is a power of two, else -1)
 template <typename C, int R>
 __device__ __forceinline__ void stockham_stage(const FftPlan1 &P, const C *a, C *b, int lt, int nt, int inv,
@@ -160,7 +166,7 @@ __device__ __forceinline__ void stockham_stage(const FftPlan1 &P, const C *a, C 
         const int tstep = kk * tmul;
         C v[R];
 #pragma unroll
-        for (int r = 0; r < R; r++) v[r] = a[j + r * nb];
+        for (int r = 0; r < R; r++) v[r] = a[pidx(j + r * nb)];
         if (tstep != 0) {
 #pragma unroll
             for (int r = 1; r < R; r++) v[r] = cmul(v[r], twid<C>(P, tstep * r, inv));
@@ -168,7 +174,7 @@ __device__ __forceinline__ void stockham_stage(const FftPlan1 &P, const C *a, C 
         dft_small<C, R>(v, inv);
         const int idxD = jq * Ns * R + kk;
 #pragma unroll
-        for (int r = 0; r < R; r++) b[idxD + r * Ns] = v[r];
+        for (int r = 0; r < R; r++) b[pidx(idxD + r * Ns)] = v[r];
     }
 }
 
@@ -210,6 +216,14 @@ __device__ __forceinline__ bool converged(const Skip &k)
 
 // -------------------- step 1: rhs + x transform --------------------
 constexpr int ROWS = 8;   // rows per x-transform block (4 packed pairs)
+// element (kx, c) of a [kx][ROWS] staging tile of the x transforms, c = 0..7 in a row of
+// its own: rows written at stride 8 by consecutive kx and read along c stay in distinct
+// banks with c permuted by kx (by kx/2 for 8-byte elements, two rows per 128 bytes)
+template <typename C>
+__device__ __forceinline__ int stg(int kx, int c)
+{
+    return kx * ROWS + (c ^ ((sizeof(C) == 16 ? kx : kx >> 1) & 7));
+}
 
 struct XArgs {
     int mode;                     // 0: rhs = div(m)/(dt0*rho0) from momentum; 1: external rhs in rbuf;
@@ -271,8 +285,9 @@ __device__ __forceinline__ void fft_x_fwd_run(const DevGrid &G, const FftPlan1 &
     const int jb = jg * ROWS;                       // first interior row (0-based)
     const int nt_pair = blockDim.x / (ROWS / 2);
     const int pair = threadIdx.x / nt_pair, lt = threadIdx.x % nt_pair;
-    C *ahalf = smc, *bhalf = smc + (ROWS / 2) * n;
-    C *a = ahalf + pair * n, *b = bhalf + pair * n;
+    const int np = padded_len(n);
+    C *ahalf = smc, *bhalf = smc + (ROWS / 2) * np;
+    C *a = ahalf + pair * np, *b = bhalf + pair * np;
     __shared__ unsigned long long bmax;
     __shared__ double wsum[32];
     if (converged(A.prev)) {   // uniform over the grid: nothing left to refine
@@ -360,7 +375,7 @@ __device__ __forceinline__ void fft_x_fwd_run(const DevGrid &G, const FftPlan1 &
                     }
                     mx = fmax(mx, fmax(fabs(v0), fabs(v1)));
                     sm += v0 + v1;
-                    a[t] = mkc<C>((R)v0, (R)v1);
+                    a[pidx(t)] = mkc<C>((R)v0, (R)v1);
                 }
             }
         }
@@ -418,7 +433,7 @@ __device__ __forceinline__ void fft_x_fwd_run(const DevGrid &G, const FftPlan1 &
                     }
                     mx = fmax(mx, fmax(fabs(vv[0]), fabs(vv[1])));
                     sm += vv[0] + vv[1];
-                    a[t] = mkc<C>((R)vv[0], (R)vv[1]);
+                    a[pidx(t)] = mkc<C>((R)vv[0], (R)vv[1]);
                 }
             }
         }
@@ -427,7 +442,7 @@ __device__ __forceinline__ void fft_x_fwd_run(const DevGrid &G, const FftPlan1 &
             const double v0 = rhs(r0, t), v1 = rhs(r1, t);
             mx = fmax(mx, fmax(fabs(v0), fabs(v1)));
             sm += v0 + v1;
-            a[t] = mkc<C>((R)v0, (R)v1);
+            a[pidx(t)] = mkc<C>((R)v0, (R)v1);
         }
     }
     if (A.store_b) {   // deterministic block sum of b: fixed shuffle tree, warps in order
@@ -452,12 +467,12 @@ __device__ __forceinline__ void fft_x_fwd_run(const DevGrid &G, const FftPlan1 &
     const int hn = n / 2;
     C *T = (res == a) ? bhalf : ahalf;
     for (int kx = lt; kx < nh; kx += nt_pair) {
-        C z = res[kx], w = res[(n - kx) % n];
+        C z = res[pidx(kx)], w = res[pidx((n - kx) % n)];
         C Av = mkc<C>((z.x + w.x) * (R)0.5, (z.y - w.y) * (R)0.5);
         C Bv = mkc<C>((z.y + w.y) * (R)0.5, (w.x - z.x) * (R)0.5);
         if (kx < hn) {
-            T[kx * ROWS + 2 * pair] = Av;
-            T[kx * ROWS + 2 * pair + 1] = Bv;
+            T[stg<C>(kx, 2 * pair)] = Av;
+            T[stg<C>(kx, 2 * pair + 1)] = Bv;
         } else {
             const long long base = ((long long)(k - 1) * nh + kx) * maxy;
             if (r0 < maxy) spec[base + r0] = Av;
@@ -466,8 +481,8 @@ __device__ __forceinline__ void fft_x_fwd_run(const DevGrid &G, const FftPlan1 &
     }
     __syncthreads();
     for (int e = threadIdx.x; e < hn * ROWS; e += blockDim.x) {
-        const int kx = e / ROWS, jr = jb + (e - kx * ROWS);
-        if (jr < maxy) spec[((long long)(k - 1) * nh + kx) * maxy + jr] = T[e];
+        const int kx = e / ROWS, c = e - kx * ROWS, jr = jb + c;
+        if (jr < maxy) spec[((long long)(k - 1) * nh + kx) * maxy + jr] = T[stg<C>(kx, c)];
     }
 }
 
@@ -492,14 +507,15 @@ __device__ __forceinline__ void fft_y_run(const FftPlan1 &P, void *spec_v, int n
     const int nt_row = blockDim.x / YROWS;
     const int rr = threadIdx.x / nt_row, lt = threadIdx.x % nt_row;
     const long long row = (long long)bid * YROWS + rr;
-    C *a = smc + rr * 2 * n, *b = a + n;
+    const int np = padded_len(n);
+    C *a = smc + rr * 2 * np, *b = a + np;
     const bool ok = row < nrows;
     if (ok)
-        for (int t = lt; t < n; t += nt_row) a[t] = spec[row * n + t];
+        for (int t = lt; t < n; t += nt_row) a[pidx(t)] = spec[row * n + t];
     __syncthreads();
     C *res = stockham<C>(P, a, b, lt, nt_row, inv);
     if (ok)
-        for (int t = lt; t < n; t += nt_row) spec[row * n + t] = res[t];
+        for (int t = lt; t < n; t += nt_row) spec[row * n + t] = res[pidx(t)];
 }
 template <typename C>
 __global__ void fft_y(DevGrid G, const __grid_constant__ FftPlan1 P, void *spec_v, int nrows, int inv, Skip sk)
@@ -765,34 +781,35 @@ __device__ __forceinline__ void fft_x_inv_run(const DevGrid &G, const FftPlan1 &
     const int jb = jg * ROWS;
     const int nt_pair = blockDim.x / (ROWS / 2);
     const int pair = threadIdx.x / nt_pair, lt = threadIdx.x % nt_pair;
-    C *ahalf = smc, *bhalf = smc + (ROWS / 2) * n;
-    C *a = ahalf + pair * n, *b = bhalf + pair * n;
+    const int np = padded_len(n);
+    C *ahalf = smc, *bhalf = smc + (ROWS / 2) * np;
+    C *a = ahalf + pair * np, *b = bhalf + pair * np;
     const int r0 = jb + 2 * pair, r1 = r0 + 1;
     // the block's half spectra for kx < n/2, 8 consecutive ky per kx, staged in the b half
     const int hn = n / 2;
     for (int e = threadIdx.x; e < hn * ROWS; e += blockDim.x) {
-        const int kx = e / ROWS, jr = jb + (e - kx * ROWS);
-        bhalf[e] = jr < maxy ? spec[((long long)(k - 1) * nh + kx) * maxy + jr] : mkc<C>(0, 0);
+        const int kx = e / ROWS, c = e - kx * ROWS, jr = jb + c;
+        bhalf[stg<C>(kx, c)] = jr < maxy ? spec[((long long)(k - 1) * nh + kx) * maxy + jr] : mkc<C>(0, 0);
     }
     __syncthreads();
     // rebuild Z_k = A_k + i B_k over the full circle from the half spectra
     for (int kx = lt; kx < nh; kx += nt_pair) {
         C Av, Bv;
         if (kx < hn) {
-            Av = bhalf[kx * ROWS + 2 * pair];
-            Bv = bhalf[kx * ROWS + 2 * pair + 1];
+            Av = bhalf[stg<C>(kx, 2 * pair)];
+            Bv = bhalf[stg<C>(kx, 2 * pair + 1)];
         } else {
             const long long base = ((long long)(k - 1) * nh + kx) * maxy;
             Av = r0 < maxy ? spec[base + r0] : mkc<C>(0, 0);
             Bv = r1 < maxy ? spec[base + r1] : mkc<C>(0, 0);
         }
-        a[kx] = mkc<C>(Av.x - Bv.y, Av.y + Bv.x);
-        if (kx > 0 && kx < n - kx) a[n - kx] = mkc<C>(Av.x + Bv.y, Bv.x - Av.y);
+        a[pidx(kx)] = mkc<C>(Av.x - Bv.y, Av.y + Bv.x);
+        if (kx > 0 && kx < n - kx) a[pidx(n - kx)] = mkc<C>(Av.x + Bv.y, Bv.x - Av.y);
     }
     __syncthreads();   // the b half is scratch for the transform from here on
     C *res = stockham<C>(P, a, b, lt, nt_pair, 1);
     for (int t = lt; t < n; t += nt_pair) {
-        C z = res[t];
+        C z = res[pidx(t)];
         const long long o0 = ((long long)(k - 1) * maxy + r0) * G.maxx + t, o1 = o0 + G.maxx;
         if (A.accumulate) {
             if (r0 < maxy) A.dp[o0] = A.dp[o0] + (double)z.x / A.scale_div;
@@ -1408,7 +1425,7 @@ static cudaError_t launch_x_fwd_t(const DevGrid &g, PressurePlan *pp, const XArg
 {
     int groups = (g.maxy + ROWS - 1) / ROWS;
     const int nt_pair = pp->xt;
-    size_t sm = (size_t)(ROWS / 2) * 2 * g.maxx * sizeof(C);
+    size_t sm = (size_t)(ROWS / 2) * 2 * padded_len(g.maxx) * sizeof(C);
     cudaError_t e = cudaFuncSetAttribute(fft_x_fwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     fft_x_fwd<C><<<g.nz * groups, nt_pair * (ROWS / 2), sm, s>>>(g, pp->px, a);
@@ -1469,7 +1486,7 @@ static cudaError_t pressure_solve_t(const DevGrid &g, PressurePlan *pp, int keep
     const int nh = g.maxx / 2 + 1;
     const int nrows = g.nz * nh;
     const int nt_row = pp->yt;
-    size_t smy = (size_t)YROWS * 2 * g.maxy * sizeof(C);
+    size_t smy = (size_t)YROWS * 2 * padded_len(g.maxy) * sizeof(C);
     e = cudaFuncSetAttribute(fft_y<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy);
     if (e != cudaSuccess) return e;
     // FP32 spectra of a length the warp-shuffle transform covers take it
@@ -1499,7 +1516,7 @@ static cudaError_t pressure_solve_t(const DevGrid &g, PressurePlan *pp, int keep
     if (e != cudaSuccess) return e;
     int groups = (g.maxy + ROWS - 1) / ROWS;
     const int nt_pair = pp->xt;
-    size_t smx = (size_t)(ROWS / 2) * 2 * g.maxx * sizeof(C);
+    size_t smx = (size_t)(ROWS / 2) * 2 * padded_len(g.maxx) * sizeof(C);
     e = cudaFuncSetAttribute(fft_x_inv<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
     if (e != cudaSuccess) return e;
     XInvArgs xa{};
@@ -1778,7 +1795,7 @@ void group_x(GroupProgram &P, const std::vector<GroupProjIn> &in, const std::vec
             const DevGrid &g = *in[sub[q]].G;
             nb[q] = g.nz * ((g.maxy + ROWS - 1) / ROWS);
             cost[q] = (double)g.maxx;
-            sm = std::max(sm, (size_t)(ROWS / 2) * 2 * g.maxx * sizeof(C));
+            sm = std::max(sm, (size_t)(ROWS / 2) * 2 * padded_len(g.maxx) * sizeof(C));
         }
         const std::vector<GItem> it = group_items(nb, cost);
         const int ni = (int)it.size(), threads = in[sub[0]].pp->xt * (ROWS / 2);
@@ -1829,7 +1846,7 @@ void group_solve(GroupProgram &P, const std::vector<GroupProjIn> &in, const Pass
         const int nh = g.maxx / 2 + 1;
         yt = std::max(yt, in[q].pp->yt);
         tb = std::max(tb, in[q].pp->tb);
-        smy = std::max(smy, (size_t)YROWS * 2 * g.maxy * sizeof(C));
+        smy = std::max(smy, (size_t)YROWS * 2 * padded_len(g.maxy) * sizeof(C));
         nby[q] = (g.nz * nh + YROWS - 1) / YROWS;
         cy[q] = (double)g.maxy;
         ct[q] = (double)g.nz;
