@@ -510,8 +510,22 @@ __device__ __forceinline__ void fft_y_run(const FftPlan1 &P, void *spec_v, int n
     const int np = padded_len(n);
     C *a = smc + rr * 2 * np, *b = a + np;
     const bool ok = row < nrows;
-    if (ok)
-        for (int t = lt; t < n; t += nt_row) a[pidx(t)] = spec[row * n + t];
+    if (ok) {   // YI elements per thread at a time, their loads issued before the shared stores
+        constexpr int YI = 8;
+        for (int t0 = lt; t0 < n; t0 += YI * nt_row) {
+            C v[YI];
+#pragma unroll
+            for (int q = 0; q < YI; q++) {
+                const int t = t0 + q * nt_row;
+                if (t < n) v[q] = spec[row * n + t];
+            }
+#pragma unroll
+            for (int q = 0; q < YI; q++) {
+                const int t = t0 + q * nt_row;
+                if (t < n) a[pidx(t)] = v[q];
+            }
+        }
+    }
     __syncthreads();
     C *res = stockham<C>(P, a, b, lt, nt_row, inv);
     if (ok)
@@ -759,6 +773,10 @@ __global__ void gam_kernel(DevGrid G, TriArgs T, double *gam, int *err)
 }
 
 // -------------------- step 5: inverse x transform --------------------
+__device__ __forceinline__ void prefetch_l2(const void *p)
+{
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
 struct XInvArgs {
     const void *spec;
     double *dp;          // [nz][maxy][maxx] real
@@ -787,9 +805,22 @@ __device__ __forceinline__ void fft_x_inv_run(const DevGrid &G, const FftPlan1 &
     const int r0 = jb + 2 * pair, r1 = r0 + 1;
     // the block's half spectra for kx < n/2, 8 consecutive ky per kx, staged in the b half
     const int hn = n / 2;
-    for (int e = threadIdx.x; e < hn * ROWS; e += blockDim.x) {
-        const int kx = e / ROWS, c = e - kx * ROWS, jr = jb + c;
-        bhalf[stg<C>(kx, c)] = jr < maxy ? spec[((long long)(k - 1) * nh + kx) * maxy + jr] : mkc<C>(0, 0);
+    // XI elements per thread at a time, all their loads issued before the shared stores
+    constexpr int XI = 8;
+    for (int e0 = threadIdx.x; e0 < hn * ROWS; e0 += XI * blockDim.x) {
+        C v[XI];
+#pragma unroll
+        for (int q = 0; q < XI; q++) {
+            const int e = e0 + q * blockDim.x;
+            const int kx = e / ROWS, jr = jb + (e - kx * ROWS);
+            v[q] = (e < hn * ROWS && jr < maxy) ? spec[((long long)(k - 1) * nh + kx) * maxy + jr] : mkc<C>(0, 0);
+        }
+#pragma unroll
+        for (int q = 0; q < XI; q++) {
+            const int e = e0 + q * blockDim.x;
+            const int kx = e / ROWS, c = e - kx * ROWS;
+            if (e < hn * ROWS) bhalf[stg<C>(kx, c)] = v[q];
+        }
     }
     __syncthreads();
     // rebuild Z_k = A_k + i B_k over the full circle from the half spectra
@@ -807,6 +838,13 @@ __device__ __forceinline__ void fft_x_inv_run(const DevGrid &G, const FftPlan1 &
         if (kx > 0 && kx < n - kx) a[pidx(n - kx)] = mkc<C>(Av.x + Bv.y, Bv.x - Av.y);
     }
     __syncthreads();   // the b half is scratch for the transform from here on
+    if (A.accumulate) {   // the rows dp is added to, brought into L2 while the transform runs
+        for (int t = lt; t < n; t += nt_pair) {
+            const long long o0 = ((long long)(k - 1) * maxy + r0) * G.maxx + t;
+            if (r0 < maxy) prefetch_l2(A.dp + o0);
+            if (r1 < maxy) prefetch_l2(A.dp + o0 + G.maxx);
+        }
+    }
     C *res = stockham<C>(P, a, b, lt, nt_pair, 1);
     for (int t = lt; t < n; t += nt_pair) {
         C z = res[pidx(t)];
@@ -876,18 +914,35 @@ __device__ __forceinline__ void level_sums_run(const DevGrid &G, const double *x
     double acc = 0., accd = 0.;
     // q = jy * maxx + ix runs from threadIdx.x in steps of blockDim.x; (ix, jy) advance
     // incrementally instead of by a division per element
+    // LI elements at a time: all their loads first, then the sums in element order
+    constexpr int LI = 8;
     int ix = (int)threadIdx.x % maxx, jy = (int)threadIdx.x / maxx;
-    for (; jy < maxy;) {
-        long long c = gidx(G, ix + 4, jy + 4, k);
-        double v = x[c];
-        acc += v;
-        if (out_mean_d) {
-            double wo = __ldg(xold + c);
-            if (old_rep >= 0) wo = rep_value(old_rep, wo, a0);
-            accd += (v - wo) / dt0;
+    while (jy < maxy) {
+        double v[LI], wo[LI];
+        bool in[LI];
+#pragma unroll
+        for (int q = 0; q < LI; q++) {
+            in[q] = jy < maxy;
+            v[q] = 0.;
+            wo[q] = 0.;
+            if (in[q]) {
+                const long long c = gidx(G, ix + 4, jy + 4, k);
+                v[q] = x[c];
+                if (out_mean_d) wo[q] = __ldg(xold + c);
+            }
+            ix += blockDim.x;
+            while (ix >= maxx) { ix -= maxx; ++jy; }
         }
-        ix += blockDim.x;
-        while (ix >= maxx) { ix -= maxx; ++jy; }
+#pragma unroll
+        for (int q = 0; q < LI; q++) {
+            if (!in[q]) continue;
+            acc += v[q];
+            if (out_mean_d) {
+                double w = wo[q];
+                if (old_rep >= 0) w = rep_value(old_rep, w, a0);
+                accd += (v[q] - w) / dt0;
+            }
+        }
     }
     s1[threadIdx.x] = acc;
     s2[threadIdx.x] = accd;
