@@ -970,11 +970,31 @@ __global__ void __launch_bounds__(LSUM_THREADS) level_sums(const __grid_constant
 __device__ __forceinline__ void subtract_level_mean_run(const DevGrid &G, double *x, const double *mean, int natural_w,
                                                         const int bid, const int nblk)
 {
-    const long long n = G.ps * G.nz;
-    for (long long t = (long long)bid * blockDim.x + threadIdx.x; t < n; t += (long long)nblk * blockDim.x) {
-        int k = (int)(t / G.ps) + 1;
-        const double v = x[t] - __ldg(mean + k - 1);
-        x[t] = natural_w ? v / __ldg(G.avden0 + k - 1) : v;
+    const long long n = G.ps * G.nz, ps = G.ps, stride = (long long)nblk * blockDim.x;
+    // the level of element t advances with t (one 64-bit division per thread, not per
+    // element), and SI elements per thread are loaded before any is written back
+    long long t = (long long)bid * blockDim.x + threadIdx.x;
+    long long k0 = t / ps, rem = t - k0 * ps;
+    constexpr int SI = 4;
+    while (t < n) {
+        double v[SI];
+        long long tt[SI];
+        int kk[SI];
+#pragma unroll
+        for (int q = 0; q < SI; q++) {
+            tt[q] = t;
+            kk[q] = (int)k0;
+            v[q] = t < n ? x[t] : 0.;
+            t += stride;
+            rem += stride;
+            while (rem >= ps) { rem -= ps; ++k0; }
+        }
+#pragma unroll
+        for (int q = 0; q < SI; q++) {
+            if (tt[q] >= n) break;
+            const double w = v[q] - __ldg(mean + kk[q]);
+            x[tt[q]] = natural_w ? w / __ldg(G.avden0 + kk[q]) : w;
+        }
     }
 }
 __global__ void subtract_level_mean(const __grid_constant__ DevGrid G, double *x, const double *mean, int natural_w)
