@@ -219,15 +219,17 @@ __device__ __forceinline__ void k2_run(const DevGrid &G, const K2Args &A, const 
             e_pw = ldg(A.p, idx - 1);
             e_ps = ldg(A.p, idx - G.px);
             if (G.with_buoy) {
-                e_dn = ldg(A.dens, idx);
-                e_es = ldg(A.es, idx);
-                e_fes = ldg(A.fes, idx);
-                if (A.qt) { e_qt = ldg(A.qt, idx); e_fqt = ldg(A.fqt, idx); }
+                e_dn = ldg_stream(A.dens + idx);
+                e_es = ldg_stream(A.es + idx);
+                e_fes = ldg_stream(A.fes + idx);
+                if (A.qt) { e_qt = ldg_stream(A.qt + idx); e_fqt = ldg_stream(A.fqt + idx); }
             }
-            if (A.stage != 1) { e_tu = A.tu[idx]; e_tv = A.tv[idx]; e_tw = A.tw[idx]; }
-            e_un = ldg(A.mu_n, idx);
-            e_vn = ldg(A.mv_n, idx);
-            e_wn = ldg(A.mw_n, idx);
+            // single-use operands are read without allocating L1 lines, which the level
+            // coefficients and the pressure's neighbours keep
+            if (A.stage != 1) { e_tu = ld_stream(A.tu + idx); e_tv = ld_stream(A.tv + idx); e_tw = ld_stream(A.tw + idx); }
+            e_un = ldg_stream(A.mu_n + idx);
+            e_vn = ldg_stream(A.mv_n + idx);
+            e_wn = ldg_stream(A.mw_n + idx);
         }
 #pragma unroll
         for (int d = -2; d <= 2; d++) lb[d + 2] = ring_m + (((k + d + NSLOT) % NSLOT) * 3) * PL + own;
