@@ -253,25 +253,31 @@ __device__ __forceinline__ void k1_run(const DevGrid &G, const K1Args &A, const 
     // cell's 1/dz and avden0 at level k+1, the vertical face's w), off the critical path
     // of the level's first faces (the mixed step 1863 -> 1902 Mcell-updates/s); the FP64
     // form loads them where they are used, its registers having no room for three more
-    double nd0 = 0., ndzw = 0., naw = 1.;
+    // (with their reciprocals, the context's 1/rho0 profiles, for the two divisions per
+    // level that the mixed form turns into products)
+    double nd0 = 0., ndzw = 0., naw = 1., nrd0 = 0., nraw = 1.;
     if constexpr (MIXED) {
         nd0 = ldg(G.den0, kp - 1);
+        nrd0 = ldg(G.rden0, kp - 1);
         ndzw = ldg(G.dz1w, kp - 1);
         naw = kp <= nz - 1 ? ldg(G.avden0, kp) : 1.;
+        nraw = kp <= nz - 1 ? ldg(G.ravden0, kp) : 1.;
     }
     for (int k = kp; k <= ke; k++) {
         const bool pro = k < kb;   // prologue level: its vertical face only
         k_cur = k;
-        const double lv_d0 = nd0, lv_dzw = ndzw, lv_aw = naw;
+        const double lv_d0 = nd0, lv_dzw = ndzw, lv_aw = naw, lv_rd0 = nrd0, lv_raw = nraw;
         if (MIXED && k + 1 <= ke) {
             nd0 = ldg(G.den0, k);
+            nrd0 = ldg(G.rden0, k);
             ndzw = ldg(G.dz1w, k);
             naw = k + 1 <= nz - 1 ? ldg(G.avden0, k + 1) : 1.;
+            nraw = k + 1 <= nz - 1 ? ldg(G.ravden0, k + 1) : 1.;
         }
 #pragma unroll
         for (int m = 0; m < L + 2; m++) zsl[m] = (k - 1 + m) % ZS;
         const double d0 = MIXED ? lv_d0 : ldg(G.den0, k - 1);
-        const double rd0 = MIXED ? 1. / d0 : 0.;   // the mixed form multiplies by 1/rho0
+        const double rd0 = MIXED ? lv_rd0 : 0.;   // the mixed form multiplies by 1/rho0
         // momentum boxes of level k -> face velocities.  Each thread converts the two
         // velocities of its own faces (su[tid]: x face, sv[tid]: y face), so the faces need
         // no barrier after this; the boxes are refilled for level k+1 after this level's
@@ -499,7 +505,7 @@ __device__ __forceinline__ void k1_run(const DevGrid &G, const K1Args &A, const 
                     const double a0 = MIXED ? lv_aw : ldg(G.avden0, k);
                     double x = wring[((k + 1) % ZS) * NCELL + cid];
                     if (conv1) x = x * a0;
-                    wz2 = x / a0;
+                    wz2 = MIXED ? x * lv_raw : x / a0;
                 } else {
                     wz2 = 0.;
                 }
