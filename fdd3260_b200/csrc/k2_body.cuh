@@ -124,7 +124,7 @@ __device__ __forceinline__ void k2_run(const DevGrid &G, const K2Args &A, const 
         const int slot = l % NSLOT;
         const double d0 = ldg(G.den0, l - 1), a0 = ldg(G.avden0, l - 1);
         // the mixed form multiplies by the level's reciprocal densities instead of dividing
-        const double rd0 = MIXED ? 1. / d0 : 0., ra0 = MIXED ? 1. / a0 : 0.;
+        const double rd0 = MIXED ? ldg(G.rden0, l - 1) : 0., ra0 = MIXED ? ldg(G.ravden0, l - 1) : 0.;
 #pragma unroll
         for (int arr = 0; arr < 3; arr++) {
             const double w = arr == 2 ? a0 : d0;
@@ -197,7 +197,7 @@ __device__ __forceinline__ void k2_run(const DevGrid &G, const K2Args &A, const 
     // segment below computes them
     if (kb > 1 && act && A.mode != 1) {
         const long long idm = gidx(G, i, j, kb - 1);
-        pp_below = ldg(A.p, idm) / ldg(G.den0, kb - 2);
+        pp_below = MIXED ? ldg(A.p, idm) * ldg(G.rden0, kb - 2) : ldg(A.p, idm) / ldg(G.den0, kb - 2);
         if (G.with_buoy)
             bb_prev = buoy_bb(kb - 1, ldg(A.dens, idm), ldg(A.es, idm), A.qt ? ldg(A.qt, idm) : 0., ldg(A.fes, idm),
                               A.qt ? ldg(A.fqt, idm) : 0.);
@@ -418,9 +418,19 @@ __device__ __forceinline__ void k2_run(const DevGrid &G, const K2Args &A, const 
 
         // ---------------- explicit pressure gradient (gradp on p/rho0) ----------------
         const double d0 = ldg(G.den0, k - 1), a0 = ldg(G.avden0, k - 1);
-        const double ppc = e_p / d0;
-        const double gpx = (ppc - e_pw / d0) * dx1d;
-        const double gpy = (ppc - e_ps / d0) * dy1d;
+        // p/rho0: the mixed form multiplies by the context's 1/rho0 profile (the same
+        // product at a segment's first level, above), the FP64 form divides
+        double ppc, gpx, gpy;
+        if constexpr (MIXED) {
+            const double rd0 = ldg(G.rden0, k - 1);
+            ppc = e_p * rd0;
+            gpx = (ppc - e_pw * rd0) * dx1d;
+            gpy = (ppc - e_ps * rd0) * dy1d;
+        } else {
+            ppc = e_p / d0;
+            gpx = (ppc - e_pw / d0) * dx1d;
+            gpy = (ppc - e_ps / d0) * dy1d;
+        }
         double gpz;
         if (k >= 2) gpz = (ppc - pp_below) * ldg(dz1, k - 2);
         else gpz = (double)MM(2, 0, 0, 0) / (dt0 * ldg(G.avden0, 0));
