@@ -867,17 +867,24 @@ __global__ void __launch_bounds__(XT_THREADS, 3)
 }
 
 // -------------------- step 6: correction --------------------
+// The blocks of a level are consecutive (corr_blocks_per_level of them), so a thread finds
+// its level and cell with 32-bit arithmetic; 1/dx and 1/dy come from the host.
+__host__ __device__ inline unsigned corr_blocks_per_level(const DevGrid &G, unsigned threads)
+{
+    return ((unsigned)G.maxx * (unsigned)G.maxy + threads - 1) / threads;
+}
 __device__ __forceinline__ void correction_run(const DevGrid &G, const double *dp, double *mu, double *mv, double *mw,
-                                               double *p, int natural_uv, const int bid)
+                                               double *p, int natural_uv, double dx1, double dy1, const int bid)
 {
     const int maxx = G.maxx, maxy = G.maxy;
-    const long long t = (long long)bid * blockDim.x + threadIdx.x;
-    if (t >= (long long)maxx * maxy * G.nz) return;
-    const int ix = (int)(t % maxx), jy = (int)((t / maxx) % maxy), k = (int)(t / ((long long)maxx * maxy)) + 1;
+    const unsigned plane = (unsigned)maxx * (unsigned)maxy, bpl = corr_blocks_per_level(G, blockDim.x);
+    const unsigned kl = (unsigned)bid / bpl;
+    const unsigned rem = ((unsigned)bid - kl * bpl) * blockDim.x + threadIdx.x;
+    if (rem >= plane || (int)kl >= G.nz) return;
+    const int k = (int)kl + 1, jy = (int)(rem / (unsigned)maxx), ix = (int)(rem - (unsigned)jy * (unsigned)maxx);
     const int i = ix + 4, j = jy + 4;
     auto DP = [&](int a, int b, int kk) { return __ldg(dp + ((long long)(kk - 1) * maxy + b) * maxx + a); };
     const double d0 = __ldg(G.den0 + k - 1), a0 = __ldg(G.avden0 + k - 1);
-    const double dx1 = 1. / G.dx, dy1 = 1. / G.dy;
     const double dpc = DP(ix, jy, k);
     const long long c = gidx(G, i, j, k);
     p[c] = p[c] + d0 * dpc;
@@ -894,9 +901,9 @@ __device__ __forceinline__ void correction_run(const DevGrid &G, const double *d
     mv[c] = natural_uv ? mvn / d0 : mvn;
 }
 __global__ void correction_kernel(const __grid_constant__ DevGrid G, const double *dp, double *mu, double *mv, double *mw,
-                                  double *p, int natural_uv)
+                                  double *p, int natural_uv, double dx1, double dy1)
 {
-    correction_run(G, dp, mu, mv, mw, p, natural_uv, blockIdx.x);
+    correction_run(G, dp, mu, mv, mw, p, natural_uv, dx1, dy1, blockIdx.x);
 }
 
 // -------------------- reductions --------------------
@@ -1093,21 +1100,24 @@ __global__ void interior_scatter(DevGrid G, const double *src, double *dst)
 struct HaloArgs { double *f[MG_MAXF]; int nf; };
 __device__ __forceinline__ void halo_fill_run(const DevGrid &G, const HaloArgs &H, const int bid, const int nblk)
 {
+    // 32-bit index arithmetic: at most 5 (nx + maxy) < 41,100 ghost cells per level and
+    // 4096 levels, below 2^31
     const int nx = G.nx, ny = G.ny, maxx = G.maxx, maxy = G.maxy;
-    const long long per_plane = 5LL * nx + 5LL * maxy;
-    const long long tot = per_plane * G.nz;
-    for (long long t = (long long)bid * blockDim.x + threadIdx.x; t < tot; t += (long long)nblk * blockDim.x) {
-        int k = (int)(t / per_plane) + 1;
-        long long g = t % per_plane;
+    const unsigned per_plane = 5u * (unsigned)nx + 5u * (unsigned)maxy;
+    const unsigned tot = per_plane * (unsigned)G.nz;
+    for (unsigned t = (unsigned)bid * blockDim.x + threadIdx.x; t < tot; t += (unsigned)nblk * blockDim.x) {
+        const unsigned kq = t / per_plane;
+        const int k = (int)kq + 1;
+        const unsigned g = t - kq * per_plane;
         int i, j;
-        if (g < 5LL * nx) {
-            int r = (int)(g / nx);
-            i = (int)(g % nx) + 1;
+        if (g < 5u * (unsigned)nx) {
+            const int r = (int)(g / (unsigned)nx);
+            i = (int)(g - (unsigned)r * (unsigned)nx) + 1;
             j = r < 3 ? r + 1 : ny - 4 + r;   // 1,2,3, ny-1, ny
         } else {
-            long long g2 = g - 5LL * nx;
-            j = (int)(g2 / 5) + 4;
-            int c = (int)(g2 % 5);
+            const unsigned g2 = g - 5u * (unsigned)nx;
+            j = (int)(g2 / 5u) + 4;
+            const int c = (int)(g2 - (g2 / 5u) * 5u);
             i = c < 3 ? c + 1 : nx - 4 + c;
         }
         int si = i <= 3 ? i + maxx : (i >= nx - 1 ? i - maxx : i);
@@ -1161,7 +1171,7 @@ struct XFwdMember { DevGrid G; FftPlan1 P; XArgs A; };
 struct YMember { FftPlan1 P; void *spec; int nrows, inv; Skip sk; };
 struct TriMember { DevGrid G; TriArgs T; };
 struct XInvMember { DevGrid G; FftPlan1 P; XInvArgs A; };
-struct CorrMember { DevGrid G; const double *dp; double *mu, *mv, *mw, *p; int natural_uv; };
+struct CorrMember { DevGrid G; const double *dp; double *mu, *mv, *mw, *p; int natural_uv; double dx1, dy1; };
 struct LevelMember { DevGrid G; double *w; const double *wold; int wold_rep; double *mean; int natural_w, nb; };
 struct HaloMember { DevGrid G; HaloArgs H; int nb; };
 
@@ -1202,7 +1212,7 @@ __global__ void correction_grp(const CorrMember *__restrict__ mem, const GItem *
 {
     const GItem g = it[blockIdx.x];
     const CorrMember &m = mem[g.m];
-    correction_run(m.G, m.dp, m.mu, m.mv, m.mw, m.p, m.natural_uv, g.b);
+    correction_run(m.G, m.dp, m.mu, m.mv, m.mw, m.p, m.natural_uv, m.dx1, m.dy1, g.b);
 }
 __global__ void __launch_bounds__(LSUM_THREADS) level_sums_grp(const LevelMember *__restrict__ mem,
                                                                const GItem *__restrict__ it)
@@ -1622,8 +1632,8 @@ cudaError_t launch_store_solution(const DevGrid &g, PressurePlan *pp, double *ou
 cudaError_t launch_correction(const DevGrid &g, PressurePlan *pp, double *mu, double *mv, double *mw, double *p,
                               int natural_uv, cudaStream_t s)
 {
-    long long n = (long long)g.maxx * g.maxy * g.nz;
-    correction_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, pp->dp, mu, mv, mw, p, natural_uv);
+    const unsigned nb = corr_blocks_per_level(g, 256) * (unsigned)g.nz;
+    correction_kernel<<<nb, 256, 0, s>>>(g, pp->dp, mu, mv, mw, p, natural_uv, 1. / g.dx, 1. / g.dy);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     double *f[4] = {mu, mv, mw, p};
@@ -2065,8 +2075,8 @@ void group_projection_t(GroupProgram &P, const std::vector<GroupProjIn> &in, int
             std::vector<GroupHaloIn> h(n);
             for (int q = 0; q < n; q++) {
                 const DevGrid &g = *in[q].G;
-                cm[q] = CorrMember{g, in[q].pp->dp, in[q].mu, in[q].mv, in[q].mw, in[q].p, finalize && last};
-                nb[q] = (int)(((long long)g.maxx * g.maxy * g.nz + 255) / 256);
+                cm[q] = CorrMember{g, in[q].pp->dp, in[q].mu, in[q].mv, in[q].mw, in[q].p, finalize && last, 1. / g.dx, 1. / g.dy};
+                nb[q] = (int)(corr_blocks_per_level(g, 256) * (unsigned)g.nz);
                 h[q].G = in[q].G;
                 h[q].nf = 4;
                 h[q].f[0] = in[q].mu; h[q].f[1] = in[q].mv; h[q].f[2] = in[q].mw; h[q].f[3] = in[q].p;
