@@ -102,6 +102,12 @@ def alg_bytes(nf_scalar: int, nsubp: int, sgs: bool = False) -> dict:
 MEASURED_TRAFFIC_PER_CELL = {"k1_scalar_advection": 211.3, "k2_momentum": 143.9}
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one stage-1 and one stage-2 launch at "
                   "384x384x64 (profiles/k1_k2_traffic_cumulus.md), per interior cell, times this launch's cells")
+# The same for an ensemble member (dry warm bubble, WENO, density + theta + one passive
+# scalar, SGS off) at 256x256x96, plain FP64 (the mixed form: K1 116.4, K2 131.4)
+MEMBER_TRAFFIC_PER_CELL = {"k1_scalar_advection": 118.4, "k2_momentum": 128.9}
+MEMBER_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one stage-1 and one stage-2 launch of "
+                         "a 256x256x96 warm-bubble member (profiles/k1_k2_traffic_warmbubble256x96.md), per interior "
+                         "cell, times this launch's cells")
 
 
 class ClockSampler:
@@ -575,14 +581,18 @@ def run_ensemble(args, ws, rank, local):
     dom = max((k for k in kern if k in ab), key=lambda k: kern[k][1])
     avg_ms = kern[dom][1] / kern[dom][0]
     achieved = ab[dom] * mb.domain.cells / (avg_ms / 1e3) / 1e9
-    # the traffic captures are of the 5-scalar cumulus workload; the profiled member's own
-    # field count and SGS setting decide whether they apply
-    measured = (args.scheme == "weno" and len(states[big].scal) == 5 and getattr(mb.domain, "sgs", None) is None
-                and dom in MEASURED_TRAFFIC_PER_CELL)
-    traffic = MEASURED_TRAFFIC_PER_CELL[dom] * mb.domain.cells if measured else None
+    # the traffic captures are of a warm-bubble member (two scalars) and of the 5-scalar
+    # cumulus workload; the profiled member's own field count and SGS setting decide which
+    # applies
+    nsc = len(states[big].scal)
+    plain = args.scheme == "weno" and getattr(mb.domain, "sgs", None) is None
+    table, src = ((MEMBER_TRAFFIC_PER_CELL, MEMBER_TRAFFIC_SOURCE) if nsc == 2 else
+                  (MEASURED_TRAFFIC_PER_CELL, TRAFFIC_SOURCE) if nsc == 5 else (None, None))
+    measured = plain and table is not None and dom in table
+    traffic = table[dom] * mb.domain.cells if measured else None
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "traffic_unit": "bytes per launch",
-            "traffic_source": TRAFFIC_SOURCE if measured else "no capture of this configuration",
+            "traffic_source": src if measured else "no capture of this configuration",
             "peak_source": pk_src, "algorithmic_bytes_per_cell": ab[dom], "avg_launch_ms": avg_ms,
             "measured_on": f"largest member of rank 0 ({mb.domain.maxx}x{mb.domain.maxy}x{mb.domain.nz}), eager",
             "step_frac": ab["step"] * total_cells * args.steps / (t_ms / 1e3) / 1e9 / pk["hbm_gbs"] / ws}
