@@ -690,7 +690,7 @@ __device__ __forceinline__ void k1_run(const DevGrid &G, const K1Args &A, const 
                         if constexpr (STAGE == 2) {
                             // get_scalars (funcpack.f90:488-542): natural value with the new density
                             if constexpr (MIXED) {   // one reciprocal per cell
-                                if (f == 0) { dn_new = xnew; rdn_new = 1. / xnew; }
+                                if (f == 0) { dn_new = xnew; rdn_new = rcp_nr(xnew); }
                                 A.xout[f][idx] = weighted ? xnew * rdn_new : xnew;
                             } else {
                                 if (f == 0) dn_new = xnew;

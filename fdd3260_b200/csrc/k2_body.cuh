@@ -187,11 +187,16 @@ __device__ __forceinline__ void k2_run(const DevGrid &G, const K2Args &A, const 
         }
         double est = esv + cdiag * dt0 * fesv;
         double qtt = A.qt ? qtv + cdiag * dt0 * fqtv : 0.;
-        double den1 = 1. / dn;
-        double pt = den1 * est;
         double sumh = 0.;
         double ref = ldg(G.pt0, k - 1) * (1. + epsm * ldg(G.qv0, k - 1));
-        return dn * grav * (pt * (1. + epsm * den1 * (qtt - sumh) - den1 * sumh) / ref - 1.);
+        if constexpr (MIXED) {   // reciprocals instead of the two divisions
+            const double den1 = rcp_nr(dn), pt = den1 * est;
+            return dn * grav * (pt * (1. + epsm * den1 * (qtt - sumh) - den1 * sumh) * rcp_nr(ref) - 1.);
+        } else {
+            double den1 = 1. / dn;
+            double pt = den1 * est;
+            return dn * grav * (pt * (1. + epsm * den1 * (qtt - sumh) - den1 * sumh) / ref - 1.);
+        }
     };
     // a segment above the surface: p/rho0 and the buoyancy of level kb-1, as the
     // segment below computes them

@@ -47,6 +47,21 @@ __host__ __device__ inline long long gidx(const DevGrid &g, int i, int j, int k)
 //             again at the start of the next one, so value = (x / w) * w.
 enum { REP_NAT = 0, REP_CONS = 1 };
 
+// 1/x for the mixed form's kernels: the FP32 hardware reciprocal refined by two Newton
+// steps r <- r (2 - x r) in FP64, which square the FP32 estimate's relative error
+// (about 2^-23) twice, to within a few ulps of the quotient 1/x; for x in FP32's normal
+// range (densities, reference temperatures).  The FP64 form divides.
+__device__ __forceinline__ double rcp_nr(double x)
+{
+    const float xf = (float)x;
+    float rf;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rf) : "f"(xf));
+    double r = (double)rf;
+    r = r * (2. - x * r);
+    r = r * (2. - x * r);
+    return r;
+}
+
 __device__ __forceinline__ double rep_value(int rep, double x, double w) {
     return rep == REP_NAT ? x * w : (x / w) * w;
 }
