@@ -1437,9 +1437,12 @@ void pressure_get_knobs(const PressurePlan *pp, PressureKnobs *k)
 
 bool pressure_knobs_valid(const DevGrid &g, const PressureKnobs &k)
 {
+    // thread counts: multiples of 8 (whole warps per block) within the launch limits, which
+    // covers the defaults (maxx/8 and maxy/8, clamped) as well as the tuner's powers of two
+    auto mult8_in = [](int v, int lo, int hi) { return v >= lo && v <= hi && v % 8 == 0; };
     auto pow2_in = [](int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; };
-    return radices_ok(g.maxx, k.xr, k.xst) && radices_ok(g.maxy, k.yr, k.yst) && pow2_in(k.xt, 8, XT_THREADS / (ROWS / 2)) &&
-           pow2_in(k.yt, 16, 128) && pow2_in(k.tb, 64, 256);
+    return radices_ok(g.maxx, k.xr, k.xst) && radices_ok(g.maxy, k.yr, k.yst) && mult8_in(k.xt, 8, XT_THREADS / (ROWS / 2)) &&
+           mult8_in(k.yt, 16, 128) && pow2_in(k.tb, 64, 256);
 }
 
 bool pressure_set_knobs(PressurePlan *pp, const DevGrid &g, const PressureKnobs &k)

@@ -198,8 +198,8 @@ int mg_profile_report(mg_ctx *ctx, char *buf, size_t len);
 typedef struct mg_tune {
     int x_nstage, x_radix[16];
     int y_nstage, y_radix[16];
-    int x_threads;      /* threads per packed pair of rows, x transforms: 8, 16, 32, 64 */
-    int y_threads;      /* threads per row, y transforms: 16, 32, 64, 128 */
+    int x_threads;      /* threads per packed pair of rows, x transforms: a multiple of 8 in [8, 64] */
+    int y_threads;      /* threads per row, y transforms: a multiple of 8 in [16, 128] */
     int tri_block;      /* threads per block, tridiagonal solve: 64, 128, 256 */
     int k1_segments;    /* scalar advection: k segments per 32 x 8 column tile (0: chosen per
                            launch from the grid by a wave model; PPM keeps whole columns) */

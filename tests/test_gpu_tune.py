@@ -80,12 +80,35 @@ def test_invalid_plans_rejected():
     with Mimica(d, nscal=1) as m:
         base = m.tune_get()
         for bad in (dict(base, x_radix=[8, 8]), dict(base, y_radix=[7, 3]), dict(base, x_threads=128),
-                    dict(base, y_threads=256), dict(base, tri_block=96), dict(base, x_radix=[6, 4]),
+                    dict(base, y_threads=256), dict(base, x_threads=12), dict(base, tri_block=96),
+                    dict(base, x_radix=[6, 4]),
                     dict(base, k1_segments=-1), dict(base, k1_segments=13), dict(base, k2_segments=-1),
                     dict(base, k2_segments=13)):
             with pytest.raises(_lib.MimicaError):
                 m.tune_set(bad)
         assert m.tune_get() == base
+
+
+def test_default_plan_round_trips_on_a_384_wide_grid():
+    """A grid whose maxx/8 and maxy/8 are not powers of two gets 48 threads per row of the
+    transforms by default; mg_tune_set takes that plan back (the bench's end-to-end leg
+    copies a plan from one context to another), and a step with it set again equals the
+    step before, bit for bit."""
+    d = config.warm_bubble_domain(384, 384, 8)
+    st = config.warm_bubble_state(d, seed=3, centre=(9600.0, 9600.0, 200.0), radius=150.0)
+    with Mimica(d, nscal=len(st.scal)) as m:
+        plan = m.tune_get()
+        assert plan["x_threads"] == 48 and plan["y_threads"] == 48
+        m.upload(st)
+        m.stepping(1, ntime0=1)
+        a = m.download()
+        m.tune_set(plan)
+        assert m.tune_get() == plan
+        m.upload(st)
+        m.stepping(1, ntime0=1)
+        b = m.download()
+    for x, y in zip(_fields(a), _fields(b)):
+        assert np.array_equal(x, y)
 
 
 def test_wisdom_replays_a_plan(tmp_path):
