@@ -461,11 +461,11 @@ int mg_time_adjoint(mg_ctx *ctx, int reps, double *out5);
  * mu, mv, mw: device pointers to momentum in the reference layout (nx = maxx+5,
  * ny = maxy+5, nz); dz1w: device pointer (nz); maxdiv: device pointer receiving the
  * result; stream: a cudaStream_t (or NULL for the legacy default stream).
- * Limits: maxx, maxy <= 4096, 3 <= nz <= 4096 (MG_ERR_PARAM beyond).  The first call
- * on a device resolves the scratch address and must precede any stream capture that
- * is to contain the call; the address is kept for the process's life, so the entry must
- * not be used across a cudaDeviceReset of that device; calls in flight together on one
- * device race on the scratch. */
+ * Limits: maxx, maxy <= 4096, 3 <= nz <= 4096 (MG_ERR_PARAM beyond).  A call outside
+ * a stream capture resolves the scratch address of the current device; a call inside
+ * a capture uses the address of that device's last call outside one, so make one call
+ * outside any capture first (again after a cudaDeviceReset of the device).  Calls in
+ * flight together on one device race on the scratch. */
 int mg_maxdiv_noalloc(int maxx, int maxy, int nz, double dx, double dy, const double *dz1w,
                       const double *mu, const double *mv, const double *mw, double *maxdiv,
                       void *stream);
